@@ -1,0 +1,194 @@
+/*
+ * mindgpu.h — C-ABI of libmindgpu.so, the B200 implementation of MIND.jl's
+ * per-micro-timestep simulation loop.
+ *
+ * The library sits where MIND.jl's runtime sits today: behind build!() the Julia
+ * host owns a packed, immutable ModelLayout (src/model/build.jl:101-115) and the
+ * runtime uploads it, runs INITIAL and steps it.  Every entry point below
+ * replaces one runtime seam of the reference:
+ *
+ *   mind_create       allocate_simulation(plan::ModelLayout)   src/runtime/initialize.jl:4-250
+ *   mind_initialize   initialize!(state)                       src/runtime/initialize.jl:270-429
+ *   mind_run          run!(state, stop; records, ...)          src/runtime/step.jl:4-74
+ *   mind_step         step!(state)                             src/runtime/step.jl:77-86
+ *   mind_get_trace    SimulationResult.traces                  src/runtime/recording.jl:256-295
+ *   mind_get_spikes   SimulationResult.spike_times/_sources    src/runtime/recording.jl:256-295
+ *   mind_read_voltage read_value(voltage_ref)                  src/runtime/state.jl:586-659
+ *   mind_inject_event inject_event!(state, connection, time)   src/runtime/state.jl:586-659
+ *   mind_destroy      release of SimulationState               src/runtime/state.jl:177-212
+ *
+ * Conventions follow the Julia side so that its arrays pass without copies:
+ * indices are 1-based (0 = none), mechanism data is column-major
+ * data[row, field] (src/model/utils/build.jl:96-101), times are ms, voltages mV,
+ * point currents nA, density currents mA/cm2, weights uS.
+ *
+ * Ownership: every pointer in MindLayout is read during mind_create only; the
+ * library copies what it needs into device memory it owns and frees at
+ * mind_destroy.  Outputs go to caller-provided host buffers.  A handle is
+ * not reentrant: one handle per host thread, as the reference keeps one
+ * SimulationState per Julia task (src/runtime/utils/step.jl:201-211).
+ *
+ * Status codes keep the reference's device error word
+ * (src/runtime/utils/step.jl:190-196) and add codes for conditions the
+ * library reports itself.  Any non-zero status from mind_run / mind_step
+ * leaves the handle uninitialized, as run! does (src/runtime/step.jl:67-70).
+ */
+#ifndef MINDGPU_H
+#define MINDGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MIND_ABI_VERSION 1
+
+/* Status codes. 3/5/6/8 are the reference's error-word codes. */
+enum {
+    MIND_OK = 0,
+    MIND_ECAPACITY = 3,   /* event ring, window inbox or spike record exhausted */
+    MIND_ESELFEVENT = 5,  /* invalid self-event delay or target */
+    MIND_ESINGULAR = 6,   /* zero or non-finite pivot in the cable solve */
+    MIND_ENONFINITE = 8,  /* non-finite voltage or mechanism state */
+    MIND_ETIMEOUT = 9,    /* a device wait exceeded its iteration budget */
+    MIND_ELAYOUT = 10,    /* layout rejected (unsupported mechanism, bad index, ...) */
+    MIND_ECUDA = 11,      /* CUDA runtime error; see mind_last_error */
+    MIND_EARG = 12        /* invalid argument or call order */
+};
+
+/* Numerical modes (mind_set_precision). */
+enum {
+    MIND_FP64 = 0,   /* everything in FP64; reproduces the FP64 oracle bit for bit */
+    MIND_MIXED = 1   /* FP32 gating and synaptic conductances; FP64 cable, voltage, clock */
+};
+
+/* Builtin mechanism kinds understood by the device kernels (the reference mod directory). */
+enum {
+    MIND_MECH_HH = 1,       /* mod/hh.mod       density  */
+    MIND_MECH_PAS = 2,      /* mod/pas.mod      density  */
+    MIND_MECH_EXPSYN = 3,   /* mod/ExpSyn.mod   point    */
+    MIND_MECH_EXP2SYN = 4,  /* mod/Exp2Syn.mod  point    */
+    MIND_MECH_NETSTIM = 5,  /* mod/NetStim.mod  artificial */
+    MIND_MECH_ICLAMP = 6    /* mod/IClamp.mod   point (electrode current) */
+};
+
+/*
+ * One mechanism group: the reference's MechanismPlan (src/model/build.jl:1-60)
+ * restricted to what the hot path reads.  Group order is significant: when
+ * several groups write the same node, their currents are accumulated in group
+ * order, and rows of one group in row order.
+ */
+typedef struct MindMechanism {
+    int32_t kind;                      /* MIND_MECH_* */
+    int32_t n_fields;                  /* columns of data */
+    int64_t rows;
+    const double *data;                /* column-major [rows x n_fields] initial values */
+    const char *const *field_names;    /* n_fields names, the MOD's own field names */
+    const int32_t *nodes;              /* [rows] 1-based node; 0 for artificial cells */
+    const uint64_t *logical_ids;       /* [rows] random-stream identity (micro/model.jl:510-530) */
+    uint64_t digest;                   /* first 16 hex digits of the MOD source SHA-256 */
+} MindMechanism;
+
+/*
+ * The packed micro layout: a POD view of ModelLayout.micro (MicroPlan,
+ * src/model/build.jl:15-60) plus the build! settings the step loop reads.
+ * Nodes may come in any order that forms a forest through `parent`
+ * (the reference passes its DHS permutation, src/model/micro/model.jl:989-1077);
+ * where the numerical result depends on an order (siblings eliminated into
+ * one parent, point processes on one node) the order is ascending index.
+ */
+typedef struct MindLayout {
+    int32_t abi_version;               /* MIND_ABI_VERSION */
+    int32_t secondorder;               /* build!(secondorder=); only 0 is supported */
+    int64_t n_nodes;
+    const int32_t *parent;             /* [n_nodes] 1-based, 0 = root */
+    const double *voltage;             /* [n_nodes] initial membrane voltage (mV) */
+    const double *area;                /* [n_nodes] um2 */
+    const double *capacitance;         /* [n_nodes] cm*area*1e-5 */
+    const double *axial;               /* [n_nodes] conductance to parent (uS) */
+    const double *axial_diagonal;      /* [n_nodes] sum of own and children's axial */
+
+    int32_t n_mechanisms;
+    const MindMechanism *mechanisms;
+
+    int64_t n_points;                  /* point processes and artificial cells */
+    const int32_t *point_group;        /* [n_points] 1-based mechanism index */
+    const int32_t *point_row;          /* [n_points] 1-based row in that group */
+
+    int64_t n_sources;                 /* spike sources (micro/model.jl:590-600) */
+    const int64_t *source_ids;         /* [n_sources] user-visible sid */
+    const int32_t *source_nodes;       /* [n_sources] 1-based detector node, 0 if event source */
+    const double *source_thresholds;   /* [n_sources] detector threshold (mV) */
+    const int32_t *source_points;      /* [n_sources] 1-based point whose net_event feeds it, 0 if none */
+
+    int64_t n_edges;                   /* NetCons, grouped by source (micro/model.jl:638-671) */
+    const int64_t *fanout_offsets;     /* [n_sources+1] 1-based CSR into the edge arrays */
+    const int32_t *edge_targets;       /* [n_edges] 1-based point index */
+    const double *edge_delays;         /* [n_edges] ms */
+    const double *edge_weights;        /* [n_edges] first NET_RECEIVE weight (uS) */
+
+    double dt;                         /* dt_micro (ms) */
+    double celsius;
+    uint64_t seed;                     /* build!(seed=) : Philox key */
+    int64_t event_capacity;            /* events per delivery bin (ring slot) */
+    int64_t spike_capacity;            /* recorded spikes per run */
+} MindLayout;
+
+/* A recorded quantity (RecordSpec, src/model/references.jl:4-12). */
+enum { MIND_RECORD_VOLTAGE = 1 };
+typedef struct MindRecord {
+    int32_t kind;                      /* MIND_RECORD_VOLTAGE */
+    int32_t node;                      /* 1-based node */
+} MindRecord;
+
+typedef struct MindHandle MindHandle;
+
+/* allocate_simulation: validate and pack the layout onto the current device. */
+int mind_create(const MindLayout *layout, MindHandle **out);
+
+/* initialize!: reset clocks, queues and detectors; run INITIAL blocks. */
+int mind_initialize(MindHandle *h);
+
+/* mind_set_precision: MIND_FP64 (default) or MIND_MIXED; takes effect at the next mind_initialize. */
+int mind_set_precision(MindHandle *h, int32_t mode);
+
+/*
+ * run!: advance `steps` micro steps, recording `records` at the starting
+ * boundary and after every step (steps+1 samples) and, when record_spikes is
+ * non-zero, every spike.  Results stay in the handle until the next run.
+ */
+int mind_run(MindHandle *h, int64_t steps, const MindRecord *records, int32_t n_records,
+             int32_t record_spikes);
+
+/* step!: one micro step without recording. */
+int mind_step(MindHandle *h);
+
+/* Current micro step count and simulation time (step * dt). */
+int mind_time(const MindHandle *h, int64_t *step, double *time);
+
+/* Traces of the last mind_run, sample-major [samples x n_records]; n must equal that size. */
+int mind_get_trace(const MindHandle *h, double *out, int64_t n);
+
+/* Spikes of the last mind_run, sorted by (time, sid); *n receives the count (also when cap is short). */
+int mind_get_spikes(const MindHandle *h, double *times, int64_t *sids, int64_t cap, int64_t *n);
+
+/* read_value for a voltage reference: v at a 1-based node. */
+int mind_read_voltage(const MindHandle *h, int32_t node, double *value);
+
+/* inject_event!: deliver connection `edge` (1-based) at absolute time t (ms, >= now). */
+int mind_inject_event(MindHandle *h, int64_t edge, double t);
+
+/* Message for the last non-zero status of this handle (or of mind_create when h is NULL). */
+const char *mind_last_error(const MindHandle *h);
+
+/* Device-side wall time of the last mind_run, in milliseconds (CUDA events). */
+int mind_last_run_ms(const MindHandle *h, double *ms);
+
+int mind_destroy(MindHandle *h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MINDGPU_H */

@@ -1,0 +1,140 @@
+/*
+ * device.cuh — device-side data layout and kernels of libmindgpu.so.
+ *
+ * Layout in HBM (built by mindgpu.cu from the C-ABI layout):
+ *   - Nodes are packed cell by cell.  Inside a cell, nodes are grouped into
+ *     chains (maximal unbranched paths: every node but the chain's top is the
+ *     only child of its parent), chains sorted by level (0 = ends in a leaf,
+ *     otherwise 1 + the highest level among its child chains), each chain's
+ *     nodes contiguous from top to bottom.  A cell is staged in shared memory
+ *     once per window of steps.
+ *   - Mechanism rows are structure-of-arrays per group, sorted by
+ *     (cell, local node, layout row) so a cell owns one contiguous row range
+ *     per group and rows on one node are adjacent (a "segment").
+ *   - Events live in a ring of delivery bins (bin m = the events NEURON's two
+ *     half-step deliveries hand to step m's currents, i.e. event times in
+ *     ((m-1) dt + dt/2, m dt + dt/2]).  Before a window, the bins of the
+ *     window are moved into per-cell inboxes; the cell sorts its inbox by
+ *     (bin, target, time, edge) and applies it in that order, which is the
+ *     heap order of the reference (src/runtime/utils/events.jl:7-62) for every
+ *     target.
+ *
+ * Arithmetic order in FP64 mode is the oracle's (oracle/mind_oracle.cpp):
+ * group order, row order inside a segment, own axial term before children,
+ * children in ascending layout index.  The file is compiled with -fmad=false
+ * so that no multiply-add is fused behind the source's back.
+ */
+#pragma once
+
+#include <cstdint>
+#include "mind_math.h"
+#include "../../include/mindgpu.h"
+
+namespace mind {
+
+constexpr int kMaxGroups = 16;
+constexpr int kThreads = 128;
+
+struct RingEvent {       // an event waiting in a delivery bin
+    double time;
+    int32_t edge;        // 0-based edge, -1 for an injected event without weight
+    int32_t point;       // 0-based point
+};
+
+struct InboxEvent {      // an event moved to its cell's window inbox
+    double time;
+    int32_t edge;
+    int32_t point;
+    int64_t bin;
+};
+
+struct DevGroup {
+    int32_t kind;
+    int32_t rows;
+    const int32_t *row_off;   // [ncells+1] per-cell row ranges
+    int32_t *node;            // local node per row
+    int32_t *seg;             // rows in the segment starting here (0 = not a segment head)
+    double *f[12];            // field arrays, meaning by kind (see mindgpu.cu)
+    float *s[4];              // FP32 state for mixed mode
+};
+
+/* Field slots per kind. */
+enum { HH_GNABAR, HH_GKBAR, HH_GL, HH_EL, HH_ENA, HH_EK, HH_SCALE, HH_M, HH_H, HH_N, HH_NSLOT };
+enum { PAS_G, PAS_E, PAS_SCALE, PAS_NSLOT };
+enum { ES_E, ES_G, ES_TAU, ES_DECAY, ES_NSLOT };
+enum { E2_E, E2_A, E2_B, E2_FACTOR, E2_TAU1, E2_TAU2, E2_DECAY1, E2_DECAY2, E2_NSLOT };
+enum { IC_DEL, IC_DUR, IC_AMP, IC_NSLOT };
+enum { NS_INTERVAL, NS_NUMBER, NS_START, NS_NOISE, NS_EVENT, NS_ON, NS_ISPIKE, NS_NEXT_T,
+       NS_NEXT_FLAG, NS_NSLOT };
+/* FP32 state slots (mixed mode). */
+enum { HHS_M, HHS_H, HHS_N };
+enum { ESS_G, ESS_DECAY };
+enum { E2S_A, E2S_B, E2S_DECAY1, E2S_DECAY2 };
+
+struct Params {
+    int32_t ncells;
+    int32_t ngroups;
+    double dt;
+    double celsius;
+    uint64_t seed;
+    // nodes (packed, local order)
+    const int64_t *node_off;   // [ncells+1]
+    double *v;
+    const double *a, *cdt, *ad;
+    const int32_t *parent;     // local parent index or -1
+    const int32_t *kid_off;    // [packed+1] global CSR over local kid indices
+    const int32_t *kids;
+    // chains
+    const int32_t *chain_off;  // [ncells+1]
+    const int32_t *chain_top, *chain_len, *chain_kid_off, *chain_kids;  // chain_kid_off global CSR
+    const int32_t *level_off;  // [ncells+1] into level_chain
+    const int32_t *level_chain;  // per cell: nlevels+1 entries of local chain starts
+    DevGroup groups[kMaxGroups];
+    // detectors
+    const int32_t *det_off;    // [ncells+1]
+    const int32_t *det_node;   // local node
+    const int32_t *det_source; // 0-based source
+    const double *det_thr;
+    uint8_t *above;            // per source
+    // window spikes (cell detectors)
+    int32_t *win_spike_source;
+    int64_t *win_spike_step;
+    int32_t *win_spike_count;
+    int32_t win_spike_cap;
+    // recorded spikes
+    int32_t *rec_spike_source;
+    double *rec_spike_time;
+    int32_t *rec_spike_count;
+    int32_t rec_spike_cap;
+    int32_t record_spikes;
+    // events
+    RingEvent *ring;
+    int32_t *ring_count;
+    int32_t ring_slots;
+    int32_t ring_cap;
+    InboxEvent *inbox;
+    int32_t *inbox_count;
+    int32_t inbox_cap;
+    const double *edge_weight;
+    const double *edge_delay;
+    const int32_t *edge_target;    // 0-based point
+    const int64_t *fanout_off;     // [nsources+1] 0-based
+    const int32_t *point_cell;     // per point
+    const int32_t *point_group;    // per point, 0-based
+    const int32_t *point_row;      // per point, device row
+    // NetStim
+    int32_t ns_group;              // -1 if none
+    MindRan *ns_ran;
+    const int32_t *ns_source;      // per NetStim row: 0-based source or -1
+    // recording
+    const int32_t *rec_off;        // [ncells+1]
+    const int32_t *rec_node;       // local node
+    const int32_t *rec_col;
+    double *trace;
+    int32_t nrec;
+    int64_t trace_samples;
+    int64_t run_start;             // step at sample 0
+    int32_t *error;
+};
+
+}  // namespace mind

@@ -1,0 +1,872 @@
+/*
+ * mindgpu.cu — host runtime and C-ABI of libmindgpu.so (include/mindgpu.h).
+ *
+ * mind_create validates the layout and packs it for the device:
+ *   cells      connected components of the parent forest;
+ *   chains     per cell, maximal unbranched paths, ordered by level so that a
+ *              level's chains can be eliminated in parallel after the level
+ *              below (the role of the reference's DHS rounds,
+ *              src/model/micro/model.jl:906-1077);
+ *   kids       per node, children in ascending layout index (the order in
+ *              which their axial currents and eliminated pivots are added);
+ *   rows       mechanism rows per group sorted by (cell, node, layout row);
+ *   events     a ring of delivery bins sized for the longest NetCon delay.
+ * mind_run advances in windows of W steps, W bounded by the shortest NetCon
+ * delay out of a cell detector: a spike detected inside a window can only be
+ * delivered after it, so each cell advances a whole window on its own.
+ */
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+
+using namespace mind;
+
+namespace {
+
+constexpr int32_t kMaxWindow = 64;
+thread_local std::string g_create_error;
+
+struct DeviceBuffers {
+    std::vector<void *> owned;
+    ~DeviceBuffers() {
+        for (void *p : owned) cudaFree(p);
+    }
+};
+
+}  // namespace
+
+struct MindHandle {
+    // host copies
+    int32_t ncells = 0;
+    int64_t n_nodes = 0;
+    double dt = 0.0;
+    std::vector<int64_t> packed_of_layout;   // layout node -> packed index
+    std::vector<int64_t> node_off;           // [ncells+1] packed node ranges
+    std::vector<int32_t> edge_target;        // 0-based point per edge
+    std::vector<double> v0_packed;
+    int64_t n_sources = 0;
+    std::vector<int64_t> source_ids;
+    int32_t precision = MIND_FP64;
+    bool initialized = false;
+    int64_t step = 0;
+    int32_t window = 1;
+    int32_t max_delay_bins = 0;
+    std::string error;
+    double last_ms = 0.0;
+    // per-group initial data for restore at initialize
+    struct GroupInit {
+        int32_t kind;
+        int32_t rows;
+        std::vector<std::vector<double>> f;   // device slot order
+        uint64_t digest;
+        std::vector<uint64_t> logical;        // device row order (NetStim)
+    };
+    std::vector<GroupInit> group_init;
+    // results
+    std::vector<double> trace;
+    int64_t trace_samples = 0;
+    int32_t trace_records = 0;
+    std::vector<double> spike_times;
+    std::vector<int64_t> spike_sids;
+    // device
+    DeviceBuffers buffers;
+    Params P{};
+    uint64_t *ns_logical = nullptr;
+    size_t smem_bytes = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+    int32_t *rec_off_dev = nullptr;
+    int32_t *rec_node_dev = nullptr;
+    int32_t *rec_col_dev = nullptr;
+    int64_t *rec_global_dev = nullptr;
+    double *trace_dev = nullptr;
+    size_t trace_capacity = 0;
+    size_t rec_capacity = 0;
+
+    template <class T>
+    T *alloc(size_t count) {
+        void *p = nullptr;
+        if (count == 0) count = 1;
+        if (cudaMalloc(&p, count * sizeof(T)) != cudaSuccess) throw std::bad_alloc();
+        buffers.owned.push_back(p);
+        return static_cast<T *>(p);
+    }
+    template <class T>
+    T *upload(const std::vector<T> &host) {
+        T *p = alloc<T>(host.size());
+        if (!host.empty() &&
+            cudaMemcpy(p, host.data(), host.size() * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess)
+            throw std::bad_alloc();
+        return p;
+    }
+    void release(void *p) {
+        if (!p) return;
+        auto it = std::find(buffers.owned.begin(), buffers.owned.end(), p);
+        if (it != buffers.owned.end()) buffers.owned.erase(it);
+        cudaFree(p);
+    }
+};
+
+namespace {
+
+int fail(MindHandle *h, int code, const std::string &why) {
+    if (h) {
+        h->error = why;
+        if (code != MIND_ELAYOUT && code != MIND_EARG) h->initialized = false;
+    } else {
+        g_create_error = why;
+    }
+    return code;
+}
+
+int cuda_fail(MindHandle *h, cudaError_t e, const char *where) {
+    return fail(h, MIND_ECUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define CUDA_TRY(h, call)                                          \
+    do {                                                           \
+        cudaError_t _e = (call);                                   \
+        if (_e != cudaSuccess) return cuda_fail((h), _e, #call);   \
+    } while (0)
+
+int field_index(const MindMechanism &m, const char *name) {
+    for (int32_t j = 0; j < m.n_fields; ++j)
+        if (m.field_names && m.field_names[j] && std::strcmp(m.field_names[j], name) == 0) return j;
+    return -1;
+}
+
+struct KindSpec {
+    int32_t kind;
+    std::vector<const char *> fields;   // layout fields copied to device slots 0..k-1
+    int32_t nslot;
+    int32_t nfloat;
+};
+
+KindSpec spec_of(int32_t kind) {
+    switch (kind) {
+        case MIND_MECH_HH:
+            return {kind, {"gnabar", "gkbar", "gl", "el", "ena", "ek"}, HH_NSLOT, 3};
+        case MIND_MECH_PAS:
+            return {kind, {"g", "e"}, PAS_NSLOT, 0};
+        case MIND_MECH_EXPSYN:
+            return {kind, {"e", "g", "tau"}, ES_NSLOT, 2};
+        case MIND_MECH_EXP2SYN:
+            return {kind, {"e", "A", "B", "factor", "tau1", "tau2"}, E2_NSLOT, 4};
+        case MIND_MECH_ICLAMP:
+            return {kind, {"del", "dur", "amp"}, IC_NSLOT, 0};
+        case MIND_MECH_NETSTIM:
+            return {kind, {"interval", "number", "start", "noise", "event", "on", "ispike"}, NS_NSLOT, 0};
+        default:
+            return {0, {}, 0, 0};
+    }
+}
+
+/* Device slot of each copied layout field (same order as spec_of fields). */
+int slot_of(int32_t kind, int k) {
+    static const int hh[] = {HH_GNABAR, HH_GKBAR, HH_GL, HH_EL, HH_ENA, HH_EK};
+    static const int pas[] = {PAS_G, PAS_E};
+    static const int es[] = {ES_E, ES_G, ES_TAU};
+    static const int e2[] = {E2_E, E2_A, E2_B, E2_FACTOR, E2_TAU1, E2_TAU2};
+    static const int ic[] = {IC_DEL, IC_DUR, IC_AMP};
+    static const int ns[] = {NS_INTERVAL, NS_NUMBER, NS_START, NS_NOISE, NS_EVENT, NS_ON, NS_ISPIKE};
+    switch (kind) {
+        case MIND_MECH_HH: return hh[k];
+        case MIND_MECH_PAS: return pas[k];
+        case MIND_MECH_EXPSYN: return es[k];
+        case MIND_MECH_EXP2SYN: return e2[k];
+        case MIND_MECH_ICLAMP: return ic[k];
+        case MIND_MECH_NETSTIM: return ns[k];
+        default: return 0;
+    }
+}
+
+int launch_grid(int64_t work) {
+    int64_t blocks = (work + kThreads - 1) / kThreads;
+    if (blocks < 1) blocks = 1;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    return (int)blocks;
+}
+
+int create(const MindLayout *L, MindHandle *h) {
+    if (!L) return fail(h, MIND_EARG, "null layout");
+    if (L->abi_version != MIND_ABI_VERSION) return fail(h, MIND_ELAYOUT, "ABI version mismatch");
+    if (L->secondorder != 0) return fail(h, MIND_ELAYOUT, "only secondorder = 0 is supported");
+    if (!(L->dt > 0.0) || !std::isfinite(L->dt)) return fail(h, MIND_ELAYOUT, "dt must be positive");
+    if (L->n_mechanisms > kMaxGroups) return fail(h, MIND_ELAYOUT, "too many mechanism groups");
+    const int64_t n = L->n_nodes;
+    if (n < 0 || n >= INT32_MAX) return fail(h, MIND_ELAYOUT, "node count out of range");
+    h->n_nodes = n;
+    h->dt = L->dt;
+
+    // ---- cells and children (ascending layout index) ----
+    std::vector<int32_t> parent(n);
+    for (int64_t i = 0; i < n; ++i) {
+        int32_t p = L->parent[i];
+        if (p < 0 || p > n || p == i + 1) return fail(h, MIND_ELAYOUT, "parent index out of range");
+        parent[i] = p - 1;
+    }
+    std::vector<int64_t> child_off(n + 1, 0);
+    for (int64_t i = 0; i < n; ++i)
+        if (parent[i] >= 0) child_off[parent[i] + 1]++;
+    for (int64_t i = 0; i < n; ++i) child_off[i + 1] += child_off[i];
+    std::vector<int32_t> child(child_off[n]);
+    {
+        std::vector<int64_t> cur(child_off.begin(), child_off.end() - 1);
+        for (int64_t i = 0; i < n; ++i)
+            if (parent[i] >= 0) child[cur[parent[i]]++] = (int32_t)i;
+    }
+    std::vector<int64_t> node_off{0};
+    std::vector<int32_t> layout_of_packed;
+    layout_of_packed.reserve(n);
+    std::vector<int32_t> cell_of(n, -1);
+    std::vector<int32_t> chain_off{0}, chain_top, chain_len, chain_kid_off{0}, chain_kids;
+    std::vector<int32_t> level_off{0}, level_chain;
+    std::vector<int32_t> parent_local, kid_off{0}, kids;
+    h->packed_of_layout.assign(n, -1);
+    int64_t max_nodes = 0, max_chains = 0;
+    for (int64_t root = 0; root < n; ++root) {
+        if (parent[root] >= 0) continue;
+        const int32_t cell = (int32_t)(node_off.size() - 1);
+        // BFS over the cell
+        std::vector<int32_t> bfs{(int32_t)root};
+        for (size_t k = 0; k < bfs.size(); ++k) {
+            cell_of[bfs[k]] = cell;
+            for (int64_t c = child_off[bfs[k]]; c < child_off[bfs[k] + 1]; ++c) bfs.push_back(child[c]);
+        }
+        // chains: a node starts a chain unless it is the only child of its parent
+        auto only_child = [&](int32_t i) {
+            return parent[i] >= 0 && child_off[parent[i] + 1] - child_off[parent[i]] == 1;
+        };
+        std::vector<int32_t> tops;
+        for (int32_t i : bfs)
+            if (!only_child(i)) tops.push_back(i);
+        std::vector<std::vector<int32_t>> chains(tops.size());
+        // top node -> chain id, by binary search over (top, id) pairs
+        std::vector<std::pair<int32_t, int32_t>> top_id;
+        top_id.reserve(tops.size());
+        for (size_t k = 0; k < tops.size(); ++k) {
+            int32_t i = tops[k];
+            chains[k].push_back(i);
+            while (child_off[i + 1] - child_off[i] == 1) {
+                i = child[child_off[i]];
+                chains[k].push_back(i);
+            }
+            top_id.push_back({tops[k], (int32_t)k});
+        }
+        std::sort(top_id.begin(), top_id.end());
+        auto chain_id_of = [&](int32_t top) {
+            auto it = std::lower_bound(top_id.begin(), top_id.end(), std::make_pair(top, INT32_MIN));
+            return it->second;
+        };
+        // levels: children chains first (tops in reverse BFS order are processed after their subtrees)
+        std::vector<int32_t> level(tops.size(), 0);
+        for (size_t k = tops.size(); k-- > 0;) {
+            int32_t bottom = chains[k].back();
+            int32_t lv = 0;
+            for (int64_t c = child_off[bottom]; c < child_off[bottom + 1]; ++c)
+                lv = std::max(lv, level[chain_id_of(child[c])] + 1);
+            level[k] = lv;
+        }
+        std::vector<int32_t> order(tops.size());
+        for (size_t k = 0; k < order.size(); ++k) order[k] = (int32_t)k;
+        std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) { return level[x] < level[y]; });
+        std::vector<int32_t> rank(tops.size());
+        for (size_t k = 0; k < order.size(); ++k) rank[order[k]] = (int32_t)k;
+        // packed order: chains by rank, nodes top -> bottom
+        const int64_t base = (int64_t)layout_of_packed.size();
+        std::vector<int32_t> local_chain_top(tops.size());
+        for (size_t k = 0; k < order.size(); ++k) {
+            const auto &ch = chains[order[k]];
+            local_chain_top[k] = (int32_t)(layout_of_packed.size() - base);
+            for (int32_t i : ch) {
+                h->packed_of_layout[i] = (int64_t)layout_of_packed.size();
+                layout_of_packed.push_back(i);
+            }
+        }
+        const int64_t cell_nodes = (int64_t)layout_of_packed.size() - base;
+        node_off.push_back((int64_t)layout_of_packed.size());
+        max_nodes = std::max(max_nodes, cell_nodes);
+        max_chains = std::max(max_chains, (int64_t)tops.size());
+        for (int64_t j = base; j < base + cell_nodes; ++j) {
+            int32_t i = layout_of_packed[j];
+            parent_local.push_back(parent[i] >= 0 ? (int32_t)(h->packed_of_layout[parent[i]] - base) : -1);
+            for (int64_t c = child_off[i]; c < child_off[i + 1]; ++c)
+                kids.push_back((int32_t)(h->packed_of_layout[child[c]] - base));
+            kid_off.push_back((int32_t)kids.size());
+        }
+        for (size_t k = 0; k < order.size(); ++k) {
+            const auto &ch = chains[order[k]];
+            chain_top.push_back(local_chain_top[k]);
+            chain_len.push_back((int32_t)ch.size());
+            int32_t bottom = ch.back();
+            for (int64_t c = child_off[bottom]; c < child_off[bottom + 1]; ++c)
+                chain_kids.push_back(rank[chain_id_of(child[c])]);
+            chain_kid_off.push_back((int32_t)chain_kids.size());
+        }
+        chain_off.push_back((int32_t)chain_top.size());
+        int32_t nlev = 0;
+        for (int32_t lv : level) nlev = std::max(nlev, lv + 1);
+        for (int32_t lv = 0, k = 0; lv <= nlev; ++lv) {
+            while (k < (int32_t)order.size() && level[order[k]] < lv) ++k;
+            level_chain.push_back(k);
+        }
+        level_off.push_back((int32_t)level_chain.size());
+    }
+    if ((int64_t)layout_of_packed.size() != n) return fail(h, MIND_ELAYOUT, "parent links form a cycle");
+    const int32_t ncells = (int32_t)(node_off.size() - 1);
+    h->ncells = ncells;
+    h->node_off = node_off;
+
+    // ---- node coefficients in packed order ----
+    std::vector<double> a(n), cdt(n), ad(n), v0(n);
+    for (int64_t j = 0; j < n; ++j) {
+        int32_t i = layout_of_packed[j];
+        a[j] = L->axial[i];
+        cdt[j] = L->capacitance[i] / L->dt;
+        ad[j] = L->axial_diagonal[i];
+        v0[j] = L->voltage[i];
+    }
+    h->v0_packed = v0;
+
+    // ---- mechanism groups ----
+    Params &P = h->P;
+    P.ncells = ncells;
+    P.ngroups = L->n_mechanisms;
+    P.dt = L->dt;
+    P.celsius = L->celsius;
+    P.seed = L->seed;
+    P.ns_group = -1;
+    std::vector<std::vector<int32_t>> dev_row_of(L->n_mechanisms);  // layout row -> device row
+    std::vector<std::vector<int32_t>> row_cell(L->n_mechanisms);
+    for (int32_t g = 0; g < L->n_mechanisms; ++g) {
+        const MindMechanism &m = L->mechanisms[g];
+        KindSpec spec = spec_of(m.kind);
+        if (!spec.kind) return fail(h, MIND_ELAYOUT, "unsupported mechanism kind " + std::to_string(m.kind));
+        if (m.rows < 0 || m.rows >= INT32_MAX) return fail(h, MIND_ELAYOUT, "mechanism rows out of range");
+        const int32_t rows = (int32_t)m.rows;
+        std::vector<int> src(spec.fields.size());
+        for (size_t k = 0; k < spec.fields.size(); ++k) {
+            src[k] = field_index(m, spec.fields[k]);
+            if (src[k] < 0)
+                return fail(h, MIND_ELAYOUT, std::string("mechanism lacks field ") + spec.fields[k]);
+        }
+        const bool artificial = m.kind == MIND_MECH_NETSTIM;
+        if (artificial) {
+            if (P.ns_group >= 0) return fail(h, MIND_ELAYOUT, "more than one NetStim group");
+            P.ns_group = g;
+        }
+        // sort rows by (cell, local node, layout row)
+        std::vector<int64_t> key(rows);
+        for (int32_t r = 0; r < rows; ++r) {
+            int32_t node = m.nodes[r];
+            if (artificial) {
+                if (node != 0) return fail(h, MIND_ELAYOUT, "artificial cell with a node");
+                key[r] = r;
+            } else {
+                if (node < 1 || node > n) return fail(h, MIND_ELAYOUT, "mechanism node out of range");
+                key[r] = h->packed_of_layout[node - 1];
+            }
+        }
+        std::vector<int32_t> perm(rows);
+        for (int32_t r = 0; r < rows; ++r) perm[r] = r;
+        std::stable_sort(perm.begin(), perm.end(), [&](int32_t x, int32_t y) { return key[x] < key[y]; });
+        dev_row_of[g].assign(rows, 0);
+        for (int32_t r = 0; r < rows; ++r) dev_row_of[g][perm[r]] = r;
+        MindHandle::GroupInit init;
+        init.kind = m.kind;
+        init.rows = rows;
+        init.digest = m.digest;
+        init.f.assign(spec.nslot, std::vector<double>(rows, 0.0));
+        for (size_t k = 0; k < spec.fields.size(); ++k) {
+            int slot = slot_of(m.kind, (int)k);
+            for (int32_t r = 0; r < rows; ++r) init.f[slot][r] = m.data[(int64_t)src[k] * m.rows + perm[r]];
+        }
+        std::vector<int32_t> node_dev(rows, -1), seg(rows, 1), row_off(ncells + 1, 0);
+        row_cell[g].assign(rows, -1);
+        if (!artificial) {
+            for (int32_t r = 0; r < rows; ++r) {
+                int64_t packed = key[perm[r]];
+                node_dev[r] = (int32_t)packed;
+                row_cell[g][r] = cell_of[layout_of_packed[packed]];
+            }
+            for (int32_t r = 0; r < rows; ++r) {
+                if (r > 0 && node_dev[r] == node_dev[r - 1]) {
+                    seg[r] = 0;
+                } else {
+                    int32_t len = 1;
+                    while (r + len < rows && node_dev[r + len] == node_dev[r]) ++len;
+                    seg[r] = len;
+                }
+            }
+            if ((m.kind == MIND_MECH_HH || m.kind == MIND_MECH_PAS)) {
+                for (int32_t r = 0; r < rows; ++r)
+                    if (seg[r] > 1) return fail(h, MIND_ELAYOUT, "density mechanism twice on one node");
+                int slot = m.kind == MIND_MECH_HH ? HH_SCALE : PAS_SCALE;
+                for (int32_t r = 0; r < rows; ++r) init.f[slot][r] = L->area[layout_of_packed[node_dev[r]]] * 0.01;
+            }
+            for (int32_t r = 0; r < rows; ++r) row_off[row_cell[g][r] + 1]++;
+            for (int32_t c = 0; c < ncells; ++c) row_off[c + 1] += row_off[c];
+        }
+        if (artificial) {
+            init.logical.resize(rows);
+            for (int32_t r = 0; r < rows; ++r) init.logical[r] = m.logical_ids[perm[r]];
+        }
+        DevGroup &G = P.groups[g];
+        G.kind = m.kind;
+        G.rows = rows;
+        G.row_off = h->upload(row_off);
+        G.node = h->upload(node_dev);
+        G.seg = h->upload(seg);
+        for (int k = 0; k < 12; ++k) G.f[k] = nullptr;
+        for (int k = 0; k < 4; ++k) G.s[k] = nullptr;
+        for (int k = 0; k < spec.nslot; ++k) G.f[k] = h->alloc<double>(rows);
+        for (int k = 0; k < spec.nfloat; ++k) G.s[k] = h->alloc<float>(rows);
+        h->group_init.push_back(std::move(init));
+    }
+
+    // ---- points, sources, detectors, edges ----
+    const int64_t np = L->n_points;
+    std::vector<int32_t> point_cell(np, -1), point_group(np, -1), point_row(np, -1);
+    for (int64_t p = 0; p < np; ++p) {
+        int32_t g = L->point_group[p] - 1, r = L->point_row[p] - 1;
+        if (g < 0 || g >= L->n_mechanisms || r < 0 || r >= L->mechanisms[g].rows)
+            return fail(h, MIND_ELAYOUT, "point index out of range");
+        point_group[p] = g;
+        point_row[p] = dev_row_of[g][r];
+        point_cell[p] = row_cell[g][point_row[p]];
+    }
+    h->n_sources = L->n_sources;
+    h->source_ids.assign(L->source_ids, L->source_ids + L->n_sources);
+    std::vector<std::vector<std::pair<int32_t, int32_t>>> det_by_cell(ncells);
+    std::vector<double> det_thr_by_source(L->n_sources, 0.0);
+    std::vector<int32_t> ns_source(P.ns_group >= 0 ? L->mechanisms[P.ns_group].rows : 0, -1);
+    for (int64_t s = 0; s < L->n_sources; ++s) {
+        int32_t node = L->source_nodes[s];
+        int32_t point = L->source_points[s];
+        if (node < 0 || node > n) return fail(h, MIND_ELAYOUT, "source node out of range");
+        if (point < 0 || point > np) return fail(h, MIND_ELAYOUT, "source point out of range");
+        if (node > 0) {
+            int64_t packed = h->packed_of_layout[node - 1];
+            int32_t cell = cell_of[node - 1];
+            det_by_cell[cell].push_back({(int32_t)(packed - node_off[cell]), (int32_t)s});
+            det_thr_by_source[s] = L->source_thresholds[s];
+        } else if (point > 0) {
+            int32_t g = point_group[point - 1];
+            if (g == P.ns_group) ns_source[point_row[point - 1]] = (int32_t)s;
+        }
+    }
+    std::vector<int32_t> det_off{0}, det_node, det_source;
+    std::vector<double> det_thr;
+    for (int32_t c = 0; c < ncells; ++c) {
+        for (auto &d : det_by_cell[c]) {
+            det_node.push_back(d.first);
+            det_source.push_back(d.second);
+            det_thr.push_back(det_thr_by_source[d.second]);
+        }
+        det_off.push_back((int32_t)det_node.size());
+    }
+    const int64_t ne = L->n_edges;
+    std::vector<int64_t> fanout(L->n_sources + 1);
+    for (int64_t s = 0; s <= L->n_sources; ++s) fanout[s] = L->fanout_offsets[s] - 1;
+    if (fanout[0] != 0 || fanout[L->n_sources] != ne) return fail(h, MIND_ELAYOUT, "fanout offsets inconsistent");
+    std::vector<int32_t> edge_target(ne);
+    std::vector<double> edge_delay(L->edge_delays, L->edge_delays + ne), edge_weight(L->edge_weights, L->edge_weights + ne);
+    double min_cell_delay = INFINITY, max_delay = 0.0;
+    for (int64_t s = 0; s < L->n_sources; ++s) {
+        if (fanout[s + 1] < fanout[s]) return fail(h, MIND_ELAYOUT, "fanout offsets decrease");
+        for (int64_t e = fanout[s]; e < fanout[s + 1]; ++e) {
+            int32_t t = L->edge_targets[e];
+            if (t < 1 || t > np) return fail(h, MIND_ELAYOUT, "edge target out of range");
+            int32_t kind = L->mechanisms[point_group[t - 1]].kind;
+            if (kind != MIND_MECH_EXPSYN && kind != MIND_MECH_EXP2SYN)
+                return fail(h, MIND_ELAYOUT, "NetCon target must be ExpSyn or Exp2Syn in this build");
+            double d = edge_delay[e];
+            if (!(d >= 0.0) || !std::isfinite(d) || !std::isfinite(edge_weight[e]))
+                return fail(h, MIND_ELAYOUT, "invalid NetCon delay or weight");
+            edge_target[e] = t - 1;
+            max_delay = std::max(max_delay, d);
+            if (L->source_nodes[s] > 0) min_cell_delay = std::min(min_cell_delay, d);
+        }
+    }
+    // Window: a spike detected at step s arrives in bin >= s + floor((d - dt/2)/dt); keep one bin margin.
+    int32_t window = kMaxWindow;
+    if (std::isfinite(min_cell_delay)) {
+        double k = std::floor((min_cell_delay - 0.5 * L->dt) / L->dt) - 1.0;
+        window = (int32_t)std::max(1.0, std::min((double)kMaxWindow, k));
+    }
+    h->window = window;
+    h->edge_target = edge_target;
+    h->max_delay_bins = (int32_t)std::ceil(max_delay / L->dt) + 2;
+
+    // ---- device arrays ----
+    P.node_off = h->upload(node_off);
+    P.v = h->alloc<double>(n);
+    P.a = h->upload(a);
+    P.cdt = h->upload(cdt);
+    P.ad = h->upload(ad);
+    P.parent = h->upload(parent_local);
+    P.kid_off = h->upload(kid_off);
+    P.kids = h->upload(kids);
+    P.chain_off = h->upload(chain_off);
+    P.chain_top = h->upload(chain_top);
+    P.chain_len = h->upload(chain_len);
+    P.chain_kid_off = h->upload(chain_kid_off);
+    P.chain_kids = h->upload(chain_kids);
+    P.level_off = h->upload(level_off);
+    P.level_chain = h->upload(level_chain);
+    P.det_off = h->upload(det_off);
+    P.det_node = h->upload(det_node);
+    P.det_source = h->upload(det_source);
+    P.det_thr = h->upload(det_thr);
+    P.above = h->alloc<uint8_t>(L->n_sources);
+    P.win_spike_cap = std::max<int32_t>(1024, ncells * 4);
+    P.win_spike_source = h->alloc<int32_t>(P.win_spike_cap);
+    P.win_spike_step = h->alloc<int64_t>(P.win_spike_cap);
+    P.win_spike_count = h->alloc<int32_t>(1);
+    int64_t spike_cap = L->spike_capacity > 0 ? L->spike_capacity : (int64_t)1 << 22;
+    P.rec_spike_cap = (int32_t)std::min<int64_t>(spike_cap, INT32_MAX);
+    P.rec_spike_source = h->alloc<int32_t>(P.rec_spike_cap);
+    P.rec_spike_time = h->alloc<double>(P.rec_spike_cap);
+    P.rec_spike_count = h->alloc<int32_t>(1);
+    P.ring_slots = window + h->max_delay_bins + 4;
+    int64_t ring_cap = L->event_capacity > 0 ? L->event_capacity
+                                             : std::max<int64_t>(4096, std::min<int64_t>(ne / 16 + 1, 1 << 20));
+    P.ring_cap = (int32_t)ring_cap;
+    P.ring = h->alloc<RingEvent>((size_t)P.ring_slots * P.ring_cap);
+    P.ring_count = h->alloc<int32_t>(P.ring_slots);
+    P.inbox_cap = 512;
+    P.inbox = h->alloc<InboxEvent>((size_t)ncells * P.inbox_cap);
+    P.inbox_count = h->alloc<int32_t>(ncells);
+    P.edge_weight = h->upload(edge_weight);
+    P.edge_delay = h->upload(edge_delay);
+    P.edge_target = h->upload(edge_target);
+    P.fanout_off = h->upload(fanout);
+    P.point_cell = h->upload(point_cell);
+    P.point_group = h->upload(point_group);
+    P.point_row = h->upload(point_row);
+    if (P.ns_group >= 0) {
+        P.ns_ran = h->alloc<MindRan>(ns_source.size());
+        P.ns_source = h->upload(ns_source);
+        h->ns_logical = h->upload(h->group_init[P.ns_group].logical);
+    }
+    P.error = h->alloc<int32_t>(1);
+    P.nrec = 0;
+    std::vector<int32_t> zero_off(ncells + 1, 0);
+    P.rec_off = h->upload(zero_off);
+
+    h->smem_bytes = (size_t)(4 * max_nodes + 2 * max_chains) * sizeof(double) +
+                    (size_t)P.inbox_cap * (sizeof(InboxEvent) + sizeof(int32_t));
+    if (h->smem_bytes > 227 * 1024)
+        return fail(h, MIND_ELAYOUT, "a cell needs more shared memory than one CTA has");
+    CUDA_TRY(h, cudaFuncSetAttribute(window_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)h->smem_bytes));
+    CUDA_TRY(h, cudaFuncSetAttribute(window_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)h->smem_bytes));
+    CUDA_TRY(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    CUDA_TRY(h, cudaEventCreate(&h->ev_start));
+    CUDA_TRY(h, cudaEventCreate(&h->ev_stop));
+    return MIND_OK;
+}
+
+int upload_group_state(MindHandle *h) {
+    for (size_t g = 0; g < h->group_init.size(); ++g) {
+        const auto &init = h->group_init[g];
+        DevGroup &G = h->P.groups[g];
+        for (size_t k = 0; k < init.f.size(); ++k)
+            if (G.f[k] && init.rows)
+                CUDA_TRY(h, cudaMemcpyAsync(G.f[k], init.f[k].data(), init.rows * sizeof(double),
+                                            cudaMemcpyHostToDevice, h->stream));
+    }
+    return MIND_OK;
+}
+
+int check_device_error(MindHandle *h) {
+    int32_t code = 0;
+    CUDA_TRY(h, cudaMemcpyAsync(&code, h->P.error, sizeof code, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    if (code == 0) return MIND_OK;
+    const char *what = code == MIND_ECAPACITY   ? "event ring, cell inbox or spike record capacity exhausted"
+                       : code == MIND_ESELFEVENT ? "invalid self-event delay or an event behind its delivery step"
+                       : code == MIND_ESINGULAR  ? "singular or non-finite cable system"
+                       : code == MIND_ENONFINITE ? "non-finite numerical state"
+                                                 : "device error";
+    return fail(h, code, what);
+}
+
+int set_records(MindHandle *h, const MindRecord *records, int32_t nrec, int64_t samples) {
+    Params &P = h->P;
+    std::vector<std::vector<std::pair<int32_t, int32_t>>> by_cell(h->ncells);
+    std::vector<int64_t> global(nrec);
+    for (int32_t k = 0; k < nrec; ++k) {
+        if (records[k].kind != MIND_RECORD_VOLTAGE) return fail(h, MIND_EARG, "unsupported record kind");
+        int32_t node = records[k].node;
+        if (node < 1 || node > h->n_nodes) return fail(h, MIND_EARG, "record node out of range");
+        global[k] = h->packed_of_layout[node - 1];
+    }
+    const std::vector<int64_t> &node_off = h->node_off;
+    for (int32_t k = 0; k < nrec; ++k) {
+        int64_t packed = global[k];
+        int32_t cell = (int32_t)(std::upper_bound(node_off.begin(), node_off.end(), packed) - node_off.begin() - 1);
+        by_cell[cell].push_back({(int32_t)(packed - node_off[cell]), k});
+    }
+    std::vector<int32_t> off{0}, node, col;
+    for (int32_t c = 0; c < h->ncells; ++c) {
+        for (auto &x : by_cell[c]) {
+            node.push_back(x.first);
+            col.push_back(x.second);
+        }
+        off.push_back((int32_t)node.size());
+    }
+    h->release(h->rec_off_dev);
+    h->release(h->rec_node_dev);
+    h->release(h->rec_col_dev);
+    h->release(h->rec_global_dev);
+    h->rec_off_dev = h->upload(off);
+    h->rec_node_dev = h->upload(node);
+    h->rec_col_dev = h->upload(col);
+    h->rec_global_dev = h->upload(global);
+    P.rec_off = h->rec_off_dev;
+    P.rec_node = h->rec_node_dev;
+    P.rec_col = h->rec_col_dev;
+    P.nrec = nrec;
+    size_t need = (size_t)samples * (size_t)std::max(nrec, 1);
+    if (nrec > 0 && need > h->trace_capacity) {
+        h->release(h->trace_dev);
+        h->trace_dev = h->alloc<double>(need);
+        h->trace_capacity = need;
+    }
+    P.trace = h->trace_dev;
+    P.trace_samples = samples;
+    return MIND_OK;
+}
+
+int advance(MindHandle *h, int64_t steps, bool record_spikes) {
+    Params &P = h->P;
+    P.record_spikes = record_spikes ? 1 : 0;
+    P.run_start = h->step;
+    CUDA_TRY(h, cudaMemsetAsync(P.rec_spike_count, 0, sizeof(int32_t), h->stream));
+    if (P.nrec)
+        record_initial_kernel<<<launch_grid(P.nrec), kThreads, 0, h->stream>>>(P, h->rec_global_dev, P.nrec);
+    CUDA_TRY(h, cudaEventRecord(h->ev_start, h->stream));
+    int64_t n0 = h->step;
+    const int64_t end = h->step + steps;
+    const int ns_blocks = P.ns_group >= 0 ? launch_grid(P.groups[P.ns_group].rows) : 0;
+    while (n0 < end) {
+        const int32_t W = (int32_t)std::min<int64_t>(h->window, end - n0);
+        const double horizon = (double)(n0 + W - 1) * P.dt + 0.5 * P.dt;
+        if (P.ns_group >= 0) netstim_kernel<<<ns_blocks, kThreads, 0, h->stream>>>(P, horizon, n0);
+        bucket_kernel<<<dim3(64, W), kThreads, 0, h->stream>>>(P, n0);
+        if (h->ncells > 0) {
+            if (h->precision == MIND_MIXED)
+                window_kernel<true><<<h->ncells, kThreads, h->smem_bytes, h->stream>>>(P, n0, W);
+            else
+                window_kernel<false><<<h->ncells, kThreads, h->smem_bytes, h->stream>>>(P, n0, W);
+        }
+        route_kernel<<<64, kThreads, 0, h->stream>>>(P, n0 + W);
+        n0 += W;
+    }
+    CUDA_TRY(h, cudaGetLastError());
+    CUDA_TRY(h, cudaEventRecord(h->ev_stop, h->stream));
+    finite_kernel<<<launch_grid(h->n_nodes), kThreads, 0, h->stream>>>(P.v, h->n_nodes, P.error);
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    float ms = 0.0f;
+    CUDA_TRY(h, cudaEventElapsedTime(&ms, h->ev_start, h->ev_stop));
+    h->last_ms = ms;
+    h->step = end;
+    return check_device_error(h);
+}
+
+int collect(MindHandle *h, bool record_spikes) {
+    Params &P = h->P;
+    h->spike_times.clear();
+    h->spike_sids.clear();
+    if (record_spikes) {
+        int32_t count = 0;
+        CUDA_TRY(h, cudaMemcpy(&count, P.rec_spike_count, sizeof count, cudaMemcpyDeviceToHost));
+        count = std::min(count, P.rec_spike_cap);
+        std::vector<int32_t> src(count);
+        std::vector<double> t(count);
+        if (count) {
+            CUDA_TRY(h, cudaMemcpy(src.data(), P.rec_spike_source, count * sizeof(int32_t), cudaMemcpyDeviceToHost));
+            CUDA_TRY(h, cudaMemcpy(t.data(), P.rec_spike_time, count * sizeof(double), cudaMemcpyDeviceToHost));
+        }
+        std::vector<int32_t> idx(count);
+        for (int32_t i = 0; i < count; ++i) idx[i] = i;
+        std::sort(idx.begin(), idx.end(), [&](int32_t x, int32_t y) {
+            if (t[x] != t[y]) return t[x] < t[y];
+            if (h->source_ids[src[x]] != h->source_ids[src[y]]) return h->source_ids[src[x]] < h->source_ids[src[y]];
+            return x < y;
+        });
+        h->spike_times.resize(count);
+        h->spike_sids.resize(count);
+        for (int32_t i = 0; i < count; ++i) {
+            h->spike_times[i] = t[idx[i]];
+            h->spike_sids[i] = h->source_ids[src[idx[i]]];
+        }
+    }
+    h->trace_records = P.nrec;
+    h->trace_samples = P.trace_samples;
+    h->trace.assign((size_t)h->trace_samples * P.nrec, 0.0);
+    if (P.nrec && !h->trace.empty())
+        CUDA_TRY(h, cudaMemcpy(h->trace.data(), P.trace, h->trace.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    return MIND_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mind_create(const MindLayout *layout, MindHandle **out) {
+    if (!out) return MIND_EARG;
+    *out = nullptr;
+    MindHandle *h = nullptr;
+    try {
+        h = new MindHandle();
+        int status = create(layout, h);
+        if (status != MIND_OK) {
+            g_create_error = h->error;
+            delete h;
+            return status;
+        }
+    } catch (const std::bad_alloc &) {
+        g_create_error = "device or host allocation failed";
+        delete h;
+        return MIND_ECUDA;
+    }
+    *out = h;
+    return MIND_OK;
+}
+
+int mind_set_precision(MindHandle *h, int32_t mode) {
+    if (!h) return MIND_EARG;
+    if (mode != MIND_FP64 && mode != MIND_MIXED) return fail(h, MIND_EARG, "unknown precision mode");
+    h->precision = mode;
+    return MIND_OK;
+}
+
+int mind_initialize(MindHandle *h) {
+    if (!h) return MIND_EARG;
+    Params &P = h->P;
+    h->initialized = false;
+    h->step = 0;
+    CUDA_TRY(h, cudaMemcpyAsync(P.v, h->v0_packed.data(), h->n_nodes * sizeof(double), cudaMemcpyHostToDevice,
+                                h->stream));
+    CUDA_TRY(h, cudaMemsetAsync(P.error, 0, sizeof(int32_t), h->stream));
+    CUDA_TRY(h, cudaMemsetAsync(P.above, 0, std::max<int64_t>(1, h->n_sources), h->stream));
+    CUDA_TRY(h, cudaMemsetAsync(P.ring_count, 0, P.ring_slots * sizeof(int32_t), h->stream));
+    CUDA_TRY(h, cudaMemsetAsync(P.inbox_count, 0, std::max(1, h->ncells) * sizeof(int32_t), h->stream));
+    CUDA_TRY(h, cudaMemsetAsync(P.win_spike_count, 0, sizeof(int32_t), h->stream));
+    int status = upload_group_state(h);
+    if (status) return status;
+    for (int32_t g = 0; g < P.ngroups; ++g) {
+        if (g == P.ns_group || P.groups[g].rows == 0) continue;
+        mechanism_init_kernel<<<launch_grid(P.groups[g].rows), kThreads, 0, h->stream>>>(P, g);
+    }
+    if (P.ns_group >= 0 && P.groups[P.ns_group].rows > 0)
+        netstim_init_kernel<<<launch_grid(P.groups[P.ns_group].rows), kThreads, 0, h->stream>>>(
+            P, h->group_init[P.ns_group].digest, h->ns_logical);
+    CUDA_TRY(h, cudaGetLastError());
+    status = check_device_error(h);
+    if (status) return status;
+    h->initialized = true;
+    return MIND_OK;
+}
+
+int mind_run(MindHandle *h, int64_t steps, const MindRecord *records, int32_t n_records, int32_t record_spikes) {
+    if (!h) return MIND_EARG;
+    if (!h->initialized) return fail(h, MIND_EARG, "simulation is not initialized");
+    if (steps < 0 || n_records < 0 || (n_records > 0 && !records)) return fail(h, MIND_EARG, "invalid run arguments");
+    int status = set_records(h, records, n_records, steps + 1);
+    if (status) return status;
+    status = advance(h, steps, record_spikes != 0);
+    if (status) {
+        h->initialized = false;
+        return status;
+    }
+    return collect(h, record_spikes != 0);
+}
+
+int mind_step(MindHandle *h) {
+    if (!h) return MIND_EARG;
+    if (!h->initialized) return fail(h, MIND_EARG, "simulation is not initialized");
+    int status = set_records(h, nullptr, 0, 2);
+    if (status) return status;
+    status = advance(h, 1, false);
+    if (status) h->initialized = false;
+    return status;
+}
+
+int mind_time(const MindHandle *h, int64_t *step, double *time) {
+    if (!h) return MIND_EARG;
+    if (step) *step = h->step;
+    if (time) *time = (double)h->step * h->dt;
+    return MIND_OK;
+}
+
+int mind_get_trace(const MindHandle *h, double *out, int64_t n) {
+    if (!h) return MIND_EARG;
+    if (n != (int64_t)h->trace.size()) return MIND_EARG;
+    if (n) std::memcpy(out, h->trace.data(), n * sizeof(double));
+    return MIND_OK;
+}
+
+int mind_get_spikes(const MindHandle *h, double *times, int64_t *sids, int64_t cap, int64_t *n) {
+    if (!h || !n) return MIND_EARG;
+    *n = (int64_t)h->spike_times.size();
+    int64_t m = std::min<int64_t>(cap, *n);
+    if (m > 0) {
+        if (!times || !sids) return MIND_EARG;
+        std::memcpy(times, h->spike_times.data(), m * sizeof(double));
+        std::memcpy(sids, h->spike_sids.data(), m * sizeof(int64_t));
+    }
+    return MIND_OK;
+}
+
+int mind_read_voltage(const MindHandle *h, int32_t node, double *value) {
+    if (!h || !value) return MIND_EARG;
+    if (node < 1 || node > h->n_nodes) return MIND_EARG;
+    cudaError_t e = cudaMemcpy(value, h->P.v + h->packed_of_layout[node - 1], sizeof(double), cudaMemcpyDeviceToHost);
+    return e == cudaSuccess ? MIND_OK : MIND_ECUDA;
+}
+
+int mind_inject_event(MindHandle *h, int64_t edge, double t) {
+    if (!h) return MIND_EARG;
+    if (!h->initialized) return fail(h, MIND_EARG, "simulation is not initialized");
+    const Params &P = h->P;
+    if (edge < 1 || edge > (int64_t)h->edge_target.size()) return fail(h, MIND_EARG, "edge index out of range");
+    if (!(t >= (double)h->step * h->dt) || !std::isfinite(t)) return fail(h, MIND_EARG, "event time is in the past");
+    inject_kernel<<<1, 1, 0, h->stream>>>(P, t, (int32_t)(edge - 1), h->edge_target[edge - 1], h->step);
+    CUDA_TRY(h, cudaGetLastError());
+    return check_device_error(h);
+}
+
+const char *mind_last_error(const MindHandle *h) {
+    if (!h) return g_create_error.c_str();
+    return h->error.c_str();
+}
+
+int mind_last_run_ms(const MindHandle *h, double *ms) {
+    if (!h || !ms) return MIND_EARG;
+    *ms = h->last_ms;
+    return MIND_OK;
+}
+
+int mind_destroy(MindHandle *h) {
+    if (!h) return MIND_OK;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->ev_start) cudaEventDestroy(h->ev_start);
+    if (h->ev_stop) cudaEventDestroy(h->ev_stop);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return MIND_OK;
+}
+
+}  // extern "C"

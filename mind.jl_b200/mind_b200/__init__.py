@@ -1,0 +1,24 @@
+"""mind_b200 — host-side mirror of MIND.jl's micro model/runtime API over libmindgpu.so.
+
+The Julia names map one to one (`add_population!` -> `add_population`,
+`insert!` -> `insert`, `build!` -> `build`, `initialize!` -> `initialize`,
+`run!` -> `run`, `step!` -> `step`).  Model construction and packing run on
+the host; every simulation step runs in the CUDA library through its C-ABI.
+"""
+from .mechanisms import Mechanism, builtin
+from .morphology import Point3D, Section, discretize, location_node
+from .model import (Cell, IonSpecies, MicroModel, PointProcess, Population, SpikeSource,
+                    add_pointprocess, add_pointprocesses, add_population, connect, connect_many,
+                    insert, register_point_sources, register_spike_source, spike_source)
+from .layout import Layout, build
+from .runtime import (RecordSpec, SimulationResult, initialize, run, simulation_time, step,
+                      voltage_record)
+
+__all__ = [
+    "Mechanism", "builtin", "Point3D", "Section", "discretize", "location_node", "Cell",
+    "IonSpecies", "MicroModel", "PointProcess", "Population", "SpikeSource", "add_pointprocess",
+    "add_pointprocesses", "add_population", "connect", "connect_many", "insert",
+    "register_point_sources", "register_spike_source", "spike_source", "Layout", "build",
+    "RecordSpec", "SimulationResult", "initialize", "run", "simulation_time", "step",
+    "voltage_record",
+]

@@ -1,0 +1,154 @@
+"""ctypes view of include/mindgpu.h and the loader for libmindgpu.so.
+
+This is the Python side of the same boundary the Julia adapter binds with
+ccall (mind.jl_b200/julia/MINDGPU.jl): plain pointers and sizes, no torch types.
+The library is built in-tree by mind.jl_b200/csrc/build.py; there is no
+fallback — a missing or unloadable library raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import (POINTER, Structure, c_char_p, c_double, c_int32, c_int64, c_uint64, c_void_p)
+
+MIND_ABI_VERSION = 1
+
+MIND_OK = 0
+MIND_ECAPACITY = 3
+MIND_ESELFEVENT = 5
+MIND_ESINGULAR = 6
+MIND_ENONFINITE = 8
+MIND_ETIMEOUT = 9
+MIND_ELAYOUT = 10
+MIND_ECUDA = 11
+MIND_EARG = 12
+
+MIND_FP64 = 0
+MIND_MIXED = 1
+
+MIND_RECORD_VOLTAGE = 1
+
+STATUS_NAMES = {
+    MIND_ECAPACITY: "capacity exhausted",
+    MIND_ESELFEVENT: "invalid self-event delay or target",
+    MIND_ESINGULAR: "singular or non-finite cable system",
+    MIND_ENONFINITE: "non-finite numerical state",
+    MIND_ETIMEOUT: "device wait timeout",
+    MIND_ELAYOUT: "layout rejected",
+    MIND_ECUDA: "CUDA runtime error",
+    MIND_EARG: "invalid argument",
+}
+
+
+class MindMechanism(Structure):
+    _fields_ = [
+        ("kind", c_int32),
+        ("n_fields", c_int32),
+        ("rows", c_int64),
+        ("data", POINTER(c_double)),
+        ("field_names", POINTER(c_char_p)),
+        ("nodes", POINTER(c_int32)),
+        ("logical_ids", POINTER(c_uint64)),
+        ("digest", c_uint64),
+    ]
+
+
+class MindLayout(Structure):
+    _fields_ = [
+        ("abi_version", c_int32),
+        ("secondorder", c_int32),
+        ("n_nodes", c_int64),
+        ("parent", POINTER(c_int32)),
+        ("voltage", POINTER(c_double)),
+        ("area", POINTER(c_double)),
+        ("capacitance", POINTER(c_double)),
+        ("axial", POINTER(c_double)),
+        ("axial_diagonal", POINTER(c_double)),
+        ("n_mechanisms", c_int32),
+        ("mechanisms", POINTER(MindMechanism)),
+        ("n_points", c_int64),
+        ("point_group", POINTER(c_int32)),
+        ("point_row", POINTER(c_int32)),
+        ("n_sources", c_int64),
+        ("source_ids", POINTER(c_int64)),
+        ("source_nodes", POINTER(c_int32)),
+        ("source_thresholds", POINTER(c_double)),
+        ("source_points", POINTER(c_int32)),
+        ("n_edges", c_int64),
+        ("fanout_offsets", POINTER(c_int64)),
+        ("edge_targets", POINTER(c_int32)),
+        ("edge_delays", POINTER(c_double)),
+        ("edge_weights", POINTER(c_double)),
+        ("dt", c_double),
+        ("celsius", c_double),
+        ("seed", c_uint64),
+        ("event_capacity", c_int64),
+        ("spike_capacity", c_int64),
+    ]
+
+
+class MindRecord(Structure):
+    _fields_ = [("kind", c_int32), ("node", c_int32)]
+
+
+class MindError(RuntimeError):
+    """A non-zero status from libmindgpu, with the library's message."""
+
+    def __init__(self, status: int, message: str):
+        self.status = status
+        super().__init__(f"mindgpu status {status} ({STATUS_NAMES.get(status, 'error')}): {message}")
+
+
+_LIB = None
+
+PACKAGE_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIBRARY_PATH = os.path.join(PACKAGE_ROOT, "lib", "libmindgpu.so")
+
+
+def library_path() -> str:
+    return os.environ.get("MINDGPU_LIBRARY", LIBRARY_PATH)
+
+
+def load_library():
+    """Load libmindgpu.so (built in-tree); raises if it is absent."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    path = library_path()
+    if not os.path.exists(path):
+        raise OSError(f"{path} is missing; build it with `python -c 'import __graft_entry__ as g; g.build()'`")
+    lib = ctypes.CDLL(path)
+    handle = c_void_p
+    lib.mind_create.argtypes = [POINTER(MindLayout), POINTER(handle)]
+    lib.mind_initialize.argtypes = [handle]
+    lib.mind_set_precision.argtypes = [handle, c_int32]
+    lib.mind_run.argtypes = [handle, c_int64, POINTER(MindRecord), c_int32, c_int32]
+    lib.mind_step.argtypes = [handle]
+    lib.mind_time.argtypes = [handle, POINTER(c_int64), POINTER(c_double)]
+    lib.mind_get_trace.argtypes = [handle, POINTER(c_double), c_int64]
+    lib.mind_get_spikes.argtypes = [handle, POINTER(c_double), POINTER(c_int64), c_int64, POINTER(c_int64)]
+    lib.mind_read_voltage.argtypes = [handle, c_int32, POINTER(c_double)]
+    lib.mind_inject_event.argtypes = [handle, c_int64, c_double]
+    lib.mind_last_error.argtypes = [handle]
+    lib.mind_last_error.restype = c_char_p
+    lib.mind_last_run_ms.argtypes = [handle, POINTER(c_double)]
+    lib.mind_destroy.argtypes = [handle]
+    for name in ("mind_create", "mind_initialize", "mind_set_precision", "mind_run", "mind_step",
+                 "mind_time", "mind_get_trace", "mind_get_spikes", "mind_read_voltage",
+                 "mind_inject_event", "mind_last_run_ms", "mind_destroy"):
+        getattr(lib, name).restype = c_int32
+    _LIB = lib
+    return lib
+
+
+EXPORTED_SYMBOLS = (
+    "mind_create", "mind_initialize", "mind_set_precision", "mind_run", "mind_step", "mind_time",
+    "mind_get_trace", "mind_get_spikes", "mind_read_voltage", "mind_inject_event",
+    "mind_last_error", "mind_last_run_ms", "mind_destroy",
+)
+
+
+def check(lib, handle, status: int) -> None:
+    if status != MIND_OK:
+        message = lib.mind_last_error(handle)
+        raise MindError(status, message.decode() if message else "")

@@ -1,0 +1,123 @@
+"""Builtin mechanism descriptors: the field tables the device kernels understand.
+
+MIND.jl compiles each MOD file into a CompiledMechanism whose IR lists the
+instance fields, their defaults and the NET_RECEIVE arity
+(src/compiler/ir.jl:264-288, src/compiler/frontend.jl:58-72).  The hot path of
+this library evaluates the six builtins the benchmark networks use with
+hand-written sm_100a device code, so a mechanism here is a descriptor: its MOD
+name, its kind, the C-ABI kind code, its fields with MOD defaults, and the
+digest that keys its random streams.
+
+The digest is the first 16 hex digits of the SHA-256 of the MOD source, as the
+reference derives it for Philox keys (src/compiler/ir.jl:316-324,
+src/runtime/initialize.jl:309).  The values below were computed from the
+reference's mod/*.mod files; only NetStim draws random numbers.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import Dict, Tuple
+
+# C-ABI kind codes (include/mindgpu.h).
+MIND_MECH_HH = 1
+MIND_MECH_PAS = 2
+MIND_MECH_EXPSYN = 3
+MIND_MECH_EXP2SYN = 4
+MIND_MECH_NETSTIM = 5
+MIND_MECH_ICLAMP = 6
+
+
+@dataclass(frozen=True)
+class Mechanism:
+    """A compiled mechanism as the model builders see it (CompiledMechanism)."""
+
+    name: str
+    kind: str  # "density" | "point" | "artificial"
+    code: int
+    fields: Tuple[str, ...]
+    defaults: Tuple[float, ...]
+    digest: int
+    receive_arity: int = 0
+    # Fields filled from ion species at build time (USEION ... READ e<ion>).
+    ion_reads: Tuple[Tuple[str, str], ...] = field(default_factory=tuple)
+
+    def field_index(self, name: str) -> int:
+        try:
+            return self.fields.index(name)
+        except ValueError:
+            raise ValueError(f"{self.name} has no field {name}") from None
+
+    @property
+    def has_net_receive(self) -> bool:
+        return self.receive_arity > 0
+
+
+def _mechanism(name, kind, code, table, digest, arity=0, ion_reads=()):
+    fields = tuple(name for name, _ in table)
+    defaults = tuple(float(value) for _, value in table)
+    return Mechanism(name, kind, code, fields, defaults, digest, arity, tuple(ion_reads))
+
+
+# PARAMETER defaults from mod/*.mod; ASSIGNED and STATE fields start at 0.
+_BUILTINS: Dict[str, Mechanism] = {
+    "hh": _mechanism(
+        "hh",
+        "density",
+        MIND_MECH_HH,
+        [
+            ("gnabar", 0.12), ("gkbar", 0.036), ("gl", 0.0003), ("el", -54.3),
+            ("m", 0.0), ("h", 0.0), ("n", 0.0),
+            ("ena", 50.0), ("ek", -77.0),
+            ("gna", 0.0), ("gk", 0.0), ("ina", 0.0), ("ik", 0.0), ("il", 0.0),
+            ("minf", 0.0), ("hinf", 0.0), ("ninf", 0.0),
+            ("mtau", 0.0), ("htau", 0.0), ("ntau", 0.0),
+        ],
+        0x06A1D0784470B30B,
+        ion_reads=(("ena", "na"), ("ek", "k")),
+    ),
+    "pas": _mechanism(
+        "pas", "density", MIND_MECH_PAS,
+        [("g", 0.001), ("e", -70.0), ("i", 0.0)],
+        0x7C96D2C7CB7FE0C5,
+    ),
+    "ExpSyn": _mechanism(
+        "ExpSyn", "point", MIND_MECH_EXPSYN,
+        [("tau", 0.1), ("e", 0.0), ("g", 0.0), ("i", 0.0)],
+        0x9704333E132D681C,
+        arity=1,
+    ),
+    "Exp2Syn": _mechanism(
+        "Exp2Syn", "point", MIND_MECH_EXP2SYN,
+        [("tau1", 0.1), ("tau2", 10.0), ("e", 0.0), ("A", 0.0), ("B", 0.0),
+         ("g", 0.0), ("i", 0.0), ("factor", 0.0)],
+        0xC42E524B775C6D4D,
+        arity=1,
+    ),
+    "NetStim": _mechanism(
+        "NetStim", "artificial", MIND_MECH_NETSTIM,
+        [("interval", 10.0), ("number", 10.0), ("start", 50.0), ("noise", 0.0),
+         ("event", 0.0), ("on", 0.0), ("ispike", 0.0)],
+        0xA186833B569FF3B2,
+        arity=1,
+    ),
+    "IClamp": _mechanism(
+        "IClamp", "point", MIND_MECH_ICLAMP,
+        [("del", 0.0), ("dur", 0.0), ("amp", 0.0), ("i", 0.0)],
+        0x6EB0551A76C267F8,
+    ),
+}
+
+
+def builtin(name) -> Mechanism:
+    """Select a packaged builtin by its MOD name (frontend.jl:58-72)."""
+    key = str(name)
+    try:
+        return _BUILTINS[key]
+    except KeyError:
+        raise ValueError(
+            f"unknown mechanism {key}; this build evaluates {sorted(_BUILTINS)} on the device"
+        ) from None
+
+
+def resolve_mechanism(mechanism) -> Mechanism:
+    return mechanism if isinstance(mechanism, Mechanism) else builtin(mechanism)

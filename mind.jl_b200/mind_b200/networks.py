@@ -1,0 +1,273 @@
+"""Seeded synthetic networks for the benchmark configurations, built through the public API.
+
+Each generator uses numpy's PCG64 stream seeded with 0x4D494E44 + config number
+and the builders of this package exactly as a MIND.jl user script would use
+the Julia builders.  Choices the configuration text leaves open are fixed here
+and stated in each docstring.  No external dataset is involved.
+
+Units: lengths um, Ra ohm cm, cm uF/cm2, conductances S/cm2, synaptic weights
+uS (NET_RECEIVE weights are uS in mod/ExpSyn.mod and mod/Exp2Syn.mod, so nS
+draws are divided by 1000).
+"""
+from __future__ import annotations
+
+import math
+from typing import List, Tuple
+
+import numpy as np
+
+from . import model as M
+from .mechanisms import builtin
+from .morphology import Section
+
+SEED_BASE = 0x4D494E44
+
+
+def _rng(config: int) -> np.random.Generator:
+    return np.random.default_rng(SEED_BASE + config)
+
+
+def config1(n_cells: int = 64, synapses_per_cell: int = 10) -> M.MicroModel:
+    """Ball-and-stick cells with Poisson-driven ExpSyn (64 cells in the benchmark).
+
+    Soma 1 compartment (L = diam = 20 um, hh); dendrite 50 compartments
+    (L = 500 um, diam = 2 um, pas g = 1e-4 S/cm2, e = -65 mV); Ra 100, cm 1.
+    Each cell has a soma(0.5) detector at -10 mV and `synapses_per_cell`
+    ExpSyn (tau 2 ms, e 0 mV) at uniform-random dendritic x, each driven by its
+    own NetStim (10 Hz: interval 100 ms, noise 1, start 0, number 1e9) through a
+    NetCon with delay 0 and weight lognormal(ln 0.5 nS, 0.5).
+    Point order: all ExpSyn (cell-major), then all NetStims in the same order.
+    """
+    rng = _rng(1)
+    model = M.MicroModel(celsius=6.3)
+    soma = Section("soma", label="soma", length=20.0, diameter=20.0, nseg=1, Ra=100.0, cm=1.0)
+    dend = Section("dend", label="dend", parent="soma", parent_x=1.0, length=500.0, diameter=2.0,
+                   nseg=50, Ra=100.0, cm=1.0)
+    cells = M.add_population(model, [soma, dend], n_cells, voltage=-65.0)
+    for cell in cells:
+        M.insert(cell, builtin("hh"), sections="soma")
+        M.insert(cell, builtin("pas"), sections="dend", params={"g": 1.0e-4, "e": -65.0})
+        M.register_spike_source(cell, threshold=-10.0)
+    n = n_cells * synapses_per_cell
+    xs = rng.uniform(0.0, 1.0, n)
+    weights = rng.lognormal(math.log(0.5), 0.5, n) / 1000.0
+    owners = np.repeat(np.arange(1, n_cells + 1), synapses_per_cell)
+    first_syn = M.add_pointprocesses(model, builtin("ExpSyn"), owners, "dend", xs,
+                                     {"tau": 2.0, "e": 0.0})
+    first_stim = M.add_pointprocesses(model, builtin("NetStim"), np.zeros(n, np.int64), "none",
+                                      np.zeros(n), {"interval": 100.0, "number": 1e9, "start": 0.0,
+                                                    "noise": 1.0})
+    sources = M.register_point_sources(model, np.arange(first_stim, first_stim + n))
+    M.connect_many(model, sources, np.arange(first_syn, first_syn + n), weights, np.zeros(n))
+    return model
+
+
+def _binary_tree(rng, compartments: int, soma: Section) -> List[Section]:
+    """Random binary dendritic tree with exactly `compartments` dendritic compartments.
+
+    Branch lengths lognormal(ln 50 um, 0.5) at 10 um per compartment (nseg =
+    max(1, round(L/10))); the first branch starts at soma(1) with diam 3 um and
+    each generation tapers 0.9x.  A random leaf is split into two children until
+    the budget is spent; the last branch is shortened to fit (L = 10 um x nseg).
+    """
+    sections = [soma]
+    budget = compartments
+
+    def branch(name, parent, diameter):
+        nonlocal budget
+        length = float(rng.lognormal(math.log(50.0), 0.5))
+        nseg = max(1, int(round(length / 10.0)))
+        if nseg >= budget:
+            nseg = budget
+            length = 10.0 * nseg
+        budget -= nseg
+        sections.append(Section(name, label="dend", parent=parent, parent_x=1.0, length=length,
+                                diameter=diameter, nseg=nseg, Ra=100.0, cm=1.0))
+        return name
+
+    leaves = [(branch("d0", soma.name, 3.0), 3.0)]
+    count = 1
+    while budget > 0:
+        pick = int(rng.integers(len(leaves)))
+        name, diameter = leaves.pop(pick)
+        for _ in range(2):
+            if budget <= 0:
+                break
+            child = branch(f"d{count}", name, diameter * 0.9)
+            count += 1
+            leaves.append((child, diameter * 0.9))
+    return sections
+
+
+def _dendritic_sites(rng, sections: List[Section], count: int, labels=None):
+    """Uniform-random dendritic positions: section with probability proportional to nseg, x ~ U(0,1)."""
+    dends = [s for s in sections if s.label != "soma" and (labels is None or s.label in labels)]
+    weights = np.array([s.nseg for s in dends], dtype=np.float64)
+    picks = rng.choice(len(dends), size=count, p=weights / weights.sum())
+    xs = rng.uniform(0.0, 1.0, count)
+    return [dends[i].name for i in picks], xs
+
+
+def config2(n_cells: int = 10000, synapses_per_cell: int = 100, background_hz: float = 5.0,
+            compartment_range: Tuple[int, int] = (100, 1000)) -> M.MicroModel:
+    """Uneven random binary trees in a recurrent Exp2Syn network (10,000 cells).
+
+    Each cell: soma (1 compartment, L = diam = 20 um, hh) plus a random binary
+    tree (`_binary_tree`) so that the total compartment count is uniform in
+    `compartment_range`; pas (g 1e-4 S/cm2, e -65 mV) on every dendrite.
+    100 Exp2Syn per cell (tau1 0.5 ms, tau2 5 ms; 80% e = 0 mV, 20% e = -80 mV)
+    at uniform-random dendritic positions; each gets one NetCon from a
+    uniform-random presynaptic cell (soma(0.5) detector, -10 mV) with delay
+    U[1,5] ms and weight lognormal(ln 0.3 nS, 0.7), and its own 5 Hz Poisson
+    NetStim (interval 200 ms, noise 1, start 0) through a NetCon with delay 0
+    and a weight from the same lognormal.
+    Point order: all Exp2Syn (cell-major), then all NetStims.
+    """
+    rng = _rng(2)
+    model = M.MicroModel(celsius=6.3)
+    sizes = rng.integers(compartment_range[0], compartment_range[1] + 1, n_cells)
+    cells = []
+    for c in range(n_cells):
+        soma = Section("soma", label="soma", length=20.0, diameter=20.0, nseg=1, Ra=100.0, cm=1.0)
+        secs = _binary_tree(rng, int(sizes[c]) - 1, soma)
+        cell = M.add_population(model, secs, 1, voltage=-65.0)[0]
+        M.insert(cell, builtin("hh"), sections="soma")
+        M.insert(cell, builtin("pas"), sections="dend", params={"g": 1.0e-4, "e": -65.0})
+        M.register_spike_source(cell, threshold=-10.0)
+        cells.append((cell, secs))
+    n = n_cells * synapses_per_cell
+    owners = np.repeat(np.arange(1, n_cells + 1), synapses_per_cell)
+    names, xs = [], []
+    for cell, secs in cells:
+        nm, x = _dendritic_sites(rng, secs, synapses_per_cell)
+        names.extend(nm)
+        xs.append(x)
+    xs = np.concatenate(xs)
+    e_rev = np.where(rng.uniform(size=n) < 0.8, 0.0, -80.0)
+    first_syn = M.add_pointprocesses(model, builtin("Exp2Syn"), owners, names, xs,
+                                     {"tau1": 0.5, "tau2": 5.0, "e": e_rev})
+    presyn = rng.integers(1, n_cells + 1, n)  # detector source index == cell index
+    delays = rng.uniform(1.0, 5.0, n)
+    weights = rng.lognormal(math.log(0.3), 0.7, n) / 1000.0
+    targets = np.arange(first_syn, first_syn + n)
+    M.connect_many(model, presyn, targets, weights, delays)
+    first_stim = M.add_pointprocesses(model, builtin("NetStim"), np.zeros(n, np.int64), "none",
+                                      np.zeros(n), {"interval": 1000.0 / background_hz,
+                                                    "number": 1e9, "start": 0.0, "noise": 1.0})
+    sources = M.register_point_sources(model, np.arange(first_stim, first_stim + n))
+    bg_weights = rng.lognormal(math.log(0.3), 0.7, n) / 1000.0
+    M.connect_many(model, sources, targets, bg_weights, np.zeros(n))
+    return model
+
+
+def _pyramidal(rng, target: int) -> List[Section]:
+    """Pyramidal-like morphology with about `target` compartments (10 um each).
+
+    Soma (1 compartment, 20x20 um); apical trunk of 600 um split into a
+    proximal 100 um section (`trunk0`, label "prox") and the rest; 10-20
+    oblique branches on the trunk and 5-10 tuft branches at its end; 4-8 basal
+    dendrites of 150-250 um from soma(0), each with a proximal 100 um section
+    (label "prox").  Diameters are seeded draws in [0.6, 4] um.  Oblique and
+    tuft lengths share the compartments left after trunk and basals.
+    """
+    soma = Section("soma", label="soma", length=20.0, diameter=20.0, nseg=1, Ra=100.0, cm=1.0)
+    secs = [soma]
+    trunk_d = float(rng.uniform(2.5, 4.0))
+    secs.append(Section("trunk0", label="prox", parent="soma", parent_x=1.0, length=100.0,
+                        diameter=trunk_d, nseg=10))
+    secs.append(Section("trunk1", label="apical", parent="trunk0", parent_x=1.0, length=500.0,
+                        diameter=trunk_d * 0.6, nseg=50))
+    used = 1 + 60
+    n_basal = int(rng.integers(4, 9))
+    for b in range(n_basal):
+        length = float(rng.uniform(150.0, 250.0))
+        nseg = int(round(length / 10.0))
+        d = float(rng.uniform(0.8, 2.0))
+        secs.append(Section(f"basal{b}p", label="prox", parent="soma", parent_x=0.0, length=100.0,
+                            diameter=d, nseg=10))
+        secs.append(Section(f"basal{b}d", label="basal", parent=f"basal{b}p", parent_x=1.0,
+                            length=length - 100.0, diameter=d * 0.8, nseg=nseg - 10))
+        used += nseg
+    n_oblique = int(rng.integers(10, 21))
+    n_tuft = int(rng.integers(5, 11))
+    remaining = max(target - used, n_oblique + n_tuft)
+    shares = rng.dirichlet(np.ones(n_oblique + n_tuft)) * remaining
+    nsegs = np.maximum(1, np.round(shares).astype(int))
+    for k in range(n_oblique):
+        x = float(rng.uniform(0.05, 0.95))
+        secs.append(Section(f"obl{k}", label="apical", parent="trunk1", parent_x=x,
+                            length=10.0 * nsegs[k], diameter=float(rng.uniform(0.6, 1.5)),
+                            nseg=int(nsegs[k])))
+    for k in range(n_tuft):
+        nseg = int(nsegs[n_oblique + k])
+        secs.append(Section(f"tuft{k}", label="apical", parent="trunk1", parent_x=1.0,
+                            length=10.0 * nseg, diameter=float(rng.uniform(0.6, 1.5)), nseg=nseg))
+    return secs
+
+
+def config3(n_cells: int = 1000, synapses_per_cell: int = 300, connectivity: float = 0.03,
+            background_hz: float = 2.0, iclamp_onset: float = 100.0) -> M.MicroModel:
+    """Pyramidal-like micro network (1,000 cells of 700-1,200 compartments).
+
+    hh at the soma and on the proximal 100 um sections (trunk0, basal*p), pas
+    (g 1e-4, e -65) elsewhere.  300 Exp2Syn per cell (tau1 0.5, tau2 5 ms; 85%
+    e = 0 mV, 15% e = -80 mV; 80% on basal, 20% on apical sections); 3%
+    recurrent connectivity (each cell receives from round(0.03 N) distinct
+    random presynaptic cells, each NetCon to a random synapse of the target)
+    with delays U[0.5,3] ms and weights lognormal(ln 0.3 nS, 0.7); a 2 Hz
+    Poisson NetStim per synapse (delay 0, same weight law); IClamp 0.1 nA for
+    50 ms from `iclamp_onset` ms at soma(0.5) on the first 10% of cells.
+    """
+    rng = _rng(3)
+    model = M.MicroModel(celsius=6.3)
+    targets_n = rng.integers(700, 1201, n_cells)
+    morph = []
+    for c in range(n_cells):
+        secs = _pyramidal(rng, int(targets_n[c]))
+        cell = M.add_population(model, secs, 1, voltage=-65.0)[0]
+        M.insert(cell, builtin("hh"), sections=["soma", "prox"])
+        M.insert(cell, builtin("pas"), sections=["apical", "basal"], params={"g": 1.0e-4, "e": -65.0})
+        M.register_spike_source(cell, threshold=-10.0)
+        morph.append((cell, secs))
+    n = n_cells * synapses_per_cell
+    owners = np.repeat(np.arange(1, n_cells + 1), synapses_per_cell)
+    names, xs = [], []
+    n_basal = int(round(0.8 * synapses_per_cell))
+    for cell, secs in morph:
+        nb, xb = _dendritic_sites(rng, secs, n_basal, labels=("basal", "prox"))
+        na, xa = _dendritic_sites(rng, secs, synapses_per_cell - n_basal, labels=("apical",))
+        names.extend(nb + na)
+        xs.append(np.concatenate([xb, xa]))
+    xs = np.concatenate(xs)
+    e_rev = np.where(rng.uniform(size=n) < 0.85, 0.0, -80.0)
+    first_syn = M.add_pointprocesses(model, builtin("Exp2Syn"), owners, names, xs,
+                                     {"tau1": 0.5, "tau2": 5.0, "e": e_rev})
+    k_in = int(round(connectivity * n_cells))
+    pre, post = [], []
+    for c in range(n_cells):
+        choices = rng.choice(n_cells - 1, size=k_in, replace=False)
+        choices = np.where(choices >= c, choices + 1, choices)
+        pre.append(choices + 1)
+        post.append(first_syn + c * synapses_per_cell + rng.integers(0, synapses_per_cell, k_in))
+    pre = np.concatenate(pre) if pre else np.zeros(0, np.int64)
+    post = np.concatenate(post) if post else np.zeros(0, np.int64)
+    M.connect_many(model, pre, post, rng.lognormal(math.log(0.3), 0.7, len(pre)) / 1000.0,
+                   rng.uniform(0.5, 3.0, len(pre)))
+    first_stim = M.add_pointprocesses(model, builtin("NetStim"), np.zeros(n, np.int64), "none",
+                                      np.zeros(n), {"interval": 1000.0 / background_hz,
+                                                    "number": 1e9, "start": 0.0, "noise": 1.0})
+    sources = M.register_point_sources(model, np.arange(first_stim, first_stim + n))
+    M.connect_many(model, sources, np.arange(first_syn, first_syn + n),
+                   rng.lognormal(math.log(0.3), 0.7, n) / 1000.0, np.zeros(n))
+    n_clamp = max(1, n_cells // 10) if n_cells >= 1 else 0
+    M.add_pointprocesses(model, builtin("IClamp"), np.arange(1, n_clamp + 1), "soma",
+                         np.full(n_clamp, 0.5), {"del": iclamp_onset, "dur": 50.0, "amp": 0.1})
+    return model
+
+
+CONFIGS = {1: config1, 2: config2, 3: config3}
+
+
+def compartment_count(layout) -> int:
+    """Number of compartments (segments) in a built layout: the metric's unit."""
+    return layout.segment_count

@@ -1,0 +1,165 @@
+"""initialize / run / step through libmindgpu.so (the reference's runtime seams).
+
+Mirrors MIND.jl's runtime API (src/runtime/initialize.jl:256-429,
+src/runtime/step.jl:4-86, src/runtime/recording.jl:1-295): `initialize`
+uploads the built layout and runs INITIAL, `run` advances to an absolute stop
+time that must be an integer number of steps away and returns a
+SimulationResult with the recorded traces and the spike raster sorted by
+(time, sid).  Every call goes through the C-ABI; nothing here computes.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+from typing import Dict, List, Sequence
+
+import numpy as np
+
+from . import abi
+
+
+@dataclass(frozen=True)
+class RecordSpec:
+    """A recorded quantity (src/model/references.jl:4-12); this build records voltages."""
+
+    node: int  # global 1-based node
+    name: str
+    kind: int = abi.MIND_RECORD_VOLTAGE
+
+
+@dataclass
+class SimulationResult:
+    time: np.ndarray
+    traces: Dict[str, np.ndarray] = field(default_factory=dict)
+    spike_times: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    spike_sources: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
+    device_ms: float = 0.0
+
+
+class DeviceState:
+    """Owns one libmindgpu handle for a built layout."""
+
+    def __init__(self, layout, precision: str = "fp64"):
+        self.lib = abi.load_library()
+        self.layout = layout
+        self.c_layout = layout.to_c()
+        handle = ctypes.c_void_p()
+        status = self.lib.mind_create(ctypes.byref(self.c_layout), ctypes.byref(handle))
+        if status != abi.MIND_OK:
+            message = self.lib.mind_last_error(None)
+            raise abi.MindError(status, message.decode() if message else "")
+        self.handle = handle
+        self.set_precision(precision)
+
+    def set_precision(self, precision: str) -> None:
+        mode = {"fp64": abi.MIND_FP64, "mixed": abi.MIND_MIXED}[precision]
+        abi.check(self.lib, self.handle, self.lib.mind_set_precision(self.handle, mode))
+
+    def initialize(self) -> None:
+        abi.check(self.lib, self.handle, self.lib.mind_initialize(self.handle))
+
+    def time(self):
+        step = ctypes.c_int64()
+        t = ctypes.c_double()
+        abi.check(self.lib, self.handle, self.lib.mind_time(self.handle, ctypes.byref(step), ctypes.byref(t)))
+        return step.value, t.value
+
+    def run_steps(self, steps: int, records: Sequence[RecordSpec], record_spikes: bool = True):
+        recs = (abi.MindRecord * max(1, len(records)))()
+        for i, r in enumerate(records):
+            recs[i].kind = r.kind
+            recs[i].node = r.node
+        start_step, _ = self.time()
+        abi.check(self.lib, self.handle,
+                  self.lib.mind_run(self.handle, steps, recs, len(records), 1 if record_spikes else 0))
+        samples = steps + 1
+        trace = np.zeros((samples, len(records)))
+        if records:
+            abi.check(self.lib, self.handle, self.lib.mind_get_trace(
+                self.handle, trace.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), trace.size))
+        n = ctypes.c_int64()
+        abi.check(self.lib, self.handle, self.lib.mind_get_spikes(self.handle, None, None, 0, ctypes.byref(n)))
+        times = np.zeros(n.value)
+        sids = np.zeros(n.value, dtype=np.int64)
+        if n.value:
+            abi.check(self.lib, self.handle, self.lib.mind_get_spikes(
+                self.handle, times.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                sids.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), n.value, ctypes.byref(n)))
+        ms = ctypes.c_double()
+        abi.check(self.lib, self.handle, self.lib.mind_last_run_ms(self.handle, ctypes.byref(ms)))
+        time = np.arange(start_step, start_step + samples, dtype=np.float64) * self.layout.dt
+        result = SimulationResult(time, {}, times, sids, ms.value)
+        for i, r in enumerate(records):
+            result.traces[r.name] = trace[:, i].copy()
+        return result
+
+    def step(self) -> None:
+        abi.check(self.lib, self.handle, self.lib.mind_step(self.handle))
+
+    def read_voltage(self, node: int) -> float:
+        value = ctypes.c_double()
+        abi.check(self.lib, self.handle, self.lib.mind_read_voltage(self.handle, node, ctypes.byref(value)))
+        return value.value
+
+    def inject_event(self, connection: int, t: float) -> None:
+        edge = int(self.layout.connection_edges[connection - 1])
+        abi.check(self.lib, self.handle, self.lib.mind_inject_event(self.handle, edge, float(t)))
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            self.lib.mind_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def initialize(model, precision: str = "fp64"):
+    """initialize!: allocate on the device (first call) and run INITIAL."""
+    if model.layout is None:
+        raise ValueError("model is not built")
+    if model.state is None:
+        model.state = DeviceState(model.layout, precision)
+    else:
+        model.state.set_precision(precision)
+    model.state.initialize()
+    return model
+
+
+def _steps_to(layout, state: DeviceState, stop_time: float) -> int:
+    _, now = state.time()
+    duration = float(stop_time) - now
+    if not np.isfinite(duration):
+        raise ValueError("stop time must be finite")
+    count = int(round(duration / layout.dt))
+    tolerance = 64.0 * np.spacing(max(abs(stop_time), abs(now), layout.dt))
+    if count < 0 or abs(duration - count * layout.dt) > tolerance:
+        raise ValueError("stop time must be an integer number of steps after the current time")
+    return count
+
+
+def run(model, stop_time: float, *, records: Sequence[RecordSpec] = (), record_spikes: bool = True):
+    """run!: advance to an absolute stop time and return a SimulationResult."""
+    if model.state is None:
+        raise ValueError("simulation is not initialized")
+    steps = _steps_to(model.layout, model.state, stop_time)
+    return model.state.run_steps(steps, list(records), record_spikes)
+
+
+def step(model):
+    if model.state is None:
+        raise ValueError("simulation is not initialized")
+    model.state.step()
+    return model
+
+
+def voltage_record(model, cell, *, section: str = "soma", x: float = 0.5, name=None) -> RecordSpec:
+    node = model.layout.voltage_node(cell.index, section, x)
+    return RecordSpec(node, name if name is not None else f"v_{cell.gid}")
+
+
+def simulation_time(model) -> float:
+    return model.state.time()[1]

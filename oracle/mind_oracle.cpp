@@ -1,0 +1,613 @@
+/*
+ * mind_oracle.cpp — CPU FP64 restatement of MIND.jl's per-micro-step loop.
+ *
+ * TEST INFRASTRUCTURE.  This is the checker for libmindgpu.so's FP64 mode and
+ * the timed CPU baseline; only tests/, __graft_entry__.smoke() and bench.py's
+ * CPU legs load it.  The product never calls it.
+ *
+ * It consumes the same MindLayout the library receives (include/mindgpu.h)
+ * and follows the reference's algorithm, not the library's:
+ *   - step order of advance_micro! (src/runtime/step.jl:91-151): detection at
+ *     t + 1e-10 from the completed boundary (src/runtime/utils/step.jl:143-156,
+ *     src/runtime/cuda/micro.jl:285-302), routing, delivery through t + dt/2,
+ *     currents at t + dt/2, assembly, Hines solve, voltage update, state
+ *     advance at t + dt, recording, delivery through the new boundary;
+ *   - a CPU binary heap keyed (time, order, target) with order assigned at
+ *     enqueue (src/runtime/utils/events.jl:7-62) and NET_RECEIVE applied in
+ *     pop order (src/runtime/events.jl:57-165), NetStim self-events and
+ *     net_event fanout re-entering the heap before the next pop;
+ *   - the current probe at v + 0.001 and v with rhs -= s*i, d += s*di/0.001,
+ *     s = area*0.01 for density and 1 for point mechanisms
+ *     (src/runtime/cuda/micro.jl:427-500), currents summed in the MOD's
+ *     order (NONSPECIFIC then USEION writes, src/runtime/initialize.jl:496-501);
+ *   - assembly d = C/dt + d + axial_diagonal, rhs += a (v_p - v)
+ *     (src/runtime/cuda/micro.jl:633-657), Hines elimination
+ *     d_p -= (a/d) a, rhs_p += (a/d) rhs and back-substitution
+ *     x = (rhs + a x_p)/d (src/runtime/cuda/micro.jl:688-749);
+ *   - cnexp as the reference lowers relaxation equations:
+ *     s += (1 - exp(dt * (-1/tau))) (s_inf - s) (src/compiler/codegen.jl:569-641);
+ *   - mechanism equations of mod/{hh,pas,ExpSyn,Exp2Syn,NetStim,IClamp}.mod;
+ *   - NetStim's Philox streams (src/runtime/cuda/micro.jl:3-91).
+ * Where the reference's result depends on the order of concurrent FP64
+ * atomics (siblings eliminated into one parent, several point processes or
+ * children adding into one node) this restatement fixes the order: a node's
+ * own term first, then children in ascending node index; mechanism groups in
+ * layout order; rows in row order.  The library uses the same order, which
+ * makes FP64 parity bit-exact.  Both sides call mind_math.h for exp/log/pow.
+ */
+#include "../include/mindgpu.h"
+#include "../mind.jl_b200/csrc/mind_math.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <queue>
+#include <string>
+#include <vector>
+
+#include <atomic>
+#include <thread>
+
+namespace {
+
+struct Event {
+    double time;
+    double flag;
+    int64_t edge;   // 1-based, 0 = self event
+    int64_t order;
+    int32_t target; // 1-based point index
+};
+
+struct Later {
+    bool operator()(const Event &a, const Event &b) const {
+        // priority_queue pops the largest; "largest" = earliest by event_before.
+        if (a.time != b.time) return a.time > b.time;
+        if (a.order != b.order) return a.order > b.order;
+        return a.target > b.target;
+    }
+};
+
+struct Group {
+    int32_t kind;
+    int64_t rows;
+    std::vector<int32_t> node;     // 0-based, -1 for artificial
+    std::vector<std::vector<double>> f;  // fields by canonical slot
+    uint64_t digest;
+    std::vector<uint64_t> logical;
+};
+
+enum { HH_GNABAR, HH_GKBAR, HH_GL, HH_EL, HH_M, HH_H, HH_N, HH_ENA, HH_EK, HH_NF };
+enum { PAS_G, PAS_E, PAS_NF };
+enum { ES_TAU, ES_E, ES_G, ES_NF };
+enum { E2_TAU1, E2_TAU2, E2_E, E2_A, E2_B, E2_FACTOR, E2_NF };
+enum { NS_INTERVAL, NS_NUMBER, NS_START, NS_NOISE, NS_EVENT, NS_ON, NS_ISPIKE, NS_NF };
+enum { IC_DEL, IC_DUR, IC_AMP, IC_NF };
+
+const char *const HH_NAMES[] = {"gnabar", "gkbar", "gl", "el", "m", "h", "n", "ena", "ek"};
+const char *const PAS_NAMES[] = {"g", "e"};
+const char *const ES_NAMES[] = {"tau", "e", "g"};
+const char *const E2_NAMES[] = {"tau1", "tau2", "e", "A", "B", "factor"};
+const char *const NS_NAMES[] = {"interval", "number", "start", "noise", "event", "on", "ispike"};
+const char *const IC_NAMES[] = {"del", "dur", "amp"};
+
+struct Oracle {
+    const MindLayout *L;
+    int64_t n;
+    double dt, celsius;
+    uint64_t seed;
+    std::vector<int32_t> parent;  // 0-based, -1 root
+    std::vector<double> v, d, rhs, cap, a, ad, area, xd, xr;
+    std::vector<int64_t> child_off;
+    std::vector<int32_t> child;   // ascending
+    std::vector<std::vector<int32_t>> cell_up;    // per cell: nodes children-before-parent
+    std::vector<Group> groups;
+    std::vector<MindRan> ran;     // per NetStim row, indexed via group
+    std::vector<char> above;
+    std::priority_queue<Event, std::vector<Event>, Later> heap;
+    int64_t next_order = 0;
+    int64_t step = 0;
+    int error = 0;
+    std::string message;
+    std::vector<double> spike_t;
+    std::vector<int64_t> spike_sid;
+    std::vector<int64_t> point_source;  // per point (0-based) -> source index (0-based) or -1
+
+    int fail(int code, const std::string &why) {
+        if (!error) {
+            error = code;
+            message = why;
+        }
+        return code;
+    }
+
+    int load(const MindLayout *layout) {
+        L = layout;
+        if (L->abi_version != MIND_ABI_VERSION) return fail(MIND_ELAYOUT, "ABI version");
+        if (L->secondorder != 0) return fail(MIND_ELAYOUT, "secondorder must be 0");
+        n = L->n_nodes;
+        dt = L->dt;
+        celsius = L->celsius;
+        seed = L->seed;
+        parent.resize(n);
+        for (int64_t i = 0; i < n; ++i) parent[i] = L->parent[i] - 1;
+        v.assign(L->voltage, L->voltage + n);
+        cap.assign(L->capacitance, L->capacitance + n);
+        a.assign(L->axial, L->axial + n);
+        ad.assign(L->axial_diagonal, L->axial_diagonal + n);
+        area.assign(L->area, L->area + n);
+        d.assign(n, 0.0);
+        rhs.assign(n, 0.0);
+        xd.assign(n, 0.0);
+        xr.assign(n, 0.0);
+        // children CSR, ascending
+        std::vector<int64_t> count(n + 1, 0);
+        for (int64_t i = 0; i < n; ++i)
+            if (parent[i] >= 0) count[parent[i] + 1]++;
+        child_off.assign(n + 1, 0);
+        for (int64_t i = 0; i < n; ++i) child_off[i + 1] = child_off[i] + count[i + 1];
+        child.assign(child_off[n], 0);
+        std::vector<int64_t> cursor(child_off.begin(), child_off.end() - 1);
+        for (int64_t i = 0; i < n; ++i)
+            if (parent[i] >= 0) child[cursor[parent[i]]++] = (int32_t)i;
+        // cells: BFS from each root; up-order = reverse BFS
+        for (int64_t r = 0; r < n; ++r) {
+            if (parent[r] >= 0) continue;
+            std::vector<int32_t> bfs{(int32_t)r};
+            for (size_t k = 0; k < bfs.size(); ++k)
+                for (int64_t c = child_off[bfs[k]]; c < child_off[bfs[k] + 1]; ++c) bfs.push_back(child[c]);
+            std::reverse(bfs.begin(), bfs.end());
+            cell_up.push_back(std::move(bfs));
+        }
+        // mechanisms
+        for (int32_t g = 0; g < L->n_mechanisms; ++g) {
+            const MindMechanism &m = L->mechanisms[g];
+            Group G;
+            G.kind = m.kind;
+            G.rows = m.rows;
+            G.digest = m.digest;
+            const char *const *names = nullptr;
+            int nf = 0;
+            switch (m.kind) {
+                case MIND_MECH_HH: names = HH_NAMES; nf = HH_NF; break;
+                case MIND_MECH_PAS: names = PAS_NAMES; nf = PAS_NF; break;
+                case MIND_MECH_EXPSYN: names = ES_NAMES; nf = ES_NF; break;
+                case MIND_MECH_EXP2SYN: names = E2_NAMES; nf = E2_NF; break;
+                case MIND_MECH_NETSTIM: names = NS_NAMES; nf = NS_NF; break;
+                case MIND_MECH_ICLAMP: names = IC_NAMES; nf = IC_NF; break;
+                default: return fail(MIND_ELAYOUT, "unsupported mechanism kind");
+            }
+            G.f.resize(nf);
+            for (int k = 0; k < nf; ++k) {
+                int found = -1;
+                for (int j = 0; j < m.n_fields; ++j)
+                    if (std::strcmp(m.field_names[j], names[k]) == 0) found = j;
+                if (found < 0) return fail(MIND_ELAYOUT, std::string("missing field ") + names[k]);
+                G.f[k].assign(m.data + (int64_t)found * m.rows, m.data + (int64_t)(found + 1) * m.rows);
+            }
+            G.node.resize(m.rows);
+            for (int64_t r = 0; r < m.rows; ++r) G.node[r] = m.nodes[r] - 1;
+            G.logical.assign(m.logical_ids, m.logical_ids + m.rows);
+            groups.push_back(std::move(G));
+        }
+        point_source.assign(L->n_points, -1);
+        for (int64_t s = 0; s < L->n_sources; ++s)
+            if (L->source_points[s] > 0) point_source[L->source_points[s] - 1] = s;
+        above.assign(L->n_sources, 0);
+        return 0;
+    }
+
+    void enqueue(double time, double flag, int64_t edge, int32_t target) {
+        heap.push(Event{time, flag, edge, ++next_order, target});
+    }
+
+    void emit_spike(int64_t source, double time) {
+        spike_t.push_back(time);
+        spike_sid.push_back(L->source_ids[source]);
+        for (int64_t e = L->fanout_offsets[source] - 1; e < L->fanout_offsets[source + 1] - 1; ++e)
+            enqueue(time + L->edge_delays[e], 0.0, e + 1, L->edge_targets[e]);
+    }
+
+    // ---- NetStim (mod/NetStim.mod) ----
+    double invl(Group &G, int64_t r, double mean) {
+        if (mean <= 0.0) mean = 0.01;
+        double noise = G.f[NS_NOISE][r];
+        if (noise == 0.0) return mean;
+        double erand = mind_ran_negexp(&ran[r], seed);
+        return (1.0 - noise) * mean + noise * mean * erand;
+    }
+    void init_sequence(Group &G, int64_t r) {
+        if (G.f[NS_NUMBER][r] > 0.0) {
+            G.f[NS_ON][r] = 1.0;
+            G.f[NS_EVENT][r] = 0.0;
+            G.f[NS_ISPIKE][r] = 0.0;
+        }
+    }
+    void next_invl(Group &G, int64_t r) {
+        if (G.f[NS_NUMBER][r] > 0.0) G.f[NS_EVENT][r] = invl(G, r, G.f[NS_INTERVAL][r]);
+        if (G.f[NS_ISPIKE][r] >= G.f[NS_NUMBER][r]) G.f[NS_ON][r] = 0.0;
+    }
+    void net_send(double t, double delay, double flag, int32_t point) {
+        if (delay < 0.0 || !std::isfinite(delay)) {
+            fail(MIND_ESELFEVENT, "invalid self-event delay");
+            return;
+        }
+        enqueue(t + delay, flag, 0, point);
+    }
+    void netstim_receive(Group &G, int64_t r, int32_t point, double t, double flag, double w) {
+        if (flag == 0.0) {
+            if (w > 0.0 && G.f[NS_ON][r] == 0.0) {
+                init_sequence(G, r);
+                next_invl(G, r);
+                G.f[NS_EVENT][r] = G.f[NS_EVENT][r] - G.f[NS_INTERVAL][r] * (1.0 - G.f[NS_NOISE][r]);
+                net_send(t, G.f[NS_EVENT][r], 1.0, point);
+            } else if (w < 0.0) {
+                G.f[NS_ON][r] = 0.0;
+            }
+        }
+        if (flag == 3.0) {
+            if (G.f[NS_ON][r] == 1.0) {
+                init_sequence(G, r);
+                net_send(t, 0.0, 1.0, point);
+            }
+        }
+        if (flag == 1.0 && G.f[NS_ON][r] == 1.0) {
+            G.f[NS_ISPIKE][r] = G.f[NS_ISPIKE][r] + 1.0;
+            int64_t source = point_source[point - 1];
+            if (source >= 0) emit_spike(source, t);
+            next_invl(G, r);
+            if (G.f[NS_ON][r] == 1.0) net_send(t, G.f[NS_EVENT][r], 1.0, point);
+        }
+    }
+
+    // ---- hh rates (mod/hh.mod) ----
+    static double vtrap(double x, double y) {
+        if (std::fabs(x / y) < 1e-6) return y * (1.0 - x / y / 2.0);
+        return x / (mind_exp(x / y) - 1.0);
+    }
+    struct Rates { double minf, hinf, ninf, mtau, htau, ntau; };
+    Rates rates(double vv) const {
+        Rates R;
+        double q10 = mind_pow(3.0, (celsius - 6.3) / 10.0);
+        double alpha = 0.1 * vtrap(-(vv + 40.0), 10.0);
+        double beta = 4.0 * mind_exp(-(vv + 65.0) / 18.0);
+        double sum = alpha + beta;
+        R.mtau = 1.0 / (q10 * sum);
+        R.minf = alpha / sum;
+        alpha = 0.07 * mind_exp(-(vv + 65.0) / 20.0);
+        beta = 1.0 / (mind_exp(-(vv + 35.0) / 10.0) + 1.0);
+        sum = alpha + beta;
+        R.htau = 1.0 / (q10 * sum);
+        R.hinf = alpha / sum;
+        alpha = 0.01 * vtrap(-(vv + 55.0), 10.0);
+        beta = 0.125 * mind_exp(-(vv + 65.0) / 80.0);
+        sum = alpha + beta;
+        R.ntau = 1.0 / (q10 * sum);
+        R.ninf = alpha / sum;
+        return R;
+    }
+    static double cnexp(double s, double inf, double tau, double step_dt) {
+        return s + (1.0 - mind_exp(step_dt * (-1.0 / tau))) * (inf - s);
+    }
+
+    void initialize() {
+        step = 0;
+        for (auto &G : groups) {
+            for (int64_t r = 0; r < G.rows; ++r) {
+                switch (G.kind) {
+                    case MIND_MECH_HH: {
+                        Rates R = rates(v[G.node[r]]);
+                        G.f[HH_M][r] = R.minf;
+                        G.f[HH_H][r] = R.hinf;
+                        G.f[HH_N][r] = R.ninf;
+                    } break;
+                    case MIND_MECH_EXPSYN: G.f[ES_G][r] = 0.0; break;
+                    case MIND_MECH_EXP2SYN: {
+                        double &tau1 = G.f[E2_TAU1][r];
+                        double tau2 = G.f[E2_TAU2][r];
+                        if (tau1 / tau2 > 0.9999) tau1 = 0.9999 * tau2;
+                        if (tau1 / tau2 < 1e-9) tau1 = tau2 * 1e-9;
+                        G.f[E2_A][r] = 0.0;
+                        G.f[E2_B][r] = 0.0;
+                        double tp = (tau1 * tau2) / (tau2 - tau1) * mind_log(tau2 / tau1);
+                        double factor = -mind_exp(-tp / tau1) + mind_exp(-tp / tau2);
+                        G.f[E2_FACTOR][r] = 1.0 / factor;
+                    } break;
+                    default: break;
+                }
+            }
+        }
+        // NetStim INITIAL, groups in order, rows in order (t = 0).
+        for (size_t g = 0; g < groups.size(); ++g) {
+            Group &G = groups[g];
+            if (G.kind != MIND_MECH_NETSTIM) continue;
+            ran.assign(G.rows, MindRan{});
+            for (int64_t r = 0; r < G.rows; ++r) {
+                mind_ran_init(&ran[r], G.logical[r], G.digest, 0u, seed);
+                mind_ran_setseq(&ran[r], 0.0, seed);
+                G.f[NS_ON][r] = 0.0;
+                G.f[NS_ISPIKE][r] = 0.0;
+                if (G.f[NS_NOISE][r] < 0.0) G.f[NS_NOISE][r] = 0.0;
+                if (G.f[NS_NOISE][r] > 1.0) G.f[NS_NOISE][r] = 1.0;
+                if (G.f[NS_START][r] >= 0.0 && G.f[NS_NUMBER][r] > 0.0) {
+                    G.f[NS_ON][r] = 1.0;
+                    double ev = G.f[NS_START][r] + invl(G, r, G.f[NS_INTERVAL][r]) -
+                                G.f[NS_INTERVAL][r] * (1.0 - G.f[NS_NOISE][r]);
+                    if (ev < 0.0) ev = 0.0;
+                    G.f[NS_EVENT][r] = ev;
+                    net_send(0.0, ev, 3.0, point_of(g, r));
+                }
+            }
+        }
+        deliver(0.0);
+    }
+
+    std::vector<std::vector<int32_t>> row_point;  // group -> row -> point (1-based)
+    int32_t point_of(size_t g, int64_t r) { return row_point[g][r]; }
+
+    void build_row_points() {
+        row_point.assign(groups.size(), {});
+        for (size_t g = 0; g < groups.size(); ++g) row_point[g].assign(groups[g].rows, 0);
+        for (int64_t p = 0; p < L->n_points; ++p)
+            row_point[L->point_group[p] - 1][L->point_row[p] - 1] = (int32_t)(p + 1);
+    }
+
+    void receive(const Event &e) {
+        int32_t point = e.target;
+        int32_t g = L->point_group[point - 1] - 1;
+        int64_t r = L->point_row[point - 1] - 1;
+        Group &G = groups[g];
+        double w = e.edge == 0 ? 0.0 : L->edge_weights[e.edge - 1];
+        switch (G.kind) {
+            case MIND_MECH_EXPSYN: G.f[ES_G][r] = G.f[ES_G][r] + w; break;
+            case MIND_MECH_EXP2SYN:
+                G.f[E2_A][r] = G.f[E2_A][r] + w * G.f[E2_FACTOR][r];
+                G.f[E2_B][r] = G.f[E2_B][r] + w * G.f[E2_FACTOR][r];
+                break;
+            case MIND_MECH_NETSTIM: netstim_receive(G, r, point, e.time, e.flag, w); break;
+            default: break;
+        }
+    }
+
+    void deliver(double cutoff) {
+        while (!heap.empty() && heap.top().time <= cutoff) {
+            Event e = heap.top();
+            heap.pop();
+            receive(e);
+        }
+    }
+
+    void currents(double tc) {
+        for (int64_t i = 0; i < n; ++i) {
+            rhs[i] = 0.0;
+            d[i] = 0.0;
+        }
+        for (auto &G : groups) {
+            for (int64_t r = 0; r < G.rows; ++r) {
+                int32_t node = G.node[r];
+                if (node < 0) continue;
+                double vv = v[node];
+                double probe = vv + 0.001;
+                double shifted = 0.0, value = 0.0;
+                double scale = 1.0;
+                bool density = false;
+                switch (G.kind) {
+                    case MIND_MECH_HH: {
+                        density = true;
+                        auto eval = [&](double u) {
+                            double m = G.f[HH_M][r], h = G.f[HH_H][r], nn = G.f[HH_N][r];
+                            double gna = G.f[HH_GNABAR][r] * m * m * m * h;
+                            double ina = gna * (u - G.f[HH_ENA][r]);
+                            double gk = G.f[HH_GKBAR][r] * nn * nn * nn * nn;
+                            double ik = gk * (u - G.f[HH_EK][r]);
+                            double il = G.f[HH_GL][r] * (u - G.f[HH_EL][r]);
+                            return ((0.0 + il) + ina) + ik;
+                        };
+                        shifted = eval(probe);
+                        value = eval(vv);
+                    } break;
+                    case MIND_MECH_PAS: {
+                        density = true;
+                        shifted = 0.0 + G.f[PAS_G][r] * (probe - G.f[PAS_E][r]);
+                        value = 0.0 + G.f[PAS_G][r] * (vv - G.f[PAS_E][r]);
+                    } break;
+                    case MIND_MECH_EXPSYN: {
+                        shifted = 0.0 + G.f[ES_G][r] * (probe - G.f[ES_E][r]);
+                        value = 0.0 + G.f[ES_G][r] * (vv - G.f[ES_E][r]);
+                    } break;
+                    case MIND_MECH_EXP2SYN: {
+                        double gs = G.f[E2_B][r] - G.f[E2_A][r];
+                        shifted = 0.0 + gs * (probe - G.f[E2_E][r]);
+                        value = 0.0 + gs * (vv - G.f[E2_E][r]);
+                    } break;
+                    case MIND_MECH_ICLAMP: {
+                        double del = G.f[IC_DEL][r];
+                        double i = (tc < del + G.f[IC_DUR][r] && tc >= del) ? G.f[IC_AMP][r] : 0.0;
+                        shifted = 0.0 - i;
+                        value = 0.0 - i;
+                    } break;
+                    default: continue;
+                }
+                if (density) {
+                    scale = area[node] * 0.01;
+                    rhs[node] -= scale * value;
+                    d[node] += scale * (shifted - value) / 0.001;
+                } else {
+                    rhs[node] += -scale * value;
+                    d[node] += scale * (shifted - value) / 0.001;
+                }
+            }
+        }
+    }
+
+    int cable(int64_t cell) {
+        const std::vector<int32_t> &up = cell_up[cell];
+        for (int32_t i : up) d[i] = cap[i] / dt + d[i] + ad[i];
+        for (int32_t i : up) {
+            double R = rhs[i];
+            if (parent[i] >= 0) R = R + a[i] * (v[parent[i]] - v[i]);
+            for (int64_t c = child_off[i]; c < child_off[i + 1]; ++c) {
+                int32_t k = child[c];
+                R = R - a[k] * (v[i] - v[k]);
+            }
+            rhs[i] = R;
+        }
+        int status = 0;
+        for (int32_t i : up) {
+            double D = d[i], R = rhs[i];
+            for (int64_t c = child_off[i]; c < child_off[i + 1]; ++c) {
+                int32_t k = child[c];
+                D = D - xd[k];
+                R = R + xr[k];
+            }
+            d[i] = D;
+            rhs[i] = R;
+            if (D == 0.0 || !std::isfinite(D)) status = MIND_ESINGULAR;
+            if (parent[i] >= 0) {
+                double f = a[i] / D;
+                xd[i] = f * a[i];
+                xr[i] = f * R;
+            }
+        }
+        for (auto it = up.rbegin(); it != up.rend(); ++it) {
+            int32_t i = *it;
+            double value = rhs[i];
+            if (parent[i] >= 0) value = value + a[i] * rhs[parent[i]];
+            rhs[i] = value / d[i];
+        }
+        for (int32_t i : up) v[i] = v[i] + rhs[i];
+        return status;
+    }
+
+    void advance(double ta) {
+        (void)ta;
+        for (auto &G : groups) {
+            for (int64_t r = 0; r < G.rows; ++r) {
+                switch (G.kind) {
+                    case MIND_MECH_HH: {
+                        Rates R = rates(v[G.node[r]]);
+                        G.f[HH_M][r] = cnexp(G.f[HH_M][r], R.minf, R.mtau, dt);
+                        G.f[HH_H][r] = cnexp(G.f[HH_H][r], R.hinf, R.htau, dt);
+                        G.f[HH_N][r] = cnexp(G.f[HH_N][r], R.ninf, R.ntau, dt);
+                    } break;
+                    case MIND_MECH_EXPSYN:
+                        G.f[ES_G][r] = cnexp(G.f[ES_G][r], 0.0, G.f[ES_TAU][r], dt);
+                        break;
+                    case MIND_MECH_EXP2SYN:
+                        G.f[E2_A][r] = cnexp(G.f[E2_A][r], 0.0, G.f[E2_TAU1][r], dt);
+                        G.f[E2_B][r] = cnexp(G.f[E2_B][r], 0.0, G.f[E2_TAU2][r], dt);
+                        break;
+                    default: break;
+                }
+            }
+        }
+    }
+
+    void detect(double t) {
+        double time = t + 1.0e-10;
+        for (int64_t s = 0; s < L->n_sources; ++s) {
+            int32_t node = L->source_nodes[s];
+            if (node <= 0) continue;
+            bool current = v[node - 1] > L->source_thresholds[s];
+            if (current && !above[s]) emit_spike(s, time);
+            above[s] = current;
+        }
+    }
+
+    int advance_step(int threads) {
+        double t = (double)step * dt;
+        detect(t);
+        deliver(t + 0.5 * dt);
+        currents(t + 0.5 * dt);
+        int64_t cells = (int64_t)cell_up.size();
+        int status = 0;
+        if (threads <= 1 || cells < 2) {
+            for (int64_t c = 0; c < cells; ++c) {
+                int s = cable(c);
+                if (s > status) status = s;
+            }
+        } else {
+            // Cells are independent: a shared counter hands them out in chunks.
+            std::atomic<int64_t> next{0};
+            std::atomic<int> worst{0};
+            auto worker = [&]() {
+                for (;;) {
+                    int64_t lo = next.fetch_add(16);
+                    if (lo >= cells) break;
+                    int64_t hi = std::min(cells, lo + 16);
+                    for (int64_t c = lo; c < hi; ++c) {
+                        int s = cable(c);
+                        int w = worst.load();
+                        while (s > w && !worst.compare_exchange_weak(w, s)) {
+                        }
+                    }
+                }
+            };
+            std::vector<std::thread> pool;
+            for (int k = 0; k < threads; ++k) pool.emplace_back(worker);
+            for (auto &th : pool) th.join();
+            status = worst.load();
+        }
+        if (status) return fail(status, "singular or non-finite cable system");
+        advance(t + dt);
+        step += 1;
+        return 0;
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+/* Initialize from the layout and run `steps` micro steps.  trace is
+ * [(steps+1) x nrec] sample-major; spikes sorted by (time, sid). */
+int oracle_run(const MindLayout *layout, int64_t steps, const MindRecord *records, int32_t nrec,
+               int32_t threads, double *trace, double *spike_t, int64_t *spike_sid, int64_t cap,
+               int64_t *nspikes, double *run_ms, char *message, int32_t message_len) {
+    Oracle o;
+    int status = o.load(layout);
+    if (!status) {
+        o.build_row_points();
+        o.initialize();
+        status = o.error;
+    }
+    auto record = [&](int64_t sample) {
+        for (int32_t k = 0; k < nrec; ++k) trace[sample * nrec + k] = o.v[records[k].node - 1];
+    };
+    auto t0 = std::chrono::steady_clock::now();
+    if (!status) {
+        if (nrec) record(0);
+        for (int64_t s = 0; s < steps && !status; ++s) {
+            status = o.advance_step(threads);
+            if (status) break;
+            if (nrec) record(s + 1);
+            o.deliver((double)o.step * o.dt);
+            status = o.error;
+        }
+    }
+    auto t1 = std::chrono::steady_clock::now();
+    if (run_ms) *run_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    if (!status) {
+        for (int64_t i = 0; i < o.n; ++i)
+            if (!std::isfinite(o.v[i])) status = o.fail(MIND_ENONFINITE, "non-finite voltage");
+    }
+    std::vector<int64_t> idx(o.spike_t.size());
+    for (size_t i = 0; i < idx.size(); ++i) idx[i] = (int64_t)i;
+    std::stable_sort(idx.begin(), idx.end(), [&](int64_t x, int64_t y) {
+        if (o.spike_t[x] != o.spike_t[y]) return o.spike_t[x] < o.spike_t[y];
+        return o.spike_sid[x] < o.spike_sid[y];
+    });
+    *nspikes = (int64_t)idx.size();
+    for (int64_t i = 0; i < (int64_t)idx.size() && i < cap; ++i) {
+        spike_t[i] = o.spike_t[idx[i]];
+        spike_sid[i] = o.spike_sid[idx[i]];
+    }
+    if (message && message_len > 0) {
+        std::strncpy(message, o.message.c_str(), (size_t)message_len - 1);
+        message[message_len - 1] = 0;
+    }
+    return status;
+}
+
+}  // extern "C"

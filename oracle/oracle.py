@@ -1,0 +1,83 @@
+"""ctypes wrapper of the CPU FP64 oracle (test infrastructure).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU legs import this module;
+it is the checker for the CUDA path and the timed CPU baseline, never part of it.
+`build_oracle()` compiles liboracle.so with the Makefile beside this file.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+_LIB = None
+
+
+def build_oracle() -> str:
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+def _load():
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            build_oracle()
+        lib = ctypes.CDLL(LIB_PATH)
+        lib.oracle_run.restype = ctypes.c_int32
+        lib.oracle_run.argtypes = [
+            ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
+            ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+            ctypes.POINTER(ctypes.c_int64), ctypes.c_int64, ctypes.POINTER(ctypes.c_int64),
+            ctypes.POINTER(ctypes.c_double), ctypes.c_char_p, ctypes.c_int32,
+        ]
+        _LIB = lib
+    return _LIB
+
+
+@dataclass
+class OracleResult:
+    status: int
+    message: str
+    trace: np.ndarray        # [steps+1, n_records]
+    spike_times: np.ndarray
+    spike_sids: np.ndarray
+    run_ms: float
+
+
+def run(layout, steps: int, record_nodes=(), threads: int = 1, spike_cap: int = 1 << 22) -> OracleResult:
+    """Initialize the layout on the CPU and advance `steps` micro steps."""
+    import sys
+
+    pkg = os.path.join(os.path.dirname(HERE), "mind.jl_b200")
+    if pkg not in sys.path:
+        sys.path.insert(0, pkg)
+    from mind_b200 import abi
+
+    lib = _load()
+    c_layout = layout.to_c()
+    nodes = list(record_nodes)
+    recs = (abi.MindRecord * max(1, len(nodes)))()
+    for i, node in enumerate(nodes):
+        recs[i].kind = abi.MIND_RECORD_VOLTAGE
+        recs[i].node = int(node)
+    trace = np.zeros((steps + 1, max(1, len(nodes))))
+    spike_t = np.zeros(spike_cap)
+    spike_sid = np.zeros(spike_cap, dtype=np.int64)
+    count = ctypes.c_int64()
+    ms = ctypes.c_double()
+    message = ctypes.create_string_buffer(256)
+    status = lib.oracle_run(
+        ctypes.addressof(c_layout), steps, ctypes.addressof(recs), len(nodes), threads,
+        trace.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+        spike_t.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+        spike_sid.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), spike_cap, ctypes.byref(count),
+        ctypes.byref(ms), message, 256)
+    n = min(count.value, spike_cap)
+    return OracleResult(status, message.value.decode(), trace[:, :len(nodes)],
+                        spike_t[:n].copy(), spike_sid[:n].copy(), ms.value)
