@@ -1,0 +1,312 @@
+"""Benchmark: compartment-steps/s of the per-micro-step loop on the seeded config-2 network.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mine|reference]
+                    [--cells C] [--precision fp64|mixed|both]
+
+Workload: 10,000 cells with uneven random binary trees (total compartments
+uniform in [100, 1000]), 100 Exp2Syn per cell, recurrent NetCons (delays
+U[1,5] ms), a 5 Hz Poisson NetStim per synapse, dt = 0.025 ms — the seeded
+synthetic network of mind_b200.networks.config2 (no dataset is involved).
+A step is one micro step of the whole network.  `value` is whole-job
+compartment-steps/s with all state resident in HBM; `e2e` is the same metric
+through the public run() call (C-ABI), including the host copies of the
+recorded soma voltages and the spike raster.  Under torchrun every rank
+simulates its own replica of the network (weak scaling; the path has no
+collective).  --impl reference times the CPU FP64 restatement of the
+reference's step loop (oracle/) on the host cores; MIND.jl itself is Julia
+and cannot run on this box.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "mind.jl_b200"))
+
+import numpy as np  # noqa: E402
+
+METRIC = "compartment-steps/s (config 2: 10,000 uneven cells, recurrent Exp2Syn, dt 0.025 ms)"
+UNIT = "compartment-steps/s"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=800)
+    p.add_argument("--warmup", type=int, default=40)
+    p.add_argument("--impl", default="mine", choices=["mine", "reference"])
+    p.add_argument("--cells", type=int, default=10000)
+    p.add_argument("--precision", default="fp64", choices=["fp64", "mixed", "both"])
+    p.add_argument("--cpu-steps", type=int, default=8)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def build_network(cells: int, seed: int):
+    import mind_b200 as mb
+    from mind_b200 import networks
+
+    model = networks.config2(n_cells=cells)
+    layout = mb.build(model, seed=seed)
+    return model, layout
+
+
+def algorithmic_bytes_per_step(layout, events_per_step: float) -> float:
+    """Minimal one-pass HBM traffic of one FP64 micro step.
+
+    Per node 44 B (v read+write, parent index, axial, C, axial_diagonal); per
+    pas row 24 B; per hh row 104 B; per Exp2Syn row 68 B; per ExpSyn row 36 B;
+    per delivered event 44 B.
+    """
+    per_kind = {"pas": 24, "hh": 104, "Exp2Syn": 68, "ExpSyn": 36, "IClamp": 28}
+    total = 44.0 * layout.n_nodes
+    for g in layout.groups:
+        total += per_kind.get(g.mechanism.name, 0) * g.rows
+    return total + 44.0 * events_per_step
+
+
+def delivered_events(layout, spike_sids) -> int:
+    if len(spike_sids) == 0:
+        return 0
+    index = {int(s): k for k, s in enumerate(layout.source_ids)}
+    fan = np.diff(layout.fanout_offsets)
+    return int(sum(fan[index[int(s)]] for s in spike_sids))
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        self.file.flush()
+        self.file.seek(0)
+        rows = [r.strip().split(", ") for r in self.file.read().splitlines() if r.strip()]
+        sm, maxes, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                maxes.append(float(r[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, r[5:9]):
+                if flag.strip().lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        loaded = [x for x in sm if x > 0.5 * max(sm)] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": max(maxes), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline(layout, steps: int, threads: int):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    result = oracle.run(layout, steps, (), threads=threads)
+    if result.status != 0:
+        raise RuntimeError(f"oracle failed: {result.message}")
+    value = layout.segment_count * steps / (result.run_ms / 1000.0)
+    return value, result.run_ms
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+        return float(peaks["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def recorded_traffic():
+    """DRAM bytes per window-kernel launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "window_kernel_traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return None
+
+
+def run_reference(args, rank: int):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    model, layout = build_network(args.cells, seed=1)
+    steps = max(1, args.cpu_steps)
+    values = []
+    for _ in range(max(1, args.steps and 1)):
+        value, ms = cpu_baseline(layout, steps, threads)
+        values.append(value)
+    value = statistics.median(values)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": steps, "warmup": 0, "ms_per_step": ms / steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded config-2 network)",
+        "config": {"workload": "config2", "cells": args.cells, "compartments": layout.segment_count,
+                   "dt_ms": layout.dt, "l2": "state larger than L2"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"first {steps} micro steps of the full config-2 network"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "MIND.jl is Julia (absent here); the reference arm is the CPU FP64 restatement of its step loop",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    import mind_b200 as mb
+
+    model, layout = build_network(args.cells, seed=1 + rank)
+    soma = [mb.RecordSpec(layout.voltage_node(c), f"v{c}") for c in range(1, layout.n_cells + 1)]
+    precisions = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
+    results = {}
+    clocks = None
+    for precision in precisions:
+        mb.initialize(model, precision=precision)
+        model.state.set_profiling(True)
+        dt = layout.dt
+        mb.run(model, args.warmup * dt, record_spikes=False)
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        sampler = ClockSampler(local_rank)
+        with sampler:
+            result = mb.run(model, (args.warmup + args.steps) * dt, record_spikes=True)
+            torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        stats = model.state.run_stats()
+        clocks = sampler.summary()
+        run_ms = stats.run_ms
+        if dist is not None:
+            t = torch.tensor([run_ms], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            run_ms = float(t.item())
+        units = layout.segment_count * args.steps * world
+        value = units / (run_ms / 1000.0)
+        events = delivered_events(layout, result.spike_sources)
+        algo = algorithmic_bytes_per_step(layout, events / args.steps)
+        window_ms = stats.window_ms
+        achieved = algo * args.steps / (window_ms / 1000.0) / 1e9 if window_ms > 0 else None
+        # End to end through the public API: a fresh run call with host recording.
+        mb.initialize(model, precision=precision)
+        mb.run(model, args.warmup * dt, record_spikes=False)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e2e_result = mb.run(model, (args.warmup + args.steps) * dt, records=soma, record_spikes=True)
+        e2e_s = time.perf_counter() - t0
+        if dist is not None:
+            t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        d2h = (len(soma) * 8 * (args.steps + 1) + 16 * len(e2e_result.spike_times)) / args.steps
+        h2d = 8 * len(soma) / args.steps
+        results[precision] = {
+            "value": value, "ms_per_step": run_ms / args.steps, "window_ms": window_ms,
+            "window_launches": stats.window_launches, "launches": stats.launches, "window_steps": stats.window_steps,
+            "bins": stats.bins, "algo_bytes_per_step": algo, "achieved_gbs": achieved,
+            "spikes": int(len(result.spike_times)), "delivered_events": events,
+            "e2e": units / e2e_s, "d2h": d2h, "h2d": h2d,
+        }
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    head = results[precisions[0]]
+    peak, peak_kind = measured_peaks()
+    traffic = recorded_traffic()
+    line = {
+        "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if precisions[0] == "fp64" else "f32-gating/f64-cable",
+        "data": "synthetic (seeded config-2 network, mind_b200.networks.config2)",
+        "config": {"workload": "config2", "cells": args.cells, "compartments": layout.segment_count,
+                   "nodes": layout.n_nodes, "dt_ms": layout.dt, "precision": precisions[0],
+                   "parallelism": f"replica x{world}", "l2": "working set larger than L2 (no flush needed)",
+                   "window_steps": head["window_steps"], "size_bins": head["bins"]},
+        "e2e": {"value": head["e2e"], "unit": UNIT, "h2d_bytes_per_step": head["h2d"],
+                "d2h_bytes_per_step": head["d2h"]},
+        "roofline": {
+            "bound": "hbm",
+            "achieved": head["achieved_gbs"], "peak": peak, "unit": "GB/s",
+            "frac": (head["achieved_gbs"] / peak) if head["achieved_gbs"] else None,
+            "traffic": traffic.get("dram_bytes_per_launch") if traffic else None,
+            "kernel": "window_kernel", "algo_bytes_per_step": head["algo_bytes_per_step"],
+            "peak_source": f"{peak_kind} hbm_gbs",
+            "note": "algorithmic bytes of one pass per step; the window kernel keeps each cell on-chip "
+                    "for a window of steps, so its DRAM traffic is below the algorithmic bytes",
+        },
+        "gpu_launches": head["launches"] + 2,
+        "clocks": clocks,
+        "modes": {k: {"value": v["value"], "ms_per_step": v["ms_per_step"], "e2e": v["e2e"]}
+                  for k, v in results.items()},
+        "spikes": head["spikes"],
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        cpu_value, _ = cpu_baseline(layout, args.cpu_steps, threads)
+        line["cpu_baseline"] = {"value": cpu_value, "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": f"first {args.cpu_steps} micro steps of the full config-2 network"}
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -185,6 +185,24 @@ const char *mind_last_error(const MindHandle *h);
 /* Device-side wall time of the last mind_run, in milliseconds (CUDA events). */
 int mind_last_run_ms(const MindHandle *h, double *ms);
 
+/*
+ * Launch statistics of the last mind_run (no reference counterpart: the
+ * reference has no timers; this is the cudaEvent instrumentation of the run
+ * loop).  window_ms is filled only while profiling is enabled, which brackets
+ * every window-kernel launch with CUDA events on the library's stream.
+ */
+typedef struct MindRunStats {
+    double run_ms;            /* device time of the whole run loop */
+    double window_ms;         /* summed device time of window-kernel launches */
+    int64_t launches;         /* kernels launched by the run loop */
+    int64_t window_launches;  /* window-kernel launches */
+    int64_t steps;            /* micro steps advanced */
+    int32_t window_steps;     /* steps per window (W) */
+    int32_t bins;             /* window-kernel launches per window (cell size bins) */
+} MindRunStats;
+int mind_run_stats(const MindHandle *h, MindRunStats *stats);
+int mind_set_profiling(MindHandle *h, int32_t enable);
+
 int mind_destroy(MindHandle *h);
 
 #ifdef __cplusplus

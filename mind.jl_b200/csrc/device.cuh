@@ -33,7 +33,9 @@
 namespace mind {
 
 constexpr int kMaxGroups = 16;
-constexpr int kThreads = 128;
+constexpr int kThreads = 128;      // auxiliary kernels
+constexpr int kCellThreads = 64;   // window kernel: one cell per CTA of two warps
+
 
 struct RingEvent {       // an event waiting in a delivery bin
     double time;
@@ -71,6 +73,87 @@ enum { HHS_M, HHS_H, HHS_N };
 enum { ESS_G, ESS_DECAY };
 enum { E2S_A, E2S_B, E2S_DECAY1, E2S_DECAY2 };
 
+/* Number of FP64 slots and FP32 (mixed-mode) state slots of each kind. */
+__host__ __device__ inline int kind_slots(int32_t kind) {
+    switch (kind) {
+        case MIND_MECH_HH: return HH_NSLOT;
+        case MIND_MECH_PAS: return PAS_NSLOT;
+        case MIND_MECH_EXPSYN: return ES_NSLOT;
+        case MIND_MECH_EXP2SYN: return E2_NSLOT;
+        case MIND_MECH_ICLAMP: return IC_NSLOT;
+        case MIND_MECH_NETSTIM: return NS_NSLOT;
+        default: return 0;
+    }
+}
+/*
+ * Rows whose state changes every step keep that state in shared memory for the
+ * window; everything else of a row (parameters, decay factors) is streamed
+ * from HBM.  hh rows are few per cell and keep all their slots on chip.
+ *   staged_doubles  FP64 slots staged per row (FP64 mode: hh all, ExpSyn g, Exp2Syn A,B)
+ *   staged_floats   FP32 slots staged per row (mixed mode: hh m,h,n, ExpSyn g, Exp2Syn A,B)
+ */
+__host__ __device__ inline bool kind_staged(int32_t kind) {
+    return kind == MIND_MECH_HH || kind == MIND_MECH_EXPSYN || kind == MIND_MECH_EXP2SYN;
+}
+__host__ __device__ inline int staged_doubles(int32_t kind, bool mixed) {
+    switch (kind) {
+        case MIND_MECH_HH: return HH_NSLOT;
+        case MIND_MECH_EXPSYN: return mixed ? 0 : 1;
+        case MIND_MECH_EXP2SYN: return mixed ? 0 : 2;
+        default: return 0;
+    }
+}
+__host__ __device__ inline int staged_floats(int32_t kind, bool mixed) {
+    if (!mixed) return 0;
+    switch (kind) {
+        case MIND_MECH_HH: return 3;
+        case MIND_MECH_EXPSYN: return 1;
+        case MIND_MECH_EXP2SYN: return 2;
+        default: return 0;
+    }
+}
+/* FP32 state arrays per kind in device memory (mixed mode). */
+/* FP32 state arrays per kind in device memory (mixed mode). */
+__host__ __device__ inline int kind_floats(int32_t kind) {
+    switch (kind) {
+        case MIND_MECH_HH: return 3;
+        case MIND_MECH_EXPSYN: return 2;
+        case MIND_MECH_EXP2SYN: return 4;
+        default: return 0;
+    }
+}
+
+/*
+ * Shared-memory image of one cell for a window (all sizes in elements):
+ *   doubles  v, d, rhs, a [n each]; eliminated pivot and rhs contributions of
+ *            chain tops [nch each]; event increments [inbox_cap]; staged FP64
+ *            slots of the staged rows;
+ *   events   the cell's inbox for the window [inbox_cap];
+ *   floats   staged FP32 slots (mixed mode);
+ *   ints     per staged row: local node and segment length; chain top, length,
+ *            parent, child-chain CSR; level starts; inbox order;
+ *   shorts   chain of every node [n].
+ * Host (to size the launch) and device (to carve the buffer) use this one function.
+ */
+struct CellShape {
+    int32_t n, nch, nkids, nlev;
+    int32_t rows[kMaxGroups];
+};
+
+__host__ __device__ inline size_t cell_smem_bytes(const CellShape &s, const int32_t *kinds, int32_t ngroups,
+                                                  bool mixed, int32_t inbox_cap) {
+    size_t doubles = 4 * (size_t)s.n + 2 * (size_t)s.nch + (size_t)inbox_cap;
+    size_t floats = 0, ints = 0;
+    for (int32_t g = 0; g < ngroups; ++g) {
+        if (!kind_staged(kinds[g])) continue;
+        doubles += (size_t)staged_doubles(kinds[g], mixed) * s.rows[g];
+        floats += (size_t)staged_floats(kinds[g], mixed) * s.rows[g];
+        ints += 2 * (size_t)s.rows[g];
+    }
+    ints += 4 * (size_t)s.nch + 1 + (size_t)s.nkids + (size_t)s.nlev + 1 + (size_t)inbox_cap;
+    return doubles * 8 + (size_t)inbox_cap * sizeof(InboxEvent) + floats * 4 + ints * 4 + 2 * (size_t)s.n;
+}
+
 struct Params {
     int32_t ncells;
     int32_t ngroups;
@@ -81,14 +164,14 @@ struct Params {
     const int64_t *node_off;   // [ncells+1]
     double *v;
     const double *a, *cdt, *ad;
-    const int32_t *parent;     // local parent index or -1
-    const int32_t *kid_off;    // [packed+1] global CSR over local kid indices
-    const int32_t *kids;
+    const int32_t *parent;     // [packed] local parent index or -1
+    const int32_t *kid_off;    // [packed+1] CSR into kids (children in ascending layout index)
+    const int32_t *kids;       // local child indices
     // chains
     const int32_t *chain_off;  // [ncells+1]
-    const int32_t *chain_top, *chain_len, *chain_kid_off, *chain_kids;  // chain_kid_off global CSR
-    const int32_t *level_off;  // [ncells+1] into level_chain
-    const int32_t *level_chain;  // per cell: nlevels+1 entries of local chain starts
+    const int32_t *chain_top, *chain_len, *chain_par, *chain_kid_off, *chain_kids;  // chain_kid_off global CSR
+    const int32_t *level_off;    // [ncells+1] into level_chain
+    const int32_t *level_chain;  // per cell: nlevels+1 local chain starts (chains sorted by level)
     DevGroup groups[kMaxGroups];
     // detectors
     const int32_t *det_off;    // [ncells+1]

@@ -337,53 +337,142 @@ __device__ __forceinline__ bool event_before(const InboxEvent &x, const InboxEve
     return x.edge < y.edge;
 }
 
-__device__ __forceinline__ void apply_event(const Params &P, const InboxEvent &e, bool mixed) {
-    const int32_t g = P.point_group[e.point];
-    const int32_t row = P.point_row[e.point];
-    const DevGroup &G = P.groups[g];
-    const double w = e.edge >= 0 ? P.edge_weight[e.edge] : 0.0;
+/* One mechanism group of the resident cell: staged state in shared memory, the rest in HBM. */
+struct StagedGroup {
+    int32_t kind, rows, r0;   // r0 = first device row of the cell
+    double *f;                // staged FP64 slots [slots][rows]
+    float *s;                 // staged FP32 slots [slots][rows] (mixed mode)
+    int32_t *node, *seg;      // local node and segment length per row
+    __device__ __forceinline__ double &at(int slot, int r) const { return f[slot * rows + r]; }
+    __device__ __forceinline__ float &fat(int slot, int r) const { return s[slot * rows + r]; }
+};
+
+/* NET_RECEIVE of the synapses (mod/ExpSyn.mod: g += w; mod/Exp2Syn.mod: A += w*factor,
+ * B += w*factor) on a staged row; `inc` is w, or w*factor for Exp2Syn. */
+template <bool MIXED>
+__device__ __forceinline__ void apply_event(const StagedGroup &G, int32_t row, double inc) {
     if (G.kind == MIND_MECH_EXPSYN) {
-        if (mixed)
-            G.s[ESS_G][row] = G.s[ESS_G][row] + (float)w;
+        if (MIXED)
+            G.fat(0, row) = G.fat(0, row) + (float)inc;
         else
-            G.f[ES_G][row] = G.f[ES_G][row] + w;
+            G.at(0, row) = G.at(0, row) + inc;
     } else if (G.kind == MIND_MECH_EXP2SYN) {
-        if (mixed) {
-            float wf = (float)(w * G.f[E2_FACTOR][row]);
-            G.s[E2S_A][row] = G.s[E2S_A][row] + wf;
-            G.s[E2S_B][row] = G.s[E2S_B][row] + wf;
+        if (MIXED) {
+            const float wf = (float)inc;
+            G.fat(0, row) = G.fat(0, row) + wf;
+            G.fat(1, row) = G.fat(1, row) + wf;
         } else {
-            G.f[E2_A][row] = G.f[E2_A][row] + w * G.f[E2_FACTOR][row];
-            G.f[E2_B][row] = G.f[E2_B][row] + w * G.f[E2_FACTOR][row];
+            G.at(0, row) = G.at(0, row) + inc;
+            G.at(1, row) = G.at(1, row) + inc;
         }
     }
 }
 
+/*
+ * One CTA of two warps advances one cell through W micro steps.  Shared memory
+ * holds what the serial parts of the step touch: v, d, rhs and axial
+ * conductance of every node, the chain tables of the Hines solve, the state
+ * that changes every step (hh gates, synaptic conductances) and the window's
+ * events.  Parameter-only data (pas rows, synapse constants, IClamp rows,
+ * C/dt, axial_diagonal) is streamed from HBM each step with coalesced loads.
+ *
+ * The Hines solve runs level by level (a chain's level exceeds its children's),
+ * one chain per thread; along a chain only subtract -> divide -> multiply stays
+ * on the dependency chain, the next node's operands being loaded ahead.
+ */
 template <bool MIXED>
-__global__ void __launch_bounds__(kThreads) window_kernel(const Params P, int64_t n0, int32_t W) {
+__global__ void __launch_bounds__(kCellThreads, 8) window_kernel(const Params P, const int32_t *cells, int64_t n0,
+                                                              int32_t W) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int32_t s_nev;
-    const int32_t c = blockIdx.x;
+    __shared__ StagedGroup sg[kMaxGroups];
+    const int32_t c = cells[blockIdx.x];
     const int32_t tid = threadIdx.x;
-    const int32_t T = blockDim.x;
+    constexpr int32_t T = kCellThreads;
     const int64_t nb = P.node_off[c];
     const int32_t n = (int32_t)(P.node_off[c + 1] - nb);
     const int32_t cb = P.chain_off[c];
     const int32_t nch = P.chain_off[c + 1] - cb;
-    double *sv = reinterpret_cast<double *>(smem_raw);
-    double *sd = sv + n;
-    double *sr = sd + n;
-    double *sa = sr + n;
-    double *sxd = sa + n;
-    double *sxr = sxd + nch;
-    InboxEvent *sev = reinterpret_cast<InboxEvent *>(sxr + nch);
-    int32_t *sorder = reinterpret_cast<int32_t *>(sev + P.inbox_cap);
+    const int32_t kb = P.chain_kid_off[cb];
+    const int32_t nkids = P.chain_kid_off[cb + nch] - kb;
+    const int32_t lv0 = P.level_off[c];
+    const int32_t nlev = P.level_off[c + 1] - lv0 - 1;
 
-    if (c == 0 && tid < W) P.ring_count[(n0 + tid) % P.ring_slots] = 0;
+    // ---- carve shared memory (order fixed by cell_smem_bytes) ----
+    double *dp = reinterpret_cast<double *>(smem_raw);
+    double *sv = dp; dp += n;
+    double *sd = dp; dp += n;
+    double *sr = dp; dp += n;
+    double *sa = dp; dp += n;
+    double *sxd = dp; dp += nch;
+    double *sxr = dp; dp += nch;
+    double *sw = dp; dp += P.inbox_cap;
+    for (int32_t g = 0; g < P.ngroups; ++g) {
+        const DevGroup &G = P.groups[g];
+        const bool staged = kind_staged(G.kind);
+        const int32_t r0 = G.row_off[c];
+        const int32_t rows = G.kind == MIND_MECH_NETSTIM ? 0 : G.row_off[c + 1] - r0;
+        if (tid == 0) {
+            sg[g].kind = G.kind;
+            sg[g].rows = rows;
+            sg[g].r0 = r0;
+            sg[g].f = dp;
+        }
+        if (staged) dp += (size_t)staged_doubles(G.kind, MIXED) * rows;
+    }
+    InboxEvent *sev = reinterpret_cast<InboxEvent *>(dp);
+    float *fp = reinterpret_cast<float *>(sev + P.inbox_cap);
+    for (int32_t g = 0; g < P.ngroups; ++g) {
+        const DevGroup &G = P.groups[g];
+        const int32_t rows = kind_staged(G.kind) ? G.row_off[c + 1] - G.row_off[c] : 0;
+        if (tid == 0) sg[g].s = fp;
+        fp += (size_t)staged_floats(G.kind, MIXED) * rows;
+    }
+    int32_t *ip = reinterpret_cast<int32_t *>(fp);
+    for (int32_t g = 0; g < P.ngroups; ++g) {
+        const DevGroup &G = P.groups[g];
+        const int32_t rows = kind_staged(G.kind) ? G.row_off[c + 1] - G.row_off[c] : 0;
+        if (tid == 0) {
+            sg[g].node = ip;
+            sg[g].seg = ip + rows;
+        }
+        ip += 2 * rows;
+    }
+    int32_t *ctop = ip; ip += nch;
+    int32_t *clen = ip; ip += nch;
+    int32_t *cpar = ip; ip += nch;
+    int32_t *ckoff = ip; ip += nch + 1;
+    int32_t *ckids = ip; ip += nkids;
+    int32_t *lvc = ip; ip += nlev + 1;
+    int32_t *sorder = ip; ip += P.inbox_cap;
+    int16_t *chain_of = reinterpret_cast<int16_t *>(ip);
+    {
+        // The launch sized shared memory for this cell's bin; refuse rather than overrun.
+        uint32_t dynamic_bytes;
+        asm volatile("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dynamic_bytes));
+        const size_t used = (size_t)(reinterpret_cast<unsigned char *>(chain_of + n) - smem_raw);
+        if (used > dynamic_bytes) {
+            if (tid == 0) raise_error(P.error, MIND_ELAYOUT);
+            return;
+        }
+    }
+
+    // ---- stage the cell ----
+    if (blockIdx.x == 0)
+        for (int32_t k = tid; k < W; k += T) P.ring_count[(n0 + k) % P.ring_slots] = 0;
     for (int32_t i = tid; i < n; i += T) {
         sv[i] = P.v[nb + i];
         sa[i] = P.a[nb + i];
     }
+    for (int32_t k = tid; k < nch; k += T) {
+        ctop[k] = P.chain_top[cb + k];
+        clen[k] = P.chain_len[cb + k];
+        cpar[k] = P.chain_par[cb + k];
+        ckoff[k] = P.chain_kid_off[cb + k] - kb;
+    }
+    if (tid == 0) ckoff[nch] = nkids;
+    for (int32_t k = tid; k < nkids; k += T) ckids[k] = P.chain_kids[kb + k];
+    for (int32_t k = tid; k <= nlev; k += T) lvc[k] = P.level_chain[lv0 + k];
     if (tid == 0) {
         int32_t count = P.inbox_count[c];
         if (count > P.inbox_cap) {
@@ -394,8 +483,56 @@ __global__ void __launch_bounds__(kThreads) window_kernel(const Params P, int64_
         P.inbox_count[c] = 0;
     }
     __syncthreads();
+    for (int32_t k = tid; k < nch; k += T)
+        for (int32_t i = ctop[k]; i < ctop[k] + clen[k]; ++i) chain_of[i] = (int16_t)k;
+    for (int32_t g = 0; g < P.ngroups; ++g) {
+        const DevGroup &G = P.groups[g];
+        const StagedGroup &S = sg[g];
+        if (!kind_staged(S.kind) || S.rows == 0) continue;
+        for (int32_t r = tid; r < S.rows; r += T) {
+            const int32_t row = S.r0 + r;
+            switch (S.kind) {
+                case MIND_MECH_HH:
+                    for (int k = 0; k < HH_NSLOT; ++k) S.at(k, r) = G.f[k][row];
+                    if (MIXED) {
+                        S.fat(0, r) = G.s[HHS_M][row];
+                        S.fat(1, r) = G.s[HHS_H][row];
+                        S.fat(2, r) = G.s[HHS_N][row];
+                    }
+                    break;
+                case MIND_MECH_EXPSYN:
+                    if (MIXED)
+                        S.fat(0, r) = G.s[ESS_G][row];
+                    else
+                        S.at(0, r) = G.f[ES_G][row];
+                    break;
+                case MIND_MECH_EXP2SYN:
+                    if (MIXED) {
+                        S.fat(0, r) = G.s[E2S_A][row];
+                        S.fat(1, r) = G.s[E2S_B][row];
+                    } else {
+                        S.at(0, r) = G.f[E2_A][row];
+                        S.at(1, r) = G.f[E2_B][row];
+                    }
+                    break;
+            }
+            S.node[r] = (int32_t)(G.node[row] - nb);
+            S.seg[r] = G.seg[row];
+        }
+    }
     const int32_t nev = s_nev;
     for (int32_t k = tid; k < nev; k += T) sev[k] = P.inbox[(int64_t)c * P.inbox_cap + k];
+    // Detectors stay in registers for the window (at most one per lane; checked at mind_create).
+    const int32_t d0 = P.det_off[c], d1 = P.det_off[c + 1];
+    int32_t my_det = -1, my_src = 0;
+    double my_thr = 0.0;
+    bool my_above = false;
+    if (tid < d1 - d0) {
+        my_det = P.det_node[d0 + tid];
+        my_src = P.det_source[d0 + tid];
+        my_thr = P.det_thr[d0 + tid];
+        my_above = P.above[my_src] != 0;
+    }
     __syncthreads();
     for (int32_t k = tid; k < nev; k += T) {
         int32_t rank = 0;
@@ -407,38 +544,47 @@ __global__ void __launch_bounds__(kThreads) window_kernel(const Params P, int64_
         sorder[rank] = k;
     }
     __syncthreads();
+    // Resolve each event's target to (group, staged row) and its increment once per window.
+    for (int32_t k = tid; k < nev; k += T) {
+        InboxEvent &e = sev[k];
+        const int32_t g = P.point_group[e.point];
+        const int32_t drow = P.point_row[e.point];
+        const double w = e.edge >= 0 ? P.edge_weight[e.edge] : 0.0;
+        sw[k] = P.groups[g].kind == MIND_MECH_EXP2SYN ? w * P.groups[g].f[E2_FACTOR][drow] : w;
+        e.point = (g << 24) | (drow - sg[g].r0);
+    }
+    __syncthreads();
 
-    const int32_t lv0 = P.level_off[c];
-    const int32_t nlev = P.level_off[c + 1] - lv0 - 1;
     const float q10f = (float)mind_pow(3.0, (P.celsius - 6.3) / 10.0);
     int32_t cursor = 0;
+    bool singular = false;
 
     for (int32_t s = 0; s < W; ++s) {
         const int64_t step = n0 + s;
         const double t = (double)step * P.dt;
 
         // 1. Threshold detection from the completed boundary.
-        for (int32_t k = P.det_off[c] + tid; k < P.det_off[c + 1]; k += T) {
-            const int32_t src = P.det_source[k];
-            const bool current = sv[P.det_node[k]] > P.det_thr[k];
-            if (current && !P.above[src]) {
+        if (my_det >= 0) {
+            const bool current = sv[my_det] > my_thr;
+            if (current && !my_above) {
                 int32_t idx = atomicAdd(P.win_spike_count, 1);
                 if (idx < P.win_spike_cap) {
-                    P.win_spike_source[idx] = src;
+                    P.win_spike_source[idx] = my_src;
                     P.win_spike_step[idx] = step;
                 } else {
                     raise_error(P.error, MIND_ECAPACITY);
                 }
             }
-            P.above[src] = current ? 1 : 0;
+            my_above = current;
         }
         // 2. Deliver this step's bin in (target, time, edge) order.
         if (tid == 0) {
             while (cursor < nev) {
-                const InboxEvent &e = sev[sorder[cursor]];
+                const int32_t k = sorder[cursor];
+                const InboxEvent &e = sev[k];
                 if (e.bin > step) break;
                 if (e.bin < step) raise_error(P.error, MIND_ESELFEVENT);
-                apply_event(P, e, MIXED);
+                apply_event<MIXED>(sg[e.point >> 24], e.point & 0xffffff, sw[k]);
                 ++cursor;
             }
         }
@@ -449,127 +595,174 @@ __global__ void __launch_bounds__(kThreads) window_kernel(const Params P, int64_
         }
         __syncthreads();
 
-        // 4. BREAKPOINT currents at v + 0.001 and v, group by group.
+        // 4. BREAKPOINT currents at v + 0.001 and v, group by group; rows of one node in row order.
         const double tc = t + 0.5 * P.dt;
         for (int32_t g = 0; g < P.ngroups; ++g) {
-            const DevGroup &G = P.groups[g];
-            if (G.kind == MIND_MECH_NETSTIM) continue;
-            const int32_t r0 = G.row_off[c], r1 = G.row_off[c + 1];
-            if (r0 == r1) continue;
-            for (int32_t r = r0 + tid; r < r1; r += T) {
-                const int32_t len = G.seg[r];
-                if (len == 0) continue;
-                const int32_t node = (int32_t)(G.node[r] - nb);
-                const double vv = sv[node];
-                const double probe = vv + 0.001;
-                double R = sr[node], D = sd[node];
-                for (int32_t q = r; q < r + len; ++q) {
-                    double shifted, value;
-                    bool density = false;
-                    switch (G.kind) {
-                        case MIND_MECH_HH: {
-                            density = true;
-                            double m, h, nn;
-                            if (MIXED) {
-                                m = (double)G.s[HHS_M][q];
-                                h = (double)G.s[HHS_H][q];
-                                nn = (double)G.s[HHS_N][q];
-                            } else {
-                                m = G.f[HH_M][q];
-                                h = G.f[HH_H][q];
-                                nn = G.f[HH_N][q];
-                            }
-                            shifted = hh_current(probe, m, h, nn, G.f[HH_GNABAR][q], G.f[HH_GKBAR][q],
-                                                 G.f[HH_GL][q], G.f[HH_EL][q], G.f[HH_ENA][q], G.f[HH_EK][q]);
-                            value = hh_current(vv, m, h, nn, G.f[HH_GNABAR][q], G.f[HH_GKBAR][q],
-                                               G.f[HH_GL][q], G.f[HH_EL][q], G.f[HH_ENA][q], G.f[HH_EK][q]);
-                        } break;
-                        case MIND_MECH_PAS: {
-                            density = true;
-                            shifted = 0.0 + G.f[PAS_G][q] * (probe - G.f[PAS_E][q]);
-                            value = 0.0 + G.f[PAS_G][q] * (vv - G.f[PAS_E][q]);
-                        } break;
-                        case MIND_MECH_EXPSYN: {
-                            double gs = MIXED ? (double)G.s[ESS_G][q] : G.f[ES_G][q];
-                            shifted = 0.0 + gs * (probe - G.f[ES_E][q]);
-                            value = 0.0 + gs * (vv - G.f[ES_E][q]);
-                        } break;
-                        case MIND_MECH_EXP2SYN: {
-                            double gs = MIXED ? (double)(G.s[E2S_B][q] - G.s[E2S_A][q])
-                                              : G.f[E2_B][q] - G.f[E2_A][q];
-                            shifted = 0.0 + gs * (probe - G.f[E2_E][q]);
-                            value = 0.0 + gs * (vv - G.f[E2_E][q]);
-                        } break;
-                        case MIND_MECH_ICLAMP: {
-                            const double del = G.f[IC_DEL][q];
-                            const double i = (tc < del + G.f[IC_DUR][q] && tc >= del) ? G.f[IC_AMP][q] : 0.0;
-                            shifted = 0.0 - i;
-                            value = 0.0 - i;
-                        } break;
-                        default:
-                            shifted = value = 0.0;
-                    }
-                    if (density) {
-                        const double scale = G.f[G.kind == MIND_MECH_HH ? HH_SCALE : PAS_SCALE][q];
-                        R = R - scale * value;
-                        D = D + scale * (shifted - value) / 0.001;
-                    } else {
+            const DevGroup &GG = P.groups[g];
+            const StagedGroup G = sg[g];
+            if (G.rows == 0) continue;
+            if (G.kind == MIND_MECH_PAS) {
+                // One row per node; parameters streamed from HBM.
+                const double *pg = GG.f[PAS_G] + G.r0, *pe = GG.f[PAS_E] + G.r0, *ps = GG.f[PAS_SCALE] + G.r0;
+                const int32_t *pn = GG.node + G.r0;
+#pragma unroll 4
+                for (int32_t r = tid; r < G.rows; r += T) {
+                    const int32_t node = (int32_t)(pn[r] - nb);
+                    const double gp = pg[r], ep = pe[r], scale = ps[r];
+                    const double vv = sv[node];
+                    const double probe = vv + 0.001;
+                    const double shifted = 0.0 + gp * (probe - ep);
+                    const double value = 0.0 + gp * (vv - ep);
+                    sr[node] = sr[node] - scale * value;
+                    sd[node] = sd[node] + scale * (shifted - value) / 0.001;
+                }
+            } else if (G.kind == MIND_MECH_ICLAMP) {
+                const int32_t *pn = GG.node + G.r0, *psg = GG.seg + G.r0;
+                for (int32_t r = tid; r < G.rows; r += T) {
+                    const int32_t len = psg[r];
+                    if (len == 0) continue;
+                    const int32_t node = (int32_t)(pn[r] - nb);
+                    double R = sr[node], D = sd[node];
+                    for (int32_t q = G.r0 + r; q < G.r0 + r + len; ++q) {
+                        const double del = GG.f[IC_DEL][q];
+                        const double i = (tc < del + GG.f[IC_DUR][q] && tc >= del) ? GG.f[IC_AMP][q] : 0.0;
+                        const double shifted = 0.0 - i;
+                        const double value = 0.0 - i;
                         R = R + -1.0 * value;
                         D = D + 1.0 * (shifted - value) / 0.001;
                     }
+                    sr[node] = R;
+                    sd[node] = D;
                 }
-                sr[node] = R;
-                sd[node] = D;
+            } else if (G.kind == MIND_MECH_HH) {
+                for (int32_t r = tid; r < G.rows; r += T) {
+                    const int32_t node = G.node[r];
+                    const double vv = sv[node];
+                    const double probe = vv + 0.001;
+                    double m, h, nn;
+                    if (MIXED) {
+                        m = (double)G.fat(0, r);
+                        h = (double)G.fat(1, r);
+                        nn = (double)G.fat(2, r);
+                    } else {
+                        m = G.at(HH_M, r);
+                        h = G.at(HH_H, r);
+                        nn = G.at(HH_N, r);
+                    }
+                    const double shifted = hh_current(probe, m, h, nn, G.at(HH_GNABAR, r), G.at(HH_GKBAR, r),
+                                                      G.at(HH_GL, r), G.at(HH_EL, r), G.at(HH_ENA, r), G.at(HH_EK, r));
+                    const double value = hh_current(vv, m, h, nn, G.at(HH_GNABAR, r), G.at(HH_GKBAR, r),
+                                                    G.at(HH_GL, r), G.at(HH_EL, r), G.at(HH_ENA, r), G.at(HH_EK, r));
+                    const double scale = G.at(HH_SCALE, r);
+                    sr[node] = sr[node] - scale * value;
+                    sd[node] = sd[node] + scale * (shifted - value) / 0.001;
+                }
+            } else if (G.kind == MIND_MECH_EXPSYN || G.kind == MIND_MECH_EXP2SYN) {
+                const bool two = G.kind == MIND_MECH_EXP2SYN;
+                const double *pe = GG.f[two ? E2_E : ES_E] + G.r0;
+                for (int32_t r = tid; r < G.rows; r += T) {
+                    const int32_t len = G.seg[r];
+                    if (len == 0) continue;
+                    const int32_t node = G.node[r];
+                    const double vv = sv[node];
+                    const double probe = vv + 0.001;
+                    double R = sr[node], D = sd[node];
+                    for (int32_t q = r; q < r + len; ++q) {
+                        double gs;
+                        if (two)
+                            gs = MIXED ? (double)(G.fat(1, q) - G.fat(0, q)) : G.at(1, q) - G.at(0, q);
+                        else
+                            gs = MIXED ? (double)G.fat(0, q) : G.at(0, q);
+                        const double e = pe[q];
+                        const double shifted = 0.0 + gs * (probe - e);
+                        const double value = 0.0 + gs * (vv - e);
+                        R = R + -1.0 * value;
+                        D = D + 1.0 * (shifted - value) / 0.001;
+                    }
+                    sr[node] = R;
+                    sd[node] = D;
+                }
             }
             __syncthreads();
         }
 
-        // 5. Cable assembly: d = C/dt + d + axial_diagonal; own axial term, then children.
+        // 5. Cable assembly, node-parallel: d = C/dt + d + axial_diagonal; own axial term, then children.
+#pragma unroll 2
         for (int32_t i = tid; i < n; i += T) {
             const int64_t gi = nb + i;
+            const int32_t k = chain_of[i];
+            const int32_t top = ctop[k];
+            const int32_t bottom = top + clen[k] - 1;
+            const double vi = sv[i];
             sd[i] = (P.cdt[gi] + sd[i]) + P.ad[gi];
             double R = sr[i];
-            const int32_t p = P.parent[gi];
-            if (p >= 0) R = R + sa[i] * (sv[p] - sv[i]);
-            for (int32_t k = P.kid_off[gi]; k < P.kid_off[gi + 1]; ++k) {
-                const int32_t kk = P.kids[k];
-                R = R - sa[kk] * (sv[i] - sv[kk]);
+            const int32_t p = i == top ? cpar[k] : i - 1;
+            if (p >= 0) R = R + sa[i] * (sv[p] - vi);
+            if (i < bottom) {
+                R = R - sa[i + 1] * (vi - sv[i + 1]);
+            } else {
+                for (int32_t q = ckoff[k]; q < ckoff[k + 1]; ++q) {
+                    const int32_t kt = ctop[ckids[q]];
+                    R = R - sa[kt] * (vi - sv[kt]);
+                }
             }
             sr[i] = R;
         }
         __syncthreads();
 
-        // 6. Hines elimination, chains level by level, each chain bottom to top.
+        // 6. Hines elimination, level by level; each chain bottom to top into its parent.
+        //    The inner loop keeps only subtract -> divide -> multiply on the dependency
+        //    chain: the next node's operands are loaded before the current division.
         for (int32_t lv = 0; lv < nlev; ++lv) {
-            const int32_t c0 = P.level_chain[lv0 + lv], c1 = P.level_chain[lv0 + lv + 1];
-            for (int32_t ch = c0 + tid; ch < c1; ch += T) {
-                const int32_t top = P.chain_top[cb + ch];
-                const int32_t bottom = top + P.chain_len[cb + ch] - 1;
+            for (int32_t ch = lvc[lv] + tid; ch < lvc[lv + 1]; ch += T) {
+                const int32_t top = ctop[ch];
+                const int32_t bottom = top + clen[ch] - 1;
+                const bool rooted = cpar[ch] < 0;
                 double D = sd[bottom], R = sr[bottom];
-                for (int32_t k = P.chain_kid_off[cb + ch]; k < P.chain_kid_off[cb + ch + 1]; ++k) {
-                    const int32_t cc = P.chain_kids[k];
+                for (int32_t q = ckoff[ch]; q < ckoff[ch + 1]; ++q) {
+                    const int32_t cc = ckids[q];
                     D = D - sxd[cc];
                     R = R + sxr[cc];
                 }
-                if (D == 0.0 || !isfinite(D)) raise_error(P.error, MIND_ESINGULAR);
+                singular |= (D == 0.0) | !isfinite(D);
                 sd[bottom] = D;
                 sr[bottom] = R;
                 double pxd = 0.0, pxr = 0.0;
-                if (P.parent[nb + bottom] >= 0) {
-                    const double f = sa[bottom] / D;
-                    pxd = f * sa[bottom];
+                if (bottom > top || !rooted) {
+                    const double ab = sa[bottom];
+                    double dn = 0.0, rn = 0.0, an = 0.0;
+                    if (bottom > top) {
+                        dn = sd[bottom - 1];
+                        rn = sr[bottom - 1];
+                        an = sa[bottom - 1];
+                    }
+                    const double f = ab / D;
+                    pxd = f * ab;
                     pxr = f * R;
-                }
-                for (int32_t i = bottom - 1; i >= top; --i) {
-                    D = sd[i] - pxd;
-                    R = sr[i] + pxr;
-                    if (D == 0.0 || !isfinite(D)) raise_error(P.error, MIND_ESINGULAR);
-                    sd[i] = D;
-                    sr[i] = R;
-                    if (P.parent[nb + i] >= 0) {
-                        const double f = sa[i] / D;
-                        pxd = f * sa[i];
-                        pxr = f * R;
+                    // interior nodes: every one has its parent at i - 1
+                    int32_t i = bottom - 1;
+                    for (; i > top; --i) {
+                        const double Di = dn - pxd, Ri = rn + pxr, ai = an;
+                        dn = sd[i - 1];
+                        rn = sr[i - 1];
+                        an = sa[i - 1];
+                        singular |= (Di == 0.0) | !isfinite(Di);
+                        sd[i] = Di;
+                        sr[i] = Ri;
+                        const double fi = ai / Di;
+                        pxd = fi * ai;
+                        pxr = fi * Ri;
+                    }
+                    if (i == top && bottom > top) {
+                        const double Dt = dn - pxd, Rt = rn + pxr;
+                        singular |= (Dt == 0.0) | !isfinite(Dt);
+                        sd[top] = Dt;
+                        sr[top] = Rt;
+                        if (!rooted) {
+                            const double ft = an / Dt;
+                            pxd = ft * an;
+                            pxr = ft * Rt;
+                        }
                     }
                 }
                 sxd[ch] = pxd;
@@ -577,78 +770,96 @@ __global__ void __launch_bounds__(kThreads) window_kernel(const Params P, int64_
             }
             __syncthreads();
         }
-        // 7. Back-substitution, root chain first.
+        // 7. Back-substitution, root chain first, with the voltage update.
         for (int32_t lv = nlev - 1; lv >= 0; --lv) {
-            const int32_t c0 = P.level_chain[lv0 + lv], c1 = P.level_chain[lv0 + lv + 1];
-            for (int32_t ch = c0 + tid; ch < c1; ch += T) {
-                const int32_t top = P.chain_top[cb + ch];
-                const int32_t bottom = top + P.chain_len[cb + ch] - 1;
-                const int32_t p = P.parent[nb + top];
-                double x = p >= 0 ? sr[p] : 0.0;
-                for (int32_t i = top; i <= bottom; ++i) {
-                    double value = sr[i];
-                    if (P.parent[nb + i] >= 0) value = value + sa[i] * x;
-                    x = value / sd[i];
+            for (int32_t ch = lvc[lv] + tid; ch < lvc[lv + 1]; ch += T) {
+                const int32_t top = ctop[ch];
+                const int32_t bottom = top + clen[ch] - 1;
+                const int32_t par = cpar[ch];
+                double rn = sr[top], an = sa[top], dn = sd[top];
+                double x;
+                {
+                    const double ri = rn, ai = an, di = dn;
+                    const double xp = par >= 0 ? sr[par] : 0.0;
+                    if (top < bottom) {
+                        rn = sr[top + 1];
+                        an = sa[top + 1];
+                        dn = sd[top + 1];
+                    }
+                    x = (par >= 0 ? ri + ai * xp : ri) / di;
+                    sr[top] = x;
+                    sv[top] = sv[top] + x;
+                }
+                for (int32_t i = top + 1; i <= bottom; ++i) {
+                    const double ri = rn, ai = an, di = dn;
+                    if (i < bottom) {
+                        rn = sr[i + 1];
+                        an = sa[i + 1];
+                        dn = sd[i + 1];
+                    }
+                    x = (ri + ai * x) / di;
                     sr[i] = x;
+                    sv[i] = sv[i] + x;
                 }
             }
             __syncthreads();
         }
-        // 8. Voltage update.
-        for (int32_t i = tid; i < n; i += T) sv[i] = sv[i] + sr[i];
-        __syncthreads();
 
-        // 9. cnexp state advance on the new voltage (time t + dt).
+        // 8. cnexp state advance on the new voltage (time t + dt).
         for (int32_t g = 0; g < P.ngroups; ++g) {
-            const DevGroup &G = P.groups[g];
-            const int32_t r0 = G.row_off[c], r1 = G.row_off[c + 1];
+            const DevGroup &GG = P.groups[g];
+            const StagedGroup G = sg[g];
             switch (G.kind) {
                 case MIND_MECH_HH:
-                    for (int32_t r = r0 + tid; r < r1; r += T) {
-                        const double vv = sv[G.node[r] - nb];
+                    for (int32_t r = tid; r < G.rows; r += T) {
+                        const double vv = sv[G.node[r]];
                         if (MIXED) {
-                            float m = G.s[HHS_M][r], h = G.s[HHS_H][r], nn = G.s[HHS_N][r];
+                            float m = G.fat(0, r), h = G.fat(1, r), nn = G.fat(2, r);
                             hh_advance_f32((float)vv, q10f, (float)P.dt, m, h, nn);
-                            G.s[HHS_M][r] = m;
-                            G.s[HHS_H][r] = h;
-                            G.s[HHS_N][r] = nn;
+                            G.fat(0, r) = m;
+                            G.fat(1, r) = h;
+                            G.fat(2, r) = nn;
                         } else {
                             HHRates R = hh_rates(vv, P.celsius);
-                            G.f[HH_M][r] = cnexp(G.f[HH_M][r], R.minf, R.mtau, P.dt);
-                            G.f[HH_H][r] = cnexp(G.f[HH_H][r], R.hinf, R.htau, P.dt);
-                            G.f[HH_N][r] = cnexp(G.f[HH_N][r], R.ninf, R.ntau, P.dt);
+                            G.at(HH_M, r) = cnexp(G.at(HH_M, r), R.minf, R.mtau, P.dt);
+                            G.at(HH_H, r) = cnexp(G.at(HH_H, r), R.hinf, R.htau, P.dt);
+                            G.at(HH_N, r) = cnexp(G.at(HH_N, r), R.ninf, R.ntau, P.dt);
                         }
                     }
                     break;
-                case MIND_MECH_EXPSYN:
-                    for (int32_t r = r0 + tid; r < r1; r += T) {
+                case MIND_MECH_EXPSYN: {
+                    const double *pdec = GG.f[ES_DECAY] + G.r0;
+                    const float *pdecf = GG.s[ESS_DECAY] + G.r0;
+                    for (int32_t r = tid; r < G.rows; r += T) {
                         if (MIXED) {
-                            float gs = G.s[ESS_G][r];
-                            G.s[ESS_G][r] = gs + G.s[ESS_DECAY][r] * (0.0f - gs);
+                            const float gs = G.fat(0, r);
+                            G.fat(0, r) = gs + pdecf[r] * (0.0f - gs);
                         } else {
-                            double gs = G.f[ES_G][r];
-                            G.f[ES_G][r] = gs + G.f[ES_DECAY][r] * (0.0 - gs);
+                            const double gs = G.at(0, r);
+                            G.at(0, r) = gs + pdec[r] * (0.0 - gs);
                         }
                     }
-                    break;
-                case MIND_MECH_EXP2SYN:
-                    for (int32_t r = r0 + tid; r < r1; r += T) {
+                } break;
+                case MIND_MECH_EXP2SYN: {
+                    const double *pd1 = GG.f[E2_DECAY1] + G.r0, *pd2 = GG.f[E2_DECAY2] + G.r0;
+                    const float *pd1f = GG.s[E2S_DECAY1] + G.r0, *pd2f = GG.s[E2S_DECAY2] + G.r0;
+                    for (int32_t r = tid; r < G.rows; r += T) {
                         if (MIXED) {
-                            float A = G.s[E2S_A][r], B = G.s[E2S_B][r];
-                            G.s[E2S_A][r] = A + G.s[E2S_DECAY1][r] * (0.0f - A);
-                            G.s[E2S_B][r] = B + G.s[E2S_DECAY2][r] * (0.0f - B);
+                            const float A = G.fat(0, r), B = G.fat(1, r);
+                            G.fat(0, r) = A + pd1f[r] * (0.0f - A);
+                            G.fat(1, r) = B + pd2f[r] * (0.0f - B);
                         } else {
-                            double A = G.f[E2_A][r], B = G.f[E2_B][r];
-                            G.f[E2_A][r] = A + G.f[E2_DECAY1][r] * (0.0 - A);
-                            G.f[E2_B][r] = B + G.f[E2_DECAY2][r] * (0.0 - B);
+                            const double A = G.at(0, r), B = G.at(1, r);
+                            G.at(0, r) = A + pd1[r] * (0.0 - A);
+                            G.at(1, r) = B + pd2[r] * (0.0 - B);
                         }
                     }
-                    break;
+                } break;
                 default:
                     break;
             }
         }
-        // 10. Record the completed boundary.
+        // 9. Record the completed boundary.
         if (P.nrec) {
             const int64_t sample = step + 1 - P.run_start;
             for (int32_t k = P.rec_off[c] + tid; k < P.rec_off[c + 1]; k += T)
@@ -656,7 +867,47 @@ __global__ void __launch_bounds__(kThreads) window_kernel(const Params P, int64_
         }
         __syncthreads();
     }
+    if (singular) raise_error(P.error, MIND_ESINGULAR);
+
+    // ---- write back ----
+    if (my_det >= 0) P.above[my_src] = my_above ? 1 : 0;
     for (int32_t i = tid; i < n; i += T) P.v[nb + i] = sv[i];
+    for (int32_t g = 0; g < P.ngroups; ++g) {
+        const DevGroup &G = P.groups[g];
+        const StagedGroup &S = sg[g];
+        if (!kind_staged(S.kind)) continue;
+        for (int32_t r = tid; r < S.rows; r += T) {
+            const int32_t row = S.r0 + r;
+            switch (S.kind) {
+                case MIND_MECH_HH:
+                    if (MIXED) {
+                        G.s[HHS_M][row] = S.fat(0, r);
+                        G.s[HHS_H][row] = S.fat(1, r);
+                        G.s[HHS_N][row] = S.fat(2, r);
+                    } else {
+                        G.f[HH_M][row] = S.at(HH_M, r);
+                        G.f[HH_H][row] = S.at(HH_H, r);
+                        G.f[HH_N][row] = S.at(HH_N, r);
+                    }
+                    break;
+                case MIND_MECH_EXPSYN:
+                    if (MIXED)
+                        G.s[ESS_G][row] = S.fat(0, r);
+                    else
+                        G.f[ES_G][row] = S.at(0, r);
+                    break;
+                case MIND_MECH_EXP2SYN:
+                    if (MIXED) {
+                        G.s[E2S_A][row] = S.fat(0, r);
+                        G.s[E2S_B][row] = S.fat(1, r);
+                    } else {
+                        G.f[E2_A][row] = S.at(0, r);
+                        G.f[E2_B][row] = S.at(1, r);
+                    }
+                    break;
+            }
+        }
+    }
 }
 
 __global__ void record_initial_kernel(const Params P, const int64_t *rec_global, int32_t nrec) {

@@ -18,6 +18,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -90,6 +91,15 @@ struct MindHandle {
     double *trace_dev = nullptr;
     size_t trace_capacity = 0;
     size_t rec_capacity = 0;
+    struct Bin {
+        int32_t first, count;
+        size_t smem_bytes;
+    };
+    std::vector<Bin> bins;           // cells grouped by shared-memory need
+    bool profiling = false;
+    std::vector<cudaEvent_t> prof_events;
+    MindRunStats stats{};
+    int32_t *bin_cells = nullptr;    // cell ids, bins contiguous
 
     template <class T>
     T *alloc(size_t count) {
@@ -227,11 +237,9 @@ int create(const MindLayout *L, MindHandle *h) {
     std::vector<int32_t> layout_of_packed;
     layout_of_packed.reserve(n);
     std::vector<int32_t> cell_of(n, -1);
-    std::vector<int32_t> chain_off{0}, chain_top, chain_len, chain_kid_off{0}, chain_kids;
+    std::vector<int32_t> chain_off{0}, chain_top, chain_len, chain_par, chain_kid_off{0}, chain_kids;
     std::vector<int32_t> level_off{0}, level_chain;
-    std::vector<int32_t> parent_local, kid_off{0}, kids;
     h->packed_of_layout.assign(n, -1);
-    int64_t max_nodes = 0, max_chains = 0;
     for (int64_t root = 0; root < n; ++root) {
         if (parent[root] >= 0) continue;
         const int32_t cell = (int32_t)(node_off.size() - 1);
@@ -293,19 +301,12 @@ int create(const MindLayout *L, MindHandle *h) {
         }
         const int64_t cell_nodes = (int64_t)layout_of_packed.size() - base;
         node_off.push_back((int64_t)layout_of_packed.size());
-        max_nodes = std::max(max_nodes, cell_nodes);
-        max_chains = std::max(max_chains, (int64_t)tops.size());
-        for (int64_t j = base; j < base + cell_nodes; ++j) {
-            int32_t i = layout_of_packed[j];
-            parent_local.push_back(parent[i] >= 0 ? (int32_t)(h->packed_of_layout[parent[i]] - base) : -1);
-            for (int64_t c = child_off[i]; c < child_off[i + 1]; ++c)
-                kids.push_back((int32_t)(h->packed_of_layout[child[c]] - base));
-            kid_off.push_back((int32_t)kids.size());
-        }
         for (size_t k = 0; k < order.size(); ++k) {
             const auto &ch = chains[order[k]];
             chain_top.push_back(local_chain_top[k]);
             chain_len.push_back((int32_t)ch.size());
+            int32_t top_parent = parent[ch.front()];
+            chain_par.push_back(top_parent >= 0 ? (int32_t)(h->packed_of_layout[top_parent] - base) : -1);
             int32_t bottom = ch.back();
             for (int64_t c = child_off[bottom]; c < child_off[bottom + 1]; ++c)
                 chain_kids.push_back(rank[chain_id_of(child[c])]);
@@ -466,6 +467,8 @@ int create(const MindLayout *L, MindHandle *h) {
     std::vector<int32_t> det_off{0}, det_node, det_source;
     std::vector<double> det_thr;
     for (int32_t c = 0; c < ncells; ++c) {
+        if ((int32_t)det_by_cell[c].size() > kCellThreads)
+            return fail(h, MIND_ELAYOUT, "more than 64 threshold detectors on one cell");
         for (auto &d : det_by_cell[c]) {
             det_node.push_back(d.first);
             det_source.push_back(d.second);
@@ -512,12 +515,10 @@ int create(const MindLayout *L, MindHandle *h) {
     P.a = h->upload(a);
     P.cdt = h->upload(cdt);
     P.ad = h->upload(ad);
-    P.parent = h->upload(parent_local);
-    P.kid_off = h->upload(kid_off);
-    P.kids = h->upload(kids);
     P.chain_off = h->upload(chain_off);
     P.chain_top = h->upload(chain_top);
     P.chain_len = h->upload(chain_len);
+    P.chain_par = h->upload(chain_par);
     P.chain_kid_off = h->upload(chain_kid_off);
     P.chain_kids = h->upload(chain_kids);
     P.level_off = h->upload(level_off);
@@ -542,7 +543,7 @@ int create(const MindLayout *L, MindHandle *h) {
     P.ring_cap = (int32_t)ring_cap;
     P.ring = h->alloc<RingEvent>((size_t)P.ring_slots * P.ring_cap);
     P.ring_count = h->alloc<int32_t>(P.ring_slots);
-    P.inbox_cap = 512;
+    P.inbox_cap = 64;
     P.inbox = h->alloc<InboxEvent>((size_t)ncells * P.inbox_cap);
     P.inbox_count = h->alloc<int32_t>(ncells);
     P.edge_weight = h->upload(edge_weight);
@@ -562,14 +563,55 @@ int create(const MindLayout *L, MindHandle *h) {
     std::vector<int32_t> zero_off(ncells + 1, 0);
     P.rec_off = h->upload(zero_off);
 
-    h->smem_bytes = (size_t)(4 * max_nodes + 2 * max_chains) * sizeof(double) +
-                    (size_t)P.inbox_cap * (sizeof(InboxEvent) + sizeof(int32_t));
-    if (h->smem_bytes > 227 * 1024)
-        return fail(h, MIND_ELAYOUT, "a cell needs more shared memory than one CTA has");
+    // Shared-memory image per cell; cells are launched in bins of similar size so a
+    // launch's dynamic shared memory matches its cells.
+    std::vector<int32_t> kinds(L->n_mechanisms);
+    for (int32_t g = 0; g < L->n_mechanisms; ++g) kinds[g] = L->mechanisms[g].kind;
+    std::vector<std::vector<int32_t>> group_row_off(L->n_mechanisms);
+    for (int32_t g = 0; g < L->n_mechanisms; ++g) {
+        group_row_off[g].assign(ncells + 1, 0);
+        if (kinds[g] == MIND_MECH_NETSTIM) continue;
+        for (int32_t r = 0; r < (int32_t)row_cell[g].size(); ++r) group_row_off[g][row_cell[g][r] + 1]++;
+        for (int32_t c = 0; c < ncells; ++c) group_row_off[g][c + 1] += group_row_off[g][c];
+    }
+    std::vector<std::pair<size_t, int32_t>> need(ncells);
+    size_t worst[2] = {0, 0};
+    for (int32_t c = 0; c < ncells; ++c) {
+        CellShape shape{};
+        shape.n = (int32_t)(node_off[c + 1] - node_off[c]);
+        shape.nch = chain_off[c + 1] - chain_off[c];
+        shape.nkids = chain_kid_off[chain_off[c + 1]] - chain_kid_off[chain_off[c]];
+        shape.nlev = level_off[c + 1] - level_off[c] - 1;
+        for (int32_t g = 0; g < L->n_mechanisms; ++g) shape.rows[g] = group_row_off[g][c + 1] - group_row_off[g][c];
+        size_t b64 = cell_smem_bytes(shape, kinds.data(), L->n_mechanisms, false, P.inbox_cap);
+        size_t b32 = cell_smem_bytes(shape, kinds.data(), L->n_mechanisms, true, P.inbox_cap);
+        need[c] = {std::max(b64, b32), c};
+        worst[0] = std::max(worst[0], b64);
+        worst[1] = std::max(worst[1], b32);
+    }
+    const size_t worst_any = std::max(worst[0], worst[1]);
+    if (worst_any > 227 * 1024)
+        return fail(h, MIND_ELAYOUT, "a cell needs more shared memory than one CTA has (" +
+                                         std::to_string(worst_any) + " bytes)");
+    std::stable_sort(need.begin(), need.end(), [](const auto &x, const auto &y) { return x.first > y.first; });
+    std::vector<int32_t> bin_cells;
+    for (size_t k = 0; k < need.size();) {
+        size_t top = need[k].first;
+        size_t first = k;
+        while (k < need.size() && need[k].first * 4 >= top * 3) ++k;
+        MindHandle::Bin bin;
+        bin.first = (int32_t)first;
+        bin.count = (int32_t)(k - first);
+        bin.smem_bytes = top;
+        h->bins.push_back(bin);
+    }
+    for (auto &x : need) bin_cells.push_back(x.second);
+    h->bin_cells = h->upload(bin_cells);
+    h->smem_bytes = worst_any;
     CUDA_TRY(h, cudaFuncSetAttribute(window_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)h->smem_bytes));
+                                     (int)std::max<size_t>(worst_any, 1)));
     CUDA_TRY(h, cudaFuncSetAttribute(window_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)h->smem_bytes));
+                                     (int)std::max<size_t>(worst_any, 1)));
     CUDA_TRY(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     CUDA_TRY(h, cudaEventCreate(&h->ev_start));
     CUDA_TRY(h, cudaEventCreate(&h->ev_stop));
@@ -659,18 +701,41 @@ int advance(MindHandle *h, int64_t steps, bool record_spikes) {
     int64_t n0 = h->step;
     const int64_t end = h->step + steps;
     const int ns_blocks = P.ns_group >= 0 ? launch_grid(P.groups[P.ns_group].rows) : 0;
+    MindRunStats st{};
+    st.window_steps = h->window;
+    st.bins = (int32_t)h->bins.size();
+    st.steps = steps;
+    size_t prof_used = 0;
+    auto prof_event = [&]() -> cudaEvent_t {
+        if (prof_used == h->prof_events.size()) {
+            cudaEvent_t e;
+            cudaEventCreate(&e);
+            h->prof_events.push_back(e);
+        }
+        return h->prof_events[prof_used++];
+    };
     while (n0 < end) {
         const int32_t W = (int32_t)std::min<int64_t>(h->window, end - n0);
         const double horizon = (double)(n0 + W - 1) * P.dt + 0.5 * P.dt;
-        if (P.ns_group >= 0) netstim_kernel<<<ns_blocks, kThreads, 0, h->stream>>>(P, horizon, n0);
+        if (P.ns_group >= 0) {
+            netstim_kernel<<<ns_blocks, kThreads, 0, h->stream>>>(P, horizon, n0);
+            ++st.launches;
+        }
         bucket_kernel<<<dim3(64, W), kThreads, 0, h->stream>>>(P, n0);
-        if (h->ncells > 0) {
+        ++st.launches;
+        for (const auto &bin : h->bins) {
+            const int32_t *cells = h->bin_cells + bin.first;
+            if (h->profiling) cudaEventRecord(prof_event(), h->stream);
             if (h->precision == MIND_MIXED)
-                window_kernel<true><<<h->ncells, kThreads, h->smem_bytes, h->stream>>>(P, n0, W);
+                window_kernel<true><<<bin.count, kCellThreads, bin.smem_bytes, h->stream>>>(P, cells, n0, W);
             else
-                window_kernel<false><<<h->ncells, kThreads, h->smem_bytes, h->stream>>>(P, n0, W);
+                window_kernel<false><<<bin.count, kCellThreads, bin.smem_bytes, h->stream>>>(P, cells, n0, W);
+            if (h->profiling) cudaEventRecord(prof_event(), h->stream);
+            ++st.launches;
+            ++st.window_launches;
         }
         route_kernel<<<64, kThreads, 0, h->stream>>>(P, n0 + W);
+        ++st.launches;
         n0 += W;
     }
     CUDA_TRY(h, cudaGetLastError());
@@ -680,6 +745,13 @@ int advance(MindHandle *h, int64_t steps, bool record_spikes) {
     float ms = 0.0f;
     CUDA_TRY(h, cudaEventElapsedTime(&ms, h->ev_start, h->ev_stop));
     h->last_ms = ms;
+    st.run_ms = ms;
+    for (size_t k = 0; k + 1 < prof_used; k += 2) {
+        float part = 0.0f;
+        CUDA_TRY(h, cudaEventElapsedTime(&part, h->prof_events[k], h->prof_events[k + 1]));
+        st.window_ms += part;
+    }
+    h->stats = st;
     h->step = end;
     return check_device_error(h);
 }
@@ -859,9 +931,22 @@ int mind_last_run_ms(const MindHandle *h, double *ms) {
     return MIND_OK;
 }
 
+int mind_run_stats(const MindHandle *h, MindRunStats *stats) {
+    if (!h || !stats) return MIND_EARG;
+    *stats = h->stats;
+    return MIND_OK;
+}
+
+int mind_set_profiling(MindHandle *h, int32_t enable) {
+    if (!h) return MIND_EARG;
+    h->profiling = enable != 0;
+    return MIND_OK;
+}
+
 int mind_destroy(MindHandle *h) {
     if (!h) return MIND_OK;
     if (h->stream) cudaStreamSynchronize(h->stream);
+    for (cudaEvent_t e : h->prof_events) cudaEventDestroy(e);
     if (h->ev_start) cudaEventDestroy(h->ev_start);
     if (h->ev_stop) cudaEventDestroy(h->ev_stop);
     if (h->stream) cudaStreamDestroy(h->stream);

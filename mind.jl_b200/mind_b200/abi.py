@@ -91,6 +91,18 @@ class MindRecord(Structure):
     _fields_ = [("kind", c_int32), ("node", c_int32)]
 
 
+class MindRunStats(Structure):
+    _fields_ = [
+        ("run_ms", c_double),
+        ("window_ms", c_double),
+        ("launches", c_int64),
+        ("window_launches", c_int64),
+        ("steps", c_int64),
+        ("window_steps", c_int32),
+        ("bins", c_int32),
+    ]
+
+
 class MindError(RuntimeError):
     """A non-zero status from libmindgpu, with the library's message."""
 
@@ -133,9 +145,12 @@ def load_library():
     lib.mind_last_error.restype = c_char_p
     lib.mind_last_run_ms.argtypes = [handle, POINTER(c_double)]
     lib.mind_destroy.argtypes = [handle]
+    lib.mind_run_stats.argtypes = [handle, POINTER(MindRunStats)]
+    lib.mind_set_profiling.argtypes = [handle, c_int32]
     for name in ("mind_create", "mind_initialize", "mind_set_precision", "mind_run", "mind_step",
                  "mind_time", "mind_get_trace", "mind_get_spikes", "mind_read_voltage",
-                 "mind_inject_event", "mind_last_run_ms", "mind_destroy"):
+                 "mind_inject_event", "mind_last_run_ms", "mind_destroy", "mind_run_stats",
+                 "mind_set_profiling"):
         getattr(lib, name).restype = c_int32
     _LIB = lib
     return lib
@@ -144,7 +159,7 @@ def load_library():
 EXPORTED_SYMBOLS = (
     "mind_create", "mind_initialize", "mind_set_precision", "mind_run", "mind_step", "mind_time",
     "mind_get_trace", "mind_get_spikes", "mind_read_voltage", "mind_inject_event",
-    "mind_last_error", "mind_last_run_ms", "mind_destroy",
+    "mind_last_error", "mind_last_run_ms", "mind_destroy", "mind_run_stats", "mind_set_profiling",
 )
 
 

@@ -93,6 +93,14 @@ class DeviceState:
             result.traces[r.name] = trace[:, i].copy()
         return result
 
+    def run_stats(self) -> abi.MindRunStats:
+        stats = abi.MindRunStats()
+        abi.check(self.lib, self.handle, self.lib.mind_run_stats(self.handle, ctypes.byref(stats)))
+        return stats
+
+    def set_profiling(self, enable: bool) -> None:
+        abi.check(self.lib, self.handle, self.lib.mind_set_profiling(self.handle, 1 if enable else 0))
+
     def step(self) -> None:
         abi.check(self.lib, self.handle, self.lib.mind_step(self.handle))
 
