@@ -211,8 +211,9 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
 
     import mind_b200 as mb
+    from mind_b200 import replicas
 
-    model, layout = build_network(args.cells, seed=1 + rank)
+    model, layout = build_network(args.cells, seed=replicas.replica_seed(1, rank))
     soma = [mb.RecordSpec(layout.voltage_node(c), f"v{c}") for c in range(1, layout.n_cells + 1)]
     precisions = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
     results = {}
@@ -233,12 +234,7 @@ def main():
             dist.barrier()
         stats = model.state.run_stats()
         clocks = sampler.summary()
-        run_ms = stats.run_ms
-        if dist is not None:
-            t = torch.tensor([run_ms], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            run_ms = float(t.item())
-        units = layout.segment_count * args.steps * world
+        run_ms, units = replicas.reduce_timing(stats.run_ms, layout.segment_count * args.steps, device="cuda")
         value = units / (run_ms / 1000.0)
         events = delivered_events(layout, result.spike_sources)
         algo = algorithmic_bytes_per_step(layout, events / args.steps)
@@ -250,11 +246,7 @@ def main():
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         e2e_result = mb.run(model, (args.warmup + args.steps) * dt, records=soma, record_spikes=True)
-        e2e_s = time.perf_counter() - t0
-        if dist is not None:
-            t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = float(t.item())
+        e2e_s, _ = replicas.reduce_timing(time.perf_counter() - t0, 0.0, device="cuda")
         d2h = (len(soma) * 8 * (args.steps + 1) + 16 * len(e2e_result.spike_times)) / args.steps
         h2d = 8 * len(soma) / args.steps
         results[precision] = {

@@ -611,3 +611,22 @@ int oracle_run(const MindLayout *layout, int64_t steps, const MindRecord *record
 }
 
 }  // extern "C"
+
+extern "C" {
+
+/* The project-owned elementary functions and Philox, exposed for the tests that
+ * pin them against glibc and the published Random123 known-answer vectors. */
+double oracle_exp(double x) { return mind_exp(x); }
+double oracle_log(double x) { return mind_log(x); }
+double oracle_pow(double x, double y) { return mind_pow(x, y); }
+void oracle_philox(uint32_t *ctr, uint32_t key0, uint32_t key1) { mind_philox4x32_10(ctr, key0, key1); }
+
+/* One random stream in the nrnran123 layout: `n` negexp draws from a fresh
+ * stream keyed by (logical id, digest, stream 0, seed). */
+void oracle_negexp_stream(uint64_t logical_id, uint64_t digest, uint64_t seed, int64_t n, double *out) {
+    MindRan ran;
+    mind_ran_init(&ran, logical_id, digest, 0u, seed);
+    for (int64_t i = 0; i < n; ++i) out[i] = mind_ran_negexp(&ran, seed);
+}
+
+}  // extern "C"

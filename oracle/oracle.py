@@ -36,8 +36,43 @@ def _load():
             ctypes.POINTER(ctypes.c_int64), ctypes.c_int64, ctypes.POINTER(ctypes.c_int64),
             ctypes.POINTER(ctypes.c_double), ctypes.c_char_p, ctypes.c_int32,
         ]
+        lib.oracle_exp.restype = ctypes.c_double
+        lib.oracle_exp.argtypes = [ctypes.c_double]
+        lib.oracle_log.restype = ctypes.c_double
+        lib.oracle_log.argtypes = [ctypes.c_double]
+        lib.oracle_pow.restype = ctypes.c_double
+        lib.oracle_pow.argtypes = [ctypes.c_double, ctypes.c_double]
+        lib.oracle_philox.restype = None
+        lib.oracle_philox.argtypes = [ctypes.POINTER(ctypes.c_uint32), ctypes.c_uint32, ctypes.c_uint32]
+        lib.oracle_negexp_stream.restype = None
+        lib.oracle_negexp_stream.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int64,
+                                             ctypes.POINTER(ctypes.c_double)]
         _LIB = lib
     return _LIB
+
+
+def exp(x: float) -> float:
+    return _load().oracle_exp(x)
+
+
+def log(x: float) -> float:
+    return _load().oracle_log(x)
+
+
+def pow(x: float, y: float) -> float:
+    return _load().oracle_pow(x, y)
+
+
+def philox4x32_10(ctr, key0: int, key1: int):
+    words = (ctypes.c_uint32 * 4)(*ctr)
+    _load().oracle_philox(words, key0, key1)
+    return list(words)
+
+
+def negexp_stream(logical_id: int, digest: int, seed: int, n: int) -> np.ndarray:
+    out = np.zeros(n)
+    _load().oracle_negexp_stream(logical_id, digest, seed, n, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+    return out
 
 
 @dataclass
