@@ -96,6 +96,9 @@ struct MindHandle {
         size_t smem_bytes;
     };
     std::vector<Bin> bins;           // cells grouped by shared-memory need
+    std::vector<cudaStream_t> bin_streams;   // size bins run concurrently
+    std::vector<cudaEvent_t> bin_done;
+    cudaEvent_t fork = nullptr;
     bool profiling = false;
     std::vector<cudaEvent_t> prof_events;
     MindRunStats stats{};
@@ -613,6 +616,15 @@ int create(const MindLayout *L, MindHandle *h) {
     CUDA_TRY(h, cudaFuncSetAttribute(window_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)std::max<size_t>(worst_any, 1)));
     CUDA_TRY(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    CUDA_TRY(h, cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming));
+    for (size_t b = 0; b < h->bins.size(); ++b) {
+        cudaStream_t s;
+        cudaEvent_t e;
+        CUDA_TRY(h, cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        CUDA_TRY(h, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        h->bin_streams.push_back(s);
+        h->bin_done.push_back(e);
+    }
     CUDA_TRY(h, cudaEventCreate(&h->ev_start));
     CUDA_TRY(h, cudaEventCreate(&h->ev_stop));
     return MIND_OK;
@@ -723,17 +735,25 @@ int advance(MindHandle *h, int64_t steps, bool record_spikes) {
         }
         bucket_kernel<<<dim3(64, W), kThreads, 0, h->stream>>>(P, n0);
         ++st.launches;
-        for (const auto &bin : h->bins) {
+        // Size bins run side by side on their own streams so SMs mix CTAs of
+        // different shared-memory images; the main stream joins them.
+        if (h->profiling) cudaEventRecord(prof_event(), h->stream);
+        cudaEventRecord(h->fork, h->stream);
+        for (size_t b = 0; b < h->bins.size(); ++b) {
+            const auto &bin = h->bins[b];
+            cudaStream_t s = h->bin_streams[b];
+            cudaStreamWaitEvent(s, h->fork, 0);
             const int32_t *cells = h->bin_cells + bin.first;
-            if (h->profiling) cudaEventRecord(prof_event(), h->stream);
             if (h->precision == MIND_MIXED)
-                window_kernel<true><<<bin.count, kCellThreads, bin.smem_bytes, h->stream>>>(P, cells, n0, W);
+                window_kernel<true><<<bin.count, kCellThreads, bin.smem_bytes, s>>>(P, cells, n0, W);
             else
-                window_kernel<false><<<bin.count, kCellThreads, bin.smem_bytes, h->stream>>>(P, cells, n0, W);
-            if (h->profiling) cudaEventRecord(prof_event(), h->stream);
+                window_kernel<false><<<bin.count, kCellThreads, bin.smem_bytes, s>>>(P, cells, n0, W);
+            cudaEventRecord(h->bin_done[b], s);
+            cudaStreamWaitEvent(h->stream, h->bin_done[b], 0);
             ++st.launches;
             ++st.window_launches;
         }
+        if (h->profiling) cudaEventRecord(prof_event(), h->stream);
         route_kernel<<<64, kThreads, 0, h->stream>>>(P, n0 + W);
         ++st.launches;
         n0 += W;
@@ -947,6 +967,9 @@ int mind_destroy(MindHandle *h) {
     if (!h) return MIND_OK;
     if (h->stream) cudaStreamSynchronize(h->stream);
     for (cudaEvent_t e : h->prof_events) cudaEventDestroy(e);
+    for (cudaEvent_t e : h->bin_done) cudaEventDestroy(e);
+    for (cudaStream_t s : h->bin_streams) cudaStreamDestroy(s);
+    if (h->fork) cudaEventDestroy(h->fork);
     if (h->ev_start) cudaEventDestroy(h->ev_start);
     if (h->ev_stop) cudaEventDestroy(h->ev_stop);
     if (h->stream) cudaStreamDestroy(h->stream);
