@@ -203,6 +203,30 @@ typedef struct MindRunStats {
 int mind_run_stats(const MindHandle *h, MindRunStats *stats);
 int mind_set_profiling(MindHandle *h, int32_t enable);
 
+/*
+ * run! without device allocation.  No counterpart in the reference.
+ *
+ * For callers that may not allocate device memory while they step a model —
+ * for example a host whose device memory is owned by another allocator and is
+ * sized up front, or a control loop that must not enter the CUDA allocator
+ * once it is running.  mind_create still allocates the model's state once; this
+ * call then advances `steps` micro steps exactly as mind_run does with voltage
+ * records and no spike recording, and writes the (steps+1) x n_records trace,
+ * sample-major, into the caller's host buffer `trace`.
+ *
+ * Its per-run scratch (record maps and the trace staging area) lives in one
+ * static device array of MIND_NOALLOC_SCRATCH_BYTES (16 MiB) that every GPU
+ * loading the library holds until the process exits.  Runs that need more
+ * return MIND_ECAPACITY with a message giving the size.  The first call on a
+ * device looks up that array's device address (cudaGetSymbolAddress) with the
+ * device current, so make the first call before any stream capture.  All
+ * handles on a device share the array and it keeps the previous call's
+ * contents: calls that overlap on the GPU (two threads, two handles) race and
+ * must be serialized by the caller.
+ */
+#define MIND_NOALLOC_SCRATCH_BYTES (16u << 20)
+int mind_run_noalloc(MindHandle *h, int64_t steps, const MindRecord *records, int32_t n_records, double *trace);
+
 int mind_destroy(MindHandle *h);
 
 #ifdef __cplusplus

@@ -19,6 +19,7 @@
 
 #include <algorithm>
 #include <array>
+#include <mutex>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -960,6 +961,113 @@ int mind_run_stats(const MindHandle *h, MindRunStats *stats) {
 int mind_set_profiling(MindHandle *h, int32_t enable) {
     if (!h) return MIND_EARG;
     h->profiling = enable != 0;
+    return MIND_OK;
+}
+
+/* ---- run! without device allocation (see include/mindgpu.h) ---- */
+
+namespace {
+
+// The per-run scratch of mind_run_noalloc: record maps and trace staging.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[MIND_NOALLOC_SCRATCH_BYTES];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+void *g_noalloc_address[kMaxDevices] = {nullptr};
+
+// Device address of g_noalloc_scratch on the current device, looked up once per device.
+int noalloc_scratch(MindHandle *h, unsigned char **out) {
+    int device = 0;
+    CUDA_TRY(h, cudaGetDevice(&device));
+    if (device < 0 || device >= kMaxDevices) return fail(h, MIND_EARG, "device index out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (g_noalloc_address[device] == nullptr) {
+        void *ptr = nullptr;
+        CUDA_TRY(h, cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+        g_noalloc_address[device] = ptr;
+    }
+    *out = static_cast<unsigned char *>(g_noalloc_address[device]);
+    return MIND_OK;
+}
+
+}  // namespace
+
+int mind_run_noalloc(MindHandle *h, int64_t steps, const MindRecord *records, int32_t n_records, double *trace) {
+    if (!h) return MIND_EARG;
+    if (!h->initialized) return fail(h, MIND_EARG, "simulation is not initialized");
+    if (steps < 0 || n_records < 0 || (n_records > 0 && (!records || !trace)))
+        return fail(h, MIND_EARG, "invalid run arguments");
+    // Scratch carve: rec_off [ncells+1] i32 | rec_node [n] i32 | rec_col [n] i32 | rec_global [n] i64 | trace.
+    auto align = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    const size_t off_bytes = align((size_t)(h->ncells + 1) * sizeof(int32_t));
+    const size_t node_bytes = align((size_t)std::max(n_records, 1) * sizeof(int32_t));
+    const size_t global_bytes = align((size_t)std::max(n_records, 1) * sizeof(int64_t));
+    const size_t trace_bytes = (size_t)(steps + 1) * (size_t)n_records * sizeof(double);
+    const size_t need = off_bytes + 2 * node_bytes + global_bytes + trace_bytes;
+    if (need > MIND_NOALLOC_SCRATCH_BYTES) {
+        // Refused before any work: the simulation state is unchanged and stays usable.
+        h->error = "mind_run_noalloc needs " + std::to_string(need) + " bytes of scratch; its static array holds " +
+                   std::to_string((size_t)MIND_NOALLOC_SCRATCH_BYTES) + " bytes (fewer steps or records per call)";
+        return MIND_ECAPACITY;
+    }
+    unsigned char *scratch = nullptr;
+    int status = noalloc_scratch(h, &scratch);
+    if (status) return status;
+    int32_t *d_off = reinterpret_cast<int32_t *>(scratch);
+    int32_t *d_node = reinterpret_cast<int32_t *>(scratch + off_bytes);
+    int32_t *d_col = reinterpret_cast<int32_t *>(scratch + off_bytes + node_bytes);
+    int64_t *d_global = reinterpret_cast<int64_t *>(scratch + off_bytes + 2 * node_bytes);
+    double *d_trace = reinterpret_cast<double *>(scratch + off_bytes + 2 * node_bytes + global_bytes);
+
+    // Record maps (host side), then into the scratch: every entry is written, nothing needs clearing.
+    std::vector<std::vector<std::pair<int32_t, int32_t>>> by_cell(h->ncells);
+    std::vector<int64_t> global(n_records);
+    for (int32_t k = 0; k < n_records; ++k) {
+        if (records[k].kind != MIND_RECORD_VOLTAGE) return fail(h, MIND_EARG, "unsupported record kind");
+        const int32_t node = records[k].node;
+        if (node < 1 || node > h->n_nodes) return fail(h, MIND_EARG, "record node out of range");
+        const int64_t packed = h->packed_of_layout[node - 1];
+        global[k] = packed;
+        const int32_t cell =
+            (int32_t)(std::upper_bound(h->node_off.begin(), h->node_off.end(), packed) - h->node_off.begin() - 1);
+        by_cell[cell].push_back({(int32_t)(packed - h->node_off[cell]), k});
+    }
+    std::vector<int32_t> off{0}, local, col;
+    for (int32_t c = 0; c < h->ncells; ++c) {
+        for (auto &x : by_cell[c]) {
+            local.push_back(x.first);
+            col.push_back(x.second);
+        }
+        off.push_back((int32_t)local.size());
+    }
+    CUDA_TRY(h, cudaMemcpyAsync(d_off, off.data(), off.size() * sizeof(int32_t), cudaMemcpyHostToDevice, h->stream));
+    if (n_records) {
+        CUDA_TRY(h, cudaMemcpyAsync(d_node, local.data(), local.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                                    h->stream));
+        CUDA_TRY(h, cudaMemcpyAsync(d_col, col.data(), col.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                                    h->stream));
+        CUDA_TRY(h, cudaMemcpyAsync(d_global, global.data(), global.size() * sizeof(int64_t),
+                                    cudaMemcpyHostToDevice, h->stream));
+    }
+    // Point the run at the scratch for this call; the handle's own record buffers stay untouched.
+    Params &P = h->P;
+    P.rec_off = d_off;
+    P.rec_node = d_node;
+    P.rec_col = d_col;
+    P.nrec = n_records;
+    P.trace = d_trace;
+    P.trace_samples = steps + 1;
+    int64_t *own_global = h->rec_global_dev;
+    h->rec_global_dev = d_global;
+    status = advance(h, steps, false);
+    h->rec_global_dev = own_global;
+    if (status) {
+        h->initialized = false;
+        return status;
+    }
+    if (trace_bytes)
+        CUDA_TRY(h, cudaMemcpyAsync(trace, d_trace, trace_bytes, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     return MIND_OK;
 }
 

@@ -147,10 +147,11 @@ def load_library():
     lib.mind_destroy.argtypes = [handle]
     lib.mind_run_stats.argtypes = [handle, POINTER(MindRunStats)]
     lib.mind_set_profiling.argtypes = [handle, c_int32]
+    lib.mind_run_noalloc.argtypes = [handle, c_int64, POINTER(MindRecord), c_int32, POINTER(c_double)]
     for name in ("mind_create", "mind_initialize", "mind_set_precision", "mind_run", "mind_step",
                  "mind_time", "mind_get_trace", "mind_get_spikes", "mind_read_voltage",
                  "mind_inject_event", "mind_last_run_ms", "mind_destroy", "mind_run_stats",
-                 "mind_set_profiling"):
+                 "mind_set_profiling", "mind_run_noalloc"):
         getattr(lib, name).restype = c_int32
     _LIB = lib
     return lib
@@ -160,7 +161,10 @@ EXPORTED_SYMBOLS = (
     "mind_create", "mind_initialize", "mind_set_precision", "mind_run", "mind_step", "mind_time",
     "mind_get_trace", "mind_get_spikes", "mind_read_voltage", "mind_inject_event",
     "mind_last_error", "mind_last_run_ms", "mind_destroy", "mind_run_stats", "mind_set_profiling",
+    "mind_run_noalloc",
 )
+
+MIND_NOALLOC_SCRATCH_BYTES = 16 << 20
 
 
 def check(lib, handle, status: int) -> None:
