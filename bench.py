@@ -43,18 +43,23 @@ def parse():
     p.add_argument("--steps", type=int, default=800)
     p.add_argument("--warmup", type=int, default=40)
     p.add_argument("--impl", default="mine", choices=["mine", "reference"])
-    p.add_argument("--cells", type=int, default=10000)
+    p.add_argument("--cells", type=int, default=None, help="cells (default: the configuration's count)")
+    p.add_argument("--config", type=int, default=2, choices=[2, 3],
+                   help="2: 10,000 uneven binary-tree cells (the headline); 3: 1,000 pyramidal-like cells")
     p.add_argument("--precision", default="fp64", choices=["fp64", "mixed", "both"])
     p.add_argument("--cpu-steps", type=int, default=8)
     p.add_argument("--no-cpu-baseline", action="store_true")
     return p.parse_args()
 
 
-def build_network(cells: int, seed: int):
+def build_network(cells, seed: int, config: int = 2):
     import mind_b200 as mb
     from mind_b200 import networks
 
-    model = networks.config2(n_cells=cells)
+    if config == 3:
+        model = networks.config3(n_cells=cells or 1000)
+    else:
+        model = networks.config2(n_cells=cells or 10000)
     layout = mb.build(model, seed=seed)
     return model, layout
 
@@ -169,7 +174,7 @@ def run_reference(args, rank: int):
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    model, layout = build_network(args.cells, seed=1)
+    model, layout = build_network(args.cells, seed=1, config=args.config)
     steps = max(1, args.cpu_steps)
     values = []
     for _ in range(max(1, args.steps and 1)):
@@ -180,10 +185,10 @@ def run_reference(args, rank: int):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": steps, "warmup": 0, "ms_per_step": ms / steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded config-2 network)",
-        "config": {"workload": "config2", "cells": args.cells, "compartments": layout.segment_count,
+        "config": {"workload": f"config{args.config}", "cells": layout.n_cells, "compartments": layout.segment_count,
                    "dt_ms": layout.dt, "l2": "state larger than L2"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"first {steps} micro steps of the full config-2 network"},
+                         "sample": f"first {steps} micro steps of the full config-{args.config} network"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "MIND.jl is Julia (absent here); the reference arm is the CPU FP64 restatement of its step loop",
     }
@@ -213,7 +218,7 @@ def main():
     import mind_b200 as mb
     from mind_b200 import replicas
 
-    model, layout = build_network(args.cells, seed=replicas.replica_seed(1, rank))
+    model, layout = build_network(args.cells, seed=replicas.replica_seed(1, rank), config=args.config)
     soma = [mb.RecordSpec(layout.voltage_node(c), f"v{c}") for c in range(1, layout.n_cells + 1)]
     precisions = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
     results = {}
@@ -267,8 +272,8 @@ def main():
         "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64" if precisions[0] == "fp64" else "f32-gating/f64-cable",
-        "data": "synthetic (seeded config-2 network, mind_b200.networks.config2)",
-        "config": {"workload": "config2", "cells": args.cells, "compartments": layout.segment_count,
+        "data": f"synthetic (seeded config-{args.config} network, mind_b200.networks.config{args.config})",
+        "config": {"workload": f"config{args.config}", "cells": layout.n_cells, "compartments": layout.segment_count,
                    "nodes": layout.n_nodes, "dt_ms": layout.dt, "precision": precisions[0],
                    "parallelism": f"replica x{world}", "l2": "working set larger than L2 (no flush needed)",
                    "window_steps": head["window_steps"], "size_bins": head["bins"]},
@@ -294,7 +299,7 @@ def main():
         threads = os.cpu_count() or 1
         cpu_value, _ = cpu_baseline(layout, args.cpu_steps, threads)
         line["cpu_baseline"] = {"value": cpu_value, "unit": UNIT, "cores": threads, "kind": "port",
-                                "sample": f"first {args.cpu_steps} micro steps of the full config-2 network"}
+                                "sample": f"first {args.cpu_steps} micro steps of the full config-{args.config} network"}
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()

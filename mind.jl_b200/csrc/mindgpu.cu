@@ -53,6 +53,12 @@ struct MindHandle {
     std::vector<int64_t> packed_of_layout;   // layout node -> packed index
     std::vector<int64_t> node_off;           // [ncells+1] packed node ranges
     std::vector<int32_t> edge_target;        // 0-based point per edge
+    struct Injected {
+        int64_t bin;
+        double time;
+        int32_t edge, point;
+    };
+    std::vector<Injected> injected;          // inject_event! beyond the ring's horizon, by bin
     std::vector<double> v0_packed;
     int64_t n_sources = 0;
     std::vector<int64_t> source_ids;
@@ -734,6 +740,13 @@ int advance(MindHandle *h, int64_t steps, bool record_spikes) {
             netstim_kernel<<<ns_blocks, kThreads, 0, h->stream>>>(P, horizon, n0);
             ++st.launches;
         }
+        // Injected events whose bin falls in this window enter the ring now.
+        while (!h->injected.empty() && h->injected.front().bin < n0 + W) {
+            const auto &e = h->injected.front();
+            inject_kernel<<<1, 1, 0, h->stream>>>(P, e.time, e.edge, e.point, n0);
+            ++st.launches;
+            h->injected.erase(h->injected.begin());
+        }
         bucket_kernel<<<dim3(64, W), kThreads, 0, h->stream>>>(P, n0);
         ++st.launches;
         // Size bins run side by side on their own streams so SMs mix CTAs of
@@ -850,6 +863,7 @@ int mind_initialize(MindHandle *h) {
     Params &P = h->P;
     h->initialized = false;
     h->step = 0;
+    h->injected.clear();
     CUDA_TRY(h, cudaMemcpyAsync(P.v, h->v0_packed.data(), h->n_nodes * sizeof(double), cudaMemcpyHostToDevice,
                                 h->stream));
     CUDA_TRY(h, cudaMemsetAsync(P.error, 0, sizeof(int32_t), h->stream));
@@ -936,9 +950,13 @@ int mind_inject_event(MindHandle *h, int64_t edge, double t) {
     const Params &P = h->P;
     if (edge < 1 || edge > (int64_t)h->edge_target.size()) return fail(h, MIND_EARG, "edge index out of range");
     if (!(t >= (double)h->step * h->dt) || !std::isfinite(t)) return fail(h, MIND_EARG, "event time is in the past");
-    inject_kernel<<<1, 1, 0, h->stream>>>(P, t, (int32_t)(edge - 1), h->edge_target[edge - 1], h->step);
-    CUDA_TRY(h, cudaGetLastError());
-    return check_device_error(h);
+    // The ring holds bins up to one window plus the longest delay ahead; the event
+    // waits on the host until the window that delivers it.
+    MindHandle::Injected e{delivery_bin(t, h->dt), t, (int32_t)(edge - 1), h->edge_target[edge - 1]};
+    auto at = std::upper_bound(h->injected.begin(), h->injected.end(), e,
+                               [](const MindHandle::Injected &x, const MindHandle::Injected &y) { return x.bin < y.bin; });
+    h->injected.insert(at, e);
+    return MIND_OK;
 }
 
 const char *mind_last_error(const MindHandle *h) {

@@ -23,3 +23,18 @@ def test_library_exports_every_declared_symbol():
     lib = ctypes.CDLL(abi.library_path())
     for name in declared_functions():
         assert hasattr(lib, name), name
+
+
+def test_malformed_layout_rejected_before_any_device_work():
+    """A parent index out of range is refused with status 10 (no CUDA call is reached)."""
+    import mind_b200 as mb
+    from mind_b200 import networks
+
+    layout = mb.build(networks.config1(n_cells=1))
+    layout.parent[5] = 10_000
+    lib = abi.load_library()
+    c_layout = layout.to_c()
+    handle = ctypes.c_void_p()
+    status = lib.mind_create(ctypes.byref(c_layout), ctypes.byref(handle))
+    assert status == abi.MIND_ELAYOUT
+    assert b"parent" in lib.mind_last_error(None)
