@@ -22,7 +22,8 @@
  * Arithmetic order in FP64 mode is the oracle's (oracle/mind_oracle.cpp):
  * group order, row order inside a segment, own axial term before children,
  * children in ascending layout index.  The file is compiled with -fmad=false
- * so that no multiply-add is fused behind the source's back.
+ * so that no multiply-add is fused behind the source's back; the fused
+ * multiply-adds it does contain are explicit and exact (mind_div_milli).
  */
 #pragma once
 
@@ -130,8 +131,9 @@ __host__ __device__ inline int kind_floats(int32_t kind) {
  *            slots of the staged rows;
  *   events   the cell's inbox for the window [inbox_cap];
  *   floats   staged FP32 slots (mixed mode);
- *   ints     per staged row: local node and segment length; chain top, length,
- *            parent, child-chain CSR; level starts; inbox order;
+ *   ints     per staged row: local node; chain top, length,
+ *            parent, child-chain CSR; level starts; inbox order; the
+ *            threads' row ranges per group [ngroups][threads + 1];
  *   shorts   chain of every node [n].
  * Host (to size the launch) and device (to carve the buffer) use this one function.
  */
@@ -148,9 +150,10 @@ __host__ __device__ inline size_t cell_smem_bytes(const CellShape &s, const int3
         if (!kind_staged(kinds[g])) continue;
         doubles += (size_t)staged_doubles(kinds[g], mixed) * s.rows[g];
         floats += (size_t)staged_floats(kinds[g], mixed) * s.rows[g];
-        ints += 2 * (size_t)s.rows[g];
+        ints += (size_t)s.rows[g];
     }
     ints += 4 * (size_t)s.nch + 1 + (size_t)s.nkids + (size_t)s.nlev + 1 + (size_t)inbox_cap;
+    ints += (size_t)ngroups * (kCellThreads + 1);
     return doubles * 8 + (size_t)inbox_cap * sizeof(InboxEvent) + floats * 4 + ints * 4 + 2 * (size_t)s.n;
 }
 
@@ -173,6 +176,9 @@ struct Params {
     const int32_t *level_off;    // [ncells+1] into level_chain
     const int32_t *level_chain;  // per cell: nlevels+1 local chain starts (chains sorted by level)
     DevGroup groups[kMaxGroups];
+    // per cell, group and thread: first row (relative to the cell's first row of the group)
+    // whose node lies in the thread's contiguous node range [t*n/T, (t+1)*n/T)
+    const int32_t *part;       // [ncells][ngroups][kCellThreads + 1]
     // detectors
     const int32_t *det_off;    // [ncells+1]
     const int32_t *det_node;   // local node

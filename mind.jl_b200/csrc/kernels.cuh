@@ -100,9 +100,9 @@ __device__ __forceinline__ HHRates hh_rates(double v, double celsius) {
 }
 
 /* One gate of hh_rates (0 = m, 1 = h, 2 = n) with the identical operations, so the
- * three gates of a row can advance on three threads. */
-__device__ __forceinline__ void hh_gate(double v, double celsius, int gate, double &inf, double &tau) {
-    const double q10 = mind_pow(3.0, (celsius - 6.3) / 10.0);
+ * three gates of a row can advance on three threads; q10 = 3^((celsius - 6.3)/10)
+ * is computed once by the caller with the same pow. */
+__device__ __forceinline__ void hh_gate(double v, double q10, int gate, double &inf, double &tau) {
     double alpha, beta;
     if (gate == 0) {
         alpha = 0.1 * vtrap(-(v + 40.0), 10.0);
@@ -121,6 +121,26 @@ __device__ __forceinline__ void hh_gate(double v, double celsius, int gate, doub
 
 __device__ __forceinline__ double cnexp(double s, double inf, double tau, double dt) {
     return s + (1.0 - mind_exp(dt * (-1.0 / tau))) * (inf - s);
+}
+
+/* (x)/0.001 of the current probe: the IEEE quotient in FP64 mode (division-free,
+ * mind_div_milli); in the mixed mode a multiplication by 1000, within one ulp. */
+template <bool MIXED>
+__device__ __forceinline__ double milli_quotient(double x) {
+    return MIXED ? x * 1000.0 : mind_div_milli(x);
+}
+
+/* 1/x for the mixed mode's Hines solve: the hardware reciprocal seed refined by two
+ * Newton-Raphson steps y <- y + y(1 - x y), each roughly doubling the correct bits,
+ * so the result is within a few ulp of 1/x (FP64 arithmetic throughout; only the
+ * FP64 mode needs the correctly rounded quotient of the reference). */
+__device__ __forceinline__ double approx_reciprocal(double x) {
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    double e = fma(-x, y, 1.0);
+    y = fma(y, e, y);
+    e = fma(-x, y, 1.0);
+    return fma(y, e, y);
 }
 
 /* FP32 gating for the mixed mode: same equations, single precision, fast exp. */
@@ -362,7 +382,7 @@ struct StagedGroup {
     int32_t kind, rows, r0;   // r0 = first device row of the cell
     double *f;                // staged FP64 slots [slots][rows]
     float *s;                 // staged FP32 slots [slots][rows] (mixed mode)
-    int32_t *node, *seg;      // local node and segment length per row
+    int32_t *node;            // local node per row
     __device__ __forceinline__ double &at(int slot, int r) const { return f[slot * rows + r]; }
     __device__ __forceinline__ float &fat(int slot, int r) const { return s[slot * rows + r]; }
 };
@@ -452,11 +472,8 @@ __global__ void __launch_bounds__(kCellThreads, 8) window_kernel(const Params P,
     for (int32_t g = 0; g < P.ngroups; ++g) {
         const DevGroup &G = P.groups[g];
         const int32_t rows = kind_staged(G.kind) ? G.row_off[c + 1] - G.row_off[c] : 0;
-        if (tid == 0) {
-            sg[g].node = ip;
-            sg[g].seg = ip + rows;
-        }
-        ip += 2 * rows;
+        if (tid == 0) sg[g].node = ip;
+        ip += rows;
     }
     int32_t *ctop = ip; ip += nch;
     int32_t *clen = ip; ip += nch;
@@ -465,6 +482,7 @@ __global__ void __launch_bounds__(kCellThreads, 8) window_kernel(const Params P,
     int32_t *ckids = ip; ip += nkids;
     int32_t *lvc = ip; ip += nlev + 1;
     int32_t *sorder = ip; ip += P.inbox_cap;
+    int32_t *spart = ip; ip += P.ngroups * (T + 1);
     int16_t *chain_of = reinterpret_cast<int16_t *>(ip);
     {
         // The launch sized shared memory for this cell's bin; refuse rather than overrun.
@@ -493,6 +511,7 @@ __global__ void __launch_bounds__(kCellThreads, 8) window_kernel(const Params P,
     if (tid == 0) ckoff[nch] = nkids;
     for (int32_t k = tid; k < nkids; k += T) ckids[k] = P.chain_kids[kb + k];
     for (int32_t k = tid; k <= nlev; k += T) lvc[k] = P.level_chain[lv0 + k];
+    for (int32_t k = tid; k < P.ngroups * (T + 1); k += T) spart[k] = P.part[(int64_t)c * P.ngroups * (T + 1) + k];
     if (tid == 0) {
         int32_t count = P.inbox_count[c];
         if (count > P.inbox_cap) {
@@ -537,7 +556,6 @@ __global__ void __launch_bounds__(kCellThreads, 8) window_kernel(const Params P,
                     break;
             }
             S.node[r] = (int32_t)(G.node[row] - nb);
-            S.seg[r] = G.seg[row];
         }
     }
     const int32_t nev = s_nev;
@@ -575,7 +593,9 @@ __global__ void __launch_bounds__(kCellThreads, 8) window_kernel(const Params P,
     }
     __syncthreads();
 
-    const float q10f = (float)mind_pow(3.0, (P.celsius - 6.3) / 10.0);
+    const double q10 = mind_pow(3.0, (P.celsius - 6.3) / 10.0);
+    const float q10f = (float)q10;
+    const int32_t nlo = (int32_t)(((int64_t)tid * n) / T), nhi = (int32_t)(((int64_t)(tid + 1) * n) / T);
     int32_t cursor = 0;
     bool singular = false;
 
@@ -608,54 +628,50 @@ __global__ void __launch_bounds__(kCellThreads, 8) window_kernel(const Params P,
                 ++cursor;
             }
         }
-        // 3. Clear the membrane sums.
-        for (int32_t i = tid; i < n; i += T) {
+        __syncthreads();  // NET_RECEIVE above wrote staged synapse state
+
+        // 3-5. Each thread owns the contiguous nodes [nlo, nhi) and the rows of every group
+        //      on them (rows are sorted by node), so the mechanism sums of a node are
+        //      accumulated in group order, rows in row order, by one thread, and its
+        //      assembly follows without a barrier (it reads only the unchanged v of
+        //      neighbours).  Parameters are streamed from HBM through the read-only path.
+        for (int32_t i = nlo; i < nhi; ++i) {
             sd[i] = 0.0;
             sr[i] = 0.0;
         }
-        __syncthreads();
-
-        // 4. BREAKPOINT currents at v + 0.001 and v, group by group; rows of one node in row order.
         const double tc = t + 0.5 * P.dt;
         for (int32_t g = 0; g < P.ngroups; ++g) {
             const DevGroup &GG = P.groups[g];
             const StagedGroup G = sg[g];
-            if (G.rows == 0) continue;
+            const int32_t lo = spart[g * (T + 1) + tid], hi = spart[g * (T + 1) + tid + 1];
+            if (lo >= hi) continue;
             if (G.kind == MIND_MECH_PAS) {
-                // One row per node; parameters streamed from HBM.
                 const double *pg = GG.f[PAS_G] + G.r0, *pe = GG.f[PAS_E] + G.r0, *ps = GG.f[PAS_SCALE] + G.r0;
                 const int32_t *pn = GG.node + G.r0;
-#pragma unroll 4
-                for (int32_t r = tid; r < G.rows; r += T) {
-                    const int32_t node = (int32_t)(pn[r] - nb);
-                    const double gp = pg[r], ep = pe[r], scale = ps[r];
+                for (int32_t r = lo; r < hi; ++r) {
+                    const int32_t node = (int32_t)(__ldg(pn + r) - nb);
+                    const double gp = __ldg(pg + r), ep = __ldg(pe + r), scale = __ldg(ps + r);
                     const double vv = sv[node];
                     const double probe = vv + 0.001;
                     const double shifted = 0.0 + gp * (probe - ep);
                     const double value = 0.0 + gp * (vv - ep);
                     sr[node] = sr[node] - scale * value;
-                    sd[node] = sd[node] + scale * (shifted - value) / 0.001;
+                    sd[node] = sd[node] + milli_quotient<MIXED>(scale * (shifted - value));
                 }
             } else if (G.kind == MIND_MECH_ICLAMP) {
-                const int32_t *pn = GG.node + G.r0, *psg = GG.seg + G.r0;
-                for (int32_t r = tid; r < G.rows; r += T) {
-                    const int32_t len = psg[r];
-                    if (len == 0) continue;
-                    const int32_t node = (int32_t)(pn[r] - nb);
-                    double R = sr[node], D = sd[node];
-                    for (int32_t q = G.r0 + r; q < G.r0 + r + len; ++q) {
-                        const double del = GG.f[IC_DEL][q];
-                        const double i = (tc < del + GG.f[IC_DUR][q] && tc >= del) ? GG.f[IC_AMP][q] : 0.0;
-                        const double shifted = 0.0 - i;
-                        const double value = 0.0 - i;
-                        R = R + -1.0 * value;
-                        D = D + 1.0 * (shifted - value) / 0.001;
-                    }
-                    sr[node] = R;
-                    sd[node] = D;
+                const int32_t *pn = GG.node + G.r0;
+                for (int32_t r = lo; r < hi; ++r) {
+                    const int32_t node = (int32_t)(__ldg(pn + r) - nb);
+                    const int64_t q = (int64_t)G.r0 + r;
+                    const double del = __ldg(GG.f[IC_DEL] + q);
+                    const double i = (tc < del + __ldg(GG.f[IC_DUR] + q) && tc >= del) ? __ldg(GG.f[IC_AMP] + q) : 0.0;
+                    const double shifted = 0.0 - i;
+                    const double value = 0.0 - i;
+                    sr[node] = sr[node] + -1.0 * value;
+                    sd[node] = sd[node] + milli_quotient<MIXED>(1.0 * (shifted - value));
                 }
             } else if (G.kind == MIND_MECH_HH) {
-                for (int32_t r = tid; r < G.rows; r += T) {
+                for (int32_t r = lo; r < hi; ++r) {
                     const int32_t node = G.node[r];
                     const double vv = sv[node];
                     const double probe = vv + 0.001;
@@ -675,46 +691,37 @@ __global__ void __launch_bounds__(kCellThreads, 8) window_kernel(const Params P,
                                                     G.at(HH_GL, r), G.at(HH_EL, r), G.at(HH_ENA, r), G.at(HH_EK, r));
                     const double scale = G.at(HH_SCALE, r);
                     sr[node] = sr[node] - scale * value;
-                    sd[node] = sd[node] + scale * (shifted - value) / 0.001;
+                    sd[node] = sd[node] + milli_quotient<MIXED>(scale * (shifted - value));
                 }
             } else if (G.kind == MIND_MECH_EXPSYN || G.kind == MIND_MECH_EXP2SYN) {
                 const bool two = G.kind == MIND_MECH_EXP2SYN;
                 const double *pe = GG.f[two ? E2_E : ES_E] + G.r0;
-                for (int32_t r = tid; r < G.rows; r += T) {
-                    const int32_t len = G.seg[r];
-                    if (len == 0) continue;
+                for (int32_t r = lo; r < hi; ++r) {
                     const int32_t node = G.node[r];
+                    const double e = __ldg(pe + r);
+                    double gs;
+                    if (two)
+                        gs = MIXED ? (double)(G.fat(1, r) - G.fat(0, r)) : G.at(1, r) - G.at(0, r);
+                    else
+                        gs = MIXED ? (double)G.fat(0, r) : G.at(0, r);
                     const double vv = sv[node];
                     const double probe = vv + 0.001;
-                    double R = sr[node], D = sd[node];
-                    for (int32_t q = r; q < r + len; ++q) {
-                        double gs;
-                        if (two)
-                            gs = MIXED ? (double)(G.fat(1, q) - G.fat(0, q)) : G.at(1, q) - G.at(0, q);
-                        else
-                            gs = MIXED ? (double)G.fat(0, q) : G.at(0, q);
-                        const double e = pe[q];
-                        const double shifted = 0.0 + gs * (probe - e);
-                        const double value = 0.0 + gs * (vv - e);
-                        R = R + -1.0 * value;
-                        D = D + 1.0 * (shifted - value) / 0.001;
-                    }
-                    sr[node] = R;
-                    sd[node] = D;
+                    const double shifted = 0.0 + gs * (probe - e);
+                    const double value = 0.0 + gs * (vv - e);
+                    sr[node] = sr[node] + -1.0 * value;
+                    sd[node] = sd[node] + milli_quotient<MIXED>(1.0 * (shifted - value));
                 }
             }
-            __syncthreads();
         }
-
-        // 5. Cable assembly, node-parallel: d = C/dt + d + axial_diagonal; own axial term, then children.
-#pragma unroll 2
-        for (int32_t i = tid; i < n; i += T) {
+        // Cable assembly of the owned nodes: d = C/dt + d + axial_diagonal; own axial term, then children.
+        for (int32_t i = nlo; i < nhi; ++i) {
             const int64_t gi = nb + i;
+            const double cdt = __ldg(P.cdt + gi), adi = __ldg(P.ad + gi);
             const int32_t k = chain_of[i];
             const int32_t top = ctop[k];
             const int32_t bottom = top + clen[k] - 1;
             const double vi = sv[i];
-            sd[i] = (P.cdt[gi] + sd[i]) + P.ad[gi];
+            sd[i] = (cdt + sd[i]) + adi;
             double R = sr[i];
             const int32_t p = i == top ? cpar[k] : i - 1;
             if (p >= 0) R = R + sa[i] * (sv[p] - vi);
@@ -745,7 +752,10 @@ __global__ void __launch_bounds__(kCellThreads, 8) window_kernel(const Params P,
                     R = R + sxr[cc];
                 }
                 singular |= (D == 0.0) | !isfinite(D);
-                sd[bottom] = D;
+                // Mixed mode keeps the pivot's reciprocal in place of the pivot: the
+                // back-substitution then multiplies instead of dividing.
+                const double yb = MIXED ? approx_reciprocal(D) : 0.0;
+                sd[bottom] = MIXED ? yb : D;
                 sr[bottom] = R;
                 double pxd = 0.0, pxr = 0.0;
                 if (bottom > top || !rooted) {
@@ -756,7 +766,7 @@ __global__ void __launch_bounds__(kCellThreads, 8) window_kernel(const Params P,
                         rn = sr[bottom - 1];
                         an = sa[bottom - 1];
                     }
-                    const double f = ab / D;
+                    const double f = MIXED ? ab * yb : ab / D;
                     pxd = f * ab;
                     pxr = f * R;
                     // interior nodes: every one has its parent at i - 1
@@ -767,19 +777,27 @@ __global__ void __launch_bounds__(kCellThreads, 8) window_kernel(const Params P,
                         rn = sr[i - 1];
                         an = sa[i - 1];
                         singular |= (Di == 0.0) | !isfinite(Di);
-                        sd[i] = Di;
                         sr[i] = Ri;
-                        const double fi = ai / Di;
+                        double fi;
+                        if (MIXED) {
+                            const double yi = approx_reciprocal(Di);
+                            sd[i] = yi;
+                            fi = ai * yi;
+                        } else {
+                            sd[i] = Di;
+                            fi = ai / Di;
+                        }
                         pxd = fi * ai;
                         pxr = fi * Ri;
                     }
                     if (i == top && bottom > top) {
                         const double Dt = dn - pxd, Rt = rn + pxr;
                         singular |= (Dt == 0.0) | !isfinite(Dt);
-                        sd[top] = Dt;
+                        const double yt = MIXED ? approx_reciprocal(Dt) : 0.0;
+                        sd[top] = MIXED ? yt : Dt;
                         sr[top] = Rt;
                         if (!rooted) {
-                            const double ft = an / Dt;
+                            const double ft = MIXED ? an * yt : an / Dt;
                             pxd = ft * an;
                             pxr = ft * Rt;
                         }
@@ -806,7 +824,8 @@ __global__ void __launch_bounds__(kCellThreads, 8) window_kernel(const Params P,
                         an = sa[top + 1];
                         dn = sd[top + 1];
                     }
-                    x = (par >= 0 ? ri + ai * xp : ri) / di;
+                    const double num = par >= 0 ? ri + ai * xp : ri;
+                    x = MIXED ? num * di : num / di;   // mixed mode: di holds 1/pivot
                     sr[top] = x;
                     sv[top] = sv[top] + x;
                 }
@@ -817,7 +836,7 @@ __global__ void __launch_bounds__(kCellThreads, 8) window_kernel(const Params P,
                         an = sa[i + 1];
                         dn = sd[i + 1];
                     }
-                    x = (ri + ai * x) / di;
+                    x = MIXED ? (ri + ai * x) * di : (ri + ai * x) / di;
                     sr[i] = x;
                     sv[i] = sv[i] + x;
                 }
@@ -846,7 +865,7 @@ __global__ void __launch_bounds__(kCellThreads, 8) window_kernel(const Params P,
                             const int32_t r = w / 3, gate = w - 3 * r;
                             const double vv = sv[G.node[r]];
                             double inf, tau;
-                            hh_gate(vv, P.celsius, gate, inf, tau);
+                            hh_gate(vv, q10, gate, inf, tau);
                             const int slot = HH_M + gate;
                             G.at(slot, r) = cnexp(G.at(slot, r), inf, tau, P.dt);
                         }

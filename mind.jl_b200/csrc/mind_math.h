@@ -175,6 +175,26 @@ MIND_HD double mind_pow(double x, double y) {
     return NAN;
 }
 
+/* x / 0.001, bit for bit equal to the IEEE quotient, without a division.
+ * 1000 is the correctly rounded reciprocal of the double 0.001 and differs from
+ * 1/0.001 by 0.19 units in its last place, so q0 = x*1000 lies within one ulp of
+ * x/0.001; the residual x - q0*0.001 is then exact in one FMA, and one correction
+ * step rounds to the IEEE quotient (Markstein's theorem: P. W. Markstein,
+ * "Computation of elementary functions on the IBM RISC System/6000 processor",
+ * IBM J. Res. Dev. 34(1), 1990; J.-M. Muller et al., Handbook of Floating-Point
+ * Arithmetic, chapter on FMA-based division).  The theorem assumes no underflow
+ * or overflow, so magnitudes outside [2^-900, 2^900], and non-finite values,
+ * take the division; zeros come back unchanged, as 0/0.001 keeps the sign. */
+MIND_HD double mind_div_milli(double x) {
+    const double ax = fabs(x);
+    if (ax >= 0x1p-900 && ax <= 0x1p+900) {
+        const double q0 = x * 1000.0;
+        const double r = fma(-q0, 0.001, x);
+        return fma(r, 1000.0, q0);
+    }
+    return x == 0.0 ? x : x / 0.001;
+}
+
 /* ---- Philox4x32-10 ---- */
 #define MIND_PHILOX_M0 0xD2511F53u
 #define MIND_PHILOX_M1 0xCD9E8D57u

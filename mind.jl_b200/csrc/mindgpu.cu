@@ -356,6 +356,7 @@ int create(const MindLayout *L, MindHandle *h) {
     P.seed = L->seed;
     P.ns_group = -1;
     std::vector<std::vector<int32_t>> dev_row_of(L->n_mechanisms);  // layout row -> device row
+    std::vector<int32_t> part((size_t)ncells * L->n_mechanisms * (kCellThreads + 1), 0);
     std::vector<std::vector<int32_t>> row_cell(L->n_mechanisms);
     for (int32_t g = 0; g < L->n_mechanisms; ++g) {
         const MindMechanism &m = L->mechanisms[g];
@@ -425,6 +426,17 @@ int create(const MindLayout *L, MindHandle *h) {
             }
             for (int32_t r = 0; r < rows; ++r) row_off[row_cell[g][r] + 1]++;
             for (int32_t c = 0; c < ncells; ++c) row_off[c + 1] += row_off[c];
+            // thread partition: rows of a cell are sorted by node, so each thread's rows are a range
+            for (int32_t c = 0; c < ncells; ++c) {
+                const int64_t nc = node_off[c + 1] - node_off[c];
+                int32_t *pc = part.data() + ((size_t)c * L->n_mechanisms + g) * (kCellThreads + 1);
+                int32_t r = row_off[c];
+                for (int32_t t = 0; t <= kCellThreads; ++t) {
+                    const int64_t first_node = node_off[c] + (int64_t)t * nc / kCellThreads;
+                    while (r < row_off[c + 1] && node_dev[r] < first_node) ++r;
+                    pc[t] = r - row_off[c];
+                }
+            }
         }
         if (artificial) {
             init.logical.resize(rows);
@@ -533,6 +545,7 @@ int create(const MindLayout *L, MindHandle *h) {
     P.chain_kids = h->upload(chain_kids);
     P.level_off = h->upload(level_off);
     P.level_chain = h->upload(level_chain);
+    P.part = h->upload(part);
     P.det_off = h->upload(det_off);
     P.det_node = h->upload(det_node);
     P.det_source = h->upload(det_source);

@@ -619,6 +619,10 @@ extern "C" {
 double oracle_exp(double x) { return mind_exp(x); }
 double oracle_log(double x) { return mind_log(x); }
 double oracle_pow(double x, double y) { return mind_pow(x, y); }
+/* The division-free x/0.001 of the CUDA path, exported so its equality with x/0.001 can be tested. */
+void oracle_div_milli(const double *x, double *out, int64_t n) {
+    for (int64_t i = 0; i < n; ++i) out[i] = mind_div_milli(x[i]);
+}
 void oracle_philox(uint32_t *ctr, uint32_t key0, uint32_t key1) { mind_philox4x32_10(ctr, key0, key1); }
 
 /* One random stream in the nrnran123 layout: `n` negexp draws from a fresh

@@ -42,6 +42,8 @@ def _load():
         lib.oracle_log.argtypes = [ctypes.c_double]
         lib.oracle_pow.restype = ctypes.c_double
         lib.oracle_pow.argtypes = [ctypes.c_double, ctypes.c_double]
+        lib.oracle_div_milli.restype = None
+        lib.oracle_div_milli.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64]
         lib.oracle_philox.restype = None
         lib.oracle_philox.argtypes = [ctypes.POINTER(ctypes.c_uint32), ctypes.c_uint32, ctypes.c_uint32]
         lib.oracle_negexp_stream.restype = None
@@ -61,6 +63,16 @@ def log(x: float) -> float:
 
 def pow(x: float, y: float) -> float:
     return _load().oracle_pow(x, y)
+
+
+def div_milli(x):
+    """The CUDA path's division-free x / 0.001 (mind_math.h), element-wise."""
+    import numpy as np
+
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    out = np.empty_like(x)
+    _load().oracle_div_milli(x.ctypes.data, out.ctypes.data, x.size)
+    return out
 
 
 def philox4x32_10(ctr, key0: int, key1: int):

@@ -47,6 +47,22 @@ def test_special_values():
     assert abs(oracle.pow(3.0, 0.5) - math.sqrt(3.0)) < 4e-16
 
 
+def test_division_free_milli_quotient_equals_ieee_division():
+    """x / 0.001 without a division (the CUDA path's current and dI/dV terms) is the IEEE quotient."""
+    rng = np.random.default_rng(7)
+    bits = rng.integers(0, 2**63, size=2_000_000, dtype=np.uint64)
+    exponent = rng.integers(1023 - 900, 1023 + 901, size=bits.size).astype(np.uint64)
+    bits = (bits & np.uint64(0x800FFFFFFFFFFFFF)) | (exponent << np.uint64(52))
+    xs = np.concatenate([bits.view(np.float64), np.linspace(-1.0, 1.0, 200_001), np.arange(-5000, 5001) * 1e-7,
+                         np.array([0.0, -0.0, 1e-310, -1e-310, 5e-324, 1e300, np.inf, -np.inf, 2.0**-900,
+                                   2.0**900, np.nextafter(2.0**-900, 0.0)])])
+    got = oracle.div_milli(xs)
+    want = xs / 0.001
+    assert np.array_equal(got.view(np.uint64), want.view(np.uint64))
+    nan = oracle.div_milli(np.array([np.nan]))
+    assert np.isnan(nan[0])
+
+
 @pytest.mark.parametrize("ctr,key,want", [
     ((0, 0, 0, 0), (0, 0), (0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8)),
     ((0xFFFFFFFF,) * 4, (0xFFFFFFFF,) * 2, (0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD)),
