@@ -46,7 +46,10 @@ def parse():
     p.add_argument("--cells", type=int, default=None, help="cells (default: the configuration's count)")
     p.add_argument("--config", type=int, default=2, choices=[2, 3],
                    help="2: 10,000 uneven binary-tree cells (the headline); 3: 1,000 pyramidal-like cells")
-    p.add_argument("--precision", default="fp64", choices=["fp64", "mixed", "both"])
+    p.add_argument("--precision", default="both", choices=["fp64", "mixed", "both"],
+                   help="both: the FP64 headline plus the mixed mode and its accuracy against FP64")
+    p.add_argument("--accuracy-ms", type=float, default=0.0,
+                   help="instead of timing: run FP64 and mixed from t=0 for this long and print their differences")
     p.add_argument("--cpu-steps", type=int, default=8)
     p.add_argument("--no-cpu-baseline", action="store_true")
     return p.parse_args()
@@ -170,6 +173,42 @@ def recorded_traffic():
         return None
 
 
+def mixed_accuracy(layout, fp64, mixed, warmup: int, steps: int) -> dict:
+    """Mixed mode against FP64 on the same run: soma voltages of every cell and the cell spike raster.
+
+    The FP64 path reproduces the CPU FP64 oracle bit for bit (tests/test_parity_gpu.py), so
+    these are also the differences to the oracle.  A spike counts as matched when the same cell
+    has a spike in the other run within one dt.
+    """
+    v64, sid64, t64 = fp64
+    v32, sid32, t32 = mixed
+    dv = np.abs(v32 - v64)
+    sub = (v64 < -50.0) & (v32 < -50.0)
+    n_cells = layout.n_cells
+    dt = layout.dt
+    shifts = []
+    matched = 0
+    cell64 = sid64 < n_cells
+    for sid, t in zip(sid64[cell64], t64[cell64]):
+        same = t32[sid32 == sid]
+        if same.size:
+            d = np.min(np.abs(same - t))
+            if d <= dt + 1e-9:
+                matched += 1
+                shifts.append(d)
+    n64 = int(np.sum(cell64))
+    n32 = int(np.sum(sid32 < n_cells))
+    return {
+        "reference": "FP64 path (bit-identical to the CPU FP64 oracle)",
+        "window_ms": [warmup * dt, (warmup + steps) * dt],
+        "max_dv_mv": float(dv.max()), "max_dv_subthreshold_mv": float(dv[sub].max()) if sub.any() else None,
+        "p99_dv_mv": float(np.percentile(dv, 99)),
+        "cell_spikes_fp64": n64, "cell_spikes_mixed": n32,
+        "spikes_within_1dt": (matched / n64) if n64 else None,
+        "mean_shift_ms": float(np.mean(shifts)) if shifts else None,
+    }
+
+
 def run_reference(args, rank: int):
     if rank != 0:
         return
@@ -219,9 +258,23 @@ def main():
     from mind_b200 import replicas
 
     model, layout = build_network(args.cells, seed=replicas.replica_seed(1, rank), config=args.config)
+    if args.accuracy_ms > 0:
+        if rank == 0:
+            soma_all = [mb.RecordSpec(layout.voltage_node(c), f"v{c}") for c in range(1, layout.n_cells + 1)]
+            runs = {}
+            for precision in ("fp64", "mixed"):
+                mb.initialize(model, precision=precision)
+                r = mb.run(model, args.accuracy_ms, records=soma_all, record_spikes=True)
+                runs[precision] = (np.stack([r.traces[x.name] for x in soma_all]), r.spike_sources, r.spike_times)
+            steps = int(round(args.accuracy_ms / layout.dt))
+            print(json.dumps({"config": f"config{args.config}", "cells": layout.n_cells,
+                              "accuracy": mixed_accuracy(layout, runs["fp64"], runs["mixed"], 0, steps)}), flush=True)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
     soma = [mb.RecordSpec(layout.voltage_node(c), f"v{c}") for c in range(1, layout.n_cells + 1)]
     precisions = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
-    results = {}
+    results, runs = {}, {}
     clocks = None
     for precision in precisions:
         mb.initialize(model, precision=precision)
@@ -254,6 +307,8 @@ def main():
         e2e_s, _ = replicas.reduce_timing(time.perf_counter() - t0, 0.0, device="cuda")
         d2h = (len(soma) * 8 * (args.steps + 1) + 16 * len(e2e_result.spike_times)) / args.steps
         h2d = 8 * len(soma) / args.steps
+        runs[precision] = (np.stack([e2e_result.traces[r.name] for r in soma]), e2e_result.spike_sources,
+                           e2e_result.spike_times)
         results[precision] = {
             "value": value, "ms_per_step": run_ms / args.steps, "window_ms": window_ms,
             "window_launches": stats.window_launches, "launches": stats.launches, "window_steps": stats.window_steps,
@@ -293,6 +348,8 @@ def main():
         "clocks": clocks,
         "modes": {k: {"value": v["value"], "ms_per_step": v["ms_per_step"], "e2e": v["e2e"]}
                   for k, v in results.items()},
+        "accuracy": (mixed_accuracy(layout, runs["fp64"], runs["mixed"], args.warmup, args.steps)
+                     if "fp64" in runs and "mixed" in runs else None),
         "spikes": head["spikes"],
     }
     if world == 1 and not args.no_cpu_baseline:

@@ -177,8 +177,9 @@ struct Params {
     const int32_t *level_chain;  // per cell: nlevels+1 local chain starts (chains sorted by level)
     DevGroup groups[kMaxGroups];
     // per cell, group and thread: first row (relative to the cell's first row of the group)
-    // whose node lies in the thread's contiguous node range [t*n/T, (t+1)*n/T)
+    // whose node lies in the thread's contiguous node range (node_part)
     const int32_t *part;       // [ncells][ngroups][kCellThreads + 1]
+    const int32_t *node_part;  // [ncells][kCellThreads + 1]: thread t owns local nodes [node_part[t], node_part[t+1])
     // detectors
     const int32_t *det_off;    // [ncells+1]
     const int32_t *det_node;   // local node

@@ -595,7 +595,7 @@ __global__ void __launch_bounds__(kCellThreads, 8) window_kernel(const Params P,
 
     const double q10 = mind_pow(3.0, (P.celsius - 6.3) / 10.0);
     const float q10f = (float)q10;
-    const int32_t nlo = (int32_t)(((int64_t)tid * n) / T), nhi = (int32_t)(((int64_t)(tid + 1) * n) / T);
+    const int32_t nlo = P.node_part[(int64_t)c * (T + 1) + tid], nhi = P.node_part[(int64_t)c * (T + 1) + tid + 1];
     int32_t cursor = 0;
     bool singular = false;
 

@@ -357,6 +357,31 @@ int create(const MindLayout *L, MindHandle *h) {
     P.ns_group = -1;
     std::vector<std::vector<int32_t>> dev_row_of(L->n_mechanisms);  // layout row -> device row
     std::vector<int32_t> part((size_t)ncells * L->n_mechanisms * (kCellThreads + 1), 0);
+    // Thread node ranges: contiguous, cut where the prefix of estimated per-node work (the
+    // node's assembly plus its mechanism rows, hh weighing most) crosses t/threads of the cell's.
+    std::vector<double> work(n, 1.0);
+    for (int32_t g = 0; g < L->n_mechanisms; ++g) {
+        const MindMechanism &m = L->mechanisms[g];
+        if (m.kind == MIND_MECH_NETSTIM) continue;
+        const double w = m.kind == MIND_MECH_HH ? 4.0 : m.kind == MIND_MECH_ICLAMP ? 1.0 : 1.4;
+        for (int64_t r = 0; r < m.rows; ++r)
+            if (m.nodes[r] >= 1 && m.nodes[r] <= n) work[h->packed_of_layout[m.nodes[r] - 1]] += w;
+    }
+    std::vector<int32_t> node_part((size_t)ncells * (kCellThreads + 1), 0);
+    for (int32_t c = 0; c < ncells; ++c) {
+        const int64_t b = node_off[c], nc = node_off[c + 1] - b;
+        double total = 0.0;
+        for (int64_t i = 0; i < nc; ++i) total += work[b + i];
+        int32_t *np = node_part.data() + (size_t)c * (kCellThreads + 1);
+        double acc = 0.0;
+        int64_t i = 0;
+        for (int32_t t = 0; t < kCellThreads; ++t) {
+            np[t] = (int32_t)i;
+            const double goal = total * (t + 1) / kCellThreads;
+            while (i < nc && acc + 0.5 * work[b + i] < goal) acc += work[b + i++];
+        }
+        np[kCellThreads] = (int32_t)nc;
+    }
     std::vector<std::vector<int32_t>> row_cell(L->n_mechanisms);
     for (int32_t g = 0; g < L->n_mechanisms; ++g) {
         const MindMechanism &m = L->mechanisms[g];
@@ -428,11 +453,10 @@ int create(const MindLayout *L, MindHandle *h) {
             for (int32_t c = 0; c < ncells; ++c) row_off[c + 1] += row_off[c];
             // thread partition: rows of a cell are sorted by node, so each thread's rows are a range
             for (int32_t c = 0; c < ncells; ++c) {
-                const int64_t nc = node_off[c + 1] - node_off[c];
                 int32_t *pc = part.data() + ((size_t)c * L->n_mechanisms + g) * (kCellThreads + 1);
                 int32_t r = row_off[c];
                 for (int32_t t = 0; t <= kCellThreads; ++t) {
-                    const int64_t first_node = node_off[c] + (int64_t)t * nc / kCellThreads;
+                    const int64_t first_node = node_off[c] + node_part[(size_t)c * (kCellThreads + 1) + t];
                     while (r < row_off[c + 1] && node_dev[r] < first_node) ++r;
                     pc[t] = r - row_off[c];
                 }
@@ -546,6 +570,7 @@ int create(const MindLayout *L, MindHandle *h) {
     P.level_off = h->upload(level_off);
     P.level_chain = h->upload(level_chain);
     P.part = h->upload(part);
+    P.node_part = h->upload(node_part);
     P.det_off = h->upload(det_off);
     P.det_node = h->upload(det_node);
     P.det_source = h->upload(det_source);
