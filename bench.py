@@ -338,11 +338,13 @@ def main():
             "bound": "hbm",
             "achieved": head["achieved_gbs"], "peak": peak, "unit": "GB/s",
             "frac": (head["achieved_gbs"] / peak) if head["achieved_gbs"] else None,
-            "traffic": traffic.get("dram_bytes_per_launch") if traffic else None,
+            "traffic": traffic.get("dram_bytes_per_step") if traffic and args.config == 2 else None,
+            "traffic_unit": "DRAM bytes per micro step (all bins of a window / window steps), from one ncu capture",
             "kernel": "window_kernel", "algo_bytes_per_step": head["algo_bytes_per_step"],
             "peak_source": f"{peak_kind} hbm_gbs",
-            "note": "algorithmic bytes of one pass per step; the window kernel keeps each cell on-chip "
-                    "for a window of steps, so its DRAM traffic is below the algorithmic bytes",
+            "note": "achieved = algorithmic bytes of one pass per step / device time per step; the window "
+                    "kernel keeps each cell on-chip for a window of steps, so its DRAM traffic (traffic) is "
+                    "far below the algorithmic bytes and the kernel is latency-bound, not HBM-bound",
         },
         "gpu_launches": head["launches"] + 2,
         "clocks": clocks,

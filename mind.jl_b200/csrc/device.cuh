@@ -58,7 +58,7 @@ struct DevGroup {
     int32_t *node;            // local node per row
     int32_t *seg;             // rows in the segment starting here (0 = not a segment head)
     double *f[12];            // field arrays, meaning by kind (see mindgpu.cu)
-    float *s[4];              // FP32 state for mixed mode
+    float *s[4];              // FP32 decay factors of the synapses (mixed mode)
 };
 
 /* Field slots per kind. */
@@ -69,12 +69,11 @@ enum { E2_E, E2_A, E2_B, E2_FACTOR, E2_TAU1, E2_TAU2, E2_DECAY1, E2_DECAY2, E2_N
 enum { IC_DEL, IC_DUR, IC_AMP, IC_NSLOT };
 enum { NS_INTERVAL, NS_NUMBER, NS_START, NS_NOISE, NS_EVENT, NS_ON, NS_ISPIKE, NS_NEXT_T,
        NS_NEXT_FLAG, NS_NSLOT };
-/* FP32 state slots (mixed mode). */
-enum { HHS_M, HHS_H, HHS_N };
-enum { ESS_G, ESS_DECAY };
-enum { E2S_A, E2S_B, E2S_DECAY1, E2S_DECAY2 };
+/* FP32 parameter slots (mixed mode). */
+enum { ESS_DECAY };
+enum { E2S_DECAY1, E2S_DECAY2 };
 
-/* Number of FP64 slots and FP32 (mixed-mode) state slots of each kind. */
+/* Number of FP64 slots and FP32 (mixed-mode) parameter slots of each kind. */
 __host__ __device__ inline int kind_slots(int32_t kind) {
     switch (kind) {
         case MIND_MECH_HH: return HH_NSLOT;
@@ -90,36 +89,18 @@ __host__ __device__ inline int kind_slots(int32_t kind) {
  * Rows whose state changes every step keep that state in shared memory for the
  * window; everything else of a row (parameters, decay factors) is streamed
  * from HBM.  hh rows are few per cell and keep all their slots on chip.
- *   staged_doubles  FP64 slots staged per row (FP64 mode: hh all, ExpSyn g, Exp2Syn A,B)
- *   staged_floats   FP32 slots staged per row (mixed mode: hh m,h,n, ExpSyn g, Exp2Syn A,B)
+ *   staged_doubles  FP64 slots staged per row: hh all, ExpSyn g, Exp2Syn A,B.  State is
+ *                   FP64 in both modes; the mixed mode computes hh's rates and the
+ *                   synapses' per-step decrements in FP32 and accumulates them in FP64.
  */
 __host__ __device__ inline bool kind_staged(int32_t kind) {
     return kind == MIND_MECH_HH || kind == MIND_MECH_EXPSYN || kind == MIND_MECH_EXP2SYN;
 }
-__host__ __device__ inline int staged_doubles(int32_t kind, bool mixed) {
+__host__ __device__ inline int staged_doubles(int32_t kind) {
     switch (kind) {
         case MIND_MECH_HH: return HH_NSLOT;
-        case MIND_MECH_EXPSYN: return mixed ? 0 : 1;
-        case MIND_MECH_EXP2SYN: return mixed ? 0 : 2;
-        default: return 0;
-    }
-}
-__host__ __device__ inline int staged_floats(int32_t kind, bool mixed) {
-    if (!mixed) return 0;
-    switch (kind) {
-        case MIND_MECH_HH: return 3;
         case MIND_MECH_EXPSYN: return 1;
         case MIND_MECH_EXP2SYN: return 2;
-        default: return 0;
-    }
-}
-/* FP32 state arrays per kind in device memory (mixed mode). */
-/* FP32 state arrays per kind in device memory (mixed mode). */
-__host__ __device__ inline int kind_floats(int32_t kind) {
-    switch (kind) {
-        case MIND_MECH_HH: return 3;
-        case MIND_MECH_EXPSYN: return 2;
-        case MIND_MECH_EXP2SYN: return 4;
         default: return 0;
     }
 }
@@ -130,7 +111,6 @@ __host__ __device__ inline int kind_floats(int32_t kind) {
  *            chain tops [nch each]; event increments [inbox_cap]; staged FP64
  *            slots of the staged rows;
  *   events   the cell's inbox for the window [inbox_cap];
- *   floats   staged FP32 slots (mixed mode);
  *   ints     per staged row: local node; chain top, length,
  *            parent, child-chain CSR; level starts; inbox order; the
  *            threads' row ranges per group [ngroups][threads + 1];
@@ -143,18 +123,17 @@ struct CellShape {
 };
 
 __host__ __device__ inline size_t cell_smem_bytes(const CellShape &s, const int32_t *kinds, int32_t ngroups,
-                                                  bool mixed, int32_t inbox_cap) {
+                                                  int32_t inbox_cap) {
     size_t doubles = 4 * (size_t)s.n + 2 * (size_t)s.nch + (size_t)inbox_cap;
-    size_t floats = 0, ints = 0;
+    size_t ints = 0;
     for (int32_t g = 0; g < ngroups; ++g) {
         if (!kind_staged(kinds[g])) continue;
-        doubles += (size_t)staged_doubles(kinds[g], mixed) * s.rows[g];
-        floats += (size_t)staged_floats(kinds[g], mixed) * s.rows[g];
+        doubles += (size_t)staged_doubles(kinds[g]) * s.rows[g];
         ints += (size_t)s.rows[g];
     }
     ints += 4 * (size_t)s.nch + 1 + (size_t)s.nkids + (size_t)s.nlev + 1 + (size_t)inbox_cap;
     ints += (size_t)ngroups * (kCellThreads + 1);
-    return doubles * 8 + (size_t)inbox_cap * sizeof(InboxEvent) + floats * 4 + ints * 4 + 2 * (size_t)s.n;
+    return doubles * 8 + (size_t)inbox_cap * sizeof(InboxEvent) + ints * 4 + 2 * (size_t)s.n;
 }
 
 struct Params {

@@ -143,28 +143,37 @@ __device__ __forceinline__ double approx_reciprocal(double x) {
     return fma(y, e, y);
 }
 
-/* FP32 gating for the mixed mode: same equations, single precision, fast exp. */
+/* FP32 gating for the mixed mode: hh's rate equations in single precision.  The cnexp
+ * factor 1 - exp(-dt/tau) is formed as -expm1f(-dt/tau) and vtrap's x/(exp(x/y) - 1) as
+ * x/expm1f(x/y): 1 - exp(-x) for the x = dt/tau ~ 0.005-0.2 of a step would lose up to
+ * four of FP32's seven digits to cancellation, and the gate increment is that product. */
 __device__ __forceinline__ float vtrapf(float x, float y) {
     if (fabsf(x / y) < 1e-6f) return y * (1.0f - x / y / 2.0f);
-    return x / (__expf(x / y) - 1.0f);
+    return x / expm1f(x / y);
 }
 
-__device__ __forceinline__ void hh_advance_f32(float v, float q10, float dt, float &m, float &h, float &n) {
-    float alpha = 0.1f * vtrapf(-(v + 40.0f), 10.0f);
-    float beta = 4.0f * __expf(-(v + 65.0f) / 18.0f);
-    float sum = alpha + beta;
-    float tau = 1.0f / (q10 * sum);
-    m = m + (1.0f - __expf(dt * (-1.0f / tau))) * (alpha / sum - m);
-    alpha = 0.07f * __expf(-(v + 65.0f) / 20.0f);
-    beta = 1.0f / (__expf(-(v + 35.0f) / 10.0f) + 1.0f);
-    sum = alpha + beta;
-    tau = 1.0f / (q10 * sum);
-    h = h + (1.0f - __expf(dt * (-1.0f / tau))) * (alpha / sum - h);
-    alpha = 0.01f * vtrapf(-(v + 55.0f), 10.0f);
-    beta = 0.125f * __expf(-(v + 65.0f) / 80.0f);
-    sum = alpha + beta;
-    tau = 1.0f / (q10 * sum);
-    n = n + (1.0f - __expf(dt * (-1.0f / tau))) * (alpha / sum - n);
+__device__ __forceinline__ float cnexp_factor_f32(float dt, float tau) { return -expm1f(dt * (-1.0f / tau)); }
+
+/* One gate's steady state and cnexp factor in FP32 (0 = m, 1 = h, 2 = n); the caller
+ * applies s + factor * (inf - s) to the FP64 state, so rounding does not accumulate in
+ * the stored gates over a long run. */
+__device__ __forceinline__ void hh_gate_f32(double v, float q10, float dt, int gate, float &inf, float &factor) {
+    // The voltage offsets are formed in FP64 before rounding to FP32, so a membrane near
+    // rest keeps its small distance from each rate's midpoint exactly.
+    float alpha, beta;
+    if (gate == 0) {
+        alpha = 0.1f * vtrapf((float)(-(v + 40.0)), 10.0f);
+        beta = 4.0f * expf((float)(-(v + 65.0)) / 18.0f);
+    } else if (gate == 1) {
+        alpha = 0.07f * expf((float)(-(v + 65.0)) / 20.0f);
+        beta = 1.0f / (expf((float)(-(v + 35.0)) / 10.0f) + 1.0f);
+    } else {
+        alpha = 0.01f * vtrapf((float)(-(v + 55.0)), 10.0f);
+        beta = 0.125f * expf((float)(-(v + 65.0)) / 80.0f);
+    }
+    const float sum = alpha + beta;
+    inf = alpha / sum;
+    factor = cnexp_factor_f32(dt, 1.0f / (q10 * sum));
 }
 
 /* Sum of hh's current fields in the reference's order: il, then ina, then ik. */
@@ -299,15 +308,11 @@ __global__ void mechanism_init_kernel(const Params P, int32_t g) {
                 G.f[HH_M][r] = R.minf;
                 G.f[HH_H][r] = R.hinf;
                 G.f[HH_N][r] = R.ninf;
-                G.s[HHS_M][r] = (float)R.minf;
-                G.s[HHS_H][r] = (float)R.hinf;
-                G.s[HHS_N][r] = (float)R.ninf;
             } break;
             case MIND_MECH_EXPSYN: {
                 G.f[ES_G][r] = 0.0;
                 double decay = 1.0 - mind_exp(P.dt * (-1.0 / G.f[ES_TAU][r]));
                 G.f[ES_DECAY][r] = decay;
-                G.s[ESS_G][r] = 0.0f;
                 G.s[ESS_DECAY][r] = (float)decay;
             } break;
             case MIND_MECH_EXP2SYN: {
@@ -325,8 +330,6 @@ __global__ void mechanism_init_kernel(const Params P, int32_t g) {
                 double d2 = 1.0 - mind_exp(P.dt * (-1.0 / tau2));
                 G.f[E2_DECAY1][r] = d1;
                 G.f[E2_DECAY2][r] = d2;
-                G.s[E2S_A][r] = 0.0f;
-                G.s[E2S_B][r] = 0.0f;
                 G.s[E2S_DECAY1][r] = (float)d1;
                 G.s[E2S_DECAY2][r] = (float)d2;
             } break;
@@ -381,30 +384,18 @@ __device__ __forceinline__ bool event_before(const InboxEvent &x, const InboxEve
 struct StagedGroup {
     int32_t kind, rows, r0;   // r0 = first device row of the cell
     double *f;                // staged FP64 slots [slots][rows]
-    float *s;                 // staged FP32 slots [slots][rows] (mixed mode)
     int32_t *node;            // local node per row
     __device__ __forceinline__ double &at(int slot, int r) const { return f[slot * rows + r]; }
-    __device__ __forceinline__ float &fat(int slot, int r) const { return s[slot * rows + r]; }
 };
 
 /* NET_RECEIVE of the synapses (mod/ExpSyn.mod: g += w; mod/Exp2Syn.mod: A += w*factor,
  * B += w*factor) on a staged row; `inc` is w, or w*factor for Exp2Syn. */
-template <bool MIXED>
 __device__ __forceinline__ void apply_event(const StagedGroup &G, int32_t row, double inc) {
     if (G.kind == MIND_MECH_EXPSYN) {
-        if (MIXED)
-            G.fat(0, row) = G.fat(0, row) + (float)inc;
-        else
-            G.at(0, row) = G.at(0, row) + inc;
+        G.at(0, row) = G.at(0, row) + inc;
     } else if (G.kind == MIND_MECH_EXP2SYN) {
-        if (MIXED) {
-            const float wf = (float)inc;
-            G.fat(0, row) = G.fat(0, row) + wf;
-            G.fat(1, row) = G.fat(1, row) + wf;
-        } else {
-            G.at(0, row) = G.at(0, row) + inc;
-            G.at(1, row) = G.at(1, row) + inc;
-        }
+        G.at(0, row) = G.at(0, row) + inc;
+        G.at(1, row) = G.at(1, row) + inc;
     }
 }
 
@@ -458,17 +449,10 @@ __global__ void __launch_bounds__(kCellThreads, 8) window_kernel(const Params P,
             sg[g].r0 = r0;
             sg[g].f = dp;
         }
-        if (staged) dp += (size_t)staged_doubles(G.kind, MIXED) * rows;
+        if (staged) dp += (size_t)staged_doubles(G.kind) * rows;
     }
     InboxEvent *sev = reinterpret_cast<InboxEvent *>(dp);
-    float *fp = reinterpret_cast<float *>(sev + P.inbox_cap);
-    for (int32_t g = 0; g < P.ngroups; ++g) {
-        const DevGroup &G = P.groups[g];
-        const int32_t rows = kind_staged(G.kind) ? G.row_off[c + 1] - G.row_off[c] : 0;
-        if (tid == 0) sg[g].s = fp;
-        fp += (size_t)staged_floats(G.kind, MIXED) * rows;
-    }
-    int32_t *ip = reinterpret_cast<int32_t *>(fp);
+    int32_t *ip = reinterpret_cast<int32_t *>(sev + P.inbox_cap);
     for (int32_t g = 0; g < P.ngroups; ++g) {
         const DevGroup &G = P.groups[g];
         const int32_t rows = kind_staged(G.kind) ? G.row_off[c + 1] - G.row_off[c] : 0;
@@ -533,26 +517,13 @@ __global__ void __launch_bounds__(kCellThreads, 8) window_kernel(const Params P,
             switch (S.kind) {
                 case MIND_MECH_HH:
                     for (int k = 0; k < HH_NSLOT; ++k) S.at(k, r) = G.f[k][row];
-                    if (MIXED) {
-                        S.fat(0, r) = G.s[HHS_M][row];
-                        S.fat(1, r) = G.s[HHS_H][row];
-                        S.fat(2, r) = G.s[HHS_N][row];
-                    }
                     break;
                 case MIND_MECH_EXPSYN:
-                    if (MIXED)
-                        S.fat(0, r) = G.s[ESS_G][row];
-                    else
-                        S.at(0, r) = G.f[ES_G][row];
+                    S.at(0, r) = G.f[ES_G][row];
                     break;
                 case MIND_MECH_EXP2SYN:
-                    if (MIXED) {
-                        S.fat(0, r) = G.s[E2S_A][row];
-                        S.fat(1, r) = G.s[E2S_B][row];
-                    } else {
-                        S.at(0, r) = G.f[E2_A][row];
-                        S.at(1, r) = G.f[E2_B][row];
-                    }
+                    S.at(0, r) = G.f[E2_A][row];
+                    S.at(1, r) = G.f[E2_B][row];
                     break;
             }
             S.node[r] = (int32_t)(G.node[row] - nb);
@@ -624,7 +595,7 @@ __global__ void __launch_bounds__(kCellThreads, 8) window_kernel(const Params P,
                 const InboxEvent &e = sev[k];
                 if (e.bin > step) break;
                 if (e.bin < step) raise_error(P.error, MIND_ESELFEVENT);
-                apply_event<MIXED>(sg[e.point >> 24], e.point & 0xffffff, sw[k]);
+                apply_event(sg[e.point >> 24], e.point & 0xffffff, sw[k]);
                 ++cursor;
             }
         }
@@ -675,16 +646,7 @@ __global__ void __launch_bounds__(kCellThreads, 8) window_kernel(const Params P,
                     const int32_t node = G.node[r];
                     const double vv = sv[node];
                     const double probe = vv + 0.001;
-                    double m, h, nn;
-                    if (MIXED) {
-                        m = (double)G.fat(0, r);
-                        h = (double)G.fat(1, r);
-                        nn = (double)G.fat(2, r);
-                    } else {
-                        m = G.at(HH_M, r);
-                        h = G.at(HH_H, r);
-                        nn = G.at(HH_N, r);
-                    }
+                    const double m = G.at(HH_M, r), h = G.at(HH_H, r), nn = G.at(HH_N, r);
                     const double shifted = hh_current(probe, m, h, nn, G.at(HH_GNABAR, r), G.at(HH_GKBAR, r),
                                                       G.at(HH_GL, r), G.at(HH_EL, r), G.at(HH_ENA, r), G.at(HH_EK, r));
                     const double value = hh_current(vv, m, h, nn, G.at(HH_GNABAR, r), G.at(HH_GKBAR, r),
@@ -701,9 +663,9 @@ __global__ void __launch_bounds__(kCellThreads, 8) window_kernel(const Params P,
                     const double e = __ldg(pe + r);
                     double gs;
                     if (two)
-                        gs = MIXED ? (double)(G.fat(1, r) - G.fat(0, r)) : G.at(1, r) - G.at(0, r);
+                        gs = G.at(1, r) - G.at(0, r);
                     else
-                        gs = MIXED ? (double)G.fat(0, r) : G.at(0, r);
+                        gs = G.at(0, r);
                     const double vv = sv[node];
                     const double probe = vv + 0.001;
                     const double shifted = 0.0 + gs * (probe - e);
@@ -850,17 +812,17 @@ __global__ void __launch_bounds__(kCellThreads, 8) window_kernel(const Params P,
             const StagedGroup G = sg[g];
             switch (G.kind) {
                 case MIND_MECH_HH:
+                    // one thread per (row, gate): m, h and n advance independently
                     if (MIXED) {
-                        for (int32_t r = tid; r < G.rows; r += T) {
-                            const double vv = sv[G.node[r]];
-                            float m = G.fat(0, r), h = G.fat(1, r), nn = G.fat(2, r);
-                            hh_advance_f32((float)vv, q10f, (float)P.dt, m, h, nn);
-                            G.fat(0, r) = m;
-                            G.fat(1, r) = h;
-                            G.fat(2, r) = nn;
+                        for (int32_t w = tid; w < 3 * G.rows; w += T) {
+                            const int32_t r = w / 3, gate = w - 3 * r;
+                            float inf, factor;
+                            hh_gate_f32(sv[G.node[r]], q10f, (float)P.dt, gate, inf, factor);
+                            const int slot = HH_M + gate;
+                            const double state = G.at(slot, r);
+                            G.at(slot, r) = state + (double)factor * ((double)inf - state);
                         }
                     } else {
-                        // one thread per (row, gate): m, h and n advance independently
                         for (int32_t w = tid; w < 3 * G.rows; w += T) {
                             const int32_t r = w / 3, gate = w - 3 * r;
                             const double vv = sv[G.node[r]];
@@ -876,8 +838,9 @@ __global__ void __launch_bounds__(kCellThreads, 8) window_kernel(const Params P,
                     const float *pdecf = GG.s[ESS_DECAY] + G.r0;
                     for (int32_t r = tid; r < G.rows; r += T) {
                         if (MIXED) {
-                            const float gs = G.fat(0, r);
-                            G.fat(0, r) = gs + pdecf[r] * (0.0f - gs);
+                            // FP32 decrement, FP64 accumulation
+                            const double gs = G.at(0, r);
+                            G.at(0, r) = gs + (double)(pdecf[r] * (0.0f - (float)gs));
                         } else {
                             const double gs = G.at(0, r);
                             G.at(0, r) = gs + pdec[r] * (0.0 - gs);
@@ -889,9 +852,10 @@ __global__ void __launch_bounds__(kCellThreads, 8) window_kernel(const Params P,
                     const float *pd1f = GG.s[E2S_DECAY1] + G.r0, *pd2f = GG.s[E2S_DECAY2] + G.r0;
                     for (int32_t r = tid; r < G.rows; r += T) {
                         if (MIXED) {
-                            const float A = G.fat(0, r), B = G.fat(1, r);
-                            G.fat(0, r) = A + pd1f[r] * (0.0f - A);
-                            G.fat(1, r) = B + pd2f[r] * (0.0f - B);
+                            // FP32 decrements, FP64 accumulation
+                            const double A = G.at(0, r), B = G.at(1, r);
+                            G.at(0, r) = A + (double)(pd1f[r] * (0.0f - (float)A));
+                            G.at(1, r) = B + (double)(pd2f[r] * (0.0f - (float)B));
                         } else {
                             const double A = G.at(0, r), B = G.at(1, r);
                             G.at(0, r) = A + pd1[r] * (0.0 - A);
@@ -924,30 +888,16 @@ __global__ void __launch_bounds__(kCellThreads, 8) window_kernel(const Params P,
             const int32_t row = S.r0 + r;
             switch (S.kind) {
                 case MIND_MECH_HH:
-                    if (MIXED) {
-                        G.s[HHS_M][row] = S.fat(0, r);
-                        G.s[HHS_H][row] = S.fat(1, r);
-                        G.s[HHS_N][row] = S.fat(2, r);
-                    } else {
-                        G.f[HH_M][row] = S.at(HH_M, r);
-                        G.f[HH_H][row] = S.at(HH_H, r);
-                        G.f[HH_N][row] = S.at(HH_N, r);
-                    }
+                    G.f[HH_M][row] = S.at(HH_M, r);
+                    G.f[HH_H][row] = S.at(HH_H, r);
+                    G.f[HH_N][row] = S.at(HH_N, r);
                     break;
                 case MIND_MECH_EXPSYN:
-                    if (MIXED)
-                        G.s[ESS_G][row] = S.fat(0, r);
-                    else
-                        G.f[ES_G][row] = S.at(0, r);
+                    G.f[ES_G][row] = S.at(0, r);
                     break;
                 case MIND_MECH_EXP2SYN:
-                    if (MIXED) {
-                        G.s[E2S_A][row] = S.fat(0, r);
-                        G.s[E2S_B][row] = S.fat(1, r);
-                    } else {
-                        G.f[E2_A][row] = S.at(0, r);
-                        G.f[E2_B][row] = S.at(1, r);
-                    }
+                    G.f[E2_A][row] = S.at(0, r);
+                    G.f[E2_B][row] = S.at(1, r);
                     break;
             }
         }

@@ -173,13 +173,13 @@ struct KindSpec {
 KindSpec spec_of(int32_t kind) {
     switch (kind) {
         case MIND_MECH_HH:
-            return {kind, {"gnabar", "gkbar", "gl", "el", "ena", "ek"}, HH_NSLOT, 3};
+            return {kind, {"gnabar", "gkbar", "gl", "el", "ena", "ek"}, HH_NSLOT, 0};
         case MIND_MECH_PAS:
             return {kind, {"g", "e"}, PAS_NSLOT, 0};
         case MIND_MECH_EXPSYN:
-            return {kind, {"e", "g", "tau"}, ES_NSLOT, 2};
+            return {kind, {"e", "g", "tau"}, ES_NSLOT, 1};
         case MIND_MECH_EXP2SYN:
-            return {kind, {"e", "A", "B", "factor", "tau1", "tau2"}, E2_NSLOT, 4};
+            return {kind, {"e", "A", "B", "factor", "tau1", "tau2"}, E2_NSLOT, 2};
         case MIND_MECH_ICLAMP:
             return {kind, {"del", "dur", "amp"}, IC_NSLOT, 0};
         case MIND_MECH_NETSTIM:
@@ -623,7 +623,7 @@ int create(const MindLayout *L, MindHandle *h) {
         for (int32_t c = 0; c < ncells; ++c) group_row_off[g][c + 1] += group_row_off[g][c];
     }
     std::vector<std::pair<size_t, int32_t>> need(ncells);
-    size_t worst[2] = {0, 0};
+    size_t worst_any = 0;
     for (int32_t c = 0; c < ncells; ++c) {
         CellShape shape{};
         shape.n = (int32_t)(node_off[c + 1] - node_off[c]);
@@ -631,13 +631,10 @@ int create(const MindLayout *L, MindHandle *h) {
         shape.nkids = chain_kid_off[chain_off[c + 1]] - chain_kid_off[chain_off[c]];
         shape.nlev = level_off[c + 1] - level_off[c] - 1;
         for (int32_t g = 0; g < L->n_mechanisms; ++g) shape.rows[g] = group_row_off[g][c + 1] - group_row_off[g][c];
-        size_t b64 = cell_smem_bytes(shape, kinds.data(), L->n_mechanisms, false, P.inbox_cap);
-        size_t b32 = cell_smem_bytes(shape, kinds.data(), L->n_mechanisms, true, P.inbox_cap);
-        need[c] = {std::max(b64, b32), c};
-        worst[0] = std::max(worst[0], b64);
-        worst[1] = std::max(worst[1], b32);
+        const size_t bytes = cell_smem_bytes(shape, kinds.data(), L->n_mechanisms, P.inbox_cap);
+        need[c] = {bytes, c};
+        worst_any = std::max(worst_any, bytes);
     }
-    const size_t worst_any = std::max(worst[0], worst[1]);
     if (worst_any > 227 * 1024)
         return fail(h, MIND_ELAYOUT, "a cell needs more shared memory than one CTA has (" +
                                          std::to_string(worst_any) + " bytes)");
