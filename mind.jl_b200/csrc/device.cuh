@@ -9,8 +9,9 @@
  *     nodes contiguous from top to bottom.  A cell is staged in shared memory
  *     once per window of steps.
  *   - Mechanism rows are structure-of-arrays per group, sorted by
- *     (cell, local node, layout row) so a cell owns one contiguous row range
- *     per group and rows on one node are adjacent (a "segment").
+ *     (cell, owner thread = local node mod 64, local node, layout row): a cell
+ *     owns one contiguous row range per group, each thread of its CTA one
+ *     sub-range, and rows on one node are adjacent (a "segment").
  *   - Events live in a ring of delivery bins (bin m = the events NEURON's two
  *     half-step deliveries hand to step m's currents, i.e. event times in
  *     ((m-1) dt + dt/2, m dt + dt/2]).  Before a window, the bins of the
@@ -156,9 +157,8 @@ struct Params {
     const int32_t *level_chain;  // per cell: nlevels+1 local chain starts (chains sorted by level)
     DevGroup groups[kMaxGroups];
     // per cell, group and thread: first row (relative to the cell's first row of the group)
-    // whose node lies in the thread's contiguous node range (node_part)
+    // of the thread's rows; thread t owns the local nodes i with i % kCellThreads == t
     const int32_t *part;       // [ncells][ngroups][kCellThreads + 1]
-    const int32_t *node_part;  // [ncells][kCellThreads + 1]: thread t owns local nodes [node_part[t], node_part[t+1])
     // detectors
     const int32_t *det_off;    // [ncells+1]
     const int32_t *det_node;   // local node

@@ -566,7 +566,6 @@ __global__ void __launch_bounds__(kCellThreads, 8) window_kernel(const Params P,
 
     const double q10 = mind_pow(3.0, (P.celsius - 6.3) / 10.0);
     const float q10f = (float)q10;
-    const int32_t nlo = P.node_part[(int64_t)c * (T + 1) + tid], nhi = P.node_part[(int64_t)c * (T + 1) + tid + 1];
     int32_t cursor = 0;
     bool singular = false;
 
@@ -601,12 +600,14 @@ __global__ void __launch_bounds__(kCellThreads, 8) window_kernel(const Params P,
         }
         __syncthreads();  // NET_RECEIVE above wrote staged synapse state
 
-        // 3-5. Each thread owns the contiguous nodes [nlo, nhi) and the rows of every group
-        //      on them (rows are sorted by node), so the mechanism sums of a node are
-        //      accumulated in group order, rows in row order, by one thread, and its
-        //      assembly follows without a barrier (it reads only the unchanged v of
-        //      neighbours).  Parameters are streamed from HBM through the read-only path.
-        for (int32_t i = nlo; i < nhi; ++i) {
+        // 3-5. Thread t owns the nodes i with i % T == t (a warp's lanes touch consecutive
+        //      nodes, so shared memory serves them without bank conflicts) and the rows of
+        //      every group on them, which the device row order keeps as one range per
+        //      thread.  The mechanism sums of a node are accumulated in group order, rows in
+        //      row order, by one thread, and its assembly follows without a barrier (it reads
+        //      only the unchanged v of neighbours).  Parameters are streamed from HBM through
+        //      the read-only path.
+        for (int32_t i = tid; i < n; i += T) {
             sd[i] = 0.0;
             sr[i] = 0.0;
         }
@@ -676,7 +677,7 @@ __global__ void __launch_bounds__(kCellThreads, 8) window_kernel(const Params P,
             }
         }
         // Cable assembly of the owned nodes: d = C/dt + d + axial_diagonal; own axial term, then children.
-        for (int32_t i = nlo; i < nhi; ++i) {
+        for (int32_t i = tid; i < n; i += T) {
             const int64_t gi = nb + i;
             const double cdt = __ldg(P.cdt + gi), adi = __ldg(P.ad + gi);
             const int32_t k = chain_of[i];

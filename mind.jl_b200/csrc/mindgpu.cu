@@ -356,32 +356,11 @@ int create(const MindLayout *L, MindHandle *h) {
     P.seed = L->seed;
     P.ns_group = -1;
     std::vector<std::vector<int32_t>> dev_row_of(L->n_mechanisms);  // layout row -> device row
+    // Thread t of a cell's CTA owns the local nodes i with i % kCellThreads == t, so that the
+    // threads of a warp touch consecutive nodes (distinct shared-memory banks).  Each
+    // group's rows are sorted by (cell, owner thread, node, layout row): a thread's rows are
+    // one range, and rows of one node stay in layout order.
     std::vector<int32_t> part((size_t)ncells * L->n_mechanisms * (kCellThreads + 1), 0);
-    // Thread node ranges: contiguous, cut where the prefix of estimated per-node work (the
-    // node's assembly plus its mechanism rows, hh weighing most) crosses t/threads of the cell's.
-    std::vector<double> work(n, 1.0);
-    for (int32_t g = 0; g < L->n_mechanisms; ++g) {
-        const MindMechanism &m = L->mechanisms[g];
-        if (m.kind == MIND_MECH_NETSTIM) continue;
-        const double w = m.kind == MIND_MECH_HH ? 4.0 : m.kind == MIND_MECH_ICLAMP ? 1.0 : 1.4;
-        for (int64_t r = 0; r < m.rows; ++r)
-            if (m.nodes[r] >= 1 && m.nodes[r] <= n) work[h->packed_of_layout[m.nodes[r] - 1]] += w;
-    }
-    std::vector<int32_t> node_part((size_t)ncells * (kCellThreads + 1), 0);
-    for (int32_t c = 0; c < ncells; ++c) {
-        const int64_t b = node_off[c], nc = node_off[c + 1] - b;
-        double total = 0.0;
-        for (int64_t i = 0; i < nc; ++i) total += work[b + i];
-        int32_t *np = node_part.data() + (size_t)c * (kCellThreads + 1);
-        double acc = 0.0;
-        int64_t i = 0;
-        for (int32_t t = 0; t < kCellThreads; ++t) {
-            np[t] = (int32_t)i;
-            const double goal = total * (t + 1) / kCellThreads;
-            while (i < nc && acc + 0.5 * work[b + i] < goal) acc += work[b + i++];
-        }
-        np[kCellThreads] = (int32_t)nc;
-    }
     std::vector<std::vector<int32_t>> row_cell(L->n_mechanisms);
     for (int32_t g = 0; g < L->n_mechanisms; ++g) {
         const MindMechanism &m = L->mechanisms[g];
@@ -400,21 +379,26 @@ int create(const MindLayout *L, MindHandle *h) {
             if (P.ns_group >= 0) return fail(h, MIND_ELAYOUT, "more than one NetStim group");
             P.ns_group = g;
         }
-        // sort rows by (cell, local node, layout row)
-        std::vector<int64_t> key(rows);
+        // sort rows by (cell, owner thread, local node, layout row)
+        std::vector<int64_t> key(rows), order_key(rows);
         for (int32_t r = 0; r < rows; ++r) {
             int32_t node = m.nodes[r];
             if (artificial) {
                 if (node != 0) return fail(h, MIND_ELAYOUT, "artificial cell with a node");
                 key[r] = r;
+                order_key[r] = r;
             } else {
                 if (node < 1 || node > n) return fail(h, MIND_ELAYOUT, "mechanism node out of range");
                 key[r] = h->packed_of_layout[node - 1];
+                const int32_t cell = cell_of[node - 1];
+                const int64_t local = key[r] - node_off[cell];
+                const int64_t per_thread = (node_off[cell + 1] - node_off[cell] + kCellThreads - 1) / kCellThreads;
+                order_key[r] = ((int64_t)cell << 32) | ((local % kCellThreads) * per_thread + local / kCellThreads);
             }
         }
         std::vector<int32_t> perm(rows);
         for (int32_t r = 0; r < rows; ++r) perm[r] = r;
-        std::stable_sort(perm.begin(), perm.end(), [&](int32_t x, int32_t y) { return key[x] < key[y]; });
+        std::stable_sort(perm.begin(), perm.end(), [&](int32_t x, int32_t y) { return order_key[x] < order_key[y]; });
         dev_row_of[g].assign(rows, 0);
         for (int32_t r = 0; r < rows; ++r) dev_row_of[g][perm[r]] = r;
         MindHandle::GroupInit init;
@@ -451,15 +435,12 @@ int create(const MindLayout *L, MindHandle *h) {
             }
             for (int32_t r = 0; r < rows; ++r) row_off[row_cell[g][r] + 1]++;
             for (int32_t c = 0; c < ncells; ++c) row_off[c + 1] += row_off[c];
-            // thread partition: rows of a cell are sorted by node, so each thread's rows are a range
+            // thread t's rows: the range after the rows of the owners before it
             for (int32_t c = 0; c < ncells; ++c) {
                 int32_t *pc = part.data() + ((size_t)c * L->n_mechanisms + g) * (kCellThreads + 1);
-                int32_t r = row_off[c];
-                for (int32_t t = 0; t <= kCellThreads; ++t) {
-                    const int64_t first_node = node_off[c] + node_part[(size_t)c * (kCellThreads + 1) + t];
-                    while (r < row_off[c + 1] && node_dev[r] < first_node) ++r;
-                    pc[t] = r - row_off[c];
-                }
+                for (int32_t r = row_off[c]; r < row_off[c + 1]; ++r)
+                    pc[(node_dev[r] - node_off[c]) % kCellThreads + 1]++;
+                for (int32_t t = 0; t < kCellThreads; ++t) pc[t + 1] += pc[t];
             }
         }
         if (artificial) {
@@ -570,7 +551,6 @@ int create(const MindLayout *L, MindHandle *h) {
     P.level_off = h->upload(level_off);
     P.level_chain = h->upload(level_chain);
     P.part = h->upload(part);
-    P.node_part = h->upload(node_part);
     P.det_off = h->upload(det_off);
     P.det_node = h->upload(det_node);
     P.det_source = h->upload(det_source);
