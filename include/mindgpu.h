@@ -15,6 +15,7 @@
  *   mind_get_spikes   SimulationResult.spike_times/_sources    src/runtime/recording.jl:256-295
  *   mind_read_voltage read_value(voltage_ref)                  src/runtime/state.jl:586-659
  *   mind_inject_event inject_event!(state, connection, time)   src/runtime/state.jl:586-659
+ *   mind_inject_spikes inject_spike!(state, source, time)      src/runtime/state.jl:637-659
  *   mind_destroy      release of SimulationState               src/runtime/state.jl:177-212
  *
  * Conventions follow the Julia side so that its arrays pass without copies:
@@ -178,6 +179,22 @@ int mind_read_voltage(const MindHandle *h, int32_t node, double *value);
 
 /* inject_event!: deliver connection `edge` (1-based) at absolute time t (ms, >= now). */
 int mind_inject_event(MindHandle *h, int64_t edge, double t);
+
+/* inject_spike! for n spikes: each external spike input sources[k] (a 1-based source with
+ * neither a detector node nor a point, created by register_spike_source!(model; sid))
+ * fires at absolute time times[k] (ms).  Every outgoing NetCon delivers at times[k] + its
+ * delay.  A spike at or after the current time also enters the raster of the run that
+ * reaches it.  A spike before the current time (one that a cell simulated elsewhere, on
+ * another GPU, fired during the last window) is accepted when each of its NetCons still
+ * delivers at or after the current step; it is routed but not recorded here.  Returns
+ * MIND_EARG, with nothing queued, for any other source or a delivery in the past. */
+int mind_inject_spikes(MindHandle *h, int64_t n, const int64_t *sources, const double *times);
+
+/* Steps per device window: the largest step count a run advances without routing cell
+ * spikes, set by the shortest NetCon delay out of cell detectors and external inputs.
+ * A host that exchanges spikes with other handles runs at most this many steps between
+ * exchanges (no reference counterpart: the reference routes every step on the host). */
+int mind_window_steps(const MindHandle *h, int32_t *steps);
 
 /* Message for the last non-zero status of this handle (or of mind_create when h is NULL). */
 const char *mind_last_error(const MindHandle *h);

@@ -45,6 +45,11 @@ struct RingEvent {       // an event waiting in a delivery bin
     int32_t point;       // 0-based point
 };
 
+struct InjectedEvent {
+    double time;
+    int32_t edge;   // 0-based edge, or -1 for the raster entry of an external spike input
+    int32_t point;  // 0-based target point, or the 0-based source for a raster entry
+};
 struct InboxEvent {      // an event moved to its cell's window inbox
     double time;
     int32_t edge;

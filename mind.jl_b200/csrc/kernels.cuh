@@ -915,8 +915,16 @@ __global__ void finite_kernel(const double *values, int64_t count, int32_t *erro
         if (!isfinite(values[i])) atomicCAS(error, 0, MIND_ENONFINITE);
 }
 
-__global__ void inject_kernel(const Params P, double time, int32_t edge, int32_t point, int64_t min_bin) {
-    ring_insert(P, time, edge, point, min_bin);
+/* Host-injected events of one window: NetCon events into the ring, and the raster
+ * entries of external spike inputs (edge < 0, point = 0-based source). */
+__global__ void inject_kernel(const Params P, const InjectedEvent *events, int32_t n, int64_t min_bin) {
+    for (int32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const InjectedEvent e = events[k];
+        if (e.edge >= 0)
+            ring_insert(P, e.time, e.edge, e.point, min_bin);
+        else
+            record_spike(P, e.point, e.time);
+    }
 }
 
 }  // namespace mind

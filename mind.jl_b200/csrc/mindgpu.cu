@@ -55,10 +55,18 @@ struct MindHandle {
     std::vector<int32_t> edge_target;        // 0-based point per edge
     struct Injected {
         int64_t bin;
-        double time;
-        int32_t edge, point;
+        InjectedEvent event;                 // edge < 0: the raster entry of external source `point`
     };
-    std::vector<Injected> injected;          // inject_event! beyond the ring's horizon, by bin
+    // Events from inject_event!/inject_spike! wait on the host until the window that
+    // delivers them (the ring holds one window plus the longest delay); appended in
+    // call order and stably sorted by bin before a window drains them.
+    std::vector<Injected> injected;
+    bool injected_sorted = true;
+    InjectedEvent *inject_dev = nullptr;     // staging for one window's due events
+    size_t inject_cap = 0;
+    std::vector<int64_t> fanout;             // [n_sources+1] 0-based edge ranges
+    std::vector<double> edge_delay;
+    std::vector<uint8_t> source_external;    // no detector and no point: an inject_spike! input
     std::vector<double> v0_packed;
     int64_t n_sources = 0;
     std::vector<int64_t> source_ids;
@@ -523,7 +531,9 @@ int create(const MindLayout *L, MindHandle *h) {
                 return fail(h, MIND_ELAYOUT, "invalid NetCon delay or weight");
             edge_target[e] = t - 1;
             max_delay = std::max(max_delay, d);
-            if (L->source_nodes[s] > 0) min_cell_delay = std::min(min_cell_delay, d);
+            // cell detectors and external inputs bound the window (their spikes are routed
+            // between windows); point sources (NetStim) are planned ahead on the device
+            if (L->source_nodes[s] > 0 || L->source_points[s] == 0) min_cell_delay = std::min(min_cell_delay, d);
         }
     }
     // Window: a spike detected at step s arrives in bin >= s + floor((d - dt/2)/dt); keep one bin margin.
@@ -534,6 +544,11 @@ int create(const MindLayout *L, MindHandle *h) {
     }
     h->window = window;
     h->edge_target = edge_target;
+    h->fanout = fanout;
+    h->edge_delay = edge_delay;
+    h->source_external.assign(L->n_sources, 0);
+    for (int64_t s = 0; s < L->n_sources; ++s)
+        h->source_external[s] = L->source_nodes[s] == 0 && L->source_points[s] == 0;
     h->max_delay_bins = (int32_t)std::ceil(max_delay / L->dt) + 2;
 
     // ---- device arrays ----
@@ -755,12 +770,26 @@ int advance(MindHandle *h, int64_t steps, bool record_spikes) {
             netstim_kernel<<<ns_blocks, kThreads, 0, h->stream>>>(P, horizon, n0);
             ++st.launches;
         }
-        // Injected events whose bin falls in this window enter the ring now.
-        while (!h->injected.empty() && h->injected.front().bin < n0 + W) {
-            const auto &e = h->injected.front();
-            inject_kernel<<<1, 1, 0, h->stream>>>(P, e.time, e.edge, e.point, n0);
-            ++st.launches;
-            h->injected.erase(h->injected.begin());
+        // Injected events whose bin falls in this window enter the ring now, in one launch
+        // (the staging buffer was sized when they were injected).
+        if (!h->injected.empty()) {
+            if (!h->injected_sorted) {
+                std::stable_sort(h->injected.begin(), h->injected.end(),
+                                 [](const MindHandle::Injected &x, const MindHandle::Injected &y) { return x.bin < y.bin; });
+                h->injected_sorted = true;
+            }
+            size_t due = 0;
+            while (due < h->injected.size() && h->injected[due].bin < n0 + W) ++due;
+            if (due > 0) {
+                std::vector<InjectedEvent> batch(due);
+                for (size_t k = 0; k < due; ++k) batch[k] = h->injected[k].event;
+                cudaMemcpyAsync(h->inject_dev, batch.data(), due * sizeof(InjectedEvent), cudaMemcpyHostToDevice,
+                                h->stream);
+                inject_kernel<<<(unsigned)((due + kThreads - 1) / kThreads), kThreads, 0, h->stream>>>(
+                    P, h->inject_dev, (int32_t)due, n0);
+                ++st.launches;
+                h->injected.erase(h->injected.begin(), h->injected.begin() + due);
+            }
         }
         bucket_kernel<<<dim3(64, W), kThreads, 0, h->stream>>>(P, n0);
         ++st.launches;
@@ -879,6 +908,7 @@ int mind_initialize(MindHandle *h) {
     h->initialized = false;
     h->step = 0;
     h->injected.clear();
+    h->injected_sorted = true;
     CUDA_TRY(h, cudaMemcpyAsync(P.v, h->v0_packed.data(), h->n_nodes * sizeof(double), cudaMemcpyHostToDevice,
                                 h->stream));
     CUDA_TRY(h, cudaMemsetAsync(P.error, 0, sizeof(int32_t), h->stream));
@@ -959,18 +989,74 @@ int mind_read_voltage(const MindHandle *h, int32_t node, double *value) {
     return e == cudaSuccess ? MIND_OK : MIND_ECUDA;
 }
 
+namespace {
+
+/* Grows the staging buffer so that every pending injected event fits one window's batch;
+ * allocation happens here, at injection, never inside a run. */
+int reserve_injected(MindHandle *h) {
+    if (h->injected.size() <= h->inject_cap) return MIND_OK;
+    const size_t cap = std::max<size_t>(h->injected.size(), std::max<size_t>(1024, 2 * h->inject_cap));
+    void *p = nullptr;
+    CUDA_TRY(h, cudaMalloc(&p, cap * sizeof(InjectedEvent)));
+    if (h->inject_dev) {
+        cudaStreamSynchronize(h->stream);
+        h->release(h->inject_dev);
+    }
+    h->buffers.owned.push_back(p);
+    h->inject_dev = static_cast<InjectedEvent *>(p);
+    h->inject_cap = cap;
+    return MIND_OK;
+}
+
+void push_injected(MindHandle *h, double time, int32_t edge, int32_t point) {
+    MindHandle::Injected e;
+    e.bin = delivery_bin(time, h->dt);
+    e.event.time = time;
+    e.event.edge = edge;
+    e.event.point = point;
+    if (!h->injected.empty() && h->injected.back().bin > e.bin) h->injected_sorted = false;
+    h->injected.push_back(e);
+}
+
+}  // namespace
+
 int mind_inject_event(MindHandle *h, int64_t edge, double t) {
     if (!h) return MIND_EARG;
     if (!h->initialized) return fail(h, MIND_EARG, "simulation is not initialized");
-    const Params &P = h->P;
     if (edge < 1 || edge > (int64_t)h->edge_target.size()) return fail(h, MIND_EARG, "edge index out of range");
     if (!(t >= (double)h->step * h->dt) || !std::isfinite(t)) return fail(h, MIND_EARG, "event time is in the past");
-    // The ring holds bins up to one window plus the longest delay ahead; the event
-    // waits on the host until the window that delivers it.
-    MindHandle::Injected e{delivery_bin(t, h->dt), t, (int32_t)(edge - 1), h->edge_target[edge - 1]};
-    auto at = std::upper_bound(h->injected.begin(), h->injected.end(), e,
-                               [](const MindHandle::Injected &x, const MindHandle::Injected &y) { return x.bin < y.bin; });
-    h->injected.insert(at, e);
+    push_injected(h, t, (int32_t)(edge - 1), h->edge_target[edge - 1]);
+    return reserve_injected(h);
+}
+
+int mind_inject_spikes(MindHandle *h, int64_t n, const int64_t *sources, const double *times) {
+    if (!h) return MIND_EARG;
+    if (!h->initialized) return fail(h, MIND_EARG, "simulation is not initialized");
+    if (n < 0 || (n > 0 && (!sources || !times))) return fail(h, MIND_EARG, "invalid spike list");
+    const double now = (double)h->step * h->dt;
+    for (int64_t k = 0; k < n; ++k) {
+        const int64_t s = sources[k];
+        if (s < 1 || s > h->n_sources || !h->source_external[s - 1])
+            return fail(h, MIND_EARG, "source " + std::to_string(s) + " is not an external spike input");
+        if (!std::isfinite(times[k])) return fail(h, MIND_EARG, "spike time is not finite");
+        if (times[k] < now)
+            for (int64_t e = h->fanout[s - 1]; e < h->fanout[s]; ++e)
+                if (delivery_bin(times[k] + h->edge_delay[e], h->dt) < h->step)
+                    return fail(h, MIND_EARG, "spike time precedes the current time by more than its NetCon delays");
+    }
+    for (int64_t k = 0; k < n; ++k) {
+        const int64_t s = sources[k] - 1;
+        const double t = times[k];
+        if (t >= now) push_injected(h, t, -1, (int32_t)s);  // the raster entry, in the window of its time
+        for (int64_t e = h->fanout[s]; e < h->fanout[s + 1]; ++e)
+            push_injected(h, t + h->edge_delay[e], (int32_t)e, h->edge_target[e]);
+    }
+    return reserve_injected(h);
+}
+
+int mind_window_steps(const MindHandle *h, int32_t *steps) {
+    if (!h || !steps) return MIND_EARG;
+    *steps = h->window;
     return MIND_OK;
 }
 

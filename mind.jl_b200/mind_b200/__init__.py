@@ -11,7 +11,7 @@ from .model import (Cell, IonSpecies, MicroModel, PointProcess, Population, Spik
                     add_pointprocess, add_pointprocesses, add_population, connect, connect_many,
                     insert, register_point_sources, register_spike_source, spike_source)
 from .layout import Layout, build
-from .runtime import (RecordSpec, SimulationResult, initialize, run, simulation_time, step,
+from .runtime import (RecordSpec, SimulationResult, initialize, inject_spike, run, simulation_time, step,
                       voltage_record)
 
 __all__ = [
@@ -19,6 +19,6 @@ __all__ = [
     "IonSpecies", "MicroModel", "PointProcess", "Population", "SpikeSource", "add_pointprocess",
     "add_pointprocesses", "add_population", "connect", "connect_many", "insert",
     "register_point_sources", "register_spike_source", "spike_source", "Layout", "build",
-    "RecordSpec", "SimulationResult", "initialize", "run", "simulation_time", "step",
+    "RecordSpec", "SimulationResult", "initialize", "inject_spike", "run", "simulation_time", "step",
     "voltage_record",
 ]

@@ -148,10 +148,12 @@ def load_library():
     lib.mind_run_stats.argtypes = [handle, POINTER(MindRunStats)]
     lib.mind_set_profiling.argtypes = [handle, c_int32]
     lib.mind_run_noalloc.argtypes = [handle, c_int64, POINTER(MindRecord), c_int32, POINTER(c_double)]
+    lib.mind_inject_spikes.argtypes = [handle, c_int64, POINTER(c_int64), POINTER(c_double)]
+    lib.mind_window_steps.argtypes = [handle, POINTER(c_int32)]
     for name in ("mind_create", "mind_initialize", "mind_set_precision", "mind_run", "mind_step",
                  "mind_time", "mind_get_trace", "mind_get_spikes", "mind_read_voltage",
                  "mind_inject_event", "mind_last_run_ms", "mind_destroy", "mind_run_stats",
-                 "mind_set_profiling", "mind_run_noalloc"):
+                 "mind_set_profiling", "mind_run_noalloc", "mind_inject_spikes", "mind_window_steps"):
         getattr(lib, name).restype = c_int32
     _LIB = lib
     return lib
@@ -161,7 +163,7 @@ EXPORTED_SYMBOLS = (
     "mind_create", "mind_initialize", "mind_set_precision", "mind_run", "mind_step", "mind_time",
     "mind_get_trace", "mind_get_spikes", "mind_read_voltage", "mind_inject_event",
     "mind_last_error", "mind_last_run_ms", "mind_destroy", "mind_run_stats", "mind_set_profiling",
-    "mind_run_noalloc",
+    "mind_run_noalloc", "mind_inject_spikes", "mind_window_steps",
 )
 
 MIND_NOALLOC_SCRATCH_BYTES = 16 << 20

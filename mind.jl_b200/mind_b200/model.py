@@ -280,13 +280,19 @@ def _new_sid(model: MicroModel, sid: Optional[int]) -> int:
     return identity
 
 
-def register_spike_source(source: Union[Cell, PointProcess], *, sid: Optional[int] = None,
+def register_spike_source(source: Union[Cell, PointProcess, "MicroModel"], *, sid: Optional[int] = None,
                           section="soma", x=0.5, threshold: Optional[float] = None) -> SpikeSource:
-    """Register a cell's voltage detector or a point process's net_event output.
+    """Register a cell's voltage detector, a point process's net_event output, or (given the
+    model itself) an external spike input that only `inject_spike` drives.
 
     Defaults follow micro/model.jl:286-371: detectors at soma(0.5) with threshold
     10 mV; a point source reuses one registration for all its connections.
     """
+    if isinstance(source, MicroModel):
+        identity = _new_sid(source, sid)
+        index = _append_sources(source, np.array([identity]), np.array([0]), "none", np.array([0.0]),
+                                np.array([0]), np.array([0.0]))
+        return SpikeSource(source, index, identity)
     if isinstance(source, PointProcess):
         model = source.model
         existing = model.point_sources.get(source.index)

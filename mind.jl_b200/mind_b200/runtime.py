@@ -113,6 +113,21 @@ class DeviceState:
         edge = int(self.layout.connection_edges[connection - 1])
         abi.check(self.lib, self.handle, self.lib.mind_inject_event(self.handle, edge, float(t)))
 
+    def inject_spikes(self, sources, times) -> None:
+        """inject_spike! for many spikes: 1-based external source indices and absolute times."""
+        sources = np.ascontiguousarray(sources, dtype=np.int64)
+        times = np.ascontiguousarray(times, dtype=np.float64)
+        if sources.shape != times.shape:
+            raise ValueError("sources and times differ in length")
+        abi.check(self.lib, self.handle, self.lib.mind_inject_spikes(
+            self.handle, sources.size, sources.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+            times.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+
+    def window_steps(self) -> int:
+        steps = ctypes.c_int32()
+        abi.check(self.lib, self.handle, self.lib.mind_window_steps(self.handle, ctypes.byref(steps)))
+        return steps.value
+
     def close(self) -> None:
         if getattr(self, "handle", None):
             self.lib.mind_destroy(self.handle)
@@ -161,6 +176,14 @@ def step(model):
     if model.state is None:
         raise ValueError("simulation is not initialized")
     model.state.step()
+    return model
+
+
+def inject_spike(model, source, t: float):
+    """inject_spike!(state, source, time) (src/runtime/state.jl:637-659): an external input fires at t."""
+    if model.state is None:
+        raise ValueError("simulation is not initialized")
+    model.state.inject_spikes([source.index], [float(t)])
     return model
 
 

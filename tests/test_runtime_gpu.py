@@ -93,6 +93,39 @@ def test_injected_event_equals_a_netstim_spike():
     assert np.max(np.abs(want - want[0])) > 1e-3
 
 
+def test_injected_spike_equals_a_netstim_spike():
+    """inject_spike!(external input, 4.0) through a 1 ms NetCon drives the synapse exactly like a
+    NetStim spike at 4.0 through the same NetCon, and enters the raster under its sid."""
+    def build(external):
+        model, cell = passive_cell()
+        syn = M.add_pointprocess(cell, mb.builtin("ExpSyn"), section="soma", x=0.5, params={"tau": 2.0})
+        stim = M.add_pointprocess(model, mb.builtin("NetStim"),
+                                  params={"interval": 10.0, "number": 0 if external else 1, "start": 4.0})
+        M.connect(stim, syn, weight=0.002, delay=1.0)
+        source = M.register_spike_source(model, sid=900) if external else None
+        if external:
+            M.connect(source, syn, weight=0.002, delay=1.0)
+        return model, source, mb.build(model)
+
+    model_a, _, layout_a = build(external=False)
+    model_b, source, layout_b = build(external=True)
+    rec = [mb.RecordSpec(layout_a.voltage_node(1), "v")]
+    mb.initialize(model_a)
+    want = mb.run(model_a, 20.0, records=rec)
+    mb.initialize(model_b)
+    mb.inject_spike(model_b, source, 4.0)
+    got = mb.run(model_b, 20.0, records=rec)
+    np.testing.assert_array_equal(got.traces["v"], want.traces["v"])
+    assert np.max(np.abs(want.traces["v"] - want.traces["v"][0])) > 1e-3
+    assert got.spike_sources.tolist() == [900] and got.spike_times.tolist() == [4.0]
+    # only external inputs accept injected spikes, and never in the past
+    with pytest.raises(abi.MindError) as info:
+        model_b.state.inject_spikes([1], [30.0])
+    assert info.value.status == abi.MIND_EARG
+    with pytest.raises(abi.MindError):
+        mb.inject_spike(model_b, source, 1.0)
+
+
 def test_step_matches_run_and_read_voltage():
     model = netcases.recurrent_trees(n_cells=6, synapses=8)
     layout = mb.build(model)
