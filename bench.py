@@ -10,9 +10,13 @@ synthetic network of mind_b200.networks.config2 (no dataset is involved).
 A step is one micro step of the whole network.  `value` is whole-job
 compartment-steps/s with all state resident in HBM; `e2e` is the same metric
 through the public run() call (C-ABI), including the host copies of the
-recorded soma voltages and the spike raster.  Under torchrun every rank
-simulates its own replica of the network (weak scaling; the path has no
-collective).  --impl reference times the CPU FP64 restatement of the
+recorded soma voltages and the spike raster.  Under torchrun (N GPUs) the
+config-2 network has 10,000 x N cells, each rank owning 10,000 of them (weak
+scaling): NetCons from cells on other ranks arrive as external spike inputs,
+and the ranks all-gather their cells' spikes over NCCL once per window
+(mind_b200.sharding); config 3 runs one network per rank.  Timing is CUDA
+events around the window loop, exchanges included, max over ranks.
+--impl reference times the CPU FP64 restatement of the
 reference's step loop (oracle/) on the host cores; MIND.jl itself is Julia
 and cannot run on this box.
 """
@@ -33,6 +37,7 @@ sys.path.insert(0, os.path.join(ROOT, "mind.jl_b200"))
 
 import numpy as np  # noqa: E402
 
+COLLECTIVE_DEVICE = "cuda"   # device of the tensors handed to torch.distributed
 METRIC = "compartment-steps/s (config 2: 10,000 uneven cells, recurrent Exp2Syn, dt 0.025 ms)"
 UNIT = "compartment-steps/s"
 
@@ -55,14 +60,16 @@ def parse():
     return p.parse_args()
 
 
-def build_network(cells, seed: int, config: int = 2):
+def build_network(cells, seed: int, config: int = 2, rank: int = 0, world: int = 1):
+    """Config 3 (one network per rank), or rank `rank`'s block of a config-2 network of
+    `cells` x `world` cells (world = 1: the whole 10,000-cell network)."""
     import mind_b200 as mb
     from mind_b200 import networks
 
     if config == 3:
         model = networks.config3(n_cells=cells or 1000)
     else:
-        model = networks.config2(n_cells=cells or 10000)
+        model = networks.config2(n_cells=cells or 10000, rank=rank, world=world)
     layout = mb.build(model, seed=seed)
     return model, layout
 
@@ -209,6 +216,59 @@ def mixed_accuracy(layout, fp64, mixed, warmup: int, steps: int) -> dict:
     }
 
 
+def device_timed(fn):
+    """fn() bracketed by CUDA events on the current stream (the library's calls are
+    synchronous), after a device synchronize and a barrier; returns (result, ms)."""
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.synchronize()
+    if dist.is_available() and dist.is_initialized():
+        dist.barrier()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    out = fn()
+    stop.record()
+    torch.cuda.synchronize()
+    return out, start.elapsed_time(stop)
+
+
+def measure_sharded(args, layout, rank: int, world: int, precision: str, local_rank: int):
+    """One config-2 network over `world` GPUs: this rank's cells, spikes exchanged per window
+    (mind_b200.sharding).  Timed on the device around the window loop, exchanges included;
+    the job figure uses the slowest rank."""
+    import mind_b200 as mb
+    from mind_b200 import replicas, sharding
+
+    run = sharding.ShardedRun(layout, rank, world, precision=precision, device=COLLECTIVE_DEVICE, local=True)
+    run.run_steps(args.warmup, (), False)
+    run.launches = 0
+    sampler = ClockSampler(local_rank)
+    with sampler:
+        result, ms = device_timed(lambda: run.run_steps(args.steps, (), True))
+    clocks = sampler.summary()
+    launches = run.launches
+    run_ms, units = replicas.reduce_timing(ms, layout.segment_count * args.steps, device=COLLECTIVE_DEVICE)
+    events = delivered_events(layout, result.spike_sources)
+    algo = algorithmic_bytes_per_step(layout, events / args.steps)
+    achieved = algo * args.steps / (result.device_ms / 1000.0) / 1e9 if result.device_ms > 0 else None
+    soma = run.records([layout.voltage_node(c) for c in range(1, layout.n_cells + 1)])
+    run.state.initialize()
+    run.run_steps(args.warmup, (), False)
+    e2e_result, e2e_ms = device_timed(lambda: run.run_steps(args.steps, soma, True))
+    e2e_ms, _ = replicas.reduce_timing(e2e_ms, 0.0, device=COLLECTIVE_DEVICE)
+    d2h = (len(soma) * 8 * (args.steps + 1) + 16 * len(e2e_result.spike_times)) / args.steps
+    run.close()
+    trace = np.stack([e2e_result.traces[r.name] for r in soma])
+    return ({"value": units / (run_ms / 1000.0), "ms_per_step": run_ms / args.steps,
+             "window_ms": result.device_ms, "window_launches": None, "launches": launches,
+             "window_steps": run.window, "bins": None, "algo_bytes_per_step": algo, "achieved_gbs": achieved,
+             "spikes": int(len(result.spike_times)), "delivered_events": events,
+             "e2e": units / (e2e_ms / 1000.0), "d2h": d2h, "h2d": 8 * len(soma) / args.steps,
+             "exchange": "all-gather of (sid, time) per window over NCCL"},
+            (trace, e2e_result.spike_sources, e2e_result.spike_times), clocks)
+
+
 def run_reference(args, rank: int):
     if rank != 0:
         return
@@ -245,19 +305,26 @@ def main():
 
     import torch
 
-    torch.cuda.set_device(local_rank)
+    torch.cuda.set_device(local_rank % torch.cuda.device_count())
     dist = None
+    global COLLECTIVE_DEVICE
     if world > 1:
         import datetime
 
         import torch.distributed as dist
 
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        # NCCL between GPUs; MIND_BENCH_BACKEND=gloo exercises the same exchange with host
+        # tensors (e.g. several ranks sharing one GPU in a test).
+        backend = os.environ.get("MIND_BENCH_BACKEND", "nccl")
+        COLLECTIVE_DEVICE = "cuda" if backend == "nccl" else "cpu"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
 
     import mind_b200 as mb
     from mind_b200 import replicas
 
-    model, layout = build_network(args.cells, seed=replicas.replica_seed(1, rank), config=args.config)
+    model, layout = build_network(args.cells, seed=replicas.replica_seed(1, rank), config=args.config,
+                                  rank=rank, world=world)
+    sharded = world > 1 and args.config == 2
     if args.accuracy_ms > 0:
         if rank == 0:
             soma_all = [mb.RecordSpec(layout.voltage_node(c), f"v{c}") for c in range(1, layout.n_cells + 1)]
@@ -277,6 +344,10 @@ def main():
     results, runs = {}, {}
     clocks = None
     for precision in precisions:
+        if sharded:
+            results[precision], runs[precision], clocks = measure_sharded(args, layout, rank, world, precision,
+                                                                          local_rank)
+            continue
         mb.initialize(model, precision=precision)
         model.state.set_profiling(True)
         dt = layout.dt
@@ -292,7 +363,7 @@ def main():
             dist.barrier()
         stats = model.state.run_stats()
         clocks = sampler.summary()
-        run_ms, units = replicas.reduce_timing(stats.run_ms, layout.segment_count * args.steps, device="cuda")
+        run_ms, units = replicas.reduce_timing(stats.run_ms, layout.segment_count * args.steps, device=COLLECTIVE_DEVICE)
         value = units / (run_ms / 1000.0)
         events = delivered_events(layout, result.spike_sources)
         algo = algorithmic_bytes_per_step(layout, events / args.steps)
@@ -301,10 +372,10 @@ def main():
         # End to end through the public API: a fresh run call with host recording.
         mb.initialize(model, precision=precision)
         mb.run(model, args.warmup * dt, record_spikes=False)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        e2e_result = mb.run(model, (args.warmup + args.steps) * dt, records=soma, record_spikes=True)
-        e2e_s, _ = replicas.reduce_timing(time.perf_counter() - t0, 0.0, device="cuda")
+        e2e_result, e2e_ms = device_timed(
+            lambda: mb.run(model, (args.warmup + args.steps) * dt, records=soma, record_spikes=True))
+        e2e_ms, _ = replicas.reduce_timing(e2e_ms, 0.0, device=COLLECTIVE_DEVICE)
+        e2e_s = e2e_ms / 1000.0
         d2h = (len(soma) * 8 * (args.steps + 1) + 16 * len(e2e_result.spike_times)) / args.steps
         h2d = 8 * len(soma) / args.steps
         runs[precision] = (np.stack([e2e_result.traces[r.name] for r in soma]), e2e_result.spike_sources,
@@ -330,7 +401,9 @@ def main():
         "data": f"synthetic (seeded config-{args.config} network, mind_b200.networks.config{args.config})",
         "config": {"workload": f"config{args.config}", "cells": layout.n_cells, "compartments": layout.segment_count,
                    "nodes": layout.n_nodes, "dt_ms": layout.dt, "precision": precisions[0],
-                   "parallelism": f"replica x{world}", "l2": "working set larger than L2 (no flush needed)",
+                   "parallelism": (f"cells sharded over {world} GPUs, spike all-gather per window" if sharded
+                                   else f"replica x{world}" if world > 1 else "1 GPU"),
+                   "l2": "working set larger than L2 (no flush needed)",
                    "window_steps": head["window_steps"], "size_bins": head["bins"]},
         "e2e": {"value": head["e2e"], "unit": UNIT, "h2d_bytes_per_step": head["h2d"],
                 "d2h_bytes_per_step": head["d2h"]},

@@ -321,8 +321,11 @@ def register_spike_source(source: Union[Cell, PointProcess, "MicroModel"], *, si
     return SpikeSource(model, index, identity)
 
 
-def register_point_sources(model: MicroModel, points) -> np.ndarray:
-    """Bulk: register net_event sources for 1-based point indices; returns source indices."""
+def register_point_sources(model: MicroModel, points, sids=None) -> np.ndarray:
+    """Bulk: register net_event sources for 1-based point indices; returns source indices.
+
+    `sids` optionally fixes the source ids of newly registered points (they must be unused).
+    """
     points = np.asarray(points, dtype=np.int64).reshape(-1)
     out = np.empty(len(points), dtype=np.int64)
     fresh = []
@@ -333,7 +336,12 @@ def register_point_sources(model: MicroModel, points) -> np.ndarray:
         else:
             fresh.append(j)
     if fresh:
-        ids = np.arange(model.next_source_id, model.next_source_id + len(fresh), dtype=np.int64)
+        if sids is not None:
+            ids = np.asarray(sids, dtype=np.int64).reshape(-1)[fresh]
+            if any(int(i) in model.source_ids for i in ids):
+                raise ValueError("source id already in use")
+        else:
+            ids = np.arange(model.next_source_id, model.next_source_id + len(fresh), dtype=np.int64)
         first = _append_sources(model, ids, np.zeros(len(fresh), np.int64), "none",
                                 np.zeros(len(fresh)), points[fresh], np.full(len(fresh), 10.0))
         for k, j in enumerate(fresh):

@@ -109,54 +109,71 @@ def _dendritic_sites(rng, sections: List[Section], count: int, labels=None):
 
 
 def config2(n_cells: int = 10000, synapses_per_cell: int = 100, background_hz: float = 5.0,
-            compartment_range: Tuple[int, int] = (100, 1000)) -> M.MicroModel:
-    """Uneven random binary trees in a recurrent Exp2Syn network (10,000 cells).
+            compartment_range: Tuple[int, int] = (100, 1000), *, rank: int = 0, world: int = 1) -> M.MicroModel:
+    """Uneven random binary trees in a recurrent Exp2Syn network (10,000 cells per rank).
+
+    The network has `n_cells * world` cells; this call builds rank `rank`'s block of
+    `n_cells` consecutive cells (world = 1: the whole network).  Every cell draws from its
+    own stream, numpy PCG64 seeded with (0x4D494E44 + 2, global cell index), so a rank
+    builds its cells alone and the cells do not depend on the rank count.
 
     Each cell: soma (1 compartment, L = diam = 20 um, hh) plus a random binary
     tree (`_binary_tree`) so that the total compartment count is uniform in
     `compartment_range`; pas (g 1e-4 S/cm2, e -65 mV) on every dendrite.
     100 Exp2Syn per cell (tau1 0.5 ms, tau2 5 ms; 80% e = 0 mV, 20% e = -80 mV)
     at uniform-random dendritic positions; each gets one NetCon from a
-    uniform-random presynaptic cell (soma(0.5) detector, -10 mV) with delay
-    U[1,5] ms and weight lognormal(ln 0.3 nS, 0.7), and its own 5 Hz Poisson
+    uniform-random presynaptic cell of the whole network (soma(0.5) detector, -10 mV)
+    with delay U[1,5] ms and weight lognormal(ln 0.3 nS, 0.7), and its own 5 Hz Poisson
     NetStim (interval 200 ms, noise 1, start 0) through a NetCon with delay 0
-    and a weight from the same lognormal.
-    Point order: all Exp2Syn (cell-major), then all NetStims.
+    and a weight from the same lognormal.  A presynaptic cell on another rank enters as
+    an external spike input with the cell's sid.
+    Source ids: cell g's detector is g + 1; synapse k of cell g's NetStim is
+    cells + g * synapses_per_cell + k + 1.  Point order: all Exp2Syn (cell-major), then all
+    NetStims.
     """
-    rng = _rng(2)
+    total = n_cells * world
+    first_cell = rank * n_cells
     model = M.MicroModel(celsius=6.3)
-    sizes = rng.integers(compartment_range[0], compartment_range[1] + 1, n_cells)
+    S = synapses_per_cell
     cells = []
-    for c in range(n_cells):
+    draws = []
+    for k in range(n_cells):
+        g = first_cell + k
+        rng = np.random.default_rng([SEED_BASE + 2, g])
+        size = int(rng.integers(compartment_range[0], compartment_range[1] + 1))
         soma = Section("soma", label="soma", length=20.0, diameter=20.0, nseg=1, Ra=100.0, cm=1.0)
-        secs = _binary_tree(rng, int(sizes[c]) - 1, soma)
+        secs = _binary_tree(rng, size - 1, soma)
         cell = M.add_population(model, secs, 1, voltage=-65.0)[0]
         M.insert(cell, builtin("hh"), sections="soma")
         M.insert(cell, builtin("pas"), sections="dend", params={"g": 1.0e-4, "e": -65.0})
-        M.register_spike_source(cell, threshold=-10.0)
-        cells.append((cell, secs))
-    n = n_cells * synapses_per_cell
-    owners = np.repeat(np.arange(1, n_cells + 1), synapses_per_cell)
-    names, xs = [], []
-    for cell, secs in cells:
-        nm, x = _dendritic_sites(rng, secs, synapses_per_cell)
-        names.extend(nm)
-        xs.append(x)
-    xs = np.concatenate(xs)
-    e_rev = np.where(rng.uniform(size=n) < 0.8, 0.0, -80.0)
-    first_syn = M.add_pointprocesses(model, builtin("Exp2Syn"), owners, names, xs,
-                                     {"tau1": 0.5, "tau2": 5.0, "e": e_rev})
-    presyn = rng.integers(1, n_cells + 1, n)  # detector source index == cell index
-    delays = rng.uniform(1.0, 5.0, n)
-    weights = rng.lognormal(math.log(0.3), 0.7, n) / 1000.0
+        M.register_spike_source(cell, sid=g + 1, threshold=-10.0)
+        names, xs = _dendritic_sites(rng, secs, S)
+        e_rev = np.where(rng.uniform(size=S) < 0.8, 0.0, -80.0)
+        presyn = rng.integers(1, total + 1, S)
+        delays = rng.uniform(1.0, 5.0, S)
+        weights = rng.lognormal(math.log(0.3), 0.7, S) / 1000.0
+        bg_weights = rng.lognormal(math.log(0.3), 0.7, S) / 1000.0
+        cells.append(cell)
+        draws.append((names, xs, e_rev, presyn, delays, weights, bg_weights))
+    n = n_cells * S
+    owners = np.repeat(np.arange(1, n_cells + 1), S)
+    names = [nm for d in draws for nm in d[0]]
+    first_syn = M.add_pointprocesses(model, builtin("Exp2Syn"), owners, names, np.concatenate([d[1] for d in draws]),
+                                     {"tau1": 0.5, "tau2": 5.0, "e": np.concatenate([d[2] for d in draws])})
+    presyn = np.concatenate([d[3] for d in draws])
+    local = (presyn > first_cell) & (presyn <= first_cell + n_cells)
+    sources = np.empty(n, dtype=np.int64)
+    sources[local] = presyn[local] - first_cell          # detector of local cell c is source c
+    for gid in np.unique(presyn[~local]):
+        sources[presyn == gid] = M.register_spike_source(model, sid=int(gid)).index
     targets = np.arange(first_syn, first_syn + n)
-    M.connect_many(model, presyn, targets, weights, delays)
+    M.connect_many(model, sources, targets, np.concatenate([d[5] for d in draws]), np.concatenate([d[4] for d in draws]))
     first_stim = M.add_pointprocesses(model, builtin("NetStim"), np.zeros(n, np.int64), "none",
                                       np.zeros(n), {"interval": 1000.0 / background_hz,
                                                     "number": 1e9, "start": 0.0, "noise": 1.0})
-    sources = M.register_point_sources(model, np.arange(first_stim, first_stim + n))
-    bg_weights = rng.lognormal(math.log(0.3), 0.7, n) / 1000.0
-    M.connect_many(model, sources, targets, bg_weights, np.zeros(n))
+    stim_sids = total + first_cell * S + np.arange(n) + 1
+    stim_sources = M.register_point_sources(model, np.arange(first_stim, first_stim + n), sids=stim_sids)
+    M.connect_many(model, stim_sources, targets, np.concatenate([d[6] for d in draws]), np.zeros(n))
     return model
 
 

@@ -169,6 +169,17 @@ def shard_layout(layout: Layout, cells: Sequence[int]) -> Shard:
     return Shard(sub, cells, node_map, np.array(detector_sids, dtype=np.int64), external, sids[src_keep].copy())
 
 
+def local_shard(layout: Layout) -> Shard:
+    """A rank's layout built directly for its cells (networks.config2(rank=, world=)): its
+    external inputs already stand for the other ranks' cells."""
+    sids = np.asarray(layout.source_ids, dtype=np.int64)
+    nodes = np.asarray(layout.source_nodes)
+    points = np.asarray(layout.source_points)
+    external = {int(sids[k]): k + 1 for k in np.nonzero((nodes == 0) & (points == 0))[0]}
+    return Shard(layout, np.arange(layout.n_cells), np.arange(layout.n_nodes + 1, dtype=np.int64),
+                 sids[nodes > 0].copy(), external, sids.copy())
+
+
 def exchange_spikes(sids: np.ndarray, times: np.ndarray, device="cpu"):
     """All-gather variable-length (sid, time) lists: counts first, then the padded lists."""
     import torch
@@ -208,15 +219,22 @@ class ShardedRun:
     """This rank's part of a network partitioned over the process group's ranks."""
 
     def __init__(self, layout: Layout, rank: int, world: int, *, precision: str = "fp64", device="cpu",
-                 owners: np.ndarray = None):
-        self.owners = partition_cells(layout, world) if owners is None else np.asarray(owners)
-        self.shard = shard_layout(layout, np.nonzero(self.owners == rank)[0])
+                 owners: np.ndarray = None, local: bool = False):
+        """`layout` is the whole network, partitioned here (by `owners` or partition_cells), or,
+        with local=True, this rank's own part with external inputs for the other ranks' cells."""
+        if local:
+            self.owners = None
+            self.shard = local_shard(layout)
+        else:
+            self.owners = partition_cells(layout, world) if owners is None else np.asarray(owners)
+            self.shard = shard_layout(layout, np.nonzero(self.owners == rank)[0])
         self.device = device
         self.dt = layout.dt
         self.state = DeviceState(self.shard.layout, precision)
         self.state.initialize()
         self.window = global_window(self.state.window_steps(), device)
-        self._detector = set(int(s) for s in self.shard.detector_sids)
+        self._external_sids = np.array(sorted(self.shard.external_source), dtype=np.int64)
+        self.launches = 0
 
     def records(self, nodes: Sequence[int]):
         """RecordSpecs for global 1-based nodes of owned cells (named by the global node)."""
@@ -243,15 +261,16 @@ class ShardedRun:
             k = min(self.window, steps - done)
             result = self.state.run_steps(k, list(records), True)
             device_ms += result.device_ms
+            self.launches += self.state.run_stats().launches
             if start is None:
                 start = result.time[0]
             for r in records:
                 traces[r.name].append(result.traces[r.name] if not traces[r.name] else result.traces[r.name][1:])
-            mine = np.array([int(s) not in self.shard.external_source for s in result.spike_sources], dtype=bool)
+            mine = ~np.isin(result.spike_sources, self._external_sids)
             if record_spikes:
                 times.append(result.spike_times[mine])
                 sids.append(result.spike_sources[mine])
-            cell = np.array([int(s) in self._detector for s in result.spike_sources], dtype=bool)
+            cell = np.isin(result.spike_sources, self.shard.detector_sids)
             all_s, all_t = exchange_spikes(result.spike_sources[cell], result.spike_times[cell], self.device)
             local = [self.shard.external_source.get(int(s), 0) for s in all_s]
             want = np.array([x > 0 for x in local], dtype=bool)
