@@ -171,6 +171,16 @@ function mindgpu_run!(model, stop_time::Real; records = (), record_spikes::Bool 
     return (; time, traces, spike_times = times, spike_sources = sids)
 end
 
+"""inject_spike!: external spike inputs (1-based source indices) fire at absolute times."""
+function mindgpu_inject_spikes!(model, sources::AbstractVector{<:Integer}, times::AbstractVector{<:Real})
+    h = model.runtime.state::Handle
+    src = Int64.(sources)
+    t = Float64.(times)
+    check(h.ptr, ccall((:mind_inject_spikes, libmindgpu), Cint, (Ptr{Cvoid}, Int64, Ptr{Int64}, Ptr{Float64}),
+                       h.ptr, length(src), src, t))
+    return model
+end
+
 mindgpu_step!(model) = (check(model.runtime.state.ptr,
                               ccall((:mind_step, libmindgpu), Cint, (Ptr{Cvoid},), model.runtime.state.ptr)); model)
 
