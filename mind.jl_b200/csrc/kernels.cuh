@@ -399,6 +399,203 @@ __device__ __forceinline__ void apply_event(const StagedGroup &G, int32_t row, d
 }
 
 /*
+ * Hines solve of one resident cell, FP64 mode: the reference's operations in the
+ * canonical order (gather-form elimination, f = a/D, back-substitution (R + a x_p)/D).
+ * Level by level, one chain per thread; along a chain only subtract -> divide ->
+ * multiply stays on the dependency chain, the next node's operands being loaded
+ * before the current division.
+ */
+__device__ __forceinline__ void hines_exact(double *sd, double *sr, const double *sa, double *sv, double *sxd,
+                                            double *sxr, const int32_t *ctop, const int32_t *clen,
+                                            const int32_t *cpar, const int32_t *ckoff, const int32_t *ckids,
+                                            const int32_t *lvc, int32_t nlev, bool &singular) {
+    constexpr int32_t T = kCellThreads;
+    const int32_t tid = threadIdx.x;
+    for (int32_t lv = 0; lv < nlev; ++lv) {
+        for (int32_t ch = lvc[lv] + tid; ch < lvc[lv + 1]; ch += T) {
+            const int32_t top = ctop[ch];
+            const int32_t bottom = top + clen[ch] - 1;
+            const bool rooted = cpar[ch] < 0;
+            double D = sd[bottom], R = sr[bottom];
+            for (int32_t q = ckoff[ch]; q < ckoff[ch + 1]; ++q) {
+                const int32_t cc = ckids[q];
+                D = D - sxd[cc];
+                R = R + sxr[cc];
+            }
+            singular |= (D == 0.0) | !isfinite(D);
+            sd[bottom] = D;
+            sr[bottom] = R;
+            double pxd = 0.0, pxr = 0.0;
+            if (bottom > top || !rooted) {
+                const double ab = sa[bottom];
+                double dn = 0.0, rn = 0.0, an = 0.0;
+                if (bottom > top) {
+                    dn = sd[bottom - 1];
+                    rn = sr[bottom - 1];
+                    an = sa[bottom - 1];
+                }
+                const double f = ab / D;
+                pxd = f * ab;
+                pxr = f * R;
+                // interior nodes: every one has its parent at i - 1
+                int32_t i = bottom - 1;
+                for (; i > top; --i) {
+                    const double Di = dn - pxd, Ri = rn + pxr, ai = an;
+                    dn = sd[i - 1];
+                    rn = sr[i - 1];
+                    an = sa[i - 1];
+                    singular |= (Di == 0.0) | !isfinite(Di);
+                    sd[i] = Di;
+                    sr[i] = Ri;
+                    const double fi = ai / Di;
+                    pxd = fi * ai;
+                    pxr = fi * Ri;
+                }
+                if (i == top && bottom > top) {
+                    const double Dt = dn - pxd, Rt = rn + pxr;
+                    singular |= (Dt == 0.0) | !isfinite(Dt);
+                    sd[top] = Dt;
+                    sr[top] = Rt;
+                    if (!rooted) {
+                        const double ft = an / Dt;
+                        pxd = ft * an;
+                        pxr = ft * Rt;
+                    }
+                }
+            }
+            sxd[ch] = pxd;
+            sxr[ch] = pxr;
+        }
+        __syncthreads();
+    }
+    for (int32_t lv = nlev - 1; lv >= 0; --lv) {
+        for (int32_t ch = lvc[lv] + tid; ch < lvc[lv + 1]; ch += T) {
+            const int32_t top = ctop[ch];
+            const int32_t bottom = top + clen[ch] - 1;
+            const int32_t par = cpar[ch];
+            double rn = sr[top], an = sa[top], dn = sd[top];
+            double x;
+            {
+                const double ri = rn, ai = an, di = dn;
+                const double xp = par >= 0 ? sr[par] : 0.0;
+                if (top < bottom) {
+                    rn = sr[top + 1];
+                    an = sa[top + 1];
+                    dn = sd[top + 1];
+                }
+                x = (par >= 0 ? ri + ai * xp : ri) / di;
+                sr[top] = x;
+                sv[top] = sv[top] + x;
+            }
+            for (int32_t i = top + 1; i <= bottom; ++i) {
+                const double ri = rn, ai = an, di = dn;
+                if (i < bottom) {
+                    rn = sr[i + 1];
+                    an = sa[i + 1];
+                    dn = sd[i + 1];
+                }
+                x = (ri + ai * x) / di;
+                sr[i] = x;
+                sv[i] = sv[i] + x;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+/*
+ * Hines solve, mixed mode: FP64 arithmetic with reciprocals.  Elimination keeps, per
+ * node, f = a/D in place of D and R/D in place of R, so the back-substitution is one
+ * FMA per node, x = f x_p + R/D; the pivot chain is D -> 1/D -> (a^2)(1/D) -> next D.
+ */
+__device__ __forceinline__ void hines_mixed(double *sd, double *sr, const double *sa, double *sv, double *sxd,
+                                            double *sxr, const int32_t *ctop, const int32_t *clen,
+                                            const int32_t *cpar, const int32_t *ckoff, const int32_t *ckids,
+                                            const int32_t *lvc, int32_t nlev, bool &singular) {
+    constexpr int32_t T = kCellThreads;
+    const int32_t tid = threadIdx.x;
+    for (int32_t lv = 0; lv < nlev; ++lv) {
+        for (int32_t ch = lvc[lv] + tid; ch < lvc[lv + 1]; ch += T) {
+            const int32_t top = ctop[ch];
+            const int32_t bottom = top + clen[ch] - 1;
+            const bool rooted = cpar[ch] < 0;
+            double D = sd[bottom], R = sr[bottom];
+            for (int32_t q = ckoff[ch]; q < ckoff[ch + 1]; ++q) {
+                const int32_t cc = ckids[q];
+                D = D - sxd[cc];
+                R = R + sxr[cc];
+            }
+            singular |= (D == 0.0) | !isfinite(D);
+            const double ab = sa[bottom];
+            double dn = 0.0, rn = 0.0, an = 0.0;
+            if (bottom > top) {
+                dn = sd[bottom - 1];
+                rn = sr[bottom - 1];
+                an = sa[bottom - 1];
+            }
+            const double y = approx_reciprocal(D);
+            const double f = ab * y;
+            sd[bottom] = f;
+            sr[bottom] = R * y;
+            double pxd = (ab * ab) * y, pxr = f * R;
+            int32_t i = bottom - 1;
+            for (; i > top; --i) {
+                const double Di = dn - pxd, Ri = rn + pxr, ai = an, asq = an * an;
+                dn = sd[i - 1];
+                rn = sr[i - 1];
+                an = sa[i - 1];
+                singular |= (Di == 0.0) | !isfinite(Di);
+                const double yi = approx_reciprocal(Di);
+                const double fi = ai * yi;
+                sd[i] = fi;
+                sr[i] = Ri * yi;
+                pxd = asq * yi;
+                pxr = fi * Ri;
+            }
+            if (bottom > top) {
+                const double Dt = dn - pxd, Rt = rn + pxr;
+                singular |= (Dt == 0.0) | !isfinite(Dt);
+                const double yt = approx_reciprocal(Dt);
+                const double ft = an * yt;
+                sd[top] = ft;
+                sr[top] = Rt * yt;
+                pxd = (an * an) * yt;
+                pxr = ft * Rt;
+            }
+            sxd[ch] = rooted ? 0.0 : pxd;
+            sxr[ch] = rooted ? 0.0 : pxr;
+        }
+        __syncthreads();
+    }
+    for (int32_t lv = nlev - 1; lv >= 0; --lv) {
+        for (int32_t ch = lvc[lv] + tid; ch < lvc[lv + 1]; ch += T) {
+            const int32_t top = ctop[ch];
+            const int32_t bottom = top + clen[ch] - 1;
+            const int32_t par = cpar[ch];
+            double fn = sd[top], qn = sr[top];
+            double x = par >= 0 ? fma(fn, sr[par], qn) : qn;
+            sr[top] = x;
+            sv[top] = sv[top] + x;
+            if (top < bottom) {
+                fn = sd[top + 1];
+                qn = sr[top + 1];
+            }
+            for (int32_t i = top + 1; i <= bottom; ++i) {
+                const double fi = fn, qi = qn;
+                if (i < bottom) {
+                    fn = sd[i + 1];
+                    qn = sr[i + 1];
+                }
+                x = fma(fi, x, qi);
+                sr[i] = x;
+                sv[i] = sv[i] + x;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+/*
  * One CTA of two warps advances one cell through W micro steps.  Shared memory
  * holds what the serial parts of the step touch: v, d, rhs and axial
  * conductance of every node, the chain tables of the Hines solve, the state
@@ -699,111 +896,12 @@ __global__ void __launch_bounds__(kCellThreads, 8) window_kernel(const Params P,
         }
         __syncthreads();
 
-        // 6. Hines elimination, level by level; each chain bottom to top into its parent.
-        //    The inner loop keeps only subtract -> divide -> multiply on the dependency
-        //    chain: the next node's operands are loaded before the current division.
-        for (int32_t lv = 0; lv < nlev; ++lv) {
-            for (int32_t ch = lvc[lv] + tid; ch < lvc[lv + 1]; ch += T) {
-                const int32_t top = ctop[ch];
-                const int32_t bottom = top + clen[ch] - 1;
-                const bool rooted = cpar[ch] < 0;
-                double D = sd[bottom], R = sr[bottom];
-                for (int32_t q = ckoff[ch]; q < ckoff[ch + 1]; ++q) {
-                    const int32_t cc = ckids[q];
-                    D = D - sxd[cc];
-                    R = R + sxr[cc];
-                }
-                singular |= (D == 0.0) | !isfinite(D);
-                // Mixed mode keeps the pivot's reciprocal in place of the pivot: the
-                // back-substitution then multiplies instead of dividing.
-                const double yb = MIXED ? approx_reciprocal(D) : 0.0;
-                sd[bottom] = MIXED ? yb : D;
-                sr[bottom] = R;
-                double pxd = 0.0, pxr = 0.0;
-                if (bottom > top || !rooted) {
-                    const double ab = sa[bottom];
-                    double dn = 0.0, rn = 0.0, an = 0.0;
-                    if (bottom > top) {
-                        dn = sd[bottom - 1];
-                        rn = sr[bottom - 1];
-                        an = sa[bottom - 1];
-                    }
-                    const double f = MIXED ? ab * yb : ab / D;
-                    pxd = f * ab;
-                    pxr = f * R;
-                    // interior nodes: every one has its parent at i - 1
-                    int32_t i = bottom - 1;
-                    for (; i > top; --i) {
-                        const double Di = dn - pxd, Ri = rn + pxr, ai = an;
-                        dn = sd[i - 1];
-                        rn = sr[i - 1];
-                        an = sa[i - 1];
-                        singular |= (Di == 0.0) | !isfinite(Di);
-                        sr[i] = Ri;
-                        double fi;
-                        if (MIXED) {
-                            const double yi = approx_reciprocal(Di);
-                            sd[i] = yi;
-                            fi = ai * yi;
-                        } else {
-                            sd[i] = Di;
-                            fi = ai / Di;
-                        }
-                        pxd = fi * ai;
-                        pxr = fi * Ri;
-                    }
-                    if (i == top && bottom > top) {
-                        const double Dt = dn - pxd, Rt = rn + pxr;
-                        singular |= (Dt == 0.0) | !isfinite(Dt);
-                        const double yt = MIXED ? approx_reciprocal(Dt) : 0.0;
-                        sd[top] = MIXED ? yt : Dt;
-                        sr[top] = Rt;
-                        if (!rooted) {
-                            const double ft = MIXED ? an * yt : an / Dt;
-                            pxd = ft * an;
-                            pxr = ft * Rt;
-                        }
-                    }
-                }
-                sxd[ch] = pxd;
-                sxr[ch] = pxr;
-            }
-            __syncthreads();
-        }
-        // 7. Back-substitution, root chain first, with the voltage update.
-        for (int32_t lv = nlev - 1; lv >= 0; --lv) {
-            for (int32_t ch = lvc[lv] + tid; ch < lvc[lv + 1]; ch += T) {
-                const int32_t top = ctop[ch];
-                const int32_t bottom = top + clen[ch] - 1;
-                const int32_t par = cpar[ch];
-                double rn = sr[top], an = sa[top], dn = sd[top];
-                double x;
-                {
-                    const double ri = rn, ai = an, di = dn;
-                    const double xp = par >= 0 ? sr[par] : 0.0;
-                    if (top < bottom) {
-                        rn = sr[top + 1];
-                        an = sa[top + 1];
-                        dn = sd[top + 1];
-                    }
-                    const double num = par >= 0 ? ri + ai * xp : ri;
-                    x = MIXED ? num * di : num / di;   // mixed mode: di holds 1/pivot
-                    sr[top] = x;
-                    sv[top] = sv[top] + x;
-                }
-                for (int32_t i = top + 1; i <= bottom; ++i) {
-                    const double ri = rn, ai = an, di = dn;
-                    if (i < bottom) {
-                        rn = sr[i + 1];
-                        an = sa[i + 1];
-                        dn = sd[i + 1];
-                    }
-                    x = MIXED ? (ri + ai * x) * di : (ri + ai * x) / di;
-                    sr[i] = x;
-                    sv[i] = sv[i] + x;
-                }
-            }
-            __syncthreads();
+        // 6-7. Hines elimination level by level, each chain bottom to top into its parent,
+        //      then back-substitution root chain first with the voltage update.
+        if (MIXED) {
+            hines_mixed(sd, sr, sa, sv, sxd, sxr, ctop, clen, cpar, ckoff, ckids, lvc, nlev, singular);
+        } else {
+            hines_exact(sd, sr, sa, sv, sxd, sxr, ctop, clen, cpar, ckoff, ckids, lvc, nlev, singular);
         }
 
         // 8. cnexp state advance on the new voltage (time t + dt).
