@@ -152,6 +152,8 @@ struct Params {
     const int64_t *node_off;   // [ncells+1]
     double *v;
     const double *a, *cdt, *ad;
+    // mixed mode: C/dt + axial_diagonal + pas conductance, pas conductance, and it times e
+    const double *mix_dc, *mix_gs, *mix_gse;
     const int32_t *parent;     // [packed] local parent index or -1
     const int32_t *kid_off;    // [packed+1] CSR into kids (children in ascending layout index)
     const int32_t *kids;       // local child indices

@@ -814,6 +814,7 @@ __global__ void __launch_bounds__(kCellThreads, 8) window_kernel(const Params P,
             const int32_t lo = spart[g * (T + 1) + tid], hi = spart[g * (T + 1) + tid + 1];
             if (lo >= hi) continue;
             if (G.kind == MIND_MECH_PAS) {
+                if (MIXED) continue;  // folded into the node constants of the assembly below
                 const double *pg = GG.f[PAS_G] + G.r0, *pe = GG.f[PAS_E] + G.r0, *ps = GG.f[PAS_SCALE] + G.r0;
                 const int32_t *pn = GG.node + G.r0;
                 for (int32_t r = lo; r < hi; ++r) {
@@ -844,6 +845,18 @@ __global__ void __launch_bounds__(kCellThreads, 8) window_kernel(const Params P,
                     const double vv = sv[node];
                     const double probe = vv + 0.001;
                     const double m = G.at(HH_M, r), h = G.at(HH_H, r), nn = G.at(HH_N, r);
+                    if (MIXED) {
+                        // at fixed gates the current is linear in v: dI/dv is the summed conductance
+                        const double gna = G.at(HH_GNABAR, r) * m * m * m * h;
+                        const double gk = G.at(HH_GKBAR, r) * nn * nn * nn * nn;
+                        const double gl = G.at(HH_GL, r);
+                        const double i = gl * (vv - G.at(HH_EL, r)) + gna * (vv - G.at(HH_ENA, r)) +
+                                         gk * (vv - G.at(HH_EK, r));
+                        const double scale = G.at(HH_SCALE, r);
+                        sr[node] = sr[node] - scale * i;
+                        sd[node] = sd[node] + scale * (gna + gk + gl);
+                        continue;
+                    }
                     const double shifted = hh_current(probe, m, h, nn, G.at(HH_GNABAR, r), G.at(HH_GKBAR, r),
                                                       G.at(HH_GL, r), G.at(HH_EL, r), G.at(HH_ENA, r), G.at(HH_EK, r));
                     const double value = hh_current(vv, m, h, nn, G.at(HH_GNABAR, r), G.at(HH_GKBAR, r),
@@ -864,6 +877,11 @@ __global__ void __launch_bounds__(kCellThreads, 8) window_kernel(const Params P,
                     else
                         gs = G.at(0, r);
                     const double vv = sv[node];
+                    if (MIXED) {  // linear in v: the probe's difference quotient is the conductance
+                        sr[node] = sr[node] - gs * (vv - e);
+                        sd[node] = sd[node] + gs;
+                        continue;
+                    }
                     const double probe = vv + 0.001;
                     const double shifted = 0.0 + gs * (probe - e);
                     const double value = 0.0 + gs * (vv - e);
@@ -875,13 +893,17 @@ __global__ void __launch_bounds__(kCellThreads, 8) window_kernel(const Params P,
         // Cable assembly of the owned nodes: d = C/dt + d + axial_diagonal; own axial term, then children.
         for (int32_t i = tid; i < n; i += T) {
             const int64_t gi = nb + i;
-            const double cdt = __ldg(P.cdt + gi), adi = __ldg(P.ad + gi);
             const int32_t k = chain_of[i];
             const int32_t top = ctop[k];
             const int32_t bottom = top + clen[k] - 1;
             const double vi = sv[i];
-            sd[i] = (cdt + sd[i]) + adi;
             double R = sr[i];
+            if (MIXED) {
+                sd[i] = __ldg(P.mix_dc + gi) + sd[i];
+                R = R + (__ldg(P.mix_gse + gi) - __ldg(P.mix_gs + gi) * vi);
+            } else {
+                sd[i] = (__ldg(P.cdt + gi) + sd[i]) + __ldg(P.ad + gi);
+            }
             const int32_t p = i == top ? cpar[k] : i - 1;
             if (p >= 0) R = R + sa[i] * (sv[p] - vi);
             if (i < bottom) {

@@ -369,6 +369,9 @@ int create(const MindLayout *L, MindHandle *h) {
     // group's rows are sorted by (cell, owner thread, node, layout row): a thread's rows are
     // one range, and rows of one node stay in layout order.
     std::vector<int32_t> part((size_t)ncells * L->n_mechanisms * (kCellThreads + 1), 0);
+    // Mixed mode folds pas into per-node constants: its conductance g*area*0.01 and
+    // that times e (the probe's (i(v+0.001)-i(v))/0.001 of a linear current is g).
+    std::vector<double> mix_gs(n, 0.0), mix_gse(n, 0.0);
     std::vector<std::vector<int32_t>> row_cell(L->n_mechanisms);
     for (int32_t g = 0; g < L->n_mechanisms; ++g) {
         const MindMechanism &m = L->mechanisms[g];
@@ -440,6 +443,12 @@ int create(const MindLayout *L, MindHandle *h) {
                     if (seg[r] > 1) return fail(h, MIND_ELAYOUT, "density mechanism twice on one node");
                 int slot = m.kind == MIND_MECH_HH ? HH_SCALE : PAS_SCALE;
                 for (int32_t r = 0; r < rows; ++r) init.f[slot][r] = L->area[layout_of_packed[node_dev[r]]] * 0.01;
+                if (m.kind == MIND_MECH_PAS)
+                    for (int32_t r = 0; r < rows; ++r) {
+                        const double gs = init.f[PAS_G][r] * init.f[PAS_SCALE][r];
+                        mix_gs[node_dev[r]] += gs;
+                        mix_gse[node_dev[r]] += gs * init.f[PAS_E][r];
+                    }
             }
             for (int32_t r = 0; r < rows; ++r) row_off[row_cell[g][r] + 1]++;
             for (int32_t c = 0; c < ncells; ++c) row_off[c + 1] += row_off[c];
@@ -557,6 +566,13 @@ int create(const MindLayout *L, MindHandle *h) {
     P.a = h->upload(a);
     P.cdt = h->upload(cdt);
     P.ad = h->upload(ad);
+    {
+        std::vector<double> mix_dc(n);
+        for (int64_t j = 0; j < n; ++j) mix_dc[j] = cdt[j] + ad[j] + mix_gs[j];
+        P.mix_dc = h->upload(mix_dc);
+        P.mix_gs = h->upload(mix_gs);
+        P.mix_gse = h->upload(mix_gse);
+    }
     P.chain_off = h->upload(chain_off);
     P.chain_top = h->upload(chain_top);
     P.chain_len = h->upload(chain_len);
