@@ -196,6 +196,63 @@ int mind_inject_spikes(MindHandle *h, int64_t n, const int64_t *sources, const d
  * exchanges (no reference counterpart: the reference routes every step on the host). */
 int mind_window_steps(const MindHandle *h, int32_t *steps);
 
+/*
+ * Cross-scale coupling (advance_macro!, src/runtime/step.jl:156-204;
+ * src/runtime/cuda/macro.jl): neural-mass regions advanced every dt_macro and coupled
+ * to the micro network both ways.
+ *
+ * Regions are Jansen-Rit second-order PSP masses, six states per region (mV, mV/s):
+ *   y0' = y3   y3' = A a S(y1 - y2) - 2 a y3 - a^2 y0
+ *   y1' = y4   y4' = A a (p + C2 S(C1 y0)) - 2 a y4 - a^2 y1
+ *   y2' = y5   y5' = B b C4 S(C3 y0) - 2 b y5 - b^2 y2
+ *   S(v) = 2 e0 / (1 + exp(r (v0 - v))),  C1..C4 = C, 0.8 C, 0.25 C, 0.25 C,
+ * integrated by classical RK4 over dt_macro (time in s inside the right-hand side) with
+ * the input p held over the step.  A region's output is out = S(y1 - y2) (s^-1), taken at
+ * the start of each macro step k.  Its input over step k is
+ *   p(k) = p0 + micro_gain * rate(bin(k) - 1) + sum over edges into it (in edge order)
+ *          of gain * out_src(k - delay),
+ * where rate(b) is the spike rate (Hz per cell) of the detector sources mapped to the
+ * region during rate bin b (bin_ms long; bin(k) = the bin containing step k; rate 0 before
+ * the first bin), and out_src(m) for m < 0 is out_src(0).  Macro to micro: every input
+ * source (an external spike input of the layout) fires as a Poisson process of rate
+ * scale * out(k) Hz over macro step k; its n events in step k (n by inversion of the Poisson
+ * CDF, at most 3) fall at k dt_macro + dt_macro u_j, with u_0 (count) and u_1..u_3 the
+ * words of Philox4x32-10 on counter (k low, k high, input index, 0x4D4D), key = seed,
+ * mapped to (w + 1)/(2^32 + 1); they then follow the source's NetCons.
+ * dt_macro must be a multiple of dt and bin_ms a multiple of dt_macro; the library's
+ * window becomes a divisor of the bin that is a multiple of the macro step, so bins are
+ * complete before the regions read them.
+ */
+typedef struct {
+    int32_t n_regions;
+    const double *params;         /* [n_regions][9]: A, B, a, b, e0, r, v0, C, p0 */
+    const double *y0;             /* [n_regions][6] initial states */
+    const double *micro_gain;     /* [n_regions] */
+    int64_t n_edges;
+    const int32_t *edge_src;      /* 1-based regions */
+    const int32_t *edge_dst;
+    const double *edge_gain;
+    const int32_t *edge_delay;    /* macro steps, >= 1 */
+    int64_t n_inputs;
+    const int32_t *input_region;  /* 1-based region driving each input */
+    const int64_t *input_source;  /* 1-based external source of the micro layout */
+    const double *input_scale;    /* Hz of input rate per s^-1 of region output */
+    int64_t n_outputs;
+    const int32_t *output_region; /* 1-based region fed by each detector source */
+    const int64_t *output_source; /* 1-based detector source of the micro layout */
+    double dt_macro;              /* ms */
+    double bin_ms;                /* population-rate bin, ms */
+} MindMacroLayout;
+
+/* Attach regions and coupling to a created handle (before mind_initialize; allocation
+ * happens here).  Runs then advance regions, inputs and rate bins with the micro steps. */
+int mind_attach_macro(MindHandle *h, const MindMacroLayout *macro);
+
+/* The regions' outputs out(k) recorded by the last run for every macro step boundary it
+ * covered, [samples][n_regions] sample-major; `n` is the buffer length.  samples =
+ * floor(end / steps per macro step) - ceil(start / steps per macro step) + 1. */
+int mind_get_macro_trace(const MindHandle *h, double *out, int64_t n, int64_t *samples);
+
 /* Message for the last non-zero status of this handle (or of mind_create when h is NULL). */
 const char *mind_last_error(const MindHandle *h);
 

@@ -361,14 +361,21 @@ __global__ void bucket_kernel(const Params P, int64_t n0) {
     }
 }
 
-/* Routes the window's cell spikes (detected at step s, time s*dt + 1e-10). */
-__global__ void route_kernel(const Params P, int64_t window_end) {
+/* Routes the window's cell spikes (detected at step s, time s*dt + 1e-10); with regions
+ * attached, also counts each spike into its region's rate bin (bin_steps micro steps). */
+__global__ void route_kernel(const Params P, int64_t window_end, const int32_t *source_region, int32_t *bins,
+                             int32_t n_regions, int32_t bin_steps, int32_t bin_ring) {
     const int32_t count = min(*P.win_spike_count, P.win_spike_cap);
     for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
         int32_t source = P.win_spike_source[i];
-        double time = (double)P.win_spike_step[i] * P.dt + 1.0e-10;
+        const int64_t step = P.win_spike_step[i];
+        double time = (double)step * P.dt + 1.0e-10;
         record_spike(P, source, time);
         fan_out(P, source, time, window_end);
+        if (n_regions > 0) {
+            const int32_t region = source_region[source];
+            if (region >= 0) atomicAdd(&bins[((step / bin_steps) % bin_ring) * n_regions + region], 1);
+        }
     }
 }
 

@@ -28,6 +28,7 @@
 #include <vector>
 
 #include "kernels.cuh"
+#include "macro.cuh"
 
 using namespace mind;
 
@@ -67,6 +68,16 @@ struct MindHandle {
     std::vector<int64_t> fanout;             // [n_sources+1] 0-based edge ranges
     std::vector<double> edge_delay;
     std::vector<uint8_t> source_external;    // no detector and no point: an inject_spike! input
+    std::vector<uint8_t> source_detector;
+    // regions coupled to the cells (mind_attach_macro)
+    MacroParams M{};
+    double *macro_y0 = nullptr;
+    int32_t bin_steps = 0;                   // micro steps per rate bin
+    int32_t macro_threads = 32;
+    double *macro_trace_dev = nullptr;
+    size_t macro_trace_cap = 0;
+    std::vector<double> macro_trace;
+    int64_t macro_trace_samples = 0;
     std::vector<double> v0_packed;
     int64_t n_sources = 0;
     std::vector<int64_t> source_ids;
@@ -164,6 +175,13 @@ int cuda_fail(MindHandle *h, cudaError_t e, const char *where) {
         cudaError_t _e = (call);                                   \
         if (_e != cudaSuccess) return cuda_fail((h), _e, #call);   \
     } while (0)
+
+/* Window: a spike detected at step s arrives in bin >= s + floor((d - dt/2)/dt); keep one bin margin. */
+int32_t window_for_delay(double min_delay, double dt) {
+    if (!std::isfinite(min_delay)) return kMaxWindow;
+    const double k = std::floor((min_delay - 0.5 * dt) / dt) - 1.0;
+    return (int32_t)std::max(1.0, std::min((double)kMaxWindow, k));
+}
 
 int field_index(const MindMechanism &m, const char *name) {
     for (int32_t j = 0; j < m.n_fields; ++j)
@@ -545,19 +563,16 @@ int create(const MindLayout *L, MindHandle *h) {
             if (L->source_nodes[s] > 0 || L->source_points[s] == 0) min_cell_delay = std::min(min_cell_delay, d);
         }
     }
-    // Window: a spike detected at step s arrives in bin >= s + floor((d - dt/2)/dt); keep one bin margin.
-    int32_t window = kMaxWindow;
-    if (std::isfinite(min_cell_delay)) {
-        double k = std::floor((min_cell_delay - 0.5 * L->dt) / L->dt) - 1.0;
-        window = (int32_t)std::max(1.0, std::min((double)kMaxWindow, k));
-    }
-    h->window = window;
+    h->window = window_for_delay(min_cell_delay, L->dt);
     h->edge_target = edge_target;
     h->fanout = fanout;
     h->edge_delay = edge_delay;
     h->source_external.assign(L->n_sources, 0);
-    for (int64_t s = 0; s < L->n_sources; ++s)
+    h->source_detector.assign(L->n_sources, 0);
+    for (int64_t s = 0; s < L->n_sources; ++s) {
         h->source_external[s] = L->source_nodes[s] == 0 && L->source_points[s] == 0;
+        h->source_detector[s] = L->source_nodes[s] > 0;
+    }
     h->max_delay_bins = (int32_t)std::ceil(max_delay / L->dt) + 2;
 
     // ---- device arrays ----
@@ -596,7 +611,8 @@ int create(const MindLayout *L, MindHandle *h) {
     P.rec_spike_source = h->alloc<int32_t>(P.rec_spike_cap);
     P.rec_spike_time = h->alloc<double>(P.rec_spike_cap);
     P.rec_spike_count = h->alloc<int32_t>(1);
-    P.ring_slots = window + h->max_delay_bins + 4;
+    // Room for the longest window (attaching regions can lengthen it) plus the longest delay.
+    P.ring_slots = kMaxWindow + h->max_delay_bins + 4;
     int64_t ring_cap = L->event_capacity > 0 ? L->event_capacity
                                              : std::max<int64_t>(4096, std::min<int64_t>(ne / 16 + 1, 1 << 20));
     P.ring_cap = (int32_t)ring_cap;
@@ -779,9 +795,28 @@ int advance(MindHandle *h, int64_t steps, bool record_spikes) {
         }
         return h->prof_events[prof_used++];
     };
+    const MacroParams &M = h->M;
+    if (M.n > 0 && M.trace) {
+        macro_trace_start_kernel<<<1, h->macro_threads, 0, h->stream>>>(M, M.trace_k0);
+        ++st.launches;
+    }
     while (n0 < end) {
-        const int32_t W = (int32_t)std::min<int64_t>(h->window, end - n0);
+        int32_t W = (int32_t)std::min<int64_t>(h->window, end - n0);
+        // With regions attached, windows stay inside multiples of the window length (a
+        // divisor of the rate bin), so a bin is complete before the regions read it.
+        if (M.n > 0) W = (int32_t)std::min<int64_t>(W, h->window - n0 % h->window);
         const double horizon = (double)(n0 + W - 1) * P.dt + 0.5 * P.dt;
+        if (M.n > 0) {
+            const int64_t spm = M.steps_per_macro;
+            const int64_t k0 = (n0 + spm - 1) / spm, k1 = (n0 + W + spm - 1) / spm;
+            const int32_t zero_slot = n0 % h->bin_steps == 0 ? (int32_t)((n0 / h->bin_steps) % M.bin_ring) : -1;
+            macro_advance_kernel<<<1, h->macro_threads, 0, h->stream>>>(M, k0, k1, zero_slot);
+            ++st.launches;
+            if (k1 > k0 && M.n_inputs > 0) {
+                macro_input_kernel<<<launch_grid(M.n_inputs), kThreads, 0, h->stream>>>(P, M, k0, k1, n0);
+                ++st.launches;
+            }
+        }
         if (P.ns_group >= 0) {
             netstim_kernel<<<ns_blocks, kThreads, 0, h->stream>>>(P, horizon, n0);
             ++st.launches;
@@ -828,7 +863,8 @@ int advance(MindHandle *h, int64_t steps, bool record_spikes) {
             ++st.window_launches;
         }
         if (h->profiling) cudaEventRecord(prof_event(), h->stream);
-        route_kernel<<<64, kThreads, 0, h->stream>>>(P, n0 + W);
+        route_kernel<<<64, kThreads, 0, h->stream>>>(P, n0 + W, M.source_region, M.bins, M.n, h->bin_steps,
+                                                     M.bin_ring);
         ++st.launches;
         n0 += W;
     }
@@ -848,6 +884,37 @@ int advance(MindHandle *h, int64_t steps, bool record_spikes) {
     h->stats = st;
     h->step = end;
     return check_device_error(h);
+}
+
+/* Device buffer for the regions' outputs at the run's macro boundaries (mind_run only). */
+int set_macro_trace(MindHandle *h, int64_t steps) {
+    MacroParams &M = h->M;
+    M.trace = nullptr;
+    h->macro_trace_samples = 0;
+    if (M.n == 0) return MIND_OK;
+    const int64_t spm = M.steps_per_macro;
+    const int64_t k0 = (h->step + spm - 1) / spm, k1 = (h->step + steps) / spm;
+    const int64_t samples = std::max<int64_t>(0, k1 - k0 + 1);
+    if (samples == 0) return MIND_OK;
+    const size_t need = (size_t)samples * M.n;
+    if (need > h->macro_trace_cap) {
+        if (h->macro_trace_dev) h->release(h->macro_trace_dev);
+        h->macro_trace_dev = nullptr;
+        h->macro_trace_dev = h->alloc<double>(need);
+        h->macro_trace_cap = need;
+    }
+    M.trace = h->macro_trace_dev;
+    M.trace_k0 = k0;
+    M.trace_samples = samples;
+    h->macro_trace_samples = samples;
+    return MIND_OK;
+}
+
+int collect_macro_trace(MindHandle *h) {
+    const size_t n = (size_t)h->macro_trace_samples * h->M.n;
+    h->macro_trace.assign(n, 0.0);
+    if (n) CUDA_TRY(h, cudaMemcpy(h->macro_trace.data(), h->macro_trace_dev, n * sizeof(double), cudaMemcpyDeviceToHost));
+    return MIND_OK;
 }
 
 int collect(MindHandle *h, bool record_spikes) {
@@ -941,10 +1008,130 @@ int mind_initialize(MindHandle *h) {
     if (P.ns_group >= 0 && P.groups[P.ns_group].rows > 0)
         netstim_init_kernel<<<launch_grid(P.groups[P.ns_group].rows), kThreads, 0, h->stream>>>(
             P, h->group_init[P.ns_group].digest, h->ns_logical);
+    if (h->M.n > 0) macro_init_kernel<<<1, h->macro_threads, 0, h->stream>>>(h->M, h->macro_y0);
     CUDA_TRY(h, cudaGetLastError());
     status = check_device_error(h);
     if (status) return status;
     h->initialized = true;
+    return MIND_OK;
+}
+
+int mind_attach_macro(MindHandle *h, const MindMacroLayout *L) {
+    if (!h || !L) return MIND_EARG;
+    if (h->M.n > 0) return fail(h, MIND_EARG, "regions are already attached");
+    const int32_t n = L->n_regions;
+    if (n < 1 || n > 1024) return fail(h, MIND_ELAYOUT, "region count must be in [1, 1024]");
+    if (!L->params || !L->y0 || !L->micro_gain) return fail(h, MIND_ELAYOUT, "missing region arrays");
+    const double spm_f = L->dt_macro / h->dt, mpb_f = L->bin_ms / L->dt_macro;
+    const int32_t spm = (int32_t)std::llround(spm_f), mpb = (int32_t)std::llround(mpb_f);
+    if (spm < 1 || std::fabs(spm_f - spm) > 1e-9 * spm || mpb < 1 || std::fabs(mpb_f - mpb) > 1e-9 * mpb)
+        return fail(h, MIND_ELAYOUT, "dt_macro must be a multiple of dt and bin_ms of dt_macro");
+    const int32_t bin_steps = spm * mpb;
+    // Region inputs are planned per window on the device, like NetStims: only cell
+    // detectors and the other external inputs bound the window.
+    std::vector<uint8_t> is_input(h->n_sources, 0);
+    for (int64_t q = 0; q < L->n_inputs; ++q)
+        if (L->input_source[q] >= 1 && L->input_source[q] <= h->n_sources) is_input[L->input_source[q] - 1] = 1;
+    double min_delay = INFINITY;
+    for (int64_t s = 0; s < h->n_sources; ++s)
+        if (h->source_detector[s] || (h->source_external[s] && !is_input[s]))
+            for (int64_t e = h->fanout[s]; e < h->fanout[s + 1]; ++e) min_delay = std::min(min_delay, h->edge_delay[e]);
+    const int32_t base_window = window_for_delay(min_delay, h->dt);
+    // the window: the longest divisor of the bin that is a multiple of the macro step
+    int32_t window = 0;
+    for (int32_t w = spm; w <= std::min(base_window, bin_steps); w += spm)
+        if (bin_steps % w == 0) window = w;
+    if (window == 0)
+        return fail(h, MIND_ELAYOUT, "the shortest NetCon delay out of a cell is shorter than a macro step");
+    std::vector<int32_t> order(L->n_edges), in_off(n + 1, 0), e_src, e_delay;
+    std::vector<double> e_gain;
+    int32_t max_delay = 1;
+    for (int64_t e = 0; e < L->n_edges; ++e) {
+        if (L->edge_src[e] < 1 || L->edge_src[e] > n || L->edge_dst[e] < 1 || L->edge_dst[e] > n ||
+            L->edge_delay[e] < 1 || !std::isfinite(L->edge_gain[e]))
+            return fail(h, MIND_ELAYOUT, "region edge out of range (delays are >= 1 macro step)");
+        order[e] = (int32_t)e;
+        in_off[L->edge_dst[e]]++;
+        max_delay = std::max(max_delay, L->edge_delay[e]);
+    }
+    for (int32_t i = 0; i < n; ++i) in_off[i + 1] += in_off[i];
+    std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) { return L->edge_dst[x] < L->edge_dst[y]; });
+    for (int32_t e : order) {
+        e_src.push_back(L->edge_src[e] - 1);
+        e_gain.push_back(L->edge_gain[e]);
+        e_delay.push_back(L->edge_delay[e]);
+    }
+    std::vector<int32_t> inp_region(L->n_inputs), inp_source(L->n_inputs);
+    std::vector<double> inp_scale(L->n_inputs);
+    for (int64_t q = 0; q < L->n_inputs; ++q) {
+        const int64_t s = L->input_source[q];
+        if (L->input_region[q] < 1 || L->input_region[q] > n || s < 1 || s > h->n_sources || !h->source_external[s - 1])
+            return fail(h, MIND_ELAYOUT, "region input must name a region and an external spike input");
+        if (!(L->input_scale[q] >= 0.0)) return fail(h, MIND_ELAYOUT, "region input scale must be >= 0");
+        inp_region[q] = L->input_region[q] - 1;
+        inp_source[q] = (int32_t)(s - 1);
+        inp_scale[q] = L->input_scale[q];
+    }
+    std::vector<int32_t> source_region(h->n_sources, -1);
+    std::vector<double> cells(n, 0.0);
+    for (int64_t q = 0; q < L->n_outputs; ++q) {
+        const int64_t s = L->output_source[q];
+        if (L->output_region[q] < 1 || L->output_region[q] > n || s < 1 || s > h->n_sources || !h->source_detector[s - 1] ||
+            source_region[s - 1] >= 0)
+            return fail(h, MIND_ELAYOUT, "region output must name a region and a detector source, once");
+        source_region[s - 1] = L->output_region[q] - 1;
+        cells[L->output_region[q] - 1] += 1.0;
+    }
+    for (int32_t i = 0; i < n; ++i)
+        if (L->micro_gain[i] != 0.0 && cells[i] == 0.0)
+            return fail(h, MIND_ELAYOUT, "a region with a micro gain has no detector sources");
+    for (int32_t i = 0; i < n; ++i)
+        if (cells[i] == 0.0) cells[i] = 1.0;   // rate of an empty population: 0 / 1
+    try {
+        MacroParams &M = h->M;
+        M.steps_per_macro = spm;
+        M.macro_per_bin = mpb;
+        M.hist_cap = max_delay + 2;
+        M.bin_ring = 4;
+        M.dt_ms = L->dt_macro;
+        M.dt_s = L->dt_macro * 1e-3;
+        M.bin_s = L->bin_ms * 1e-3;
+        M.seed = h->P.seed;
+        M.par = h->upload(std::vector<double>(L->params, L->params + (size_t)n * 9));
+        M.y = h->alloc<double>((size_t)n * 6);
+        h->macro_y0 = h->upload(std::vector<double>(L->y0, L->y0 + (size_t)n * 6));
+        M.micro_gain = h->upload(std::vector<double>(L->micro_gain, L->micro_gain + n));
+        M.cells = h->upload(cells);
+        M.hist = h->alloc<double>((size_t)M.hist_cap * n);
+        M.bins = h->alloc<int32_t>((size_t)M.bin_ring * n);
+        M.in_off = h->upload(in_off);
+        M.e_src = h->upload(e_src);
+        M.e_gain = h->upload(e_gain);
+        M.e_delay = h->upload(e_delay);
+        M.n_inputs = L->n_inputs;
+        M.inp_region = h->upload(inp_region);
+        M.inp_source = h->upload(inp_source);
+        M.inp_scale = h->upload(inp_scale);
+        M.source_region = h->upload(source_region);
+        M.trace = nullptr;
+        M.n = n;
+    } catch (const std::bad_alloc &) {
+        h->M.n = 0;
+        return fail(h, MIND_ECUDA, "device allocation failed");
+    }
+    h->bin_steps = bin_steps;
+    h->window = window;
+    h->macro_threads = ((n + 31) / 32) * 32;
+    h->initialized = false;
+    return MIND_OK;
+}
+
+int mind_get_macro_trace(const MindHandle *h, double *out, int64_t n, int64_t *samples) {
+    if (!h) return MIND_EARG;
+    if (samples) *samples = h->macro_trace_samples;
+    if (n == 0) return MIND_OK;
+    if (n != (int64_t)h->macro_trace.size() || !out) return MIND_EARG;
+    std::memcpy(out, h->macro_trace.data(), n * sizeof(double));
     return MIND_OK;
 }
 
@@ -954,12 +1141,17 @@ int mind_run(MindHandle *h, int64_t steps, const MindRecord *records, int32_t n_
     if (steps < 0 || n_records < 0 || (n_records > 0 && !records)) return fail(h, MIND_EARG, "invalid run arguments");
     int status = set_records(h, records, n_records, steps + 1);
     if (status) return status;
+    status = set_macro_trace(h, steps);
+    if (status) return status;
     status = advance(h, steps, record_spikes != 0);
+    h->M.trace = nullptr;
     if (status) {
         h->initialized = false;
         return status;
     }
-    return collect(h, record_spikes != 0);
+    status = collect(h, record_spikes != 0);
+    if (status) return status;
+    return collect_macro_trace(h);
 }
 
 int mind_step(MindHandle *h) {

@@ -103,6 +103,29 @@ class MindRunStats(Structure):
     ]
 
 
+class MindMacroLayout(Structure):
+    _fields_ = [
+        ("n_regions", c_int32),
+        ("params", POINTER(c_double)),
+        ("y0", POINTER(c_double)),
+        ("micro_gain", POINTER(c_double)),
+        ("n_edges", c_int64),
+        ("edge_src", POINTER(c_int32)),
+        ("edge_dst", POINTER(c_int32)),
+        ("edge_gain", POINTER(c_double)),
+        ("edge_delay", POINTER(c_int32)),
+        ("n_inputs", c_int64),
+        ("input_region", POINTER(c_int32)),
+        ("input_source", POINTER(c_int64)),
+        ("input_scale", POINTER(c_double)),
+        ("n_outputs", c_int64),
+        ("output_region", POINTER(c_int32)),
+        ("output_source", POINTER(c_int64)),
+        ("dt_macro", c_double),
+        ("bin_ms", c_double),
+    ]
+
+
 class MindError(RuntimeError):
     """A non-zero status from libmindgpu, with the library's message."""
 
@@ -150,10 +173,13 @@ def load_library():
     lib.mind_run_noalloc.argtypes = [handle, c_int64, POINTER(MindRecord), c_int32, POINTER(c_double)]
     lib.mind_inject_spikes.argtypes = [handle, c_int64, POINTER(c_int64), POINTER(c_double)]
     lib.mind_window_steps.argtypes = [handle, POINTER(c_int32)]
+    lib.mind_attach_macro.argtypes = [handle, POINTER(MindMacroLayout)]
+    lib.mind_get_macro_trace.argtypes = [handle, POINTER(c_double), c_int64, POINTER(c_int64)]
     for name in ("mind_create", "mind_initialize", "mind_set_precision", "mind_run", "mind_step",
                  "mind_time", "mind_get_trace", "mind_get_spikes", "mind_read_voltage",
                  "mind_inject_event", "mind_last_run_ms", "mind_destroy", "mind_run_stats",
-                 "mind_set_profiling", "mind_run_noalloc", "mind_inject_spikes", "mind_window_steps"):
+                 "mind_set_profiling", "mind_run_noalloc", "mind_inject_spikes", "mind_window_steps",
+                 "mind_attach_macro", "mind_get_macro_trace"):
         getattr(lib, name).restype = c_int32
     _LIB = lib
     return lib
@@ -163,7 +189,7 @@ EXPORTED_SYMBOLS = (
     "mind_create", "mind_initialize", "mind_set_precision", "mind_run", "mind_step", "mind_time",
     "mind_get_trace", "mind_get_spikes", "mind_read_voltage", "mind_inject_event",
     "mind_last_error", "mind_last_run_ms", "mind_destroy", "mind_run_stats", "mind_set_profiling",
-    "mind_run_noalloc", "mind_inject_spikes", "mind_window_steps",
+    "mind_run_noalloc", "mind_inject_spikes", "mind_window_steps", "mind_attach_macro", "mind_get_macro_trace",
 )
 
 MIND_NOALLOC_SCRATCH_BYTES = 16 << 20

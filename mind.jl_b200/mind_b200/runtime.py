@@ -34,6 +34,7 @@ class SimulationResult:
     spike_times: np.ndarray = field(default_factory=lambda: np.zeros(0))
     spike_sources: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
     device_ms: float = 0.0
+    macro_trace: np.ndarray = None   # [macro boundaries, regions] region outputs, when regions are attached
 
 
 class DeviceState:
@@ -50,6 +51,12 @@ class DeviceState:
             raise abi.MindError(status, message.decode() if message else "")
         self.handle = handle
         self.set_precision(precision)
+
+    def attach_macro(self, macro) -> None:
+        """mind_attach_macro: regions and coupling (mind_b200.macro.MacroModel); before initialize."""
+        c = macro.to_c()
+        abi.check(self.lib, self.handle, self.lib.mind_attach_macro(self.handle, ctypes.byref(c)))
+        self.n_regions = macro.n_regions
 
     def set_precision(self, precision: str) -> None:
         mode = {"fp64": abi.MIND_FP64, "mixed": abi.MIND_MIXED}[precision]
@@ -89,6 +96,14 @@ class DeviceState:
         abi.check(self.lib, self.handle, self.lib.mind_last_run_ms(self.handle, ctypes.byref(ms)))
         time = np.arange(start_step, start_step + samples, dtype=np.float64) * self.layout.dt
         result = SimulationResult(time, {}, times, sids, ms.value)
+        if getattr(self, "n_regions", 0):
+            samples = ctypes.c_int64()
+            abi.check(self.lib, self.handle, self.lib.mind_get_macro_trace(self.handle, None, 0, ctypes.byref(samples)))
+            mt = np.zeros((samples.value, self.n_regions))
+            if mt.size:
+                abi.check(self.lib, self.handle, self.lib.mind_get_macro_trace(
+                    self.handle, mt.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), mt.size, ctypes.byref(samples)))
+            result.macro_trace = mt
         for i, r in enumerate(records):
             result.traces[r.name] = trace[:, i].copy()
         return result
@@ -146,6 +161,9 @@ def initialize(model, precision: str = "fp64"):
         raise ValueError("model is not built")
     if model.state is None:
         model.state = DeviceState(model.layout, precision)
+        macro = getattr(model, "macro", None)
+        if macro is not None:
+            model.state.attach_macro(macro)
     else:
         model.state.set_precision(precision)
     model.state.initialize()

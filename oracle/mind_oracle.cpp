@@ -114,6 +114,115 @@ struct Oracle {
     std::vector<int64_t> spike_sid;
     std::vector<int64_t> point_source;  // per point (0-based) -> source index (0-based) or -1
 
+    // ---- regions (mind_attach_macro's specification in include/mindgpu.h) ----
+    const MindMacroLayout *ML = nullptr;
+    int32_t spm = 0, mpb = 0, bin_steps = 0;
+    std::vector<double> ry;                       // [n][6]
+    std::vector<std::vector<double>> out_hist;    // out(k) per macro step
+    std::vector<std::vector<int64_t>> bin_count;  // spikes per rate bin and region
+    std::vector<int32_t> source_region;           // detector source -> region or -1
+    std::vector<double> region_cells;
+    std::vector<std::vector<int64_t>> edges_in;   // per region: edge indices into it, in edge order
+
+    int load_macro(const MindMacroLayout *M) {
+        ML = M;
+        spm = (int32_t)std::llround(M->dt_macro / dt);
+        mpb = (int32_t)std::llround(M->bin_ms / M->dt_macro);
+        bin_steps = spm * mpb;
+        const int32_t nr = M->n_regions;
+        ry.assign(M->y0, M->y0 + (size_t)nr * 6);
+        source_region.assign(L->n_sources, -1);
+        region_cells.assign(nr, 0.0);
+        for (int64_t q = 0; q < M->n_outputs; ++q) {
+            source_region[M->output_source[q] - 1] = M->output_region[q] - 1;
+            region_cells[M->output_region[q] - 1] += 1.0;
+        }
+        for (auto &c : region_cells)
+            if (c == 0.0) c = 1.0;
+        edges_in.assign(nr, {});
+        for (int64_t e = 0; e < M->n_edges; ++e) edges_in[M->edge_dst[e] - 1].push_back(e);
+        std::vector<double> out0(nr);
+        for (int32_t i = 0; i < nr; ++i) out0[i] = region_output(&ry[(size_t)i * 6], M->params + (size_t)i * 9);
+        out_hist.assign(1, out0);
+        return 0;
+    }
+
+    static double sigmoid(double v, double e0, double r, double v0) {
+        return (2.0 * e0) / (1.0 + mind_exp(r * (v0 - v)));
+    }
+    static double region_output(const double *y, const double *par) { return sigmoid(y[1] - y[2], par[4], par[5], par[6]); }
+    static void region_rhs(const double *y, double p, const double *par, double *dy) {
+        const double A = par[0], B = par[1], a = par[2], b = par[3], e0 = par[4], r = par[5], v0 = par[6], C = par[7];
+        dy[0] = y[3];
+        dy[1] = y[4];
+        dy[2] = y[5];
+        dy[3] = ((A * a) * sigmoid(y[1] - y[2], e0, r, v0) - (2.0 * a) * y[3]) - (a * a) * y[0];
+        dy[4] = ((A * a) * (p + (0.8 * C) * sigmoid(C * y[0], e0, r, v0)) - (2.0 * a) * y[4]) - (a * a) * y[1];
+        dy[5] = ((B * b) * ((0.25 * C) * sigmoid((0.25 * C) * y[0], e0, r, v0)) - (2.0 * b) * y[5]) - (b * b) * y[2];
+    }
+    static void region_rk4(double *y, double p, const double *par, double h) {
+        double k1[6], k2[6], k3[6], k4[6], t[6];
+        region_rhs(y, p, par, k1);
+        for (int j = 0; j < 6; ++j) t[j] = y[j] + (0.5 * h) * k1[j];
+        region_rhs(t, p, par, k2);
+        for (int j = 0; j < 6; ++j) t[j] = y[j] + (0.5 * h) * k2[j];
+        region_rhs(t, p, par, k3);
+        for (int j = 0; j < 6; ++j) t[j] = y[j] + h * k3[j];
+        region_rhs(t, p, par, k4);
+        const double w = h / 6.0;
+        for (int j = 0; j < 6; ++j) y[j] = y[j] + w * (((k1[j] + 2.0 * k2[j]) + 2.0 * k3[j]) + k4[j]);
+    }
+
+    /* Macro step k begins: advance every region over it, then queue its input spikes. */
+    void macro_step(int64_t k) {
+        const int32_t nr = ML->n_regions;
+        const double dt_s = ML->dt_macro * 1e-3, bin_s = ML->bin_ms * 1e-3;
+        std::vector<double> next(nr);
+        for (int32_t i = 0; i < nr; ++i) {
+            const double *par = ML->params + (size_t)i * 9;
+            const int64_t b = k / mpb - 1;
+            double rate = 0.0;
+            if (b >= 0 && b < (int64_t)bin_count.size()) rate = (double)bin_count[b][i] / (region_cells[i] * bin_s);
+            double p = par[8] + ML->micro_gain[i] * rate;
+            for (int64_t e : edges_in[i]) {
+                int64_t m = k - ML->edge_delay[e];
+                if (m < 0) m = 0;
+                p = p + ML->edge_gain[e] * out_hist[m][ML->edge_src[e] - 1];
+            }
+            region_rk4(&ry[(size_t)i * 6], p, par, dt_s);
+            next[i] = region_output(&ry[(size_t)i * 6], par);
+        }
+        // inputs over [k dt_macro, (k+1) dt_macro) from out(k)
+        for (int64_t q = 0; q < ML->n_inputs; ++q) {
+            const double out = out_hist[k][ML->input_region[q] - 1];
+            const double mu = (ML->input_scale[q] * out) * dt_s;
+            uint32_t ctr[4] = {(uint32_t)k, (uint32_t)((uint64_t)k >> 32), (uint32_t)q, 0x4D4Du};
+            mind_philox4x32_10(ctr, (uint32_t)seed, (uint32_t)(seed >> 32));
+            const double u0 = ((double)ctr[0] + 1.0) * MIND_INV_2P32P1;
+            double pr = mind_exp(-mu), F = pr;
+            int count = 0;
+            while (u0 > F && count < 3) {
+                ++count;
+                pr = (pr * mu) / (double)count;
+                F = F + pr;
+            }
+            const int64_t source = ML->input_source[q] - 1;
+            for (int j = 0; j < count; ++j) {
+                const double t = (double)k * ML->dt_macro + ML->dt_macro * (((double)ctr[1 + j] + 1.0) * MIND_INV_2P32P1);
+                for (int64_t e = L->fanout_offsets[source] - 1; e < L->fanout_offsets[source + 1] - 1; ++e)
+                    enqueue(t + L->edge_delays[e], 0.0, e + 1, L->edge_targets[e]);
+            }
+        }
+        out_hist.push_back(next);
+    }
+
+    void count_spike(int64_t source) {
+        if (!ML || source_region[source] < 0) return;
+        const int64_t b = step / bin_steps;
+        while ((int64_t)bin_count.size() <= b) bin_count.emplace_back(ML->n_regions, 0);
+        bin_count[b][source_region[source]] += 1;
+    }
+
     int fail(int code, const std::string &why) {
         if (!error) {
             error = code;
@@ -510,13 +619,17 @@ struct Oracle {
             int32_t node = L->source_nodes[s];
             if (node <= 0) continue;
             bool current = v[node - 1] > L->source_thresholds[s];
-            if (current && !above[s]) emit_spike(s, time);
+            if (current && !above[s]) {
+                emit_spike(s, time);
+                count_spike(s);
+            }
             above[s] = current;
         }
     }
 
     int advance_step(int threads) {
         double t = (double)step * dt;
+        if (ML && step % spm == 0) macro_step(step / spm);
         detect(t);
         deliver(t + 0.5 * dt);
         currents(t + 0.5 * dt);
@@ -560,13 +673,15 @@ struct Oracle {
 
 extern "C" {
 
-/* Initialize from the layout and run `steps` micro steps.  trace is
- * [(steps+1) x nrec] sample-major; spikes sorted by (time, sid). */
-int oracle_run(const MindLayout *layout, int64_t steps, const MindRecord *records, int32_t nrec,
-               int32_t threads, double *trace, double *spike_t, int64_t *spike_sid, int64_t cap,
-               int64_t *nspikes, double *run_ms, char *message, int32_t message_len) {
+/* Initialize from the layout (and regions, if `macro` is given) and run `steps` micro
+ * steps.  trace is [(steps+1) x nrec] sample-major; spikes sorted by (time, sid);
+ * macro_trace is [(steps / steps per macro step + 1) x regions] region outputs. */
+int oracle_run_macro(const MindLayout *layout, const MindMacroLayout *macro, int64_t steps, const MindRecord *records,
+                     int32_t nrec, int32_t threads, double *trace, double *spike_t, int64_t *spike_sid, int64_t cap,
+                     int64_t *nspikes, double *macro_trace, double *run_ms, char *message, int32_t message_len) {
     Oracle o;
     int status = o.load(layout);
+    if (!status && macro) status = o.load_macro(macro);
     if (!status) {
         o.build_row_points();
         o.initialize();
@@ -592,6 +707,13 @@ int oracle_run(const MindLayout *layout, int64_t steps, const MindRecord *record
         for (int64_t i = 0; i < o.n; ++i)
             if (!std::isfinite(o.v[i])) status = o.fail(MIND_ENONFINITE, "non-finite voltage");
     }
+    if (!status && macro && macro_trace) {
+        // out(k) for k = 0 .. steps / spm; the last boundary's out needs macro step k-1 done
+        const int64_t last = steps / o.spm;
+        while ((int64_t)o.out_hist.size() <= last) o.macro_step((int64_t)o.out_hist.size() - 1);
+        for (int64_t k = 0; k <= last; ++k)
+            for (int32_t i = 0; i < macro->n_regions; ++i) macro_trace[k * macro->n_regions + i] = o.out_hist[k][i];
+    }
     std::vector<int64_t> idx(o.spike_t.size());
     for (size_t i = 0; i < idx.size(); ++i) idx[i] = (int64_t)i;
     std::stable_sort(idx.begin(), idx.end(), [&](int64_t x, int64_t y) {
@@ -610,6 +732,13 @@ int oracle_run(const MindLayout *layout, int64_t steps, const MindRecord *record
     return status;
 }
 
+int oracle_run(const MindLayout *layout, int64_t steps, const MindRecord *records, int32_t nrec,
+               int32_t threads, double *trace, double *spike_t, int64_t *spike_sid, int64_t cap,
+               int64_t *nspikes, double *run_ms, char *message, int32_t message_len) {
+    return oracle_run_macro(layout, nullptr, steps, records, nrec, threads, trace, spike_t, spike_sid, cap, nspikes,
+                            nullptr, run_ms, message, message_len);
+}
+
 }  // extern "C"
 
 extern "C" {
@@ -624,6 +753,21 @@ void oracle_div_milli(const double *x, double *out, int64_t n) {
     for (int64_t i = 0; i < n; ++i) out[i] = mind_div_milli(x[i]);
 }
 void oracle_philox(uint32_t *ctr, uint32_t key0, uint32_t key1) { mind_philox4x32_10(ctr, key0, key1); }
+
+/* The region inputs' per-step Poisson counts (the rule of mind_attach_macro), for statistics tests. */
+int32_t oracle_region_input_count(uint64_t seed, int64_t input, int64_t k, double mu) {
+    uint32_t ctr[4] = {(uint32_t)k, (uint32_t)((uint64_t)k >> 32), (uint32_t)input, 0x4D4Du};
+    mind_philox4x32_10(ctr, (uint32_t)seed, (uint32_t)(seed >> 32));
+    const double u0 = ((double)ctr[0] + 1.0) * MIND_INV_2P32P1;
+    double p = mind_exp(-mu), F = p;
+    int32_t n = 0;
+    while (u0 > F && n < 3) {
+        ++n;
+        p = (p * mu) / (double)n;
+        F = F + p;
+    }
+    return n;
+}
 
 /* One random stream in the nrnran123 layout: `n` negexp draws from a fresh
  * stream keyed by (logical id, digest, stream 0, seed). */

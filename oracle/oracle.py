@@ -36,6 +36,15 @@ def _load():
             ctypes.POINTER(ctypes.c_int64), ctypes.c_int64, ctypes.POINTER(ctypes.c_int64),
             ctypes.POINTER(ctypes.c_double), ctypes.c_char_p, ctypes.c_int32,
         ]
+        lib.oracle_run_macro.restype = ctypes.c_int32
+        lib.oracle_run_macro.argtypes = [
+            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
+            ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+            ctypes.POINTER(ctypes.c_int64), ctypes.c_int64, ctypes.POINTER(ctypes.c_int64),
+            ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), ctypes.c_char_p, ctypes.c_int32,
+        ]
+        lib.oracle_region_input_count.restype = ctypes.c_int32
+        lib.oracle_region_input_count.argtypes = [ctypes.c_uint64, ctypes.c_int64, ctypes.c_int64, ctypes.c_double]
         lib.oracle_exp.restype = ctypes.c_double
         lib.oracle_exp.argtypes = [ctypes.c_double]
         lib.oracle_log.restype = ctypes.c_double
@@ -75,6 +84,10 @@ def div_milli(x):
     return out
 
 
+def region_input_count(seed: int, input_index: int, k: int, mu: float) -> int:
+    return _load().oracle_region_input_count(seed, input_index, k, mu)
+
+
 def philox4x32_10(ctr, key0: int, key1: int):
     words = (ctypes.c_uint32 * 4)(*ctr)
     _load().oracle_philox(words, key0, key1)
@@ -95,10 +108,12 @@ class OracleResult:
     spike_times: np.ndarray
     spike_sids: np.ndarray
     run_ms: float
+    macro_trace: np.ndarray = None   # [macro boundaries, regions], with regions
 
 
-def run(layout, steps: int, record_nodes=(), threads: int = 1, spike_cap: int = 1 << 22) -> OracleResult:
-    """Initialize the layout on the CPU and advance `steps` micro steps."""
+def run(layout, steps: int, record_nodes=(), threads: int = 1, spike_cap: int = 1 << 22, macro=None) -> OracleResult:
+    """Initialize the layout (and the regions of `macro`, a MacroModel) on the CPU and advance
+    `steps` micro steps; with regions, `macro_trace` holds out(k) for k = 0 .. steps / (dt_macro/dt)."""
     import sys
 
     pkg = os.path.join(os.path.dirname(HERE), "mind.jl_b200")
@@ -119,12 +134,21 @@ def run(layout, steps: int, record_nodes=(), threads: int = 1, spike_cap: int = 
     count = ctypes.c_int64()
     ms = ctypes.c_double()
     message = ctypes.create_string_buffer(256)
-    status = lib.oracle_run(
-        ctypes.addressof(c_layout), steps, ctypes.addressof(recs), len(nodes), threads,
+    c_macro = macro.to_c() if macro is not None else None
+    macro_trace = None
+    if macro is not None:
+        spm = int(round(macro.dt_macro / layout.dt))
+        macro_trace = np.zeros((steps // spm + 1, macro.n_regions))
+    status = lib.oracle_run_macro(
+        ctypes.addressof(c_layout), ctypes.addressof(c_macro) if c_macro is not None else None, steps,
+        ctypes.addressof(recs), len(nodes), threads,
         trace.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
         spike_t.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
         spike_sid.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), spike_cap, ctypes.byref(count),
+        macro_trace.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if macro_trace is not None else None,
         ctypes.byref(ms), message, 256)
     n = min(count.value, spike_cap)
-    return OracleResult(status, message.value.decode(), trace[:, :len(nodes)],
-                        spike_t[:n].copy(), spike_sid[:n].copy(), ms.value)
+    result = OracleResult(status, message.value.decode(), trace[:, :len(nodes)],
+                          spike_t[:n].copy(), spike_sid[:n].copy(), ms.value)
+    result.macro_trace = macro_trace
+    return result

@@ -57,3 +57,50 @@ def recurrent_trees(n_cells=24, synapses=20, seed=7, min_delay=0.6):
 
 def soma_nodes(layout):
     return [layout.voltage_node(c) for c in range(1, layout.n_cells + 1)]
+
+
+def coupled_regions(n_regions=3, cells_per_region=4, synapses=8, seed=11, input_scale=300.0):
+    """Ball-and-stick populations coupled to Jansen-Rit regions (config 4 in miniature).
+
+    Every synapse (Exp2Syn) gets its own external spike input driven by its population's
+    region; every cell's soma detector feeds the region's rate bin; regions are coupled by
+    random edges with delays of 1-5 macro steps; recurrent NetCons between cells (0.6-2 ms).
+    Returns (model, macro) with model built.
+    """
+    from mind_b200.macro import MacroModel
+
+    rng = np.random.default_rng(seed)
+    model = M.MicroModel(celsius=6.3)
+    soma = mb.Section("soma", label="soma", length=20.0, diameter=20.0, nseg=1)
+    dend = mb.Section("dend", label="dend", parent="soma", parent_x=1.0, length=300.0, diameter=2.0, nseg=15)
+    n_cells = n_regions * cells_per_region
+    cells = M.add_population(model, [soma, dend], n_cells, voltage=-65.0)
+    detectors = []
+    for cell in cells:
+        M.insert(cell, mb.builtin("hh"), sections="soma")
+        M.insert(cell, mb.builtin("pas"), sections="dend", params={"g": 1e-4, "e": -65.0})
+        detectors.append(M.register_spike_source(cell, threshold=-10.0).index)
+    n = n_cells * synapses
+    owners = np.repeat(np.arange(1, n_cells + 1), synapses)
+    first = M.add_pointprocesses(model, mb.builtin("Exp2Syn"), owners, "dend", rng.uniform(0, 1, n),
+                                 {"tau1": 0.5, "tau2": 5.0, "e": np.where(rng.uniform(size=n) < 0.8, 0.0, -80.0)})
+    inputs = [M.register_spike_source(model).index for _ in range(n)]
+    M.connect_many(model, inputs, np.arange(first, first + n), rng.lognormal(math.log(4.0), 0.4, n) / 1000.0,
+                   np.zeros(n))
+    k = n // 4
+    M.connect_many(model, rng.choice(detectors, k), rng.integers(first, first + n, k),
+                   rng.lognormal(math.log(2.0), 0.4, k) / 1000.0, rng.uniform(0.6, 2.0, k))
+    macro = MacroModel(dt_macro=0.1, bin_ms=1.0)
+    for r in range(n_regions):
+        macro.add_region(micro_gain=2.0, y0=[0.0, rng.uniform(0, 5), rng.uniform(0, 5), 0.0, 0.0, 0.0])
+    for src in range(1, n_regions + 1):
+        for dst in range(1, n_regions + 1):
+            if src != dst and rng.uniform() < 0.5:
+                macro.connect(src, dst, float(rng.uniform(0, 1)) * 50.0, int(rng.integers(1, 6)))
+    for c in range(n_cells):
+        region = c // cells_per_region + 1
+        macro.add_inputs(region, inputs[c * synapses:(c + 1) * synapses], input_scale)
+        macro.add_outputs(region, [detectors[c]])
+    model.macro = macro
+    mb.build(model)
+    return model, macro
