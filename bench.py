@@ -49,8 +49,9 @@ def parse():
     p.add_argument("--warmup", type=int, default=40)
     p.add_argument("--impl", default="mine", choices=["mine", "reference"])
     p.add_argument("--cells", type=int, default=None, help="cells (default: the configuration's count)")
-    p.add_argument("--config", type=int, default=2, choices=[2, 3],
-                   help="2: 10,000 uneven binary-tree cells (the headline); 3: 1,000 pyramidal-like cells")
+    p.add_argument("--config", type=int, default=2, choices=[2, 3, 4],
+                   help="2: 10,000 uneven binary-tree cells (the headline); 3: 1,000 pyramidal-like cells; "
+                        "4: 2,000 pyramidal-like cells coupled to 20 Jansen-Rit regions")
     p.add_argument("--precision", default="both", choices=["fp64", "mixed", "both"],
                    help="both: the FP64 headline plus the mixed mode and its accuracy against FP64")
     p.add_argument("--accuracy-ms", type=float, default=0.0,
@@ -66,7 +67,9 @@ def build_network(cells, seed: int, config: int = 2, rank: int = 0, world: int =
     import mind_b200 as mb
     from mind_b200 import networks
 
-    if config == 3:
+    if config == 4:
+        model = networks.config4(n_cells=cells or 2000)
+    elif config == 3:
         model = networks.config3(n_cells=cells or 1000)
     else:
         model = networks.config2(n_cells=cells or 10000, rank=rank, world=world)

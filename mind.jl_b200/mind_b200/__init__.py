@@ -9,7 +9,7 @@ from .mechanisms import Mechanism, builtin
 from .morphology import Point3D, Section, discretize, location_node
 from .model import (Cell, IonSpecies, MicroModel, PointProcess, Population, SpikeSource,
                     add_pointprocess, add_pointprocesses, add_population, connect, connect_many,
-                    insert, register_point_sources, register_spike_source, spike_source)
+                    insert, register_external_sources, register_point_sources, register_spike_source, spike_source)
 from .layout import Layout, build
 from .runtime import (RecordSpec, SimulationResult, initialize, inject_spike, run, simulation_time, step,
                       voltage_record)
@@ -18,7 +18,7 @@ __all__ = [
     "Mechanism", "builtin", "Point3D", "Section", "discretize", "location_node", "Cell",
     "IonSpecies", "MicroModel", "PointProcess", "Population", "SpikeSource", "add_pointprocess",
     "add_pointprocesses", "add_population", "connect", "connect_many", "insert",
-    "register_point_sources", "register_spike_source", "spike_source", "Layout", "build",
+    "register_external_sources", "register_point_sources", "register_spike_source", "spike_source", "Layout", "build",
     "RecordSpec", "SimulationResult", "initialize", "inject_spike", "run", "simulation_time", "step",
     "voltage_record",
 ]

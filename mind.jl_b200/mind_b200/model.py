@@ -321,6 +321,14 @@ def register_spike_source(source: Union[Cell, PointProcess, "MicroModel"], *, si
     return SpikeSource(model, index, identity)
 
 
+def register_external_sources(model: MicroModel, count: int) -> np.ndarray:
+    """Bulk register_spike_source!(model): `count` external spike inputs; returns their indices."""
+    ids = np.arange(model.next_source_id, model.next_source_id + int(count), dtype=np.int64)
+    first = _append_sources(model, ids, np.zeros(len(ids), np.int64), "none", np.zeros(len(ids)),
+                            np.zeros(len(ids), np.int64), np.zeros(len(ids)))
+    return np.arange(first, first + len(ids), dtype=np.int64)
+
+
 def register_point_sources(model: MicroModel, points, sids=None) -> np.ndarray:
     """Bulk: register net_event sources for 1-based point indices; returns source indices.
 

@@ -282,7 +282,82 @@ def config3(n_cells: int = 1000, synapses_per_cell: int = 300, connectivity: flo
     return model
 
 
-CONFIGS = {1: config1, 2: config2, 3: config3}
+def config4(n_cells: int = 2000, populations: int = 20, synapses_per_cell: int = 300, connectivity: float = 0.03,
+            input_scale: float = 2.0, micro_gain: float = 1.0, iclamp_onset: float = 100.0) -> M.MicroModel:
+    """Micro-macro coupling: 2,000 pyramidal-like cells (300-600 compartments) in 20
+    populations of 100, each population coupled to a Jansen-Rit region.
+
+    Cells, synapses, recurrent NetCons and IClamps follow config 3 (hh soma and proximal,
+    pas elsewhere; 300 Exp2Syn; 3% recurrence, delays U[0.5,3] ms), except that the
+    synapses are driven by their population's region instead of NetStims: every synapse has
+    its own external spike input (NetCon delay 0, weight lognormal(ln 0.3 nS, 0.7)) firing as
+    a Poisson process at `input_scale` x the region's output (s^-1 -> Hz).  Regions: the
+    Jansen-Rit defaults of mind_b200.macro (A 3.25 mV, B 22 mV, a 100 /s, b 50 /s, e0 2.5 /s,
+    r 0.56 /mV, v0 6 mV, C 135, p0 120 /s), states from 0; region input += `micro_gain` x
+    the population's spike rate (Hz per cell, 1 ms bins); a random region graph of density
+    0.2 with gains U[0,1] and delays of U{1..20} macro steps (0.1-2 ms, a choice: the
+    configuration leaves delays open); RK4 at dt_macro = 0.1 ms.  The model's `macro`
+    attribute holds the MacroModel.
+    """
+    from .macro import MacroModel
+
+    rng = _rng(4)
+    model = M.MicroModel(celsius=6.3)
+    targets_n = rng.integers(300, 601, n_cells)
+    morph = []
+    detectors = np.empty(n_cells, dtype=np.int64)
+    for c in range(n_cells):
+        secs = _pyramidal(rng, int(targets_n[c]))
+        cell = M.add_population(model, secs, 1, voltage=-65.0)[0]
+        M.insert(cell, builtin("hh"), sections=["soma", "prox"])
+        M.insert(cell, builtin("pas"), sections=["apical", "basal"], params={"g": 1.0e-4, "e": -65.0})
+        detectors[c] = M.register_spike_source(cell, threshold=-10.0).index
+        morph.append((cell, secs))
+    S = synapses_per_cell
+    n = n_cells * S
+    owners = np.repeat(np.arange(1, n_cells + 1), S)
+    names, xs = [], []
+    n_basal = int(round(0.8 * S))
+    for cell, secs in morph:
+        nb, xb = _dendritic_sites(rng, secs, n_basal, labels=("basal", "prox"))
+        na, xa = _dendritic_sites(rng, secs, S - n_basal, labels=("apical",))
+        names.extend(nb + na)
+        xs.append(np.concatenate([xb, xa]))
+    e_rev = np.where(rng.uniform(size=n) < 0.85, 0.0, -80.0)
+    first_syn = M.add_pointprocesses(model, builtin("Exp2Syn"), owners, names, np.concatenate(xs),
+                                     {"tau1": 0.5, "tau2": 5.0, "e": e_rev})
+    k_in = int(round(connectivity * n_cells))
+    pre, post = [], []
+    for c in range(n_cells):
+        choices = rng.choice(n_cells - 1, size=k_in, replace=False)
+        choices = np.where(choices >= c, choices + 1, choices)
+        pre.append(detectors[choices])
+        post.append(first_syn + c * S + rng.integers(0, S, k_in))
+    M.connect_many(model, np.concatenate(pre), np.concatenate(post),
+                   rng.lognormal(math.log(0.3), 0.7, n_cells * k_in) / 1000.0, rng.uniform(0.5, 3.0, n_cells * k_in))
+    inputs = M.register_external_sources(model, n)
+    M.connect_many(model, inputs, np.arange(first_syn, first_syn + n), rng.lognormal(math.log(0.3), 0.7, n) / 1000.0,
+                   np.zeros(n))
+    n_clamp = max(1, n_cells // 10)
+    M.add_pointprocesses(model, builtin("IClamp"), np.arange(1, n_clamp + 1), "soma",
+                         np.full(n_clamp, 0.5), {"del": iclamp_onset, "dur": 50.0, "amp": 0.1})
+    macro = MacroModel(dt_macro=0.1, bin_ms=1.0)
+    for _ in range(populations):
+        macro.add_region(micro_gain=micro_gain)
+    for src in range(1, populations + 1):
+        for dst in range(1, populations + 1):
+            if src != dst and rng.uniform() < 0.2:
+                macro.connect(src, dst, float(rng.uniform(0.0, 1.0)), int(rng.integers(1, 21)))
+    per_pop = n_cells // populations
+    for c in range(n_cells):
+        region = min(c // per_pop, populations - 1) + 1
+        macro.add_inputs(region, inputs[c * S:(c + 1) * S], input_scale)
+        macro.add_outputs(region, [detectors[c]])
+    model.macro = macro
+    return model
+
+
+CONFIGS = {1: config1, 2: config2, 3: config3, 4: config4}
 
 
 def compartment_count(layout) -> int:
