@@ -253,6 +253,42 @@ int mind_attach_macro(MindHandle *h, const MindMacroLayout *macro);
  * floor(end / steps per macro step) - ceil(start / steps per macro step) + 1. */
 int mind_get_macro_trace(const MindHandle *h, double *out, int64_t n, int64_t *samples);
 
+/*
+ * Spike-output surrogate (no counterpart in the reference): a multilayer perceptron
+ * n_in -> hidden (SiLU) x layers -> sigmoid, the probability that a cell spikes in the
+ * next 1 ms bin given its recent synaptic drive and output.  Products run in BF16 with
+ * FP32 accumulation on the tensor cores, parameters and Adam state in FP32.
+ * Parameters: for each linear map in order, W [out x in] row-major then b [out].
+ */
+/* Record, during each mind_run, every cell's synaptic drive: the summed NetCon weights
+ * (uS) of the events its synapses receive, per bin of bin_ms (a multiple of dt) and per
+ * synapse group (the synapse's row within its cell, mod 32) — the surrogate's training
+ * inputs.  bin_ms <= 0 stops recording (no counterpart in the reference). */
+int mind_set_drive_recording(MindHandle *h, double bin_ms);
+/* The last run's drive, [bins][cells][32] (cells in layout order); bins = run steps / bin. */
+int mind_get_drive(const MindHandle *h, float *out, int64_t n, int64_t *bins);
+
+typedef struct MindMlp MindMlp;
+typedef struct {
+    int32_t n_in, hidden, layers;
+    uint64_t seed;                 /* initial weights uniform(+-1/sqrt(fan_in)), zero biases */
+} MindMlpConfig;
+
+int mind_mlp_create(const MindMlpConfig *config, MindMlp **mlp);
+int mind_mlp_destroy(MindMlp *mlp);
+const char *mind_mlp_last_error(const MindMlp *mlp);
+int mind_mlp_param_count(const MindMlp *mlp, int64_t *n);
+int mind_mlp_set_params(MindMlp *mlp, const float *params, int64_t n);
+int mind_mlp_get_params(const MindMlp *mlp, float *params, int64_t n);
+/* prob[k] for the n rows x[k][n_in] (host arrays). */
+int mind_mlp_predict(MindMlp *mlp, const float *x, int64_t n, float *prob);
+/* Gradient of the mean sigmoid cross-entropy over the n rows (targets y in [0, 1]). */
+int mind_mlp_gradients(MindMlp *mlp, const float *x, const float *y, int64_t n, float *grad, float *loss);
+/* Keep a training set on the device; then `steps` Adam steps (beta 0.9/0.999, eps 1e-8) on
+ * batches drawn with replacement; losses[k] = the batch loss before step k (may be NULL). */
+int mind_mlp_set_data(MindMlp *mlp, const float *x, const float *y, int64_t n);
+int mind_mlp_train(MindMlp *mlp, int32_t steps, int32_t batch, float lr, float *losses, float *ms);
+
 /* Message for the last non-zero status of this handle (or of mind_create when h is NULL). */
 const char *mind_last_error(const MindHandle *h);
 

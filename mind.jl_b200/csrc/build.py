@@ -16,8 +16,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 PACKAGE = os.path.dirname(HERE)
 OUT_DIR = os.path.join(PACKAGE, "lib")
 OUTPUT = os.path.join(OUT_DIR, "libmindgpu.so")
-SOURCES = [os.path.join(HERE, "mindgpu.cu")]
-DEPENDS = SOURCES + [os.path.join(HERE, f) for f in ("device.cuh", "kernels.cuh", "mind_math.h")] + [
+SOURCES = [os.path.join(HERE, "mindgpu.cu"), os.path.join(HERE, "surrogate.cu")]
+DEPENDS = SOURCES + [os.path.join(HERE, f) for f in ("device.cuh", "kernels.cuh", "macro.cuh", "mind_math.h")] + [
     os.path.join(os.path.dirname(PACKAGE), "include", "mindgpu.h")]
 
 NVCC_FLAGS = [
@@ -46,7 +46,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if not force and up_to_date():
         return OUTPUT
     os.makedirs(OUT_DIR, exist_ok=True)
-    cmd = [nvcc(), *NVCC_FLAGS, *(["-Xptxas", "-v"] if verbose else []), "-o", OUTPUT, *SOURCES]
+    cmd = [nvcc(), *NVCC_FLAGS, *(["-Xptxas", "-v"] if verbose else []), "-o", OUTPUT, *SOURCES, "-lcublas"]
     result = subprocess.run(cmd, capture_output=True, text=True)
     if result.returncode != 0:
         raise RuntimeError(f"nvcc failed ({result.returncode}):\n{result.stderr}\n{result.stdout}")

@@ -207,6 +207,10 @@ struct Params {
     const int32_t *rec_node;       // local node
     const int32_t *rec_col;
     double *trace;
+    // surrogate training data: synaptic drive [drive_bins][ncells][32] of the run (or null)
+    float *drive;
+    int32_t drive_bin_steps;
+    int64_t drive_bins;
     int32_t nrec;
     int64_t trace_samples;
     int64_t run_start;             // step at sample 0

@@ -798,6 +798,13 @@ __global__ void __launch_bounds__(kCellThreads, 8) window_kernel(const Params P,
                 if (e.bin > step) break;
                 if (e.bin < step) raise_error(P.error, MIND_ESELFEVENT);
                 apply_event(sg[e.point >> 24], e.point & 0xffffff, sw[k]);
+                if (P.drive && e.edge >= 0) {
+                    // synaptic drive for the surrogate's training data: NetCon weight by
+                    // (run bin, cell, synapse row mod 32)
+                    const int64_t b = (step - P.run_start) / P.drive_bin_steps;
+                    if (b < P.drive_bins)
+                        P.drive[(b * P.ncells + c) * 32 + ((e.point & 0xffffff) & 31)] += (float)P.edge_weight[e.edge];
+                }
                 ++cursor;
             }
         }

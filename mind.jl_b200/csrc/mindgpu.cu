@@ -78,6 +78,12 @@ struct MindHandle {
     size_t macro_trace_cap = 0;
     std::vector<double> macro_trace;
     int64_t macro_trace_samples = 0;
+    // synaptic drive recording (mind_set_drive_recording)
+    int32_t drive_bin_steps = 0;
+    float *drive_dev = nullptr;
+    size_t drive_cap = 0;
+    std::vector<float> drive;
+    int64_t drive_bins = 0;
     std::vector<double> v0_packed;
     int64_t n_sources = 0;
     std::vector<int64_t> source_ids;
@@ -910,6 +916,40 @@ int set_macro_trace(MindHandle *h, int64_t steps) {
     return MIND_OK;
 }
 
+/* Zeroed device buffer for the run's synaptic drive bins, when recording is on (mind_run only). */
+int set_drive(MindHandle *h, int64_t steps) {
+    Params &P = h->P;
+    P.drive = nullptr;
+    h->drive_bins = 0;
+    if (h->drive_bin_steps <= 0) return MIND_OK;
+    const int64_t bins = steps / h->drive_bin_steps;
+    if (bins == 0) return MIND_OK;
+    const size_t need = (size_t)bins * h->ncells * 32;
+    if (need > h->drive_cap) {
+        if (h->drive_dev) h->release(h->drive_dev);
+        h->drive_dev = nullptr;
+        try {
+            h->drive_dev = h->alloc<float>(need);
+        } catch (const std::bad_alloc &) {
+            return fail(h, MIND_ECAPACITY, "no device memory for the drive recording");
+        }
+        h->drive_cap = need;
+    }
+    CUDA_TRY(h, cudaMemsetAsync(h->drive_dev, 0, need * sizeof(float), h->stream));
+    P.drive = h->drive_dev;
+    P.drive_bin_steps = h->drive_bin_steps;
+    P.drive_bins = bins;
+    h->drive_bins = bins;
+    return MIND_OK;
+}
+
+int collect_drive(MindHandle *h) {
+    const size_t n = (size_t)h->drive_bins * h->ncells * 32;
+    h->drive.assign(n, 0.0f);
+    if (n) CUDA_TRY(h, cudaMemcpy(h->drive.data(), h->drive_dev, n * sizeof(float), cudaMemcpyDeviceToHost));
+    return MIND_OK;
+}
+
 int collect_macro_trace(MindHandle *h) {
     const size_t n = (size_t)h->macro_trace_samples * h->M.n;
     h->macro_trace.assign(n, 0.0);
@@ -1126,6 +1166,28 @@ int mind_attach_macro(MindHandle *h, const MindMacroLayout *L) {
     return MIND_OK;
 }
 
+int mind_set_drive_recording(MindHandle *h, double bin_ms) {
+    if (!h) return MIND_EARG;
+    if (bin_ms <= 0.0) {
+        h->drive_bin_steps = 0;
+        return MIND_OK;
+    }
+    const double k = bin_ms / h->dt;
+    const int32_t steps = (int32_t)std::llround(k);
+    if (steps < 1 || std::fabs(k - steps) > 1e-9 * steps) return fail(h, MIND_EARG, "bin_ms must be a multiple of dt");
+    h->drive_bin_steps = steps;
+    return MIND_OK;
+}
+
+int mind_get_drive(const MindHandle *h, float *out, int64_t n, int64_t *bins) {
+    if (!h) return MIND_EARG;
+    if (bins) *bins = h->drive_bins;
+    if (n == 0) return MIND_OK;
+    if (n != (int64_t)h->drive.size() || !out) return MIND_EARG;
+    std::memcpy(out, h->drive.data(), n * sizeof(float));
+    return MIND_OK;
+}
+
 int mind_get_macro_trace(const MindHandle *h, double *out, int64_t n, int64_t *samples) {
     if (!h) return MIND_EARG;
     if (samples) *samples = h->macro_trace_samples;
@@ -1143,15 +1205,20 @@ int mind_run(MindHandle *h, int64_t steps, const MindRecord *records, int32_t n_
     if (status) return status;
     status = set_macro_trace(h, steps);
     if (status) return status;
+    status = set_drive(h, steps);
+    if (status) return status;
     status = advance(h, steps, record_spikes != 0);
     h->M.trace = nullptr;
+    h->P.drive = nullptr;
     if (status) {
         h->initialized = false;
         return status;
     }
     status = collect(h, record_spikes != 0);
     if (status) return status;
-    return collect_macro_trace(h);
+    status = collect_macro_trace(h);
+    if (status) return status;
+    return collect_drive(h);
 }
 
 int mind_step(MindHandle *h) {

@@ -126,6 +126,10 @@ class MindMacroLayout(Structure):
     ]
 
 
+class MindMlpConfig(Structure):
+    _fields_ = [("n_in", c_int32), ("hidden", c_int32), ("layers", c_int32), ("seed", c_uint64)]
+
+
 class MindError(RuntimeError):
     """A non-zero status from libmindgpu, with the library's message."""
 
@@ -175,11 +179,28 @@ def load_library():
     lib.mind_window_steps.argtypes = [handle, POINTER(c_int32)]
     lib.mind_attach_macro.argtypes = [handle, POINTER(MindMacroLayout)]
     lib.mind_get_macro_trace.argtypes = [handle, POINTER(c_double), c_int64, POINTER(c_int64)]
+    f32 = POINTER(ctypes.c_float)
+    lib.mind_set_drive_recording.argtypes = [handle, c_double]
+    lib.mind_get_drive.argtypes = [handle, f32, c_int64, POINTER(c_int64)]
+    lib.mind_mlp_create.argtypes = [POINTER(MindMlpConfig), POINTER(handle)]
+    lib.mind_mlp_destroy.argtypes = [handle]
+    lib.mind_mlp_last_error.argtypes = [handle]
+    lib.mind_mlp_last_error.restype = c_char_p
+    lib.mind_mlp_param_count.argtypes = [handle, POINTER(c_int64)]
+    lib.mind_mlp_set_params.argtypes = [handle, f32, c_int64]
+    lib.mind_mlp_get_params.argtypes = [handle, f32, c_int64]
+    lib.mind_mlp_predict.argtypes = [handle, f32, c_int64, f32]
+    lib.mind_mlp_gradients.argtypes = [handle, f32, f32, c_int64, f32, f32]
+    lib.mind_mlp_set_data.argtypes = [handle, f32, f32, c_int64]
+    lib.mind_mlp_train.argtypes = [handle, c_int32, c_int32, ctypes.c_float, f32, f32]
     for name in ("mind_create", "mind_initialize", "mind_set_precision", "mind_run", "mind_step",
                  "mind_time", "mind_get_trace", "mind_get_spikes", "mind_read_voltage",
                  "mind_inject_event", "mind_last_run_ms", "mind_destroy", "mind_run_stats",
                  "mind_set_profiling", "mind_run_noalloc", "mind_inject_spikes", "mind_window_steps",
-                 "mind_attach_macro", "mind_get_macro_trace"):
+                 "mind_attach_macro", "mind_get_macro_trace", "mind_set_drive_recording", "mind_get_drive",
+                 "mind_mlp_create", "mind_mlp_destroy",
+                 "mind_mlp_param_count", "mind_mlp_set_params", "mind_mlp_get_params", "mind_mlp_predict",
+                 "mind_mlp_gradients", "mind_mlp_set_data", "mind_mlp_train"):
         getattr(lib, name).restype = c_int32
     _LIB = lib
     return lib
@@ -190,6 +211,8 @@ EXPORTED_SYMBOLS = (
     "mind_get_trace", "mind_get_spikes", "mind_read_voltage", "mind_inject_event",
     "mind_last_error", "mind_last_run_ms", "mind_destroy", "mind_run_stats", "mind_set_profiling",
     "mind_run_noalloc", "mind_inject_spikes", "mind_window_steps", "mind_attach_macro", "mind_get_macro_trace",
+    "mind_set_drive_recording", "mind_get_drive", "mind_mlp_create", "mind_mlp_destroy", "mind_mlp_last_error", "mind_mlp_param_count", "mind_mlp_set_params",
+    "mind_mlp_get_params", "mind_mlp_predict", "mind_mlp_gradients", "mind_mlp_set_data", "mind_mlp_train",
 )
 
 MIND_NOALLOC_SCRATCH_BYTES = 16 << 20

@@ -35,6 +35,7 @@ class SimulationResult:
     spike_sources: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
     device_ms: float = 0.0
     macro_trace: np.ndarray = None   # [macro boundaries, regions] region outputs, when regions are attached
+    drive: np.ndarray = None         # [bins, cells, 32] synaptic drive, when recording it
 
 
 class DeviceState:
@@ -57,6 +58,11 @@ class DeviceState:
         c = macro.to_c()
         abi.check(self.lib, self.handle, self.lib.mind_attach_macro(self.handle, ctypes.byref(c)))
         self.n_regions = macro.n_regions
+
+    def set_drive_recording(self, bin_ms: float) -> None:
+        """mind_set_drive_recording: each run also returns the cells' binned synaptic drive."""
+        abi.check(self.lib, self.handle, self.lib.mind_set_drive_recording(self.handle, float(bin_ms)))
+        self.drive_on = bin_ms > 0
 
     def set_precision(self, precision: str) -> None:
         mode = {"fp64": abi.MIND_FP64, "mixed": abi.MIND_MIXED}[precision]
@@ -96,6 +102,14 @@ class DeviceState:
         abi.check(self.lib, self.handle, self.lib.mind_last_run_ms(self.handle, ctypes.byref(ms)))
         time = np.arange(start_step, start_step + samples, dtype=np.float64) * self.layout.dt
         result = SimulationResult(time, {}, times, sids, ms.value)
+        if getattr(self, "drive_on", False):
+            bins = ctypes.c_int64()
+            abi.check(self.lib, self.handle, self.lib.mind_get_drive(self.handle, None, 0, ctypes.byref(bins)))
+            drive = np.zeros((bins.value, self.layout.n_cells, 32), dtype=np.float32)
+            if drive.size:
+                abi.check(self.lib, self.handle, self.lib.mind_get_drive(
+                    self.handle, drive.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), drive.size, ctypes.byref(bins)))
+            result.drive = drive
         if getattr(self, "n_regions", 0):
             samples = ctypes.c_int64()
             abi.check(self.lib, self.handle, self.lib.mind_get_macro_trace(self.handle, None, 0, ctypes.byref(samples)))

@@ -1,0 +1,142 @@
+"""The spike-output surrogate: an MLP that predicts a cell's spike in the next 1 ms bin.
+
+Inputs per cell and bin (645 features): the cell's synaptic drive in the last 20 bins of
+1 ms over 32 synapse groups (the summed NetCon weights of the events its synapses
+received, synapse k in group k mod 32), then its own spike counts in the last 5 bins.  (The
+configuration names the last 5 ms of somatic voltage as the last five features; a cell
+that the surrogate replaces has no membrane voltage, so its recent output takes that
+place.)  Output: the spike probability of the next bin.  Training data come from the
+cable solver's own runs (`windows_from_run`); training and inference run in
+libmindgpu.so (BF16 products on the tensor cores, FP32 masters, fused kernels around
+them).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import abi
+
+WINDOW_BINS = 20
+GROUPS = 32
+HISTORY_BINS = 5
+N_FEATURES = WINDOW_BINS * GROUPS + HISTORY_BINS
+
+
+def _f32(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+class Mlp:
+    """mind_mlp_*: n_in -> hidden (SiLU) x layers -> sigmoid."""
+
+    def __init__(self, n_in: int = N_FEATURES, hidden: int = 256, layers: int = 3, seed: int = 1):
+        self.lib = abi.load_library()
+        cfg = abi.MindMlpConfig(n_in, hidden, layers, seed)
+        h = ctypes.c_void_p()
+        status = self.lib.mind_mlp_create(ctypes.byref(cfg), ctypes.byref(h))
+        self.handle = h
+        self._check(status)
+        n = ctypes.c_int64()
+        self._check(self.lib.mind_mlp_param_count(self.handle, ctypes.byref(n)))
+        self.n_params = n.value
+        self.n_in, self.hidden, self.layers = n_in, hidden, layers
+
+    def _check(self, status):
+        if status != abi.MIND_OK:
+            msg = self.lib.mind_mlp_last_error(self.handle) if self.handle else b""
+            raise abi.MindError(status, msg.decode() if msg else "")
+
+    @property
+    def params(self) -> np.ndarray:
+        out = np.zeros(self.n_params, dtype=np.float32)
+        self._check(self.lib.mind_mlp_get_params(self.handle, _f32(out), self.n_params))
+        return out
+
+    @params.setter
+    def params(self, values) -> None:
+        v = np.ascontiguousarray(values, dtype=np.float32)
+        self._check(self.lib.mind_mlp_set_params(self.handle, _f32(v), v.size))
+
+    def predict(self, x) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        out = np.zeros(x.shape[0], dtype=np.float32)
+        self._check(self.lib.mind_mlp_predict(self.handle, _f32(x), x.shape[0], _f32(out)))
+        return out
+
+    def gradients(self, x, y):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.ascontiguousarray(y, dtype=np.float32)
+        g = np.zeros(self.n_params, dtype=np.float32)
+        loss = ctypes.c_float()
+        self._check(self.lib.mind_mlp_gradients(self.handle, _f32(x), _f32(y), x.shape[0], _f32(g),
+                                                ctypes.byref(loss)))
+        return g, float(loss.value)
+
+    def train(self, x, y, steps: int, batch: int = 4096, lr: float = 1e-3):
+        """Adam on batches drawn from (x, y); returns (per-step batch losses, device ms)."""
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.ascontiguousarray(y, dtype=np.float32)
+        self._check(self.lib.mind_mlp_set_data(self.handle, _f32(x), _f32(y), x.shape[0]))
+        losses = np.zeros(steps, dtype=np.float32)
+        ms = ctypes.c_float()
+        self._check(self.lib.mind_mlp_train(self.handle, steps, batch, lr, _f32(losses), ctypes.byref(ms)))
+        return losses, float(ms.value)
+
+    def close(self):
+        if self.handle:
+            self.lib.mind_mlp_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def unpack(params: np.ndarray, dims):
+    """[(W [out x in], b [out]) per linear map] views of a flat parameter vector."""
+    out, k = [], 0
+    for i, o in zip(dims[:-1], dims[1:]):
+        W = params[k:k + i * o].reshape(o, i)
+        k += i * o
+        b = params[k:k + o]
+        k += o
+        out.append((W, b))
+    return out
+
+
+def cell_spike_bins(layout, result, bins: int, bin_ms: float = 1.0, start_ms: float = 0.0) -> np.ndarray:
+    """[bins, cells] spike counts of the cells' detectors from a run's raster."""
+    counts = np.zeros((bins, layout.n_cells), dtype=np.float32)
+    nodes = np.asarray(layout.source_nodes)
+    offsets = np.asarray(layout.cell_offsets)
+    sid_cell = {}
+    for s, node in enumerate(nodes):
+        if node > 0:
+            sid_cell[int(layout.source_ids[s])] = int(np.searchsorted(offsets, node - 1, side="right") - 1)
+    for t, sid in zip(result.spike_times, result.spike_sources):
+        c = sid_cell.get(int(sid))
+        b = int((t - start_ms) // bin_ms)
+        if c is not None and 0 <= b < bins:
+            counts[b, c] += 1.0
+    return counts
+
+
+def windows(drive: np.ndarray, spikes: np.ndarray, first_bin: int = WINDOW_BINS, last_bin: int = None,
+            cells=None):
+    """(x [n, 645], y [n]) for every cell and target bin b in [first_bin, last_bin): the drive of
+    bins b-20..b-1, the cell's spikes in bins b-5..b-1, and whether it spikes in bin b."""
+    bins, n_cells, groups = drive.shape
+    assert groups == GROUPS
+    last_bin = bins if last_bin is None else last_bin
+    cells = np.arange(n_cells) if cells is None else np.asarray(cells)
+    xs, ys = [], []
+    for b in range(max(first_bin, WINDOW_BINS), last_bin):
+        d = drive[b - WINDOW_BINS:b][:, cells, :].transpose(1, 0, 2).reshape(len(cells), -1)
+        h = spikes[b - HISTORY_BINS:b][:, cells].T
+        xs.append(np.concatenate([d, h], axis=1))
+        ys.append((spikes[b, cells] > 0).astype(np.float32))
+    return np.concatenate(xs).astype(np.float32), np.concatenate(ys)
