@@ -284,6 +284,15 @@ int mind_mlp_get_params(const MindMlp *mlp, float *params, int64_t n);
 int mind_mlp_predict(MindMlp *mlp, const float *x, int64_t n, float *prob);
 /* Gradient of the mean sigmoid cross-entropy over the n rows (targets y in [0, 1]). */
 int mind_mlp_gradients(MindMlp *mlp, const float *x, const float *y, int64_t n, float *grad, float *loss);
+/* Let a trained network stand in for the cells with surrogate_cells[c] != 0 (layout cell
+ * order): their membranes are no longer simulated; at the start of every rate bin b each
+ * such cell spikes with the network's probability for its inputs (drive of bins b-20..b-1
+ * times drive_scale, then its own spikes in bins b-5..b-1), decided by Philox4x32-10 on
+ * (b, cell) and placed uniformly in the bin; the spike is recorded, follows the cell's
+ * NetCons and counts in its region's bin.  Regions must be attached first (the rate bin
+ * is theirs); the handle keeps `mlp`, which must outlive it; mind_initialize follows. */
+int mind_attach_surrogate(MindHandle *h, MindMlp *mlp, const uint8_t *surrogate_cells, float drive_scale);
+
 /* Keep a training set on the device; then `steps` Adam steps (beta 0.9/0.999, eps 1e-8) on
  * batches drawn with replacement; losses[k] = the batch loss before step k (may be NULL). */
 int mind_mlp_set_data(MindMlp *mlp, const float *x, const float *y, int64_t n);

@@ -37,6 +37,7 @@ namespace mind {
 constexpr int kMaxGroups = 16;
 constexpr int kThreads = 128;      // auxiliary kernels
 constexpr int kCellThreads = 64;   // window kernel: one cell per CTA of two warps
+constexpr int kSurrogateRing = 21;  // drive bins kept for the surrogate: the last 20 and the current
 
 
 struct RingEvent {       // an event waiting in a delivery bin
@@ -207,6 +208,10 @@ struct Params {
     const int32_t *rec_node;       // local node
     const int32_t *rec_col;
     double *trace;
+    // cells the surrogate stands in for (null: none) and their drive ring [kSurrogateRing][ncells][32]
+    const uint8_t *cell_mode;
+    float *sur_drive;
+    int32_t sur_bin_steps;
     // surrogate training data: synaptic drive [drive_bins][ncells][32] of the run (or null)
     float *drive;
     int32_t drive_bin_steps;

@@ -767,6 +767,21 @@ __global__ void __launch_bounds__(kCellThreads, 8) window_kernel(const Params P,
     }
     __syncthreads();
 
+    if (P.cell_mode && P.cell_mode[c]) {
+        // A cell the surrogate stands in for: its membrane is not simulated; only the
+        // synaptic drive of its events is kept, per rate bin and synapse group, for the
+        // surrogate's next prediction.
+        if (tid == 0)
+            for (int32_t k = 0; k < nev; ++k) {
+                const InboxEvent &e = sev[k];
+                if (e.edge < 0) continue;
+                const int64_t bin = e.bin / P.sur_bin_steps;
+                P.sur_drive[((bin % kSurrogateRing) * P.ncells + c) * 32 + ((e.point & 0xffffff) & 31)] +=
+                    (float)P.edge_weight[e.edge];
+            }
+        return;
+    }
+
     const double q10 = mind_pow(3.0, (P.celsius - 6.3) / 10.0);
     const float q10f = (float)q10;
     int32_t cursor = 0;

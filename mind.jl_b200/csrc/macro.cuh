@@ -167,3 +167,52 @@ __global__ void macro_init_kernel(const MacroParams M, const double *y0) {
 }
 
 }  // namespace mind
+
+namespace mind {
+
+/* Surrogate cells' inputs for the bin `b` that starts now: the drive of bins b-20..b-1
+ * (times `scale`, 0 before the run's first bin) and their own spikes in bins b-5..b-1. */
+__global__ void surrogate_features_kernel(const Params P, const int32_t *cells, int32_t n, const int32_t *spikes,
+                                          float scale, int64_t b, float *x) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < (int64_t)n * 645;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = k / 645, j = k % 645;
+        const int32_t c = cells[i];
+        float v = 0.0f;
+        if (j < 640) {
+            const int64_t bin = b - 20 + j / 32;
+            if (bin >= 0) v = scale * P.sur_drive[((bin % kSurrogateRing) * P.ncells + c) * 32 + (j % 32)];
+        } else {
+            const int64_t bin = b - 5 + (j - 640);
+            if (bin >= 0) v = (float)spikes[(bin % 6) * (int64_t)n + i];
+        }
+        x[k] = v;
+    }
+}
+
+/* Each surrogate cell spikes in bin b with the predicted probability (u0 < p, Philox on
+ * (b, cell)), at b * bin_ms + bin_ms * u1; the spike is recorded, fanned out through the
+ * cell's NetCons and counted in its region's bin like a detected spike. */
+__global__ void surrogate_spike_kernel(const Params P, const int32_t *cells, const int32_t *sources, int32_t n,
+                                       const float *prob, int32_t *spikes, int64_t b, double bin_ms,
+                                       const int32_t *source_region, int32_t *bins, int32_t n_regions,
+                                       int32_t bin_ring, int64_t min_bin) {
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t ctr[4] = {(uint32_t)b, (uint32_t)((uint64_t)b >> 32), (uint32_t)cells[i], 0x5355u};
+        mind_philox4x32_10(ctr, (uint32_t)P.seed, (uint32_t)(P.seed >> 32));
+        const double u0 = ((double)ctr[0] + 1.0) * MIND_INV_2P32P1, u1 = ((double)ctr[1] + 1.0) * MIND_INV_2P32P1;
+        const bool fire = u0 < (double)prob[i];
+        spikes[(b % 6) * (int64_t)n + i] = fire ? 1 : 0;
+        const int32_t src = sources[i];
+        if (!fire || src < 0) continue;
+        const double t = (double)b * bin_ms + bin_ms * u1;
+        record_spike(P, src, t);
+        fan_out(P, src, t, min_bin);
+        if (n_regions > 0) {
+            const int32_t region = source_region[src];
+            if (region >= 0) atomicAdd(&bins[(b % bin_ring) * n_regions + region], 1);
+        }
+    }
+}
+
+}  // namespace mind

@@ -32,6 +32,10 @@
 
 using namespace mind;
 
+int mind_mlp_forward_device(MindMlp *m, const float *x, int64_t n, float *prob, cudaStream_t stream);
+int mind_mlp_reserve_device(MindMlp *m, int64_t rows);
+int32_t mind_mlp_inputs(const MindMlp *m);
+
 namespace {
 
 constexpr int32_t kMaxWindow = 64;
@@ -78,6 +82,13 @@ struct MindHandle {
     size_t macro_trace_cap = 0;
     std::vector<double> macro_trace;
     int64_t macro_trace_samples = 0;
+    std::vector<int32_t> cell_detector;      // first detector source of each cell, or -1
+    // cells the surrogate stands in for (mind_attach_surrogate)
+    MindMlp *sur_mlp = nullptr;
+    int32_t n_sur = 0;
+    float sur_scale = 1.0f;
+    int32_t *sur_cells = nullptr, *sur_sources = nullptr, *sur_spikes = nullptr;
+    float *sur_x = nullptr, *sur_prob = nullptr;
     // synaptic drive recording (mind_set_drive_recording)
     int32_t drive_bin_steps = 0;
     float *drive_dev = nullptr;
@@ -535,6 +546,7 @@ int create(const MindLayout *L, MindHandle *h) {
     std::vector<int32_t> det_off{0}, det_node, det_source;
     std::vector<double> det_thr;
     for (int32_t c = 0; c < ncells; ++c) {
+        h->cell_detector.push_back(det_by_cell[c].empty() ? -1 : det_by_cell[c].front().second);
         if ((int32_t)det_by_cell[c].size() > kCellThreads)
             return fail(h, MIND_ELAYOUT, "more than 64 threshold detectors on one cell");
         for (auto &d : det_by_cell[c]) {
@@ -818,6 +830,20 @@ int advance(MindHandle *h, int64_t steps, bool record_spikes) {
             const int32_t zero_slot = n0 % h->bin_steps == 0 ? (int32_t)((n0 / h->bin_steps) % M.bin_ring) : -1;
             macro_advance_kernel<<<1, h->macro_threads, 0, h->stream>>>(M, k0, k1, zero_slot);
             ++st.launches;
+            if (h->n_sur > 0 && n0 % h->bin_steps == 0) {
+                // bin b starts: the surrogate cells' spikes of bin b from their last 20 bins
+                const int64_t b = n0 / h->bin_steps;
+                CUDA_TRY(h, cudaMemsetAsync(P.sur_drive + (b % kSurrogateRing) * (int64_t)h->ncells * 32, 0,
+                                            (size_t)h->ncells * 32 * sizeof(float), h->stream));
+                surrogate_features_kernel<<<launch_grid((int64_t)h->n_sur * 645), kThreads, 0, h->stream>>>(
+                    P, h->sur_cells, h->n_sur, h->sur_spikes, h->sur_scale, b, h->sur_x);
+                if (mind_mlp_forward_device(h->sur_mlp, h->sur_x, h->n_sur, h->sur_prob, h->stream))
+                    return fail(h, MIND_ECUDA, "surrogate inference failed");
+                surrogate_spike_kernel<<<launch_grid(h->n_sur), kThreads, 0, h->stream>>>(
+                    P, h->sur_cells, h->sur_sources, h->n_sur, h->sur_prob, h->sur_spikes, b,
+                    (double)h->bin_steps * P.dt, M.source_region, M.bins, M.n, M.bin_ring, n0);
+                st.launches += 3;
+            }
             if (k1 > k0 && M.n_inputs > 0) {
                 macro_input_kernel<<<launch_grid(M.n_inputs), kThreads, 0, h->stream>>>(P, M, k0, k1, n0);
                 ++st.launches;
@@ -1049,6 +1075,10 @@ int mind_initialize(MindHandle *h) {
         netstim_init_kernel<<<launch_grid(P.groups[P.ns_group].rows), kThreads, 0, h->stream>>>(
             P, h->group_init[P.ns_group].digest, h->ns_logical);
     if (h->M.n > 0) macro_init_kernel<<<1, h->macro_threads, 0, h->stream>>>(h->M, h->macro_y0);
+    if (h->n_sur > 0) {
+        CUDA_TRY(h, cudaMemsetAsync(P.sur_drive, 0, (size_t)kSurrogateRing * h->ncells * 32 * sizeof(float), h->stream));
+        CUDA_TRY(h, cudaMemsetAsync(h->sur_spikes, 0, (size_t)6 * h->n_sur * sizeof(int32_t), h->stream));
+    }
     CUDA_TRY(h, cudaGetLastError());
     status = check_device_error(h);
     if (status) return status;
@@ -1162,6 +1192,40 @@ int mind_attach_macro(MindHandle *h, const MindMacroLayout *L) {
     h->bin_steps = bin_steps;
     h->window = window;
     h->macro_threads = ((n + 31) / 32) * 32;
+    h->initialized = false;
+    return MIND_OK;
+}
+
+int mind_attach_surrogate(MindHandle *h, MindMlp *mlp, const uint8_t *surrogate_cells, float drive_scale) {
+    if (!h || !mlp || !surrogate_cells) return MIND_EARG;
+    if (h->M.n == 0) return fail(h, MIND_EARG, "attach regions first: the surrogate predicts their rate bins");
+    if (h->n_sur > 0) return fail(h, MIND_EARG, "a surrogate is already attached");
+    if (mind_mlp_inputs(mlp) != 645) return fail(h, MIND_EARG, "the surrogate network must take 645 inputs");
+    std::vector<uint8_t> mode(h->ncells, 0);
+    std::vector<int32_t> cells, sources;
+    for (int32_t c = 0; c < h->ncells; ++c)
+        if (surrogate_cells[c]) {
+            mode[c] = 1;
+            cells.push_back(c);
+            sources.push_back(h->cell_detector[c]);
+        }
+    if (cells.empty()) return MIND_OK;
+    if (mind_mlp_reserve_device(mlp, (int64_t)cells.size())) return fail(h, MIND_ECUDA, "surrogate buffers");
+    try {
+        h->P.cell_mode = h->upload(mode);
+        h->P.sur_drive = h->alloc<float>((size_t)kSurrogateRing * h->ncells * 32);
+        h->sur_cells = h->upload(cells);
+        h->sur_sources = h->upload(sources);
+        h->sur_spikes = h->alloc<int32_t>((size_t)6 * cells.size());
+        h->sur_x = h->alloc<float>((size_t)645 * cells.size());
+        h->sur_prob = h->alloc<float>(cells.size());
+    } catch (const std::bad_alloc &) {
+        return fail(h, MIND_ECUDA, "device allocation failed");
+    }
+    h->P.sur_bin_steps = h->bin_steps;
+    h->sur_mlp = mlp;
+    h->sur_scale = drive_scale;
+    h->n_sur = (int32_t)cells.size();
     h->initialized = false;
     return MIND_OK;
 }

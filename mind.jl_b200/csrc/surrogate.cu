@@ -232,6 +232,29 @@ int upload_rows(MindMlp *m, const float *x, int64_t n) {
 
 }  // namespace
 
+/* For the library's own runs (surrogate cells): probabilities of n rows of FP32 inputs that
+ * are already on the device, ordered after `stream`'s work and before its later work.
+ * The rows must fit the buffers reserved by mind_mlp_reserve_device. */
+int mind_mlp_forward_device(MindMlp *m, const float *x, int64_t n, float *prob, cudaStream_t stream) {
+    if (n > m->cap) return fail(m, MIND_ECAPACITY, "more rows than reserved");
+    cudaEvent_t ready, done;
+    MLP_CUDA(m, cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+    MLP_CUDA(m, cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+    cudaEventRecord(ready, stream);
+    cudaStreamWaitEvent(m->stream, ready, 0);
+    to_bf16_kernel<<<grid(n * m->dims[0]), kT, 0, m->stream>>>(x, m->h[0], n * m->dims[0]);
+    int s = forward(m, n);
+    if (!s) sigmoid_kernel<<<grid(n), kT, 0, m->stream>>>(m->z.back(), prob, n);
+    cudaEventRecord(done, m->stream);
+    cudaStreamWaitEvent(stream, done, 0);
+    cudaEventDestroy(ready);
+    cudaEventDestroy(done);
+    return s;
+}
+
+int mind_mlp_reserve_device(MindMlp *m, int64_t rows) { return reserve(m, rows); }
+int32_t mind_mlp_inputs(const MindMlp *m) { return m->dims[0]; }
+
 extern "C" {
 
 int mind_mlp_create(const MindMlpConfig *config, MindMlp **out) {

@@ -181,6 +181,7 @@ def load_library():
     lib.mind_get_macro_trace.argtypes = [handle, POINTER(c_double), c_int64, POINTER(c_int64)]
     f32 = POINTER(ctypes.c_float)
     lib.mind_set_drive_recording.argtypes = [handle, c_double]
+    lib.mind_attach_surrogate.argtypes = [handle, handle, POINTER(ctypes.c_uint8), ctypes.c_float]
     lib.mind_get_drive.argtypes = [handle, f32, c_int64, POINTER(c_int64)]
     lib.mind_mlp_create.argtypes = [POINTER(MindMlpConfig), POINTER(handle)]
     lib.mind_mlp_destroy.argtypes = [handle]
@@ -198,6 +199,7 @@ def load_library():
                  "mind_inject_event", "mind_last_run_ms", "mind_destroy", "mind_run_stats",
                  "mind_set_profiling", "mind_run_noalloc", "mind_inject_spikes", "mind_window_steps",
                  "mind_attach_macro", "mind_get_macro_trace", "mind_set_drive_recording", "mind_get_drive",
+                 "mind_attach_surrogate",
                  "mind_mlp_create", "mind_mlp_destroy",
                  "mind_mlp_param_count", "mind_mlp_set_params", "mind_mlp_get_params", "mind_mlp_predict",
                  "mind_mlp_gradients", "mind_mlp_set_data", "mind_mlp_train"):
@@ -211,7 +213,7 @@ EXPORTED_SYMBOLS = (
     "mind_get_trace", "mind_get_spikes", "mind_read_voltage", "mind_inject_event",
     "mind_last_error", "mind_last_run_ms", "mind_destroy", "mind_run_stats", "mind_set_profiling",
     "mind_run_noalloc", "mind_inject_spikes", "mind_window_steps", "mind_attach_macro", "mind_get_macro_trace",
-    "mind_set_drive_recording", "mind_get_drive", "mind_mlp_create", "mind_mlp_destroy", "mind_mlp_last_error", "mind_mlp_param_count", "mind_mlp_set_params",
+    "mind_set_drive_recording", "mind_get_drive", "mind_attach_surrogate", "mind_mlp_create", "mind_mlp_destroy", "mind_mlp_last_error", "mind_mlp_param_count", "mind_mlp_set_params",
     "mind_mlp_get_params", "mind_mlp_predict", "mind_mlp_gradients", "mind_mlp_set_data", "mind_mlp_train",
 )
 

@@ -59,6 +59,16 @@ class DeviceState:
         abi.check(self.lib, self.handle, self.lib.mind_attach_macro(self.handle, ctypes.byref(c)))
         self.n_regions = macro.n_regions
 
+    def attach_surrogate(self, mlp, surrogate_cells, drive_scale: float) -> None:
+        """mind_attach_surrogate: `mlp` (mind_b200.surrogate.Mlp) stands in for the cells where
+        surrogate_cells (one flag per cell) is true; regions must be attached; initialize follows."""
+        mask = np.ascontiguousarray(np.asarray(surrogate_cells, dtype=bool).astype(np.uint8))
+        if mask.size != self.layout.n_cells:
+            raise ValueError("one flag per cell")
+        abi.check(self.lib, self.handle, self.lib.mind_attach_surrogate(
+            self.handle, mlp.handle, mask.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), float(drive_scale)))
+        self._surrogate = mlp   # the network must outlive the handle's use of it
+
     def set_drive_recording(self, bin_ms: float) -> None:
         """mind_set_drive_recording: each run also returns the cells' binned synaptic drive."""
         abi.check(self.lib, self.handle, self.lib.mind_set_drive_recording(self.handle, float(bin_ms)))

@@ -140,3 +140,41 @@ def windows(drive: np.ndarray, spikes: np.ndarray, first_bin: int = WINDOW_BINS,
         xs.append(np.concatenate([d, h], axis=1))
         ys.append((spikes[b, cells] > 0).astype(np.float32))
     return np.concatenate(xs).astype(np.float32), np.concatenate(ys)
+
+
+def train_from_run(model, t_ms: float, steps: int = 150, batch: int = 1024, lr: float = 1e-3, seed: int = 1,
+                   hidden: int = 256, layers: int = 3):
+    """Run the detailed network for t_ms with drive recording (from initialize), build the
+    windows of every cell and bin, and train a surrogate on them.  Returns (mlp, drive_scale,
+    result of the detailed run)."""
+    from . import runtime
+
+    runtime.initialize(model)
+    model.state.set_drive_recording(1.0)
+    result = runtime.run(model, t_ms)
+    model.state.set_drive_recording(0.0)
+    spikes = cell_spike_bins(model.layout, result, result.drive.shape[0])
+    x, y = windows(result.drive, spikes)
+    scale = float(1.0 / (x[:, :-HISTORY_BINS].std() + 1e-12))
+    x[:, :-HISTORY_BINS] *= scale
+    net = Mlp(hidden=hidden, layers=layers, seed=seed)
+    net.train(x, y, steps=steps, batch=batch, lr=lr)
+    return net, scale, result
+
+
+def region_rates(layout, result, macro, t_ms: float, bin_ms: float = 10.0) -> np.ndarray:
+    """[bins, regions] spike rate (Hz per cell) of each region's cells from a run's raster."""
+    region_of = {}
+    for region, source in macro.outputs:
+        region_of[int(layout.source_ids[source - 1])] = region - 1
+    cells = np.zeros(macro.n_regions)
+    for region, _ in macro.outputs:
+        cells[region - 1] += 1
+    bins = int(round(t_ms / bin_ms))
+    rates = np.zeros((bins, macro.n_regions))
+    for t, sid in zip(result.spike_times, result.spike_sources):
+        r = region_of.get(int(sid))
+        b = int(t // bin_ms)
+        if r is not None and 0 <= b < bins:
+            rates[b, r] += 1.0
+    return rates / np.maximum(cells, 1.0) / (bin_ms * 1e-3)

@@ -58,3 +58,30 @@ def test_trained_surrogate_beats_a_constant_rate():
     base = -np.mean(y_te * np.log(q) + (1 - y_te) * np.log(1 - q))
     assert ce < 0.85 * base, (ce, base)
     net.close()
+
+
+def test_surrogate_cells_drive_the_regions():
+    """Train on a detailed run, then let the network stand in for 90% of the cells: the run
+    stays finite, surrogate cells fire at the detailed cells' order of magnitude, the regions
+    keep moving, and the same seed gives the same run."""
+    model, macro = netcases.coupled_regions(n_regions=4, cells_per_region=50, synapses=32, seed=21)
+    layout = model.layout
+    net, scale, detailed = surrogate.train_from_run(model, 400.0, steps=150)
+    mask = np.ones(layout.n_cells, dtype=bool)
+    mask[::10] = False                      # every tenth cell stays detailed
+    runs = []
+    for _ in range(2):
+        state = mb.runtime.DeviceState(layout)
+        state.attach_macro(macro)
+        state.attach_surrogate(net, mask, scale)
+        state.initialize()
+        runs.append(state.run_steps(int(round(400.0 / layout.dt)), []))
+        state.close()
+    a, b = runs
+    np.testing.assert_array_equal(a.spike_times, b.spike_times)
+    np.testing.assert_array_equal(a.macro_trace, b.macro_trace)
+    assert np.all(np.isfinite(a.macro_trace)) and np.ptp(a.macro_trace) > 0.1
+    n_detailed = np.sum(detailed.spike_sources <= layout.n_cells)
+    n_sur = np.sum(a.spike_sources <= layout.n_cells)
+    assert n_detailed / 4 < n_sur < 4 * n_detailed, (n_sur, n_detailed)
+    net.close()
