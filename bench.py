@@ -56,6 +56,9 @@ def parse():
                    help="both: the FP64 headline plus the mixed mode and its accuracy against FP64")
     p.add_argument("--accuracy-ms", type=float, default=0.0,
                    help="instead of timing: run FP64 and mixed from t=0 for this long and print their differences")
+    p.add_argument("--surrogate", action="store_true",
+                   help="config 4: train the spike-output surrogate on a detailed run, then time the coupled run "
+                        "with 98%% of the cells replaced, against the plain FP64 run, and their region rates")
     p.add_argument("--cpu-steps", type=int, default=8)
     p.add_argument("--no-cpu-baseline", action="store_true")
     return p.parse_args()
@@ -272,6 +275,53 @@ def measure_sharded(args, layout, rank: int, world: int, precision: str, local_r
             (trace, e2e_result.spike_sources, e2e_result.spike_times), clocks)
 
 
+def measure_surrogate(args, model, layout, train_ms: float = 300.0, eval_ms: float = 200.0, keep: float = 0.02):
+    """Config 4 with the surrogate: train on a detailed FP64 run of train_ms, then run eval_ms
+    from initialize twice — plain FP64, and with all but `keep` of the cells replaced — and
+    compare time per step and the regions' population rates (10 ms bins)."""
+    import mind_b200 as mb
+    from mind_b200 import surrogate
+
+    if args.config != 4:
+        raise SystemExit("--surrogate needs --config 4")
+    macro = model.macro
+    t0 = time.perf_counter()
+    net, scale, train_run = surrogate.train_from_run(model, train_ms, steps=500, batch=4096)
+    train_s = time.perf_counter() - t0
+    steps = int(round(eval_ms / layout.dt))
+    mb.initialize(model)
+    plain, plain_ms = device_timed(lambda: model.state.run_steps(steps, []))
+    rng = np.random.default_rng(0)
+    mask = rng.uniform(size=layout.n_cells) >= keep
+    state = mb.runtime.DeviceState(layout, "mixed")   # the tuned mode for the detailed sample
+    state.attach_macro(macro)
+    state.attach_surrogate(net, mask, scale)
+    state.initialize()
+    sur, sur_ms = device_timed(lambda: state.run_steps(steps, []))
+    state.close()
+    r_plain = surrogate.region_rates(layout, plain, macro, eval_ms)
+    r_sur = surrogate.region_rates(layout, sur, macro, eval_ms)
+    mean_plain = r_plain.mean(axis=0)
+    rel = np.abs(r_sur.mean(axis=0) - mean_plain) / np.maximum(mean_plain, 1e-9)
+    units = layout.segment_count * steps
+    return {
+        "metric": "compartment-steps/s (config 4, equivalent: every cell's compartments counted)",
+        "config": {"workload": "config4", "cells": layout.n_cells, "compartments": layout.segment_count,
+                   "surrogate_cells": int(mask.sum()), "train_ms": train_ms, "eval_ms": eval_ms},
+        "plain_fp64": {"value": units / (plain_ms / 1000.0), "ms_per_step": plain_ms / steps},
+        "surrogate": {"value": units / (sur_ms / 1000.0), "ms_per_step": sur_ms / steps},
+        "speedup": plain_ms / sur_ms,
+        "population_rate_error": {"per_region_mean_rel": rel.tolist(), "max_rel": float(rel.max()),
+                                  "mean_rel": float(rel.mean()),
+                                  "plain_rate_hz": mean_plain.tolist(),
+                                  "surrogate_rate_hz": r_sur.mean(axis=0).tolist()},
+        "training": {"windows": int((train_run.drive.shape[0] - surrogate.WINDOW_BINS) * layout.n_cells),
+                     "steps": 500, "batch": 4096, "wall_s": train_s},
+        "note": "plain: every cell in FP64; surrogate: the detailed sample in the mixed mode, the rest "
+                "replaced; regions FP64 in both; rates from the rasters",
+    }
+
+
 def run_reference(args, rank: int):
     if rank != 0:
         return
@@ -328,6 +378,12 @@ def main():
     model, layout = build_network(args.cells, seed=replicas.replica_seed(1, rank), config=args.config,
                                   rank=rank, world=world)
     sharded = world > 1 and args.config == 2
+    if args.surrogate:
+        if rank == 0:
+            print(json.dumps(measure_surrogate(args, model, layout)), flush=True)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
     if args.accuracy_ms > 0:
         if rank == 0:
             soma_all = [mb.RecordSpec(layout.voltage_node(c), f"v{c}") for c in range(1, layout.n_cells + 1)]

@@ -685,6 +685,44 @@ __global__ void __launch_bounds__(kCellThreads, 8) window_kernel(const Params P,
     // ---- stage the cell ----
     if (blockIdx.x == 0)
         for (int32_t k = tid; k < W; k += T) P.ring_count[(n0 + k) % P.ring_slots] = 0;
+    if (P.cell_mode && P.cell_mode[c]) {
+        // A cell the surrogate stands in for: its membrane is not simulated; its window's
+        // events only add their NetCon weights to its drive, per rate bin and synapse group,
+        // in the canonical event order (so the sums, and the run, are reproducible).
+        if (tid == 0) {
+            int32_t count = P.inbox_count[c];
+            if (count > P.inbox_cap) {
+                raise_error(P.error, MIND_ECAPACITY);
+                count = P.inbox_cap;
+            }
+            s_nev = count;
+            P.inbox_count[c] = 0;
+        }
+        __syncthreads();
+        const int32_t m = s_nev;
+        for (int32_t k = tid; k < m; k += T) sev[k] = P.inbox[(int64_t)c * P.inbox_cap + k];
+        __syncthreads();
+        for (int32_t k = tid; k < m; k += T) {
+            int32_t rank = 0;
+            const InboxEvent mine = sev[k];
+            for (int32_t j = 0; j < m; ++j) {
+                const InboxEvent other = sev[j];
+                if (event_before(other, mine) || (j < k && !event_before(mine, other))) ++rank;
+            }
+            sorder[rank] = k;
+        }
+        __syncthreads();
+        if (tid == 0)
+            for (int32_t k = 0; k < m; ++k) {
+                const InboxEvent e = sev[sorder[k]];
+                if (e.edge < 0) continue;
+                const int32_t g = P.point_group[e.point];
+                const int32_t row = P.point_row[e.point] - P.groups[g].row_off[c];
+                const int64_t bin = e.bin / P.sur_bin_steps;
+                P.sur_drive[((bin % kSurrogateRing) * P.ncells + c) * 32 + (row & 31)] += (float)P.edge_weight[e.edge];
+            }
+        return;
+    }
     for (int32_t i = tid; i < n; i += T) {
         sv[i] = P.v[nb + i];
         sa[i] = P.a[nb + i];
@@ -766,21 +804,6 @@ __global__ void __launch_bounds__(kCellThreads, 8) window_kernel(const Params P,
         e.point = (g << 24) | (drow - sg[g].r0);
     }
     __syncthreads();
-
-    if (P.cell_mode && P.cell_mode[c]) {
-        // A cell the surrogate stands in for: its membrane is not simulated; only the
-        // synaptic drive of its events is kept, per rate bin and synapse group, for the
-        // surrogate's next prediction.
-        if (tid == 0)
-            for (int32_t k = 0; k < nev; ++k) {
-                const InboxEvent &e = sev[k];
-                if (e.edge < 0) continue;
-                const int64_t bin = e.bin / P.sur_bin_steps;
-                P.sur_drive[((bin % kSurrogateRing) * P.ncells + c) * 32 + ((e.point & 0xffffff) & 31)] +=
-                    (float)P.edge_weight[e.edge];
-            }
-        return;
-    }
 
     const double q10 = mind_pow(3.0, (P.celsius - 6.3) / 10.0);
     const float q10f = (float)q10;
