@@ -39,6 +39,10 @@ import numpy as np  # noqa: E402
 
 COLLECTIVE_DEVICE = "cuda"   # device of the tensors handed to torch.distributed
 METRIC = "compartment-steps/s (config 2: 10,000 uneven cells, recurrent Exp2Syn, dt 0.025 ms)"
+WORKLOAD_METRICS = {
+    2: METRIC,
+    3: "compartment-steps/s (config 3: 1,000 uneven cells, 3e5 NetStim-driven Exp2Syn, dt 0.025 ms)",
+}
 UNIT = "compartment-steps/s"
 
 
@@ -334,7 +338,7 @@ def run_reference(args, rank: int):
         values.append(value)
     value = statistics.median(values)
     line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "impl": "reference", "metric": WORKLOAD_METRICS.get(args.config, METRIC), "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": steps, "warmup": 0, "ms_per_step": ms / steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded config-2 network)",
         "config": {"workload": f"config{args.config}", "cells": layout.n_cells, "compartments": layout.segment_count,
@@ -454,7 +458,8 @@ def main():
     peak, peak_kind = measured_peaks()
     traffic = recorded_traffic()
     line = {
-        "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "metric": WORKLOAD_METRICS.get(args.config, METRIC), "value": head["value"], "unit": UNIT, "n_gpus": world,
+        "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64" if precisions[0] == "fp64" else "f32-gating/f64-cable",
         "data": f"synthetic (seeded config-{args.config} network, mind_b200.networks.config{args.config})",

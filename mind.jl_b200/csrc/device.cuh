@@ -36,7 +36,7 @@ namespace mind {
 
 constexpr int kMaxGroups = 16;
 constexpr int kThreads = 128;      // auxiliary kernels
-constexpr int kCellThreads = 64;   // window kernel: one cell per CTA of two warps
+constexpr int kCellThreads = 128;  // window kernel: one cell per CTA of four warps
 constexpr int kSurrogateRing = 21;  // drive bins kept for the surrogate: the last 20 and the current
 
 

@@ -603,7 +603,7 @@ __device__ __forceinline__ void hines_mixed(double *sd, double *sr, const double
 }
 
 /*
- * One CTA of two warps advances one cell through W micro steps.  Shared memory
+ * One CTA of four warps advances one cell through W micro steps.  Shared memory
  * holds what the serial parts of the step touch: v, d, rhs and axial
  * conductance of every node, the chain tables of the Hines solve, the state
  * that changes every step (hh gates, synaptic conductances) and the window's
@@ -615,7 +615,7 @@ __device__ __forceinline__ void hines_mixed(double *sd, double *sr, const double
  * on the dependency chain, the next node's operands being loaded ahead.
  */
 template <bool MIXED>
-__global__ void __launch_bounds__(kCellThreads, 8) window_kernel(const Params P, const int32_t *cells, int64_t n0,
+__global__ void __launch_bounds__(kCellThreads, 5) window_kernel(const Params P, const int32_t *cells, int64_t n0,
                                                               int32_t W) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int32_t s_nev;
