@@ -136,11 +136,28 @@ typedef struct MindLayout {
     int64_t spike_capacity;            /* recorded spikes per run */
 } MindLayout;
 
-/* A recorded quantity (RecordSpec, src/model/references.jl:4-12). */
-enum { MIND_RECORD_VOLTAGE = 1 };
+/*
+ * A recorded or read quantity: RecordSpec / VariableRef (src/model/references.jl:4-80)
+ * for the :voltage and :mechanism kinds.  A mechanism reference names a layout column
+ * (MindMechanism.data) of one row; the columns kept on the device are the PARAMETER and
+ * STATE fields the kernels use:
+ *   hh       gnabar gkbar gl el ena ek m h n
+ *   pas      g e
+ *   ExpSyn   tau e g
+ *   Exp2Syn  tau1 tau2 e A B factor
+ *   IClamp   del dur amp
+ *   NetStim  interval number start noise event on ispike   (mind_read_value only)
+ * ASSIGNED fields that the reference writes during BREAKPOINT (hh ina/gna/minf/..., pas
+ * i, ExpSyn i, Exp2Syn g/i, IClamp i) are not kept: referencing one returns MIND_EARG.
+ * A recorded mechanism field is sampled at the same boundaries as voltages.
+ */
+enum { MIND_RECORD_VOLTAGE = 1, MIND_RECORD_MECHANISM = 2 };
 typedef struct MindRecord {
-    int32_t kind;                      /* MIND_RECORD_VOLTAGE */
-    int32_t node;                      /* 1-based node */
+    int32_t kind;                      /* MIND_RECORD_VOLTAGE or MIND_RECORD_MECHANISM */
+    int32_t node;                      /* VOLTAGE: 1-based node */
+    int32_t group;                     /* MECHANISM: 1-based mechanism group (MindLayout.mechanisms) */
+    int32_t row;                       /* MECHANISM: 1-based row of that group */
+    int32_t field;                     /* MECHANISM: 1-based column of the group's data */
 } MindRecord;
 
 typedef struct MindHandle MindHandle;
@@ -176,6 +193,10 @@ int mind_get_spikes(const MindHandle *h, double *times, int64_t *sids, int64_t c
 
 /* read_value for a voltage reference: v at a 1-based node. */
 int mind_read_voltage(const MindHandle *h, int32_t node, double *value);
+
+/* read_value (src/runtime/state.jl:585-599): the current value of a voltage or mechanism
+ * reference (MindRecord); MIND_EARG for an index out of range or a field not kept. */
+int mind_read_value(const MindHandle *h, const MindRecord *ref, double *value);
 
 /* inject_event!: deliver connection `edge` (1-based) at absolute time t (ms, >= now). */
 int mind_inject_event(MindHandle *h, int64_t edge, double t);

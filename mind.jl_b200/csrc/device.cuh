@@ -205,7 +205,11 @@ struct Params {
     const int32_t *ns_source;      // per NetStim row: 0-based source or -1
     // recording
     const int32_t *rec_off;        // [ncells+1]
-    const int32_t *rec_node;       // local node
+    // per record of the cell: rec_ptr non-null reads that HBM value (a constant parameter);
+    // else rec_node >= 0 is a local node's v and rec_node < 0 a staged field,
+    // -1 - rec_node = group << 24 | staged slot << 20 | row within the cell's rows
+    const int32_t *rec_node;
+    const double *const *rec_ptr;
     const int32_t *rec_col;
     double *trace;
     // cells the surrogate stands in for (null: none) and their drive ring [kSurrogateRing][ncells][32]

@@ -1042,8 +1042,20 @@ __global__ void __launch_bounds__(kCellThreads, 5) window_kernel(const Params P,
         // 9. Record the completed boundary.
         if (P.nrec) {
             const int64_t sample = step + 1 - P.run_start;
-            for (int32_t k = P.rec_off[c] + tid; k < P.rec_off[c + 1]; k += T)
-                P.trace[sample * P.nrec + P.rec_col[k]] = sv[P.rec_node[k]];
+            for (int32_t k = P.rec_off[c] + tid; k < P.rec_off[c + 1]; k += T) {
+                const double *gp = P.rec_ptr[k];
+                const int32_t code = P.rec_node[k];
+                double value;
+                if (gp) {
+                    value = *gp;
+                } else if (code >= 0) {
+                    value = sv[code];
+                } else {
+                    const int32_t x = -1 - code;
+                    value = sg[x >> 24].at((x >> 20) & 15, x & 0xFFFFF);
+                }
+                P.trace[sample * P.nrec + P.rec_col[k]] = value;
+            }
         }
         __syncthreads();
     }
@@ -1076,9 +1088,10 @@ __global__ void __launch_bounds__(kCellThreads, 5) window_kernel(const Params P,
     }
 }
 
-__global__ void record_initial_kernel(const Params P, const int64_t *rec_global, int32_t nrec) {
+/* The run's first sample: every recorded value as it stands in HBM between runs. */
+__global__ void record_initial_kernel(const Params P, const double *const *rec_initial, int32_t nrec) {
     for (int32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nrec; k += gridDim.x * blockDim.x)
-        P.trace[k] = P.v[rec_global[k]];
+        P.trace[k] = *rec_initial[k];
 }
 
 __global__ void finite_kernel(const double *values, int64_t count, int32_t *error) {

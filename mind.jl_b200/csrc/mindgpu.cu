@@ -114,6 +114,11 @@ struct MindHandle {
         std::vector<uint64_t> logical;        // device row order (NetStim)
     };
     std::vector<GroupInit> group_init;
+    // references (MindRecord): per group, layout row -> device row, layout column -> device
+    // slot (-1: not kept), and each cell's first device row
+    std::vector<std::vector<int32_t>> dev_row_of;
+    std::vector<std::vector<int32_t>> field_slot;
+    std::vector<std::vector<int32_t>> group_row_off;
     // results
     std::vector<double> trace;
     int64_t trace_samples = 0;
@@ -130,7 +135,8 @@ struct MindHandle {
     int32_t *rec_off_dev = nullptr;
     int32_t *rec_node_dev = nullptr;
     int32_t *rec_col_dev = nullptr;
-    int64_t *rec_global_dev = nullptr;
+    const double **rec_initial_dev = nullptr;   // per record: its value in HBM (first sample)
+    const double **rec_ptr_dev = nullptr;       // per cell-sorted record: HBM parameter or null
     double *trace_dev = nullptr;
     size_t trace_capacity = 0;
     size_t rec_capacity = 0;
@@ -248,6 +254,45 @@ int slot_of(int32_t kind, int k) {
         case MIND_MECH_ICLAMP: return ic[k];
         case MIND_MECH_NETSTIM: return ns[k];
         default: return 0;
+    }
+}
+
+/* Device slot of a MOD field that a reference may name (the PARAMETER and STATE fields
+ * the kernels keep), or -1. */
+int readable_slot(int32_t kind, const char *name) {
+    struct Entry {
+        int32_t kind;
+        const char *name;
+        int slot;
+    };
+    static const Entry table[] = {
+        {MIND_MECH_HH, "gnabar", HH_GNABAR}, {MIND_MECH_HH, "gkbar", HH_GKBAR}, {MIND_MECH_HH, "gl", HH_GL},
+        {MIND_MECH_HH, "el", HH_EL},         {MIND_MECH_HH, "ena", HH_ENA},     {MIND_MECH_HH, "ek", HH_EK},
+        {MIND_MECH_HH, "m", HH_M},           {MIND_MECH_HH, "h", HH_H},         {MIND_MECH_HH, "n", HH_N},
+        {MIND_MECH_PAS, "g", PAS_G},         {MIND_MECH_PAS, "e", PAS_E},
+        {MIND_MECH_EXPSYN, "tau", ES_TAU},   {MIND_MECH_EXPSYN, "e", ES_E},     {MIND_MECH_EXPSYN, "g", ES_G},
+        {MIND_MECH_EXP2SYN, "tau1", E2_TAU1}, {MIND_MECH_EXP2SYN, "tau2", E2_TAU2},
+        {MIND_MECH_EXP2SYN, "e", E2_E},      {MIND_MECH_EXP2SYN, "A", E2_A},    {MIND_MECH_EXP2SYN, "B", E2_B},
+        {MIND_MECH_EXP2SYN, "factor", E2_FACTOR},
+        {MIND_MECH_ICLAMP, "del", IC_DEL},   {MIND_MECH_ICLAMP, "dur", IC_DUR}, {MIND_MECH_ICLAMP, "amp", IC_AMP},
+        {MIND_MECH_NETSTIM, "interval", NS_INTERVAL}, {MIND_MECH_NETSTIM, "number", NS_NUMBER},
+        {MIND_MECH_NETSTIM, "start", NS_START},       {MIND_MECH_NETSTIM, "noise", NS_NOISE},
+        {MIND_MECH_NETSTIM, "event", NS_EVENT},       {MIND_MECH_NETSTIM, "on", NS_ON},
+        {MIND_MECH_NETSTIM, "ispike", NS_ISPIKE},
+    };
+    if (!name) return -1;
+    for (const Entry &e : table)
+        if (e.kind == kind && std::strcmp(e.name, name) == 0) return e.slot;
+    return -1;
+}
+
+/* Index of a device slot in a group's staged shared-memory rows, or -1 (read from HBM). */
+int staged_slot(int32_t kind, int slot) {
+    switch (kind) {
+        case MIND_MECH_HH: return slot;
+        case MIND_MECH_EXPSYN: return slot == ES_G ? 0 : -1;
+        case MIND_MECH_EXP2SYN: return slot == E2_A ? 0 : slot == E2_B ? 1 : -1;
+        default: return -1;
     }
 }
 
@@ -398,7 +443,9 @@ int create(const MindLayout *L, MindHandle *h) {
     P.celsius = L->celsius;
     P.seed = L->seed;
     P.ns_group = -1;
-    std::vector<std::vector<int32_t>> dev_row_of(L->n_mechanisms);  // layout row -> device row
+    std::vector<std::vector<int32_t>> &dev_row_of = h->dev_row_of;  // layout row -> device row
+    dev_row_of.assign(L->n_mechanisms, {});
+    h->field_slot.assign(L->n_mechanisms, {});
     // Thread t of a cell's CTA owns the local nodes i with i % kCellThreads == t, so that the
     // threads of a warp touch consecutive nodes (distinct shared-memory banks).  Each
     // group's rows are sorted by (cell, owner thread, node, layout row): a thread's rows are
@@ -420,6 +467,8 @@ int create(const MindLayout *L, MindHandle *h) {
             if (src[k] < 0)
                 return fail(h, MIND_ELAYOUT, std::string("mechanism lacks field ") + spec.fields[k]);
         }
+        for (int32_t j = 0; j < m.n_fields; ++j)
+            h->field_slot[g].push_back(readable_slot(m.kind, m.field_names ? m.field_names[j] : nullptr));
         const bool artificial = m.kind == MIND_MECH_NETSTIM;
         if (artificial) {
             if (P.ns_group >= 0) return fail(h, MIND_ELAYOUT, "more than one NetStim group");
@@ -476,7 +525,7 @@ int create(const MindLayout *L, MindHandle *h) {
             if ((m.kind == MIND_MECH_HH || m.kind == MIND_MECH_PAS)) {
                 for (int32_t r = 0; r < rows; ++r)
                     if (seg[r] > 1) return fail(h, MIND_ELAYOUT, "density mechanism twice on one node");
-                int slot = m.kind == MIND_MECH_HH ? HH_SCALE : PAS_SCALE;
+                int slot = m.kind == MIND_MECH_HH ? (int)HH_SCALE : (int)PAS_SCALE;
                 for (int32_t r = 0; r < rows; ++r) init.f[slot][r] = L->area[layout_of_packed[node_dev[r]]] * 0.01;
                 if (m.kind == MIND_MECH_PAS)
                     for (int32_t r = 0; r < rows; ++r) {
@@ -660,7 +709,8 @@ int create(const MindLayout *L, MindHandle *h) {
     // launch's dynamic shared memory matches its cells.
     std::vector<int32_t> kinds(L->n_mechanisms);
     for (int32_t g = 0; g < L->n_mechanisms; ++g) kinds[g] = L->mechanisms[g].kind;
-    std::vector<std::vector<int32_t>> group_row_off(L->n_mechanisms);
+    std::vector<std::vector<int32_t>> &group_row_off = h->group_row_off;
+    group_row_off.assign(L->n_mechanisms, {});
     for (int32_t g = 0; g < L->n_mechanisms; ++g) {
         group_row_off[g].assign(ncells + 1, 0);
         if (kinds[g] == MIND_MECH_NETSTIM) continue;
@@ -742,40 +792,107 @@ int check_device_error(MindHandle *h) {
     return fail(h, code, what);
 }
 
-int set_records(MindHandle *h, const MindRecord *records, int32_t nrec, int64_t samples) {
-    Params &P = h->P;
-    std::vector<std::vector<std::pair<int32_t, int32_t>>> by_cell(h->ncells);
-    std::vector<int64_t> global(nrec);
-    for (int32_t k = 0; k < nrec; ++k) {
-        if (records[k].kind != MIND_RECORD_VOLTAGE) return fail(h, MIND_EARG, "unsupported record kind");
-        int32_t node = records[k].node;
-        if (node < 1 || node > h->n_nodes) return fail(h, MIND_EARG, "record node out of range");
-        global[k] = h->packed_of_layout[node - 1];
+/* Where a reference's value lives.  `cell` is the cell whose window kernel records it
+ * (-1: no cell, read only); `code`/`ptr` follow Params::rec_node/rec_ptr; `initial` points
+ * at the value in HBM. */
+struct RecordTarget {
+    int32_t cell = -1;
+    int32_t code = 0;
+    const double *ptr = nullptr;
+    const double *initial = nullptr;
+};
+
+int resolve_record(MindHandle *h, const MindRecord &rec, RecordTarget &out) {
+    const Params &P = h->P;
+    if (rec.kind == MIND_RECORD_VOLTAGE) {
+        if (rec.node < 1 || rec.node > h->n_nodes) return fail(h, MIND_EARG, "record node out of range");
+        const int64_t packed = h->packed_of_layout[rec.node - 1];
+        out.cell = (int32_t)(std::upper_bound(h->node_off.begin(), h->node_off.end(), packed) -
+                             h->node_off.begin() - 1);
+        out.code = (int32_t)(packed - h->node_off[out.cell]);
+        out.ptr = nullptr;
+        out.initial = P.v + packed;
+        return MIND_OK;
     }
-    const std::vector<int64_t> &node_off = h->node_off;
-    for (int32_t k = 0; k < nrec; ++k) {
-        int64_t packed = global[k];
-        int32_t cell = (int32_t)(std::upper_bound(node_off.begin(), node_off.end(), packed) - node_off.begin() - 1);
-        by_cell[cell].push_back({(int32_t)(packed - node_off[cell]), k});
+    if (rec.kind != MIND_RECORD_MECHANISM) return fail(h, MIND_EARG, "unsupported record kind");
+    const int32_t g = rec.group - 1;
+    if (g < 0 || g >= P.ngroups) return fail(h, MIND_EARG, "mechanism group out of range");
+    if (rec.row < 1 || rec.row > (int64_t)h->dev_row_of[g].size()) return fail(h, MIND_EARG, "mechanism row out of range");
+    if (rec.field < 1 || rec.field > (int32_t)h->field_slot[g].size())
+        return fail(h, MIND_EARG, "mechanism field out of range");
+    const int slot = h->field_slot[g][rec.field - 1];
+    if (slot < 0) return fail(h, MIND_EARG, "mechanism field is not kept on the device (ASSIGNED in BREAKPOINT)");
+    const int32_t kind = h->group_init[g].kind;
+    const int32_t dev = h->dev_row_of[g][rec.row - 1];
+    out.initial = P.groups[g].f[slot] + dev;
+    if (kind == MIND_MECH_NETSTIM) {
+        out.cell = -1;   // artificial cells belong to no cell's window
+        return MIND_OK;
     }
-    std::vector<int32_t> off{0}, node, col;
+    const std::vector<int32_t> &off = h->group_row_off[g];
+    out.cell = (int32_t)(std::upper_bound(off.begin(), off.end(), dev) - off.begin() - 1);
+    const int32_t local = dev - off[out.cell];
+    const int ss = staged_slot(kind, slot);
+    if (ss >= 0 && local < (1 << 20)) {
+        out.code = -1 - ((g << 24) | (ss << 20) | local);
+        out.ptr = nullptr;
+    } else if (ss >= 0) {
+        return fail(h, MIND_EARG, "a recorded state row lies beyond 2^20 rows of its cell");
+    } else {
+        out.code = 0;
+        out.ptr = out.initial;   // a parameter: constant through the run
+    }
+    return MIND_OK;
+}
+
+/* Per-cell record tables of a run: rec_off [ncells+1], then per entry (cell-sorted) its
+ * code, HBM pointer and trace column; and per record its first-sample pointer. */
+struct RecordTables {
+    std::vector<int32_t> off, code, col;
+    std::vector<const double *> ptr, initial;
+};
+
+int build_records(MindHandle *h, const MindRecord *records, int32_t nrec, RecordTables &t) {
+    std::vector<std::vector<std::pair<RecordTarget, int32_t>>> by_cell(h->ncells);
+    t.initial.assign(nrec, nullptr);
+    for (int32_t k = 0; k < nrec; ++k) {
+        RecordTarget target;
+        int status = resolve_record(h, records[k], target);
+        if (status) return status;
+        if (target.cell < 0) return fail(h, MIND_EARG, "NetStim fields are read with mind_read_value, not recorded");
+        t.initial[k] = target.initial;
+        by_cell[target.cell].push_back({target, k});
+    }
+    t.off.assign(1, 0);
     for (int32_t c = 0; c < h->ncells; ++c) {
         for (auto &x : by_cell[c]) {
-            node.push_back(x.first);
-            col.push_back(x.second);
+            t.code.push_back(x.first.code);
+            t.ptr.push_back(x.first.ptr);
+            t.col.push_back(x.second);
         }
-        off.push_back((int32_t)node.size());
+        t.off.push_back((int32_t)t.code.size());
     }
+    return MIND_OK;
+}
+
+int set_records(MindHandle *h, const MindRecord *records, int32_t nrec, int64_t samples) {
+    Params &P = h->P;
+    RecordTables t;
+    int status = build_records(h, records, nrec, t);
+    if (status) return status;
     h->release(h->rec_off_dev);
     h->release(h->rec_node_dev);
     h->release(h->rec_col_dev);
-    h->release(h->rec_global_dev);
-    h->rec_off_dev = h->upload(off);
-    h->rec_node_dev = h->upload(node);
-    h->rec_col_dev = h->upload(col);
-    h->rec_global_dev = h->upload(global);
+    h->release(h->rec_ptr_dev);
+    h->release(h->rec_initial_dev);
+    h->rec_off_dev = h->upload(t.off);
+    h->rec_node_dev = h->upload(t.code);
+    h->rec_col_dev = h->upload(t.col);
+    h->rec_ptr_dev = h->upload(t.ptr);
+    h->rec_initial_dev = h->upload(t.initial);
     P.rec_off = h->rec_off_dev;
     P.rec_node = h->rec_node_dev;
+    P.rec_ptr = h->rec_ptr_dev;
     P.rec_col = h->rec_col_dev;
     P.nrec = nrec;
     size_t need = (size_t)samples * (size_t)std::max(nrec, 1);
@@ -795,7 +912,7 @@ int advance(MindHandle *h, int64_t steps, bool record_spikes) {
     P.run_start = h->step;
     CUDA_TRY(h, cudaMemsetAsync(P.rec_spike_count, 0, sizeof(int32_t), h->stream));
     if (P.nrec)
-        record_initial_kernel<<<launch_grid(P.nrec), kThreads, 0, h->stream>>>(P, h->rec_global_dev, P.nrec);
+        record_initial_kernel<<<launch_grid(P.nrec), kThreads, 0, h->stream>>>(P, h->rec_initial_dev, P.nrec);
     CUDA_TRY(h, cudaEventRecord(h->ev_start, h->stream));
     int64_t n0 = h->step;
     const int64_t end = h->step + steps;
@@ -1328,6 +1445,17 @@ int mind_read_voltage(const MindHandle *h, int32_t node, double *value) {
     return e == cudaSuccess ? MIND_OK : MIND_ECUDA;
 }
 
+int mind_read_value(const MindHandle *h, const MindRecord *ref, double *value) {
+    if (!h || !ref || !value) return MIND_EARG;
+    MindHandle *mh = const_cast<MindHandle *>(h);   // only the error text changes
+    RecordTarget target;
+    int status = resolve_record(mh, *ref, target);
+    if (status) return status;
+    // The handle's stream is idle between calls; the device state is the completed boundary.
+    cudaError_t e = cudaMemcpy(value, target.initial, sizeof(double), cudaMemcpyDeviceToHost);
+    return e == cudaSuccess ? MIND_OK : cuda_fail(mh, e, "mind_read_value");
+}
+
 namespace {
 
 /* Grows the staging buffer so that every pending injected event fits one window's batch;
@@ -1455,70 +1583,58 @@ int mind_run_noalloc(MindHandle *h, int64_t steps, const MindRecord *records, in
     if (!h->initialized) return fail(h, MIND_EARG, "simulation is not initialized");
     if (steps < 0 || n_records < 0 || (n_records > 0 && (!records || !trace)))
         return fail(h, MIND_EARG, "invalid run arguments");
-    // Scratch carve: rec_off [ncells+1] i32 | rec_node [n] i32 | rec_col [n] i32 | rec_global [n] i64 | trace.
+    // Scratch carve: rec_off [ncells+1] i32 | rec_node [n] i32 | rec_col [n] i32 | rec_ptr [n] ptr |
+    // rec_initial [n] ptr | trace.
     auto align = [](size_t x) { return (x + 255) & ~(size_t)255; };
     const size_t off_bytes = align((size_t)(h->ncells + 1) * sizeof(int32_t));
     const size_t node_bytes = align((size_t)std::max(n_records, 1) * sizeof(int32_t));
-    const size_t global_bytes = align((size_t)std::max(n_records, 1) * sizeof(int64_t));
+    const size_t ptr_bytes = align((size_t)std::max(n_records, 1) * sizeof(const double *));
     const size_t trace_bytes = (size_t)(steps + 1) * (size_t)n_records * sizeof(double);
-    const size_t need = off_bytes + 2 * node_bytes + global_bytes + trace_bytes;
+    const size_t need = off_bytes + 2 * node_bytes + 2 * ptr_bytes + trace_bytes;
     if (need > MIND_NOALLOC_SCRATCH_BYTES) {
         // Refused before any work: the simulation state is unchanged and stays usable.
         h->error = "mind_run_noalloc needs " + std::to_string(need) + " bytes of scratch; its static array holds " +
                    std::to_string((size_t)MIND_NOALLOC_SCRATCH_BYTES) + " bytes (fewer steps or records per call)";
         return MIND_ECAPACITY;
     }
+    // Record maps (host side), then into the scratch: every entry is written, nothing needs clearing.
+    RecordTables t;
+    int status = build_records(h, records, n_records, t);
+    if (status) return status;
     unsigned char *scratch = nullptr;
-    int status = noalloc_scratch(h, &scratch);
+    status = noalloc_scratch(h, &scratch);
     if (status) return status;
     int32_t *d_off = reinterpret_cast<int32_t *>(scratch);
     int32_t *d_node = reinterpret_cast<int32_t *>(scratch + off_bytes);
     int32_t *d_col = reinterpret_cast<int32_t *>(scratch + off_bytes + node_bytes);
-    int64_t *d_global = reinterpret_cast<int64_t *>(scratch + off_bytes + 2 * node_bytes);
-    double *d_trace = reinterpret_cast<double *>(scratch + off_bytes + 2 * node_bytes + global_bytes);
-
-    // Record maps (host side), then into the scratch: every entry is written, nothing needs clearing.
-    std::vector<std::vector<std::pair<int32_t, int32_t>>> by_cell(h->ncells);
-    std::vector<int64_t> global(n_records);
-    for (int32_t k = 0; k < n_records; ++k) {
-        if (records[k].kind != MIND_RECORD_VOLTAGE) return fail(h, MIND_EARG, "unsupported record kind");
-        const int32_t node = records[k].node;
-        if (node < 1 || node > h->n_nodes) return fail(h, MIND_EARG, "record node out of range");
-        const int64_t packed = h->packed_of_layout[node - 1];
-        global[k] = packed;
-        const int32_t cell =
-            (int32_t)(std::upper_bound(h->node_off.begin(), h->node_off.end(), packed) - h->node_off.begin() - 1);
-        by_cell[cell].push_back({(int32_t)(packed - h->node_off[cell]), k});
-    }
-    std::vector<int32_t> off{0}, local, col;
-    for (int32_t c = 0; c < h->ncells; ++c) {
-        for (auto &x : by_cell[c]) {
-            local.push_back(x.first);
-            col.push_back(x.second);
-        }
-        off.push_back((int32_t)local.size());
-    }
-    CUDA_TRY(h, cudaMemcpyAsync(d_off, off.data(), off.size() * sizeof(int32_t), cudaMemcpyHostToDevice, h->stream));
+    const double **d_ptr = reinterpret_cast<const double **>(scratch + off_bytes + 2 * node_bytes);
+    const double **d_initial = reinterpret_cast<const double **>(scratch + off_bytes + 2 * node_bytes + ptr_bytes);
+    double *d_trace = reinterpret_cast<double *>(scratch + off_bytes + 2 * node_bytes + 2 * ptr_bytes);
+    CUDA_TRY(h, cudaMemcpyAsync(d_off, t.off.data(), t.off.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                                h->stream));
     if (n_records) {
-        CUDA_TRY(h, cudaMemcpyAsync(d_node, local.data(), local.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+        CUDA_TRY(h, cudaMemcpyAsync(d_node, t.code.data(), t.code.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
                                     h->stream));
-        CUDA_TRY(h, cudaMemcpyAsync(d_col, col.data(), col.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+        CUDA_TRY(h, cudaMemcpyAsync(d_col, t.col.data(), t.col.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
                                     h->stream));
-        CUDA_TRY(h, cudaMemcpyAsync(d_global, global.data(), global.size() * sizeof(int64_t),
+        CUDA_TRY(h, cudaMemcpyAsync(d_ptr, t.ptr.data(), t.ptr.size() * sizeof(const double *),
+                                    cudaMemcpyHostToDevice, h->stream));
+        CUDA_TRY(h, cudaMemcpyAsync(d_initial, t.initial.data(), t.initial.size() * sizeof(const double *),
                                     cudaMemcpyHostToDevice, h->stream));
     }
     // Point the run at the scratch for this call; the handle's own record buffers stay untouched.
     Params &P = h->P;
     P.rec_off = d_off;
     P.rec_node = d_node;
+    P.rec_ptr = d_ptr;
     P.rec_col = d_col;
     P.nrec = n_records;
     P.trace = d_trace;
     P.trace_samples = steps + 1;
-    int64_t *own_global = h->rec_global_dev;
-    h->rec_global_dev = d_global;
+    const double **own_initial = h->rec_initial_dev;
+    h->rec_initial_dev = d_initial;
     status = advance(h, steps, false);
-    h->rec_global_dev = own_global;
+    h->rec_initial_dev = own_initial;
     if (status) {
         h->initialized = false;
         return status;

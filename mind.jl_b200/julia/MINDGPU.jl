@@ -19,6 +19,7 @@ const libmindgpu = get(ENV, "MINDGPU_LIBRARY", joinpath(@__DIR__, "..", "lib", "
 
 const MIND_ABI_VERSION = Int32(1)
 const MIND_RECORD_VOLTAGE = Int32(1)
+const MIND_RECORD_MECHANISM = Int32(2)
 const KIND_CODES = Dict(:hh => Int32(1), :pas => Int32(2), :ExpSyn => Int32(3), :Exp2Syn => Int32(4),
                         :NetStim => Int32(5), :IClamp => Int32(6))
 
@@ -68,6 +69,17 @@ end
 struct MindRecord
     kind::Int32
     node::Int32
+    group::Int32
+    row::Int32
+    field::Int32
+end
+
+# VariableRef (src/model/references.jl) -> MindRecord: voltage refs carry the node in `row`.
+function c_record(ref)
+    ref.kind === :voltage && return MindRecord(MIND_RECORD_VOLTAGE, Int32(ref.row), 0, 0, 0)
+    ref.kind === :mechanism &&
+        return MindRecord(MIND_RECORD_MECHANISM, 0, Int32(ref.group), Int32(ref.row), Int32(ref.field))
+    throw(ArgumentError("libmindgpu records :voltage and :mechanism references"))
 end
 
 mutable struct Handle
@@ -146,14 +158,14 @@ function mindgpu_initialize!(model; precision::Symbol = :fp64)
     return model
 end
 
-"""run!: advance to an absolute stop time; voltage records only."""
+"""run!: advance to an absolute stop time; voltage and mechanism-field records."""
 function mindgpu_run!(model, stop_time::Real; records = (), record_spikes::Bool = true)
     h = model.runtime.state::Handle
     step = Ref{Int64}(0)
     now = Ref{Float64}(0.0)
     ccall((:mind_time, libmindgpu), Cint, (Ptr{Cvoid}, Ref{Int64}, Ref{Float64}), h.ptr, step, now)
     count = round(Int, (Float64(stop_time) - now[]) / h.dt)
-    recs = [MindRecord(MIND_RECORD_VOLTAGE, Int32(spec.reference.row)) for spec in records]
+    recs = [c_record(spec.variable) for spec in records]
     check(h.ptr, ccall((:mind_run, libmindgpu), Cint, (Ptr{Cvoid}, Int64, Ptr{MindRecord}, Int32, Int32),
                        h.ptr, count, recs, Int32(length(recs)), Int32(record_spikes)))
     trace = Matrix{Float64}(undef, length(recs), count + 1)   # column-major = sample-major in C
@@ -169,6 +181,16 @@ function mindgpu_run!(model, stop_time::Real; records = (), record_spikes::Bool 
     time = [(step[] + k) * h.dt for k in 0:count]
     traces = Dict(spec.name => trace[k, :] for (k, spec) in enumerate(records))
     return (; time, traces, spike_times = times, spike_sources = sids)
+end
+
+"""read_value: the current value of a :voltage or :mechanism reference."""
+function mindgpu_read_value(model, ref)
+    h = model.runtime.state::Handle
+    value = Ref{Float64}(0.0)
+    rec = Ref(c_record(ref))
+    check(h.ptr, ccall((:mind_read_value, libmindgpu), Cint, (Ptr{Cvoid}, Ref{MindRecord}, Ref{Float64}),
+                       h.ptr, rec, value))
+    return value[]
 end
 
 """inject_spike!: external spike inputs (1-based source indices) fire at absolute times."""

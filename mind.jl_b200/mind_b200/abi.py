@@ -27,6 +27,7 @@ MIND_FP64 = 0
 MIND_MIXED = 1
 
 MIND_RECORD_VOLTAGE = 1
+MIND_RECORD_MECHANISM = 2
 
 STATUS_NAMES = {
     MIND_ECAPACITY: "capacity exhausted",
@@ -88,7 +89,7 @@ class MindLayout(Structure):
 
 
 class MindRecord(Structure):
-    _fields_ = [("kind", c_int32), ("node", c_int32)]
+    _fields_ = [("kind", c_int32), ("node", c_int32), ("group", c_int32), ("row", c_int32), ("field", c_int32)]
 
 
 class MindRunStats(Structure):
@@ -167,6 +168,7 @@ def load_library():
     lib.mind_get_trace.argtypes = [handle, POINTER(c_double), c_int64]
     lib.mind_get_spikes.argtypes = [handle, POINTER(c_double), POINTER(c_int64), c_int64, POINTER(c_int64)]
     lib.mind_read_voltage.argtypes = [handle, c_int32, POINTER(c_double)]
+    lib.mind_read_value.argtypes = [handle, POINTER(MindRecord), POINTER(c_double)]
     lib.mind_inject_event.argtypes = [handle, c_int64, c_double]
     lib.mind_last_error.argtypes = [handle]
     lib.mind_last_error.restype = c_char_p
@@ -195,7 +197,7 @@ def load_library():
     lib.mind_mlp_set_data.argtypes = [handle, f32, f32, c_int64]
     lib.mind_mlp_train.argtypes = [handle, c_int32, c_int32, ctypes.c_float, f32, f32]
     for name in ("mind_create", "mind_initialize", "mind_set_precision", "mind_run", "mind_step",
-                 "mind_time", "mind_get_trace", "mind_get_spikes", "mind_read_voltage",
+                 "mind_time", "mind_get_trace", "mind_get_spikes", "mind_read_voltage", "mind_read_value",
                  "mind_inject_event", "mind_last_run_ms", "mind_destroy", "mind_run_stats",
                  "mind_set_profiling", "mind_run_noalloc", "mind_inject_spikes", "mind_window_steps",
                  "mind_attach_macro", "mind_get_macro_trace", "mind_set_drive_recording", "mind_get_drive",
@@ -210,7 +212,7 @@ def load_library():
 
 EXPORTED_SYMBOLS = (
     "mind_create", "mind_initialize", "mind_set_precision", "mind_run", "mind_step", "mind_time",
-    "mind_get_trace", "mind_get_spikes", "mind_read_voltage", "mind_inject_event",
+    "mind_get_trace", "mind_get_spikes", "mind_read_voltage", "mind_read_value", "mind_inject_event",
     "mind_last_error", "mind_last_run_ms", "mind_destroy", "mind_run_stats", "mind_set_profiling",
     "mind_run_noalloc", "mind_inject_spikes", "mind_window_steps", "mind_attach_macro", "mind_get_macro_trace",
     "mind_set_drive_recording", "mind_get_drive", "mind_attach_surrogate", "mind_mlp_create", "mind_mlp_destroy", "mind_mlp_last_error", "mind_mlp_param_count", "mind_mlp_set_params",

@@ -20,11 +20,21 @@ from . import abi
 
 @dataclass(frozen=True)
 class RecordSpec:
-    """A recorded quantity (src/model/references.jl:4-12); this build records voltages."""
+    """A recorded or read quantity: RecordSpec / VariableRef (src/model/references.jl:4-80).
 
-    node: int  # global 1-based node
+    A voltage reference names a 1-based node; a mechanism reference a 1-based group, row and
+    field (column of the group's data).  The fields a mechanism reference may name are the
+    PARAMETER and STATE fields kept on the device (include/mindgpu.h, MindRecord)."""
+
+    node: int  # voltage: global 1-based node
     name: str
     kind: int = abi.MIND_RECORD_VOLTAGE
+    group: int = 0   # mechanism: 1-based group of the layout
+    row: int = 0     # mechanism: 1-based row of that group
+    field: int = 0   # mechanism: 1-based column of the group's data
+
+    def to_c(self) -> abi.MindRecord:
+        return abi.MindRecord(self.kind, self.node, self.group, self.row, self.field)
 
 
 @dataclass
@@ -90,8 +100,7 @@ class DeviceState:
     def run_steps(self, steps: int, records: Sequence[RecordSpec], record_spikes: bool = True):
         recs = (abi.MindRecord * max(1, len(records)))()
         for i, r in enumerate(records):
-            recs[i].kind = r.kind
-            recs[i].node = r.node
+            recs[i] = r.to_c()
         start_step, _ = self.time()
         abi.check(self.lib, self.handle,
                   self.lib.mind_run(self.handle, steps, recs, len(records), 1 if record_spikes else 0))
@@ -146,6 +155,12 @@ class DeviceState:
     def read_voltage(self, node: int) -> float:
         value = ctypes.c_double()
         abi.check(self.lib, self.handle, self.lib.mind_read_voltage(self.handle, node, ctypes.byref(value)))
+        return value.value
+
+    def read_value(self, ref: RecordSpec) -> float:
+        value = ctypes.c_double()
+        c = ref.to_c()
+        abi.check(self.lib, self.handle, self.lib.mind_read_value(self.handle, ctypes.byref(c), ctypes.byref(value)))
         return value.value
 
     def inject_event(self, connection: int, t: float) -> None:
@@ -232,6 +247,39 @@ def inject_spike(model, source, t: float):
 def voltage_record(model, cell, *, section: str = "soma", x: float = 0.5, name=None) -> RecordSpec:
     node = model.layout.voltage_node(cell.index, section, x)
     return RecordSpec(node, name if name is not None else f"v_{cell.gid}")
+
+
+def mechanism_ref(model, group, row: int, field, *, name=None) -> RecordSpec:
+    """mechanism_ref(plan, :mechanism, group, row, field) (src/model/references.jl:43-73):
+    `group` is a 1-based group index or a mechanism name (its first group), `row` 1-based,
+    `field` a MOD field name or a 1-based column."""
+    layout = model.layout
+    if layout is None:
+        raise ValueError("model is not built")
+    if isinstance(group, str):
+        matches = [i for i, g in enumerate(layout.groups) if g.mechanism.name == group]
+        if not matches:
+            raise ValueError(f"no {group} group in the layout")
+        gi = matches[0]
+    else:
+        gi = int(group) - 1
+        if not 0 <= gi < len(layout.groups):
+            raise ValueError("invalid mechanism group")
+    mech = layout.groups[gi].mechanism
+    col = mech.field_index(field) if isinstance(field, str) else int(field) - 1
+    if not 0 <= col < len(mech.fields):
+        raise ValueError("invalid mechanism field")
+    if not 1 <= int(row) <= layout.groups[gi].rows:
+        raise ValueError("invalid mechanism row")
+    label = name if name is not None else f"mechanism.{gi + 1}.{int(row)}.{mech.fields[col]}"
+    return RecordSpec(0, label, abi.MIND_RECORD_MECHANISM, gi + 1, int(row), col + 1)
+
+
+def read_value(model, ref: RecordSpec) -> float:
+    """read_value(state, selection) (src/runtime/state.jl:585-599)."""
+    if model.state is None:
+        raise ValueError("simulation is not initialized")
+    return model.state.read_value(ref)
 
 
 def simulation_time(model) -> float:

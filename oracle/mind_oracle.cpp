@@ -687,8 +687,43 @@ int oracle_run_macro(const MindLayout *layout, const MindMacroLayout *macro, int
         o.initialize();
         status = o.error;
     }
+    // Recorded values: a node's v, or a kept mechanism field of a layout row (the MindRecord
+    // reference rules of include/mindgpu.h; NetStim fields are not recorded).
+    std::vector<const std::vector<double> *> rec_vec(nrec, nullptr);
+    std::vector<int64_t> rec_idx(nrec, 0);
+    for (int32_t k = 0; k < nrec && !status; ++k) {
+        const MindRecord &r = records[k];
+        if (r.kind == MIND_RECORD_VOLTAGE) {
+            if (r.node < 1 || r.node > o.n) status = o.fail(MIND_EARG, "record node out of range");
+            rec_vec[k] = &o.v;
+            rec_idx[k] = r.node - 1;
+            continue;
+        }
+        if (r.kind != MIND_RECORD_MECHANISM || r.group < 1 || r.group > layout->n_mechanisms) {
+            status = o.fail(MIND_EARG, "unsupported record");
+            break;
+        }
+        const MindMechanism &m = layout->mechanisms[r.group - 1];
+        const Group &G = o.groups[r.group - 1];
+        if (r.row < 1 || r.row > G.rows || r.field < 1 || r.field > m.n_fields || m.kind == MIND_MECH_NETSTIM) {
+            status = o.fail(MIND_EARG, "mechanism record out of range");
+            break;
+        }
+        const char *const *names = m.kind == MIND_MECH_HH       ? HH_NAMES
+                                   : m.kind == MIND_MECH_PAS    ? PAS_NAMES
+                                   : m.kind == MIND_MECH_EXPSYN ? ES_NAMES
+                                   : m.kind == MIND_MECH_EXP2SYN ? E2_NAMES
+                                                                 : IC_NAMES;
+        for (size_t slot = 0; slot < G.f.size(); ++slot)
+            if (std::strcmp(names[slot], m.field_names[r.field - 1]) == 0) rec_vec[k] = &G.f[slot];
+        if (!rec_vec[k]) {
+            status = o.fail(MIND_EARG, "mechanism field is not kept");
+            break;
+        }
+        rec_idx[k] = r.row - 1;
+    }
     auto record = [&](int64_t sample) {
-        for (int32_t k = 0; k < nrec; ++k) trace[sample * nrec + k] = o.v[records[k].node - 1];
+        for (int32_t k = 0; k < nrec; ++k) trace[sample * nrec + k] = (*rec_vec[k])[rec_idx[k]];
     };
     auto t0 = std::chrono::steady_clock::now();
     if (!status) {

@@ -111,9 +111,12 @@ class OracleResult:
     macro_trace: np.ndarray = None   # [macro boundaries, regions], with regions
 
 
-def run(layout, steps: int, record_nodes=(), threads: int = 1, spike_cap: int = 1 << 22, macro=None) -> OracleResult:
+def run(layout, steps: int, record_nodes=(), threads: int = 1, spike_cap: int = 1 << 22, macro=None,
+        records=None) -> OracleResult:
     """Initialize the layout (and the regions of `macro`, a MacroModel) on the CPU and advance
-    `steps` micro steps; with regions, `macro_trace` holds out(k) for k = 0 .. steps / (dt_macro/dt)."""
+    `steps` micro steps; with regions, `macro_trace` holds out(k) for k = 0 .. steps / (dt_macro/dt).
+    `records` (objects with kind, node, group, row, field, such as RecordSpec) replaces
+    `record_nodes` (voltages of 1-based nodes) when given."""
     import sys
 
     pkg = os.path.join(os.path.dirname(HERE), "mind.jl_b200")
@@ -123,11 +126,14 @@ def run(layout, steps: int, record_nodes=(), threads: int = 1, spike_cap: int = 
 
     lib = _load()
     c_layout = layout.to_c()
-    nodes = list(record_nodes)
-    recs = (abi.MindRecord * max(1, len(nodes)))()
-    for i, node in enumerate(nodes):
-        recs[i].kind = abi.MIND_RECORD_VOLTAGE
-        recs[i].node = int(node)
+    if records is None:
+        specs = [(abi.MIND_RECORD_VOLTAGE, int(node), 0, 0, 0) for node in record_nodes]
+    else:
+        specs = [(r.kind, r.node, r.group, r.row, r.field) for r in records]
+    nodes = specs
+    recs = (abi.MindRecord * max(1, len(specs)))()
+    for i, spec in enumerate(specs):
+        recs[i] = abi.MindRecord(*spec)
     trace = np.zeros((steps + 1, max(1, len(nodes))))
     spike_t = np.zeros(spike_cap)
     spike_sid = np.zeros(spike_cap, dtype=np.int64)

@@ -1,0 +1,66 @@
+"""Mechanism references (MindRecord kind MIND_RECORD_MECHANISM) in the CPU oracle.
+
+A reference names a layout column of one row (mechanism_ref, src/model/references.jl:43-73);
+the kept columns are PARAMETER and STATE fields.  These checks run the oracle alone: a
+recorded parameter stays at its layout value, a synaptic state decays by the cnexp factor
+between events, hh's gates start at their steady state, and an ASSIGNED field is refused.
+"""
+import numpy as np
+
+import mind_b200 as mb
+import netcases
+import oracle
+from mind_b200 import abi
+
+
+def _model():
+    model = netcases.recurrent_trees(n_cells=4, synapses=6)
+    mb.build(model)
+    return model
+
+
+def test_parameter_and_state_records():
+    model = _model()
+    layout = model.layout
+    steps = 2000
+    syn = [g for g in layout.groups if g.mechanism.name == "Exp2Syn"][0]
+    pas = mb.mechanism_ref(model, "pas", 3, "g")
+    amp = mb.mechanism_ref(model, "IClamp", 1, "amp")
+    m = mb.mechanism_ref(model, "hh", 1, "m")
+    soma = mb.RecordSpec(layout.voltage_node(1), "v1")
+    a = [mb.mechanism_ref(model, "Exp2Syn", r, "A") for r in range(1, syn.rows + 1)]
+    b = [mb.mechanism_ref(model, "Exp2Syn", r, "B") for r in range(1, syn.rows + 1)]
+    ref = oracle.run(layout, steps, records=[soma, pas, amp, m] + a + b)
+    assert ref.status == 0, ref.message
+    g_pas = [g for g in layout.groups if g.mechanism.name == "pas"][0]
+    np.testing.assert_array_equal(ref.trace[:, 1], g_pas.column("g")[2])
+    assert np.all(ref.trace[:, 2] == 0.3)
+    # hh m starts at minf(v0) in (0, 1) and moves with the voltage
+    assert 0.0 < ref.trace[0, 3] < 1.0 and np.ptp(ref.trace[:, 3]) > 0.0
+    # A and B decay by exp(-dt/tau) per step wherever no event arrived
+    A = ref.trace[:, 4:4 + syn.rows]
+    B = ref.trace[:, 4 + syn.rows:]
+    assert np.all(A >= 0.0) and np.count_nonzero(A.max(axis=0)) >= syn.rows // 2
+    for X, tau in ((A, syn.column("tau1")), (B, syn.column("tau2"))):
+        prev, nxt = X[:-1], X[1:]
+        quiet = (prev > 0.0) & (nxt < prev)
+        assert quiet.sum() > 1000
+        ratio = nxt[quiet] / prev[quiet]
+        want = np.exp(-layout.dt / np.broadcast_to(tau, X.shape)[1:][quiet])
+        np.testing.assert_allclose(ratio, want, rtol=1e-12)
+
+
+def test_assigned_field_is_refused():
+    model = _model()
+    ref = oracle.run(model.layout, 10, records=[mb.mechanism_ref(model, "hh", 1, "ina")])
+    assert ref.status == abi.MIND_EARG
+
+
+def test_mechanism_ref_validates_indices():
+    model = _model()
+    for args in (("hh", 0, "m"), ("hh", 10**6, "m"), ("hh", 1, "nope"), (99, 1, 1)):
+        try:
+            mb.mechanism_ref(model, *args)
+        except ValueError:
+            continue
+        raise AssertionError(f"accepted {args}")
