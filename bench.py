@@ -56,6 +56,8 @@ def parse():
     p.add_argument("--config", type=int, default=2, choices=[2, 3, 4],
                    help="2: 10,000 uneven binary-tree cells (the headline); 3: 1,000 pyramidal-like cells; "
                         "4: 2,000 pyramidal-like cells coupled to 20 Jansen-Rit regions")
+    p.add_argument("--no-autotune", action="store_true",
+                   help="keep 128 threads per cell in every size bin instead of timing the shapes")
     p.add_argument("--precision", default="both", choices=["fp64", "mixed", "both"],
                    help="both: the FP64 headline plus the mixed mode and its accuracy against FP64")
     p.add_argument("--accuracy-ms", type=float, default=0.0,
@@ -412,6 +414,9 @@ def main():
                                                                           local_rank)
             continue
         mb.initialize(model, precision=precision)
+        # launch shape per size bin, timed on trial windows before the measurement (setup,
+        # like the build; the state restarts at t = 0)
+        shapes = mb.autotune(model, windows=3) if not args.no_autotune else model.state.bin_threads()
         model.state.set_profiling(True)
         dt = layout.dt
         mb.run(model, args.warmup * dt, record_spikes=False)
@@ -444,6 +449,7 @@ def main():
         runs[precision] = (np.stack([e2e_result.traces[r.name] for r in soma]), e2e_result.spike_sources,
                            e2e_result.spike_times)
         results[precision] = {
+            "bin_threads": shapes,
             "value": value, "ms_per_step": run_ms / args.steps, "window_ms": window_ms,
             "window_launches": stats.window_launches, "launches": stats.launches, "window_steps": stats.window_steps,
             "bins": stats.bins, "algo_bytes_per_step": algo, "achieved_gbs": achieved,
@@ -468,7 +474,8 @@ def main():
                    "parallelism": (f"cells sharded over {world} GPUs, spike all-gather per window" if sharded
                                    else f"replica x{world}" if world > 1 else "1 GPU"),
                    "l2": "working set larger than L2 (no flush needed)",
-                   "window_steps": head["window_steps"], "size_bins": head["bins"]},
+                   "window_steps": head["window_steps"], "size_bins": head["bins"],
+                   "threads_per_cell_by_bin": head.get("bin_threads")},
         "e2e": {"value": head["e2e"], "unit": UNIT, "h2d_bytes_per_step": head["h2d"],
                 "d2h_bytes_per_step": head["d2h"]},
         "roofline": {
@@ -485,7 +492,8 @@ def main():
         },
         "gpu_launches": head["launches"] + 2,
         "clocks": clocks,
-        "modes": {k: {"value": v["value"], "ms_per_step": v["ms_per_step"], "e2e": v["e2e"]}
+        "modes": {k: {"value": v["value"], "ms_per_step": v["ms_per_step"], "e2e": v["e2e"],
+                      "threads_per_cell_by_bin": v.get("bin_threads")}
                   for k, v in results.items()},
         "accuracy": (mixed_accuracy(layout, runs["fp64"], runs["mixed"], args.warmup, args.steps)
                      if "fp64" in runs and "mixed" in runs else None),

@@ -211,6 +211,22 @@ int mind_inject_event(MindHandle *h, int64_t edge, double t);
  * MIND_EARG, with nothing queued, for any other source or a delivery in the past. */
 int mind_inject_spikes(MindHandle *h, int64_t n, const int64_t *sources, const double *times);
 
+/*
+ * mind_autotune: the launch shape of each cell-size bin.  A bin's cells run one per CTA of
+ * 128 threads (kCellThreads) or of 64 threads (each thread serving two owner slots, so the
+ * arithmetic and its order are the same); smaller CTAs let more cells share an SM when
+ * shared memory allows it.  The call times `windows` device windows (0: 4) from a fresh
+ * initialize for the current shape and, bin by bin, for the other one, keeps a change that
+ * is more than 2% faster, and initializes again: the state returns to t = 0 and events
+ * injected before the call are dropped, as at any mind_initialize.  It needs a handle
+ * initialized at step 0 and takes the precision set for it.  No reference counterpart
+ * (the reference launches fixed shapes).  mind_bin_threads reports the shapes (*n_bins
+ * receives the bin count), mind_set_bin_threads sets them (64 or 128 per bin).
+ */
+int mind_autotune(MindHandle *h, int32_t windows);
+int mind_bin_threads(const MindHandle *h, int32_t *threads, int32_t cap, int32_t *n_bins);
+int mind_set_bin_threads(MindHandle *h, const int32_t *threads, int32_t n_bins);
+
 /* Steps per device window: the largest step count a run advances without routing cell
  * spikes, set by the shortest NetCon delay out of cell detectors and external inputs.
  * A host that exchanges spikes with other handles runs at most this many steps between

@@ -412,11 +412,12 @@ __device__ __forceinline__ void apply_event(const StagedGroup &G, int32_t row, d
  * multiply stays on the dependency chain, the next node's operands being loaded
  * before the current division.
  */
+template <int NT>
 __device__ __forceinline__ void hines_exact(double *sd, double *sr, const double *sa, double *sv, double *sxd,
                                             double *sxr, const int32_t *ctop, const int32_t *clen,
                                             const int32_t *cpar, const int32_t *ckoff, const int32_t *ckids,
                                             const int32_t *lvc, int32_t nlev, bool &singular) {
-    constexpr int32_t T = kCellThreads;
+    constexpr int32_t T = NT;
     const int32_t tid = threadIdx.x;
     for (int32_t lv = 0; lv < nlev; ++lv) {
         for (int32_t ch = lvc[lv] + tid; ch < lvc[lv + 1]; ch += T) {
@@ -515,11 +516,12 @@ __device__ __forceinline__ void hines_exact(double *sd, double *sr, const double
  * node, f = a/D in place of D and R/D in place of R, so the back-substitution is one
  * FMA per node, x = f x_p + R/D; the pivot chain is D -> 1/D -> (a^2)(1/D) -> next D.
  */
+template <int NT>
 __device__ __forceinline__ void hines_mixed(double *sd, double *sr, const double *sa, double *sv, double *sxd,
                                             double *sxr, const int32_t *ctop, const int32_t *clen,
                                             const int32_t *cpar, const int32_t *ckoff, const int32_t *ckids,
                                             const int32_t *lvc, int32_t nlev, bool &singular) {
-    constexpr int32_t T = kCellThreads;
+    constexpr int32_t T = NT;
     const int32_t tid = threadIdx.x;
     for (int32_t lv = 0; lv < nlev; ++lv) {
         for (int32_t ch = lvc[lv] + tid; ch < lvc[lv + 1]; ch += T) {
@@ -614,15 +616,17 @@ __device__ __forceinline__ void hines_mixed(double *sd, double *sr, const double
  * one chain per thread; along a chain only subtract -> divide -> multiply stays
  * on the dependency chain, the next node's operands being loaded ahead.
  */
-template <bool MIXED>
-__global__ void __launch_bounds__(kCellThreads, 5) window_kernel(const Params P, const int32_t *cells, int64_t n0,
-                                                              int32_t W) {
+template <bool MIXED, int NT>
+__global__ void __launch_bounds__(NT, NT == kCellThreads ? 5 : 10) window_kernel(const Params P, const int32_t *cells,
+                                                                               int64_t n0, int32_t W) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int32_t s_nev;
     __shared__ StagedGroup sg[kMaxGroups];
     const int32_t c = cells[blockIdx.x];
     const int32_t tid = threadIdx.x;
-    constexpr int32_t T = kCellThreads;
+    constexpr int32_t T = NT;            // threads of this launch
+    constexpr int32_t O = kCellThreads;  // owner slots: node i belongs to slot i % O
+    static_assert(O % T == 0, "a thread serves whole owner slots");
     const int64_t nb = P.node_off[c];
     const int32_t n = (int32_t)(P.node_off[c + 1] - nb);
     const int32_t cb = P.chain_off[c];
@@ -669,7 +673,7 @@ __global__ void __launch_bounds__(kCellThreads, 5) window_kernel(const Params P,
     int32_t *ckids = ip; ip += nkids;
     int32_t *lvc = ip; ip += nlev + 1;
     int32_t *sorder = ip; ip += P.inbox_cap;
-    int32_t *spart = ip; ip += P.ngroups * (T + 1);
+    int32_t *spart = ip; ip += P.ngroups * (O + 1);
     int16_t *chain_of = reinterpret_cast<int16_t *>(ip);
     {
         // The launch sized shared memory for this cell's bin; refuse rather than overrun.
@@ -736,7 +740,7 @@ __global__ void __launch_bounds__(kCellThreads, 5) window_kernel(const Params P,
     if (tid == 0) ckoff[nch] = nkids;
     for (int32_t k = tid; k < nkids; k += T) ckids[k] = P.chain_kids[kb + k];
     for (int32_t k = tid; k <= nlev; k += T) lvc[k] = P.level_chain[lv0 + k];
-    for (int32_t k = tid; k < P.ngroups * (T + 1); k += T) spart[k] = P.part[(int64_t)c * P.ngroups * (T + 1) + k];
+    for (int32_t k = tid; k < P.ngroups * (O + 1); k += T) spart[k] = P.part[(int64_t)c * P.ngroups * (O + 1) + k];
     if (tid == 0) {
         int32_t count = P.inbox_count[c];
         if (count > P.inbox_cap) {
@@ -848,13 +852,13 @@ __global__ void __launch_bounds__(kCellThreads, 5) window_kernel(const Params P,
         }
         __syncthreads();  // NET_RECEIVE above wrote staged synapse state
 
-        // 3-5. Thread t owns the nodes i with i % T == t (a warp's lanes touch consecutive
-        //      nodes, so shared memory serves them without bank conflicts) and the rows of
-        //      every group on them, which the device row order keeps as one range per
-        //      thread.  The mechanism sums of a node are accumulated in group order, rows in
-        //      row order, by one thread, and its assembly follows without a barrier (it reads
-        //      only the unchanged v of neighbours).  Parameters are streamed from HBM through
-        //      the read-only path.
+        // 3-5. Node i belongs to owner slot i % O and thread t serves the slots t, t + T, ...
+        //      (a warp's lanes touch consecutive nodes, so shared memory serves them without
+        //      bank conflicts), with the rows of every group on those nodes, which the device
+        //      row order keeps as one range per slot.  The mechanism sums of a node are
+        //      accumulated in group order, rows in row order, by one thread, and its assembly
+        //      follows without a barrier (it reads only the unchanged v of neighbours).
+        //      Parameters are streamed from HBM through the read-only path.
         for (int32_t i = tid; i < n; i += T) {
             sd[i] = 0.0;
             sr[i] = 0.0;
@@ -863,82 +867,84 @@ __global__ void __launch_bounds__(kCellThreads, 5) window_kernel(const Params P,
         for (int32_t g = 0; g < P.ngroups; ++g) {
             const DevGroup &GG = P.groups[g];
             const StagedGroup G = sg[g];
-            const int32_t lo = spart[g * (T + 1) + tid], hi = spart[g * (T + 1) + tid + 1];
-            if (lo >= hi) continue;
-            if (G.kind == MIND_MECH_PAS) {
-                if (MIXED) continue;  // folded into the node constants of the assembly below
-                const double *pg = GG.f[PAS_G] + G.r0, *pe = GG.f[PAS_E] + G.r0, *ps = GG.f[PAS_SCALE] + G.r0;
-                const int32_t *pn = GG.node + G.r0;
-                for (int32_t r = lo; r < hi; ++r) {
-                    const int32_t node = (int32_t)(__ldg(pn + r) - nb);
-                    const double gp = __ldg(pg + r), ep = __ldg(pe + r), scale = __ldg(ps + r);
-                    const double vv = sv[node];
-                    const double probe = vv + 0.001;
-                    const double shifted = 0.0 + gp * (probe - ep);
-                    const double value = 0.0 + gp * (vv - ep);
-                    sr[node] = sr[node] - scale * value;
-                    sd[node] = sd[node] + milli_quotient<MIXED>(scale * (shifted - value));
-                }
-            } else if (G.kind == MIND_MECH_ICLAMP) {
-                const int32_t *pn = GG.node + G.r0;
-                for (int32_t r = lo; r < hi; ++r) {
-                    const int32_t node = (int32_t)(__ldg(pn + r) - nb);
-                    const int64_t q = (int64_t)G.r0 + r;
-                    const double del = __ldg(GG.f[IC_DEL] + q);
-                    const double i = (tc < del + __ldg(GG.f[IC_DUR] + q) && tc >= del) ? __ldg(GG.f[IC_AMP] + q) : 0.0;
-                    const double shifted = 0.0 - i;
-                    const double value = 0.0 - i;
-                    sr[node] = sr[node] + -1.0 * value;
-                    sd[node] = sd[node] + milli_quotient<MIXED>(1.0 * (shifted - value));
-                }
-            } else if (G.kind == MIND_MECH_HH) {
-                for (int32_t r = lo; r < hi; ++r) {
-                    const int32_t node = G.node[r];
-                    const double vv = sv[node];
-                    const double probe = vv + 0.001;
-                    const double m = G.at(HH_M, r), h = G.at(HH_H, r), nn = G.at(HH_N, r);
-                    if (MIXED) {
-                        // at fixed gates the current is linear in v: dI/dv is the summed conductance
-                        const double gna = G.at(HH_GNABAR, r) * m * m * m * h;
-                        const double gk = G.at(HH_GKBAR, r) * nn * nn * nn * nn;
-                        const double gl = G.at(HH_GL, r);
-                        const double i = gl * (vv - G.at(HH_EL, r)) + gna * (vv - G.at(HH_ENA, r)) +
-                                         gk * (vv - G.at(HH_EK, r));
+            for (int32_t slot = tid; slot < O; slot += T) {
+                const int32_t lo = spart[g * (O + 1) + slot], hi = spart[g * (O + 1) + slot + 1];
+                if (lo >= hi) continue;
+                if (G.kind == MIND_MECH_PAS) {
+                    if (MIXED) continue;  // folded into the node constants of the assembly below
+                    const double *pg = GG.f[PAS_G] + G.r0, *pe = GG.f[PAS_E] + G.r0, *ps = GG.f[PAS_SCALE] + G.r0;
+                    const int32_t *pn = GG.node + G.r0;
+                    for (int32_t r = lo; r < hi; ++r) {
+                        const int32_t node = (int32_t)(__ldg(pn + r) - nb);
+                        const double gp = __ldg(pg + r), ep = __ldg(pe + r), scale = __ldg(ps + r);
+                        const double vv = sv[node];
+                        const double probe = vv + 0.001;
+                        const double shifted = 0.0 + gp * (probe - ep);
+                        const double value = 0.0 + gp * (vv - ep);
+                        sr[node] = sr[node] - scale * value;
+                        sd[node] = sd[node] + milli_quotient<MIXED>(scale * (shifted - value));
+                    }
+                } else if (G.kind == MIND_MECH_ICLAMP) {
+                    const int32_t *pn = GG.node + G.r0;
+                    for (int32_t r = lo; r < hi; ++r) {
+                        const int32_t node = (int32_t)(__ldg(pn + r) - nb);
+                        const int64_t q = (int64_t)G.r0 + r;
+                        const double del = __ldg(GG.f[IC_DEL] + q);
+                        const double i = (tc < del + __ldg(GG.f[IC_DUR] + q) && tc >= del) ? __ldg(GG.f[IC_AMP] + q) : 0.0;
+                        const double shifted = 0.0 - i;
+                        const double value = 0.0 - i;
+                        sr[node] = sr[node] + -1.0 * value;
+                        sd[node] = sd[node] + milli_quotient<MIXED>(1.0 * (shifted - value));
+                    }
+                } else if (G.kind == MIND_MECH_HH) {
+                    for (int32_t r = lo; r < hi; ++r) {
+                        const int32_t node = G.node[r];
+                        const double vv = sv[node];
+                        const double probe = vv + 0.001;
+                        const double m = G.at(HH_M, r), h = G.at(HH_H, r), nn = G.at(HH_N, r);
+                        if (MIXED) {
+                            // at fixed gates the current is linear in v: dI/dv is the summed conductance
+                            const double gna = G.at(HH_GNABAR, r) * m * m * m * h;
+                            const double gk = G.at(HH_GKBAR, r) * nn * nn * nn * nn;
+                            const double gl = G.at(HH_GL, r);
+                            const double i = gl * (vv - G.at(HH_EL, r)) + gna * (vv - G.at(HH_ENA, r)) +
+                                             gk * (vv - G.at(HH_EK, r));
+                            const double scale = G.at(HH_SCALE, r);
+                            sr[node] = sr[node] - scale * i;
+                            sd[node] = sd[node] + scale * (gna + gk + gl);
+                            continue;
+                        }
+                        const double shifted = hh_current(probe, m, h, nn, G.at(HH_GNABAR, r), G.at(HH_GKBAR, r),
+                                                          G.at(HH_GL, r), G.at(HH_EL, r), G.at(HH_ENA, r), G.at(HH_EK, r));
+                        const double value = hh_current(vv, m, h, nn, G.at(HH_GNABAR, r), G.at(HH_GKBAR, r),
+                                                        G.at(HH_GL, r), G.at(HH_EL, r), G.at(HH_ENA, r), G.at(HH_EK, r));
                         const double scale = G.at(HH_SCALE, r);
-                        sr[node] = sr[node] - scale * i;
-                        sd[node] = sd[node] + scale * (gna + gk + gl);
-                        continue;
+                        sr[node] = sr[node] - scale * value;
+                        sd[node] = sd[node] + milli_quotient<MIXED>(scale * (shifted - value));
                     }
-                    const double shifted = hh_current(probe, m, h, nn, G.at(HH_GNABAR, r), G.at(HH_GKBAR, r),
-                                                      G.at(HH_GL, r), G.at(HH_EL, r), G.at(HH_ENA, r), G.at(HH_EK, r));
-                    const double value = hh_current(vv, m, h, nn, G.at(HH_GNABAR, r), G.at(HH_GKBAR, r),
-                                                    G.at(HH_GL, r), G.at(HH_EL, r), G.at(HH_ENA, r), G.at(HH_EK, r));
-                    const double scale = G.at(HH_SCALE, r);
-                    sr[node] = sr[node] - scale * value;
-                    sd[node] = sd[node] + milli_quotient<MIXED>(scale * (shifted - value));
-                }
-            } else if (G.kind == MIND_MECH_EXPSYN || G.kind == MIND_MECH_EXP2SYN) {
-                const bool two = G.kind == MIND_MECH_EXP2SYN;
-                const double *pe = GG.f[two ? E2_E : ES_E] + G.r0;
-                for (int32_t r = lo; r < hi; ++r) {
-                    const int32_t node = G.node[r];
-                    const double e = __ldg(pe + r);
-                    double gs;
-                    if (two)
-                        gs = G.at(1, r) - G.at(0, r);
-                    else
-                        gs = G.at(0, r);
-                    const double vv = sv[node];
-                    if (MIXED) {  // linear in v: the probe's difference quotient is the conductance
-                        sr[node] = sr[node] - gs * (vv - e);
-                        sd[node] = sd[node] + gs;
-                        continue;
+                } else if (G.kind == MIND_MECH_EXPSYN || G.kind == MIND_MECH_EXP2SYN) {
+                    const bool two = G.kind == MIND_MECH_EXP2SYN;
+                    const double *pe = GG.f[two ? E2_E : ES_E] + G.r0;
+                    for (int32_t r = lo; r < hi; ++r) {
+                        const int32_t node = G.node[r];
+                        const double e = __ldg(pe + r);
+                        double gs;
+                        if (two)
+                            gs = G.at(1, r) - G.at(0, r);
+                        else
+                            gs = G.at(0, r);
+                        const double vv = sv[node];
+                        if (MIXED) {  // linear in v: the probe's difference quotient is the conductance
+                            sr[node] = sr[node] - gs * (vv - e);
+                            sd[node] = sd[node] + gs;
+                            continue;
+                        }
+                        const double probe = vv + 0.001;
+                        const double shifted = 0.0 + gs * (probe - e);
+                        const double value = 0.0 + gs * (vv - e);
+                        sr[node] = sr[node] + -1.0 * value;
+                        sd[node] = sd[node] + milli_quotient<MIXED>(1.0 * (shifted - value));
                     }
-                    const double probe = vv + 0.001;
-                    const double shifted = 0.0 + gs * (probe - e);
-                    const double value = 0.0 + gs * (vv - e);
-                    sr[node] = sr[node] + -1.0 * value;
-                    sd[node] = sd[node] + milli_quotient<MIXED>(1.0 * (shifted - value));
                 }
             }
         }
@@ -973,9 +979,9 @@ __global__ void __launch_bounds__(kCellThreads, 5) window_kernel(const Params P,
         // 6-7. Hines elimination level by level, each chain bottom to top into its parent,
         //      then back-substitution root chain first with the voltage update.
         if (MIXED) {
-            hines_mixed(sd, sr, sa, sv, sxd, sxr, ctop, clen, cpar, ckoff, ckids, lvc, nlev, singular);
+            hines_mixed<NT>(sd, sr, sa, sv, sxd, sxr, ctop, clen, cpar, ckoff, ckids, lvc, nlev, singular);
         } else {
-            hines_exact(sd, sr, sa, sv, sxd, sxr, ctop, clen, cpar, ckoff, ckids, lvc, nlev, singular);
+            hines_exact<NT>(sd, sr, sa, sv, sxd, sxr, ctop, clen, cpar, ckoff, ckids, lvc, nlev, singular);
         }
 
         // 8. cnexp state advance on the new voltage (time t + dt).

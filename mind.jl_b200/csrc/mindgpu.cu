@@ -143,6 +143,8 @@ struct MindHandle {
     struct Bin {
         int32_t first, count;
         size_t smem_bytes;
+        int32_t threads = kCellThreads;   // CTA size of the bin's launches (kCellThreads or half)
+        int32_t max_detectors = 0;        // most threshold detectors on one of its cells
     };
     std::vector<Bin> bins;           // cells grouped by shared-memory need
     std::vector<cudaStream_t> bin_streams;   // size bins run concurrently
@@ -597,7 +599,8 @@ int create(const MindLayout *L, MindHandle *h) {
     for (int32_t c = 0; c < ncells; ++c) {
         h->cell_detector.push_back(det_by_cell[c].empty() ? -1 : det_by_cell[c].front().second);
         if ((int32_t)det_by_cell[c].size() > kCellThreads)
-            return fail(h, MIND_ELAYOUT, "more than 64 threshold detectors on one cell");
+            return fail(h, MIND_ELAYOUT, "more than " + std::to_string(kCellThreads) +
+                                             " threshold detectors on one cell");
         for (auto &d : det_by_cell[c]) {
             det_node.push_back(d.first);
             det_source.push_back(d.second);
@@ -743,15 +746,22 @@ int create(const MindLayout *L, MindHandle *h) {
         bin.first = (int32_t)first;
         bin.count = (int32_t)(k - first);
         bin.smem_bytes = top;
+        for (size_t q = first; q < k; ++q)
+            bin.max_detectors = std::max(bin.max_detectors, det_off[need[q].second + 1] - det_off[need[q].second]);
         h->bins.push_back(bin);
     }
     for (auto &x : need) bin_cells.push_back(x.second);
     h->bin_cells = h->upload(bin_cells);
     h->smem_bytes = worst_any;
-    CUDA_TRY(h, cudaFuncSetAttribute(window_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)std::max<size_t>(worst_any, 1)));
-    CUDA_TRY(h, cudaFuncSetAttribute(window_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)std::max<size_t>(worst_any, 1)));
+    const int smem_attr = (int)std::max<size_t>(worst_any, 1);
+    CUDA_TRY(h, cudaFuncSetAttribute(window_kernel<false, kCellThreads>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr));
+    CUDA_TRY(h, cudaFuncSetAttribute(window_kernel<true, kCellThreads>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr));
+    CUDA_TRY(h, cudaFuncSetAttribute(window_kernel<false, kCellThreads / 2>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr));
+    CUDA_TRY(h, cudaFuncSetAttribute(window_kernel<true, kCellThreads / 2>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr));
     CUDA_TRY(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     CUDA_TRY(h, cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming));
     for (size_t b = 0; b < h->bins.size(); ++b) {
@@ -1002,10 +1012,19 @@ int advance(MindHandle *h, int64_t steps, bool record_spikes) {
             cudaStream_t s = h->bin_streams[b];
             cudaStreamWaitEvent(s, h->fork, 0);
             const int32_t *cells = h->bin_cells + bin.first;
-            if (h->precision == MIND_MIXED)
-                window_kernel<true><<<bin.count, kCellThreads, bin.smem_bytes, s>>>(P, cells, n0, W);
-            else
-                window_kernel<false><<<bin.count, kCellThreads, bin.smem_bytes, s>>>(P, cells, n0, W);
+            const bool mixed = h->precision == MIND_MIXED;
+            if (bin.threads == kCellThreads) {
+                if (mixed)
+                    window_kernel<true, kCellThreads><<<bin.count, kCellThreads, bin.smem_bytes, s>>>(P, cells, n0, W);
+                else
+                    window_kernel<false, kCellThreads><<<bin.count, kCellThreads, bin.smem_bytes, s>>>(P, cells, n0, W);
+            } else {
+                constexpr int half = kCellThreads / 2;
+                if (mixed)
+                    window_kernel<true, half><<<bin.count, half, bin.smem_bytes, s>>>(P, cells, n0, W);
+                else
+                    window_kernel<false, half><<<bin.count, half, bin.smem_bytes, s>>>(P, cells, n0, W);
+            }
             cudaEventRecord(h->bin_done[b], s);
             cudaStreamWaitEvent(h->stream, h->bin_done[b], 0);
             ++st.launches;
@@ -1519,6 +1538,68 @@ int mind_inject_spikes(MindHandle *h, int64_t n, const int64_t *sources, const d
             push_injected(h, t + h->edge_delay[e], (int32_t)e, h->edge_target[e]);
     }
     return reserve_injected(h);
+}
+
+namespace {
+
+/* Device time (ms) of `windows` windows from a fresh initialize, after one untimed window. */
+int trial_ms(MindHandle *h, int32_t windows, double *ms) {
+    int status = mind_initialize(h);
+    if (status) return status;
+    status = mind_run(h, h->window, nullptr, 0, 0);
+    if (status) return status;
+    status = mind_run(h, (int64_t)h->window * windows, nullptr, 0, 0);
+    if (status) return status;
+    *ms = h->last_ms;
+    return MIND_OK;
+}
+
+}  // namespace
+
+int mind_autotune(MindHandle *h, int32_t windows) {
+    if (!h) return MIND_EARG;
+    if (!h->initialized || h->step != 0) return fail(h, MIND_EARG, "autotune needs a handle initialized at step 0");
+    if (windows < 0) return fail(h, MIND_EARG, "negative trial window count");
+    if (windows == 0) windows = 4;
+    double best = 0.0;
+    int status = trial_ms(h, windows, &best);
+    if (status) return status;
+    const int32_t half = kCellThreads / 2;
+    for (auto &bin : h->bins) {
+        if (bin.max_detectors > half) continue;   // one detector per thread of the CTA
+        const int32_t keep = bin.threads;
+        bin.threads = keep == kCellThreads ? half : kCellThreads;
+        double ms = 0.0;
+        status = trial_ms(h, windows, &ms);
+        if (status) {
+            bin.threads = keep;
+            return status;
+        }
+        if (ms < 0.98 * best)
+            best = ms;
+        else
+            bin.threads = keep;
+    }
+    return mind_initialize(h);
+}
+
+int mind_bin_threads(const MindHandle *h, int32_t *threads, int32_t cap, int32_t *n_bins) {
+    if (!h || !n_bins || cap < 0 || (cap > 0 && !threads)) return MIND_EARG;
+    *n_bins = (int32_t)h->bins.size();
+    for (int32_t b = 0; b < cap && b < *n_bins; ++b) threads[b] = h->bins[b].threads;
+    return MIND_OK;
+}
+
+int mind_set_bin_threads(MindHandle *h, const int32_t *threads, int32_t n_bins) {
+    if (!h || !threads || n_bins != (int32_t)h->bins.size()) return MIND_EARG;
+    for (int32_t b = 0; b < n_bins; ++b) {
+        if (threads[b] != kCellThreads && threads[b] != kCellThreads / 2)
+            return fail(h, MIND_EARG, "a bin runs 128 or 64 threads per cell");
+        if (threads[b] < h->bins[b].max_detectors)
+            return fail(h, MIND_EARG, "a bin's cells have more detectors than its CTA has threads");
+    }
+    for (int32_t b = 0; b < n_bins; ++b) h->bins[b].threads = threads[b];
+    return MIND_OK;
 }
 
 int mind_window_steps(const MindHandle *h, int32_t *steps) {

@@ -177,6 +177,23 @@ class DeviceState:
             self.handle, sources.size, sources.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
             times.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
 
+    def autotune(self, windows: int = 4) -> List[int]:
+        """mind_autotune: time the launch shapes of the size bins and keep the fastest; the
+        state is initialized again (t = 0).  Returns threads per cell of each bin."""
+        abi.check(self.lib, self.handle, self.lib.mind_autotune(self.handle, int(windows)))
+        return self.bin_threads()
+
+    def bin_threads(self) -> List[int]:
+        n = ctypes.c_int32()
+        abi.check(self.lib, self.handle, self.lib.mind_bin_threads(self.handle, None, 0, ctypes.byref(n)))
+        out = (ctypes.c_int32 * max(1, n.value))()
+        abi.check(self.lib, self.handle, self.lib.mind_bin_threads(self.handle, out, n.value, ctypes.byref(n)))
+        return list(out[:n.value])
+
+    def set_bin_threads(self, threads: Sequence[int]) -> None:
+        arr = (ctypes.c_int32 * max(1, len(threads)))(*[int(t) for t in threads])
+        abi.check(self.lib, self.handle, self.lib.mind_set_bin_threads(self.handle, arr, len(threads)))
+
     def window_steps(self) -> int:
         steps = ctypes.c_int32()
         abi.check(self.lib, self.handle, self.lib.mind_window_steps(self.handle, ctypes.byref(steps)))
@@ -273,6 +290,13 @@ def mechanism_ref(model, group, row: int, field, *, name=None) -> RecordSpec:
         raise ValueError("invalid mechanism row")
     label = name if name is not None else f"mechanism.{gi + 1}.{int(row)}.{mech.fields[col]}"
     return RecordSpec(0, label, abi.MIND_RECORD_MECHANISM, gi + 1, int(row), col + 1)
+
+
+def autotune(model, windows: int = 4) -> List[int]:
+    """Choose each size bin's CTA size by timing (mind_autotune); leaves the model initialized at t = 0."""
+    if model.state is None:
+        raise ValueError("simulation is not initialized")
+    return model.state.autotune(windows)
 
 
 def read_value(model, ref: RecordSpec) -> float:
