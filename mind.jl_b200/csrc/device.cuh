@@ -167,6 +167,11 @@ struct Params {
     // per cell, group and thread: first row (relative to the cell's first row of the group)
     // of the thread's rows; thread t owns the local nodes i with i % kCellThreads == t
     const int32_t *part;       // [ncells][ngroups][kCellThreads + 1]
+    // cells whose image exceeds a CTA's shared memory keep it in HBM: slot big_slot[c] of
+    // big_image, big_stride bytes each (big_slot -1 for the others)
+    unsigned char *big_image;
+    const int32_t *big_slot;
+    int64_t big_stride;
     // detectors
     const int32_t *det_off;    // [ncells+1]
     const int32_t *det_node;   // local node

@@ -616,7 +616,7 @@ __device__ __forceinline__ void hines_mixed(double *sd, double *sr, const double
  * one chain per thread; along a chain only subtract -> divide -> multiply stays
  * on the dependency chain, the next node's operands being loaded ahead.
  */
-template <bool MIXED, int NT>
+template <bool MIXED, int NT, bool GLOBAL_IMAGE = false>
 __global__ void __launch_bounds__(NT, NT == kCellThreads ? 5 : 10) window_kernel(const Params P, const int32_t *cells,
                                                                                int64_t n0, int32_t W) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -636,8 +636,11 @@ __global__ void __launch_bounds__(NT, NT == kCellThreads ? 5 : 10) window_kernel
     const int32_t lv0 = P.level_off[c];
     const int32_t nlev = P.level_off[c + 1] - lv0 - 1;
 
-    // ---- carve shared memory (order fixed by cell_smem_bytes) ----
-    double *dp = reinterpret_cast<double *>(smem_raw);
+    // ---- carve the cell image (order fixed by cell_smem_bytes): shared memory, or for a
+    //      cell larger than one CTA's shared memory its own slot of an HBM buffer ----
+    unsigned char *image = smem_raw;
+    if (GLOBAL_IMAGE) image = P.big_image + (int64_t)P.big_slot[c] * P.big_stride;
+    double *dp = reinterpret_cast<double *>(image);
     double *sv = dp; dp += n;
     double *sd = dp; dp += n;
     double *sr = dp; dp += n;
@@ -676,10 +679,13 @@ __global__ void __launch_bounds__(NT, NT == kCellThreads ? 5 : 10) window_kernel
     int32_t *spart = ip; ip += P.ngroups * (O + 1);
     int16_t *chain_of = reinterpret_cast<int16_t *>(ip);
     {
-        // The launch sized shared memory for this cell's bin; refuse rather than overrun.
+        // The launch sized the image for this cell's bin; refuse rather than overrun.
         uint32_t dynamic_bytes;
-        asm volatile("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dynamic_bytes));
-        const size_t used = (size_t)(reinterpret_cast<unsigned char *>(chain_of + n) - smem_raw);
+        if (GLOBAL_IMAGE)
+            dynamic_bytes = (uint32_t)P.big_stride;
+        else
+            asm volatile("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dynamic_bytes));
+        const size_t used = (size_t)(reinterpret_cast<unsigned char *>(chain_of + n) - image);
         if (used > dynamic_bytes) {
             if (tid == 0) raise_error(P.error, MIND_ELAYOUT);
             return;

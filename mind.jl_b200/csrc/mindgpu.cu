@@ -145,6 +145,7 @@ struct MindHandle {
         size_t smem_bytes;
         int32_t threads = kCellThreads;   // CTA size of the bin's launches (kCellThreads or half)
         int32_t max_detectors = 0;        // most threshold detectors on one of its cells
+        bool global_image = false;        // cells too large for shared memory: image in HBM
     };
     std::vector<Bin> bins;           // cells grouped by shared-memory need
     std::vector<cudaStream_t> bin_streams;   // size bins run concurrently
@@ -726,6 +727,8 @@ int create(const MindLayout *L, MindHandle *h) {
         CellShape shape{};
         shape.n = (int32_t)(node_off[c + 1] - node_off[c]);
         shape.nch = chain_off[c + 1] - chain_off[c];
+        if (shape.nch > 32767)   // the window kernel keeps a node's chain as int16
+            return fail(h, MIND_ELAYOUT, "a cell has more than 32767 unbranched chains");
         shape.nkids = chain_kid_off[chain_off[c + 1]] - chain_kid_off[chain_off[c]];
         shape.nlev = level_off[c + 1] - level_off[c] - 1;
         for (int32_t g = 0; g < L->n_mechanisms; ++g) shape.rows[g] = group_row_off[g][c + 1] - group_row_off[g][c];
@@ -733,27 +736,41 @@ int create(const MindLayout *L, MindHandle *h) {
         need[c] = {bytes, c};
         worst_any = std::max(worst_any, bytes);
     }
-    if (worst_any > 227 * 1024)
-        return fail(h, MIND_ELAYOUT, "a cell needs more shared memory than one CTA has (" +
-                                         std::to_string(worst_any) + " bytes)");
     std::stable_sort(need.begin(), need.end(), [](const auto &x, const auto &y) { return x.first > y.first; });
+    // A cell whose image exceeds what one CTA can add to the kernel's static shared memory
+    // keeps its image in an HBM slot (one bin, launched without dynamic shared memory).
+    const size_t smem_limit = 227 * 1024 - 1024;
+    size_t n_big = 0, big_bytes = 0;
+    while (n_big < need.size() && need[n_big].first > smem_limit) big_bytes = std::max(big_bytes, need[n_big++].first);
+    std::vector<int32_t> big_slot(ncells, -1);
+    P.big_stride = (int64_t)((big_bytes + 255) / 256 * 256);
+    for (size_t k = 0; k < n_big; ++k) big_slot[need[k].second] = (int32_t)k;
+    P.big_image = n_big ? h->alloc<unsigned char>(n_big * (size_t)P.big_stride) : nullptr;
+    P.big_slot = h->upload(big_slot);
+    size_t worst_smem = 0;
     std::vector<int32_t> bin_cells;
     for (size_t k = 0; k < need.size();) {
         size_t top = need[k].first;
         size_t first = k;
-        while (k < need.size() && need[k].first * 4 >= top * 3) ++k;
+        const bool big = k < n_big;
+        if (big)
+            k = n_big;
+        else
+            while (k < need.size() && need[k].first * 4 >= top * 3) ++k;
         MindHandle::Bin bin;
         bin.first = (int32_t)first;
         bin.count = (int32_t)(k - first);
-        bin.smem_bytes = top;
+        bin.smem_bytes = big ? 0 : top;
+        bin.global_image = big;
+        if (!big) worst_smem = std::max(worst_smem, top);
         for (size_t q = first; q < k; ++q)
             bin.max_detectors = std::max(bin.max_detectors, det_off[need[q].second + 1] - det_off[need[q].second]);
         h->bins.push_back(bin);
     }
     for (auto &x : need) bin_cells.push_back(x.second);
     h->bin_cells = h->upload(bin_cells);
-    h->smem_bytes = worst_any;
-    const int smem_attr = (int)std::max<size_t>(worst_any, 1);
+    h->smem_bytes = worst_smem;
+    const int smem_attr = (int)std::max<size_t>(worst_smem, 1);
     CUDA_TRY(h, cudaFuncSetAttribute(window_kernel<false, kCellThreads>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr));
     CUDA_TRY(h, cudaFuncSetAttribute(window_kernel<true, kCellThreads>,
@@ -1013,7 +1030,12 @@ int advance(MindHandle *h, int64_t steps, bool record_spikes) {
             cudaStreamWaitEvent(s, h->fork, 0);
             const int32_t *cells = h->bin_cells + bin.first;
             const bool mixed = h->precision == MIND_MIXED;
-            if (bin.threads == kCellThreads) {
+            if (bin.global_image) {
+                if (mixed)
+                    window_kernel<true, kCellThreads, true><<<bin.count, kCellThreads, 0, s>>>(P, cells, n0, W);
+                else
+                    window_kernel<false, kCellThreads, true><<<bin.count, kCellThreads, 0, s>>>(P, cells, n0, W);
+            } else if (bin.threads == kCellThreads) {
                 if (mixed)
                     window_kernel<true, kCellThreads><<<bin.count, kCellThreads, bin.smem_bytes, s>>>(P, cells, n0, W);
                 else
@@ -1566,7 +1588,7 @@ int mind_autotune(MindHandle *h, int32_t windows) {
     if (status) return status;
     const int32_t half = kCellThreads / 2;
     for (auto &bin : h->bins) {
-        if (bin.max_detectors > half) continue;   // one detector per thread of the CTA
+        if (bin.max_detectors > half || bin.global_image) continue;   // one detector per thread; HBM images: 128
         const int32_t keep = bin.threads;
         bin.threads = keep == kCellThreads ? half : kCellThreads;
         double ms = 0.0;
@@ -1597,6 +1619,8 @@ int mind_set_bin_threads(MindHandle *h, const int32_t *threads, int32_t n_bins) 
             return fail(h, MIND_EARG, "a bin runs 128 or 64 threads per cell");
         if (threads[b] < h->bins[b].max_detectors)
             return fail(h, MIND_EARG, "a bin's cells have more detectors than its CTA has threads");
+        if (h->bins[b].global_image && threads[b] != kCellThreads)
+            return fail(h, MIND_EARG, "cells with their image in HBM run 128 threads");
     }
     for (int32_t b = 0; b < n_bins; ++b) h->bins[b].threads = threads[b];
     return MIND_OK;

@@ -178,3 +178,47 @@ def region_rates(layout, result, macro, t_ms: float, bin_ms: float = 10.0) -> np
         if r is not None and 0 <= b < bins:
             rates[b, r] += 1.0
     return rates / np.maximum(cells, 1.0) / (bin_ms * 1e-3)
+
+
+def flops_per_row(n_in: int = N_FEATURES, hidden: int = 256, layers: int = 3) -> int:
+    """Forward FLOPs of one row (2 per multiply-add of the linear maps); training is 3x."""
+    dims = [n_in] + [hidden] * layers + [1]
+    return 2 * sum(i * o for i, o in zip(dims[:-1], dims[1:]))
+
+
+def throughput(train_steps: int = 40, batch: int = 4096, rows: int = 1 << 16, infer_rows: int = 100_000,
+               seed: int = 1) -> dict:
+    """Training and inference speed of the network on synthetic windows (rows of uniform
+    drive features and 3% positive labels): device ms per Adam step, per inference call,
+    and the tensor-core FLOP rates they imply."""
+    rng = np.random.default_rng(seed)
+    x = rng.uniform(0.0, 1.0, (rows, N_FEATURES)).astype(np.float32)
+    y = (rng.uniform(size=rows) < 0.03).astype(np.float32)
+    net = Mlp(seed=seed)
+    net.train(x, y, 5, batch)                      # warm-up
+    _, ms = net.train(x, y, train_steps, batch)
+    per_step = ms / train_steps
+    xi = rng.uniform(0.0, 1.0, (infer_rows, N_FEATURES)).astype(np.float32)
+    net.predict(xi[:1024])                         # warm-up
+    lib = net.lib
+    out = np.zeros(infer_rows, dtype=np.float32)
+    import time
+    t0 = time.perf_counter()
+    net._check(lib.mind_mlp_predict(net.handle, _f32(xi), infer_rows, _f32(out)))
+    infer_wall = (time.perf_counter() - t0) * 1000.0
+    f = flops_per_row()
+    return {"train_ms_per_step": per_step, "batch": batch,
+            "train_tflops": 3 * f * batch / (per_step / 1000.0) / 1e12,
+            "infer_rows": infer_rows, "infer_wall_ms_with_copies": infer_wall,
+            "flops_per_row_forward": f}
+
+
+if __name__ == "__main__":
+    import argparse
+    import json
+
+    ap = argparse.ArgumentParser(description="surrogate MLP training/inference throughput")
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--batch", type=int, default=4096)
+    args = ap.parse_args()
+    print(json.dumps(throughput(args.steps, args.batch)))

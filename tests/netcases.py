@@ -104,3 +104,40 @@ def coupled_regions(n_regions=3, cells_per_region=4, synapses=8, seed=11, input_
     model.macro = macro
     mb.build(model)
     return model, macro
+
+
+def big_and_small_cells(big_compartments=8000, n_small=3, synapses=12, seed=5):
+    """One cell too large for a CTA's shared memory (its image lives in HBM) beside small
+    ones, with hh somata, pas dendrites, Exp2Syn driven by NetStims and recurrent NetCons."""
+    rng = np.random.default_rng(seed)
+    model = M.MicroModel(celsius=6.3)
+    cells = []
+    for c in range(1 + n_small):
+        soma = mb.Section("soma", label="soma", length=20.0, diameter=20.0, nseg=1)
+        size = big_compartments if c == 0 else int(rng.integers(40, 120))
+        secs = networks._binary_tree(rng, size, soma)
+        cell = M.add_population(model, secs, 1, voltage=-65.0)[0]
+        M.insert(cell, mb.builtin("hh"), sections="soma")
+        M.insert(cell, mb.builtin("pas"), sections="dend", params={"g": 1e-4, "e": -65.0})
+        M.register_spike_source(cell, threshold=-10.0)
+        cells.append((cell, secs))
+    n_cells = len(cells)
+    n = n_cells * synapses
+    owners = np.repeat(np.arange(1, n_cells + 1), synapses)
+    names, xs = [], []
+    for cell, secs in cells:
+        nm, x = networks._dendritic_sites(rng, secs, synapses)
+        names += nm
+        xs.append(x)
+    first = M.add_pointprocesses(model, mb.builtin("Exp2Syn"), owners, names, np.concatenate(xs),
+                                 {"tau1": 0.5, "tau2": 5.0, "e": 0.0})
+    M.connect_many(model, rng.integers(1, n_cells + 1, n), np.arange(first, first + n),
+                   rng.lognormal(math.log(3.0), 0.5, n) / 1000.0, rng.uniform(0.6, 3.0, n))
+    stims = M.add_pointprocesses(model, mb.builtin("NetStim"), np.zeros(n, np.int64), "none", np.zeros(n),
+                                 {"interval": 10.0, "number": 1e9, "start": 0.0, "noise": 1.0})
+    sources = M.register_point_sources(model, np.arange(stims, stims + n))
+    M.connect_many(model, sources, np.arange(first, first + n),
+                   rng.lognormal(math.log(8.0), 0.5, n) / 1000.0, rng.uniform(0.0, 1.0, n))
+    M.add_pointprocesses(model, mb.builtin("IClamp"), np.array([1, 2]), "soma", np.full(2, 0.5),
+                         {"del": 2.0, "dur": 30.0, "amp": 0.8})
+    return model
