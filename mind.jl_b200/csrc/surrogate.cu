@@ -26,16 +26,22 @@
 
 struct MindMlp {
     std::vector<int32_t> dims;       // n_in, hidden..., 1
+    int32_t ld0 = 0;                 // n_in rounded up to 8: row stride of the BF16 inputs and of w0
     std::vector<int64_t> w_off, b_off;
     int64_t n_params = 0;
     float *master = nullptr, *grad = nullptr, *m1 = nullptr, *m2 = nullptr;
     __nv_bfloat16 *wbf = nullptr;    // BF16 copy of the parameters
+    __nv_bfloat16 *w0 = nullptr;     // BF16 first-map weights [dims[1] x ld0], zero past n_in
+    float *gw0 = nullptr;            // FP32 first-map weight gradient [dims[1] x ld0]
+    float *part = nullptr;           // bias-gradient partial sums [chunks x widest]
+    float *loss_hist = nullptr;      // per-step batch losses of a training call
+    int32_t loss_cap = 0;
     int64_t adam_t = 0;
     cublasHandle_t blas = nullptr;
     cudaStream_t stream = nullptr;
     int64_t cap = 0;                 // rows the activation buffers hold
     std::vector<float *> z;          // pre-activations per map [cap x out]
-    std::vector<__nv_bfloat16 *> h;  // inputs of each map [cap x in] (h[0] = X)
+    std::vector<__nv_bfloat16 *> h;  // inputs of each map [cap x in] (h[0] = X, rows of ld0)
     __nv_bfloat16 *dzb = nullptr;    // BF16 gradient of a map's output [cap x widest]
     float *dh = nullptr, *dz = nullptr, *y = nullptr, *loss = nullptr;
     float *data_x = nullptr, *data_y = nullptr;  // training set (FP32 on the device)
@@ -109,35 +115,75 @@ __global__ void to_bf16_kernel(const float *x, __nv_bfloat16 *out, int64_t n) {
         out[k] = __float2bfloat16(x[k]);
 }
 
-/* db[c] = sum over rows of dz[r][c] (one warp per column). */
-__global__ void colsum_kernel(const float *dz, float *db, int64_t rows, int32_t cols) {
-    const int32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (warp >= cols) return;
+/* Bias gradients db[c] = sum over rows of dz[r][c], in a fixed order: block (x, y) of
+ * 32 x 8 threads sums columns 32x.. of the rows of chunk y (a warp reads 32 consecutive
+ * columns of one row), the 8 row phases are added in order into part[y][c]; then
+ * colsum_finish adds the chunks in order. */
+constexpr int kColChunk = 128;
+__global__ void colsum_kernel(const float *dz, float *part, int64_t rows, int32_t cols) {
+    __shared__ float acc[8][33];
+    const int32_t c = blockIdx.x * 32 + threadIdx.x;
+    const int64_t r0 = (int64_t)blockIdx.y * kColChunk;
     float s = 0.0f;
-    for (int64_t r = lane; r < rows; r += 32) s += dz[r * cols + warp];
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-    if (lane == 0) db[warp] = s;
+    if (c < cols)
+        for (int64_t r = r0 + threadIdx.y; r < rows && r < r0 + kColChunk; r += 8) s += dz[r * cols + c];
+    acc[threadIdx.y][threadIdx.x] = s;
+    __syncthreads();
+    if (threadIdx.y == 0 && c < cols) {
+        float t = acc[0][threadIdx.x];
+        for (int k = 1; k < 8; ++k) t += acc[k][threadIdx.x];
+        part[(int64_t)blockIdx.y * cols + c] = t;
+    }
 }
 
-/* Rows of the training set drawn for one step (Philox-free: a 64-bit mix of step and slot). */
-__global__ void gather_kernel(const float *x, const float *y, __nv_bfloat16 *hx, float *hy, int64_t n, int32_t d,
-                              int32_t batch, uint64_t step) {
-    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < (int64_t)batch * d;
+__global__ void colsum_finish(const float *part, float *db, int32_t chunks, int32_t cols) {
+    for (int32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < cols; c += gridDim.x * blockDim.x) {
+        float t = 0.0f;
+        for (int32_t k = 0; k < chunks; ++k) t += part[(int64_t)k * cols + c];
+        db[c] = t;
+    }
+}
+
+/* FP32 rows [n x d] -> BF16 rows of stride ld, zero past d. */
+__global__ void to_bf16_rows_kernel(const float *x, __nv_bfloat16 *out, int64_t n, int32_t d, int32_t ld) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n * ld; k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t row = k / ld;
+        const int32_t col = (int32_t)(k - row * ld);
+        out[k] = __float2bfloat16(col < d ? x[row * d + col] : 0.0f);
+    }
+}
+
+/* First-map weight gradient, [o x ld] -> the packed [o x d] of the parameter vector. */
+__global__ void compact_rows_kernel(const float *in, float *out, int32_t o, int32_t d, int32_t ld) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < (int64_t)o * d;
          k += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t row = k / d, col = k % d;
+        const int64_t row = k / d;
+        out[k] = in[row * ld + (k - row * d)];
+    }
+}
+
+/* Rows of the training set drawn for one step (Philox-free: a 64-bit mix of step and slot),
+ * as BF16 rows of stride ld (zero past d). */
+__global__ void gather_kernel(const float *x, const float *y, __nv_bfloat16 *hx, float *hy, int64_t n, int32_t d,
+                              int32_t ld, int32_t batch, uint64_t step) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < (int64_t)batch * ld;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t row = k / ld, col = k % ld;
         uint64_t s = step * 0x9E3779B97F4A7C15ull + (uint64_t)row * 0xBF58476D1CE4E5B9ull + 0x94D049BB133111EBull;
         s ^= s >> 31;
         s *= 0xD6E8FEB86659FD93ull;
         s ^= s >> 32;
         const int64_t src = (int64_t)(s % (uint64_t)n);
-        hx[k] = __float2bfloat16(x[src * d + col]);
+        hx[k] = __float2bfloat16(col < d ? x[src * d + col] : 0.0f);
         if (col == 0) hy[row] = y[src];
     }
 }
 
-/* Adam (beta1 0.9, beta2 0.999, eps 1e-8) on the FP32 masters, then the BF16 copy. */
+/* Adam (beta1 0.9, beta2 0.999, eps 1e-8) on the FP32 masters, then the BF16 copies (the
+ * first map's weights, the first n0 = o*d parameters after w0_off, also into w0 rows of
+ * stride ld). */
 __global__ void adam_kernel(float *w, const float *g, float *m1, float *m2, __nv_bfloat16 *wbf, int64_t n, float lr,
-                            float c1, float c2) {
+                            float c1, float c2, __nv_bfloat16 *w0, int64_t w0_off, int64_t n0, int32_t d, int32_t ld) {
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
         const float gk = g[k];
         const float a = 0.9f * m1[k] + 0.1f * gk, b = 0.999f * m2[k] + 0.001f * gk * gk;
@@ -146,6 +192,18 @@ __global__ void adam_kernel(float *w, const float *g, float *m1, float *m2, __nv
         const float v = w[k] - lr * (a / c1) / (sqrtf(b / c2) + 1e-8f);
         w[k] = v;
         wbf[k] = __float2bfloat16(v);
+        const int64_t j = k - w0_off;
+        if (j >= 0 && j < n0) w0[(j / d) * ld + j % d] = __float2bfloat16(v);
+    }
+}
+
+/* w0 from the BF16 copy: rows of stride ld, zero past d. */
+__global__ void pad_w0_kernel(const __nv_bfloat16 *wbf, __nv_bfloat16 *w0, int32_t o, int32_t d, int32_t ld) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < (int64_t)o * ld;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t row = k / ld;
+        const int32_t col = (int32_t)(k - row * ld);
+        w0[k] = col < d ? wbf[row * d + col] : __float2bfloat16(0.0f);
     }
 }
 
@@ -165,8 +223,10 @@ int reserve(MindMlp *m, int64_t rows) {
     m->h.assign(L, nullptr);
     for (size_t l = 0; l < L; ++l) {
         MLP_CUDA(m, cudaMalloc(&m->z[l], cap * m->dims[l + 1] * sizeof(float)));
-        MLP_CUDA(m, cudaMalloc(&m->h[l], cap * m->dims[l] * sizeof(__nv_bfloat16)));
+        MLP_CUDA(m, cudaMalloc(&m->h[l], cap * (l == 0 ? m->ld0 : m->dims[l]) * sizeof(__nv_bfloat16)));
     }
+    cudaFree(m->part);
+    MLP_CUDA(m, cudaMalloc(&m->part, ((cap + kColChunk - 1) / kColChunk) * widest * sizeof(float)));
     MLP_CUDA(m, cudaMalloc(&m->dzb, cap * widest * sizeof(__nv_bfloat16)));
     MLP_CUDA(m, cudaMalloc(&m->dh, cap * widest * sizeof(float)));
     MLP_CUDA(m, cudaMalloc(&m->dz, cap * widest * sizeof(float)));
@@ -187,8 +247,10 @@ int gemm_forward(MindMlp *m, const __nv_bfloat16 *A, const __nv_bfloat16 *W, flo
 int forward(MindMlp *m, int64_t rows) {
     const size_t L = m->dims.size() - 1;
     for (size_t l = 0; l < L; ++l) {
-        const int32_t i = m->dims[l], o = m->dims[l + 1];
-        int s = gemm_forward(m, m->h[l], m->wbf + m->w_off[l], m->z[l], rows, i, o);
+        // the first map runs over ld0 columns (zero past n_in) so every leading dimension
+        // is a multiple of 8 BF16 elements
+        const int32_t i = l == 0 ? m->ld0 : m->dims[l], o = m->dims[l + 1];
+        int s = gemm_forward(m, m->h[l], l == 0 ? m->w0 : m->wbf + m->w_off[l], m->z[l], rows, i, o);
         if (s) return s;
         bias_act_kernel<<<grid(rows * o), kT, 0, m->stream>>>(m->z[l], m->master + m->b_off[l],
                                                                l + 1 < L ? m->h[l + 1] : nullptr, rows, o, l + 1 == L);
@@ -203,13 +265,19 @@ int backward(MindMlp *m, int64_t rows) {
     bce_kernel<<<grid(rows), kT, 0, m->stream>>>(m->z[L - 1], m->y, m->dz, m->loss, rows);
     to_bf16_kernel<<<grid(rows), kT, 0, m->stream>>>(m->dz, m->dzb, rows);
     const float one = 1.0f, zero = 0.0f;
+    const int32_t chunks = (int32_t)((rows + kColChunk - 1) / kColChunk);
     for (size_t l = L; l-- > 0;) {
-        const int32_t i = m->dims[l], o = m->dims[l + 1];
+        const int32_t i = l == 0 ? m->ld0 : m->dims[l], o = m->dims[l + 1];
         // dW[o x i] = dz^T h  (column-major: dWc[i x o] = hc[i x rows] * dzc[o x rows]^T)
+        float *dw = l == 0 ? m->gw0 : m->grad + m->w_off[l];
         MLP_BLAS(m, cublasGemmEx(m->blas, CUBLAS_OP_N, CUBLAS_OP_T, i, o, (int)rows, &one, m->h[l], CUDA_R_16BF, i,
-                                 m->dzb, CUDA_R_16BF, o, &zero, m->grad + m->w_off[l], CUDA_R_32F, i, CUBLAS_COMPUTE_32F,
+                                 m->dzb, CUDA_R_16BF, o, &zero, dw, CUDA_R_32F, i, CUBLAS_COMPUTE_32F,
                                  CUBLAS_GEMM_DEFAULT));
-        colsum_kernel<<<(o * 32 + kT - 1) / kT, kT, 0, m->stream>>>(m->dz, m->grad + m->b_off[l], rows, o);
+        if (l == 0)
+            compact_rows_kernel<<<grid((int64_t)o * m->dims[0]), kT, 0, m->stream>>>(m->gw0, m->grad + m->w_off[0], o,
+                                                                                  m->dims[0], m->ld0);
+        colsum_kernel<<<dim3((o + 31) / 32, chunks), dim3(32, 8), 0, m->stream>>>(m->dz, m->part, rows, o);
+        colsum_finish<<<(o + kT - 1) / kT, kT, 0, m->stream>>>(m->part, m->grad + m->b_off[l], chunks, o);
         if (l == 0) break;
         // dh[rows x i] = dz[rows x o] W[o x i]  (column-major: dhc[i x rows] = Wc[i x o] dzc[o x rows])
         MLP_BLAS(m, cublasGemmEx(m->blas, CUBLAS_OP_N, CUBLAS_OP_N, i, (int)rows, o, &one, m->wbf + m->w_off[l],
@@ -223,8 +291,10 @@ int backward(MindMlp *m, int64_t rows) {
 int upload_rows(MindMlp *m, const float *x, int64_t n) {
     int s = reserve(m, n);
     if (s) return s;
-    std::vector<__nv_bfloat16> xb((size_t)n * m->dims[0]);
-    for (size_t k = 0; k < xb.size(); ++k) xb[k] = __float2bfloat16(x[k]);
+    const int32_t d = m->dims[0], ld = m->ld0;
+    std::vector<__nv_bfloat16> xb((size_t)n * ld, __float2bfloat16(0.0f));
+    for (int64_t r = 0; r < n; ++r)
+        for (int32_t c = 0; c < d; ++c) xb[(size_t)r * ld + c] = __float2bfloat16(x[(size_t)r * d + c]);
     MLP_CUDA(m, cudaMemcpyAsync(m->h[0], xb.data(), xb.size() * sizeof(__nv_bfloat16), cudaMemcpyHostToDevice, m->stream));
     MLP_CUDA(m, cudaStreamSynchronize(m->stream));
     return MIND_OK;
@@ -242,7 +312,7 @@ int mind_mlp_forward_device(MindMlp *m, const float *x, int64_t n, float *prob, 
     MLP_CUDA(m, cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
     cudaEventRecord(ready, stream);
     cudaStreamWaitEvent(m->stream, ready, 0);
-    to_bf16_kernel<<<grid(n * m->dims[0]), kT, 0, m->stream>>>(x, m->h[0], n * m->dims[0]);
+    to_bf16_rows_kernel<<<grid(n * m->ld0), kT, 0, m->stream>>>(x, m->h[0], n, m->dims[0], m->ld0);
     int s = forward(m, n);
     if (!s) sigmoid_kernel<<<grid(n), kT, 0, m->stream>>>(m->z.back(), prob, n);
     cudaEventRecord(done, m->stream);
@@ -265,6 +335,7 @@ int mind_mlp_create(const MindMlpConfig *config, MindMlp **out) {
     m->dims.push_back(config->n_in);
     for (int32_t l = 0; l < config->layers; ++l) m->dims.push_back(config->hidden);
     m->dims.push_back(1);
+    m->ld0 = (config->n_in + 7) / 8 * 8;
     for (size_t l = 0; l + 1 < m->dims.size(); ++l) {
         m->w_off.push_back(m->n_params);
         m->n_params += (int64_t)m->dims[l] * m->dims[l + 1];
@@ -292,7 +363,8 @@ int mind_mlp_create(const MindMlpConfig *config, MindMlp **out) {
     if (cudaMalloc(&m->grad, m->n_params * sizeof(float)) != cudaSuccess ||
         cudaMalloc(&m->m1, m->n_params * sizeof(float)) != cudaSuccess ||
         cudaMalloc(&m->m2, m->n_params * sizeof(float)) != cudaSuccess ||
-        cudaMalloc(&m->loss, sizeof(float)) != cudaSuccess)
+        cudaMalloc(&m->loss, sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&m->gw0, (size_t)m->dims[1] * m->ld0 * sizeof(float)) != cudaSuccess)
         return fail(m, MIND_ECUDA, "device allocation failed");
     cudaMemset(m->m1, 0, m->n_params * sizeof(float));
     cudaMemset(m->m2, 0, m->n_params * sizeof(float));
@@ -305,7 +377,8 @@ int mind_mlp_destroy(MindMlp *m) {
     for (float *p : m->z) cudaFree(p);
     for (__nv_bfloat16 *p : m->h) cudaFree(p);
     for (void *p : {(void *)m->master, (void *)m->grad, (void *)m->m1, (void *)m->m2, (void *)m->wbf, (void *)m->dzb,
-                    (void *)m->dh, (void *)m->dz, (void *)m->y, (void *)m->loss, (void *)m->data_x, (void *)m->data_y})
+                    (void *)m->dh, (void *)m->dz, (void *)m->y, (void *)m->loss, (void *)m->data_x, (void *)m->data_y,
+                    (void *)m->w0, (void *)m->gw0, (void *)m->part, (void *)m->loss_hist})
         cudaFree(p);
     if (m->blas) cublasDestroy(m->blas);
     if (m->stream) cudaStreamDestroy(m->stream);
@@ -332,9 +405,12 @@ int mind_mlp_set_params(MindMlp *m, const float *params, int64_t n) {
     if (!m->master) {
         MLP_CUDA(m, cudaMalloc(&m->master, n * sizeof(float)));
         MLP_CUDA(m, cudaMalloc(&m->wbf, n * sizeof(__nv_bfloat16)));
+        MLP_CUDA(m, cudaMalloc(&m->w0, (size_t)m->dims[1] * m->ld0 * sizeof(__nv_bfloat16)));
     }
     MLP_CUDA(m, cudaMemcpyAsync(m->master, params, n * sizeof(float), cudaMemcpyHostToDevice, m->stream));
     to_bf16_kernel<<<grid(n), kT, 0, m->stream>>>(m->master, m->wbf, n);
+    pad_w0_kernel<<<grid((int64_t)m->dims[1] * m->ld0), kT, 0, m->stream>>>(m->wbf + m->w_off[0], m->w0, m->dims[1],
+                                                                           m->dims[0], m->ld0);
     MLP_CUDA(m, cudaStreamSynchronize(m->stream));
     return MIND_OK;
 }
@@ -394,14 +470,20 @@ int mind_mlp_train(MindMlp *m, int32_t steps, int32_t batch, float lr, float *lo
     if (!m || steps < 0 || batch < 1 || m->data_n < 1) return MIND_EARG;
     int s = reserve(m, batch);
     if (s) return s;
+    if (steps > m->loss_cap) {
+        cudaFree(m->loss_hist);
+        m->loss_hist = nullptr;
+        MLP_CUDA(m, cudaMalloc(&m->loss_hist, (size_t)steps * sizeof(float)));
+        m->loss_cap = steps;
+    }
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, m->stream);
     for (int32_t k = 0; k < steps; ++k) {
-        gather_kernel<<<grid((int64_t)batch * m->dims[0]), kT, 0, m->stream>>>(m->data_x, m->data_y, m->h[0], m->y,
-                                                                            m->data_n, m->dims[0], batch,
-                                                                            (uint64_t)(m->adam_t + 1));
+        gather_kernel<<<grid((int64_t)batch * m->ld0), kT, 0, m->stream>>>(m->data_x, m->data_y, m->h[0], m->y,
+                                                                        m->data_n, m->dims[0], m->ld0, batch,
+                                                                        (uint64_t)(m->adam_t + 1));
         s = forward(m, batch);
         if (s) return s;
         s = backward(m, batch);
@@ -409,10 +491,15 @@ int mind_mlp_train(MindMlp *m, int32_t steps, int32_t batch, float lr, float *lo
         m->adam_t += 1;
         const float c1 = 1.0f - std::pow(0.9f, (float)m->adam_t), c2 = 1.0f - std::pow(0.999f, (float)m->adam_t);
         adam_kernel<<<grid(m->n_params), kT, 0, m->stream>>>(m->master, m->grad, m->m1, m->m2, m->wbf, m->n_params,
-                                                             lr, c1, c2);
-        if (losses) MLP_CUDA(m, cudaMemcpyAsync(losses + k, m->loss, sizeof(float), cudaMemcpyDeviceToHost, m->stream));
+                                                             lr, c1, c2, m->w0, m->w_off[0],
+                                                             (int64_t)m->dims[0] * m->dims[1], m->dims[0], m->ld0);
+        // the step's loss stays on the device: no host round trip inside the loop
+        MLP_CUDA(m, cudaMemcpyAsync(m->loss_hist + k, m->loss, sizeof(float), cudaMemcpyDeviceToDevice, m->stream));
     }
     cudaEventRecord(e1, m->stream);
+    if (losses && steps > 0)
+        MLP_CUDA(m, cudaMemcpyAsync(losses, m->loss_hist, (size_t)steps * sizeof(float), cudaMemcpyDeviceToHost,
+                                    m->stream));
     MLP_CUDA(m, cudaStreamSynchronize(m->stream));
     float t = 0.0f;
     cudaEventElapsedTime(&t, e0, e1);
