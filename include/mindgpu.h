@@ -329,6 +329,12 @@ int mind_mlp_gradients(MindMlp *mlp, const float *x, const float *y, int64_t n, 
  * NetCons and counts in its region's bin.  Regions must be attached first (the rate bin
  * is theirs); the handle keeps `mlp`, which must outlive it; mind_initialize follows. */
 int mind_attach_surrogate(MindHandle *h, MindMlp *mlp, const uint8_t *surrogate_cells, float drive_scale);
+/* Between runs, the set of cells the surrogate stands in for (a subset of the attached
+ * set).  A cell leaving it is simulated again from its next step, its membrane and
+ * synapses resuming from their state in HBM (that of mind_initialize when it never ran
+ * detailed); a cell staying keeps its spike history.  This is how a host judge reverts a
+ * population whose surrogate rate drifts from its detailed sample. */
+int mind_set_surrogate_cells(MindHandle *h, const uint8_t *surrogate_cells);
 
 /* Keep a training set on the device; then `steps` Adam steps (beta 0.9/0.999, eps 1e-8) on
  * batches drawn with replacement; losses[k] = the batch loss before step k (may be NULL). */

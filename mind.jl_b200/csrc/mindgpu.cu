@@ -86,6 +86,8 @@ struct MindHandle {
     // cells the surrogate stands in for (mind_attach_surrogate)
     MindMlp *sur_mlp = nullptr;
     int32_t n_sur = 0;
+    std::vector<uint8_t> sur_attached;   // cells named at mind_attach_surrogate (buffer capacity)
+    int32_t sur_cap = 0;
     float sur_scale = 1.0f;
     int32_t *sur_cells = nullptr, *sur_sources = nullptr, *sur_spikes = nullptr;
     float *sur_x = nullptr, *sur_prob = nullptr;
@@ -1384,7 +1386,49 @@ int mind_attach_surrogate(MindHandle *h, MindMlp *mlp, const uint8_t *surrogate_
     h->sur_mlp = mlp;
     h->sur_scale = drive_scale;
     h->n_sur = (int32_t)cells.size();
+    h->sur_cap = h->n_sur;
+    h->sur_attached = mode;
     h->initialized = false;
+    return MIND_OK;
+}
+
+int mind_set_surrogate_cells(MindHandle *h, const uint8_t *surrogate_cells) {
+    if (!h || !surrogate_cells) return MIND_EARG;
+    if (h->sur_cap == 0) return fail(h, MIND_EARG, "no surrogate is attached");
+    for (int32_t c = 0; c < h->ncells; ++c)
+        if (surrogate_cells[c] && !h->sur_attached[c])
+            return fail(h, MIND_EARG, "only cells named when the surrogate was attached can be surrogate cells");
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    std::vector<int32_t> old_cells(h->n_sur), old_spikes((size_t)6 * h->n_sur);
+    if (h->n_sur) {
+        CUDA_TRY(h, cudaMemcpy(old_cells.data(), h->sur_cells, old_cells.size() * sizeof(int32_t),
+                               cudaMemcpyDeviceToHost));
+        CUDA_TRY(h, cudaMemcpy(old_spikes.data(), h->sur_spikes, old_spikes.size() * sizeof(int32_t),
+                               cudaMemcpyDeviceToHost));
+    }
+    std::vector<int32_t> where(h->ncells, -1);
+    for (int32_t i = 0; i < h->n_sur; ++i) where[old_cells[i]] = i;
+    std::vector<uint8_t> mode(h->ncells, 0);
+    std::vector<int32_t> cells, sources;
+    for (int32_t c = 0; c < h->ncells; ++c)
+        if (surrogate_cells[c]) {
+            mode[c] = 1;
+            cells.push_back(c);
+            sources.push_back(h->cell_detector[c]);
+        }
+    const int32_t n = (int32_t)cells.size();
+    // the last bins' own spikes (features of the next bins) follow each cell to its new slot
+    std::vector<int32_t> spikes((size_t)6 * n, 0);
+    for (int32_t i = 0; i < n; ++i)
+        if (where[cells[i]] >= 0)
+            for (int32_t k = 0; k < 6; ++k) spikes[(size_t)k * n + i] = old_spikes[(size_t)k * h->n_sur + where[cells[i]]];
+    CUDA_TRY(h, cudaMemcpy(const_cast<uint8_t *>(h->P.cell_mode), mode.data(), mode.size(), cudaMemcpyHostToDevice));
+    if (n) {
+        CUDA_TRY(h, cudaMemcpy(h->sur_cells, cells.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice));
+        CUDA_TRY(h, cudaMemcpy(h->sur_sources, sources.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice));
+        CUDA_TRY(h, cudaMemcpy(h->sur_spikes, spikes.data(), spikes.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+    }
+    h->n_sur = n;
     return MIND_OK;
 }
 

@@ -79,6 +79,15 @@ class DeviceState:
             self.handle, mlp.handle, mask.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), float(drive_scale)))
         self._surrogate = mlp   # the network must outlive the handle's use of it
 
+    def set_surrogate_cells(self, surrogate_cells) -> None:
+        """mind_set_surrogate_cells: between runs, the cells (a subset of the attached ones)
+        the surrogate stands in for; the others are simulated from their next step."""
+        mask = np.ascontiguousarray(np.asarray(surrogate_cells, dtype=bool).astype(np.uint8))
+        if mask.size != self.layout.n_cells:
+            raise ValueError("one flag per cell")
+        abi.check(self.lib, self.handle, self.lib.mind_set_surrogate_cells(
+            self.handle, mask.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))))
+
     def set_drive_recording(self, bin_ms: float) -> None:
         """mind_set_drive_recording: each run also returns the cells' binned synaptic drive."""
         abi.check(self.lib, self.handle, self.lib.mind_set_drive_recording(self.handle, float(bin_ms)))

@@ -180,6 +180,80 @@ def region_rates(layout, result, macro, t_ms: float, bin_ms: float = 10.0) -> np
     return rates / np.maximum(cells, 1.0) / (bin_ms * 1e-3)
 
 
+def cell_regions(layout, macro) -> np.ndarray:
+    """Region (0-based) whose rate bin each cell's detector feeds, -1 for none."""
+    offsets = np.asarray(layout.cell_offsets)
+    nodes = np.asarray(layout.source_nodes)
+    out = np.full(layout.n_cells, -1, dtype=np.int64)
+    for region, source in macro.outputs:
+        node = int(nodes[source - 1])
+        if node > 0:
+            out[int(np.searchsorted(offsets, node - 1, side="right") - 1)] = region - 1
+    return out
+
+
+def judge_populations(sur_spikes, sur_cells, det_spikes, det_cells, seconds: float, bound: float,
+                      z: float = 3.0) -> np.ndarray:
+    """Populations to revert to the cable solver: where the surrogate cells' mean rate differs
+    from the detailed sample's by more than `bound` of the sample's rate plus z standard
+    errors of the two Poisson estimates (so a population with few sample spikes is not
+    reverted on counting noise alone).  Arguments are per population; returns a bool mask."""
+    sur_spikes = np.asarray(sur_spikes, dtype=float)
+    det_spikes = np.asarray(det_spikes, dtype=float)
+    ns = np.maximum(np.asarray(sur_cells, dtype=float), 1.0) * seconds
+    nd = np.maximum(np.asarray(det_cells, dtype=float), 1.0) * seconds
+    r_s, r_d = sur_spikes / ns, det_spikes / nd
+    se = np.sqrt(np.maximum(sur_spikes, 1.0) / ns ** 2 + np.maximum(det_spikes, 1.0) / nd ** 2)
+    judged = (np.asarray(sur_cells) > 0) & (np.asarray(det_cells) > 0)
+    return judged & (np.abs(r_s - r_d) > bound * r_d + z * se)
+
+
+def judged_run(state, layout, macro, surrogate_cells, t_ms: float, window_ms: float = 20.0,
+               bound: float = 0.05, z: float = 3.0):
+    """Run t_ms in windows with the cable solver as judge: the cells of each population that
+    stay detailed (the sample) are compared, after every window and over the run so far,
+    with the population's surrogate cells (judge_populations); a population that fails is
+    reverted (mind_set_surrogate_cells) and simulated from the next window on.  `state` is an
+    initialized DeviceState with the surrogate attached for `surrogate_cells`.
+    Returns (per-window results, [(time ms, reverted population indices)], final mask)."""
+    mask = np.asarray(surrogate_cells, dtype=bool).copy()
+    region = cell_regions(layout, macro)
+    n_pop = macro.n_regions
+    offsets = np.asarray(layout.cell_offsets)
+    nodes = np.asarray(layout.source_nodes)
+    sid_cell = {int(layout.source_ids[s]): int(np.searchsorted(offsets, node - 1, side="right") - 1)
+                for s, node in enumerate(nodes) if node > 0}
+    steps = int(round(window_ms / layout.dt))
+    total = int(round(t_ms / layout.dt))
+    sur_count = np.zeros(n_pop)
+    det_count = np.zeros(n_pop)
+    sur_time = np.zeros(n_pop)   # cell-seconds observed in each role
+    det_time = np.zeros(n_pop)
+    results, log, done = [], [], 0
+    while done < total:
+        k = min(steps, total - done)
+        res = state.run_steps(k, [])
+        results.append(res)
+        seconds = k * layout.dt * 1e-3
+        for sid in res.spike_sources:
+            c = sid_cell.get(int(sid))
+            if c is not None and region[c] >= 0:
+                (sur_count if mask[c] else det_count)[region[c]] += 1.0
+        for p in range(n_pop):
+            members = region == p
+            sur_time[p] += seconds * np.count_nonzero(mask & members)
+            det_time[p] += seconds * np.count_nonzero(~mask & members)
+        done += k
+        live = np.array([np.any(mask & (region == p)) for p in range(n_pop)])
+        revert = live & judge_populations(sur_count, sur_time, det_count, det_time, 1.0, bound, z)
+        if np.any(revert):
+            for p in np.nonzero(revert)[0]:
+                mask[region == p] = False
+            state.set_surrogate_cells(mask)
+            log.append((done * layout.dt, [int(p) for p in np.nonzero(revert)[0]]))
+    return results, log, mask
+
+
 def flops_per_row(n_in: int = N_FEATURES, hidden: int = 256, layers: int = 3) -> int:
     """Forward FLOPs of one row (2 per multiply-add of the linear maps); training is 3x."""
     dims = [n_in] + [hidden] * layers + [1]

@@ -21,3 +21,19 @@ def test_oracle_gradients_match_finite_differences():
         down, _ = oracle_mlp.loss_and_gradients(p, dims, x, y)
         assert abs((up - down) / (2 * eps) - grad[k]) < 1e-7 * max(1.0, abs(grad[k]))
     assert loss > 0
+
+
+def test_judge_reverts_on_rate_error_not_on_counting_noise():
+    from mind_b200.surrogate import judge_populations
+
+    # 100 surrogate and 2 sample cells per population, 1 s observed
+    sur_cells, det_cells = np.array([100.0] * 4), np.array([2.0] * 4)
+    det = np.array([20.0, 20.0, 2.0, 20.0])            # 10 Hz samples (1 Hz in population 2)
+    sur = np.array([1000.0, 3000.0, 200.0, 1040.0])    # 10, 30, 2, 10.4 Hz
+    revert = judge_populations(sur, sur_cells, det, det_cells, 1.0, bound=0.05, z=3.0)
+    # population 1 fires 3x its sample: reverted; population 3 is 4% off: kept; population 2
+    # is 2x off but its sample saw 2 spikes: within the counting noise
+    assert revert.tolist() == [False, True, False, False]
+    # populations without surrogate cells or without a sample are not judged
+    assert not judge_populations([5.0], [0.0], [50.0], [2.0], 1.0, 0.05).any()
+    assert not judge_populations([500.0], [100.0], [0.0], [0.0], 1.0, 0.05).any()

@@ -85,3 +85,33 @@ def test_surrogate_cells_drive_the_regions():
     n_sur = np.sum(a.spike_sources <= layout.n_cells)
     assert n_detailed / 4 < n_sur < 4 * n_detailed, (n_sur, n_detailed)
     net.close()
+
+
+def test_judge_reverts_a_failing_surrogate_to_the_cable_solver():
+    """A network that predicts a spike in every bin: after the first judge window every
+    population is reverted, and from then on its cells fire like detailed cells."""
+    model, macro = netcases.coupled_regions(n_regions=4, cells_per_region=50, synapses=32, seed=21)
+    layout = model.layout
+    net = surrogate.Mlp()
+    params = net.params
+    params[-1] = 20.0                       # output bias: p = 1 in every bin
+    net.params = params
+    mask = np.ones(layout.n_cells, dtype=bool)
+    mask[::10] = False
+    state = mb.runtime.DeviceState(layout)
+    state.attach_macro(macro)
+    state.attach_surrogate(net, mask, 1.0)
+    with pytest.raises(mb.abi.MindError):
+        state.set_surrogate_cells(np.ones(layout.n_cells, dtype=bool))   # cells that were never attached
+    state.initialize()
+    results, log, final = surrogate.judged_run(state, layout, macro, mask, 200.0, window_ms=20.0)
+    assert log and log[0][0] == 20.0 and sorted(log[0][1]) == [0, 1, 2, 3]
+    assert not final.any()
+    region = surrogate.cell_regions(layout, macro)
+    first = np.sum(results[0].spike_sources < layout.n_cells)
+    later = sum(np.sum(r.spike_sources < layout.n_cells) for r in results[2:]) / (len(results) - 2)
+    assert first > 0.5 * 20 * np.count_nonzero(mask)   # the failing surrogate fired (almost) every bin
+    assert later < 0.5 * first                          # reverted cells fire at their own rate
+    assert np.all(region >= 0)
+    state.close()
+    net.close()
