@@ -122,7 +122,7 @@ struct MindHandle {
     std::vector<std::vector<int32_t>> field_slot;
     std::vector<std::vector<int32_t>> group_row_off;
     // results
-    std::vector<double> trace;
+    const double *trace_result = nullptr;   // the last run's traces (device), [samples x records]
     int64_t trace_samples = 0;
     int32_t trace_records = 0;
     std::vector<double> spike_times;
@@ -1171,11 +1171,10 @@ int collect(MindHandle *h, bool record_spikes) {
             h->spike_sids[i] = h->source_ids[src[idx[i]]];
         }
     }
+    // the traces stay in device memory until mind_get_trace copies them out (one copy)
     h->trace_records = P.nrec;
-    h->trace_samples = P.trace_samples;
-    h->trace.assign((size_t)h->trace_samples * P.nrec, 0.0);
-    if (P.nrec && !h->trace.empty())
-        CUDA_TRY(h, cudaMemcpy(h->trace.data(), P.trace, h->trace.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    h->trace_samples = P.nrec ? P.trace_samples : 0;
+    h->trace_result = P.trace;
     return MIND_OK;
 }
 
@@ -1506,8 +1505,9 @@ int mind_time(const MindHandle *h, int64_t *step, double *time) {
 
 int mind_get_trace(const MindHandle *h, double *out, int64_t n) {
     if (!h) return MIND_EARG;
-    if (n != (int64_t)h->trace.size()) return MIND_EARG;
-    if (n) std::memcpy(out, h->trace.data(), n * sizeof(double));
+    if (n != h->trace_samples * (int64_t)h->trace_records || (n && !out)) return MIND_EARG;
+    if (n && cudaMemcpy(out, h->trace_result, n * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return MIND_ECUDA;
     return MIND_OK;
 }
 

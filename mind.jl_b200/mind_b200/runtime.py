@@ -146,8 +146,10 @@ class DeviceState:
                 abi.check(self.lib, self.handle, self.lib.mind_get_macro_trace(
                     self.handle, mt.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), mt.size, ctypes.byref(samples)))
             result.macro_trace = mt
-        for i, r in enumerate(records):
-            result.traces[r.name] = trace[:, i].copy()
+        if records:
+            by_record = np.ascontiguousarray(trace.T)   # one copy; each trace is a row view
+            for i, r in enumerate(records):
+                result.traces[r.name] = by_record[i]
         return result
 
     def run_stats(self) -> abi.MindRunStats:
