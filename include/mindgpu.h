@@ -71,7 +71,8 @@ enum {
     MIND_MECH_EXPSYN = 3,   /* mod/ExpSyn.mod   point    */
     MIND_MECH_EXP2SYN = 4,  /* mod/Exp2Syn.mod  point    */
     MIND_MECH_NETSTIM = 5,  /* mod/NetStim.mod  artificial */
-    MIND_MECH_ICLAMP = 6    /* mod/IClamp.mod   point (electrode current) */
+    MIND_MECH_ICLAMP = 6,   /* mod/IClamp.mod   point (electrode current) */
+    MIND_MECH_ALPHASYN = 7  /* mod/AlphaSynapse.mod point: g = gmax alpha((t-onset)/tau), i = g (v-e) */
 };
 
 /*
@@ -146,6 +147,7 @@ typedef struct MindLayout {
  *   ExpSyn   tau e g
  *   Exp2Syn  tau1 tau2 e A B factor
  *   IClamp   del dur amp
+ *   AlphaSynapse  onset tau gmax e
  *   NetStim  interval number start noise event on ispike   (mind_read_value only)
  * ASSIGNED fields that the reference writes during BREAKPOINT (hh ina/gna/minf/..., pas
  * i, ExpSyn i, Exp2Syn g/i, IClamp i) are not kept: referencing one returns MIND_EARG.

@@ -74,6 +74,7 @@ enum { PAS_G, PAS_E, PAS_SCALE, PAS_NSLOT };
 enum { ES_E, ES_G, ES_TAU, ES_DECAY, ES_NSLOT };
 enum { E2_E, E2_A, E2_B, E2_FACTOR, E2_TAU1, E2_TAU2, E2_DECAY1, E2_DECAY2, E2_NSLOT };
 enum { IC_DEL, IC_DUR, IC_AMP, IC_NSLOT };
+enum { AS_ONSET, AS_TAU, AS_GMAX, AS_E, AS_NSLOT };
 enum { NS_INTERVAL, NS_NUMBER, NS_START, NS_NOISE, NS_EVENT, NS_ON, NS_ISPIKE, NS_NEXT_T,
        NS_NEXT_FLAG, NS_NSLOT };
 /* FP32 parameter slots (mixed mode). */
@@ -88,6 +89,7 @@ __host__ __device__ inline int kind_slots(int32_t kind) {
         case MIND_MECH_EXPSYN: return ES_NSLOT;
         case MIND_MECH_EXP2SYN: return E2_NSLOT;
         case MIND_MECH_ICLAMP: return IC_NSLOT;
+        case MIND_MECH_ALPHASYN: return AS_NSLOT;
         case MIND_MECH_NETSTIM: return NS_NSLOT;
         default: return 0;
     }

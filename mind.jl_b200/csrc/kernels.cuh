@@ -902,6 +902,27 @@ __global__ void __launch_bounds__(NT, NT == kCellThreads ? 5 : 10) window_kernel
                         sr[node] = sr[node] + -1.0 * value;
                         sd[node] = sd[node] + milli_quotient<MIXED>(1.0 * (shifted - value));
                     }
+                } else if (G.kind == MIND_MECH_ALPHASYN) {
+                    // g = gmax alpha((t - onset)/tau), i = g (v - e) at the step's mid time
+                    const int32_t *pn = GG.node + G.r0;
+                    for (int32_t r = lo; r < hi; ++r) {
+                        const int32_t node = (int32_t)(__ldg(pn + r) - nb);
+                        const int64_t q = (int64_t)G.r0 + r;
+                        const double gs = __ldg(GG.f[AS_GMAX] + q) *
+                                          mind_alpha((tc - __ldg(GG.f[AS_ONSET] + q)) / __ldg(GG.f[AS_TAU] + q));
+                        const double e = __ldg(GG.f[AS_E] + q);
+                        const double vv = sv[node];
+                        if (MIXED) {  // linear in v: the probe's difference quotient is g
+                            sr[node] = sr[node] - gs * (vv - e);
+                            sd[node] = sd[node] + gs;
+                            continue;
+                        }
+                        const double probe = vv + 0.001;
+                        const double shifted = 0.0 + gs * (probe - e);
+                        const double value = 0.0 + gs * (vv - e);
+                        sr[node] = sr[node] + -1.0 * value;
+                        sd[node] = sd[node] + milli_quotient<MIXED>(1.0 * (shifted - value));
+                    }
                 } else if (G.kind == MIND_MECH_HH) {
                     for (int32_t r = lo; r < hi; ++r) {
                         const int32_t node = G.node[r];

@@ -185,6 +185,10 @@ MIND_HD double mind_pow(double x, double y) {
  * Arithmetic, chapter on FMA-based division).  The theorem assumes no underflow
  * or overflow, so magnitudes outside [2^-900, 2^900], and non-finite values,
  * take the division; zeros come back unchanged, as 0/0.001 keeps the sign. */
+/* AlphaSynapse's alpha(x) (mod/AlphaSynapse.mod FUNCTION alpha): x exp(1 - x) on
+ * [0, 10], else 0. */
+MIND_HD double mind_alpha(double x) { return (x < 0.0 || x > 10.0) ? 0.0 : x * mind_exp(1.0 - x); }
+
 MIND_HD double mind_div_milli(double x) {
     const double ax = fabs(x);
     if (ax >= 0x1p-900 && ax <= 0x1p+900) {

@@ -236,6 +236,8 @@ KindSpec spec_of(int32_t kind) {
             return {kind, {"e", "A", "B", "factor", "tau1", "tau2"}, E2_NSLOT, 2};
         case MIND_MECH_ICLAMP:
             return {kind, {"del", "dur", "amp"}, IC_NSLOT, 0};
+        case MIND_MECH_ALPHASYN:
+            return {kind, {"onset", "tau", "gmax", "e"}, AS_NSLOT, 0};
         case MIND_MECH_NETSTIM:
             return {kind, {"interval", "number", "start", "noise", "event", "on", "ispike"}, NS_NSLOT, 0};
         default:
@@ -250,6 +252,7 @@ int slot_of(int32_t kind, int k) {
     static const int es[] = {ES_E, ES_G, ES_TAU};
     static const int e2[] = {E2_E, E2_A, E2_B, E2_FACTOR, E2_TAU1, E2_TAU2};
     static const int ic[] = {IC_DEL, IC_DUR, IC_AMP};
+    static const int as[] = {AS_ONSET, AS_TAU, AS_GMAX, AS_E};
     static const int ns[] = {NS_INTERVAL, NS_NUMBER, NS_START, NS_NOISE, NS_EVENT, NS_ON, NS_ISPIKE};
     switch (kind) {
         case MIND_MECH_HH: return hh[k];
@@ -257,6 +260,7 @@ int slot_of(int32_t kind, int k) {
         case MIND_MECH_EXPSYN: return es[k];
         case MIND_MECH_EXP2SYN: return e2[k];
         case MIND_MECH_ICLAMP: return ic[k];
+        case MIND_MECH_ALPHASYN: return as[k];
         case MIND_MECH_NETSTIM: return ns[k];
         default: return 0;
     }
@@ -280,6 +284,8 @@ int readable_slot(int32_t kind, const char *name) {
         {MIND_MECH_EXP2SYN, "e", E2_E},      {MIND_MECH_EXP2SYN, "A", E2_A},    {MIND_MECH_EXP2SYN, "B", E2_B},
         {MIND_MECH_EXP2SYN, "factor", E2_FACTOR},
         {MIND_MECH_ICLAMP, "del", IC_DEL},   {MIND_MECH_ICLAMP, "dur", IC_DUR}, {MIND_MECH_ICLAMP, "amp", IC_AMP},
+        {MIND_MECH_ALPHASYN, "onset", AS_ONSET}, {MIND_MECH_ALPHASYN, "tau", AS_TAU},
+        {MIND_MECH_ALPHASYN, "gmax", AS_GMAX},   {MIND_MECH_ALPHASYN, "e", AS_E},
         {MIND_MECH_NETSTIM, "interval", NS_INTERVAL}, {MIND_MECH_NETSTIM, "number", NS_NUMBER},
         {MIND_MECH_NETSTIM, "start", NS_START},       {MIND_MECH_NETSTIM, "noise", NS_NOISE},
         {MIND_MECH_NETSTIM, "event", NS_EVENT},       {MIND_MECH_NETSTIM, "on", NS_ON},

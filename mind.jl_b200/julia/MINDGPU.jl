@@ -21,7 +21,7 @@ const MIND_ABI_VERSION = Int32(1)
 const MIND_RECORD_VOLTAGE = Int32(1)
 const MIND_RECORD_MECHANISM = Int32(2)
 const KIND_CODES = Dict(:hh => Int32(1), :pas => Int32(2), :ExpSyn => Int32(3), :Exp2Syn => Int32(4),
-                        :NetStim => Int32(5), :IClamp => Int32(6))
+                        :NetStim => Int32(5), :IClamp => Int32(6), :AlphaSynapse => Int32(7))
 
 struct MindMechanism
     kind::Int32

@@ -25,6 +25,7 @@ MIND_MECH_EXPSYN = 3
 MIND_MECH_EXP2SYN = 4
 MIND_MECH_NETSTIM = 5
 MIND_MECH_ICLAMP = 6
+MIND_MECH_ALPHASYN = 7
 
 
 @dataclass(frozen=True)
@@ -99,6 +100,11 @@ _BUILTINS: Dict[str, Mechanism] = {
          ("event", 0.0), ("on", 0.0), ("ispike", 0.0)],
         0xA186833B569FF3B2,
         arity=1,
+    ),
+    "AlphaSynapse": _mechanism(
+        "AlphaSynapse", "point", MIND_MECH_ALPHASYN,
+        [("onset", 0.0), ("tau", 0.1), ("gmax", 0.0), ("e", 0.0), ("i", 0.0), ("g", 0.0)],
+        0x29B06B38B5009424,
     ),
     "IClamp": _mechanism(
         "IClamp", "point", MIND_MECH_ICLAMP,

@@ -84,6 +84,7 @@ enum { ES_TAU, ES_E, ES_G, ES_NF };
 enum { E2_TAU1, E2_TAU2, E2_E, E2_A, E2_B, E2_FACTOR, E2_NF };
 enum { NS_INTERVAL, NS_NUMBER, NS_START, NS_NOISE, NS_EVENT, NS_ON, NS_ISPIKE, NS_NF };
 enum { IC_DEL, IC_DUR, IC_AMP, IC_NF };
+enum { AS_ONSET, AS_TAU, AS_GMAX, AS_E, AS_NF };
 
 const char *const HH_NAMES[] = {"gnabar", "gkbar", "gl", "el", "m", "h", "n", "ena", "ek"};
 const char *const PAS_NAMES[] = {"g", "e"};
@@ -91,6 +92,7 @@ const char *const ES_NAMES[] = {"tau", "e", "g"};
 const char *const E2_NAMES[] = {"tau1", "tau2", "e", "A", "B", "factor"};
 const char *const NS_NAMES[] = {"interval", "number", "start", "noise", "event", "on", "ispike"};
 const char *const IC_NAMES[] = {"del", "dur", "amp"};
+const char *const AS_NAMES[] = {"onset", "tau", "gmax", "e"};
 
 struct Oracle {
     const MindLayout *L;
@@ -285,6 +287,7 @@ struct Oracle {
                 case MIND_MECH_EXP2SYN: names = E2_NAMES; nf = E2_NF; break;
                 case MIND_MECH_NETSTIM: names = NS_NAMES; nf = NS_NF; break;
                 case MIND_MECH_ICLAMP: names = IC_NAMES; nf = IC_NF; break;
+                case MIND_MECH_ALPHASYN: names = AS_NAMES; nf = AS_NF; break;
                 default: return fail(MIND_ELAYOUT, "unsupported mechanism kind");
             }
             G.f.resize(nf);
@@ -536,6 +539,11 @@ struct Oracle {
                         shifted = 0.0 - i;
                         value = 0.0 - i;
                     } break;
+                    case MIND_MECH_ALPHASYN: {  // mod/AlphaSynapse.mod BREAKPOINT
+                        double g = G.f[AS_GMAX][r] * mind_alpha((tc - G.f[AS_ONSET][r]) / G.f[AS_TAU][r]);
+                        shifted = 0.0 + g * (probe - G.f[AS_E][r]);
+                        value = 0.0 + g * (vv - G.f[AS_E][r]);
+                    } break;
                     default: continue;
                 }
                 if (density) {
@@ -713,6 +721,7 @@ int oracle_run_macro(const MindLayout *layout, const MindMacroLayout *macro, int
                                    : m.kind == MIND_MECH_PAS    ? PAS_NAMES
                                    : m.kind == MIND_MECH_EXPSYN ? ES_NAMES
                                    : m.kind == MIND_MECH_EXP2SYN ? E2_NAMES
+                                   : m.kind == MIND_MECH_ALPHASYN ? AS_NAMES
                                                                  : IC_NAMES;
         for (size_t slot = 0; slot < G.f.size(); ++slot)
             if (std::strcmp(names[slot], m.field_names[r.field - 1]) == 0) rec_vec[k] = &G.f[slot];

@@ -139,3 +139,31 @@ def test_config1_poisson_counts():
     assert ref.status == 0
     stims = ref.spike_sids >= 64
     assert abs(int(stims.sum()) - 640) < 4 * math.sqrt(640)   # 640 NetStims at 10 Hz for 0.1 s
+
+
+def test_alpha_synapse_matches_linearized_backward_euler():
+    """AlphaSynapse (mod/AlphaSynapse.mod) on an isopotential soma with pas: the oracle's
+    voltage equals the one-compartment update v += -I(v) / (C/dt + G) with the synaptic
+    conductance gmax alpha((t + dt/2 - onset)/tau) of each step."""
+    dt, steps = 0.025, 600
+    gp, ep = 2.0e-4, -65.0
+    onset, tau, gmax, es = 2.0, 1.5, 0.004, 0.0
+    model, cell = single_section(params={"g": gp, "e": ep})
+    M.add_pointprocess(cell, mb.builtin("AlphaSynapse"), section="soma", x=0.5,
+                       params={"onset": onset, "tau": tau, "gmax": gmax, "e": es})
+    layout = mb.build(model, dt_micro=dt)
+    node = layout.voltage_node(1)
+    ref = oracle.run(layout, steps, [node])
+    assert ref.status == 0, ref.message
+    area = layout.area[node - 1]
+    cap = layout.capacitance[node - 1]
+    g_pas = gp * area * 0.01
+    v = np.empty(steps + 1)
+    v[0] = -65.0
+    for n in range(steps):
+        x = (n * dt + 0.5 * dt - onset) / tau
+        gs = gmax * (x * math.exp(1.0 - x) if 0.0 <= x <= 10.0 else 0.0)
+        current = g_pas * (v[n] - ep) + gs * (v[n] - es)
+        v[n + 1] = v[n] - current / (cap / dt + g_pas + gs)
+    assert np.max(np.abs(ref.trace[:, 0] - v)) < 1e-9
+    assert np.max(v) > -60.0        # the synapse depolarised the soma
