@@ -37,3 +37,66 @@ def test_judge_reverts_on_rate_error_not_on_counting_noise():
     # populations without surrogate cells or without a sample are not judged
     assert not judge_populations([5.0], [0.0], [50.0], [2.0], 1.0, 0.05).any()
     assert not judge_populations([500.0], [100.0], [0.0], [0.0], 1.0, 0.05).any()
+
+
+class _FakeState:
+    """A DeviceState stand-in: each run_steps returns a raster in which every surrogate
+    cell fires `sur_hz` and every detailed cell `det_hz` (regular spikes), and
+    set_surrogate_cells records the masks it is given."""
+
+    def __init__(self, layout, mask, sur_hz, det_hz):
+        self.layout, self.mask, self.sur_hz, self.det_hz = layout, mask.copy(), sur_hz, det_hz
+        self.t, self.calls = 0.0, []
+
+    def run_steps(self, steps, records):
+        from mind_b200.runtime import SimulationResult
+
+        dt = self.layout.dt
+        t0, t1 = self.t, self.t + steps * dt
+        times, sids = [], []
+        for c in range(self.layout.n_cells):
+            hz = self.sur_hz if self.mask[c] else self.det_hz
+            k = np.arange(np.ceil(t0 * hz / 1000.0), np.ceil(t1 * hz / 1000.0))
+            times += list(k * 1000.0 / hz)
+            sids += [c] * len(k)
+        self.t = t1
+        order = np.argsort(times, kind="stable")
+        return SimulationResult(np.zeros(1), {}, np.asarray(times)[order], np.asarray(sids, np.int64)[order], 1.0)
+
+    def set_surrogate_cells(self, mask):
+        self.mask = np.asarray(mask, dtype=bool).copy()
+        self.calls.append(self.mask.copy())
+
+
+def test_judged_run_reverts_only_the_failing_population():
+    import netcases
+    from mind_b200 import surrogate
+
+    model, macro = netcases.coupled_regions(n_regions=2, cells_per_region=50, synapses=2, seed=3)
+    layout = model.layout
+    region = surrogate.cell_regions(layout, macro)
+    assert sorted(set(region.tolist())) == [0, 1]
+    mask = np.ones(layout.n_cells, dtype=bool)
+    mask[::10] = False                                   # 10% detailed sample
+    # population 0's surrogate fires 4x its sample; population 1's matches its sample
+    state = _FakeState(layout, mask, sur_hz=40.0, det_hz=10.0)
+    good = region == 1
+    state.sur_hz = 40.0
+
+    def run_steps(steps, records, _orig=state.run_steps):
+        res = _orig(steps, records)
+        keep = np.ones(len(res.spike_sources), dtype=bool)
+        for i, sid in enumerate(res.spike_sources):
+            c = int(sid)
+            if good[c] and state.mask[c] and (i % 4 != 0):
+                keep[i] = False                          # population 1 surrogate: 10 Hz
+        res.spike_times, res.spike_sources = res.spike_times[keep], res.spike_sources[keep]
+        return res
+
+    state.run_steps = run_steps
+    results, log, final = surrogate.judged_run(state, layout, macro, mask, 200.0, window_ms=20.0)
+    assert len(results) == 10
+    assert log and all(regs == [0] for _, regs in log) and len(log) == 1
+    assert not final[region == 0].any()                  # population 0 reverted
+    assert np.array_equal(final[region == 1], mask[region == 1])   # population 1 kept
+    assert len(state.calls) == 1 and np.array_equal(state.calls[0], final)
