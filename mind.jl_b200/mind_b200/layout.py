@@ -353,11 +353,12 @@ def _point_nodes(model, morphs, offsets, chunk) -> np.ndarray:
         m = morphs[model.cells[cell - 1].morphology]
         base = offsets[cell - 1]
         if single:
-            names = [sections] * (hi - lo)
+            names = [sections]
         else:
-            names = [str(s) for s in sections[lo:hi]]
-        for name in set(names):
-            sel = np.array([n == name for n in names]) if not single else slice(None)
+            labels = np.asarray(sections[lo:hi]).astype(str)
+            names = np.unique(labels)
+        for name in names:
+            sel = (labels == name) if not single else slice(None)
             nodes = m.section_nodes[name]
             nseg = len(nodes) - 1
             x = xs[lo:hi][sel]
