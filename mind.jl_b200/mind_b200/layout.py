@@ -353,21 +353,26 @@ def _point_nodes(model, morphs, offsets, chunk) -> np.ndarray:
         m = morphs[model.cells[cell - 1].morphology]
         base = offsets[cell - 1]
         if single:
-            names = [sections]
-        else:
-            labels = np.asarray(sections[lo:hi]).astype(str)
-            names = np.unique(labels)
-        for name in names:
-            sel = (labels == name) if not single else slice(None)
-            nodes = m.section_nodes[name]
+            nodes = m.section_nodes[sections]
             nseg = len(nodes) - 1
-            x = xs[lo:hi][sel]
+            x = xs[lo:hi]
             idx = np.minimum(np.floor(x * nseg).astype(np.int64), nseg - 1)
             local = nodes[idx].astype(np.int64)
-            local = np.where(x == 0.0, m.section_starts[name], local)
+            local = np.where(x == 0.0, m.section_starts[sections], local)
             local = np.where(x == 1.0, nodes[-1], local)
-            if single:
-                out[lo:hi] = base + local
+            out[lo:hi] = base + local
+            continue
+        # points on many sections of one cell: the same rule, point by point
+        for k in range(lo, hi):
+            name = str(sections[k])
+            nodes = m.section_nodes[name]
+            x = float(xs[k])
+            if x == 0.0:
+                local = m.section_starts[name]
+            elif x == 1.0:
+                local = nodes[-1]
             else:
-                out[lo:hi][sel] = base + local
+                nseg = len(nodes) - 1
+                local = nodes[min(int(math.floor(x * nseg)), nseg - 1)]
+            out[k] = base + int(local)
     return out
