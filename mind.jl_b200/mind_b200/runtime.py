@@ -277,13 +277,48 @@ def voltage_record(model, cell, *, section: str = "soma", x: float = 0.5, name=N
     return RecordSpec(node, name if name is not None else f"v_{cell.gid}")
 
 
-def mechanism_ref(model, group, row: int, field, *, name=None) -> RecordSpec:
-    """mechanism_ref(plan, :mechanism, group, row, field) (src/model/references.jl:43-73):
-    `group` is a 1-based group index or a mechanism name (its first group), `row` 1-based,
-    `field` a MOD field name or a 1-based column."""
+def _field_ref(layout, gi: int, row: int, field, name) -> RecordSpec:
+    mech = layout.groups[gi].mechanism
+    col = mech.field_index(field) if isinstance(field, str) else int(field) - 1
+    if not 0 <= col < len(mech.fields):
+        raise ValueError("invalid mechanism field")
+    if not 1 <= int(row) <= layout.groups[gi].rows:
+        raise ValueError("invalid mechanism row")
+    label = name if name is not None else f"mechanism.{gi + 1}.{int(row)}.{mech.fields[col]}"
+    return RecordSpec(0, label, abi.MIND_RECORD_MECHANISM, gi + 1, int(row), col + 1)
+
+
+def mechanism_ref(model, target, *args, section: str = "soma", x: float = 0.5, name=None) -> RecordSpec:
+    """mechanism_ref (src/model/references.jl:43-146), in its three forms:
+
+    * ``mechanism_ref(model, group, row, field)``: `group` a 1-based group index or a
+      mechanism name (its first group), `row` 1-based, `field` a MOD field name or a
+      1-based column;
+    * ``mechanism_ref(model, point, field)``: a field of a point process;
+    * ``mechanism_ref(model, cell, mechanism, field, section=, x=)``: a density
+      mechanism's field at (section, x) of a cell.
+    """
+    from .model import Cell, PointProcess
+
     layout = model.layout
     if layout is None:
         raise ValueError("model is not built")
+    if isinstance(target, PointProcess):
+        (field,) = args
+        gi = int(layout.point_group[target.index - 1]) - 1
+        return _field_ref(layout, gi, int(layout.point_row[target.index - 1]), field, name)
+    if isinstance(target, Cell):
+        mechanism, field = args
+        node = layout.voltage_node(target.index, section, x)
+        for gi, g in enumerate(layout.groups):
+            if g.mechanism.name != mechanism or g.mechanism.kind != "density":
+                continue
+            rows = np.flatnonzero(np.asarray(g.nodes) == node)
+            if len(rows):
+                return _field_ref(layout, gi, int(rows[0]) + 1, field, name)
+        raise ValueError(f"no {mechanism} at {section}({x}) of cell {target.index}")
+    group = target
+    row, field = args
     if isinstance(group, str):
         matches = [i for i, g in enumerate(layout.groups) if g.mechanism.name == group]
         if not matches:
@@ -293,14 +328,38 @@ def mechanism_ref(model, group, row: int, field, *, name=None) -> RecordSpec:
         gi = int(group) - 1
         if not 0 <= gi < len(layout.groups):
             raise ValueError("invalid mechanism group")
-    mech = layout.groups[gi].mechanism
-    col = mech.field_index(field) if isinstance(field, str) else int(field) - 1
-    if not 0 <= col < len(mech.fields):
-        raise ValueError("invalid mechanism field")
-    if not 1 <= int(row) <= layout.groups[gi].rows:
-        raise ValueError("invalid mechanism row")
-    label = name if name is not None else f"mechanism.{gi + 1}.{int(row)}.{mech.fields[col]}"
-    return RecordSpec(0, label, abi.MIND_RECORD_MECHANISM, gi + 1, int(row), col + 1)
+    return _field_ref(layout, gi, row, field, name)
+
+
+def mechanism_record(model, target, *args, section: str = "soma", x: float = 0.5, name=None) -> RecordSpec:
+    """mechanism_record: a RecordSpec of mechanism_ref's selection (named as given)."""
+    return mechanism_ref(model, target, *args, section=section, x=x, name=name)
+
+
+def voltage_ref(model, cell, *, section: str = "soma", x: float = 0.5) -> RecordSpec:
+    """voltage_ref(plan, cell; section, x) (src/model/references.jl:93-99)."""
+    node = model.layout.voltage_node(cell.index, section, x)
+    return RecordSpec(node, f"voltage.{node}")
+
+
+def connection_weights(model, connection: int) -> np.ndarray:
+    """connection_weights(state, connection) (src/runtime/state.jl:603-616): the NetCon's
+    NET_RECEIVE weights.  The builtin synapses never write their weight, so the device
+    value is the built one."""
+    layout = model.layout
+    if not 1 <= int(connection) <= len(layout.connection_edges):
+        raise ValueError("invalid connection")
+    edge = int(layout.connection_edges[int(connection) - 1])
+    return np.array([layout.edge_weights[edge - 1]])
+
+
+def inject_event(model, connection: int, t: float):
+    """inject_event!(state, connection, time) (src/runtime/state.jl:618-635): deliver one
+    NetCon event at an absolute time, without its delay."""
+    if model.state is None:
+        raise ValueError("simulation is not initialized")
+    model.state.inject_event(int(connection), float(t))
+    return model
 
 
 def autotune(model, windows: int = 4) -> List[int]:

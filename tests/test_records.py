@@ -6,6 +6,7 @@ recorded parameter stays at its layout value, a synaptic state decays by the cne
 between events, hh's gates start at their steady state, and an ASSIGNED field is refused.
 """
 import numpy as np
+import pytest
 
 import mind_b200 as mb
 import netcases
@@ -64,3 +65,36 @@ def test_mechanism_ref_validates_indices():
         except ValueError:
             continue
         raise AssertionError(f"accepted {args}")
+
+
+def test_reference_forms_of_mechanism_ref():
+    """The point-process and cell/density forms of mechanism_ref (references.jl:101-146)
+    select the same rows as the group/row form; voltage_ref, mechanism_record and
+    connection_weights follow the layout."""
+    from mind_b200 import model as M
+
+    model = netcases.strong_config1(n_cells=3, synapses=4)
+    layout = mb.build(model)
+    # a point process of the model: the first ExpSyn's PointProcess handle
+    point = M.PointProcess(model, 1)
+    ref_point = mb.mechanism_ref(model, point, "g")
+    gi = int(layout.point_group[0]) - 1
+    assert ref_point.group == gi + 1 and ref_point.row == int(layout.point_row[0])
+    assert layout.groups[gi].mechanism.fields[ref_point.field - 1] == "g"
+    # the cell form: hh at the soma of cell 2 is the hh row on that node
+    cell2 = M.Cell(model, 2, 2)
+    ref_cell = mb.mechanism_ref(model, cell2, "hh", "m")
+    hh = layout.groups[ref_cell.group - 1]
+    assert hh.mechanism.name == "hh"
+    assert int(hh.nodes[ref_cell.row - 1]) == layout.voltage_node(2)
+    with pytest.raises(ValueError):
+        mb.mechanism_ref(model, cell2, "hh", "m", section="dend")   # hh only at the soma
+    # the same selection records the same trace
+    a = oracle.run(layout, 200, records=[ref_cell, mb.mechanism_ref(model, ref_cell.group, ref_cell.row, "m")])
+    assert a.status == 0 and np.array_equal(a.trace[:, 0], a.trace[:, 1])
+    assert mb.voltage_ref(model, cell2).node == layout.voltage_node(2)
+    assert mb.mechanism_record(model, point, "g", name="g1").name == "g1"
+    edge = int(layout.connection_edges[0])
+    np.testing.assert_array_equal(mb.connection_weights(model, 1), [layout.edge_weights[edge - 1]])
+    with pytest.raises(ValueError):
+        mb.connection_weights(model, 10 ** 6)
