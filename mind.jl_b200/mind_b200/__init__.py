@@ -12,8 +12,8 @@ from .model import (Cell, IonSpecies, MicroModel, PointProcess, Population, Spik
                     insert, register_external_sources, register_point_sources, register_spike_source, spike_source)
 from .layout import Layout, build
 from .runtime import (RecordSpec, SimulationResult, autotune, connection_weights, initialize, inject_event,
-                      inject_spike, mechanism_record, mechanism_ref, read_value, run, simulation_time, step,
-                      voltage_record, voltage_ref)
+                      inject_spike, mechanism_record, mechanism_ref, read_value, run, runtime_configuration,
+                      simulation_time, step, voltage_record, voltage_ref)
 
 __all__ = [
     "Mechanism", "builtin", "Point3D", "Section", "discretize", "location_node", "Cell",
@@ -21,6 +21,7 @@ __all__ = [
     "add_pointprocesses", "add_population", "connect", "connect_many", "insert",
     "register_external_sources", "register_point_sources", "register_spike_source", "spike_source", "Layout", "build",
     "RecordSpec", "SimulationResult", "autotune", "connection_weights", "initialize", "inject_event",
-    "inject_spike", "mechanism_record", "mechanism_ref", "read_value", "run", "simulation_time", "step",
+    "inject_spike", "mechanism_record", "mechanism_ref", "read_value", "run", "runtime_configuration",
+    "simulation_time", "step",
     "voltage_record", "voltage_ref",
 ]

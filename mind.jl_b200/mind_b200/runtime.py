@@ -376,5 +376,15 @@ def read_value(model, ref: RecordSpec) -> float:
     return model.state.read_value(ref)
 
 
+def runtime_configuration(model) -> dict:
+    """runtime_configuration(state) (src/runtime/state.jl:573-581): the built step settings."""
+    layout = model.layout
+    if layout is None:
+        raise ValueError("model is not built")
+    macro = getattr(model, "macro", None)
+    return {"dt_micro": float(layout.dt), "dt_macro": float(macro.dt_macro) if macro is not None else None,
+            "celsius": float(layout.celsius), "secondorder": int(layout.secondorder)}
+
+
 def simulation_time(model) -> float:
     return model.state.time()[1]

@@ -98,3 +98,11 @@ def test_reference_forms_of_mechanism_ref():
     np.testing.assert_array_equal(mb.connection_weights(model, 1), [layout.edge_weights[edge - 1]])
     with pytest.raises(ValueError):
         mb.connection_weights(model, 10 ** 6)
+
+
+def test_runtime_configuration_reports_the_build():
+    model = _model()
+    cfg = mb.runtime_configuration(model)
+    assert cfg == {"dt_micro": 0.025, "dt_macro": None, "celsius": 6.3, "secondorder": 0}
+    coupled, macro = netcases.coupled_regions()
+    assert mb.runtime_configuration(coupled)["dt_macro"] == macro.dt_macro
