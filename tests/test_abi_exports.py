@@ -38,3 +38,39 @@ def test_malformed_layout_rejected_before_any_device_work():
     status = lib.mind_create(ctypes.byref(c_layout), ctypes.byref(handle))
     assert status == abi.MIND_ELAYOUT
     assert b"parent" in lib.mind_last_error(None)
+
+
+def test_null_handles_are_refused_without_device_work():
+    """Every entry point that takes a handle answers a null one with MIND_EARG (12)
+    before any CUDA call; destroying nothing succeeds; the create error text is kept."""
+    lib = abi.load_library()
+    d = ctypes.c_double()
+    i32 = ctypes.c_int32()
+    i64 = ctypes.c_int64()
+    rec = abi.MindRecord(abi.MIND_RECORD_VOLTAGE, 1, 0, 0, 0)
+    calls = {
+        "mind_set_precision": (None, 0), "mind_initialize": (None,), "mind_run": (None, 1, None, 0, 0),
+        "mind_step": (None,), "mind_time": (None, ctypes.byref(i64), ctypes.byref(d)),
+        "mind_get_trace": (None, None, 0), "mind_get_spikes": (None, None, None, 0, ctypes.byref(i64)),
+        "mind_read_voltage": (None, 1, ctypes.byref(d)), "mind_read_value": (None, ctypes.byref(rec), ctypes.byref(d)),
+        "mind_inject_event": (None, 1, 0.0), "mind_inject_spikes": (None, 0, None, None),
+        "mind_window_steps": (None, ctypes.byref(i32)), "mind_autotune": (None, 0),
+        "mind_bin_threads": (None, None, 0, ctypes.byref(i32)), "mind_set_bin_threads": (None, None, 0),
+        "mind_attach_macro": (None, None), "mind_get_macro_trace": (None, None, 0, None),
+        "mind_set_drive_recording": (None, 1.0), "mind_get_drive": (None, None, 0, None),
+        "mind_attach_surrogate": (None, None, None, 1.0), "mind_set_surrogate_cells": (None, None),
+        "mind_last_run_ms": (None, ctypes.byref(d)), "mind_run_stats": (None, None),
+        "mind_set_profiling": (None, 1), "mind_run_noalloc": (None, 1, None, 0, None),
+        "mind_mlp_param_count": (None, ctypes.byref(i64)), "mind_mlp_set_params": (None, None, 0),
+        "mind_mlp_get_params": (None, None, 0), "mind_mlp_predict": (None, None, 0, None),
+        "mind_mlp_gradients": (None, None, None, 1, None, None), "mind_mlp_set_data": (None, None, None, 1),
+        "mind_mlp_train": (None, 1, 1, ctypes.c_float(1e-3), None, None), "mind_mlp_create": (None, None),
+    }
+    declared = set(declared_functions())
+    for name, args in calls.items():
+        assert name in declared, name
+        assert getattr(lib, name)(*args) == abi.MIND_EARG, name
+    assert lib.mind_destroy(None) == abi.MIND_OK and lib.mind_mlp_destroy(None) == abi.MIND_OK
+    untested = declared - set(calls) - {"mind_create", "mind_destroy", "mind_mlp_destroy", "mind_last_error",
+                                        "mind_mlp_last_error"}
+    assert not untested, untested
