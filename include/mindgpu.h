@@ -381,9 +381,14 @@ int mind_set_profiling(MindHandle *h, int32_t enable);
  * Its per-run scratch (record maps and the trace staging area) lives in one
  * static device array of MIND_NOALLOC_SCRATCH_BYTES (16 MiB) that every GPU
  * loading the library holds until the process exits.  Runs that need more
- * return MIND_ECAPACITY with a message giving the size.  The first call on a
- * device looks up that array's device address (cudaGetSymbolAddress) with the
- * device current, so make the first call before any stream capture.  All
+ * (more than about 16 MiB / (8 n_records) steps per call) return MIND_ECAPACITY
+ * before any work, with a message giving the limit; the state is unchanged.
+ * The first call on a device looks up that array's device address
+ * (cudaGetSymbolAddress) with the device current, so make the first call before
+ * any stream capture.  The call must be made with the handle's device current
+ * (the one current at mind_create), otherwise it returns MIND_EARG.  A handle
+ * with surrogate cells attached is refused with MIND_ELAYOUT: the surrogate's
+ * products run through cuBLAS, which may allocate a workspace of its own.  All
  * handles on a device share the array and it keeps the previous call's
  * contents: calls that overlap on the GPU (two threads, two handles) race and
  * must be serialized by the caller.

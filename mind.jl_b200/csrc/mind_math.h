@@ -16,7 +16,7 @@
  *   log  x = 2^e m with m in [sqrt2/2, sqrt2); ln m = 2 atanh(s), s = (m-1)/(m+1),
  *        summed as f - s (f - R) with R the atanh series in s^2 to s^22.
  *   pow  exp(y log x) (used for Q10 factors; exact for y == 0).
- * Accuracy against glibc is checked by tests/test_math.py (a few ulp at most).
+ * Accuracy against glibc is checked by tests/test_math_rng.py (a few ulp at most).
  *
  * Philox4x32-10 follows Salmon, Moraes, Dror and Shaw, "Parallel random
  * numbers: as easy as 1, 2, 3" (SC'11), with its published multipliers and

@@ -98,6 +98,7 @@ struct MindHandle {
     std::vector<float> drive;
     int64_t drive_bins = 0;
     std::vector<double> v0_packed;
+    int32_t device = 0;                      // the device current at mind_create: state and stream live there
     int64_t n_sources = 0;
     std::vector<int64_t> source_ids;
     int32_t precision = MIND_FP64;
@@ -322,6 +323,7 @@ int create(const MindLayout *L, MindHandle *h) {
     if (L->n_mechanisms > kMaxGroups) return fail(h, MIND_ELAYOUT, "too many mechanism groups");
     const int64_t n = L->n_nodes;
     if (n < 0 || n >= INT32_MAX) return fail(h, MIND_ELAYOUT, "node count out of range");
+    CUDA_TRY(h, cudaGetDevice(&h->device));
     h->n_nodes = n;
     h->dt = L->dt;
 
@@ -1738,20 +1740,38 @@ int mind_run_noalloc(MindHandle *h, int64_t steps, const MindRecord *records, in
     if (!h->initialized) return fail(h, MIND_EARG, "simulation is not initialized");
     if (steps < 0 || n_records < 0 || (n_records > 0 && (!records || !trace)))
         return fail(h, MIND_EARG, "invalid run arguments");
+    // Surrogate inference runs cuBLAS GEMMs, and cuBLAS may allocate its workspace on first
+    // use: a handle with surrogate cells cannot promise a run without allocation.
+    if (h->sur_cap > 0)
+        return fail(h, MIND_ELAYOUT, "mind_run_noalloc does not run models with surrogate cells (cuBLAS may allocate)");
+    {
+        int device = -1;
+        CUDA_TRY(h, cudaGetDevice(&device));
+        if (device != h->device)
+            return fail(h, MIND_EARG, "mind_run_noalloc called with device " + std::to_string(device) +
+                                          " current; the handle lives on device " + std::to_string(h->device));
+    }
     // Scratch carve: rec_off [ncells+1] i32 | rec_node [n] i32 | rec_col [n] i32 | rec_ptr [n] ptr |
     // rec_initial [n] ptr | trace.
     auto align = [](size_t x) { return (x + 255) & ~(size_t)255; };
     const size_t off_bytes = align((size_t)(h->ncells + 1) * sizeof(int32_t));
     const size_t node_bytes = align((size_t)std::max(n_records, 1) * sizeof(int32_t));
     const size_t ptr_bytes = align((size_t)std::max(n_records, 1) * sizeof(const double *));
-    const size_t trace_bytes = (size_t)(steps + 1) * (size_t)n_records * sizeof(double);
-    const size_t need = off_bytes + 2 * node_bytes + 2 * ptr_bytes + trace_bytes;
-    if (need > MIND_NOALLOC_SCRATCH_BYTES) {
+    const size_t fixed = off_bytes + 2 * node_bytes + 2 * ptr_bytes;
+    // The trace holds (steps + 1) samples of n_records doubles.  The sample count is bounded
+    // by division before anything is multiplied, so no product can wrap.
+    const size_t room = fixed < MIND_NOALLOC_SCRATCH_BYTES ? MIND_NOALLOC_SCRATCH_BYTES - fixed : 0;
+    const size_t max_samples = n_records > 0 ? room / ((size_t)n_records * sizeof(double)) : (size_t)INT64_MAX;
+    if (fixed > MIND_NOALLOC_SCRATCH_BYTES || (uint64_t)steps >= (uint64_t)max_samples) {
         // Refused before any work: the simulation state is unchanged and stays usable.
-        h->error = "mind_run_noalloc needs " + std::to_string(need) + " bytes of scratch; its static array holds " +
-                   std::to_string((size_t)MIND_NOALLOC_SCRATCH_BYTES) + " bytes (fewer steps or records per call)";
+        h->error = "mind_run_noalloc: " + std::to_string(steps) + " steps of " + std::to_string(n_records) +
+                   " records need more scratch than its static array holds (" +
+                   std::to_string((size_t)MIND_NOALLOC_SCRATCH_BYTES) + " bytes, at most " +
+                   std::to_string(max_samples > 0 ? max_samples - 1 : 0) +
+                   " steps per call at this record count); use fewer steps or records per call";
         return MIND_ECAPACITY;
     }
+    const size_t trace_bytes = (size_t)(steps + 1) * (size_t)n_records * sizeof(double);
     // Record maps (host side), then into the scratch: every entry is written, nothing needs clearing.
     RecordTables t;
     int status = build_records(h, records, n_records, t);
@@ -1777,8 +1797,21 @@ int mind_run_noalloc(MindHandle *h, int64_t steps, const MindRecord *records, in
         CUDA_TRY(h, cudaMemcpyAsync(d_initial, t.initial.data(), t.initial.size() * sizeof(const double *),
                                     cudaMemcpyHostToDevice, h->stream));
     }
-    // Point the run at the scratch for this call; the handle's own record buffers stay untouched.
+    // Point the run at the scratch for this call only; the handle's own record fields are
+    // restored on every return, so no later call can record into the shared array.
     Params &P = h->P;
+    const Params own = P;
+    const double **own_initial = h->rec_initial_dev;
+    auto restore = [&]() {
+        P.rec_off = own.rec_off;
+        P.rec_node = own.rec_node;
+        P.rec_ptr = own.rec_ptr;
+        P.rec_col = own.rec_col;
+        P.nrec = own.nrec;
+        P.trace = own.trace;
+        P.trace_samples = own.trace_samples;
+        h->rec_initial_dev = own_initial;
+    };
     P.rec_off = d_off;
     P.rec_node = d_node;
     P.rec_ptr = d_ptr;
@@ -1786,10 +1819,9 @@ int mind_run_noalloc(MindHandle *h, int64_t steps, const MindRecord *records, in
     P.nrec = n_records;
     P.trace = d_trace;
     P.trace_samples = steps + 1;
-    const double **own_initial = h->rec_initial_dev;
     h->rec_initial_dev = d_initial;
     status = advance(h, steps, false);
-    h->rec_initial_dev = own_initial;
+    restore();
     if (status) {
         h->initialized = false;
         return status;

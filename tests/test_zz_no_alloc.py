@@ -73,3 +73,45 @@ def test_noalloc_refuses_runs_beyond_its_scratch():
     status = model.state.lib.mind_run_noalloc(model.state.handle, steps, recs, len(nodes), dummy)
     assert status == abi.MIND_ECAPACITY
     assert b"scratch" in model.state.lib.mind_last_error(model.state.handle)
+
+
+def test_noalloc_refuses_step_counts_whose_size_would_wrap():
+    """Step counts whose trace size overflows 64 bits (steps + 1 == 2^63, or (steps+1) * 8 *
+    records past 2^64) are refused with status 3 before any launch; the clock does not move
+    and the state stays usable."""
+    model = netcases.strong_config1(n_cells=8)
+    layout = mb.build(model)
+    mb.initialize(model)
+    nodes = netcases.soma_nodes(layout)
+    recs = (abi.MindRecord * len(nodes))()
+    for i, node in enumerate(nodes):
+        recs[i].kind = abi.MIND_RECORD_VOLTAGE
+        recs[i].node = int(node)
+    dummy = (ctypes.c_double * 1)()
+    lib, handle = model.state.lib, model.state.handle
+    for steps in ((1 << 63) - 1, 1 << 61, (1 << 64) // (8 * len(nodes)) - 1):
+        assert lib.mind_run_noalloc(handle, steps, recs, len(nodes), dummy) == abi.MIND_ECAPACITY
+        assert model.state.time()[0] == 0
+    assert lib.mind_run_noalloc(handle, (1 << 63) - 1, recs, 0, dummy) == abi.MIND_ECAPACITY
+    status, trace = _noalloc(model.state, 40, nodes)
+    assert status == abi.MIND_OK
+    assert model.state.time()[0] == 40 and np.all(np.isfinite(trace))
+
+
+def test_noalloc_refuses_a_handle_with_surrogate_cells():
+    """Surrogate inference goes through cuBLAS, which may allocate: status 10, state unchanged."""
+    from mind_b200 import surrogate
+
+    model, _ = netcases.coupled_regions(n_regions=2, cells_per_region=8, synapses=8, seed=3)
+    net = surrogate.Mlp(seed=1)
+    state = mb.runtime.DeviceState(model.layout)
+    state.attach_macro(model.macro)
+    state.attach_surrogate(net, np.arange(model.layout.n_cells) % 2 == 0, 1.0)
+    state.initialize()
+    nodes = netcases.soma_nodes(model.layout)
+    status, _ = _noalloc(state, 8, nodes)
+    assert status == abi.MIND_ELAYOUT
+    assert b"surrogate" in state.lib.mind_last_error(state.handle)
+    assert state.time()[0] == 0
+    state.close()
+    net.close()
