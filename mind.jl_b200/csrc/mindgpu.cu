@@ -98,7 +98,7 @@ struct MindHandle {
     std::vector<float> drive;
     int64_t drive_bins = 0;
     std::vector<double> v0_packed;
-    int32_t device = 0;                      // the device current at mind_create: state and stream live there
+    int32_t device = -1;                     // the device current at the first allocation: state and stream live there
     int64_t n_sources = 0;
     std::vector<int64_t> source_ids;
     int32_t precision = MIND_FP64;
@@ -162,6 +162,7 @@ struct MindHandle {
     template <class T>
     T *alloc(size_t count) {
         void *p = nullptr;
+        if (device < 0 && cudaGetDevice(&device) != cudaSuccess) throw std::bad_alloc();
         if (count == 0) count = 1;
         if (cudaMalloc(&p, count * sizeof(T)) != cudaSuccess) throw std::bad_alloc();
         buffers.owned.push_back(p);
@@ -323,7 +324,6 @@ int create(const MindLayout *L, MindHandle *h) {
     if (L->n_mechanisms > kMaxGroups) return fail(h, MIND_ELAYOUT, "too many mechanism groups");
     const int64_t n = L->n_nodes;
     if (n < 0 || n >= INT32_MAX) return fail(h, MIND_ELAYOUT, "node count out of range");
-    CUDA_TRY(h, cudaGetDevice(&h->device));
     h->n_nodes = n;
     h->dt = L->dt;
 
