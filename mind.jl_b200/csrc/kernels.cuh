@@ -1094,9 +1094,14 @@ __global__ void __launch_bounds__(NT, NT == kCellThreads ? 5 : 10) window_kernel
     }
     if (singular) raise_error(P.error, MIND_ESINGULAR);
 
-    // ---- write back ----
+    // ---- write back, with validate_device_state!'s finite check (src/runtime/utils/step.jl:168-197)
+    //      of the written voltage and state; an earlier error code is kept ----
     if (my_det >= 0) P.above[my_src] = my_above ? 1 : 0;
-    for (int32_t i = tid; i < n; i += T) P.v[nb + i] = sv[i];
+    bool finite = true;
+    for (int32_t i = tid; i < n; i += T) {
+        P.v[nb + i] = sv[i];
+        finite &= isfinite(sv[i]);
+    }
     for (int32_t g = 0; g < P.ngroups; ++g) {
         const DevGroup &G = P.groups[g];
         const StagedGroup &S = sg[g];
@@ -1108,29 +1113,27 @@ __global__ void __launch_bounds__(NT, NT == kCellThreads ? 5 : 10) window_kernel
                     G.f[HH_M][row] = S.at(HH_M, r);
                     G.f[HH_H][row] = S.at(HH_H, r);
                     G.f[HH_N][row] = S.at(HH_N, r);
+                    finite &= isfinite(S.at(HH_M, r)) && isfinite(S.at(HH_H, r)) && isfinite(S.at(HH_N, r));
                     break;
                 case MIND_MECH_EXPSYN:
                     G.f[ES_G][row] = S.at(0, r);
+                    finite &= isfinite(S.at(0, r));
                     break;
                 case MIND_MECH_EXP2SYN:
                     G.f[E2_A][row] = S.at(0, r);
                     G.f[E2_B][row] = S.at(1, r);
+                    finite &= isfinite(S.at(0, r)) && isfinite(S.at(1, r));
                     break;
             }
         }
     }
+    if (!finite) atomicCAS(P.error, 0, MIND_ENONFINITE);
 }
 
 /* The run's first sample: every recorded value as it stands in HBM between runs. */
 __global__ void record_initial_kernel(const Params P, const double *const *rec_initial, int32_t nrec) {
     for (int32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nrec; k += gridDim.x * blockDim.x)
         P.trace[k] = *rec_initial[k];
-}
-
-__global__ void finite_kernel(const double *values, int64_t count, int32_t *error) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count;
-         i += (int64_t)gridDim.x * blockDim.x)
-        if (!isfinite(values[i])) atomicCAS(error, 0, MIND_ENONFINITE);
 }
 
 /* Host-injected events of one window: NetCon events into the ring, and the raster

@@ -142,7 +142,8 @@ struct MindHandle {
     const double **rec_ptr_dev = nullptr;       // per cell-sorted record: HBM parameter or null
     double *trace_dev = nullptr;
     size_t trace_capacity = 0;
-    size_t rec_capacity = 0;
+    size_t rec_capacity = 0, rec_off_cap = 0, rec_col_cap = 0, rec_ptr_cap = 0, rec_initial_cap = 0;
+    std::vector<MindRecord> rec_last;             // the record set whose tables are on the device
     struct Bin {
         int32_t first, count;
         size_t smem_bytes;
@@ -912,21 +913,50 @@ int build_records(MindHandle *h, const MindRecord *records, int32_t nrec, Record
     return MIND_OK;
 }
 
+/* Grows a device buffer to `count` elements without shrinking (contents not kept). */
+template <class T>
+T *grow(MindHandle *h, T *old, size_t &capacity, size_t count) {
+    if (count <= capacity && old) return old;
+    const size_t cap = std::max<size_t>(count, std::max<size_t>(64, capacity + capacity / 2));
+    T *p = h->alloc<T>(cap);
+    h->release(const_cast<void *>(static_cast<const void *>(old)));
+    capacity = cap;
+    return p;
+}
+
+/* The run's record maps on the device.  A run with the same records as the last one (the
+ * usual case: a host records the same set every call) reuses the uploaded tables; a new set
+ * is uploaded into buffers that only ever grow, so repeated runs allocate nothing. */
 int set_records(MindHandle *h, const MindRecord *records, int32_t nrec, int64_t samples) {
     Params &P = h->P;
-    RecordTables t;
-    int status = build_records(h, records, nrec, t);
-    if (status) return status;
-    h->release(h->rec_off_dev);
-    h->release(h->rec_node_dev);
-    h->release(h->rec_col_dev);
-    h->release(h->rec_ptr_dev);
-    h->release(h->rec_initial_dev);
-    h->rec_off_dev = h->upload(t.off);
-    h->rec_node_dev = h->upload(t.code);
-    h->rec_col_dev = h->upload(t.col);
-    h->rec_ptr_dev = h->upload(t.ptr);
-    h->rec_initial_dev = h->upload(t.initial);
+    const bool same = nrec == (int32_t)h->rec_last.size() &&
+                      (nrec == 0 || std::memcmp(records, h->rec_last.data(), (size_t)nrec * sizeof(MindRecord)) == 0);
+    if (!same || !h->rec_off_dev) {
+        RecordTables t;
+        int status = build_records(h, records, nrec, t);
+        if (status) return status;
+        const size_t n = std::max<size_t>(1, t.code.size());
+        h->rec_off_dev = grow(h, h->rec_off_dev, h->rec_off_cap, t.off.size());
+        h->rec_node_dev = grow(h, h->rec_node_dev, h->rec_capacity, n);
+        size_t cap = h->rec_capacity;   // the per-entry tables share one capacity
+        h->rec_col_dev = grow(h, h->rec_col_dev, h->rec_col_cap, cap);
+        h->rec_ptr_dev = grow(h, h->rec_ptr_dev, h->rec_ptr_cap, cap);
+        h->rec_initial_dev = grow(h, h->rec_initial_dev, h->rec_initial_cap, std::max<size_t>(1, t.initial.size()));
+        CUDA_TRY(h, cudaMemcpyAsync(h->rec_off_dev, t.off.data(), t.off.size() * sizeof(int32_t),
+                                    cudaMemcpyHostToDevice, h->stream));
+        if (!t.code.empty()) {
+            CUDA_TRY(h, cudaMemcpyAsync(h->rec_node_dev, t.code.data(), t.code.size() * sizeof(int32_t),
+                                        cudaMemcpyHostToDevice, h->stream));
+            CUDA_TRY(h, cudaMemcpyAsync(h->rec_col_dev, t.col.data(), t.col.size() * sizeof(int32_t),
+                                        cudaMemcpyHostToDevice, h->stream));
+            CUDA_TRY(h, cudaMemcpyAsync(h->rec_ptr_dev, t.ptr.data(), t.ptr.size() * sizeof(const double *),
+                                        cudaMemcpyHostToDevice, h->stream));
+            CUDA_TRY(h, cudaMemcpyAsync(h->rec_initial_dev, t.initial.data(),
+                                        t.initial.size() * sizeof(const double *), cudaMemcpyHostToDevice, h->stream));
+        }
+        // pageable sources: the copies above have consumed the host tables when they return
+        h->rec_last.assign(records, records + nrec);
+    }
     P.rec_off = h->rec_off_dev;
     P.rec_node = h->rec_node_dev;
     P.rec_ptr = h->rec_ptr_dev;
@@ -935,6 +965,7 @@ int set_records(MindHandle *h, const MindRecord *records, int32_t nrec, int64_t 
     size_t need = (size_t)samples * (size_t)std::max(nrec, 1);
     if (nrec > 0 && need > h->trace_capacity) {
         h->release(h->trace_dev);
+        h->trace_dev = nullptr;
         h->trace_dev = h->alloc<double>(need);
         h->trace_capacity = need;
     }
@@ -1070,7 +1101,6 @@ int advance(MindHandle *h, int64_t steps, bool record_spikes) {
     }
     CUDA_TRY(h, cudaGetLastError());
     CUDA_TRY(h, cudaEventRecord(h->ev_stop, h->stream));
-    finite_kernel<<<launch_grid(h->n_nodes), kThreads, 0, h->stream>>>(P.v, h->n_nodes, P.error);
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     float ms = 0.0f;
     CUDA_TRY(h, cudaEventElapsedTime(&ms, h->ev_start, h->ev_stop));

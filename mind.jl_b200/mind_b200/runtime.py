@@ -10,6 +10,7 @@ SimulationResult with the recorded traces and the spike raster sorted by
 from __future__ import annotations
 
 import ctypes
+from collections.abc import Mapping
 from dataclasses import dataclass, field
 from typing import Dict, List, Sequence
 
@@ -37,10 +38,33 @@ class RecordSpec:
         return abi.MindRecord(self.kind, self.node, self.group, self.row, self.field)
 
 
+class TraceMap(Mapping):
+    """The traces of a run by record name, each a row view of one [records, samples] array.
+
+    The array is copied out of the device once; the name index is built on the first lookup,
+    so a run recording thousands of quantities costs no per-record work until asked."""
+
+    def __init__(self, names: Sequence[str], by_record: np.ndarray):
+        self._names = list(names)
+        self.by_record = by_record
+        self._index = None
+
+    def __getitem__(self, name):
+        if self._index is None:
+            self._index = {n: i for i, n in enumerate(self._names)}
+        return self.by_record[self._index[name]]
+
+    def __iter__(self):
+        return iter(self._names)
+
+    def __len__(self):
+        return len(self._names)
+
+
 @dataclass
 class SimulationResult:
     time: np.ndarray
-    traces: Dict[str, np.ndarray] = field(default_factory=dict)
+    traces: Mapping = field(default_factory=dict)
     spike_times: np.ndarray = field(default_factory=lambda: np.zeros(0))
     spike_sources: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
     device_ms: float = 0.0
@@ -106,10 +130,21 @@ class DeviceState:
         abi.check(self.lib, self.handle, self.lib.mind_time(self.handle, ctypes.byref(step), ctypes.byref(t)))
         return step.value, t.value
 
+    def _c_records(self, records: Sequence[RecordSpec]):
+        """The MindRecord array of `records`, built once per record list (a host that records
+        the same list every call converts it once; the library keeps its tables too)."""
+        cached = getattr(self, "_rec_cache", None)
+        if cached is not None and cached[0] is records:
+            return cached[1]
+        table = np.zeros((max(1, len(records)), 5), dtype=np.int32)
+        if records:
+            table[:len(records)] = [(r.kind, r.node, r.group, r.row, r.field) for r in records]
+        self._rec_cache = (records, table)
+        return table
+
     def run_steps(self, steps: int, records: Sequence[RecordSpec], record_spikes: bool = True):
-        recs = (abi.MindRecord * max(1, len(records)))()
-        for i, r in enumerate(records):
-            recs[i] = r.to_c()
+        table = self._c_records(records)
+        recs = table.ctypes.data_as(ctypes.POINTER(abi.MindRecord))
         start_step, _ = self.time()
         abi.check(self.lib, self.handle,
                   self.lib.mind_run(self.handle, steps, recs, len(records), 1 if record_spikes else 0))
@@ -147,9 +182,8 @@ class DeviceState:
                     self.handle, mt.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), mt.size, ctypes.byref(samples)))
             result.macro_trace = mt
         if records:
-            by_record = np.ascontiguousarray(trace.T)   # one copy; each trace is a row view
-            for i, r in enumerate(records):
-                result.traces[r.name] = by_record[i]
+            # one transposed copy; each trace is a row view of it
+            result.traces = TraceMap([r.name for r in records], np.ascontiguousarray(trace.T))
         return result
 
     def run_stats(self) -> abi.MindRunStats:
@@ -254,7 +288,9 @@ def run(model, stop_time: float, *, records: Sequence[RecordSpec] = (), record_s
     if model.state is None:
         raise ValueError("simulation is not initialized")
     steps = _steps_to(model.layout, model.state, stop_time)
-    return model.state.run_steps(steps, list(records), record_spikes)
+    if not isinstance(records, (list, tuple)):
+        records = list(records)
+    return model.state.run_steps(steps, records, record_spikes)
 
 
 def step(model):

@@ -34,6 +34,12 @@
  * own term first, then children in ascending node index; mechanism groups in
  * layout order; rows in row order.  The library uses the same order, which
  * makes FP64 parity bit-exact.  Both sides call mind_math.h for exp/log/pow.
+ *
+ * Threads: cells are independent between two event deliveries, so each step hands
+ * whole cells (currents, cable assembly and solve, state advance) to a pool of worker
+ * threads created once per run; detection, the event heap and the regions stay serial.
+ * Every node is summed by one thread in the fixed order above, so the result does not
+ * depend on the thread count.
  */
 #include "../include/mindgpu.h"
 #include "../mind.jl_b200/csrc/mind_math.h"
@@ -48,6 +54,9 @@
 #include <vector>
 
 #include <atomic>
+#include <condition_variable>
+#include <functional>
+#include <mutex>
 #include <thread>
 
 namespace {
@@ -67,6 +76,69 @@ struct Later {
         if (a.order != b.order) return a.order > b.order;
         return a.target > b.target;
     }
+};
+
+/* A fixed set of worker threads, created once per run and reused every step: run(job)
+ * calls job(k) for k = 0 .. n-1 on the workers and the caller, and returns when all are
+ * done.  No thread is created or joined inside the step loop. */
+class ThreadPool {
+  public:
+    explicit ThreadPool(int n) : n_(n < 1 ? 1 : n) {
+        for (int k = 1; k < n_; ++k) workers_.emplace_back([this, k] { loop(k); });
+    }
+    ~ThreadPool() {
+        {
+            std::lock_guard<std::mutex> lock(mutex_);
+            stop_ = true;
+            ++generation_;
+        }
+        wake_.notify_all();
+        for (auto &t : workers_) t.join();
+    }
+    int size() const { return n_; }
+    void run(const std::function<void(int)> &job) {
+        if (n_ == 1) {
+            job(0);
+            return;
+        }
+        {
+            std::lock_guard<std::mutex> lock(mutex_);
+            job_ = &job;
+            pending_ = n_ - 1;
+            ++generation_;
+        }
+        wake_.notify_all();
+        job(0);
+        std::unique_lock<std::mutex> lock(mutex_);
+        done_.wait(lock, [this] { return pending_ == 0; });
+        job_ = nullptr;
+    }
+
+  private:
+    void loop(int k) {
+        uint64_t seen = 0;
+        for (;;) {
+            const std::function<void(int)> *job;
+            {
+                std::unique_lock<std::mutex> lock(mutex_);
+                wake_.wait(lock, [&] { return generation_ != seen; });
+                seen = generation_;
+                if (stop_) return;
+                job = job_;
+            }
+            (*job)(k);
+            std::lock_guard<std::mutex> lock(mutex_);
+            if (--pending_ == 0) done_.notify_one();
+        }
+    }
+    int n_;
+    std::vector<std::thread> workers_;
+    std::mutex mutex_;
+    std::condition_variable wake_, done_;
+    const std::function<void(int)> *job_ = nullptr;
+    uint64_t generation_ = 0;
+    int pending_ = 0;
+    bool stop_ = false;
 };
 
 struct Group {
@@ -104,6 +176,11 @@ struct Oracle {
     std::vector<int64_t> child_off;
     std::vector<int32_t> child;   // ascending
     std::vector<std::vector<int32_t>> cell_up;    // per cell: nodes children-before-parent
+    std::vector<int32_t> cell_of;                 // per node: its cell
+    // per cell and group: the group's rows on the cell's nodes, ascending (row order)
+    std::vector<std::vector<std::vector<int64_t>>> cell_rows;
+    std::vector<int64_t> detector_sources;        // sources with a threshold detector, ascending
+    ThreadPool *pool = nullptr;
     std::vector<Group> groups;
     std::vector<MindRan> ran;     // per NetStim row, indexed via group
     std::vector<char> above;
@@ -307,6 +384,15 @@ struct Oracle {
         for (int64_t s = 0; s < L->n_sources; ++s)
             if (L->source_points[s] > 0) point_source[L->source_points[s] - 1] = s;
         above.assign(L->n_sources, 0);
+        cell_of.assign(n, -1);
+        for (size_t c = 0; c < cell_up.size(); ++c)
+            for (int32_t i : cell_up[c]) cell_of[i] = (int32_t)c;
+        cell_rows.assign(cell_up.size(), std::vector<std::vector<int64_t>>(groups.size()));
+        for (size_t g = 0; g < groups.size(); ++g)
+            for (int64_t r = 0; r < groups[g].rows; ++r)
+                if (groups[g].node[r] >= 0) cell_rows[cell_of[groups[g].node[r]]][g].push_back(r);
+        for (int64_t s = 0; s < L->n_sources; ++s)
+            if (L->source_nodes[s] > 0) detector_sources.push_back(s);
         return 0;
     }
 
@@ -490,72 +576,77 @@ struct Oracle {
         }
     }
 
-    void currents(double tc) {
-        for (int64_t i = 0; i < n; ++i) {
+    /* BREAKPOINT currents of one row at v + 0.001 and v into rhs and d of its node. */
+    void current_row(Group &G, int64_t r, double tc) {
+        int32_t node = G.node[r];
+        if (node < 0) return;
+        double vv = v[node];
+        double probe = vv + 0.001;
+        double shifted = 0.0, value = 0.0;
+        double scale = 1.0;
+        bool density = false;
+        switch (G.kind) {
+            case MIND_MECH_HH: {
+                density = true;
+                auto eval = [&](double u) {
+                    double m = G.f[HH_M][r], h = G.f[HH_H][r], nn = G.f[HH_N][r];
+                    double gna = G.f[HH_GNABAR][r] * m * m * m * h;
+                    double ina = gna * (u - G.f[HH_ENA][r]);
+                    double gk = G.f[HH_GKBAR][r] * nn * nn * nn * nn;
+                    double ik = gk * (u - G.f[HH_EK][r]);
+                    double il = G.f[HH_GL][r] * (u - G.f[HH_EL][r]);
+                    return ((0.0 + il) + ina) + ik;
+                };
+                shifted = eval(probe);
+                value = eval(vv);
+            } break;
+            case MIND_MECH_PAS: {
+                density = true;
+                shifted = 0.0 + G.f[PAS_G][r] * (probe - G.f[PAS_E][r]);
+                value = 0.0 + G.f[PAS_G][r] * (vv - G.f[PAS_E][r]);
+            } break;
+            case MIND_MECH_EXPSYN: {
+                shifted = 0.0 + G.f[ES_G][r] * (probe - G.f[ES_E][r]);
+                value = 0.0 + G.f[ES_G][r] * (vv - G.f[ES_E][r]);
+            } break;
+            case MIND_MECH_EXP2SYN: {
+                double gs = G.f[E2_B][r] - G.f[E2_A][r];
+                shifted = 0.0 + gs * (probe - G.f[E2_E][r]);
+                value = 0.0 + gs * (vv - G.f[E2_E][r]);
+            } break;
+            case MIND_MECH_ICLAMP: {
+                double del = G.f[IC_DEL][r];
+                double i = (tc < del + G.f[IC_DUR][r] && tc >= del) ? G.f[IC_AMP][r] : 0.0;
+                shifted = 0.0 - i;
+                value = 0.0 - i;
+            } break;
+            case MIND_MECH_ALPHASYN: {  // mod/AlphaSynapse.mod BREAKPOINT
+                double g = G.f[AS_GMAX][r] * mind_alpha((tc - G.f[AS_ONSET][r]) / G.f[AS_TAU][r]);
+                shifted = 0.0 + g * (probe - G.f[AS_E][r]);
+                value = 0.0 + g * (vv - G.f[AS_E][r]);
+            } break;
+            default: return;
+        }
+        if (density) {
+            scale = area[node] * 0.01;
+            rhs[node] -= scale * value;
+            d[node] += scale * (shifted - value) / 0.001;
+        } else {
+            rhs[node] += -scale * value;
+            d[node] += scale * (shifted - value) / 0.001;
+        }
+    }
+
+    /* Currents of one cell: its nodes cleared, then groups in layout order and each group's
+     * rows in row order -- per node the order of the reference's serial loop
+     * (src/runtime/cuda/micro.jl:427-500 with the atomics' order fixed). */
+    void currents_cell(int64_t c, double tc) {
+        for (int32_t i : cell_up[c]) {
             rhs[i] = 0.0;
             d[i] = 0.0;
         }
-        for (auto &G : groups) {
-            for (int64_t r = 0; r < G.rows; ++r) {
-                int32_t node = G.node[r];
-                if (node < 0) continue;
-                double vv = v[node];
-                double probe = vv + 0.001;
-                double shifted = 0.0, value = 0.0;
-                double scale = 1.0;
-                bool density = false;
-                switch (G.kind) {
-                    case MIND_MECH_HH: {
-                        density = true;
-                        auto eval = [&](double u) {
-                            double m = G.f[HH_M][r], h = G.f[HH_H][r], nn = G.f[HH_N][r];
-                            double gna = G.f[HH_GNABAR][r] * m * m * m * h;
-                            double ina = gna * (u - G.f[HH_ENA][r]);
-                            double gk = G.f[HH_GKBAR][r] * nn * nn * nn * nn;
-                            double ik = gk * (u - G.f[HH_EK][r]);
-                            double il = G.f[HH_GL][r] * (u - G.f[HH_EL][r]);
-                            return ((0.0 + il) + ina) + ik;
-                        };
-                        shifted = eval(probe);
-                        value = eval(vv);
-                    } break;
-                    case MIND_MECH_PAS: {
-                        density = true;
-                        shifted = 0.0 + G.f[PAS_G][r] * (probe - G.f[PAS_E][r]);
-                        value = 0.0 + G.f[PAS_G][r] * (vv - G.f[PAS_E][r]);
-                    } break;
-                    case MIND_MECH_EXPSYN: {
-                        shifted = 0.0 + G.f[ES_G][r] * (probe - G.f[ES_E][r]);
-                        value = 0.0 + G.f[ES_G][r] * (vv - G.f[ES_E][r]);
-                    } break;
-                    case MIND_MECH_EXP2SYN: {
-                        double gs = G.f[E2_B][r] - G.f[E2_A][r];
-                        shifted = 0.0 + gs * (probe - G.f[E2_E][r]);
-                        value = 0.0 + gs * (vv - G.f[E2_E][r]);
-                    } break;
-                    case MIND_MECH_ICLAMP: {
-                        double del = G.f[IC_DEL][r];
-                        double i = (tc < del + G.f[IC_DUR][r] && tc >= del) ? G.f[IC_AMP][r] : 0.0;
-                        shifted = 0.0 - i;
-                        value = 0.0 - i;
-                    } break;
-                    case MIND_MECH_ALPHASYN: {  // mod/AlphaSynapse.mod BREAKPOINT
-                        double g = G.f[AS_GMAX][r] * mind_alpha((tc - G.f[AS_ONSET][r]) / G.f[AS_TAU][r]);
-                        shifted = 0.0 + g * (probe - G.f[AS_E][r]);
-                        value = 0.0 + g * (vv - G.f[AS_E][r]);
-                    } break;
-                    default: continue;
-                }
-                if (density) {
-                    scale = area[node] * 0.01;
-                    rhs[node] -= scale * value;
-                    d[node] += scale * (shifted - value) / 0.001;
-                } else {
-                    rhs[node] += -scale * value;
-                    d[node] += scale * (shifted - value) / 0.001;
-                }
-            }
-        }
+        for (size_t g = 0; g < groups.size(); ++g)
+            for (int64_t r : cell_rows[c][g]) current_row(groups[g], r, tc);
     }
 
     int cable(int64_t cell) {
@@ -597,35 +688,35 @@ struct Oracle {
         return status;
     }
 
-    void advance(double ta) {
-        (void)ta;
-        for (auto &G : groups) {
-            for (int64_t r = 0; r < G.rows; ++r) {
-                switch (G.kind) {
-                    case MIND_MECH_HH: {
-                        Rates R = rates(v[G.node[r]]);
-                        G.f[HH_M][r] = cnexp(G.f[HH_M][r], R.minf, R.mtau, dt);
-                        G.f[HH_H][r] = cnexp(G.f[HH_H][r], R.hinf, R.htau, dt);
-                        G.f[HH_N][r] = cnexp(G.f[HH_N][r], R.ninf, R.ntau, dt);
-                    } break;
-                    case MIND_MECH_EXPSYN:
-                        G.f[ES_G][r] = cnexp(G.f[ES_G][r], 0.0, G.f[ES_TAU][r], dt);
-                        break;
-                    case MIND_MECH_EXP2SYN:
-                        G.f[E2_A][r] = cnexp(G.f[E2_A][r], 0.0, G.f[E2_TAU1][r], dt);
-                        G.f[E2_B][r] = cnexp(G.f[E2_B][r], 0.0, G.f[E2_TAU2][r], dt);
-                        break;
-                    default: break;
-                }
-            }
+    /* cnexp state advance of one row on the new voltage (src/compiler/codegen.jl:569-641). */
+    void advance_row(Group &G, int64_t r) {
+        switch (G.kind) {
+            case MIND_MECH_HH: {
+                Rates R = rates(v[G.node[r]]);
+                G.f[HH_M][r] = cnexp(G.f[HH_M][r], R.minf, R.mtau, dt);
+                G.f[HH_H][r] = cnexp(G.f[HH_H][r], R.hinf, R.htau, dt);
+                G.f[HH_N][r] = cnexp(G.f[HH_N][r], R.ninf, R.ntau, dt);
+            } break;
+            case MIND_MECH_EXPSYN:
+                G.f[ES_G][r] = cnexp(G.f[ES_G][r], 0.0, G.f[ES_TAU][r], dt);
+                break;
+            case MIND_MECH_EXP2SYN:
+                G.f[E2_A][r] = cnexp(G.f[E2_A][r], 0.0, G.f[E2_TAU1][r], dt);
+                G.f[E2_B][r] = cnexp(G.f[E2_B][r], 0.0, G.f[E2_TAU2][r], dt);
+                break;
+            default: break;
         }
+    }
+
+    void advance_cell(int64_t c) {
+        for (size_t g = 0; g < groups.size(); ++g)
+            for (int64_t r : cell_rows[c][g]) advance_row(groups[g], r);
     }
 
     void detect(double t) {
         double time = t + 1.0e-10;
-        for (int64_t s = 0; s < L->n_sources; ++s) {
+        for (int64_t s : detector_sources) {
             int32_t node = L->source_nodes[s];
-            if (node <= 0) continue;
             bool current = v[node - 1] > L->source_thresholds[s];
             if (current && !above[s]) {
                 emit_spike(s, time);
@@ -635,43 +726,36 @@ struct Oracle {
         }
     }
 
-    int advance_step(int threads) {
+    /* One micro step (src/runtime/step.jl:91-151).  Detection, the macro step and event
+     * delivery are serial (heap order); the cells are independent between deliveries, so
+     * each cell's currents, cable solve and state advance run on one worker of the pool,
+     * cells handed out in small chunks. */
+    int advance_step() {
         double t = (double)step * dt;
         if (ML && step % spm == 0) macro_step(step / spm);
         detect(t);
         deliver(t + 0.5 * dt);
-        currents(t + 0.5 * dt);
-        int64_t cells = (int64_t)cell_up.size();
-        int status = 0;
-        if (threads <= 1 || cells < 2) {
-            for (int64_t c = 0; c < cells; ++c) {
-                int s = cable(c);
-                if (s > status) status = s;
-            }
-        } else {
-            // Cells are independent: a shared counter hands them out in chunks.
-            std::atomic<int64_t> next{0};
-            std::atomic<int> worst{0};
-            auto worker = [&]() {
-                for (;;) {
-                    int64_t lo = next.fetch_add(16);
-                    if (lo >= cells) break;
-                    int64_t hi = std::min(cells, lo + 16);
-                    for (int64_t c = lo; c < hi; ++c) {
-                        int s = cable(c);
-                        int w = worst.load();
-                        while (s > w && !worst.compare_exchange_weak(w, s)) {
-                        }
+        const double tc = t + 0.5 * dt;
+        const int64_t cells = (int64_t)cell_up.size();
+        std::atomic<int64_t> next{0};
+        std::atomic<int> worst{0};
+        pool->run([&](int) {
+            for (;;) {
+                const int64_t lo = next.fetch_add(4);
+                if (lo >= cells) break;
+                const int64_t hi = std::min(cells, lo + 4);
+                for (int64_t c = lo; c < hi; ++c) {
+                    currents_cell(c, tc);
+                    const int s = cable(c);
+                    advance_cell(c);
+                    int w = worst.load();
+                    while (s > w && !worst.compare_exchange_weak(w, s)) {
                     }
                 }
-            };
-            std::vector<std::thread> pool;
-            for (int k = 0; k < threads; ++k) pool.emplace_back(worker);
-            for (auto &th : pool) th.join();
-            status = worst.load();
-        }
+            }
+        });
+        const int status = worst.load();
         if (status) return fail(status, "singular or non-finite cable system");
-        advance(t + dt);
         step += 1;
         return 0;
     }
@@ -688,6 +772,8 @@ int oracle_run_macro(const MindLayout *layout, const MindMacroLayout *macro, int
                      int32_t nrec, int32_t threads, double *trace, double *spike_t, int64_t *spike_sid, int64_t cap,
                      int64_t *nspikes, double *macro_trace, double *run_ms, char *message, int32_t message_len) {
     Oracle o;
+    ThreadPool pool(threads);
+    o.pool = &pool;
     int status = o.load(layout);
     if (!status && macro) status = o.load_macro(macro);
     if (!status) {
@@ -738,7 +824,7 @@ int oracle_run_macro(const MindLayout *layout, const MindMacroLayout *macro, int
     if (!status) {
         if (nrec) record(0);
         for (int64_t s = 0; s < steps && !status; ++s) {
-            status = o.advance_step(threads);
+            status = o.advance_step();
             if (status) break;
             if (nrec) record(s + 1);
             o.deliver((double)o.step * o.dt);

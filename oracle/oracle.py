@@ -111,10 +111,12 @@ class OracleResult:
     macro_trace: np.ndarray = None   # [macro boundaries, regions], with regions
 
 
-def run(layout, steps: int, record_nodes=(), threads: int = 1, spike_cap: int = 1 << 22, macro=None,
+def run(layout, steps: int, record_nodes=(), threads: int = 0, spike_cap: int = 1 << 22, macro=None,
         records=None) -> OracleResult:
     """Initialize the layout (and the regions of `macro`, a MacroModel) on the CPU and advance
     `steps` micro steps; with regions, `macro_trace` holds out(k) for k = 0 .. steps / (dt_macro/dt).
+    `threads` worker threads (0: every host core) share the cells of each step; the result
+    does not depend on their number.
     `records` (objects with kind, node, group, row, field, such as RecordSpec) replaces
     `record_nodes` (voltages of 1-based nodes) when given."""
     import sys
@@ -125,6 +127,8 @@ def run(layout, steps: int, record_nodes=(), threads: int = 1, spike_cap: int = 
     from mind_b200 import abi
 
     lib = _load()
+    if threads <= 0:
+        threads = os.cpu_count() or 1
     c_layout = layout.to_c()
     if records is None:
         specs = [(abi.MIND_RECORD_VOLTAGE, int(node), 0, 0, 0) for node in record_nodes]
