@@ -65,6 +65,9 @@ def parse():
     p.add_argument("--surrogate", action="store_true",
                    help="config 4: train the spike-output surrogate on a detailed run, then time the coupled run "
                         "with 98%% of the cells replaced, against the plain FP64 run, and their region rates")
+    p.add_argument("--settle-ms", type=float, default=50.0,
+                   help="simulated time advanced untimed before --warmup in both arms, so the timed steps run "
+                        "on an active network (recurrent cell spikes, routing, NET_RECEIVE); config.t_start_ms")
     p.add_argument("--cpu-steps", type=int, default=8)
     p.add_argument("--no-cpu-baseline", action="store_true")
     return p.parse_args()
@@ -162,11 +165,13 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def cpu_baseline(layout, steps: int, threads: int):
+def cpu_baseline(layout, steps: int, threads: int, settle_steps: int = 0):
+    """The CPU FP64 restatement on `threads` host threads: `settle_steps` untimed, then `steps`
+    timed (the same simulated interval the GPU arm times)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
 
-    result = oracle.run(layout, steps, (), threads=threads)
+    result = oracle.run(layout, settle_steps + steps, (), threads=threads, timed_from=settle_steps)
     if result.status != 0:
         raise RuntimeError(f"oracle failed: {result.message}")
     value = layout.segment_count * steps / (result.run_ms / 1000.0)
@@ -192,8 +197,10 @@ def recorded_traffic():
         return None
 
 
-def mixed_accuracy(layout, fp64, mixed, warmup: int, steps: int) -> dict:
-    """Mixed mode against FP64 on the same run: soma voltages of every cell and the cell spike raster.
+def mixed_accuracy(layout, fp64, mixed, voltage_window_ms, raster_window_ms) -> dict:
+    """Mixed mode against FP64 on the same schedule: soma voltages of every cell over
+    `voltage_window_ms` and the cell spike raster over `raster_window_ms` (the whole run from
+    t = 0, settle included).
 
     The FP64 path reproduces the CPU FP64 oracle bit for bit (tests/test_parity_gpu.py), so
     these are also the differences to the oracle.  A spike counts as matched when the same cell
@@ -219,7 +226,7 @@ def mixed_accuracy(layout, fp64, mixed, warmup: int, steps: int) -> dict:
     n32 = int(np.sum(sid32 < n_cells))
     return {
         "reference": "FP64 path (bit-identical to the CPU FP64 oracle)",
-        "window_ms": [warmup * dt, (warmup + steps) * dt],
+        "voltage_window_ms": list(voltage_window_ms), "raster_window_ms": list(raster_window_ms),
         "max_dv_mv": float(dv.max()), "max_dv_subthreshold_mv": float(dv[sub].max()) if sub.any() else None,
         "p99_dv_mv": float(np.percentile(dv, 99)),
         "cell_spikes_fp64": n64, "cell_spikes_mixed": n32,
@@ -245,40 +252,46 @@ def device_timed(fn):
     return out, start.elapsed_time(stop)
 
 
-def measure_sharded(args, layout, rank: int, world: int, precision: str, local_rank: int):
+def measure_sharded(args, layout, rank: int, world: int, precision: str, local_rank: int, settle_steps: int = 0):
     """One config-2 network over `world` GPUs: this rank's cells, spikes exchanged per window
     (mind_b200.sharding).  Timed on the device around the window loop, exchanges included;
-    the job figure uses the slowest rank."""
+    the job figure uses the slowest rank.  The settle and warm-up run untimed first."""
     import mind_b200 as mb
     from mind_b200 import replicas, sharding
 
     run = sharding.ShardedRun(layout, rank, world, precision=precision, device=COLLECTIVE_DEVICE, local=True)
-    run.run_steps(args.warmup, (), False)
+    rasters = [run.run_steps(settle_steps, (), True), run.run_steps(args.warmup, (), True)]
     run.launches = 0
     sampler = ClockSampler(local_rank)
     with sampler:
         result, ms = device_timed(lambda: run.run_steps(args.steps, (), True))
     clocks = sampler.summary()
+    rasters.append(result)
     launches = run.launches
     run_ms, units = replicas.reduce_timing(ms, layout.segment_count * args.steps, device=COLLECTIVE_DEVICE)
     events = delivered_events(layout, result.spike_sources)
     algo = algorithmic_bytes_per_step(layout, events / args.steps)
     achieved = algo * args.steps / (result.device_ms / 1000.0) / 1e9 if result.device_ms > 0 else None
     soma = run.records([layout.voltage_node(c) for c in range(1, layout.n_cells + 1)])
-    run.state.initialize()
-    run.run_steps(args.warmup, (), False)
+    rasters.append(run.run_steps(args.steps, soma, True))
+    e2e_t0 = run.state.time()[1]
     e2e_result, e2e_ms = device_timed(lambda: run.run_steps(args.steps, soma, True))
+    rasters.append(e2e_result)
     e2e_ms, _ = replicas.reduce_timing(e2e_ms, 0.0, device=COLLECTIVE_DEVICE)
     d2h = (len(soma) * 8 * (args.steps + 1) + 16 * len(e2e_result.spike_times)) / args.steps
     run.close()
     trace = np.stack([e2e_result.traces[r.name] for r in soma])
+    end_ms = e2e_t0 + args.steps * layout.dt
     return ({"value": units / (run_ms / 1000.0), "ms_per_step": run_ms / args.steps,
              "window_ms": result.device_ms, "window_launches": None, "launches": launches,
              "window_steps": run.window, "bins": None, "algo_bytes_per_step": algo, "achieved_gbs": achieved,
              "spikes": int(len(result.spike_times)), "delivered_events": events,
-             "e2e": units / (e2e_ms / 1000.0), "d2h": d2h, "h2d": 8 * len(soma) / args.steps,
+             "cell_spikes_timed": int(np.sum(result.spike_sources < layout.n_cells)),
+             "e2e": units / (e2e_ms / 1000.0), "d2h": d2h, "h2d": 0.0,
+             "voltage_window_ms": [e2e_t0, end_ms], "raster_window_ms": [0.0, end_ms],
              "exchange": "all-gather of (sid, time) per window over NCCL"},
-            (trace, e2e_result.spike_sources, e2e_result.spike_times), clocks)
+            (trace, np.concatenate([r.spike_sources for r in rasters]),
+             np.concatenate([r.spike_times for r in rasters])), clocks)
 
 
 def measure_surrogate(args, model, layout, train_ms: float = 300.0, eval_ms: float = 200.0, keep: float = 0.02):
@@ -351,26 +364,31 @@ def measure_surrogate(args, model, layout, train_ms: float = 300.0, eval_ms: flo
 
 
 def run_reference(args, rank: int):
+    """The reference arm: the CPU FP64 restatement of MIND.jl's step loop (oracle/) on every host
+    core, on the GPU arm's network and schedule -- the same untimed settle and warm-up, then
+    the same --steps timed."""
     if rank != 0:
         return
     threads = os.cpu_count() or 1
     model, layout = build_network(args.cells, seed=1, config=args.config)
-    steps = max(1, args.cpu_steps)
-    values = []
-    for _ in range(max(1, args.steps and 1)):
-        value, ms = cpu_baseline(layout, steps, threads)
-        values.append(value)
-    value = statistics.median(values)
+    settle_steps = int(round(args.settle_ms / layout.dt))
+    steps = max(1, args.steps)
+    value, ms = cpu_baseline(layout, steps, threads, settle_steps + args.warmup)
     line = {
-        "impl": "reference", "metric": WORKLOAD_METRICS.get(args.config, METRIC), "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": steps, "warmup": 0, "ms_per_step": ms / steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded config-2 network)",
+        "impl": "reference", "metric": WORKLOAD_METRICS.get(args.config, METRIC), "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup, "ms_per_step": ms / steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": f"synthetic (seeded config-{args.config} network, mind_b200.networks.config{args.config})",
         "config": {"workload": f"config{args.config}", "cells": layout.n_cells, "compartments": layout.segment_count,
-                   "dt_ms": layout.dt, "l2": "state larger than L2"},
+                   "nodes": layout.n_nodes, "dt_ms": layout.dt, "t_start_ms": args.settle_ms,
+                   "l2": "state larger than L2"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"first {steps} micro steps of the full config-{args.config} network"},
+                         "sample": f"{steps} micro steps of the full config-{args.config} network from "
+                                   f"t = {args.settle_ms:g} ms + {args.warmup} warm-up steps (settle untimed)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "note": "MIND.jl is Julia (absent here); the reference arm is the CPU FP64 restatement of its step loop",
+        "note": "MIND.jl is Julia (absent here) and has no CPU path; the reference arm is the CPU FP64 "
+                "restatement of its step loop, every cell's currents, cable solve and state advance "
+                "spread over a pool of host threads",
     }
     print(json.dumps(line), flush=True)
 
@@ -422,35 +440,41 @@ def main():
                 runs[precision] = (np.stack([r.traces[x.name] for x in soma_all]), r.spike_sources, r.spike_times)
             steps = int(round(args.accuracy_ms / layout.dt))
             print(json.dumps({"config": f"config{args.config}", "cells": layout.n_cells,
-                              "accuracy": mixed_accuracy(layout, runs["fp64"], runs["mixed"], 0, steps)}), flush=True)
+                              "accuracy": mixed_accuracy(layout, runs["fp64"], runs["mixed"], [0.0, args.accuracy_ms],
+                                                         [0.0, args.accuracy_ms])}), flush=True)
         if dist is not None:
             dist.destroy_process_group()
         return
     soma = [mb.RecordSpec(layout.voltage_node(c), f"v{c}") for c in range(1, layout.n_cells + 1)]
     precisions = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
+    dt = layout.dt
+    settle_steps = int(round(args.settle_ms / dt))
     results, runs = {}, {}
     clocks = None
     for precision in precisions:
         if sharded:
             results[precision], runs[precision], clocks = measure_sharded(args, layout, rank, world, precision,
-                                                                          local_rank)
+                                                                          local_rank, settle_steps)
             continue
         mb.initialize(model, precision=precision)
         # launch shape per size bin, timed on trial windows before the measurement (setup,
         # like the build; the state restarts at t = 0)
         shapes = mb.autotune(model, windows=3) if not args.no_autotune else model.state.bin_threads()
+        # settle, then warm up, untimed: the timed steps start at t_start on an active network
+        rasters = [mb.run(model, settle_steps * dt, record_spikes=True)]
+        rasters.append(mb.run(model, (settle_steps + args.warmup) * dt, record_spikes=True))
         model.state.set_profiling(True)
-        dt = layout.dt
-        mb.run(model, args.warmup * dt, record_spikes=False)
         torch.cuda.synchronize()
         if dist is not None:
             dist.barrier()
         sampler = ClockSampler(local_rank)
         with sampler:
-            result = mb.run(model, (args.warmup + args.steps) * dt, record_spikes=True)
+            result = mb.run(model, (settle_steps + args.warmup + args.steps) * dt, record_spikes=True)
             torch.cuda.synchronize()
         if dist is not None:
             dist.barrier()
+        rasters.append(result)
+        model.state.set_profiling(False)
         stats = model.state.run_stats()
         clocks = sampler.summary()
         run_ms, units = replicas.reduce_timing(stats.run_ms, layout.segment_count * args.steps, device=COLLECTIVE_DEVICE)
@@ -459,25 +483,32 @@ def main():
         algo = algorithmic_bytes_per_step(layout, events / args.steps)
         window_ms = stats.window_ms
         achieved = algo * args.steps / (window_ms / 1000.0) / 1e9 if window_ms > 0 else None
-        # End to end through the public API: a run call with host recording, after one
-        # untimed call of the same shape (which sizes the library's trace and raster buffers).
-        mb.initialize(model, precision=precision)
-        mb.run(model, args.steps * dt, records=soma, record_spikes=True)
+        # End to end through the public API, continuing the same run: one untimed call with the
+        # soma records (the library uploads their tables once and keeps them), then the timed
+        # call, which copies every soma trace and the raster to the host.
+        t_now = model.state.time()[1]
+        rasters.append(mb.run(model, t_now + args.steps * dt, records=soma, record_spikes=True))
+        e2e_t0 = model.state.time()[1]
         e2e_result, e2e_ms = device_timed(
-            lambda: mb.run(model, 2 * args.steps * dt, records=soma, record_spikes=True))
+            lambda: mb.run(model, e2e_t0 + args.steps * dt, records=soma, record_spikes=True))
+        rasters.append(e2e_result)
         e2e_ms, _ = replicas.reduce_timing(e2e_ms, 0.0, device=COLLECTIVE_DEVICE)
         e2e_s = e2e_ms / 1000.0
         d2h = (len(soma) * 8 * (args.steps + 1) + 16 * len(e2e_result.spike_times)) / args.steps
-        h2d = 8 * len(soma) / args.steps
-        runs[precision] = (np.stack([e2e_result.traces[r.name] for r in soma]), e2e_result.spike_sources,
-                           e2e_result.spike_times)
+        h2d = 0.0   # the record set is unchanged since the untimed call: nothing is uploaded
+        runs[precision] = (e2e_result.traces.by_record,
+                           np.concatenate([r.spike_sources for r in rasters]),
+                           np.concatenate([r.spike_times for r in rasters]))
         results[precision] = {
             "bin_threads": shapes,
             "value": value, "ms_per_step": run_ms / args.steps, "window_ms": window_ms,
             "window_launches": stats.window_launches, "launches": stats.launches, "window_steps": stats.window_steps,
             "bins": stats.bins, "algo_bytes_per_step": algo, "achieved_gbs": achieved,
             "spikes": int(len(result.spike_times)), "delivered_events": events,
-            "e2e": units / e2e_s, "d2h": d2h, "h2d": h2d,
+            "cell_spikes_timed": int(np.sum(result.spike_sources < layout.n_cells)),
+            "e2e": units / e2e_s, "e2e_ms_per_step": e2e_ms / args.steps, "d2h": d2h, "h2d": h2d,
+            "voltage_window_ms": [e2e_t0, e2e_t0 + args.steps * dt],
+            "raster_window_ms": [0.0, e2e_t0 + args.steps * dt],
         }
     if rank != 0:
         if dist is not None:
@@ -498,7 +529,8 @@ def main():
                                    else f"replica x{world}" if world > 1 else "1 GPU"),
                    "l2": "working set larger than L2 (no flush needed)",
                    "window_steps": head["window_steps"], "size_bins": head["bins"],
-                   "threads_per_cell_by_bin": head.get("bin_threads")},
+                   "threads_per_cell_by_bin": head.get("bin_threads"), "t_start_ms": args.settle_ms,
+                   "timed_cell_spikes": head.get("cell_spikes_timed")},
         "e2e": {"value": head["e2e"], "unit": UNIT, "h2d_bytes_per_step": head["h2d"],
                 "d2h_bytes_per_step": head["d2h"]},
         "roofline": {
@@ -513,20 +545,22 @@ def main():
                     "kernel keeps each cell on-chip for a window of steps, so its DRAM traffic (traffic) is "
                     "far below the algorithmic bytes and the kernel is latency-bound, not HBM-bound",
         },
-        "gpu_launches": head["launches"] + 2,
+        "gpu_launches": head["launches"],
         "clocks": clocks,
         "modes": {k: {"value": v["value"], "ms_per_step": v["ms_per_step"], "e2e": v["e2e"],
                       "threads_per_cell_by_bin": v.get("bin_threads")}
                   for k, v in results.items()},
-        "accuracy": (mixed_accuracy(layout, runs["fp64"], runs["mixed"], args.warmup, args.steps)
+        "accuracy": (mixed_accuracy(layout, runs["fp64"], runs["mixed"], head["voltage_window_ms"],
+                                    head["raster_window_ms"])
                      if "fp64" in runs and "mixed" in runs else None),
         "spikes": head["spikes"],
     }
     if world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        cpu_value, _ = cpu_baseline(layout, args.cpu_steps, threads)
+        cpu_value, _ = cpu_baseline(layout, args.cpu_steps, threads, settle_steps)
         line["cpu_baseline"] = {"value": cpu_value, "unit": UNIT, "cores": threads, "kind": "port",
-                                "sample": f"first {args.cpu_steps} micro steps of the full config-{args.config} network"}
+                                "sample": f"{args.cpu_steps} micro steps of the full config-{args.config} network "
+                                          f"from t = {args.settle_ms:g} ms (after an untimed settle)"}
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()

@@ -259,7 +259,7 @@ class ShardedRun:
         device_ms = 0.0
         while done < steps:
             k = min(self.window, steps - done)
-            result = self.state.run_steps(k, list(records), True)
+            result = self.state.run_steps(k, records, True)
             device_ms += result.device_ms
             self.launches += self.state.run_stats().launches
             if start is None:

@@ -767,10 +767,12 @@ extern "C" {
 
 /* Initialize from the layout (and regions, if `macro` is given) and run `steps` micro
  * steps.  trace is [(steps+1) x nrec] sample-major; spikes sorted by (time, sid);
- * macro_trace is [(steps / steps per macro step + 1) x regions] region outputs. */
+ * macro_trace is [(steps / steps per macro step + 1) x regions] region outputs; run_ms
+ * is the wall time of steps timed_from .. steps-1 (a settle period before it is untimed). */
 int oracle_run_macro(const MindLayout *layout, const MindMacroLayout *macro, int64_t steps, const MindRecord *records,
                      int32_t nrec, int32_t threads, double *trace, double *spike_t, int64_t *spike_sid, int64_t cap,
-                     int64_t *nspikes, double *macro_trace, double *run_ms, char *message, int32_t message_len) {
+                     int64_t *nspikes, double *macro_trace, double *run_ms, char *message, int32_t message_len,
+                     int64_t timed_from) {
     Oracle o;
     ThreadPool pool(threads);
     o.pool = &pool;
@@ -824,6 +826,7 @@ int oracle_run_macro(const MindLayout *layout, const MindMacroLayout *macro, int
     if (!status) {
         if (nrec) record(0);
         for (int64_t s = 0; s < steps && !status; ++s) {
+            if (s == timed_from) t0 = std::chrono::steady_clock::now();   // steps before it are not timed
             status = o.advance_step();
             if (status) break;
             if (nrec) record(s + 1);
@@ -866,7 +869,7 @@ int oracle_run(const MindLayout *layout, int64_t steps, const MindRecord *record
                int32_t threads, double *trace, double *spike_t, int64_t *spike_sid, int64_t cap,
                int64_t *nspikes, double *run_ms, char *message, int32_t message_len) {
     return oracle_run_macro(layout, nullptr, steps, records, nrec, threads, trace, spike_t, spike_sid, cap, nspikes,
-                            nullptr, run_ms, message, message_len);
+                            nullptr, run_ms, message, message_len, 0);
 }
 
 }  // extern "C"

@@ -42,6 +42,7 @@ def _load():
             ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
             ctypes.POINTER(ctypes.c_int64), ctypes.c_int64, ctypes.POINTER(ctypes.c_int64),
             ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), ctypes.c_char_p, ctypes.c_int32,
+            ctypes.c_int64,
         ]
         lib.oracle_region_input_count.restype = ctypes.c_int32
         lib.oracle_region_input_count.argtypes = [ctypes.c_uint64, ctypes.c_int64, ctypes.c_int64, ctypes.c_double]
@@ -112,11 +113,11 @@ class OracleResult:
 
 
 def run(layout, steps: int, record_nodes=(), threads: int = 0, spike_cap: int = 1 << 22, macro=None,
-        records=None) -> OracleResult:
+        records=None, timed_from: int = 0) -> OracleResult:
     """Initialize the layout (and the regions of `macro`, a MacroModel) on the CPU and advance
     `steps` micro steps; with regions, `macro_trace` holds out(k) for k = 0 .. steps / (dt_macro/dt).
     `threads` worker threads (0: every host core) share the cells of each step; the result
-    does not depend on their number.
+    does not depend on their number.  `run_ms` times steps timed_from .. steps-1.
     `records` (objects with kind, node, group, row, field, such as RecordSpec) replaces
     `record_nodes` (voltages of 1-based nodes) when given."""
     import sys
@@ -156,7 +157,7 @@ def run(layout, steps: int, record_nodes=(), threads: int = 0, spike_cap: int = 
         spike_t.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
         spike_sid.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), spike_cap, ctypes.byref(count),
         macro_trace.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if macro_trace is not None else None,
-        ctypes.byref(ms), message, 256)
+        ctypes.byref(ms), message, 256, int(timed_from))
     n = min(count.value, spike_cap)
     result = OracleResult(status, message.value.decode(), trace[:, :len(nodes)],
                           spike_t[:n].copy(), spike_sid[:n].copy(), ms.value)

@@ -141,3 +141,52 @@ def big_and_small_cells(big_compartments=8000, n_small=3, synapses=12, seed=5):
     M.add_pointprocesses(model, mb.builtin("IClamp"), np.array([1, 2]), "soma", np.full(2, 0.5),
                          {"del": 2.0, "dur": 30.0, "amp": 0.8})
     return model
+
+
+def dhs_order(layout, lanes=32):
+    """A node order of the kind MIND.jl's DHS planner hands the runtime
+    (src/model/micro/model.jl:906-1077): each cell's nodes in elimination order -- reverse
+    breadth-first, children before their parent -- and the cells of each group of `lanes`
+    interleaved round by round, largest cell first.  Returns the old 1-based node of every
+    new position (0-based array)."""
+    parent = np.asarray(layout.parent, dtype=np.int64)
+    n = len(parent)
+    children = [[] for _ in range(n + 1)]
+    for i in range(n):
+        children[parent[i]].append(i + 1)
+    cells = []
+    for root in children[0]:
+        bfs = [root]
+        k = 0
+        while k < len(bfs):
+            bfs.extend(children[bfs[k]])
+            k += 1
+        cells.append(bfs[::-1])
+    order = []
+    for g in range(0, len(cells), lanes):
+        group = sorted(cells[g:g + lanes], key=len, reverse=True)
+        for r in range(len(group[0])):
+            order.extend(c[r] for c in group if r < len(c))
+    return np.asarray(order, dtype=np.int64)
+
+
+def permute_layout(layout, order):
+    """The same network with node new = position of old in `order` (1-based): parents,
+    node arrays, mechanism nodes and detector nodes renumbered; rows, points and edges kept."""
+    import dataclasses
+
+    new_of = np.zeros(len(order) + 1, dtype=np.int64)
+    new_of[order] = np.arange(1, len(order) + 1)
+    idx = order - 1
+    parent = np.asarray(layout.parent, dtype=np.int64)[idx]
+    groups = []
+    for g in layout.groups:
+        nodes = np.asarray(g.nodes, dtype=np.int64)
+        renumbered = np.where(nodes > 0, new_of[nodes], 0).astype(np.int32)
+        groups.append(dataclasses.replace(g, nodes=renumbered))
+    src = np.asarray(layout.source_nodes, dtype=np.int64)
+    return dataclasses.replace(
+        layout, parent=new_of[parent].astype(np.int32), voltage=np.asarray(layout.voltage)[idx],
+        area=np.asarray(layout.area)[idx], capacitance=np.asarray(layout.capacitance)[idx],
+        axial=np.asarray(layout.axial)[idx], axial_diagonal=np.asarray(layout.axial_diagonal)[idx],
+        groups=groups, source_nodes=np.where(src > 0, new_of[src], 0).astype(np.int32), _keep=[]), new_of
