@@ -15,7 +15,8 @@
  *   - Events live in a ring of delivery bins (bin m = the events NEURON's two
  *     half-step deliveries hand to step m's currents, i.e. event times in
  *     ((m-1) dt + dt/2, m dt + dt/2]).  Before a window, the bins of the
- *     window are moved into per-cell inboxes; the cell sorts its inbox by
+ *     window are moved into a per-window CSR of per-cell inboxes (count, scan,
+ *     fill: any number of events per cell); the cell sorts its inbox by
  *     (bin, target, time, edge) and applies it in that order, which is the
  *     heap order of the reference (src/runtime/utils/events.jl:7-62) for every
  *     target.
@@ -196,9 +197,17 @@ struct Params {
     int32_t *ring_count;
     int32_t ring_slots;
     int32_t ring_cap;
+    // the window's events by cell, a CSR rebuilt every window: cell c's events are
+    // inbox[inbox_start[c] .. inbox_start[c+1]); a cell stages up to inbox_cap of them in
+    // shared memory and sorts more in place in HBM (inbox_order), so no cell has a limit
+    // of its own -- only the window's total (inbox_total) and each delivery bin (ring_cap)
     InboxEvent *inbox;
-    int32_t *inbox_count;
-    int32_t inbox_cap;
+    int32_t *inbox_order;          // sorted order of a cell's events when they are not staged
+    int32_t *inbox_count;          // [ncells] events per cell (first pass), zeroed by the cell's window
+    int32_t *inbox_fill;           // [ncells] events placed (second pass), zeroed by the cell's window
+    int32_t *inbox_start;          // [ncells+1] exclusive prefix sum of inbox_count
+    int32_t inbox_cap;             // events staged in shared memory per cell
+    int32_t inbox_total;           // capacity of inbox and inbox_order
     const double *edge_weight;
     const double *edge_delay;
     const int32_t *edge_target;    // 0-based point

@@ -338,7 +338,57 @@ __global__ void mechanism_init_kernel(const Params P, int32_t g) {
     }
 }
 
-/* Moves bins n0 .. n0+W-1 from the ring into per-cell inboxes. */
+/* First pass of the window's inbox: events per cell in bins n0 .. n0+W-1 (grid y = bin). */
+__global__ void inbox_count_kernel(const Params P, int64_t n0) {
+    const int64_t bin = n0 + blockIdx.y;
+    const int32_t slot = (int32_t)(bin % P.ring_slots);
+    const int32_t count = min(P.ring_count[slot], P.ring_cap);
+    const RingEvent *events = P.ring + (int64_t)slot * P.ring_cap;
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
+        atomicAdd(&P.inbox_count[P.point_cell[events[i].point]], 1);
+}
+
+/* Exclusive prefix sum of the per-cell counts into inbox_start[0 .. ncells], one block of
+ * kScanThreads threads, each summing a contiguous run of cells.  A window whose events
+ * exceed the inbox raises status 3 (its cells then read no events). */
+constexpr int kScanThreads = 1024;
+__global__ void __launch_bounds__(kScanThreads) inbox_scan_kernel(const Params P) {
+    __shared__ int32_t warp_total[kScanThreads / 32];
+    const int32_t n = P.ncells;
+    const int32_t per = (n + kScanThreads - 1) / kScanThreads;
+    const int32_t lo = min(n, (int32_t)threadIdx.x * per), hi = min(n, lo + per);
+    int32_t local = 0;
+    for (int32_t i = lo; i < hi; ++i) local += P.inbox_count[i];
+    const int32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int32_t x = local;   // inclusive scan within the warp
+    for (int32_t off = 1; off < 32; off <<= 1) {
+        const int32_t y = __shfl_up_sync(0xffffffffu, x, off);
+        if (lane >= off) x += y;
+    }
+    if (lane == 31) warp_total[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        int32_t w = warp_total[lane];   // kScanThreads / 32 == 32 warps
+        for (int32_t off = 1; off < 32; off <<= 1) {
+            const int32_t y = __shfl_up_sync(0xffffffffu, w, off);
+            if (lane >= off) w += y;
+        }
+        warp_total[lane] = w;
+    }
+    __syncthreads();
+    int32_t base = (warp > 0 ? warp_total[warp - 1] : 0) + x - local;
+    for (int32_t i = lo; i < hi; ++i) {
+        P.inbox_start[i] = base;
+        base += P.inbox_count[i];
+    }
+    if (threadIdx.x == kScanThreads - 1) {
+        const int32_t total = warp_total[31];
+        P.inbox_start[n] = total;
+        if (total > P.inbox_total) raise_error(P.error, MIND_ECAPACITY);
+    }
+}
+
+/* Second pass: moves bins n0 .. n0+W-1 from the ring into the cells' inbox slices. */
 __global__ void bucket_kernel(const Params P, int64_t n0) {
     if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) *P.win_spike_count = 0;
     const int64_t bin = n0 + blockIdx.y;
@@ -349,14 +399,14 @@ __global__ void bucket_kernel(const Params P, int64_t n0) {
     for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
         RingEvent e = events[i];
         int32_t cell = P.point_cell[e.point];
-        int32_t pos = atomicAdd(&P.inbox_count[cell], 1);
-        if (pos < P.inbox_cap) {
+        const int64_t idx = (int64_t)P.inbox_start[cell] + atomicAdd(&P.inbox_fill[cell], 1);
+        if (idx < P.inbox_total) {
             InboxEvent x;
             x.time = e.time;
             x.edge = e.edge;
             x.point = e.point;
             x.bin = bin;
-            P.inbox[(int64_t)cell * P.inbox_cap + pos] = x;
+            P.inbox[idx] = x;
         }
     }
 }
@@ -384,6 +434,22 @@ __device__ __forceinline__ bool event_before(const InboxEvent &x, const InboxEve
     if (x.point != y.point) return x.point < y.point;
     if (x.time != y.time) return x.time < y.time;
     return x.edge < y.edge;
+}
+
+/* order[rank] = k for the m events ev[0..m) sorted by event_before, ties by index: each thread
+ * ranks its events against all others.  ev and order are the staged copies in shared memory,
+ * or the cell's inbox slice and order slice in HBM when its events exceed the staging. */
+template <int NT>
+__device__ __forceinline__ void sort_events(const InboxEvent *ev, int32_t m, int32_t *order) {
+    for (int32_t k = threadIdx.x; k < m; k += NT) {
+        int32_t rank = 0;
+        const InboxEvent mine = ev[k];
+        for (int32_t j = 0; j < m; ++j) {
+            const InboxEvent other = ev[j];
+            if (event_before(other, mine) || (j < k && !event_before(mine, other))) ++rank;
+        }
+        order[rank] = k;
+    }
 }
 
 /* One mechanism group of the resident cell: staged state in shared memory, the rest in HBM. */
@@ -620,7 +686,6 @@ template <bool MIXED, int NT, bool GLOBAL_IMAGE = false>
 __global__ void __launch_bounds__(NT, NT == kCellThreads ? 5 : 10) window_kernel(const Params P, const int32_t *cells,
                                                                                int64_t n0, int32_t W) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ int32_t s_nev;
     __shared__ StagedGroup sg[kMaxGroups];
     const int32_t c = cells[blockIdx.x];
     const int32_t tid = threadIdx.x;
@@ -695,36 +760,32 @@ __global__ void __launch_bounds__(NT, NT == kCellThreads ? 5 : 10) window_kernel
     // ---- stage the cell ----
     if (blockIdx.x == 0)
         for (int32_t k = tid; k < W; k += T) P.ring_count[(n0 + k) % P.ring_slots] = 0;
+    // The cell's events of this window: its slice of the window's inbox.  Up to inbox_cap of
+    // them are staged and sorted in shared memory; more are sorted in place in HBM.
+    const int32_t ib = P.inbox_start[c];
+    int32_t nev = P.inbox_start[c + 1] - ib;
+    if (ib < 0 || nev < 0 || (int64_t)ib + nev > P.inbox_total) nev = 0;   // window overflow: status 3 raised
+    const bool staged_ev = nev <= P.inbox_cap;
+    const InboxEvent *gev = P.inbox + (staged_ev ? 0 : ib);
+    int32_t *gorder = P.inbox_order + (staged_ev ? 0 : ib);
+    const InboxEvent *ev = staged_ev ? sev : gev;
+    int32_t *evorder = staged_ev ? sorder : gorder;
+    if (tid == 0) {   // the next window counts afresh
+        P.inbox_count[c] = 0;
+        P.inbox_fill[c] = 0;
+    }
+    if (staged_ev)
+        for (int32_t k = tid; k < nev; k += T) sev[k] = P.inbox[(int64_t)ib + k];
     if (P.cell_mode && P.cell_mode[c]) {
         // A cell the surrogate stands in for: its membrane is not simulated; its window's
         // events only add their NetCon weights to its drive, per rate bin and synapse group,
         // in the canonical event order (so the sums, and the run, are reproducible).
-        if (tid == 0) {
-            int32_t count = P.inbox_count[c];
-            if (count > P.inbox_cap) {
-                raise_error(P.error, MIND_ECAPACITY);
-                count = P.inbox_cap;
-            }
-            s_nev = count;
-            P.inbox_count[c] = 0;
-        }
         __syncthreads();
-        const int32_t m = s_nev;
-        for (int32_t k = tid; k < m; k += T) sev[k] = P.inbox[(int64_t)c * P.inbox_cap + k];
-        __syncthreads();
-        for (int32_t k = tid; k < m; k += T) {
-            int32_t rank = 0;
-            const InboxEvent mine = sev[k];
-            for (int32_t j = 0; j < m; ++j) {
-                const InboxEvent other = sev[j];
-                if (event_before(other, mine) || (j < k && !event_before(mine, other))) ++rank;
-            }
-            sorder[rank] = k;
-        }
+        sort_events<T>(ev, nev, evorder);
         __syncthreads();
         if (tid == 0)
-            for (int32_t k = 0; k < m; ++k) {
-                const InboxEvent e = sev[sorder[k]];
+            for (int32_t k = 0; k < nev; ++k) {
+                const InboxEvent e = ev[evorder[k]];
                 if (e.edge < 0) continue;
                 const int32_t g = P.point_group[e.point];
                 const int32_t row = P.point_row[e.point] - P.groups[g].row_off[c];
@@ -747,15 +808,6 @@ __global__ void __launch_bounds__(NT, NT == kCellThreads ? 5 : 10) window_kernel
     for (int32_t k = tid; k < nkids; k += T) ckids[k] = P.chain_kids[kb + k];
     for (int32_t k = tid; k <= nlev; k += T) lvc[k] = P.level_chain[lv0 + k];
     for (int32_t k = tid; k < P.ngroups * (O + 1); k += T) spart[k] = P.part[(int64_t)c * P.ngroups * (O + 1) + k];
-    if (tid == 0) {
-        int32_t count = P.inbox_count[c];
-        if (count > P.inbox_cap) {
-            raise_error(P.error, MIND_ECAPACITY);
-            count = P.inbox_cap;
-        }
-        s_nev = count;
-        P.inbox_count[c] = 0;
-    }
     __syncthreads();
     for (int32_t k = tid; k < nch; k += T)
         for (int32_t i = ctop[k]; i < ctop[k] + clen[k]; ++i) chain_of[i] = (int16_t)k;
@@ -780,8 +832,6 @@ __global__ void __launch_bounds__(NT, NT == kCellThreads ? 5 : 10) window_kernel
             S.node[r] = (int32_t)(G.node[row] - nb);
         }
     }
-    const int32_t nev = s_nev;
-    for (int32_t k = tid; k < nev; k += T) sev[k] = P.inbox[(int64_t)c * P.inbox_cap + k];
     // Detectors stay in registers for the window (at most one per lane; checked at mind_create).
     const int32_t d0 = P.det_off[c], d1 = P.det_off[c + 1];
     int32_t my_det = -1, my_src = 0;
@@ -794,18 +844,11 @@ __global__ void __launch_bounds__(NT, NT == kCellThreads ? 5 : 10) window_kernel
         my_above = P.above[my_src] != 0;
     }
     __syncthreads();
-    for (int32_t k = tid; k < nev; k += T) {
-        int32_t rank = 0;
-        const InboxEvent mine = sev[k];
-        for (int32_t j = 0; j < nev; ++j) {
-            const InboxEvent other = sev[j];
-            if (event_before(other, mine) || (j < k && !event_before(mine, other))) ++rank;
-        }
-        sorder[rank] = k;
-    }
+    sort_events<T>(ev, nev, evorder);
     __syncthreads();
-    // Resolve each event's target to (group, staged row) and its increment once per window.
-    for (int32_t k = tid; k < nev; k += T) {
+    // Resolve each staged event's target to (group, staged row) and its increment once per
+    // window (events read from HBM are resolved as they are applied, with the same operations).
+    for (int32_t k = tid; k < (staged_ev ? nev : 0); k += T) {
         InboxEvent &e = sev[k];
         const int32_t g = P.point_group[e.point];
         const int32_t drow = P.point_row[e.point];
@@ -841,17 +884,32 @@ __global__ void __launch_bounds__(NT, NT == kCellThreads ? 5 : 10) window_kernel
         // 2. Deliver this step's bin in (target, time, edge) order.
         if (tid == 0) {
             while (cursor < nev) {
-                const int32_t k = sorder[cursor];
-                const InboxEvent &e = sev[k];
+                InboxEvent e;
+                int32_t g, row;
+                double inc;
+                if (staged_ev) {
+                    const int32_t k = sorder[cursor];
+                    e = sev[k];
+                    g = e.point >> 24;
+                    row = e.point & 0xffffff;
+                    inc = sw[k];
+                } else {
+                    e = gev[gorder[cursor]];
+                    g = P.point_group[e.point];
+                    const int32_t drow = P.point_row[e.point];
+                    row = drow - sg[g].r0;
+                    const double w = e.edge >= 0 ? P.edge_weight[e.edge] : 0.0;
+                    inc = P.groups[g].kind == MIND_MECH_EXP2SYN ? w * P.groups[g].f[E2_FACTOR][drow] : w;
+                }
                 if (e.bin > step) break;
                 if (e.bin < step) raise_error(P.error, MIND_ESELFEVENT);
-                apply_event(sg[e.point >> 24], e.point & 0xffffff, sw[k]);
+                apply_event(sg[g], row, inc);
                 if (P.drive && e.edge >= 0) {
                     // synaptic drive for the surrogate's training data: NetCon weight by
                     // (run bin, cell, synapse row mod 32)
                     const int64_t b = (step - P.run_start) / P.drive_bin_steps;
                     if (b < P.drive_bins)
-                        P.drive[(b * P.ncells + c) * 32 + ((e.point & 0xffffff) & 31)] += (float)P.edge_weight[e.edge];
+                        P.drive[(b * P.ncells + c) * 32 + (row & 31)] += (float)P.edge_weight[e.edge];
                 }
                 ++cursor;
             }

@@ -700,9 +700,16 @@ int create(const MindLayout *L, MindHandle *h) {
     P.ring_cap = (int32_t)ring_cap;
     P.ring = h->alloc<RingEvent>((size_t)P.ring_slots * P.ring_cap);
     P.ring_count = h->alloc<int32_t>(P.ring_slots);
+    // Inbox: the events of one window by cell (a CSR rebuilt per window).  A window holds at
+    // most kMaxWindow bins of at most ring_cap events; each cell stages up to 64 of its events
+    // in shared memory and sorts any more in HBM.
     P.inbox_cap = 64;
-    P.inbox = h->alloc<InboxEvent>((size_t)ncells * P.inbox_cap);
+    P.inbox_total = (int32_t)std::min<int64_t>((int64_t)kMaxWindow * P.ring_cap, INT32_MAX / 2);
+    P.inbox = h->alloc<InboxEvent>((size_t)P.inbox_total);
+    P.inbox_order = h->alloc<int32_t>((size_t)P.inbox_total);
     P.inbox_count = h->alloc<int32_t>(ncells);
+    P.inbox_fill = h->alloc<int32_t>(ncells);
+    P.inbox_start = h->alloc<int32_t>((size_t)ncells + 1);
     P.edge_weight = h->upload(edge_weight);
     P.edge_delay = h->upload(edge_delay);
     P.edge_target = h->upload(edge_target);
@@ -822,7 +829,7 @@ int check_device_error(MindHandle *h) {
     CUDA_TRY(h, cudaMemcpyAsync(&code, h->P.error, sizeof code, cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     if (code == 0) return MIND_OK;
-    const char *what = code == MIND_ECAPACITY   ? "event ring, cell inbox or spike record capacity exhausted"
+    const char *what = code == MIND_ECAPACITY   ? "event ring, window inbox or spike record capacity exhausted"
                        : code == MIND_ESELFEVENT ? "invalid self-event delay or an event behind its delivery step"
                        : code == MIND_ESINGULAR  ? "singular or non-finite cable system"
                        : code == MIND_ENONFINITE ? "non-finite numerical state"
@@ -1059,8 +1066,10 @@ int advance(MindHandle *h, int64_t steps, bool record_spikes) {
                 h->injected.erase(h->injected.begin(), h->injected.begin() + due);
             }
         }
+        inbox_count_kernel<<<dim3(64, W), kThreads, 0, h->stream>>>(P, n0);
+        inbox_scan_kernel<<<1, kScanThreads, 0, h->stream>>>(P);
         bucket_kernel<<<dim3(64, W), kThreads, 0, h->stream>>>(P, n0);
-        ++st.launches;
+        st.launches += 3;
         // Size bins run side by side on their own streams so SMs mix CTAs of
         // different shared-memory images; the main stream joins them.
         if (h->profiling) cudaEventRecord(prof_event(), h->stream);
@@ -1261,6 +1270,7 @@ int mind_initialize(MindHandle *h) {
     CUDA_TRY(h, cudaMemsetAsync(P.above, 0, std::max<int64_t>(1, h->n_sources), h->stream));
     CUDA_TRY(h, cudaMemsetAsync(P.ring_count, 0, P.ring_slots * sizeof(int32_t), h->stream));
     CUDA_TRY(h, cudaMemsetAsync(P.inbox_count, 0, std::max(1, h->ncells) * sizeof(int32_t), h->stream));
+    CUDA_TRY(h, cudaMemsetAsync(P.inbox_fill, 0, std::max(1, h->ncells) * sizeof(int32_t), h->stream));
     CUDA_TRY(h, cudaMemsetAsync(P.win_spike_count, 0, sizeof(int32_t), h->stream));
     int status = upload_group_state(h);
     if (status) return status;

@@ -190,3 +190,36 @@ def permute_layout(layout, order):
         area=np.asarray(layout.area)[idx], capacitance=np.asarray(layout.capacitance)[idx],
         axial=np.asarray(layout.axial)[idx], axial_diagonal=np.asarray(layout.axial_diagonal)[idx],
         groups=groups, source_nodes=np.where(src > 0, new_of[src], 0).astype(np.int32), _keep=[]), new_of
+
+
+def burst_onto_one_cell(n_events=200, n_cells=3, seed=4):
+    """One NetStim that fires once (t = 2 ms, no noise) with `n_events` NetCons onto the
+    Exp2Syn of cell 1, delays U[0.5, 1.0] ms: every event lands in one window of cell 1's
+    inbox.  The other cells get a few ordinary synapses, so their inboxes stay small."""
+    rng = np.random.default_rng(seed)
+    model = M.MicroModel(celsius=6.3)
+    cells = []
+    for c in range(n_cells):
+        soma = mb.Section("soma", label="soma", length=20.0, diameter=20.0, nseg=1)
+        secs = networks._binary_tree(rng, 60, soma)
+        cell = M.add_population(model, secs, 1, voltage=-65.0)[0]
+        M.insert(cell, mb.builtin("hh"), sections="soma")
+        M.insert(cell, mb.builtin("pas"), sections="dend", params={"g": 1e-4, "e": -65.0})
+        M.register_spike_source(cell, threshold=-10.0)
+        cells.append((cell, secs))
+    counts = [n_events] + [8] * (n_cells - 1)
+    owners = np.repeat(np.arange(1, n_cells + 1), counts)
+    names, xs = [], []
+    for (cell, secs), k in zip(cells, counts):
+        nm, x = networks._dendritic_sites(rng, secs, k)
+        names += nm
+        xs.append(x)
+    n = int(sum(counts))
+    first = M.add_pointprocesses(model, mb.builtin("Exp2Syn"), owners, names, np.concatenate(xs),
+                                 {"tau1": 0.5, "tau2": 5.0, "e": 0.0})
+    stim = M.add_pointprocesses(model, mb.builtin("NetStim"), np.zeros(1, np.int64), "none", np.zeros(1),
+                                {"interval": 10.0, "number": 1.0, "start": 2.0, "noise": 0.0})
+    source = M.register_point_sources(model, np.array([stim]))
+    M.connect_many(model, np.repeat(source, n), np.arange(first, first + n),
+                   rng.lognormal(math.log(0.05), 0.3, n) / 1000.0, rng.uniform(0.5, 1.0, n))
+    return model
