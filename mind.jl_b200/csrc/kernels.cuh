@@ -683,7 +683,7 @@ __device__ __forceinline__ void hines_mixed(double *sd, double *sr, const double
  * on the dependency chain, the next node's operands being loaded ahead.
  */
 template <bool MIXED, int NT, bool GLOBAL_IMAGE = false>
-__global__ void __launch_bounds__(NT, NT == kCellThreads ? 5 : 10) window_kernel(const Params P, const int32_t *cells,
+__global__ void __launch_bounds__(NT, NT == kCellThreads ? 5 : NT == kCellThreads / 2 ? 10 : 16) window_kernel(const Params P, const int32_t *cells,
                                                                                int64_t n0, int32_t W) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ StagedGroup sg[kMaxGroups];

@@ -317,6 +317,19 @@ int launch_grid(int64_t work) {
     return (int)blocks;
 }
 
+/* The window kernel's launch shapes: 128 threads per cell (kCellThreads), 64, or one warp. */
+template <int NT>
+cudaError_t set_window_smem(int bytes) {
+    cudaError_t e = cudaFuncSetAttribute(window_kernel<false, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(window_kernel<true, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    return e;
+}
+
+bool valid_cell_threads(int32_t threads) {
+    return threads == kCellThreads || threads == kCellThreads / 2 || threads == kCellThreads / 4;
+}
+
 int create(const MindLayout *L, MindHandle *h) {
     if (!L) return fail(h, MIND_EARG, "null layout");
     if (L->abi_version != MIND_ABI_VERSION) return fail(h, MIND_ELAYOUT, "ABI version mismatch");
@@ -789,14 +802,9 @@ int create(const MindLayout *L, MindHandle *h) {
     h->bin_cells = h->upload(bin_cells);
     h->smem_bytes = worst_smem;
     const int smem_attr = (int)std::max<size_t>(worst_smem, 1);
-    CUDA_TRY(h, cudaFuncSetAttribute(window_kernel<false, kCellThreads>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr));
-    CUDA_TRY(h, cudaFuncSetAttribute(window_kernel<true, kCellThreads>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr));
-    CUDA_TRY(h, cudaFuncSetAttribute(window_kernel<false, kCellThreads / 2>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr));
-    CUDA_TRY(h, cudaFuncSetAttribute(window_kernel<true, kCellThreads / 2>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr));
+    CUDA_TRY(h, set_window_smem<kCellThreads>(smem_attr));
+    CUDA_TRY(h, set_window_smem<kCellThreads / 2>(smem_attr));
+    CUDA_TRY(h, set_window_smem<kCellThreads / 4>(smem_attr));
     CUDA_TRY(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     CUDA_TRY(h, cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming));
     for (size_t b = 0; b < h->bins.size(); ++b) {
@@ -981,6 +989,21 @@ int set_records(MindHandle *h, const MindRecord *records, int32_t nrec, int64_t 
     return MIND_OK;
 }
 
+/* One size bin's window-kernel launch in its chosen shape. */
+template <bool MIXED>
+void launch_window(const MindHandle::Bin &bin, cudaStream_t s, const Params &P, const int32_t *cells, int64_t n0,
+                   int32_t W) {
+    constexpr int T = kCellThreads;
+    if (bin.global_image)
+        window_kernel<MIXED, T, true><<<bin.count, T, 0, s>>>(P, cells, n0, W);
+    else if (bin.threads == T)
+        window_kernel<MIXED, T><<<bin.count, T, bin.smem_bytes, s>>>(P, cells, n0, W);
+    else if (bin.threads == T / 2)
+        window_kernel<MIXED, T / 2><<<bin.count, T / 2, bin.smem_bytes, s>>>(P, cells, n0, W);
+    else
+        window_kernel<MIXED, T / 4><<<bin.count, T / 4, bin.smem_bytes, s>>>(P, cells, n0, W);
+}
+
 int advance(MindHandle *h, int64_t steps, bool record_spikes) {
     Params &P = h->P;
     P.record_spikes = record_spikes ? 1 : 0;
@@ -1079,24 +1102,10 @@ int advance(MindHandle *h, int64_t steps, bool record_spikes) {
             cudaStream_t s = h->bin_streams[b];
             cudaStreamWaitEvent(s, h->fork, 0);
             const int32_t *cells = h->bin_cells + bin.first;
-            const bool mixed = h->precision == MIND_MIXED;
-            if (bin.global_image) {
-                if (mixed)
-                    window_kernel<true, kCellThreads, true><<<bin.count, kCellThreads, 0, s>>>(P, cells, n0, W);
-                else
-                    window_kernel<false, kCellThreads, true><<<bin.count, kCellThreads, 0, s>>>(P, cells, n0, W);
-            } else if (bin.threads == kCellThreads) {
-                if (mixed)
-                    window_kernel<true, kCellThreads><<<bin.count, kCellThreads, bin.smem_bytes, s>>>(P, cells, n0, W);
-                else
-                    window_kernel<false, kCellThreads><<<bin.count, kCellThreads, bin.smem_bytes, s>>>(P, cells, n0, W);
-            } else {
-                constexpr int half = kCellThreads / 2;
-                if (mixed)
-                    window_kernel<true, half><<<bin.count, half, bin.smem_bytes, s>>>(P, cells, n0, W);
-                else
-                    window_kernel<false, half><<<bin.count, half, bin.smem_bytes, s>>>(P, cells, n0, W);
-            }
+            if (h->precision == MIND_MIXED)
+                launch_window<true>(bin, s, P, cells, n0, W);
+            else
+                launch_window<false>(bin, s, P, cells, n0, W);
             cudaEventRecord(h->bin_done[b], s);
             cudaStreamWaitEvent(h->stream, h->bin_done[b], 0);
             ++st.launches;
@@ -1678,21 +1687,25 @@ int mind_autotune(MindHandle *h, int32_t windows) {
     double best = 0.0;
     int status = trial_ms(h, windows, &best);
     if (status) return status;
-    const int32_t half = kCellThreads / 2;
+    const int32_t shapes[3] = {kCellThreads, kCellThreads / 2, kCellThreads / 4};
     for (auto &bin : h->bins) {
-        if (bin.max_detectors > half || bin.global_image) continue;   // one detector per thread; HBM images: 128
+        if (bin.global_image) continue;   // HBM images run 128 threads
         const int32_t keep = bin.threads;
-        bin.threads = keep == kCellThreads ? half : kCellThreads;
-        double ms = 0.0;
-        status = trial_ms(h, windows, &ms);
-        if (status) {
-            bin.threads = keep;
-            return status;
+        for (int32_t t : shapes) {
+            if (t == keep || t < bin.max_detectors) continue;   // one detector per thread
+            const int32_t before = bin.threads;
+            bin.threads = t;
+            double ms = 0.0;
+            status = trial_ms(h, windows, &ms);
+            if (status) {
+                bin.threads = keep;
+                return status;
+            }
+            if (ms < 0.98 * best)
+                best = ms;
+            else
+                bin.threads = before;
         }
-        if (ms < 0.98 * best)
-            best = ms;
-        else
-            bin.threads = keep;
     }
     return mind_initialize(h);
 }
@@ -1707,8 +1720,8 @@ int mind_bin_threads(const MindHandle *h, int32_t *threads, int32_t cap, int32_t
 int mind_set_bin_threads(MindHandle *h, const int32_t *threads, int32_t n_bins) {
     if (!h || !threads || n_bins != (int32_t)h->bins.size()) return MIND_EARG;
     for (int32_t b = 0; b < n_bins; ++b) {
-        if (threads[b] != kCellThreads && threads[b] != kCellThreads / 2)
-            return fail(h, MIND_EARG, "a bin runs 128 or 64 threads per cell");
+        if (!valid_cell_threads(threads[b]))
+            return fail(h, MIND_EARG, "a bin runs 128, 64 or 32 threads per cell");
         if (threads[b] < h->bins[b].max_detectors)
             return fail(h, MIND_EARG, "a bin's cells have more detectors than its CTA has threads");
         if (h->bins[b].global_image && threads[b] != kCellThreads)
