@@ -72,7 +72,11 @@ enum {
     MIND_MECH_EXP2SYN = 4,  /* mod/Exp2Syn.mod  point    */
     MIND_MECH_NETSTIM = 5,  /* mod/NetStim.mod  artificial */
     MIND_MECH_ICLAMP = 6,   /* mod/IClamp.mod   point (electrode current) */
-    MIND_MECH_ALPHASYN = 7  /* mod/AlphaSynapse.mod point: g = gmax alpha((t-onset)/tau), i = g (v-e) */
+    MIND_MECH_ALPHASYN = 7, /* mod/AlphaSynapse.mod point: g = gmax alpha((t-onset)/tau), i = g (v-e) */
+    /* MIND_MECH_GENERATED + k: the k-th mechanism whose CUDA C was emitted from a MOD file
+     * (BREAKPOINT, DERIVATIVE by cnexp, PROCEDURE by after_cvode, NET_RECEIVE, INITIAL) and
+     * compiled into this library; mind_mechanism_info lists them with their fields. */
+    MIND_MECH_GENERATED = 64
 };
 
 /*
@@ -343,6 +347,31 @@ int mind_set_surrogate_cells(MindHandle *h, const uint8_t *surrogate_cells);
  * batches drawn with replacement; losses[k] = the batch loss before step k (may be NULL). */
 int mind_mlp_set_data(MindMlp *mlp, const float *x, const float *y, int64_t n);
 int mind_mlp_train(MindMlp *mlp, int32_t steps, int32_t batch, float lr, float *losses, float *ms);
+
+/*
+ * Mechanisms emitted from MOD files and compiled into this library (kinds
+ * MIND_MECH_GENERATED + index): the seam where MIND.jl's compile_mod/load_mod/builtin
+ * hand the runtime a CompiledMechanism (src/compiler/frontend.jl:15-110,
+ * src/compiler/ir.jl:340-356).  Here the CUDA C a MOD file lowers to (mind_b200.nmodl) is
+ * compiled with the library by nvcc, so a host selects a mechanism by name and passes its
+ * kind code and fields in MindLayout.  Host-side calls: no device work.
+ */
+typedef struct MindMechanismInfo {
+    const char *name;                  /* the MOD's SUFFIX or POINT_PROCESS name */
+    int32_t kind;                      /* MIND_MECH_GENERATED + index */
+    int32_t point;                     /* 1: point process, 0: density mechanism */
+    int32_t net_receive;               /* NET_RECEIVE arity (0: the mechanism takes no events) */
+    int32_t n_fields;
+    const char *const *field_names;    /* the layout columns, in order (array fields as name[k]) */
+    const double *defaults;            /* PARAMETER defaults, 0 for STATE and ASSIGNED */
+    uint64_t digest;                   /* first 16 hex digits of the MOD source's SHA-256 */
+    const char *ion_reads;             /* "field ion" pairs (space-separated) that USEION READ fills from
+                                          the model's ion species, e.g. "ena na ek k" */
+} MindMechanismInfo;
+int mind_mechanism_count(int32_t *n);
+int mind_mechanism_info(int32_t index, MindMechanismInfo *info);
+/* The kind code of the emitted mechanism named `name`; MIND_EARG if none is compiled in. */
+int mind_mechanism_kind(const char *name, int32_t *kind);
 
 /* Message for the last non-zero status of this handle (or of mind_create when h is NULL). */
 const char *mind_last_error(const MindHandle *h);

@@ -17,7 +17,8 @@ PACKAGE = os.path.dirname(HERE)
 OUT_DIR = os.path.join(PACKAGE, "lib")
 OUTPUT = os.path.join(OUT_DIR, "libmindgpu.so")
 SOURCES = [os.path.join(HERE, "mindgpu.cu"), os.path.join(HERE, "surrogate.cu")]
-DEPENDS = SOURCES + [os.path.join(HERE, f) for f in ("device.cuh", "kernels.cuh", "macro.cuh", "mind_math.h")] + [
+DEPENDS = SOURCES + [os.path.join(HERE, f) for f in ("device.cuh", "kernels.cuh", "macro.cuh", "mind_math.h",
+                                                     "gen_runtime.cuh", "generated_mechanisms.cuh")] + [
     os.path.join(os.path.dirname(PACKAGE), "include", "mindgpu.h")]
 
 NVCC_FLAGS = [

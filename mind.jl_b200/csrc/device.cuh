@@ -32,6 +32,7 @@
 #include <cstdint>
 #include "mind_math.h"
 #include "../../include/mindgpu.h"
+#include "generated_mechanisms.cuh"
 
 namespace mind {
 
@@ -67,7 +68,17 @@ struct DevGroup {
     int32_t *seg;             // rows in the segment starting here (0 = not a segment head)
     double *f[12];            // field arrays, meaning by kind (see mindgpu.cu)
     float *s[4];              // FP32 decay factors of the synapses (mixed mode)
+    // mechanisms emitted from MOD files (kind MIND_MECH_GENERATED + gen): their fields as
+    // ncols columns of `cols` (column k of row r at cols[k * rows + r]), then one column of
+    // current scale (area * 0.01 for density mechanisms, 1 for point processes)
+    double *cols;
+    int32_t ncols;
+    int32_t gen;              // index into kGenMechanisms, -1 for the hand-written kinds
 };
+
+__host__ __device__ inline bool kind_generated(int32_t kind) {
+    return kind >= MIND_MECH_GENERATED && kind < MIND_MECH_GENERATED + kGeneratedCount;
+}
 
 /* Field slots per kind. */
 enum { HH_GNABAR, HH_GKBAR, HH_GL, HH_EL, HH_ENA, HH_EK, HH_SCALE, HH_M, HH_H, HH_N, HH_NSLOT };

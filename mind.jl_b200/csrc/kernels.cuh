@@ -301,6 +301,11 @@ __global__ void netstim_init_kernel(const Params P, uint64_t digest, const uint6
 __global__ void mechanism_init_kernel(const Params P, int32_t g) {
     const DevGroup &G = P.groups[g];
     for (int32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < G.rows; r += gridDim.x * blockDim.x) {
+        if (G.gen >= 0) {   // emitted from a MOD file: INITIAL at t = 0 on the initial voltage
+            const MindGenRow row{G.cols, G.rows, r, P.v[G.node[r]], 0.0, P.dt, P.celsius};
+            gen_initial(G.gen, row);
+            continue;
+        }
         switch (G.kind) {
             case MIND_MECH_HH: {
                 HHRates R = hh_rates(P.v[G.node[r]], P.celsius);
@@ -682,7 +687,7 @@ __device__ __forceinline__ void hines_mixed(double *sd, double *sr, const double
  * one chain per thread; along a chain only subtract -> divide -> multiply stays
  * on the dependency chain, the next node's operands being loaded ahead.
  */
-template <bool MIXED, int NT, bool GLOBAL_IMAGE = false>
+template <bool MIXED, int NT, bool GLOBAL_IMAGE = false, bool GEN = false>
 __global__ void __launch_bounds__(NT, NT == kCellThreads ? 5 : NT == kCellThreads / 2 ? 10 : 16) window_kernel(const Params P, const int32_t *cells,
                                                                                int64_t n0, int32_t W) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -903,7 +908,15 @@ __global__ void __launch_bounds__(NT, NT == kCellThreads ? 5 : NT == kCellThread
                 }
                 if (e.bin > step) break;
                 if (e.bin < step) raise_error(P.error, MIND_ESELFEVENT);
-                apply_event(sg[g], row, inc);
+                if (GEN && P.groups[g].gen >= 0) {   // emitted NET_RECEIVE, flag 0, at the event's time
+                    const DevGroup &GG = P.groups[g];
+                    const int64_t grow = (int64_t)sg[g].r0 + row;
+                    const MindGenRow gr{GG.cols, GG.rows, grow, sv[(int32_t)(GG.node[grow] - nb)], e.time, P.dt,
+                                        P.celsius};
+                    gen_receive(GG.gen, gr, inc, 0.0);
+                } else {
+                    apply_event(sg[g], row, inc);
+                }
                 if (P.drive && e.edge >= 0) {
                     // synaptic drive for the surrogate's training data: NetCon weight by
                     // (run bin, cell, synapse row mod 32)
@@ -980,6 +993,22 @@ __global__ void __launch_bounds__(NT, NT == kCellThreads ? 5 : NT == kCellThread
                         const double value = 0.0 + gs * (vv - e);
                         sr[node] = sr[node] + -1.0 * value;
                         sd[node] = sd[node] + milli_quotient<MIXED>(1.0 * (shifted - value));
+                    }
+                } else if (GEN && GG.gen >= 0) {
+                    // emitted from a MOD file: BREAKPOINT probed at v + 0.001 and at v
+                    // (src/runtime/cuda/micro.jl:427-500); the second call's writes persist
+                    const int32_t *pn = GG.node + G.r0;
+                    const double *pscale = GG.cols + (int64_t)GG.ncols * GG.rows + G.r0;
+                    for (int32_t r = lo; r < hi; ++r) {
+                        const int32_t node = (int32_t)(__ldg(pn + r) - nb);
+                        const double vv = sv[node];
+                        MindGenRow row{GG.cols, GG.rows, (int64_t)G.r0 + r, vv + 0.001, tc, P.dt, P.celsius};
+                        const double shifted = gen_current(GG.gen, row);
+                        row.v = vv;
+                        const double value = gen_current(GG.gen, row);
+                        const double scale = pscale[r];
+                        sr[node] = sr[node] - scale * value;
+                        sd[node] = sd[node] + milli_quotient<MIXED>(scale * (shifted - value));
                     }
                 } else if (G.kind == MIND_MECH_HH) {
                     for (int32_t r = lo; r < hi; ++r) {
@@ -1073,6 +1102,15 @@ __global__ void __launch_bounds__(NT, NT == kCellThreads ? 5 : NT == kCellThread
         for (int32_t g = 0; g < P.ngroups; ++g) {
             const DevGroup &GG = P.groups[g];
             const StagedGroup G = sg[g];
+            if (GEN && GG.gen >= 0) {   // emitted from a MOD file: its hoisted SOLVE statements
+                for (int32_t r = tid; r < G.rows; r += T) {
+                    const int64_t row = (int64_t)G.r0 + r;
+                    const MindGenRow gr{GG.cols, GG.rows, row, sv[(int32_t)(__ldg(GG.node + row) - nb)], t + P.dt, P.dt,
+                                        P.celsius};
+                    gen_advance(GG.gen, gr);
+                }
+                continue;
+            }
             switch (G.kind) {
                 case MIND_MECH_HH:
                     // one thread per (row, gate): m, h and n advance independently

@@ -98,6 +98,7 @@ struct MindHandle {
     std::vector<float> drive;
     int64_t drive_bins = 0;
     std::vector<double> v0_packed;
+    bool has_generated = false;              // some group runs CUDA C emitted from a MOD file
     int32_t device = -1;                     // the device current at the first allocation: state and stream live there
     int64_t n_sources = 0;
     std::vector<int64_t> source_ids;
@@ -244,6 +245,12 @@ KindSpec spec_of(int32_t kind) {
         case MIND_MECH_NETSTIM:
             return {kind, {"interval", "number", "start", "noise", "event", "on", "ispike"}, NS_NSLOT, 0};
         default:
+            if (kind_generated(kind)) {   // every field of an emitted mechanism, in column order
+                const GenMechanism &g = kGenMechanisms[kind - MIND_MECH_GENERATED];
+                KindSpec spec{kind, {}, 0, 0};
+                for (int32_t k = 0; k < g.n_fields; ++k) spec.fields.push_back(kGenFieldNames[g.first_field + k]);
+                return spec;
+            }
             return {0, {}, 0, 0};
     }
 }
@@ -295,6 +302,12 @@ int readable_slot(int32_t kind, const char *name) {
         {MIND_MECH_NETSTIM, "ispike", NS_ISPIKE},
     };
     if (!name) return -1;
+    if (kind_generated(kind)) {   // every column of an emitted mechanism is kept
+        const GenMechanism &g = kGenMechanisms[kind - MIND_MECH_GENERATED];
+        for (int32_t k = 0; k < g.n_fields; ++k)
+            if (std::strcmp(kGenFieldNames[g.first_field + k], name) == 0) return k;
+        return -1;
+    }
     for (const Entry &e : table)
         if (e.kind == kind && std::strcmp(e.name, name) == 0) return e.slot;
     return -1;
@@ -527,9 +540,12 @@ int create(const MindLayout *L, MindHandle *h) {
         init.kind = m.kind;
         init.rows = rows;
         init.digest = m.digest;
-        init.f.assign(spec.nslot, std::vector<double>(rows, 0.0));
+        const bool generated = kind_generated(m.kind);
+        const int32_t gen_cols = (int32_t)spec.fields.size();
+        // an emitted mechanism keeps every field as a column, then its current scale
+        init.f.assign(generated ? gen_cols + 1 : spec.nslot, std::vector<double>(rows, generated ? 1.0 : 0.0));
         for (size_t k = 0; k < spec.fields.size(); ++k) {
-            int slot = slot_of(m.kind, (int)k);
+            int slot = generated ? (int)k : slot_of(m.kind, (int)k);
             for (int32_t r = 0; r < rows; ++r) init.f[slot][r] = m.data[(int64_t)src[k] * m.rows + perm[r]];
         }
         std::vector<int32_t> node_dev(rows, -1), seg(rows, 1), row_off(ncells + 1, 0);
@@ -548,6 +564,12 @@ int create(const MindLayout *L, MindHandle *h) {
                     while (r + len < rows && node_dev[r + len] == node_dev[r]) ++len;
                     seg[r] = len;
                 }
+            }
+            if (generated && !kGenMechanisms[m.kind - MIND_MECH_GENERATED].point) {
+                for (int32_t r = 0; r < rows; ++r)
+                    if (seg[r] > 1) return fail(h, MIND_ELAYOUT, "density mechanism twice on one node");
+                for (int32_t r = 0; r < rows; ++r)
+                    init.f[gen_cols][r] = L->area[layout_of_packed[node_dev[r]]] * 0.01;
             }
             if ((m.kind == MIND_MECH_HH || m.kind == MIND_MECH_PAS)) {
                 for (int32_t r = 0; r < rows; ++r)
@@ -585,6 +607,10 @@ int create(const MindLayout *L, MindHandle *h) {
         for (int k = 0; k < 4; ++k) G.s[k] = nullptr;
         for (int k = 0; k < spec.nslot; ++k) G.f[k] = h->alloc<double>(rows);
         for (int k = 0; k < spec.nfloat; ++k) G.s[k] = h->alloc<float>(rows);
+        G.gen = generated ? m.kind - MIND_MECH_GENERATED : -1;
+        h->has_generated |= generated;
+        G.ncols = generated ? gen_cols : 0;
+        G.cols = generated ? h->alloc<double>((size_t)(gen_cols + 1) * (size_t)std::max(rows, 1)) : nullptr;
         h->group_init.push_back(std::move(init));
     }
 
@@ -646,8 +672,11 @@ int create(const MindLayout *L, MindHandle *h) {
             int32_t t = L->edge_targets[e];
             if (t < 1 || t > np) return fail(h, MIND_ELAYOUT, "edge target out of range");
             int32_t kind = L->mechanisms[point_group[t - 1]].kind;
-            if (kind != MIND_MECH_EXPSYN && kind != MIND_MECH_EXP2SYN)
-                return fail(h, MIND_ELAYOUT, "NetCon target must be ExpSyn or Exp2Syn in this build");
+            const bool receives = kind == MIND_MECH_EXPSYN || kind == MIND_MECH_EXP2SYN ||
+                                  (kind_generated(kind) && kGenMechanisms[kind - MIND_MECH_GENERATED].net_receive > 0);
+            if (!receives)
+                return fail(h, MIND_ELAYOUT, "NetCon target has no NET_RECEIVE on the device (ExpSyn, Exp2Syn or an "
+                                             "emitted mechanism with one)");
             double d = edge_delay[e];
             if (!(d >= 0.0) || !std::isfinite(d) || !std::isfinite(edge_weight[e]))
                 return fail(h, MIND_ELAYOUT, "invalid NetCon delay or weight");
@@ -803,6 +832,10 @@ int create(const MindLayout *L, MindHandle *h) {
     h->smem_bytes = worst_smem;
     const int smem_attr = (int)std::max<size_t>(worst_smem, 1);
     CUDA_TRY(h, set_window_smem<kCellThreads>(smem_attr));
+    CUDA_TRY(h, cudaFuncSetAttribute(window_kernel<false, kCellThreads, false, true>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr));
+    CUDA_TRY(h, cudaFuncSetAttribute(window_kernel<true, kCellThreads, false, true>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr));
     CUDA_TRY(h, set_window_smem<kCellThreads / 2>(smem_attr));
     CUDA_TRY(h, set_window_smem<kCellThreads / 4>(smem_attr));
     CUDA_TRY(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
@@ -824,6 +857,12 @@ int upload_group_state(MindHandle *h) {
     for (size_t g = 0; g < h->group_init.size(); ++g) {
         const auto &init = h->group_init[g];
         DevGroup &G = h->P.groups[g];
+        if (G.gen >= 0) {
+            for (size_t k = 0; k < init.f.size() && init.rows; ++k)
+                CUDA_TRY(h, cudaMemcpyAsync(G.cols + k * (size_t)init.rows, init.f[k].data(), init.rows * sizeof(double),
+                                            cudaMemcpyHostToDevice, h->stream));
+            continue;
+        }
         for (size_t k = 0; k < init.f.size(); ++k)
             if (G.f[k] && init.rows)
                 CUDA_TRY(h, cudaMemcpyAsync(G.f[k], init.f[k].data(), init.rows * sizeof(double),
@@ -877,7 +916,8 @@ int resolve_record(MindHandle *h, const MindRecord &rec, RecordTarget &out) {
     if (slot < 0) return fail(h, MIND_EARG, "mechanism field is not kept on the device (ASSIGNED in BREAKPOINT)");
     const int32_t kind = h->group_init[g].kind;
     const int32_t dev = h->dev_row_of[g][rec.row - 1];
-    out.initial = P.groups[g].f[slot] + dev;
+    out.initial = kind_generated(kind) ? P.groups[g].cols + (int64_t)slot * P.groups[g].rows + dev
+                                       : P.groups[g].f[slot] + dev;
     if (kind == MIND_MECH_NETSTIM) {
         out.cell = -1;   // artificial cells belong to no cell's window
         return MIND_OK;
@@ -992,9 +1032,14 @@ int set_records(MindHandle *h, const MindRecord *records, int32_t nrec, int64_t 
 /* One size bin's window-kernel launch in its chosen shape. */
 template <bool MIXED>
 void launch_window(const MindHandle::Bin &bin, cudaStream_t s, const Params &P, const int32_t *cells, int64_t n0,
-                   int32_t W) {
+                   int32_t W, bool generated) {
     constexpr int T = kCellThreads;
-    if (bin.global_image)
+    if (generated) {   // models with mechanisms emitted from MOD files: the variant that runs them, 128 threads
+        if (bin.global_image)
+            window_kernel<MIXED, T, true, true><<<bin.count, T, 0, s>>>(P, cells, n0, W);
+        else
+            window_kernel<MIXED, T, false, true><<<bin.count, T, bin.smem_bytes, s>>>(P, cells, n0, W);
+    } else if (bin.global_image)
         window_kernel<MIXED, T, true><<<bin.count, T, 0, s>>>(P, cells, n0, W);
     else if (bin.threads == T)
         window_kernel<MIXED, T><<<bin.count, T, bin.smem_bytes, s>>>(P, cells, n0, W);
@@ -1103,9 +1148,9 @@ int advance(MindHandle *h, int64_t steps, bool record_spikes) {
             cudaStreamWaitEvent(s, h->fork, 0);
             const int32_t *cells = h->bin_cells + bin.first;
             if (h->precision == MIND_MIXED)
-                launch_window<true>(bin, s, P, cells, n0, W);
+                launch_window<true>(bin, s, P, cells, n0, W, h->has_generated);
             else
-                launch_window<false>(bin, s, P, cells, n0, W);
+                launch_window<false>(bin, s, P, cells, n0, W, h->has_generated);
             cudaEventRecord(h->bin_done[b], s);
             cudaStreamWaitEvent(h->stream, h->bin_done[b], 0);
             ++st.launches;
@@ -1689,7 +1734,7 @@ int mind_autotune(MindHandle *h, int32_t windows) {
     if (status) return status;
     const int32_t shapes[3] = {kCellThreads, kCellThreads / 2, kCellThreads / 4};
     for (auto &bin : h->bins) {
-        if (bin.global_image) continue;   // HBM images run 128 threads
+        if (bin.global_image || h->has_generated) continue;   // HBM images and emitted mechanisms: 128 threads
         const int32_t keep = bin.threads;
         for (int32_t t : shapes) {
             if (t == keep || t < bin.max_detectors) continue;   // one detector per thread
@@ -1724,8 +1769,8 @@ int mind_set_bin_threads(MindHandle *h, const int32_t *threads, int32_t n_bins) 
             return fail(h, MIND_EARG, "a bin runs 128, 64 or 32 threads per cell");
         if (threads[b] < h->bins[b].max_detectors)
             return fail(h, MIND_EARG, "a bin's cells have more detectors than its CTA has threads");
-        if (h->bins[b].global_image && threads[b] != kCellThreads)
-            return fail(h, MIND_EARG, "cells with their image in HBM run 128 threads");
+        if ((h->bins[b].global_image || h->has_generated) && threads[b] != kCellThreads)
+            return fail(h, MIND_EARG, "cells with their image in HBM, and models with emitted mechanisms, run 128 threads");
     }
     for (int32_t b = 0; b < n_bins; ++b) h->bins[b].threads = threads[b];
     return MIND_OK;
@@ -1735,6 +1780,37 @@ int mind_window_steps(const MindHandle *h, int32_t *steps) {
     if (!h || !steps) return MIND_EARG;
     *steps = h->window;
     return MIND_OK;
+}
+
+int mind_mechanism_count(int32_t *n) {
+    if (!n) return MIND_EARG;
+    *n = kGeneratedCount;
+    return MIND_OK;
+}
+
+int mind_mechanism_info(int32_t index, MindMechanismInfo *info) {
+    if (!info || index < 0 || index >= kGeneratedCount) return MIND_EARG;
+    const GenMechanism &g = kGenMechanisms[index];
+    info->name = g.name;
+    info->kind = MIND_MECH_GENERATED + index;
+    info->point = g.point;
+    info->net_receive = g.net_receive;
+    info->n_fields = g.n_fields;
+    info->field_names = kGenFieldNames + g.first_field;
+    info->defaults = kGenDefaults + g.first_field;
+    info->digest = g.digest;
+    info->ion_reads = g.ion_reads;
+    return MIND_OK;
+}
+
+int mind_mechanism_kind(const char *name, int32_t *kind) {
+    if (!name || !kind) return MIND_EARG;
+    for (int32_t k = 0; k < kGeneratedCount; ++k)
+        if (std::strcmp(kGenMechanisms[k].name, name) == 0) {
+            *kind = MIND_MECH_GENERATED + k;
+            return MIND_OK;
+        }
+    return MIND_EARG;
 }
 
 const char *mind_last_error(const MindHandle *h) {

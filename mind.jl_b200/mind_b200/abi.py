@@ -92,6 +92,15 @@ class MindRecord(Structure):
     _fields_ = [("kind", c_int32), ("node", c_int32), ("group", c_int32), ("row", c_int32), ("field", c_int32)]
 
 
+class MindMechanismInfo(Structure):
+    _fields_ = [("name", c_char_p), ("kind", c_int32), ("point", c_int32), ("net_receive", c_int32),
+                ("n_fields", c_int32), ("field_names", POINTER(c_char_p)), ("defaults", POINTER(c_double)),
+                ("digest", ctypes.c_uint64), ("ion_reads", c_char_p)]
+
+
+MIND_MECH_GENERATED = 64
+
+
 class MindRunStats(Structure):
     _fields_ = [
         ("run_ms", c_double),
@@ -200,6 +209,9 @@ def load_library():
     lib.mind_mlp_gradients.argtypes = [handle, f32, f32, c_int64, f32, f32]
     lib.mind_mlp_set_data.argtypes = [handle, f32, f32, c_int64]
     lib.mind_mlp_train.argtypes = [handle, c_int32, c_int32, ctypes.c_float, f32, f32]
+    lib.mind_mechanism_count.argtypes = [POINTER(c_int32)]
+    lib.mind_mechanism_info.argtypes = [c_int32, POINTER(MindMechanismInfo)]
+    lib.mind_mechanism_kind.argtypes = [c_char_p, POINTER(c_int32)]
     for name in ("mind_create", "mind_initialize", "mind_set_precision", "mind_run", "mind_step",
                  "mind_time", "mind_get_trace", "mind_get_spikes", "mind_read_voltage", "mind_read_value",
                  "mind_inject_event", "mind_last_run_ms", "mind_destroy", "mind_run_stats",
@@ -209,7 +221,8 @@ def load_library():
                  "mind_attach_surrogate",
                  "mind_mlp_create", "mind_mlp_destroy",
                  "mind_mlp_param_count", "mind_mlp_set_params", "mind_mlp_get_params", "mind_mlp_predict",
-                 "mind_mlp_gradients", "mind_mlp_set_data", "mind_mlp_train"):
+                 "mind_mlp_gradients", "mind_mlp_set_data", "mind_mlp_train", "mind_mechanism_count",
+                 "mind_mechanism_info", "mind_mechanism_kind"):
         getattr(lib, name).restype = c_int32
     _LIB = lib
     return lib
@@ -224,6 +237,7 @@ EXPORTED_SYMBOLS = (
     "mind_set_bin_threads", "mind_attach_macro", "mind_get_macro_trace",
     "mind_set_drive_recording", "mind_get_drive", "mind_attach_surrogate", "mind_mlp_create", "mind_mlp_destroy", "mind_mlp_last_error", "mind_mlp_param_count", "mind_mlp_set_params",
     "mind_mlp_get_params", "mind_mlp_predict", "mind_mlp_gradients", "mind_mlp_set_data", "mind_mlp_train",
+    "mind_mechanism_count", "mind_mechanism_info", "mind_mechanism_kind",
 )
 
 MIND_NOALLOC_SCRATCH_BYTES = 16 << 20

@@ -114,15 +114,82 @@ _BUILTINS: Dict[str, Mechanism] = {
 }
 
 
+def compiled_mechanisms() -> Dict[str, Mechanism]:
+    """The mechanisms whose CUDA C was emitted from MOD files (mind_b200.nmodl) and compiled
+    into libmindgpu.so, by name (mind_mechanism_info; kind codes MIND_MECH_GENERATED + k)."""
+    global _COMPILED
+    if _COMPILED is None:
+        import ctypes
+
+        from . import abi
+
+        lib = abi.load_library()
+        n = ctypes.c_int32()
+        abi.check(lib, None, lib.mind_mechanism_count(ctypes.byref(n)))
+        table = {}
+        for k in range(n.value):
+            info = abi.MindMechanismInfo()
+            abi.check(lib, None, lib.mind_mechanism_info(k, ctypes.byref(info)))
+            name = info.name.decode()
+            fields = tuple(info.field_names[j].decode() for j in range(info.n_fields))
+            defaults = tuple(float(info.defaults[j]) for j in range(info.n_fields))
+            words = (info.ion_reads or b"").decode().split()
+            reads = tuple(zip(words[0::2], words[1::2]))
+            table[name] = Mechanism(name, "point" if info.point else "density", int(info.kind), fields, defaults,
+                                    int(info.digest), int(info.net_receive), reads)
+        _COMPILED = table
+    return _COMPILED
+
+
+_COMPILED = None
+
+
 def builtin(name) -> Mechanism:
-    """Select a packaged builtin by its MOD name (frontend.jl:58-72)."""
+    """Select a packaged builtin by its MOD name (frontend.jl:58-72): the hand-written device
+    code for hh, pas, ExpSyn, Exp2Syn, NetStim, IClamp and AlphaSynapse, else a mechanism
+    emitted from the reference's MOD directory into the library (SEClamp, VClamp)."""
     key = str(name)
-    try:
+    if key in _BUILTINS:
         return _BUILTINS[key]
+    compiled = compiled_mechanisms()
+    if key in compiled:
+        return compiled[key]
+    raise ValueError(f"unknown mechanism {key}; the library runs {sorted(set(_BUILTINS) | set(compiled))}; "
+                     "load a MOD file with load_mod")
+
+
+def emitted(name: str) -> Mechanism:
+    """The mechanism `name` as CUDA C emitted from its MOD file and compiled into the library
+    (for hh, pas, ExpSyn, Exp2Syn, IClamp and AlphaSynapse this is the same MOD that
+    builtin() runs through hand-written device code)."""
+    try:
+        return compiled_mechanisms()[str(name)]
     except KeyError:
-        raise ValueError(
-            f"unknown mechanism {key}; this build evaluates {sorted(_BUILTINS)} on the device"
-        ) from None
+        raise ValueError(f"{name} is not compiled into this library as emitted code") from None
+
+
+def compile_mod(source: str, filename: str = "<string>") -> Mechanism:
+    """compile_mod (src/compiler/frontend.jl:85-110): parse and lower MOD source, and select
+    the emitted mechanism compiled into the library for exactly this source (same name and
+    SHA-256 digest).  The emitted CUDA C (mind_b200.nmodl.emit) runs through the window
+    kernel's generated-mechanism path, even for names that also have hand-written code."""
+    from .nmodl.cuda import compile_source
+
+    ir = compile_source(source, filename)
+    compiled = compiled_mechanisms().get(ir.name)
+    if compiled is None or compiled.digest != ir.digest:
+        raise ValueError(f"{ir.name} ({filename}) is not compiled into this library; add it with "
+                         "mind.jl_b200/csrc/gen_mechanisms.py and rebuild (mind.jl_b200/csrc/build.py)")
+    if compiled.fields != ir.field_names:
+        raise ValueError(f"{ir.name}: the library's fields differ from this source's")
+    return Mechanism(ir.name, ir.kind, compiled.code, compiled.fields, compiled.defaults, ir.digest,
+                     len(ir.receive_args), tuple(ir.ion_reads))
+
+
+def load_mod(path: str) -> Mechanism:
+    """load_mod (src/compiler/frontend.jl:15-57) for one MOD file."""
+    with open(path) as f:
+        return compile_mod(f.read(), path)
 
 
 def resolve_mechanism(mechanism) -> Mechanism:

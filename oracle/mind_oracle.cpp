@@ -166,6 +166,17 @@ const char *const NS_NAMES[] = {"interval", "number", "start", "noise", "event",
 const char *const IC_NAMES[] = {"del", "dur", "amp"};
 const char *const AS_NAMES[] = {"onset", "tau", "gmax", "e"};
 
+/* Electrode clamps of mod/SEClamp.mod and mod/VClamp.mod, restated by hand (the library runs
+ * them through CUDA C emitted from the MOD files; oracle.py hands them to this file under
+ * these kind codes).  Fields by MOD name; VClamp's dur/amp arrays as dur[0..2], amp[0..2]. */
+constexpr int32_t ORACLE_SECLAMP = 1001, ORACLE_VCLAMP = 1002;
+enum { SE_RS, SE_DUR1, SE_AMP1, SE_DUR2, SE_AMP2, SE_DUR3, SE_AMP3, SE_I, SE_VC, SE_TC2, SE_TC3, SE_ON, SE_NF };
+const char *const SE_NAMES[] = {"rs", "dur1", "amp1", "dur2", "amp2", "dur3", "amp3", "i", "vc", "tc2", "tc3", "on"};
+enum { VC_DUR, VC_AMP = VC_DUR + 3, VC_GAIN = VC_AMP + 3, VC_RSTIM, VC_TAU1, VC_TAU2, VC_E0, VC_VO0, VC_VI0, VC_FAC,
+       VC_E, VC_VO, VC_VI, VC_I, VC_STIM, VC_TC, VC_NF };
+const char *const VC_NAMES[] = {"dur[0]", "dur[1]", "dur[2]", "amp[0]", "amp[1]", "amp[2]", "gain", "rstim", "tau1",
+                                "tau2", "e0", "vo0", "vi0", "fac", "e", "vo", "vi", "i", "stim", "tc"};
+
 struct Oracle {
     const MindLayout *L;
     int64_t n;
@@ -365,6 +376,8 @@ struct Oracle {
                 case MIND_MECH_NETSTIM: names = NS_NAMES; nf = NS_NF; break;
                 case MIND_MECH_ICLAMP: names = IC_NAMES; nf = IC_NF; break;
                 case MIND_MECH_ALPHASYN: names = AS_NAMES; nf = AS_NF; break;
+                case ORACLE_SECLAMP: names = SE_NAMES; nf = SE_NF; break;
+                case ORACLE_VCLAMP: names = VC_NAMES; nf = VC_NF; break;
                 default: return fail(MIND_ELAYOUT, "unsupported mechanism kind");
             }
             G.f.resize(nf);
@@ -501,6 +514,20 @@ struct Oracle {
                         G.f[HH_N][r] = R.ninf;
                     } break;
                     case MIND_MECH_EXPSYN: G.f[ES_G][r] = 0.0; break;
+                    case ORACLE_SECLAMP:
+                        G.f[SE_TC2][r] = G.f[SE_DUR1][r] + G.f[SE_DUR2][r];
+                        G.f[SE_TC3][r] = G.f[SE_TC2][r] + G.f[SE_DUR3][r];
+                        G.f[SE_ON][r] = 0.0;
+                        break;
+                    case ORACLE_VCLAMP: {
+                        const double vv = v[G.node[r]];
+                        G.f[VC_E0][r] = 0.0;
+                        G.f[VC_VO][r] = vv;
+                        G.f[VC_VO0][r] = vv;
+                        G.f[VC_VI][r] = vv;
+                        G.f[VC_VI0][r] = vv;
+                        G.f[VC_E][r] = 0.0;
+                    } break;
                     case MIND_MECH_EXP2SYN: {
                         double &tau1 = G.f[E2_TAU1][r];
                         double tau2 = G.f[E2_TAU2][r];
@@ -576,6 +603,60 @@ struct Oracle {
         }
     }
 
+    // ---- SEClamp (mod/SEClamp.mod): vstim() then icur() in BREAKPOINT; icur() after the solve
+    static void seclamp_icur(Group &G, int64_t r, double vv) {
+        if (G.f[SE_ON][r] != 0.0)
+            G.f[SE_I][r] = (G.f[SE_VC][r] - vv) / G.f[SE_RS][r];
+        else
+            G.f[SE_I][r] = 0.0;
+    }
+    static void seclamp_vstim(Group &G, int64_t r, double t, double vv) {
+        G.f[SE_ON][r] = 1.0;
+        if (t < G.f[SE_DUR1][r]) {
+            G.f[SE_VC][r] = G.f[SE_AMP1][r];
+        } else if (t < G.f[SE_TC2][r]) {
+            G.f[SE_VC][r] = G.f[SE_AMP2][r];
+        } else if (t < G.f[SE_TC3][r]) {
+            G.f[SE_VC][r] = G.f[SE_AMP3][r];
+        } else {
+            G.f[SE_VC][r] = 0.0;
+            G.f[SE_ON][r] = 0.0;
+        }
+        seclamp_icur(G, r, vv);
+    }
+
+    // ---- VClamp (mod/VClamp.mod): the three-level clamp with its amplifier eliminated
+    static void vclamp_vstim(Group &G, int64_t r, double t) {
+        G.f[VC_TC][r] = 0.0;
+        for (int j = 0; j < 3; ++j) {
+            G.f[VC_STIM][r] = G.f[VC_AMP + j][r];
+            G.f[VC_TC][r] = G.f[VC_TC][r] + G.f[VC_DUR + j][r];
+            if (t < G.f[VC_TC][r]) {
+                G.f[VC_TC][r] = G.f[VC_TC][r] + 100.0;
+                break;
+            }
+        }
+    }
+    static void vclamp_clamp(Group &G, int64_t r, double vv, double step_dt) {
+        const double t1 = G.f[VC_TAU1][r] / step_dt, t2 = G.f[VC_TAU2][r] / step_dt;
+        const double fac = G.f[VC_FAC][r], gain = G.f[VC_GAIN][r], vo0 = G.f[VC_VO0][r];
+        const double e = ((1.0 + t1) * ((1.0 - fac) * vv + fac * t2 * vo0 / (1.0 + t2)) - G.f[VC_STIM][r] -
+                          t1 * (G.f[VC_VI0][r] - G.f[VC_E0][r])) /
+                         (2.0 + t1 + (1.0 + t1) * fac * gain / (1.0 + t2));
+        G.f[VC_E][r] = e;
+        G.f[VC_VO][r] = (t2 * vo0 - gain * e) / (1.0 + t2);
+        G.f[VC_VI][r] = vv + fac * G.f[VC_VO][r] - fac * vv;
+    }
+    static double vclamp_icur(Group &G, int64_t r, double t, double vv, double step_dt) {
+        if (t > G.f[VC_TC][r]) {
+            G.f[VC_E0][r] = 0.0;
+            G.f[VC_VO0][r] = 0.0;
+            return 0.0;
+        }
+        vclamp_clamp(G, r, vv, step_dt);
+        return (G.f[VC_VO][r] - vv) / G.f[VC_RSTIM][r];
+    }
+
     /* BREAKPOINT currents of one row at v + 0.001 and v into rhs and d of its node. */
     void current_row(Group &G, int64_t r, double tc) {
         int32_t node = G.node[r];
@@ -624,6 +705,20 @@ struct Oracle {
                 double g = G.f[AS_GMAX][r] * mind_alpha((tc - G.f[AS_ONSET][r]) / G.f[AS_TAU][r]);
                 shifted = 0.0 + g * (probe - G.f[AS_E][r]);
                 value = 0.0 + g * (vv - G.f[AS_E][r]);
+            } break;
+            case ORACLE_SECLAMP: {   // electrode current: the MOD's i counts negative
+                seclamp_vstim(G, r, tc, probe);
+                shifted = 0.0 - G.f[SE_I][r];
+                seclamp_vstim(G, r, tc, vv);
+                value = 0.0 - G.f[SE_I][r];
+            } break;
+            case ORACLE_VCLAMP: {
+                vclamp_vstim(G, r, tc);
+                G.f[VC_I][r] = vclamp_icur(G, r, tc, probe, dt);
+                shifted = 0.0 - G.f[VC_I][r];
+                vclamp_vstim(G, r, tc);
+                G.f[VC_I][r] = vclamp_icur(G, r, tc, vv, dt);
+                value = 0.0 - G.f[VC_I][r];
             } break;
             default: return;
         }
@@ -688,8 +783,9 @@ struct Oracle {
         return status;
     }
 
-    /* cnexp state advance of one row on the new voltage (src/compiler/codegen.jl:569-641). */
-    void advance_row(Group &G, int64_t r) {
+    /* cnexp state advance of one row on the new voltage at time ta = t + dt
+     * (src/compiler/codegen.jl:569-641). */
+    void advance_row(Group &G, int64_t r, double ta) {
         switch (G.kind) {
             case MIND_MECH_HH: {
                 Rates R = rates(v[G.node[r]]);
@@ -704,13 +800,22 @@ struct Oracle {
                 G.f[E2_A][r] = cnexp(G.f[E2_A][r], 0.0, G.f[E2_TAU1][r], dt);
                 G.f[E2_B][r] = cnexp(G.f[E2_B][r], 0.0, G.f[E2_TAU2][r], dt);
                 break;
+            case ORACLE_SECLAMP:   // SOLVE icur METHOD after_cvode, on the new voltage
+                seclamp_icur(G, r, v[G.node[r]]);
+                break;
+            case ORACLE_VCLAMP: {  // SOLVE update METHOD after_cvode at t + dt
+                G.f[VC_I][r] = vclamp_icur(G, r, ta, v[G.node[r]], dt);
+                G.f[VC_E0][r] = G.f[VC_E][r];
+                G.f[VC_VO0][r] = G.f[VC_VO][r];
+                G.f[VC_VI0][r] = G.f[VC_VI][r];
+            } break;
             default: break;
         }
     }
 
-    void advance_cell(int64_t c) {
+    void advance_cell(int64_t c, double ta) {
         for (size_t g = 0; g < groups.size(); ++g)
-            for (int64_t r : cell_rows[c][g]) advance_row(groups[g], r);
+            for (int64_t r : cell_rows[c][g]) advance_row(groups[g], r, ta);
     }
 
     void detect(double t) {
@@ -747,7 +852,7 @@ struct Oracle {
                 for (int64_t c = lo; c < hi; ++c) {
                     currents_cell(c, tc);
                     const int s = cable(c);
-                    advance_cell(c);
+                    advance_cell(c, t + dt);
                     int w = worst.load();
                     while (s > w && !worst.compare_exchange_weak(w, s)) {
                     }
@@ -810,6 +915,8 @@ int oracle_run_macro(const MindLayout *layout, const MindMacroLayout *macro, int
                                    : m.kind == MIND_MECH_EXPSYN ? ES_NAMES
                                    : m.kind == MIND_MECH_EXP2SYN ? E2_NAMES
                                    : m.kind == MIND_MECH_ALPHASYN ? AS_NAMES
+                                   : m.kind == ORACLE_SECLAMP    ? SE_NAMES
+                                   : m.kind == ORACLE_VCLAMP     ? VC_NAMES
                                                                  : IC_NAMES;
         for (size_t slot = 0; slot < G.f.size(); ++slot)
             if (std::strcmp(names[slot], m.field_names[r.field - 1]) == 0) rec_vec[k] = &G.f[slot];

@@ -112,6 +112,26 @@ class OracleResult:
     macro_trace: np.ndarray = None   # [macro boundaries, regions], with regions
 
 
+# Kind codes of this oracle's hand restatements of the clamps (mind_oracle.cpp).
+ORACLE_SECLAMP, ORACLE_VCLAMP = 1001, 1002
+_BUILTIN_CODES = {"hh": 1, "pas": 2, "ExpSyn": 3, "Exp2Syn": 4, "NetStim": 5, "IClamp": 6, "AlphaSynapse": 7,
+                  "SEClamp": ORACLE_SECLAMP, "VClamp": ORACLE_VCLAMP}
+
+
+def _oracle_kinds(layout, c_layout) -> None:
+    """The oracle knows mechanisms by its own restatements: a group whose mechanism the
+    library runs as CUDA C emitted from a MOD file (kind >= 64) is handed to the oracle as
+    the restatement of the same MOD (hh, pas, ... by their hand-written oracle code, SEClamp
+    and VClamp by the clamp restatements); fields are matched by name, so column order
+    does not matter."""
+    for i, g in enumerate(layout.groups):
+        if g.mechanism.code >= 64:
+            code = _BUILTIN_CODES.get(g.mechanism.name)
+            if code is None:
+                raise ValueError(f"the oracle has no restatement of {g.mechanism.name}")
+            c_layout.mechanisms[i].kind = code
+
+
 def run(layout, steps: int, record_nodes=(), threads: int = 0, spike_cap: int = 1 << 22, macro=None,
         records=None, timed_from: int = 0) -> OracleResult:
     """Initialize the layout (and the regions of `macro`, a MacroModel) on the CPU and advance
@@ -131,6 +151,7 @@ def run(layout, steps: int, record_nodes=(), threads: int = 0, spike_cap: int = 
     if threads <= 0:
         threads = os.cpu_count() or 1
     c_layout = layout.to_c()
+    _oracle_kinds(layout, c_layout)
     if records is None:
         specs = [(abi.MIND_RECORD_VOLTAGE, int(node), 0, 0, 0) for node in record_nodes]
     else:

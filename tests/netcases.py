@@ -223,3 +223,55 @@ def burst_onto_one_cell(n_events=200, n_cells=3, seed=4):
     M.connect_many(model, np.repeat(source, n), np.arange(first, first + n),
                    rng.lognormal(math.log(0.05), 0.3, n) / 1000.0, rng.uniform(0.5, 1.0, n))
     return model
+
+
+def mechanism_mix(select, n_cells=12, synapses=12, seed=9, clamps=False):
+    """Branched cells with every cell mechanism of the MOD directory, each taken from
+    `select(name)` -- mb.builtin (hand-written device code) or mb.emitted (CUDA C emitted
+    from the MOD file): hh somata, pas dendrites, Exp2Syn and ExpSyn synapses driven by
+    NetStims and recurrent NetCons, IClamp and AlphaSynapse on some somata; with `clamps`,
+    an SEClamp on cell 1's soma and a VClamp on cell 2's (three command levels each)."""
+    rng = np.random.default_rng(seed)
+    model = M.MicroModel(celsius=6.3)
+    cells = []
+    for c in range(n_cells):
+        soma = mb.Section("soma", label="soma", length=20.0, diameter=20.0, nseg=1)
+        secs = networks._binary_tree(rng, int(rng.integers(30, 90)), soma)
+        cell = M.add_population(model, secs, 1, voltage=-65.0)[0]
+        M.insert(cell, select("hh"), sections="soma")
+        M.insert(cell, select("pas"), sections="dend", params={"g": 1e-4, "e": -65.0})
+        M.register_spike_source(cell, threshold=-10.0)
+        cells.append((cell, secs))
+    n = n_cells * synapses
+    owners = np.repeat(np.arange(1, n_cells + 1), synapses)
+    names, xs = [], []
+    for cell, secs in cells:
+        nm, x = networks._dendritic_sites(rng, secs, synapses)
+        names += nm
+        xs.append(x)
+    xs = np.concatenate(xs)
+    half = n // 2
+    first2 = M.add_pointprocesses(model, select("Exp2Syn"), owners[:half], names[:half], xs[:half],
+                                  {"tau1": 0.5, "tau2": 5.0, "e": np.where(rng.uniform(size=half) < 0.8, 0.0, -80.0)})
+    first1 = M.add_pointprocesses(model, select("ExpSyn"), owners[half:], names[half:], xs[half:],
+                                  {"tau": 2.0, "e": 0.0})
+    targets = np.concatenate([np.arange(first2, first2 + half), np.arange(first1, first1 + n - half)])
+    M.connect_many(model, rng.integers(1, n_cells + 1, n), targets,
+                   rng.lognormal(math.log(3.0), 0.5, n) / 1000.0, rng.uniform(0.6, 3.0, n))
+    stims = M.add_pointprocesses(model, mb.builtin("NetStim"), np.zeros(n, np.int64), "none", np.zeros(n),
+                                 {"interval": 40.0, "number": 1e9, "start": 0.0, "noise": 1.0})
+    sources = M.register_point_sources(model, np.arange(stims, stims + n))
+    M.connect_many(model, sources, targets, rng.lognormal(math.log(6.0), 0.5, n) / 1000.0, rng.uniform(0.0, 1.0, n))
+    k = max(1, n_cells // 4)
+    M.add_pointprocesses(model, select("IClamp"), np.arange(3, 3 + k), "soma", np.full(k, 0.5),
+                         {"del": 5.0, "dur": 20.0, "amp": 0.3})
+    M.add_pointprocesses(model, select("AlphaSynapse"), np.arange(4, 4 + k), "soma", np.full(k, 0.5),
+                         {"onset": 8.0, "tau": 2.0, "gmax": 0.02, "e": 0.0})
+    if clamps:
+        M.add_pointprocesses(model, select("SEClamp"), np.array([1]), "soma", np.array([0.5]),
+                             {"dur1": 5.0, "amp1": -70.0, "dur2": 10.0, "amp2": -20.0, "dur3": 8.0, "amp3": -60.0,
+                              "rs": 0.01})
+        M.add_pointprocesses(model, select("VClamp"), np.array([2]), "soma", np.array([0.5]),
+                             {"dur[0]": 6.0, "dur[1]": 9.0, "dur[2]": 6.0, "amp[0]": -68.0, "amp[1]": -25.0,
+                              "amp[2]": -55.0})
+    return model
