@@ -23,6 +23,18 @@ const MIND_RECORD_MECHANISM = Int32(2)
 const KIND_CODES = Dict(:hh => Int32(1), :pas => Int32(2), :ExpSyn => Int32(3), :Exp2Syn => Int32(4),
                         :NetStim => Int32(5), :IClamp => Int32(6), :AlphaSynapse => Int32(7))
 
+# Kind code of a mechanism: the hand-written device code for the builtins above, else the
+# CUDA C emitted from its MOD file and compiled into the library (mind_mechanism_kind;
+# SEClamp, VClamp and any MOD added with csrc/gen_mechanisms.py).
+function kind_code(name::Symbol)
+    haskey(KIND_CODES, name) && return KIND_CODES[name]
+    kind = Ref{Int32}(0)
+    status = ccall((:mind_mechanism_kind, libmindgpu), Cint, (Cstring, Ref{Int32}), String(name), kind)
+    status == 0 || throw(ArgumentError("libmindgpu has no device code for mechanism $name; emit its MOD file " *
+                                       "with csrc/gen_mechanisms.py and rebuild the library"))
+    return kind[]
+end
+
 struct MindMechanism
     kind::Int32
     n_fields::Int32
@@ -113,8 +125,17 @@ function group_columns(plan, group)
             end
         end
     end
-    names = [Base.unsafe_convert(Ptr{UInt8}, String(f.name)) for f in ir.fields]
-    return data, String.(getfield.(ir.fields, :name)), names
+    # one name per data column: an array field of extent n is named name[0] .. name[n-1]
+    columns = String[]
+    for f in ir.fields
+        if f.extent == 0
+            push!(columns, String(f.name))
+        else
+            append!(columns, ["$(f.name)[$k]" for k in 0:(f.extent - 1)])
+        end
+    end
+    names = [Base.unsafe_convert(Ptr{UInt8}, c) for c in columns]
+    return data, columns, names
 end
 
 """Create the device state from a built model (allocate_simulation + initialize!)."""
@@ -128,7 +149,7 @@ function mindgpu_initialize!(model; precision::Symbol = :fp64)
         cnames = [pointer(s) for s in names_str]
         push!(keep, data, names_str, cnames, group.nodes, group.logical_ids)
         digest = parse(UInt64, first(group.mechanism.ir.source_digest, 16); base = 16)
-        push!(mechs, MindMechanism(KIND_CODES[group.mechanism.ir.name], Int32(size(data, 2)), size(data, 1),
+        push!(mechs, MindMechanism(kind_code(group.mechanism.ir.name), Int32(size(data, 2)), size(data, 1),
                                    pointer(data), pointer(cnames), pointer(group.nodes),
                                    pointer(group.logical_ids), digest))
     end
