@@ -373,6 +373,38 @@ int mind_mechanism_info(int32_t index, MindMechanismInfo *info);
 /* The kind code of the emitted mechanism named `name`; MIND_EARG if none is compiled in. */
 int mind_mechanism_kind(const char *name, int32_t *kind);
 
+/*
+ * discretize (src/model/micro/morphology.jl:406-484): one morphology's sections into its
+ * cable node tree, the build-time step that produces MindLayout's node arrays.  Sections
+ * are visited parents first; a root section gets a root node (area 100 um2, no
+ * capacitance or axial conductance), every section nseg segment nodes whose area, axial
+ * conductance to the previous node and capacitance (cm * area * 1e-5) integrate its
+ * geometry over half segments, then one zero-capacitance node at its x = 1 end.  Node ids
+ * are 1-based (parent 0 = none).  Host only: no device work.  Returns MIND_ECAPACITY when
+ * `capacity` is below the node count (out->node_count receives it; call again with room),
+ * MIND_ELAYOUT with a message for an invalid morphology.
+ */
+typedef struct MindSection {
+    int32_t parent;                    /* 0-based index of the parent section, -1 for a root */
+    int32_t nseg;
+    double parent_x;                   /* where on the parent it attaches, in [0, 1] */
+    double child_x;                    /* its own attached end, 0 or 1 */
+    double length, diameter;           /* um, used when there are no pt3d samples */
+    double Ra, cm;                     /* ohm cm, uF/cm2 */
+    int32_t n_points;                  /* pt3d samples (x, y, z, diameter), >= 2 to be used */
+    const double *points;              /* [n_points][4] */
+} MindSection;
+typedef struct MindMorphology {
+    int64_t node_count;                /* out */
+    int32_t *parent;                   /* [capacity] 1-based parent node, 0 = none */
+    double *area, *diameter, *axial, *capacitance, *edge_length;   /* [capacity] */
+    int64_t *section_start;            /* [n_sections] node at x = 0 (may be NULL) */
+    int64_t *section_end;              /* [n_sections] node at x = 1 (may be NULL) */
+    int64_t *section_first;            /* [n_sections] its first segment node (may be NULL) */
+} MindMorphology;
+int mind_discretize(const MindSection *sections, int32_t n_sections, int64_t capacity, MindMorphology *out,
+                    char *message, int32_t message_len);
+
 /* Message for the last non-zero status of this handle (or of mind_create when h is NULL). */
 const char *mind_last_error(const MindHandle *h);
 

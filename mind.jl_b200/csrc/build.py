@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 PACKAGE = os.path.dirname(HERE)
 OUT_DIR = os.path.join(PACKAGE, "lib")
 OUTPUT = os.path.join(OUT_DIR, "libmindgpu.so")
-SOURCES = [os.path.join(HERE, "mindgpu.cu"), os.path.join(HERE, "surrogate.cu")]
+SOURCES = [os.path.join(HERE, "mindgpu.cu"), os.path.join(HERE, "surrogate.cu"), os.path.join(HERE, "planner.cpp")]
 DEPENDS = SOURCES + [os.path.join(HERE, f) for f in ("device.cuh", "kernels.cuh", "macro.cuh", "mind_math.h",
                                                      "gen_runtime.cuh", "generated_mechanisms.cuh")] + [
     os.path.join(os.path.dirname(PACKAGE), "include", "mindgpu.h")]

@@ -101,6 +101,19 @@ class MindMechanismInfo(Structure):
 MIND_MECH_GENERATED = 64
 
 
+class MindSection(Structure):
+    _fields_ = [("parent", c_int32), ("nseg", c_int32), ("parent_x", c_double), ("child_x", c_double),
+                ("length", c_double), ("diameter", c_double), ("Ra", c_double), ("cm", c_double),
+                ("n_points", c_int32), ("points", POINTER(c_double))]
+
+
+class MindMorphology(Structure):
+    _fields_ = [("node_count", c_int64), ("parent", POINTER(c_int32)), ("area", POINTER(c_double)),
+                ("diameter", POINTER(c_double)), ("axial", POINTER(c_double)), ("capacitance", POINTER(c_double)),
+                ("edge_length", POINTER(c_double)), ("section_start", POINTER(c_int64)),
+                ("section_end", POINTER(c_int64)), ("section_first", POINTER(c_int64))]
+
+
 class MindRunStats(Structure):
     _fields_ = [
         ("run_ms", c_double),
@@ -212,6 +225,8 @@ def load_library():
     lib.mind_mechanism_count.argtypes = [POINTER(c_int32)]
     lib.mind_mechanism_info.argtypes = [c_int32, POINTER(MindMechanismInfo)]
     lib.mind_mechanism_kind.argtypes = [c_char_p, POINTER(c_int32)]
+    lib.mind_discretize.argtypes = [POINTER(MindSection), c_int32, c_int64, POINTER(MindMorphology), c_char_p,
+                                    c_int32]
     for name in ("mind_create", "mind_initialize", "mind_set_precision", "mind_run", "mind_step",
                  "mind_time", "mind_get_trace", "mind_get_spikes", "mind_read_voltage", "mind_read_value",
                  "mind_inject_event", "mind_last_run_ms", "mind_destroy", "mind_run_stats",
@@ -222,7 +237,7 @@ def load_library():
                  "mind_mlp_create", "mind_mlp_destroy",
                  "mind_mlp_param_count", "mind_mlp_set_params", "mind_mlp_get_params", "mind_mlp_predict",
                  "mind_mlp_gradients", "mind_mlp_set_data", "mind_mlp_train", "mind_mechanism_count",
-                 "mind_mechanism_info", "mind_mechanism_kind"):
+                 "mind_mechanism_info", "mind_mechanism_kind", "mind_discretize"):
         getattr(lib, name).restype = c_int32
     _LIB = lib
     return lib
@@ -237,7 +252,7 @@ EXPORTED_SYMBOLS = (
     "mind_set_bin_threads", "mind_attach_macro", "mind_get_macro_trace",
     "mind_set_drive_recording", "mind_get_drive", "mind_attach_surrogate", "mind_mlp_create", "mind_mlp_destroy", "mind_mlp_last_error", "mind_mlp_param_count", "mind_mlp_set_params",
     "mind_mlp_get_params", "mind_mlp_predict", "mind_mlp_gradients", "mind_mlp_set_data", "mind_mlp_train",
-    "mind_mechanism_count", "mind_mechanism_info", "mind_mechanism_kind",
+    "mind_mechanism_count", "mind_mechanism_info", "mind_mechanism_kind", "mind_discretize",
 )
 
 MIND_NOALLOC_SCRATCH_BYTES = 16 << 20

@@ -10,11 +10,11 @@ per morphology:
 * one zero-capacitance endpoint per section at its x=1 end, which is where
   child sections attach.
 
-Every parent is numbered before its children.  The geometry integration follows
-the reference's half-compartment walk over pt3d spans step for step, because
-the packed coefficients feed an FP64 solve whose results are compared bit for
-bit; sections given by length and diameter are evaluated for all their
-half-segments at once with the same floating-point operations.
+Every parent is numbered before its children.  The discretization itself runs in
+the library's C++ planner (csrc/planner.cpp, mind_discretize), which follows the
+reference's half-compartment walk over pt3d spans step for step, because the
+packed coefficients feed an FP64 solve whose results are compared bit for bit;
+oracle/geometry.py restates it in numpy as the tests' check.
 """
 from __future__ import annotations
 
@@ -24,7 +24,6 @@ from typing import Dict, List, Optional, Sequence
 
 import numpy as np
 
-HALF_PI = 0.5 * math.pi
 
 
 @dataclass(frozen=True)
@@ -113,258 +112,61 @@ class MorphologyLayout:
         return len(self.parent)
 
 
-def section_order(sections: Sequence[Section]) -> List[int]:
-    """Parents before children, resolving each parent chain in input order."""
-    names = {s.name: i for i, s in enumerate(sections)}
-    if len(names) != len(sections):
-        raise ValueError("duplicate section name")
-    marks = [0] * len(sections)
-    order: List[int] = []
-    pending: List[int] = []
-    for start in range(len(sections)):
-        index = start
-        while marks[index] != 2:
-            if marks[index] == 1:
-                raise ValueError("morphology contains a cycle")
-            marks[index] = 1
-            pending.append(index)
-            parent = sections[index].parent
-            if parent is None:
-                break
-            if parent not in names:
-                raise ValueError(f"unknown parent section {parent}")
-            index = names[parent]
-        while pending:
-            index = pending.pop()
-            marks[index] = 2
-            order.append(index)
-    return order
-
-
-def _integrate_geometry(points, arcs, boundary, Ra, cursor):
-    """Area, axial resistance and diameter integral from the cursor to `boundary`."""
-    area = 0.0
-    resistance = 0.0
-    diameter_integral = 0.0
-    index, previous_arc, previous_diameter = cursor
-    last = len(points) - 1
-    while True:
-        nxt = index + 1
-        at_boundary = arcs[nxt] > boundary or nxt == last
-        if at_boundary:
-            span = arcs[nxt] - arcs[index]
-            fraction = 1.0 if abs(span) < 1.0e-10 else (boundary - arcs[index]) / span
-            arc = boundary
-            diameter = (1.0 - fraction) * points[index].diameter + fraction * points[nxt].diameter
-        else:
-            arc, diameter = arcs[nxt], points[nxt].diameter
-        delta = arc - previous_arc
-        diameter_integral += (previous_diameter + diameter) * delta
-        distance = max(delta, 1.0e-15)
-        conductance = previous_diameter * diameter / distance
-        resistance += 1.0 / (1.0e-15 if conductance == 0.0 else conductance)
-        jump = diameter - previous_diameter
-        area += (previous_diameter + diameter) * math.sqrt(distance * distance + 0.25 * (jump * jump))
-        previous_arc, previous_diameter = arc, diameter
-        if at_boundary:
-            break
-        index = nxt
-    return (HALF_PI * area, ((0.04 * Ra) / math.pi) * resistance, 0.5 * diameter_integral,
-            (index, previous_arc, previous_diameter))
-
-
-def _section_points(section: Section):
-    if len(section.points) >= 2:
-        points = list(section.points)
-    else:
-        points = [Point3D(0.0, 0.0, 0.0, section.diameter),
-                  Point3D(section.length, 0.0, 0.0, section.diameter)]
-    arcs = [0.0]
-    for left, right in zip(points[:-1], points[1:]):
-        dx, dy, dz = right.x - left.x, right.y - left.y, right.z - left.z
-        arcs.append(arcs[-1] + math.sqrt(dx * dx + dy * dy + dz * dz))
-    if not arcs[-1] > 0.0:
-        raise ValueError(f"section {section.name} has zero arc length")
-    return points, arcs
-
-
-def _segment_geometry_pt3d(section: Section):
-    """Per-segment (area, diameter, axial, capacitance) and the endpoint axial, scalar walk."""
-    points, arcs = _section_points(section)
-    nseg = section.nseg
-    step = arcs[-1] / nseg
-    cursor = (0, arcs[0], points[0].diameter)
-    previous_right = 0.0
-    area = np.empty(nseg)
-    diam = np.empty(nseg)
-    axial = np.empty(nseg)
-    cap = np.empty(nseg)
-    for k in range(1, nseg + 1):
-        middle = (k - 0.5) * step
-        right = k * step
-        al, rl, dl, cursor = _integrate_geometry(points, arcs, middle, section.Ra, cursor)
-        ar, rr, dr, cursor = _integrate_geometry(points, arcs, right, section.Ra, cursor)
-        node_area = al + ar
-        area[k - 1] = node_area
-        diam[k - 1] = (dl + dr) / step
-        axial[k - 1] = 1.0 / (previous_right + rl)
-        cap[k - 1] = section.cm * node_area * 1.0e-5
-        previous_right = rr
-    return area, diam, axial, cap, 1.0 / previous_right, step
-
-
-def _segment_geometry_cylinders(lengths, diameters, nsegs, Ras, cms):
-    """Vectorized half-segment walk for sections without pt3d samples.
-
-    A two-sample section has one pt3d span, so every half-segment ends inside
-    it; the operations are those of `_integrate_geometry` on that span.
-    """
-    lengths = np.asarray(lengths, dtype=np.float64)
-    diameters = np.asarray(diameters, dtype=np.float64)
-    nsegs = np.asarray(nsegs, dtype=np.int64)
-    Ras = np.asarray(Ras, dtype=np.float64)
-    cms = np.asarray(cms, dtype=np.float64)
-    arc_end = np.sqrt(lengths * lengths + 0.0 * 0.0 + 0.0 * 0.0)
-    step = arc_end / nsegs
-    total = int(nsegs.sum())
-    sec = np.repeat(np.arange(len(nsegs)), nsegs)
-    first = np.concatenate(([0], np.cumsum(nsegs)[:-1]))
-    ordinal = (np.arange(total) - np.repeat(first, nsegs) + 1).astype(np.float64)
-    s_step = step[sec]
-    s_arc = arc_end[sec]
-    s_d = diameters[sec]
-    s_Ra = Ras[sec]
-    middle = (ordinal - 0.5) * s_step
-    right = ordinal * s_step
-    # Interleave boundaries: b[2j] = middle_j, b[2j+1] = right_j (per section).
-    bounds = np.empty(2 * total)
-    bounds[0::2] = middle
-    bounds[1::2] = right
-    b_arc = np.repeat(s_arc, 2)
-    b_d = np.repeat(s_d, 2)
-    b_Ra = np.repeat(s_Ra, 2)
-    small = np.abs(b_arc) < 1.0e-10
-    fraction = np.where(small, 1.0, bounds / np.where(small, 1.0, b_arc))
-    diameter = (1.0 - fraction) * b_d + fraction * b_d
-    # Previous boundary and diameter of each half; the first half of a section
-    # starts at arc 0 with the first sample's diameter.
-    prev_arc = np.empty_like(bounds)
-    prev_arc[1:] = bounds[:-1]
-    prev_d = np.empty_like(diameter)
-    prev_d[1:] = diameter[:-1]
-    starts = 2 * first
-    prev_arc[starts] = 0.0
-    prev_d[starts] = diameters
-    delta = bounds - prev_arc
-    diameter_integral = (prev_d + diameter) * delta
-    distance = np.maximum(delta, 1.0e-15)
-    conductance = prev_d * diameter / distance
-    resistance = 1.0 / np.where(conductance == 0.0, 1.0e-15, conductance)
-    jump = diameter - prev_d
-    area_sum = (prev_d + diameter) * np.sqrt(distance * distance + 0.25 * (jump * jump))
-    half_area = HALF_PI * area_sum
-    half_res = ((0.04 * b_Ra) / math.pi) * resistance
-    half_diam = 0.5 * diameter_integral
-    al, ar = half_area[0::2], half_area[1::2]
-    rl, rr = half_res[0::2], half_res[1::2]
-    dl, dr = half_diam[0::2], half_diam[1::2]
-    node_area = al + ar
-    node_diam = (dl + dr) / s_step
-    previous_right = np.empty(total)
-    previous_right[1:] = rr[:-1]
-    previous_right[first] = 0.0
-    axial = 1.0 / (previous_right + rl)
-    cap = cms[sec] * node_area * 1.0e-5
-    last = first + nsegs - 1
-    endpoint_axial = 1.0 / rr[last]
-    return node_area, node_diam, axial, cap, endpoint_axial, step, first
-
-
 def discretize(sections: Sequence[Section]) -> MorphologyLayout:
-    """Discretize sections into the cable node tree (morphology.jl:406-484)."""
-    sections = list(sections)
-    order = section_order(sections)
-    for s in sections:
-        if not (s.nseg > 0 and math.isfinite(s.Ra) and s.Ra > 0 and math.isfinite(s.cm) and s.cm >= 0):
-            raise ValueError(f"invalid segmentation or biophysics on section {s.name}")
-    plain = [i for i in range(len(sections)) if len(sections[i].points) < 2]
-    geometry = {}
-    if plain:
-        area, diam, axial, cap, end_axial, step, first = _segment_geometry_cylinders(
-            [sections[i].length for i in plain], [sections[i].diameter for i in plain],
-            [sections[i].nseg for i in plain], [sections[i].Ra for i in plain],
-            [sections[i].cm for i in plain])
-        for j, i in enumerate(plain):
-            lo, hi = first[j], first[j] + sections[i].nseg
-            geometry[i] = (area[lo:hi], diam[lo:hi], axial[lo:hi], cap[lo:hi], end_axial[j], step[j])
-    for i in range(len(sections)):
-        if i not in geometry:
-            geometry[i] = _segment_geometry_pt3d(sections[i])
+    """Discretize sections into the cable node tree (morphology.jl:406-484).
 
+    The work runs in the library's C++ planner (mind_discretize): sections parents first,
+    a root node per root section, nseg segment nodes integrating the geometry over half
+    segments (pt3d spans, or one span of constant diameter), and an x = 1 node per section.
+    """
+    import ctypes
+
+    from . import abi
+
+    sections = list(sections)
+    index = {s.name: i for i, s in enumerate(sections)}
+    if len(index) != len(sections):
+        raise ValueError("duplicate section name")
+    specs = (abi.MindSection * max(1, len(sections)))()
+    keep = []
+    for i, s in enumerate(sections):
+        if s.parent is not None and s.parent not in index:
+            raise ValueError(f"unknown parent section {s.parent}")
+        c = specs[i]
+        c.parent = -1 if s.parent is None else index[s.parent]
+        c.nseg = int(s.nseg)
+        c.parent_x, c.child_x = float(s.parent_x), float(s.child_x)
+        c.length, c.diameter, c.Ra, c.cm = float(s.length), float(s.diameter), float(s.Ra), float(s.cm)
+        if len(s.points) >= 2:
+            pts = np.ascontiguousarray([[p.x, p.y, p.z, p.diameter] for p in s.points], dtype=np.float64)
+            keep.append(pts)
+            c.n_points = len(s.points)
+            c.points = pts.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        else:
+            c.n_points = 0
     total = sum(s.nseg + 1 for s in sections) + sum(1 for s in sections if s.parent is None)
     parent = np.zeros(total, dtype=np.int32)
-    area = np.empty(total)
-    diameter = np.empty(total)
-    axial_c = np.empty(total)
-    capacitance = np.empty(total)
-    edge_length = np.empty(total)
+    arrays = [np.empty(total) for _ in range(5)]
+    start, end, first = (np.zeros(max(1, len(sections)), dtype=np.int64) for _ in range(3))
+    f64 = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    i64 = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))
+    out = abi.MindMorphology(0, parent.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), *[f64(a) for a in arrays],
+                             i64(start), i64(end), i64(first))
+    message = ctypes.create_string_buffer(256)
+    status = abi.load_library().mind_discretize(specs, len(sections), total, ctypes.byref(out), message, 256)
+    if status != abi.MIND_OK:
+        raise ValueError(message.value.decode() or f"mind_discretize status {status}")
+    area, diameter, axial, capacitance, edge_length = arrays
     section_nodes: Dict[str, np.ndarray] = {}
     starts: Dict[str, int] = {}
-    count = 0
-
-    def add(parent_node, a, d, g, c, span):
-        nonlocal count
-        parent[count] = parent_node
-        area[count] = a
-        diameter[count] = d
-        axial_c[count] = g
-        capacitance[count] = c
-        edge_length[count] = span
-        count += 1
-        return count
-
-    def location(name, x):
-        if x == 0.0:
-            return starts[name]
-        nodes = section_nodes[name]
-        if x == 1.0:
-            return int(nodes[-1])
-        index = min(int(math.floor(x * (len(nodes) - 1))), len(nodes) - 2)
-        return int(nodes[index])
-
-    for index in order:
-        s = sections[index]
-        seg_area, seg_diam, seg_axial, seg_cap, end_axial, step = geometry[index]
-        if s.parent is None:
-            connection = add(0, 100.0, 0.0, 0.0, 0.0, 0.0)
-        else:
-            connection = location(s.parent, s.parent_x)
+    for i, s in enumerate(sections):
+        ids = np.arange(first[i], first[i] + s.nseg, dtype=np.int32)
         nodes = np.empty(s.nseg + 1, dtype=np.int32)
-        reversed_ = s.child_x == 1.0
-        previous = connection
-        base = count
-        n = s.nseg
-        parent[base:base + n] = np.arange(base, base + n, dtype=np.int32)
-        parent[base] = previous
-        area[base:base + n] = seg_area
-        diameter[base:base + n] = seg_diam
-        axial_c[base:base + n] = seg_axial
-        capacitance[base:base + n] = seg_cap
-        edge_length[base:base + n] = step
-        edge_length[base] = 0.5 * step
-        ids = np.arange(base + 1, base + n + 1, dtype=np.int32)
-        count = base + n
-        if reversed_:
-            nodes[:n] = ids[::-1]
-        else:
-            nodes[:n] = ids
-        endpoint = add(count, 100.0, 0.0, end_axial, 0.0, 0.5 * step)
-        starts[s.name] = endpoint if reversed_ else connection
-        nodes[n] = connection if reversed_ else endpoint
+        nodes[:s.nseg] = ids[::-1] if s.child_x == 1.0 else ids
+        nodes[s.nseg] = end[i]
         section_nodes[s.name] = nodes
-    assert count == total
-    return MorphologyLayout(parent, area, diameter, axial_c, capacitance, edge_length,
-                            section_nodes, starts)
+        starts[s.name] = int(start[i])
+    return MorphologyLayout(parent, area, diameter, axial, capacitance, edge_length, section_nodes, starts)
 
 
 def location_node(layout: MorphologyLayout, section: str, x: float) -> int:
