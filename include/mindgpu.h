@@ -106,7 +106,8 @@ typedef struct MindMechanism {
  */
 typedef struct MindLayout {
     int32_t abi_version;               /* MIND_ABI_VERSION */
-    int32_t secondorder;               /* build!(secondorder=); only 0 is supported */
+    int32_t secondorder;               /* build!(secondorder=): 0 backward Euler; 1 and 2 Crank-Nicolson
+                                          (C/(dt/2) in the cable matrix, v += 2 x) */
     int64_t n_nodes;
     const int32_t *parent;             /* [n_nodes] 1-based, 0 = root */
     const double *voltage;             /* [n_nodes] initial membrane voltage (mV) */

@@ -162,6 +162,7 @@ struct Params {
     int32_t ngroups;
     double dt;
     double celsius;
+    double vscale;             // v += vscale * increment: 1 (secondorder 0), 2 (secondorder 1, 2)
     uint64_t seed;
     // nodes (packed, local order)
     const int64_t *node_off;   // [ncells+1]

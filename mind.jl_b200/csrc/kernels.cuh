@@ -487,7 +487,7 @@ template <int NT>
 __device__ __forceinline__ void hines_exact(double *sd, double *sr, const double *sa, double *sv, double *sxd,
                                             double *sxr, const int32_t *ctop, const int32_t *clen,
                                             const int32_t *cpar, const int32_t *ckoff, const int32_t *ckids,
-                                            const int32_t *lvc, int32_t nlev, bool &singular) {
+                                            const int32_t *lvc, int32_t nlev, double vscale, bool &singular) {
     constexpr int32_t T = NT;
     const int32_t tid = threadIdx.x;
     for (int32_t lv = 0; lv < nlev; ++lv) {
@@ -564,7 +564,7 @@ __device__ __forceinline__ void hines_exact(double *sd, double *sr, const double
                 }
                 x = (par >= 0 ? ri + ai * xp : ri) / di;
                 sr[top] = x;
-                sv[top] = sv[top] + x;
+                sv[top] = sv[top] + vscale * x;
             }
             for (int32_t i = top + 1; i <= bottom; ++i) {
                 const double ri = rn, ai = an, di = dn;
@@ -575,7 +575,7 @@ __device__ __forceinline__ void hines_exact(double *sd, double *sr, const double
                 }
                 x = (ri + ai * x) / di;
                 sr[i] = x;
-                sv[i] = sv[i] + x;
+                sv[i] = sv[i] + vscale * x;
             }
         }
         __syncthreads();
@@ -591,7 +591,7 @@ template <int NT>
 __device__ __forceinline__ void hines_mixed(double *sd, double *sr, const double *sa, double *sv, double *sxd,
                                             double *sxr, const int32_t *ctop, const int32_t *clen,
                                             const int32_t *cpar, const int32_t *ckoff, const int32_t *ckids,
-                                            const int32_t *lvc, int32_t nlev, bool &singular) {
+                                            const int32_t *lvc, int32_t nlev, double vscale, bool &singular) {
     constexpr int32_t T = NT;
     const int32_t tid = threadIdx.x;
     for (int32_t lv = 0; lv < nlev; ++lv) {
@@ -655,7 +655,7 @@ __device__ __forceinline__ void hines_mixed(double *sd, double *sr, const double
             double fn = sd[top], qn = sr[top];
             double x = par >= 0 ? fma(fn, sr[par], qn) : qn;
             sr[top] = x;
-            sv[top] = sv[top] + x;
+            sv[top] = sv[top] + vscale * x;
             if (top < bottom) {
                 fn = sd[top + 1];
                 qn = sr[top + 1];
@@ -668,7 +668,7 @@ __device__ __forceinline__ void hines_mixed(double *sd, double *sr, const double
                 }
                 x = fma(fi, x, qi);
                 sr[i] = x;
-                sv[i] = sv[i] + x;
+                sv[i] = sv[i] + vscale * x;
             }
         }
         __syncthreads();
@@ -1093,9 +1093,9 @@ __global__ void __launch_bounds__(NT, NT == kCellThreads ? 5 : NT == kCellThread
         // 6-7. Hines elimination level by level, each chain bottom to top into its parent,
         //      then back-substitution root chain first with the voltage update.
         if (MIXED) {
-            hines_mixed<NT>(sd, sr, sa, sv, sxd, sxr, ctop, clen, cpar, ckoff, ckids, lvc, nlev, singular);
+            hines_mixed<NT>(sd, sr, sa, sv, sxd, sxr, ctop, clen, cpar, ckoff, ckids, lvc, nlev, P.vscale, singular);
         } else {
-            hines_exact<NT>(sd, sr, sa, sv, sxd, sxr, ctop, clen, cpar, ckoff, ckids, lvc, nlev, singular);
+            hines_exact<NT>(sd, sr, sa, sv, sxd, sxr, ctop, clen, cpar, ckoff, ckids, lvc, nlev, P.vscale, singular);
         }
 
         // 8. cnexp state advance on the new voltage (time t + dt).

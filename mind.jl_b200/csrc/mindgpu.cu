@@ -346,7 +346,10 @@ bool valid_cell_threads(int32_t threads) {
 int create(const MindLayout *L, MindHandle *h) {
     if (!L) return fail(h, MIND_EARG, "null layout");
     if (L->abi_version != MIND_ABI_VERSION) return fail(h, MIND_ELAYOUT, "ABI version mismatch");
-    if (L->secondorder != 0) return fail(h, MIND_ELAYOUT, "only secondorder = 0 is supported");
+    // secondorder (src/runtime/step.jl:101-136, micro.jl:660-679): 1 and 2 assemble with
+    // C/(dt/2) and update v += 2 x; order 2's ion-current correction only feeds ion
+    // concentration mechanisms, which this runtime does not run, so 2 acts as 1 here.
+    if (L->secondorder < 0 || L->secondorder > 2) return fail(h, MIND_ELAYOUT, "secondorder must be 0, 1 or 2");
     if (!(L->dt > 0.0) || !std::isfinite(L->dt)) return fail(h, MIND_ELAYOUT, "dt must be positive");
     if (L->n_mechanisms > kMaxGroups) return fail(h, MIND_ELAYOUT, "too many mechanism groups");
     const int64_t n = L->n_nodes;
@@ -469,7 +472,7 @@ int create(const MindLayout *L, MindHandle *h) {
     for (int64_t j = 0; j < n; ++j) {
         int32_t i = layout_of_packed[j];
         a[j] = L->axial[i];
-        cdt[j] = L->capacitance[i] / L->dt;
+        cdt[j] = L->capacitance[i] / (L->secondorder == 0 ? L->dt : 0.5 * L->dt);
         ad[j] = L->axial_diagonal[i];
         v0[j] = L->voltage[i];
     }
@@ -481,6 +484,7 @@ int create(const MindLayout *L, MindHandle *h) {
     P.ngroups = L->n_mechanisms;
     P.dt = L->dt;
     P.celsius = L->celsius;
+    P.vscale = L->secondorder == 0 ? 1.0 : 2.0;
     P.seed = L->seed;
     P.ns_group = -1;
     std::vector<std::vector<int32_t>> &dev_row_of = h->dev_row_of;  // layout row -> device row

@@ -324,7 +324,7 @@ struct Oracle {
     int load(const MindLayout *layout) {
         L = layout;
         if (L->abi_version != MIND_ABI_VERSION) return fail(MIND_ELAYOUT, "ABI version");
-        if (L->secondorder != 0) return fail(MIND_ELAYOUT, "secondorder must be 0");
+        if (L->secondorder < 0 || L->secondorder > 2) return fail(MIND_ELAYOUT, "secondorder must be 0, 1 or 2");
         n = L->n_nodes;
         dt = L->dt;
         celsius = L->celsius;
@@ -746,7 +746,9 @@ struct Oracle {
 
     int cable(int64_t cell) {
         const std::vector<int32_t> &up = cell_up[cell];
-        for (int32_t i : up) d[i] = cap[i] / dt + d[i] + ad[i];
+        // secondorder 1 and 2 (src/runtime/step.jl:112): capacitance over dt/2
+        const double step_dt = L->secondorder == 0 ? dt : 0.5 * dt;
+        for (int32_t i : up) d[i] = cap[i] / step_dt + d[i] + ad[i];
         for (int32_t i : up) {
             double R = rhs[i];
             if (parent[i] >= 0) R = R + a[i] * (v[parent[i]] - v[i]);
@@ -779,7 +781,11 @@ struct Oracle {
             if (parent[i] >= 0) value = value + a[i] * rhs[parent[i]];
             rhs[i] = value / d[i];
         }
-        for (int32_t i : up) v[i] = v[i] + rhs[i];
+        // micro.jl:660-679: v += x, or v += 2 x for secondorder 1 and 2
+        if (L->secondorder == 0)
+            for (int32_t i : up) v[i] = v[i] + rhs[i];
+        else
+            for (int32_t i : up) v[i] = v[i] + 2.0 * rhs[i];
         return status;
     }
 

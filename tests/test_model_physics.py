@@ -29,6 +29,31 @@ def single_section(nseg=1, mech="pas", params=None, L=20.0, diam=20.0):
     return model, cell
 
 
+def test_secondorder_is_crank_nicolson():
+    """secondorder 1 and 2 (C/(dt/2) in the matrix, v += 2 x) step a passive compartment by
+    the trapezoidal rule, v_n = e + (v0 - e) ((1 - k/2)/(1 + k/2))^n with k = dt 1000 g / cm,
+    and its error against the exact exponential shrinks as dt^2 where backward Euler's
+    shrinks as dt."""
+    g, e, T = 1.0e-3, -70.0, 10.0
+    errors = {}
+    for order in (0, 1, 2):
+        for dt in (0.1, 0.05):
+            model, cell = single_section(params={"g": g, "e": e})
+            layout = mb.build(model, dt_micro=dt, secondorder=order)
+            steps = int(round(T / dt))
+            ref = oracle.run(layout, steps, [layout.voltage_node(1)])
+            assert ref.status == 0
+            k = dt * 1000.0 * g / 1.0
+            if order:
+                n = np.arange(steps + 1)
+                np.testing.assert_allclose(ref.trace[:, 0], e + (-65.0 - e) * ((1 - k / 2) / (1 + k / 2)) ** n,
+                                           rtol=0, atol=1e-9)
+            errors[order, dt] = abs(ref.trace[-1, 0] - (e + (-65.0 - e) * math.exp(-T * 1000.0 * g / 1.0)))
+    assert 1.8 < errors[0, 0.1] / errors[0, 0.05] < 2.2
+    assert 3.6 < errors[1, 0.1] / errors[1, 0.05] < 4.4
+    assert errors[1, 0.05] < 0.05 * errors[0, 0.05] and errors[2, 0.05] == errors[1, 0.05]
+
+
 def test_passive_decay_matches_backward_euler():
     g, e, dt, steps = 1.0e-3, -70.0, 0.025, 400
     model, cell = single_section(params={"g": g, "e": e})

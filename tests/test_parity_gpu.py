@@ -96,3 +96,24 @@ def test_mixed_precision_close_to_fp64():
         same = mixed.spike_times[mixed.spike_sources == sid]
         matched += np.any(np.abs(same - t) <= layout.dt + 1e-12)
     assert matched >= 0.9 * np.sum(cells)
+
+
+@pytest.mark.parametrize("order", [1, 2])
+def test_secondorder_crank_nicolson_fp64(order):
+    """build!(secondorder=1 or 2): the cable matrix with C/(dt/2) and v += 2 x, bit-exact
+    against the oracle on the recurrent tree network (spikes included)."""
+    from mind_b200.runtime import DeviceState
+
+    layout = mb.build(netcases.recurrent_trees(), secondorder=order)
+    nodes = netcases.soma_nodes(layout)
+    steps = 1600
+    ref = oracle.run(layout, steps, nodes)
+    assert ref.status == 0, ref.message
+    state = DeviceState(layout, "fp64")
+    state.initialize()
+    result = state.run_steps(steps, [mb.RecordSpec(n, f"n{n}") for n in nodes])
+    state.close()
+    assert np.array_equal(result.traces.by_record.T, ref.trace)
+    np.testing.assert_array_equal(result.spike_sources, ref.spike_sids)
+    np.testing.assert_array_equal(result.spike_times, ref.spike_times)
+    assert np.sum(ref.spike_sids < layout.n_cells) > 10
