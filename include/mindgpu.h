@@ -43,7 +43,7 @@
 extern "C" {
 #endif
 
-#define MIND_ABI_VERSION 1
+#define MIND_ABI_VERSION 2
 
 /* Status codes. 3/5/6/8 are the reference's error-word codes. */
 enum {
@@ -73,6 +73,7 @@ enum {
     MIND_MECH_NETSTIM = 5,  /* mod/NetStim.mod  artificial */
     MIND_MECH_ICLAMP = 6,   /* mod/IClamp.mod   point (electrode current) */
     MIND_MECH_ALPHASYN = 7, /* mod/AlphaSynapse.mod point: g = gmax alpha((t-onset)/tau), i = g (v-e) */
+    MIND_MECH_PATTERNSTIM = 8, /* mod/PatternStim.mod artificial: fires at prescribed times (MindLayout.pattern_*) */
     /* MIND_MECH_GENERATED + k: the k-th mechanism whose CUDA C was emitted from a MOD file
      * (BREAKPOINT, DERIVATIVE by cnexp, PROCEDURE by after_cvode, NET_RECEIVE, INITIAL) and
      * compiled into this library; mind_mechanism_info lists them with their fields. */
@@ -140,6 +141,14 @@ typedef struct MindLayout {
     uint64_t seed;                     /* build!(seed=) : Philox key */
     int64_t event_capacity;            /* events per delivery bin (ring slot) */
     int64_t spike_capacity;            /* recorded spikes per run */
+
+    /* PatternStim spike times (add_pointprocess!(...; spike_times), micro/model.jl:586-613),
+     * sorted by time (stable): at every mind_initialize each time becomes a firing of the
+     * spike sources fed by that PatternStim point (src/runtime/utils/events.jl:92-110) --
+     * recorded in the raster and routed through their NetCons. */
+    int64_t n_pattern;
+    const double *pattern_times;       /* [n_pattern] ms, >= 0 */
+    const int32_t *pattern_points;     /* [n_pattern] 1-based point (a PatternStim) */
 } MindLayout;
 
 /*

@@ -72,6 +72,11 @@ struct MindHandle {
     std::vector<int64_t> fanout;             // [n_sources+1] 0-based edge ranges
     std::vector<double> edge_delay;
     std::vector<uint8_t> source_external;    // no detector and no point: an inject_spike! input
+    struct PatternSpike {
+        double time;
+        int32_t source;                      // 0-based source fed by a PatternStim
+    };
+    std::vector<PatternSpike> pattern;       // PatternStim firings, in time order
     std::vector<uint8_t> source_detector;
     // regions coupled to the cells (mind_attach_macro)
     MacroParams M{};
@@ -244,6 +249,8 @@ KindSpec spec_of(int32_t kind) {
             return {kind, {"onset", "tau", "gmax", "e"}, AS_NSLOT, 0};
         case MIND_MECH_NETSTIM:
             return {kind, {"interval", "number", "start", "noise", "event", "on", "ispike"}, NS_NSLOT, 0};
+        case MIND_MECH_PATTERNSTIM:   // no fields: its spike times come with the layout
+            return {kind, {}, 0, 0};
         default:
             if (kind_generated(kind)) {   // every field of an emitted mechanism, in column order
                 const GenMechanism &g = kGenMechanisms[kind - MIND_MECH_GENERATED];
@@ -513,8 +520,8 @@ int create(const MindLayout *L, MindHandle *h) {
         }
         for (int32_t j = 0; j < m.n_fields; ++j)
             h->field_slot[g].push_back(readable_slot(m.kind, m.field_names ? m.field_names[j] : nullptr));
-        const bool artificial = m.kind == MIND_MECH_NETSTIM;
-        if (artificial) {
+        const bool artificial = m.kind == MIND_MECH_NETSTIM || m.kind == MIND_MECH_PATTERNSTIM;
+        if (m.kind == MIND_MECH_NETSTIM) {
             if (P.ns_group >= 0) return fail(h, MIND_ELAYOUT, "more than one NetStim group");
             P.ns_group = g;
         }
@@ -597,7 +604,7 @@ int create(const MindLayout *L, MindHandle *h) {
                 for (int32_t t = 0; t < kCellThreads; ++t) pc[t + 1] += pc[t];
             }
         }
-        if (artificial) {
+        if (m.kind == MIND_MECH_NETSTIM) {
             init.logical.resize(rows);
             for (int32_t r = 0; r < rows; ++r) init.logical[r] = m.logical_ids[perm[r]];
         }
@@ -634,6 +641,7 @@ int create(const MindLayout *L, MindHandle *h) {
     std::vector<std::vector<std::pair<int32_t, int32_t>>> det_by_cell(ncells);
     std::vector<double> det_thr_by_source(L->n_sources, 0.0);
     std::vector<int32_t> ns_source(P.ns_group >= 0 ? L->mechanisms[P.ns_group].rows : 0, -1);
+    std::vector<std::vector<int32_t>> pattern_sources(np);   // sources fed by each PatternStim point
     for (int64_t s = 0; s < L->n_sources; ++s) {
         int32_t node = L->source_nodes[s];
         int32_t point = L->source_points[s];
@@ -647,7 +655,19 @@ int create(const MindLayout *L, MindHandle *h) {
         } else if (point > 0) {
             int32_t g = point_group[point - 1];
             if (g == P.ns_group) ns_source[point_row[point - 1]] = (int32_t)s;
+            if (L->mechanisms[g].kind == MIND_MECH_PATTERNSTIM) pattern_sources[point - 1].push_back((int32_t)s);
         }
+    }
+    // PatternStim: every prescribed time fires the point's sources (replayed at each initialize)
+    if (L->n_pattern < 0 || (L->n_pattern > 0 && (!L->pattern_times || !L->pattern_points)))
+        return fail(h, MIND_ELAYOUT, "invalid PatternStim spike list");
+    for (int64_t k = 0; k < L->n_pattern; ++k) {
+        const int32_t point = L->pattern_points[k];
+        const double t = L->pattern_times[k];
+        if (point < 1 || point > np || L->mechanisms[point_group[point - 1]].kind != MIND_MECH_PATTERNSTIM)
+            return fail(h, MIND_ELAYOUT, "a PatternStim spike names a point that is not a PatternStim");
+        if (!(t >= 0.0) || !std::isfinite(t)) return fail(h, MIND_ELAYOUT, "PatternStim spike times must be >= 0");
+        for (int32_t s : pattern_sources[point - 1]) h->pattern.push_back({t, s});
     }
     std::vector<int32_t> det_off{0}, det_node, det_source;
     std::vector<double> det_thr;
@@ -781,7 +801,7 @@ int create(const MindLayout *L, MindHandle *h) {
     group_row_off.assign(L->n_mechanisms, {});
     for (int32_t g = 0; g < L->n_mechanisms; ++g) {
         group_row_off[g].assign(ncells + 1, 0);
-        if (kinds[g] == MIND_MECH_NETSTIM) continue;
+        if (kinds[g] == MIND_MECH_NETSTIM || kinds[g] == MIND_MECH_PATTERNSTIM) continue;
         for (int32_t r = 0; r < (int32_t)row_cell[g].size(); ++r) group_row_off[g][row_cell[g][r] + 1]++;
         for (int32_t c = 0; c < ncells; ++c) group_row_off[g][c + 1] += group_row_off[g][c];
     }
@@ -922,7 +942,7 @@ int resolve_record(MindHandle *h, const MindRecord &rec, RecordTarget &out) {
     const int32_t dev = h->dev_row_of[g][rec.row - 1];
     out.initial = kind_generated(kind) ? P.groups[g].cols + (int64_t)slot * P.groups[g].rows + dev
                                        : P.groups[g].f[slot] + dev;
-    if (kind == MIND_MECH_NETSTIM) {
+    if (kind == MIND_MECH_NETSTIM || kind == MIND_MECH_PATTERNSTIM) {
         out.cell = -1;   // artificial cells belong to no cell's window
         return MIND_OK;
     }
@@ -1315,6 +1335,11 @@ int mind_set_precision(MindHandle *h, int32_t mode) {
     return MIND_OK;
 }
 
+namespace {
+int reserve_injected(MindHandle *h);
+void push_injected(MindHandle *h, double time, int32_t edge, int32_t point);
+}  // namespace
+
 int mind_initialize(MindHandle *h) {
     if (!h) return MIND_EARG;
     Params &P = h->P;
@@ -1322,6 +1347,18 @@ int mind_initialize(MindHandle *h) {
     h->step = 0;
     h->injected.clear();
     h->injected_sorted = true;
+    // PatternStim firings (src/runtime/utils/events.jl:92-110): each prescribed time is a
+    // spike of the point's sources -- its raster entry and every NetCon event, queued now
+    // and moved into the delivery ring by the window that delivers them
+    for (const auto &ps : h->pattern) {
+        push_injected(h, ps.time, -1, ps.source);
+        for (int64_t e = h->fanout[ps.source]; e < h->fanout[ps.source + 1]; ++e)
+            push_injected(h, ps.time + h->edge_delay[e], (int32_t)e, h->edge_target[e]);
+    }
+    if (!h->pattern.empty()) {
+        const int status = reserve_injected(h);
+        if (status) return status;
+    }
     CUDA_TRY(h, cudaMemcpyAsync(P.v, h->v0_packed.data(), h->n_nodes * sizeof(double), cudaMemcpyHostToDevice,
                                 h->stream));
     CUDA_TRY(h, cudaMemsetAsync(P.error, 0, sizeof(int32_t), h->stream));

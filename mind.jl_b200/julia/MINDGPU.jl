@@ -17,11 +17,12 @@ module MINDGPU
 
 const libmindgpu = get(ENV, "MINDGPU_LIBRARY", joinpath(@__DIR__, "..", "lib", "libmindgpu.so"))
 
-const MIND_ABI_VERSION = Int32(1)
+const MIND_ABI_VERSION = Int32(2)
 const MIND_RECORD_VOLTAGE = Int32(1)
 const MIND_RECORD_MECHANISM = Int32(2)
 const KIND_CODES = Dict(:hh => Int32(1), :pas => Int32(2), :ExpSyn => Int32(3), :Exp2Syn => Int32(4),
-                        :NetStim => Int32(5), :IClamp => Int32(6), :AlphaSynapse => Int32(7))
+                        :NetStim => Int32(5), :IClamp => Int32(6), :AlphaSynapse => Int32(7),
+                        :PatternStim => Int32(8))
 
 # Kind code of a mechanism: the hand-written device code for the builtins above, else the
 # CUDA C emitted from its MOD file and compiled into the library (mind_mechanism_kind;
@@ -76,6 +77,9 @@ struct MindLayout
     seed::UInt64
     event_capacity::Int64
     spike_capacity::Int64
+    n_pattern::Int64
+    pattern_times::Ptr{Float64}
+    pattern_points::Ptr{Int32}
 end
 
 struct MindRecord
@@ -156,7 +160,10 @@ function mindgpu_initialize!(model; precision::Symbol = :fp64)
     nsrc = length(plan.source_ids)
     source_nodes = Int32[v === nothing || v.kind != :voltage ? 0 : Int32(v.row) for v in plan.source_variables]
     first_weights = plan.edge_weights[:, 1]
-    push!(keep, mechs, source_nodes, first_weights)
+    # PatternStim firings, already time-sorted by build! (micro/model.jl:586-613)
+    pattern_times = Vector{Float64}(plan.pattern_times)
+    pattern_points = Vector{Int32}(plan.pattern_targets)
+    push!(keep, mechs, source_nodes, first_weights, pattern_times, pattern_points)
     c = MindLayout(MIND_ABI_VERSION, Int32(layout.secondorder), length(plan.parent), pointer(plan.parent),
                    pointer(plan.voltage), pointer(plan.area), pointer(plan.capacitance), pointer(plan.axial),
                    pointer(plan.axial_diagonal), Int32(length(mechs)), pointer(mechs),
@@ -164,7 +171,8 @@ function mindgpu_initialize!(model; precision::Symbol = :fp64)
                    nsrc, pointer(plan.source_ids), pointer(source_nodes), pointer(plan.source_thresholds),
                    pointer(plan.source_targets), length(plan.edge_targets), pointer(plan.fanout_offsets),
                    pointer(plan.edge_targets), pointer(plan.edge_delays), pointer(first_weights),
-                   layout.dt_micro, plan.celsius, layout.seed, Int64(0), Int64(0))
+                   layout.dt_micro, plan.celsius, layout.seed, Int64(0), Int64(0),
+                   length(pattern_times), pointer(pattern_times), pointer(pattern_points))
     handle = Ref{Ptr{Cvoid}}(C_NULL)
     GC.@preserve keep c begin
         status = ccall((:mind_create, libmindgpu), Cint, (Ref{MindLayout}, Ref{Ptr{Cvoid}}), c, handle)

@@ -11,7 +11,7 @@ import ctypes
 import os
 from ctypes import (POINTER, Structure, c_char_p, c_double, c_int32, c_int64, c_uint64, c_void_p)
 
-MIND_ABI_VERSION = 1
+MIND_ABI_VERSION = 2
 
 MIND_OK = 0
 MIND_ECAPACITY = 3
@@ -85,6 +85,9 @@ class MindLayout(Structure):
         ("seed", c_uint64),
         ("event_capacity", c_int64),
         ("spike_capacity", c_int64),
+        ("n_pattern", c_int64),
+        ("pattern_times", POINTER(c_double)),
+        ("pattern_points", POINTER(c_int32)),
     ]
 
 

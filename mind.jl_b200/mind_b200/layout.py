@@ -76,6 +76,9 @@ class Layout:
     event_capacity: int
     spike_capacity: int
     secondorder: int = 0
+    # PatternStim firings sorted by time (stable, point order), micro/model.jl:586-613
+    pattern_times: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    pattern_points: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
     # Host-side maps for references (voltage_ref) and reporting.
     cell_offsets: np.ndarray = None
     cell_morphology: np.ndarray = None
@@ -159,6 +162,9 @@ class Layout:
         c.seed = self.seed
         c.event_capacity = self.event_capacity
         c.spike_capacity = self.spike_capacity
+        c.n_pattern = len(self.pattern_times)
+        c.pattern_times = ptr(np.asarray(self.pattern_times, dtype=np.float64), ctypes.c_double)
+        c.pattern_points = ptr(np.asarray(self.pattern_points, dtype=np.int32), ctypes.c_int32)
         self._keep = keep
         return c
 
@@ -320,6 +326,18 @@ def build(model, *, dt_micro: float = 0.025, seed: int = 1, event_capacity: Opti
     connection_edges = np.empty(len(src), dtype=np.int64)
     connection_edges[order] = np.arange(1, len(src) + 1)
 
+    # 5. PatternStim spike times, point order, then stably by time.
+    p_times, p_points = [], []
+    for chunk in model.point_chunks:
+        if chunk.spike_times:
+            for k, times in enumerate(chunk.spike_times):
+                p_times.append(times)
+                p_points.append(np.full(len(times), chunk.first + k, dtype=np.int32))
+    pattern_times = np.concatenate(p_times) if p_times else np.zeros(0)
+    pattern_points = np.concatenate(p_points) if p_points else np.zeros(0, np.int32)
+    by_time = np.argsort(pattern_times, kind="stable")
+    pattern_times, pattern_points = pattern_times[by_time], pattern_points[by_time]
+
     n_events = event_capacity if event_capacity is not None else 0
     n_spikes = spike_capacity if spike_capacity is not None else 0
     layout = Layout(
@@ -330,6 +348,7 @@ def build(model, *, dt_micro: float = 0.025, seed: int = 1, event_capacity: Opti
         edge_delays=dly[order].astype(np.float64), edge_weights=wts[order].astype(np.float64),
         connection_edges=connection_edges, dt=dt, celsius=model.celsius, seed=int(seed),
         event_capacity=int(n_events), spike_capacity=int(n_spikes), secondorder=int(secondorder),
+        pattern_times=pattern_times, pattern_points=pattern_points,
         cell_offsets=offsets, cell_morphology=cell_morph, morphologies=morphs,
         segment_count=int(segment_count),
     )

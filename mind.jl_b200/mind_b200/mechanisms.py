@@ -26,6 +26,7 @@ MIND_MECH_EXP2SYN = 4
 MIND_MECH_NETSTIM = 5
 MIND_MECH_ICLAMP = 6
 MIND_MECH_ALPHASYN = 7
+MIND_MECH_PATTERNSTIM = 8
 
 
 @dataclass(frozen=True)
@@ -111,6 +112,8 @@ _BUILTINS: Dict[str, Mechanism] = {
         [("del", 0.0), ("dur", 0.0), ("amp", 0.0), ("i", 0.0)],
         0x6EB0551A76C267F8,
     ),
+    # an artificial cell that fires at the spike_times given to add_pointprocess
+    "PatternStim": _mechanism("PatternStim", "artificial", MIND_MECH_PATTERNSTIM, [], 0x053F906BDBA59243),
 }
 
 

@@ -69,6 +69,7 @@ class PointChunk:
     sections: Union[str, Sequence[str]]
     xs: np.ndarray
     params: Dict[str, Any]
+    spike_times: Optional[List[np.ndarray]] = None   # PatternStim: each member's firing times (ms)
 
 
 @dataclass
@@ -234,20 +235,23 @@ def insert(cell: Cell, mechanism, *, sections="all", params: Optional[Dict[str, 
 
 
 def add_pointprocess(target: Union[Cell, MicroModel], mechanism, *, section="soma", x=0.5,
-                     params: Optional[Dict[str, Any]] = None) -> PointProcess:
-    """Create one point process on a cell, or one artificial cell on the model."""
+                     params: Optional[Dict[str, Any]] = None, spike_times=()) -> PointProcess:
+    """Create one point process on a cell, or one artificial cell on the model
+    (add_pointprocess!, src/model/micro/model.jl:178-193); `spike_times` are the firing
+    times of a PatternStim."""
     if isinstance(target, Cell):
         model, cell = target.model, target.index
     else:
         model, cell = target, 0
     first = add_pointprocesses(model, mechanism, np.array([cell]), section, np.array([float(x)]),
-                               params or {})
+                               params or {}, spike_times=[spike_times])
     return PointProcess(model, first)
 
 
 def add_pointprocesses(model: MicroModel, mechanism, cells, sections, xs,
-                       params: Optional[Dict[str, Any]] = None) -> int:
-    """Bulk variant: len(cells) point processes; params values may be arrays. Returns the first index."""
+                       params: Optional[Dict[str, Any]] = None, spike_times=None) -> int:
+    """Bulk variant: len(cells) point processes; params values may be arrays; `spike_times`,
+    one sequence per member, only for PatternStim.  Returns the first index."""
     compiled = resolve_mechanism(mechanism)
     cells = np.asarray(cells, dtype=np.int64).reshape(-1)
     xs = np.asarray(xs, dtype=np.float64).reshape(-1)
@@ -265,8 +269,17 @@ def add_pointprocesses(model: MicroModel, mechanism, cells, sections, xs,
         arr = np.asarray(value, dtype=np.float64)
         if not np.all(np.isfinite(arr)):
             raise ValueError(f"non-finite value for {name}")
+    times = None
+    if spike_times is not None and any(len(t) for t in spike_times):
+        if compiled.name != "PatternStim":
+            raise ValueError("spike_times applies to PatternStim only")
+        if len(spike_times) != len(cells):
+            raise ValueError("one spike_times sequence per point")
+        times = [np.asarray(t, dtype=np.float64).reshape(-1) for t in spike_times]
+        if any(np.any(~np.isfinite(t) | (t < 0.0)) for t in times):
+            raise ValueError("PatternStim spike times must be finite and >= 0")
     first = model.point_count + 1
-    model.point_chunks.append(PointChunk(compiled, first, len(cells), cells, sections, xs, params))
+    model.point_chunks.append(PointChunk(compiled, first, len(cells), cells, sections, xs, params, times))
     model.point_count += len(cells)
     return first
 

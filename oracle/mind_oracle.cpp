@@ -378,6 +378,7 @@ struct Oracle {
                 case MIND_MECH_ALPHASYN: names = AS_NAMES; nf = AS_NF; break;
                 case ORACLE_SECLAMP: names = SE_NAMES; nf = SE_NF; break;
                 case ORACLE_VCLAMP: names = VC_NAMES; nf = VC_NF; break;
+                case MIND_MECH_PATTERNSTIM: names = nullptr; nf = 0; break;
                 default: return fail(MIND_ELAYOUT, "unsupported mechanism kind");
             }
             G.f.resize(nf);
@@ -543,6 +544,11 @@ struct Oracle {
                 }
             }
         }
+        // PatternStim: each prescribed time fires the sources its point feeds
+        // (src/runtime/utils/events.jl:92-110), queued in time order.
+        for (int64_t k = 0; k < L->n_pattern; ++k)
+            for (int64_t s = 0; s < L->n_sources; ++s)
+                if (L->source_points[s] == L->pattern_points[k]) enqueue(L->pattern_times[k], 0.0, 0, -(int32_t)(s + 1));
         // NetStim INITIAL, groups in order, rows in order (t = 0).
         for (size_t g = 0; g < groups.size(); ++g) {
             Group &G = groups[g];
@@ -579,6 +585,10 @@ struct Oracle {
     }
 
     void receive(const Event &e) {
+        if (e.target < 0) {   // a PatternStim firing of source -target - 1 (events.jl:92-110)
+            emit_spike(-(int64_t)e.target - 1, e.time);
+            return;
+        }
         int32_t point = e.target;
         int32_t g = L->point_group[point - 1] - 1;
         int64_t r = L->point_row[point - 1] - 1;

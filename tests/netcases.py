@@ -275,3 +275,27 @@ def mechanism_mix(select, n_cells=12, synapses=12, seed=9, clamps=False):
                              {"dur[0]": 6.0, "dur[1]": 9.0, "dur[2]": 6.0, "amp[0]": -68.0, "amp[1]": -25.0,
                               "amp[2]": -55.0})
     return model
+
+
+def pattern_driven(n_cells=4, seed=6):
+    """Ball-and-stick cells driven only by two PatternStims (prescribed spike trains) through
+    Exp2Syn NetCons; returns (model, {PatternStim source sid: its spike times})."""
+    rng = np.random.default_rng(seed)
+    model = M.MicroModel(celsius=6.3)
+    soma = mb.Section("soma", label="soma", length=20.0, diameter=20.0, nseg=1)
+    dend = mb.Section("dend", label="dend", parent="soma", parent_x=1.0, length=200.0, diameter=2.0, nseg=10)
+    cells = M.add_population(model, [soma, dend], n_cells, voltage=-65.0)
+    for cell in cells:
+        M.insert(cell, mb.builtin("hh"), sections="soma")
+        M.insert(cell, mb.builtin("pas"), sections="dend", params={"g": 1e-4, "e": -65.0})
+        M.register_spike_source(cell, threshold=-10.0)
+    syn = M.add_pointprocesses(model, mb.builtin("Exp2Syn"), np.arange(1, n_cells + 1), "dend", np.full(n_cells, 0.3),
+                               {"tau1": 0.5, "tau2": 5.0, "e": 0.0})
+    trains = {}
+    for k, times in enumerate(([1.0, 4.0, 4.0, 9.5, 20.0], np.sort(rng.uniform(0.0, 30.0, 12)))):
+        stim = M.add_pointprocess(model, mb.builtin("PatternStim"), spike_times=times)
+        source = M.register_spike_source(stim)
+        trains[source.sid] = np.asarray(times, dtype=float)
+        M.connect_many(model, np.full(n_cells, source.index), np.arange(syn, syn + n_cells),
+                       np.full(n_cells, 0.012 if k == 0 else 0.004), rng.uniform(0.5, 2.0, n_cells))
+    return model, trains

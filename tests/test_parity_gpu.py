@@ -117,3 +117,20 @@ def test_secondorder_crank_nicolson_fp64(order):
     np.testing.assert_array_equal(result.spike_sources, ref.spike_sids)
     np.testing.assert_array_equal(result.spike_times, ref.spike_times)
     assert np.sum(ref.spike_sids < layout.n_cells) > 10
+
+
+def test_patternstim_trains_fp64():
+    """PatternStim firings replayed at initialize match the oracle bit for bit, twice (the
+    second initialize replays them again)."""
+    model, trains = netcases.pattern_driven()
+    layout = mb.build(model)
+    nodes = netcases.soma_nodes(layout)
+    ref = oracle.run(layout, 1400, nodes)
+    assert ref.status == 0, ref.message
+    for _ in range(2):
+        result, trace = run_gpu(model, 1400 * layout.dt, nodes)
+        assert np.array_equal(trace, ref.trace)
+        np.testing.assert_array_equal(result.spike_sources, ref.spike_sids)
+        np.testing.assert_array_equal(result.spike_times, ref.spike_times)
+    for sid, times in trains.items():
+        np.testing.assert_array_equal(result.spike_times[result.spike_sources == sid], np.sort(times))
