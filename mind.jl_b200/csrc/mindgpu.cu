@@ -1107,7 +1107,10 @@ int advance(MindHandle *h, int64_t steps, bool record_spikes) {
         // With regions attached, windows stay inside multiples of the window length (a
         // divisor of the rate bin), so a bin is complete before the regions read it.
         if (M.n > 0) W = (int32_t)std::min<int64_t>(W, h->window - n0 % h->window);
-        const double horizon = (double)(n0 + W - 1) * P.dt + 0.5 * P.dt;
+        // NetStim self-events through the window's end boundary, as the reference's delivery
+        // at the end of every step (time <= t + dt, src/runtime/step.jl:148): their spikes
+        // enter this run's raster, their NetCon events the next window's bins
+        const double horizon = (double)(n0 + W) * P.dt;
         if (M.n > 0) {
             const int64_t spm = M.steps_per_macro;
             const int64_t k0 = (n0 + spm - 1) / spm, k1 = (n0 + W + spm - 1) / spm;
@@ -1703,9 +1706,22 @@ int reserve_injected(MindHandle *h) {
     return MIND_OK;
 }
 
+/* The step whose end-of-step delivery (time <= (m + 1) dt, src/runtime/step.jl:148) reaches
+ * `time`: the smallest m >= 0 with time <= (m + 1) dt.  A spike's raster entry is recorded by
+ * the window of that step, as the reference records it when that delivery pops it. */
+int64_t record_step(double time, double dt) {
+    double estimate = std::ceil(time / dt) - 1.0;
+    int64_t m = estimate < 0.0 ? 0 : (int64_t)estimate;
+    for (int k = 0; k < 4 && m > 0 && time <= (double)m * dt; ++k) --m;
+    for (int k = 0; k < 4 && time > (double)(m + 1) * dt; ++k) ++m;
+    return m;
+}
+
 void push_injected(MindHandle *h, double time, int32_t edge, int32_t point) {
     MindHandle::Injected e;
-    e.bin = delivery_bin(time, h->dt);
+    // a NetCon event waits for the step that delivers it; a raster entry (edge < 0) for the
+    // step whose end delivery covers its time
+    e.bin = edge >= 0 ? delivery_bin(time, h->dt) : record_step(time, h->dt);
     e.event.time = time;
     e.event.edge = edge;
     e.event.point = point;
