@@ -133,8 +133,7 @@ __host__ __device__ inline int staged_doubles(int32_t kind) {
  *            slots of the staged rows;
  *   events   the cell's inbox for the window [inbox_cap];
  *   ints     per staged row: local node; chain top, length,
- *            parent, child-chain CSR; level starts; inbox order; the
- *            threads' row ranges per group [ngroups][threads + 1];
+ *            parent, child-chain CSR; level starts; inbox order;
  *   shorts   chain of every node [n].
  * Host (to size the launch) and device (to carve the buffer) use this one function.
  */
@@ -153,7 +152,6 @@ __host__ __device__ inline size_t cell_smem_bytes(const CellShape &s, const int3
         ints += (size_t)s.rows[g];
     }
     ints += 4 * (size_t)s.nch + 1 + (size_t)s.nkids + (size_t)s.nlev + 1 + (size_t)inbox_cap;
-    ints += (size_t)ngroups * (kCellThreads + 1);
     return doubles * 8 + (size_t)inbox_cap * sizeof(InboxEvent) + ints * 4 + 2 * (size_t)s.n;
 }
 

@@ -582,10 +582,197 @@ __device__ __forceinline__ void hines_exact(double *sd, double *sr, const double
     }
 }
 
+/* ---- long unbranched chains in the mixed mode: one warp per chain ----
+ *
+ * A chain's elimination is a recurrence from its bottom node up, D_i = d_i - a_{i+1}^2 / D_{i+1}
+ * and R_i = r_i + (a_{i+1} / D_{i+1}) R_{i+1}, and its back-substitution one from the top down,
+ * x_i = (a_i / D_i) x_{i-1} + R_i / D_i.  On a chain of L nodes one thread takes L dependent
+ * steps.  A warp splits the chain into 32 consecutive segments: each lane composes its
+ * segment's steps (the D step is the Mobius map D -> (d D - a^2) / D, a 2x2 matrix; the R and x
+ * steps are affine maps), a warp scan composes the segments, and each lane then runs the
+ * ordinary recurrence over its own segment from the value the scan gives at its boundary.
+ * The depth falls from L to about 2 L / 32 + 5 combining steps.  Only the rounding of the
+ * boundary values changes, so this is used in the mixed mode only; the FP64 mode keeps the
+ * oracle's sequential order. */
+constexpr int32_t kWarpChain = 24;   // chains at least this long are solved by a warp (mixed mode)
+
+struct Mobius {   // x -> (a x + b) / (c x + d)
+    double a, b, c, d;
+};
+struct Affine {   // x -> m x + c
+    double m, c;
+};
+
+/* l after r, rescaled by a power of two (exact) so long products neither overflow nor underflow. */
+__device__ __forceinline__ Mobius mobius_after(const Mobius &l, const Mobius &r) {
+    Mobius p{l.a * r.a + l.b * r.c, l.a * r.b + l.b * r.d, l.c * r.a + l.d * r.c, l.c * r.b + l.d * r.d};
+    const double big = fmax(fmax(fabs(p.a), fabs(p.b)), fmax(fabs(p.c), fabs(p.d)));
+    if (big > 0.0 && isfinite(big)) {
+        const int e = ilogb(big);
+        p.a = ldexp(p.a, -e);
+        p.b = ldexp(p.b, -e);
+        p.c = ldexp(p.c, -e);
+        p.d = ldexp(p.d, -e);
+    }
+    return p;
+}
+__device__ __forceinline__ Affine affine_after(const Affine &l, const Affine &r) { return {l.m * r.m, l.m * r.c + l.c}; }
+
+/* Exclusive warp scans (lane k gets the composition of lanes 0 .. k-1; lane 0 the identity). */
+__device__ __forceinline__ Mobius warp_exclusive(Mobius v, int lane) {
+    for (int off = 1; off < 32; off <<= 1) {
+        const Mobius o{__shfl_up_sync(0xffffffffu, v.a, off), __shfl_up_sync(0xffffffffu, v.b, off),
+                       __shfl_up_sync(0xffffffffu, v.c, off), __shfl_up_sync(0xffffffffu, v.d, off)};
+        if (lane >= off) v = mobius_after(v, o);
+    }
+    Mobius e{__shfl_up_sync(0xffffffffu, v.a, 1), __shfl_up_sync(0xffffffffu, v.b, 1),
+             __shfl_up_sync(0xffffffffu, v.c, 1), __shfl_up_sync(0xffffffffu, v.d, 1)};
+    if (lane == 0) e = Mobius{1.0, 0.0, 0.0, 1.0};
+    return e;
+}
+__device__ __forceinline__ Affine warp_exclusive(Affine v, int lane) {
+    for (int off = 1; off < 32; off <<= 1) {
+        const Affine o{__shfl_up_sync(0xffffffffu, v.m, off), __shfl_up_sync(0xffffffffu, v.c, off)};
+        if (lane >= off) v = affine_after(v, o);
+    }
+    Affine e{__shfl_up_sync(0xffffffffu, v.m, 1), __shfl_up_sync(0xffffffffu, v.c, 1)};
+    if (lane == 0) e = Affine{1.0, 0.0};
+    return e;
+}
+
+/* Calls f(ch) for the chains in [lo, hi) of at least kWarpChain nodes, each on one warp of the
+ * CTA in turn; every lane of every warp runs this with the same lo, hi. */
+template <int NT, class F>
+__device__ __forceinline__ void for_each_long_chain(const int32_t *clen, int32_t lo, int32_t hi, F f) {
+    constexpr int32_t NW = NT / 32;
+    const int32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int32_t k = 0;
+    __syncwarp();
+    for (int32_t base = lo; base < hi; base += 32) {
+        const int32_t ch = base + lane;
+        uint32_t mask = __ballot_sync(0xffffffffu, ch < hi && clen[ch] >= kWarpChain);
+        while (mask) {
+            const int32_t j = __ffs(mask) - 1;
+            mask &= mask - 1;
+            if (k % NW == warp) f(base + j);
+            ++k;
+        }
+    }
+}
+
+/* Elimination of one long chain by a warp, with the mixed mode's arithmetic (reciprocal
+ * pivots): leaves f = a/D in sd and R/D in sr for its nodes, and the chain's contribution to
+ * its parent node in sxd, sxr. */
+__device__ __forceinline__ void eliminate_chain_warp(int32_t ch, double *sd, double *sr, const double *sa,
+                                                     double *sxd, double *sxr, const int32_t *ctop,
+                                                     const int32_t *clen, const int32_t *cpar,
+                                                     const int32_t *ckoff, const int32_t *ckids, bool &singular) {
+    const int32_t lane = threadIdx.x & 31;
+    const int32_t top = ctop[ch], L = clen[ch], bottom = top + L - 1;
+    // the bottom pivot and rhs with the child chains' contributions, in child order, on every lane
+    double Db = sd[bottom], Rb = sr[bottom];
+    for (int32_t q = ckoff[ch]; q < ckoff[ch + 1]; ++q) {
+        Db = Db - sxd[ckids[q]];
+        Rb = Rb + sxr[ckids[q]];
+    }
+    // this lane's positions p (p = 0 is the bottom node, node = bottom - p)
+    const int32_t S = (L + 31) / 32;
+    const int32_t p0 = min(L, lane * S), p1 = min(L, p0 + S), first = max(p0, 1);
+    // 1. pivots D
+    Mobius T{1.0, 0.0, 0.0, 1.0};
+    for (int32_t p = first; p < p1; ++p) {
+        const int32_t i = bottom - p;
+        const double an = sa[i + 1];
+        T = mobius_after(Mobius{sd[i], -(an * an), 1.0, 0.0}, T);
+    }
+    const Mobius E = warp_exclusive(T, lane);
+    double Dprev = (E.a * Db + E.b) / (E.c * Db + E.d);   // D at position p0 - 1 (p0 = 0: the bottom's own)
+    if (p0 == 0 && L > 0) {
+        Dprev = Db;
+        singular |= (Db == 0.0) | !isfinite(Db);
+        sd[bottom] = Db;
+    }
+    for (int32_t p = first; p < p1; ++p) {
+        const int32_t i = bottom - p;
+        const double an = sa[i + 1];
+        const double Di = sd[i] - (an * an) * approx_reciprocal(Dprev);
+        singular |= (Di == 0.0) | !isfinite(Di);
+        sd[i] = Di;
+        Dprev = Di;
+    }
+    __syncwarp();
+    // 2. right-hand sides R (the step into position p multiplies by f of position p - 1)
+    Affine A{1.0, 0.0};
+    for (int32_t p = first; p < p1; ++p) {
+        const int32_t i = bottom - p;
+        const double fn = sa[i + 1] * approx_reciprocal(sd[i + 1]);
+        A = affine_after(Affine{fn, sr[i]}, A);
+    }
+    const Affine F = warp_exclusive(A, lane);
+    double Rprev = F.m * Rb + F.c;
+    if (p0 == 0 && L > 0) {
+        Rprev = Rb;
+        sr[bottom] = Rb;
+    }
+    for (int32_t p = first; p < p1; ++p) {
+        const int32_t i = bottom - p;
+        const double fn = sa[i + 1] * approx_reciprocal(sd[i + 1]);
+        const double Ri = sr[i] + fn * Rprev;
+        sr[i] = Ri;
+        Rprev = Ri;
+    }
+    __syncwarp();
+    // 3. f = a/D and R/D in place; the top node's contribution to the parent
+    for (int32_t p = p0; p < p1; ++p) {
+        const int32_t i = bottom - p;
+        const double y = approx_reciprocal(sd[i]);
+        const double ai = sa[i];
+        const double fi = ai * y;
+        const double Ri = sr[i];
+        if (p == L - 1) {
+            const bool rooted = cpar[ch] < 0;
+            sxd[ch] = rooted ? 0.0 : (ai * ai) * y;
+            sxr[ch] = rooted ? 0.0 : fi * Ri;
+        }
+        sd[i] = fi;
+        sr[i] = Ri * y;
+    }
+    __syncwarp();
+}
+
+/* Back-substitution of one long chain by a warp (mixed mode): x = f x_prev + R/D from the
+ * chain's top, the top continuing its parent node's solution. */
+__device__ __forceinline__ void substitute_chain_warp(int32_t ch, double *sd, double *sr, double *sv,
+                                                      const int32_t *ctop, const int32_t *clen, const int32_t *cpar,
+                                                      double vscale) {
+    const int32_t lane = threadIdx.x & 31;
+    const int32_t top = ctop[ch], L = clen[ch], par = cpar[ch];
+    const double xp = par >= 0 ? sr[par] : 0.0;
+    const int32_t S = (L + 31) / 32;
+    const int32_t u0 = min(L, lane * S), u1 = min(L, u0 + S);
+    Affine A{1.0, 0.0};
+    for (int32_t u = u0; u < u1; ++u) {
+        const int32_t i = top + u;
+        A = affine_after(Affine{(u == 0 && par < 0) ? 0.0 : sd[i], sr[i]}, A);
+    }
+    const Affine F = warp_exclusive(A, lane);
+    double x = F.m * xp + F.c;   // x at position u0 - 1 (u0 = 0: the parent's)
+    __syncwarp();
+    for (int32_t u = u0; u < u1; ++u) {
+        const int32_t i = top + u;
+        x = (u == 0 && par < 0) ? sr[i] : fma(sd[i], x, sr[i]);
+        sr[i] = x;
+        sv[i] = sv[i] + vscale * x;
+    }
+    __syncwarp();
+}
+
 /*
  * Hines solve, mixed mode: FP64 arithmetic with reciprocals.  Elimination keeps, per
  * node, f = a/D in place of D and R/D in place of R, so the back-substitution is one
  * FMA per node, x = f x_p + R/D; the pivot chain is D -> 1/D -> (a^2)(1/D) -> next D.
+ * Chains of kWarpChain nodes or more go to a warp each (eliminate_chain_warp,
+ * substitute_chain_warp); the others to one thread each.
  */
 template <int NT>
 __device__ __forceinline__ void hines_mixed(double *sd, double *sr, const double *sa, double *sv, double *sxd,
@@ -596,6 +783,7 @@ __device__ __forceinline__ void hines_mixed(double *sd, double *sr, const double
     const int32_t tid = threadIdx.x;
     for (int32_t lv = 0; lv < nlev; ++lv) {
         for (int32_t ch = lvc[lv] + tid; ch < lvc[lv + 1]; ch += T) {
+            if (clen[ch] >= kWarpChain) continue;   // a warp's, below
             const int32_t top = ctop[ch];
             const int32_t bottom = top + clen[ch] - 1;
             const bool rooted = cpar[ch] < 0;
@@ -645,10 +833,14 @@ __device__ __forceinline__ void hines_mixed(double *sd, double *sr, const double
             sxd[ch] = rooted ? 0.0 : pxd;
             sxr[ch] = rooted ? 0.0 : pxr;
         }
+        for_each_long_chain<NT>(clen, lvc[lv], lvc[lv + 1], [&](int32_t ch) {
+            eliminate_chain_warp(ch, sd, sr, sa, sxd, sxr, ctop, clen, cpar, ckoff, ckids, singular);
+        });
         __syncthreads();
     }
     for (int32_t lv = nlev - 1; lv >= 0; --lv) {
         for (int32_t ch = lvc[lv] + tid; ch < lvc[lv + 1]; ch += T) {
+            if (clen[ch] >= kWarpChain) continue;   // a warp's, below
             const int32_t top = ctop[ch];
             const int32_t bottom = top + clen[ch] - 1;
             const int32_t par = cpar[ch];
@@ -671,6 +863,9 @@ __device__ __forceinline__ void hines_mixed(double *sd, double *sr, const double
                 sv[i] = sv[i] + vscale * x;
             }
         }
+        for_each_long_chain<NT>(clen, lvc[lv], lvc[lv + 1], [&](int32_t ch) {
+            substitute_chain_warp(ch, sd, sr, sv, ctop, clen, cpar, vscale);
+        });
         __syncthreads();
     }
 }
@@ -746,7 +941,9 @@ __global__ void __launch_bounds__(NT, NT == kCellThreads ? 5 : NT == kCellThread
     int32_t *ckids = ip; ip += nkids;
     int32_t *lvc = ip; ip += nlev + 1;
     int32_t *sorder = ip; ip += P.inbox_cap;
-    int32_t *spart = ip; ip += P.ngroups * (O + 1);
+    // each thread's row ranges per group are read from HBM through the read-only cache
+    // (two loads per group and step, L1-resident): staging them would cost 2 KB per cell
+    const int32_t *__restrict__ gpart = P.part + (int64_t)c * P.ngroups * (O + 1);
     int16_t *chain_of = reinterpret_cast<int16_t *>(ip);
     {
         // The launch sized the image for this cell's bin; refuse rather than overrun.
@@ -812,7 +1009,6 @@ __global__ void __launch_bounds__(NT, NT == kCellThreads ? 5 : NT == kCellThread
     if (tid == 0) ckoff[nch] = nkids;
     for (int32_t k = tid; k < nkids; k += T) ckids[k] = P.chain_kids[kb + k];
     for (int32_t k = tid; k <= nlev; k += T) lvc[k] = P.level_chain[lv0 + k];
-    for (int32_t k = tid; k < P.ngroups * (O + 1); k += T) spart[k] = P.part[(int64_t)c * P.ngroups * (O + 1) + k];
     __syncthreads();
     for (int32_t k = tid; k < nch; k += T)
         for (int32_t i = ctop[k]; i < ctop[k] + clen[k]; ++i) chain_of[i] = (int16_t)k;
@@ -945,7 +1141,7 @@ __global__ void __launch_bounds__(NT, NT == kCellThreads ? 5 : NT == kCellThread
             const DevGroup &GG = P.groups[g];
             const StagedGroup G = sg[g];
             for (int32_t slot = tid; slot < O; slot += T) {
-                const int32_t lo = spart[g * (O + 1) + slot], hi = spart[g * (O + 1) + slot + 1];
+                const int32_t lo = __ldg(gpart + g * (O + 1) + slot), hi = __ldg(gpart + g * (O + 1) + slot + 1);
                 if (lo >= hi) continue;
                 if (G.kind == MIND_MECH_PAS) {
                     if (MIXED) continue;  // folded into the node constants of the assembly below

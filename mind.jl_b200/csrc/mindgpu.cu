@@ -767,9 +767,9 @@ int create(const MindLayout *L, MindHandle *h) {
     P.ring = h->alloc<RingEvent>((size_t)P.ring_slots * P.ring_cap);
     P.ring_count = h->alloc<int32_t>(P.ring_slots);
     // Inbox: the events of one window by cell (a CSR rebuilt per window).  A window holds at
-    // most kMaxWindow bins of at most ring_cap events; each cell stages up to 64 of its events
+    // most kMaxWindow bins of at most ring_cap events; each cell stages up to 32 of its events
     // in shared memory and sorts any more in HBM.
-    P.inbox_cap = 64;
+    P.inbox_cap = 32;
     P.inbox_total = (int32_t)std::min<int64_t>((int64_t)kMaxWindow * P.ring_cap, INT32_MAX / 2);
     P.inbox = h->alloc<InboxEvent>((size_t)P.inbox_total);
     P.inbox_order = h->alloc<int32_t>((size_t)P.inbox_total);

@@ -10,6 +10,7 @@ import pytest
 import mind_b200 as mb
 import netcases
 import oracle
+from mind_b200 import model as M
 from mind_b200 import networks
 
 pytestmark = pytest.mark.gpu
@@ -134,3 +135,35 @@ def test_patternstim_trains_fp64():
         np.testing.assert_array_equal(result.spike_times, ref.spike_times)
     for sid, times in trains.items():
         np.testing.assert_array_equal(result.spike_times[result.spike_sources == sid], np.sort(times))
+
+
+def test_mixed_long_chains_close_to_fp64():
+    """Chains of 24 nodes or more are eliminated and back-substituted by a whole warp in the
+    mixed mode (segment scans).  On cells whose dendrites are single chains of 60 to 400
+    nodes, driven to spike: subthreshold |dV| against FP64 stays below 1e-3 mV and every
+    FP64 spike has a mixed-mode spike of the same cell within one dt (tolerances of this
+    test); two mixed runs are identical."""
+    model = M.MicroModel(celsius=6.3)
+    for nseg in (60, 150, 400):
+        soma = mb.Section("soma", label="soma", length=20.0, diameter=20.0, nseg=1)
+        dend = mb.Section("dend", label="dend", parent="soma", parent_x=1.0, length=2.0 * nseg, diameter=2.0,
+                          nseg=nseg)
+        side = mb.Section("side", label="dend", parent="dend", parent_x=0.5, length=100.0, diameter=1.0, nseg=40)
+        cell = M.add_population(model, [soma, dend, side], 1, voltage=-65.0)[0]
+        M.insert(cell, mb.builtin("hh"), sections="soma")
+        M.insert(cell, mb.builtin("pas"), sections="dend", params={"g": 1e-4, "e": -65.0})
+        M.register_spike_source(cell, threshold=-10.0)
+    M.add_pointprocesses(model, mb.builtin("IClamp"), np.array([1, 2, 3]), "soma", np.full(3, 0.5),
+                         {"del": 2.0, "dur": 40.0, "amp": 0.4})
+    layout = mb.build(model)
+    nodes = netcases.soma_nodes(layout)
+    fp64, t64 = run_gpu(model, 50.0, nodes, "fp64")
+    mixed, t32 = run_gpu(model, 50.0, nodes, "mixed")
+    again, t32b = run_gpu(model, 50.0, nodes, "mixed")
+    assert np.array_equal(t32, t32b)
+    sub = (t64 < -55.0) & (t32 < -55.0)
+    assert np.max(np.abs(t64[sub] - t32[sub])) <= 1e-3
+    assert np.sum(fp64.spike_sources < 3) >= 6
+    for sid, t in zip(fp64.spike_sources, fp64.spike_times):
+        same = mixed.spike_times[mixed.spike_sources == sid]
+        assert np.any(np.abs(same - t) <= layout.dt + 1e-12)
