@@ -232,13 +232,17 @@ int mind_inject_spikes(MindHandle *h, int64_t n, const int64_t *sources, const d
  * 128 threads (kCellThreads), 64 threads or one warp of 32 (each thread serving 1, 2 or 4
  * owner slots, so the arithmetic and its order are the same); smaller CTAs let more cells
  * share an SM (by registers and shared memory) at the price of longer parallel phases.  The
+ * 128-thread launch comes compiled for two register budgets: the default, and a tight one
+ * that lets 7 CTAs share an SM, which a bin starts with when its shared memory allows more
+ * than 5 (the tight variant spills a few registers to L1).  The
  * call times `windows` device windows (0: 4) from a fresh initialize for the current shapes
  * and, bin by bin, for the other shapes, keeps a change that is more than 2% faster, and
  * initializes again: the state returns to t = 0 and events injected before the call are
  * dropped, as at any mind_initialize.  It needs a handle initialized at step 0 and takes the
  * precision set for it.  No reference counterpart (the reference launches fixed shapes).
  * mind_bin_threads reports the shapes (*n_bins receives the bin count), mind_set_bin_threads
- * sets them (128, 64 or 32 per bin; at least one thread per threshold detector of a cell).
+ * sets them (128, 64 or 32 per bin; at least one thread per threshold detector of a cell;
+ * a bin set to 128 takes the register budget it starts with).
  */
 int mind_autotune(MindHandle *h, int32_t windows);
 int mind_bin_threads(const MindHandle *h, int32_t *threads, int32_t cap, int32_t *n_bins);

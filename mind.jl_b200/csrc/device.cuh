@@ -39,6 +39,9 @@ namespace mind {
 constexpr int kMaxGroups = 16;
 constexpr int kThreads = 128;      // auxiliary kernels
 constexpr int kCellThreads = 128;  // window kernel: one cell per CTA of four warps
+// A 128-thread window launch whose cells need little shared memory can keep more CTAs per SM
+// than its registers allow at the default bound (5): the tight variant is compiled for 7.
+constexpr int kTightBlocks = 7;
 constexpr int kSurrogateRing = 21;  // drive bins kept for the surrogate: the last 20 and the current
 
 
@@ -133,7 +136,8 @@ __host__ __device__ inline int staged_doubles(int32_t kind) {
  *            slots of the staged rows;
  *   events   the cell's inbox for the window [inbox_cap];
  *   ints     per staged row: local node; chain top, length,
- *            parent, child-chain CSR; level starts; inbox order;
+ *            parent, child-chain CSR; level starts; inbox order; the
+ *            threads' row ranges per group [ngroups][threads + 1];
  *   shorts   chain of every node [n].
  * Host (to size the launch) and device (to carve the buffer) use this one function.
  */
@@ -152,6 +156,7 @@ __host__ __device__ inline size_t cell_smem_bytes(const CellShape &s, const int3
         ints += (size_t)s.rows[g];
     }
     ints += 4 * (size_t)s.nch + 1 + (size_t)s.nkids + (size_t)s.nlev + 1 + (size_t)inbox_cap;
+    ints += (size_t)ngroups * (kCellThreads + 1);
     return doubles * 8 + (size_t)inbox_cap * sizeof(InboxEvent) + ints * 4 + 2 * (size_t)s.n;
 }
 

@@ -882,8 +882,9 @@ __device__ __forceinline__ void hines_mixed(double *sd, double *sr, const double
  * one chain per thread; along a chain only subtract -> divide -> multiply stays
  * on the dependency chain, the next node's operands being loaded ahead.
  */
-template <bool MIXED, int NT, bool GLOBAL_IMAGE = false, bool GEN = false>
-__global__ void __launch_bounds__(NT, NT == kCellThreads ? 5 : NT == kCellThreads / 2 ? 10 : 16) window_kernel(const Params P, const int32_t *cells,
+template <bool MIXED, int NT, bool GLOBAL_IMAGE = false, bool GEN = false,
+          int MINB = NT == kCellThreads ? 5 : NT == kCellThreads / 2 ? 10 : 16>
+__global__ void __launch_bounds__(NT, MINB) window_kernel(const Params P, const int32_t *cells,
                                                                                int64_t n0, int32_t W) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ StagedGroup sg[kMaxGroups];
@@ -941,9 +942,7 @@ __global__ void __launch_bounds__(NT, NT == kCellThreads ? 5 : NT == kCellThread
     int32_t *ckids = ip; ip += nkids;
     int32_t *lvc = ip; ip += nlev + 1;
     int32_t *sorder = ip; ip += P.inbox_cap;
-    // each thread's row ranges per group are read from HBM through the read-only cache
-    // (two loads per group and step, L1-resident): staging them would cost 2 KB per cell
-    const int32_t *__restrict__ gpart = P.part + (int64_t)c * P.ngroups * (O + 1);
+    int32_t *spart = ip; ip += P.ngroups * (O + 1);
     int16_t *chain_of = reinterpret_cast<int16_t *>(ip);
     {
         // The launch sized the image for this cell's bin; refuse rather than overrun.
@@ -1009,6 +1008,7 @@ __global__ void __launch_bounds__(NT, NT == kCellThreads ? 5 : NT == kCellThread
     if (tid == 0) ckoff[nch] = nkids;
     for (int32_t k = tid; k < nkids; k += T) ckids[k] = P.chain_kids[kb + k];
     for (int32_t k = tid; k <= nlev; k += T) lvc[k] = P.level_chain[lv0 + k];
+    for (int32_t k = tid; k < P.ngroups * (O + 1); k += T) spart[k] = P.part[(int64_t)c * P.ngroups * (O + 1) + k];
     __syncthreads();
     for (int32_t k = tid; k < nch; k += T)
         for (int32_t i = ctop[k]; i < ctop[k] + clen[k]; ++i) chain_of[i] = (int16_t)k;
@@ -1141,7 +1141,7 @@ __global__ void __launch_bounds__(NT, NT == kCellThreads ? 5 : NT == kCellThread
             const DevGroup &GG = P.groups[g];
             const StagedGroup G = sg[g];
             for (int32_t slot = tid; slot < O; slot += T) {
-                const int32_t lo = __ldg(gpart + g * (O + 1) + slot), hi = __ldg(gpart + g * (O + 1) + slot + 1);
+                const int32_t lo = spart[g * (O + 1) + slot], hi = spart[g * (O + 1) + slot + 1];
                 if (lo >= hi) continue;
                 if (G.kind == MIND_MECH_PAS) {
                     if (MIXED) continue;  // folded into the node constants of the assembly below

@@ -25,6 +25,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "kernels.cuh"
@@ -154,6 +155,7 @@ struct MindHandle {
         int32_t first, count;
         size_t smem_bytes;
         int32_t threads = kCellThreads;   // CTA size of the bin's launches (kCellThreads or half)
+        bool tight = false;               // 128 threads, compiled for kTightBlocks CTAs per SM
         int32_t max_detectors = 0;        // most threshold detectors on one of its cells
         bool global_image = false;        // cells too large for shared memory: image in HBM
     };
@@ -338,13 +340,20 @@ int launch_grid(int64_t work) {
 }
 
 /* The window kernel's launch shapes: 128 threads per cell (kCellThreads), 64, or one warp. */
-template <int NT>
+template <int NT, int MINB = NT == kCellThreads ? 5 : NT == kCellThreads / 2 ? 10 : 16>
 cudaError_t set_window_smem(int bytes) {
-    cudaError_t e = cudaFuncSetAttribute(window_kernel<false, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaError_t e = cudaFuncSetAttribute(window_kernel<false, NT, false, false, MINB>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(window_kernel<true, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        e = cudaFuncSetAttribute(window_kernel<true, NT, false, false, MINB>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     return e;
 }
+
+/* Whether a bin's 128-thread launches start as the tight variant: when its shared memory
+ * leaves room for more resident CTAs per SM than the default register bound (228 KB per SM,
+ * 1 KB reserved per CTA). */
+bool tight_by_default(size_t smem_bytes) { return (smem_bytes + 1024) * 6 <= 228 * 1024; }
 
 bool valid_cell_threads(int32_t threads) {
     return threads == kCellThreads || threads == kCellThreads / 2 || threads == kCellThreads / 4;
@@ -846,6 +855,7 @@ int create(const MindLayout *L, MindHandle *h) {
         bin.count = (int32_t)(k - first);
         bin.smem_bytes = big ? 0 : top;
         bin.global_image = big;
+        bin.tight = !big && tight_by_default(top);
         if (!big) worst_smem = std::max(worst_smem, top);
         for (size_t q = first; q < k; ++q)
             bin.max_detectors = std::max(bin.max_detectors, det_off[need[q].second + 1] - det_off[need[q].second]);
@@ -856,6 +866,7 @@ int create(const MindLayout *L, MindHandle *h) {
     h->smem_bytes = worst_smem;
     const int smem_attr = (int)std::max<size_t>(worst_smem, 1);
     CUDA_TRY(h, set_window_smem<kCellThreads>(smem_attr));
+    CUDA_TRY(h, (set_window_smem<kCellThreads, kTightBlocks>(smem_attr)));
     CUDA_TRY(h, cudaFuncSetAttribute(window_kernel<false, kCellThreads, false, true>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr));
     CUDA_TRY(h, cudaFuncSetAttribute(window_kernel<true, kCellThreads, false, true>,
@@ -1065,6 +1076,8 @@ void launch_window(const MindHandle::Bin &bin, cudaStream_t s, const Params &P, 
             window_kernel<MIXED, T, false, true><<<bin.count, T, bin.smem_bytes, s>>>(P, cells, n0, W);
     } else if (bin.global_image)
         window_kernel<MIXED, T, true><<<bin.count, T, 0, s>>>(P, cells, n0, W);
+    else if (bin.threads == T && bin.tight)
+        window_kernel<MIXED, T, false, false, kTightBlocks><<<bin.count, T, bin.smem_bytes, s>>>(P, cells, n0, W);
     else if (bin.threads == T)
         window_kernel<MIXED, T><<<bin.count, T, bin.smem_bytes, s>>>(P, cells, n0, W);
     else if (bin.threads == T / 2)
@@ -1789,24 +1802,30 @@ int mind_autotune(MindHandle *h, int32_t windows) {
     double best = 0.0;
     int status = trial_ms(h, windows, &best);
     if (status) return status;
-    const int32_t shapes[3] = {kCellThreads, kCellThreads / 2, kCellThreads / 4};
+    // launch shapes: 128 threads at either register bound, 64, one warp
+    const std::pair<int32_t, bool> shapes[4] = {
+        {kCellThreads, false}, {kCellThreads, true}, {kCellThreads / 2, false}, {kCellThreads / 4, false}};
     for (auto &bin : h->bins) {
         if (bin.global_image || h->has_generated) continue;   // HBM images and emitted mechanisms: 128 threads
-        const int32_t keep = bin.threads;
-        for (int32_t t : shapes) {
-            if (t == keep || t < bin.max_detectors) continue;   // one detector per thread
-            const int32_t before = bin.threads;
-            bin.threads = t;
+        const std::pair<int32_t, bool> keep{bin.threads, bin.tight};
+        for (const auto &shape : shapes) {
+            if (shape == keep || shape.first < bin.max_detectors) continue;   // one detector per thread
+            const std::pair<int32_t, bool> before{bin.threads, bin.tight};
+            bin.threads = shape.first;
+            bin.tight = shape.second;
             double ms = 0.0;
             status = trial_ms(h, windows, &ms);
             if (status) {
-                bin.threads = keep;
+                bin.threads = keep.first;
+                bin.tight = keep.second;
                 return status;
             }
-            if (ms < 0.98 * best)
+            if (ms < 0.98 * best) {
                 best = ms;
-            else
-                bin.threads = before;
+            } else {
+                bin.threads = before.first;
+                bin.tight = before.second;
+            }
         }
     }
     return mind_initialize(h);
@@ -1829,7 +1848,11 @@ int mind_set_bin_threads(MindHandle *h, const int32_t *threads, int32_t n_bins) 
         if ((h->bins[b].global_image || h->has_generated) && threads[b] != kCellThreads)
             return fail(h, MIND_EARG, "cells with their image in HBM, and models with emitted mechanisms, run 128 threads");
     }
-    for (int32_t b = 0; b < n_bins; ++b) h->bins[b].threads = threads[b];
+    for (int32_t b = 0; b < n_bins; ++b) {
+        MindHandle::Bin &bin = h->bins[b];
+        bin.threads = threads[b];
+        bin.tight = threads[b] == kCellThreads && !bin.global_image && tight_by_default(bin.smem_bytes);
+    }
     return MIND_OK;
 }
 
