@@ -335,6 +335,9 @@ typedef struct {
 int mind_mlp_create(const MindMlpConfig *config, MindMlp **mlp);
 int mind_mlp_destroy(MindMlp *mlp);
 const char *mind_mlp_last_error(const MindMlp *mlp);
+/* Device time (ms) of the last predict, gradients or train call's network work: from the
+ * inputs on the device to the last product, without the host copies. */
+int mind_mlp_last_ms(const MindMlp *mlp, float *ms);
 int mind_mlp_param_count(const MindMlp *mlp, int64_t *n);
 int mind_mlp_set_params(MindMlp *mlp, const float *params, int64_t n);
 int mind_mlp_get_params(const MindMlp *mlp, float *params, int64_t n);
@@ -462,9 +465,8 @@ int mind_set_profiling(MindHandle *h, int32_t enable);
  * The first call on a device looks up that array's device address
  * (cudaGetSymbolAddress) with the device current, so make the first call before
  * any stream capture.  The call must be made with the handle's device current
- * (the one current at mind_create), otherwise it returns MIND_EARG.  A handle
- * with surrogate cells attached is refused with MIND_ELAYOUT: the surrogate's
- * products run through cuBLAS, which may allocate a workspace of its own.  All
+ * (the one current at mind_create), otherwise it returns MIND_EARG.  Surrogate
+ * cells run too: their network's buffers are reserved by mind_attach_surrogate.  All
  * handles on a device share the array and it keeps the previous call's
  * contents: calls that overlap on the GPU (two threads, two handles) race and
  * must be serialized by the caller.

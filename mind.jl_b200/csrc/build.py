@@ -18,7 +18,7 @@ OUT_DIR = os.path.join(PACKAGE, "lib")
 OUTPUT = os.path.join(OUT_DIR, "libmindgpu.so")
 SOURCES = [os.path.join(HERE, "mindgpu.cu"), os.path.join(HERE, "surrogate.cu"), os.path.join(HERE, "planner.cpp")]
 DEPENDS = SOURCES + [os.path.join(HERE, f) for f in ("device.cuh", "kernels.cuh", "macro.cuh", "mind_math.h",
-                                                     "gen_runtime.cuh", "generated_mechanisms.cuh")] + [
+                                                     "gen_runtime.cuh", "generated_mechanisms.cuh", "mlp_umma.cuh")] + [
     os.path.join(os.path.dirname(PACKAGE), "include", "mindgpu.h")]
 
 NVCC_FLAGS = [
@@ -47,7 +47,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if not force and up_to_date():
         return OUTPUT
     os.makedirs(OUT_DIR, exist_ok=True)
-    cmd = [nvcc(), *NVCC_FLAGS, *(["-Xptxas", "-v"] if verbose else []), "-o", OUTPUT, *SOURCES, "-lcublas"]
+    cmd = [nvcc(), *NVCC_FLAGS, *(["-Xptxas", "-v"] if verbose else []), "-o", OUTPUT, *SOURCES]
     result = subprocess.run(cmd, capture_output=True, text=True)
     if result.returncode != 0:
         raise RuntimeError(f"nvcc failed ({result.returncode}):\n{result.stderr}\n{result.stdout}")

@@ -33,7 +33,7 @@
 
 using namespace mind;
 
-int mind_mlp_forward_device(MindMlp *m, const float *x, int64_t n, float *prob, cudaStream_t stream);
+int mind_mlp_forward_device(MindMlp *m, const float *x, int64_t n, float *prob, cudaStream_t stream, int32_t *err);
 int mind_mlp_reserve_device(MindMlp *m, int64_t rows);
 int32_t mind_mlp_inputs(const MindMlp *m);
 
@@ -915,6 +915,7 @@ int check_device_error(MindHandle *h) {
                        : code == MIND_ESELFEVENT ? "invalid self-event delay or an event behind its delivery step"
                        : code == MIND_ESINGULAR  ? "singular or non-finite cable system"
                        : code == MIND_ENONFINITE ? "non-finite numerical state"
+                       : code == MIND_ETIMEOUT   ? "a device wait ran out of time"
                                                  : "device error";
     return fail(h, code, what);
 }
@@ -1137,7 +1138,7 @@ int advance(MindHandle *h, int64_t steps, bool record_spikes) {
                                             (size_t)h->ncells * 32 * sizeof(float), h->stream));
                 surrogate_features_kernel<<<launch_grid((int64_t)h->n_sur * 645), kThreads, 0, h->stream>>>(
                     P, h->sur_cells, h->n_sur, h->sur_spikes, h->sur_scale, b, h->sur_x);
-                if (mind_mlp_forward_device(h->sur_mlp, h->sur_x, h->n_sur, h->sur_prob, h->stream))
+                if (mind_mlp_forward_device(h->sur_mlp, h->sur_x, h->n_sur, h->sur_prob, h->stream, h->P.error))
                     return fail(h, MIND_ECUDA, "surrogate inference failed");
                 surrogate_spike_kernel<<<launch_grid(h->n_sur), kThreads, 0, h->stream>>>(
                     P, h->sur_cells, h->sur_sources, h->n_sur, h->sur_prob, h->sur_spikes, b,
@@ -1949,10 +1950,6 @@ int mind_run_noalloc(MindHandle *h, int64_t steps, const MindRecord *records, in
     if (!h->initialized) return fail(h, MIND_EARG, "simulation is not initialized");
     if (steps < 0 || n_records < 0 || (n_records > 0 && (!records || !trace)))
         return fail(h, MIND_EARG, "invalid run arguments");
-    // Surrogate inference runs cuBLAS GEMMs, and cuBLAS may allocate its workspace on first
-    // use: a handle with surrogate cells cannot promise a run without allocation.
-    if (h->sur_cap > 0)
-        return fail(h, MIND_ELAYOUT, "mind_run_noalloc does not run models with surrogate cells (cuBLAS may allocate)");
     {
         int device = -1;
         CUDA_TRY(h, cudaGetDevice(&device));

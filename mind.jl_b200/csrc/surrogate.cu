@@ -4,46 +4,69 @@
  *
  * Network: n_in -> hidden (SiLU) x layers -> 1 logit; the spike probability of the
  * next 1 ms bin is sigmoid(logit).  Parameters are FP32 masters; every matrix product
- * runs in BF16 with FP32 accumulation on the tensor cores (cuBLAS GEMMs, the plain
- * library case), and the parts around the products are this file's fused kernels:
- * bias + SiLU (keeping the pre-activation for the backward pass) with the BF16 cast
- * for the next product, the sigmoid cross-entropy loss and its gradient, SiLU's
- * derivative applied to the incoming gradient, bias sums, and Adam with the BF16
- * weight copy.  Parameter layout: for each linear map l, W_l [out x in] row-major, then
- * b_l [out], maps in order.
+ * runs in BF16 with FP32 accumulation on the tensor cores, in this library's own
+ * tcgen05 kernels (mlp_umma.cuh) whose epilogues carry the elementwise work:
+ *
+ *   forward   map l < last hidden:  z_l = h_l W_l^T + b_l, h_{l+1} = SiLU(z_l)      EPI_HIDDEN
+ *             last hidden map + output map: logit, sigmoid (inference), or the
+ *             cross-entropy, dlogit and dz of the last hidden map (training)          EPI_HEAD
+ *   backward  dW_l = dz_l^T h_l (rows split into K slices, summed in a fixed order)   EPI_F32
+ *             dz_{l-1} = (dz_l W_l) * SiLU'(z_{l-1})                                  EPI_BACK
+ *
+ * and small kernels here for the rest: BF16 staging and transposes of the inputs, the
+ * output map's gradients and the bias gradients (row sums in a fixed order), and Adam with
+ * the BF16 weight copies (row-major for the forward products, transposed for the backward
+ * ones).  The products' operands are K-major everywhere, so every activation and gradient
+ * that a weight gradient needs is also written transposed (rows of the batch contiguous).
+ * Parameter layout: for each linear map l, W_l [out x in] row-major, then b_l [out], maps in
+ * order.  hidden must be a multiple of 16 and at most 256 (one tile spans a hidden layer).
  */
-#include <cublas_v2.h>
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
 #include "../../include/mindgpu.h"
+#include "mlp_umma.cuh"
 
 struct MindMlp {
     std::vector<int32_t> dims;       // n_in, hidden..., 1
+    int32_t hidden = 0;
+    int32_t maps = 0;                // linear maps: layers hidden ones, then the output map
     int32_t ld0 = 0;                 // n_in rounded up to 8: row stride of the BF16 inputs and of w0
     std::vector<int64_t> w_off, b_off;
     int64_t n_params = 0;
     float *master = nullptr, *grad = nullptr, *m1 = nullptr, *m2 = nullptr;
-    __nv_bfloat16 *wbf = nullptr;    // BF16 copy of the parameters
-    __nv_bfloat16 *w0 = nullptr;     // BF16 first-map weights [dims[1] x ld0], zero past n_in
-    float *gw0 = nullptr;            // FP32 first-map weight gradient [dims[1] x ld0]
-    float *part = nullptr;           // bias-gradient partial sums [chunks x widest]
+    __nv_bfloat16 *wbf = nullptr;    // BF16 copy of the parameters (forward operands of maps >= 1)
+    __nv_bfloat16 *w0 = nullptr;     // BF16 first-map weights [hidden x ld0], zero past n_in
+    __nv_bfloat16 *wt = nullptr;     // BF16 W_l^T of the hidden maps 1..layers-1 [hidden x hidden] each
+    float *loss = nullptr;           // the last batch's mean loss
     float *loss_hist = nullptr;      // per-step batch losses of a training call
     int32_t loss_cap = 0;
     int64_t adam_t = 0;
-    cublasHandle_t blas = nullptr;
     cudaStream_t stream = nullptr;
-    int64_t cap = 0;                 // rows the activation buffers hold
-    std::vector<float *> z;          // pre-activations per map [cap x out]
-    std::vector<__nv_bfloat16 *> h;  // inputs of each map [cap x in] (h[0] = X, rows of ld0)
-    __nv_bfloat16 *dzb = nullptr;    // BF16 gradient of a map's output [cap x widest]
-    float *dh = nullptr, *dz = nullptr, *y = nullptr, *loss = nullptr;
+    cudaEvent_t ready = nullptr, done = nullptr;
+    int32_t *err = nullptr;          // device status word of the products (MIND_ETIMEOUT)
+    // activations, rows of the batch: cap rows; transposed copies: rows of capT elements
+    int64_t cap = 0, capT = 0;
+    __nv_bfloat16 *x = nullptr;      // inputs [cap x ld0]
+    __nv_bfloat16 *xt = nullptr;     // inputs transposed [ld0 x capT]
+    std::vector<float *> z;          // pre-activations of hidden maps 0..layers-2 [cap x hidden]
+    std::vector<__nv_bfloat16 *> h, ht;   // outputs of hidden maps 0..layers-2, rows and transposed
+    __nv_bfloat16 *ht_last = nullptr;     // SiLU of the last hidden map, transposed
+    __nv_bfloat16 *dzr[2] = {nullptr, nullptr}, *dzc[2] = {nullptr, nullptr};   // dz rows / transposed
+    float *y = nullptr, *prob = nullptr, *dlogit = nullptr, *row_loss = nullptr;
+    float *part = nullptr;           // weight-gradient K slices [kMaxSplits x hidden x max(n_in, hidden)]
+    float *xin = nullptr;            // FP32 rows uploaded by predict / gradients [cap x n_in]
+    float last_ms = 0.0f;            // device time of the last call's network work
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
     float *data_x = nullptr, *data_y = nullptr;  // training set (FP32 on the device)
     int64_t data_n = 0, data_cap = 0;
     std::string error;
@@ -52,6 +75,7 @@ struct MindMlp {
 namespace {
 
 constexpr int kT = 256;
+constexpr int kMaxSplits = 32;
 
 int fail(MindMlp *m, int code, const std::string &why) {
     if (m) m->error = why;
@@ -63,84 +87,58 @@ int fail(MindMlp *m, int code, const std::string &why) {
         cudaError_t _e = (call);                                                                  \
         if (_e != cudaSuccess) return fail((m), MIND_ECUDA, std::string(#call ": ") + cudaGetErrorString(_e)); \
     } while (0)
-#define MLP_BLAS(m, call)                                                        \
-    do {                                                                         \
-        cublasStatus_t _s = (call);                                              \
-        if (_s != CUBLAS_STATUS_SUCCESS) return fail((m), MIND_ECUDA, #call);    \
+#define MLP_TRY(call)         \
+    do {                      \
+        int _s = (call);      \
+        if (_s) return _s;    \
     } while (0)
 
 int grid(int64_t n) { return (int)std::min<int64_t>((n + kT - 1) / kT, 148 * 16); }
 
-__device__ __forceinline__ float sigmoidf_(float x) { return 1.0f / (1.0f + __expf(-x)); }
+// ---------------------------------------------------------------------------------------
+// small kernels
+// ---------------------------------------------------------------------------------------
 
-/* z = acc + b (per column); h_next = BF16(SiLU(z)) unless last. */
-__global__ void bias_act_kernel(float *z, const float *b, __nv_bfloat16 *h_next, int64_t rows, int32_t cols, int last) {
-    const int64_t n = rows * cols;
-    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
-        const float v = z[k] + b[k % cols];
-        z[k] = v;
-        if (!last) h_next[k] = __float2bfloat16(v * sigmoidf_(v));
+/* The BF16 copies of parameter k (value v): the flat copy, w0 (first map, rows of stride
+ * ld0), and W_l^T for the hidden maps l = 1..layers-1. */
+struct CopyLayout {
+    __nv_bfloat16 *wbf, *w0, *wt;
+    int64_t w0_off, n0, hid_off, hid_stride;
+    int32_t d, ld0, hidden, n_hidden_maps;
+};
+
+__device__ __forceinline__ void store_copies(const CopyLayout &C, int64_t k, float v) {
+    const __nv_bfloat16 b = __float2bfloat16(v);
+    C.wbf[k] = b;
+    const int64_t j = k - C.w0_off;
+    if (j >= 0 && j < C.n0) C.w0[(j / C.d) * C.ld0 + j % C.d] = b;
+    const int64_t q = k - C.hid_off;
+    if (q >= 0 && C.n_hidden_maps > 0) {
+        const int64_t map = q / C.hid_stride, r = q - map * C.hid_stride;
+        const int64_t hh = (int64_t)C.hidden * C.hidden;
+        if (map < C.n_hidden_maps && r < hh) {
+            const int64_t o = r / C.hidden, i = r - o * C.hidden;
+            C.wt[map * hh + i * C.hidden + o] = b;
+        }
     }
 }
 
-/* Mean sigmoid cross-entropy of the logits and its gradient (1/rows) (p - y). */
-__global__ void bce_kernel(const float *logit, const float *y, float *dz, float *loss, int64_t rows) {
-    float local = 0.0f;
-    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < rows; k += (int64_t)gridDim.x * blockDim.x) {
-        const float z = logit[k], t = y[k];
-        local += fmaxf(z, 0.0f) - z * t + log1pf(__expf(-fabsf(z)));
-        dz[k] = (sigmoidf_(z) - t) / (float)rows;
-    }
-    for (int o = 16; o > 0; o >>= 1) local += __shfl_down_sync(0xffffffffu, local, o);
-    if ((threadIdx.x & 31) == 0) atomicAdd(loss, local / (float)rows);
-}
-
-__global__ void sigmoid_kernel(const float *logit, float *p, int64_t rows) {
-    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < rows; k += (int64_t)gridDim.x * blockDim.x)
-        p[k] = sigmoidf_(logit[k]);
-}
-
-/* dz = dh * SiLU'(z), and its BF16 copy for the next products. */
-__global__ void silu_back_kernel(const float *dh, const float *z, float *dz, __nv_bfloat16 *dzb, int64_t n) {
-    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
-        const float s = sigmoidf_(z[k]);
-        const float g = dh[k] * (s * (1.0f + z[k] * (1.0f - s)));
-        dz[k] = g;
-        dzb[k] = __float2bfloat16(g);
-    }
-}
-
-__global__ void to_bf16_kernel(const float *x, __nv_bfloat16 *out, int64_t n) {
+__global__ void copies_kernel(const float *w, int64_t n, CopyLayout C) {
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
-        out[k] = __float2bfloat16(x[k]);
+        store_copies(C, k, w[k]);
 }
 
-/* Bias gradients db[c] = sum over rows of dz[r][c], in a fixed order: block (x, y) of
- * 32 x 8 threads sums columns 32x.. of the rows of chunk y (a warp reads 32 consecutive
- * columns of one row), the 8 row phases are added in order into part[y][c]; then
- * colsum_finish adds the chunks in order. */
-constexpr int kColChunk = 128;
-__global__ void colsum_kernel(const float *dz, float *part, int64_t rows, int32_t cols) {
-    __shared__ float acc[8][33];
-    const int32_t c = blockIdx.x * 32 + threadIdx.x;
-    const int64_t r0 = (int64_t)blockIdx.y * kColChunk;
-    float s = 0.0f;
-    if (c < cols)
-        for (int64_t r = r0 + threadIdx.y; r < rows && r < r0 + kColChunk; r += 8) s += dz[r * cols + c];
-    acc[threadIdx.y][threadIdx.x] = s;
-    __syncthreads();
-    if (threadIdx.y == 0 && c < cols) {
-        float t = acc[0][threadIdx.x];
-        for (int k = 1; k < 8; ++k) t += acc[k][threadIdx.x];
-        part[(int64_t)blockIdx.y * cols + c] = t;
-    }
-}
-
-__global__ void colsum_finish(const float *part, float *db, int32_t chunks, int32_t cols) {
-    for (int32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < cols; c += gridDim.x * blockDim.x) {
-        float t = 0.0f;
-        for (int32_t k = 0; k < chunks; ++k) t += part[(int64_t)k * cols + c];
-        db[c] = t;
+/* Adam (beta1 0.9, beta2 0.999, eps 1e-8) on the FP32 masters, then the BF16 copies. */
+__global__ void adam_kernel(float *w, const float *g, float *m1, float *m2, int64_t n, float lr, float c1, float c2,
+                            CopyLayout C) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        const float gk = g[k];
+        const float a = 0.9f * m1[k] + 0.1f * gk, b = 0.999f * m2[k] + 0.001f * gk * gk;
+        m1[k] = a;
+        m2[k] = b;
+        const float v = w[k] - lr * (a / c1) / (sqrtf(b / c2) + 1e-8f);
+        w[k] = v;
+        store_copies(C, k, v);
     }
 }
 
@@ -153,17 +151,8 @@ __global__ void to_bf16_rows_kernel(const float *x, __nv_bfloat16 *out, int64_t 
     }
 }
 
-/* First-map weight gradient, [o x ld] -> the packed [o x d] of the parameter vector. */
-__global__ void compact_rows_kernel(const float *in, float *out, int32_t o, int32_t d, int32_t ld) {
-    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < (int64_t)o * d;
-         k += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t row = k / d;
-        out[k] = in[row * ld + (k - row * d)];
-    }
-}
-
-/* Rows of the training set drawn for one step (Philox-free: a 64-bit mix of step and slot),
- * as BF16 rows of stride ld (zero past d). */
+/* Rows of the training set drawn for one step (a 64-bit mix of step and slot), as BF16 rows
+ * of stride ld (zero past d), and their targets. */
 __global__ void gather_kernel(const float *x, const float *y, __nv_bfloat16 *hx, float *hy, int64_t n, int32_t d,
                               int32_t ld, int32_t batch, uint64_t step) {
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < (int64_t)batch * ld;
@@ -179,147 +168,341 @@ __global__ void gather_kernel(const float *x, const float *y, __nv_bfloat16 *hx,
     }
 }
 
-/* Adam (beta1 0.9, beta2 0.999, eps 1e-8) on the FP32 masters, then the BF16 copies (the
- * first map's weights, the first n0 = o*d parameters after w0_off, also into w0 rows of
- * stride ld). */
-__global__ void adam_kernel(float *w, const float *g, float *m1, float *m2, __nv_bfloat16 *wbf, int64_t n, float lr,
-                            float c1, float c2, __nv_bfloat16 *w0, int64_t w0_off, int64_t n0, int32_t d, int32_t ld) {
-    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
-        const float gk = g[k];
-        const float a = 0.9f * m1[k] + 0.1f * gk, b = 0.999f * m2[k] + 0.001f * gk * gk;
-        m1[k] = a;
-        m2[k] = b;
-        const float v = w[k] - lr * (a / c1) / (sqrtf(b / c2) + 1e-8f);
-        w[k] = v;
-        wbf[k] = __float2bfloat16(v);
-        const int64_t j = k - w0_off;
-        if (j >= 0 && j < n0) w0[(j / d) * ld + j % d] = __float2bfloat16(v);
+/* dst [cols x ld_dst] = src [rows x ld_src]^T for the first `cols` columns (BF16), through
+ * 32 x 32 shared-memory tiles so that both sides are read and written along rows. */
+__global__ void transpose_kernel(const __nv_bfloat16 *src, int64_t rows, int32_t cols, int32_t ld_src,
+                                 __nv_bfloat16 *dst, int64_t ld_dst) {
+    __shared__ __nv_bfloat16 tile[32][34];
+    const int64_t r0 = (int64_t)blockIdx.x * 32;
+    const int32_t c0 = blockIdx.y * 32;
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int64_t r = r0 + k;
+        const int32_t c = c0 + threadIdx.x;
+        tile[k][threadIdx.x] = (r < rows && c < cols) ? src[r * ld_src + c] : __float2bfloat16(0.0f);
+    }
+    __syncthreads();
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int32_t c = c0 + k;
+        const int64_t r = r0 + threadIdx.x;
+        if (c < cols && r < rows) dst[(int64_t)c * ld_dst + r] = tile[threadIdx.x][k];
     }
 }
 
-/* w0 from the BF16 copy: rows of stride ld, zero past d. */
-__global__ void pad_w0_kernel(const __nv_bfloat16 *wbf, __nv_bfloat16 *w0, int32_t o, int32_t d, int32_t ld) {
-    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < (int64_t)o * ld;
-         k += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t row = k / ld;
-        const int32_t col = (int32_t)(k - row * ld);
-        w0[k] = col < d ? wbf[row * d + col] : __float2bfloat16(0.0f);
+/* Fixed-order block sum of per-thread partials (blockDim.x == kT). */
+__device__ __forceinline__ float block_sum(float v, float *scratch) {
+    scratch[threadIdx.x] = v;
+    __syncthreads();
+    for (int s = kT / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) scratch[threadIdx.x] += scratch[threadIdx.x + s];
+        __syncthreads();
     }
+    return scratch[0];
+}
+
+/* out[o] = sum over r < R of w[r] * src[o][r] (w null: 1), one block per o, in a fixed order. */
+__global__ void rowsum_kernel(const __nv_bfloat16 *src, int64_t ld, int64_t R, const float *w, float *out) {
+    __shared__ float scratch[kT];
+    const int64_t o = blockIdx.x;
+    float s = 0.0f;
+    for (int64_t r = threadIdx.x; r < R; r += kT) {
+        const float v = __bfloat162float(src[o * ld + r]);
+        s += w ? w[r] * v : v;
+    }
+    const float t = block_sum(s, scratch);
+    if (threadIdx.x == 0) out[o] = t;
+}
+
+/* The output map's bias gradient (sum of dlogit) and the batch's mean loss. */
+__global__ void head_scalars_kernel(const float *dlogit, const float *row_loss, int64_t R, float *db, float *loss) {
+    __shared__ float scratch[kT];
+    float a = 0.0f, b = 0.0f;
+    for (int64_t r = threadIdx.x; r < R; r += kT) {
+        a += dlogit[r];
+        b += row_loss[r];
+    }
+    const float sa = block_sum(a, scratch);
+    __syncthreads();
+    const float sb = block_sum(b, scratch);
+    if (threadIdx.x == 0) {
+        *db = sa;
+        *loss = sb / (float)R;
+    }
+}
+
+/* grad[k] = sum over the K slices s (in order) of part[s][k], k < n. */
+__global__ void split_sum_kernel(const float *part, int32_t splits, int64_t n, float *grad) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        float t = 0.0f;
+        for (int32_t s = 0; s < splits; ++s) t += part[(int64_t)s * n + k];
+        grad[k] = t;
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// tensor maps and product launches
+// ---------------------------------------------------------------------------------------
+
+PFN_cuTensorMapEncodeTiled encoder() {
+    static PFN_cuTensorMapEncodeTiled fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled>(p);
+    });
+    return fn;
+}
+
+/* A K-major BF16 operand: `outer` rows of `inner` elements, rows `ld` elements apart; boxes
+ * of 64 elements (128 bytes, the swizzle span) by box_rows rows. */
+int operand_map(MindMlp *m, CUtensorMap *map, const __nv_bfloat16 *ptr, int64_t inner, int64_t outer, int64_t ld,
+                int32_t box_rows) {
+    PFN_cuTensorMapEncodeTiled encode = encoder();
+    if (!encode) return fail(m, MIND_ECUDA, "cuTensorMapEncodeTiled unavailable");
+    if (((uintptr_t)ptr & 15) || (ld * 2) % 16) return fail(m, MIND_ECUDA, "operand not 16-byte aligned");
+    const cuuint64_t dims[2] = {(cuuint64_t)inner, (cuuint64_t)outer};
+    const cuuint64_t strides[1] = {(cuuint64_t)(ld * 2)};
+    const cuuint32_t box[2] = {(cuuint32_t)mlp::kBlockK, (cuuint32_t)box_rows};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16 *>(ptr), dims, strides,
+                              box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(m, MIND_ECUDA, "cuTensorMapEncodeTiled failed");
+    return MIND_OK;
+}
+
+/* D [M x N] = A [M x K] B [N x K]^T with epilogue EPI on N tiles of BN columns and `splits`
+ * K slices (EPI_F32 only). */
+template <int EPI, int BN>
+int product(MindMlp *m, const __nv_bfloat16 *A, int64_t lda, const __nv_bfloat16 *B, int64_t ldb, int32_t M, int32_t N,
+            int32_t K, int32_t splits, mlp::EpiParams E, cudaStream_t s, int32_t *splits_used = nullptr) {
+    using S = mlp::Shape<BN>;
+    MLP_CUDA(m, cudaFuncSetAttribute(mlp::umma_gemm_kernel<EPI, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     S::kSmemBytes));
+    if (M < 1 || N < 1 || K < 1) return fail(m, MIND_EARG, "empty product");
+    CUtensorMap ma, mb;
+    MLP_TRY(operand_map(m, &ma, A, K, M, lda, mlp::kTileM));
+    // B's rows: the tensor map spans the rows the operand holds (at least N)
+    MLP_TRY(operand_map(m, &mb, B, K, N, ldb, BN));
+    const int32_t kb_total = (K + mlp::kBlockK - 1) / mlp::kBlockK;
+    splits = std::max(1, std::min(splits, kb_total));
+    const int32_t per = (kb_total + splits - 1) / splits;
+    splits = (kb_total + per - 1) / per;   // no empty slice
+    if (splits_used) *splits_used = splits;
+    E.M = M;
+    E.N = N;
+    E.err = m->err;
+    const dim3 g((M + mlp::kTileM - 1) / mlp::kTileM, (N + BN - 1) / BN, splits);
+    mlp::umma_gemm_kernel<EPI, BN><<<g, mlp::kThreads, S::kSmemBytes, s>>>(ma, mb, kb_total, per, E);
+    MLP_CUDA(m, cudaGetLastError());
+    return MIND_OK;
+}
+
+/* K slices for a weight gradient: about two CTAs per SM, at least 4 K blocks per slice. */
+int32_t grad_splits(int32_t tiles, int64_t rows) {
+    const int32_t kb = (int32_t)((rows + mlp::kBlockK - 1) / mlp::kBlockK);
+    int32_t s = (2 * 148 + tiles - 1) / tiles;
+    s = std::min(s, std::max(1, kb / 4));
+    return std::max(1, std::min(s, kMaxSplits));
+}
+
+void free_activations(MindMlp *m) {
+    for (float *p : m->z) cudaFree(p);
+    for (__nv_bfloat16 *p : m->h) cudaFree(p);
+    for (__nv_bfloat16 *p : m->ht) cudaFree(p);
+    m->z.clear();
+    m->h.clear();
+    m->ht.clear();
+    for (void *p : {(void *)m->x, (void *)m->xt, (void *)m->ht_last, (void *)m->dzr[0], (void *)m->dzr[1],
+                    (void *)m->dzc[0], (void *)m->dzc[1], (void *)m->y, (void *)m->prob, (void *)m->dlogit,
+                    (void *)m->row_loss, (void *)m->part, (void *)m->xin})
+        cudaFree(p);
+    m->xin = nullptr;
+    m->x = m->xt = m->ht_last = m->dzr[0] = m->dzr[1] = m->dzc[0] = m->dzc[1] = nullptr;
+    m->y = m->prob = m->dlogit = m->row_loss = m->part = nullptr;
+    m->cap = m->capT = 0;
 }
 
 int reserve(MindMlp *m, int64_t rows) {
     if (rows <= m->cap) return MIND_OK;
     const int64_t cap = std::max<int64_t>(rows, 2 * m->cap);
-    for (float *p : m->z) cudaFree(p);
-    for (__nv_bfloat16 *p : m->h) cudaFree(p);
-    cudaFree(m->dzb);
-    cudaFree(m->dh);
-    cudaFree(m->dz);
-    cudaFree(m->y);
-    const size_t L = m->dims.size() - 1;
-    int32_t widest = 0;
-    for (int32_t d : m->dims) widest = std::max(widest, d);
-    m->z.assign(L, nullptr);
-    m->h.assign(L, nullptr);
-    for (size_t l = 0; l < L; ++l) {
-        MLP_CUDA(m, cudaMalloc(&m->z[l], cap * m->dims[l + 1] * sizeof(float)));
-        MLP_CUDA(m, cudaMalloc(&m->h[l], cap * (l == 0 ? m->ld0 : m->dims[l]) * sizeof(__nv_bfloat16)));
+    const int64_t capT = (cap + 7) / 8 * 8;
+    free_activations(m);
+    const int64_t H = m->hidden;
+    const int32_t inner = m->maps - 2;   // hidden maps whose outputs feed another hidden map
+    m->z.assign(inner, nullptr);
+    m->h.assign(inner, nullptr);
+    m->ht.assign(inner, nullptr);
+    for (int32_t l = 0; l < inner; ++l) {
+        MLP_CUDA(m, cudaMalloc(&m->z[l], cap * H * sizeof(float)));
+        MLP_CUDA(m, cudaMalloc(&m->h[l], cap * H * sizeof(__nv_bfloat16)));
+        MLP_CUDA(m, cudaMalloc(&m->ht[l], H * capT * sizeof(__nv_bfloat16)));
     }
-    cudaFree(m->part);
-    MLP_CUDA(m, cudaMalloc(&m->part, ((cap + kColChunk - 1) / kColChunk) * widest * sizeof(float)));
-    MLP_CUDA(m, cudaMalloc(&m->dzb, cap * widest * sizeof(__nv_bfloat16)));
-    MLP_CUDA(m, cudaMalloc(&m->dh, cap * widest * sizeof(float)));
-    MLP_CUDA(m, cudaMalloc(&m->dz, cap * widest * sizeof(float)));
-    MLP_CUDA(m, cudaMalloc(&m->y, cap * sizeof(float)));
+    MLP_CUDA(m, cudaMalloc(&m->x, cap * m->ld0 * sizeof(__nv_bfloat16)));
+    MLP_CUDA(m, cudaMalloc(&m->xin, cap * m->dims[0] * sizeof(float)));
+    MLP_CUDA(m, cudaMalloc(&m->xt, (int64_t)m->ld0 * capT * sizeof(__nv_bfloat16)));
+    MLP_CUDA(m, cudaMalloc(&m->ht_last, H * capT * sizeof(__nv_bfloat16)));
+    for (int k = 0; k < 2; ++k) {
+        MLP_CUDA(m, cudaMalloc(&m->dzr[k], cap * H * sizeof(__nv_bfloat16)));
+        MLP_CUDA(m, cudaMalloc(&m->dzc[k], H * capT * sizeof(__nv_bfloat16)));
+    }
+    for (float **p : {&m->y, &m->prob, &m->dlogit, &m->row_loss}) MLP_CUDA(m, cudaMalloc(p, cap * sizeof(float)));
+    MLP_CUDA(m, cudaMalloc(&m->part, (size_t)kMaxSplits * H * std::max<int64_t>(m->dims[0], H) * sizeof(float)));
     m->cap = cap;
+    m->capT = capT;
     return MIND_OK;
 }
 
-/* Row-major C[rows x o] = A[rows x i] * W[o x i]^T (BF16 in, FP32 out). */
-int gemm_forward(MindMlp *m, const __nv_bfloat16 *A, const __nv_bfloat16 *W, float *C, int64_t rows, int32_t i, int32_t o) {
-    const float one = 1.0f, zero = 0.0f;
-    MLP_BLAS(m, cublasGemmEx(m->blas, CUBLAS_OP_T, CUBLAS_OP_N, o, (int)rows, i, &one, W, CUDA_R_16BF, i, A,
-                             CUDA_R_16BF, i, &zero, C, CUDA_R_32F, o, CUBLAS_COMPUTE_32F, CUBLAS_GEMM_DEFAULT));
-    return MIND_OK;
+CopyLayout copy_layout(const MindMlp *m) {
+    CopyLayout C{};
+    C.wbf = m->wbf;
+    C.w0 = m->w0;
+    C.wt = m->wt;
+    C.w0_off = m->w_off[0];
+    C.n0 = (int64_t)m->dims[0] * m->hidden;
+    C.d = m->dims[0];
+    C.ld0 = m->ld0;
+    C.hidden = m->hidden;
+    C.n_hidden_maps = m->maps - 2;   // hidden maps 1..layers-1
+    C.hid_off = m->maps > 2 ? m->w_off[1] : 0;
+    C.hid_stride = (int64_t)m->hidden * m->hidden + m->hidden;
+    return C;
 }
 
-/* Forward over `rows` rows whose BF16 inputs are in h[0]; logits end in z.back(). */
-int forward(MindMlp *m, int64_t rows) {
-    const size_t L = m->dims.size() - 1;
-    for (size_t l = 0; l < L; ++l) {
-        // the first map runs over ld0 columns (zero past n_in) so every leading dimension
-        // is a multiple of 8 BF16 elements
-        const int32_t i = l == 0 ? m->ld0 : m->dims[l], o = m->dims[l + 1];
-        int s = gemm_forward(m, m->h[l], l == 0 ? m->w0 : m->wbf + m->w_off[l], m->z[l], rows, i, o);
-        if (s) return s;
-        bias_act_kernel<<<grid(rows * o), kT, 0, m->stream>>>(m->z[l], m->master + m->b_off[l],
-                                                               l + 1 < L ? m->h[l + 1] : nullptr, rows, o, l + 1 == L);
+/* Forward over `rows` rows whose BF16 inputs are in m->x; `train` keeps what the backward
+ * pass needs and computes the loss against m->y, otherwise m->prob receives the
+ * probabilities. */
+int forward(MindMlp *m, int64_t rows, bool train, cudaStream_t s, float *prob = nullptr) {
+    const int32_t R = (int32_t)rows, H = m->hidden, last = m->maps - 2;   // last hidden map
+    for (int32_t l = 0; l <= last; ++l) {
+        const __nv_bfloat16 *A = l == 0 ? m->x : m->h[l - 1];
+        const int64_t lda = l == 0 ? m->ld0 : H;
+        const int32_t K = l == 0 ? m->ld0 : H;
+        const __nv_bfloat16 *W = l == 0 ? m->w0 : m->wbf + m->w_off[l];
+        mlp::EpiParams E{};
+        E.bias = m->master + m->b_off[l];
+        E.ld_out = H;
+        E.ld_t = (int32_t)m->capT;
+        if (l < last) {
+            E.z = train ? m->z[l] : nullptr;
+            E.rows = m->h[l];
+            E.cols = train ? m->ht[l] : nullptr;
+            MLP_TRY((product<mlp::EPI_HIDDEN, 64>(m, A, lda, W, K, R, H, K, 1, E, s)));
+        } else {
+            E.w_out = m->master + m->w_off[m->maps - 1];
+            E.b_out = m->master + m->b_off[m->maps - 1];
+            if (train) {
+                E.y = m->y;
+                E.dlogit = m->dlogit;
+                E.row_loss = m->row_loss;
+                E.h_cols = m->ht_last;
+                E.rows = m->dzr[0];
+                E.cols = m->dzc[0];
+                E.rows_total = (float)rows;
+            } else {
+                E.prob = prob ? prob : m->prob;
+            }
+            MLP_TRY((product<mlp::EPI_HEAD, 256>(m, A, lda, W, K, R, H, K, 1, E, s)));
+        }
     }
     return MIND_OK;
 }
 
-/* Gradients of the mean loss into m->grad (targets in m->y); loss into m->loss. */
-int backward(MindMlp *m, int64_t rows) {
-    const size_t L = m->dims.size() - 1;
-    MLP_CUDA(m, cudaMemsetAsync(m->loss, 0, sizeof(float), m->stream));
-    bce_kernel<<<grid(rows), kT, 0, m->stream>>>(m->z[L - 1], m->y, m->dz, m->loss, rows);
-    to_bf16_kernel<<<grid(rows), kT, 0, m->stream>>>(m->dz, m->dzb, rows);
-    const float one = 1.0f, zero = 0.0f;
-    const int32_t chunks = (int32_t)((rows + kColChunk - 1) / kColChunk);
-    for (size_t l = L; l-- > 0;) {
-        const int32_t i = l == 0 ? m->ld0 : m->dims[l], o = m->dims[l + 1];
-        // dW[o x i] = dz^T h  (column-major: dWc[i x o] = hc[i x rows] * dzc[o x rows]^T)
-        float *dw = l == 0 ? m->gw0 : m->grad + m->w_off[l];
-        MLP_BLAS(m, cublasGemmEx(m->blas, CUBLAS_OP_N, CUBLAS_OP_T, i, o, (int)rows, &one, m->h[l], CUDA_R_16BF, i,
-                                 m->dzb, CUDA_R_16BF, o, &zero, dw, CUDA_R_32F, i, CUBLAS_COMPUTE_32F,
-                                 CUBLAS_GEMM_DEFAULT));
-        if (l == 0)
-            compact_rows_kernel<<<grid((int64_t)o * m->dims[0]), kT, 0, m->stream>>>(m->gw0, m->grad + m->w_off[0], o,
-                                                                                  m->dims[0], m->ld0);
-        colsum_kernel<<<dim3((o + 31) / 32, chunks), dim3(32, 8), 0, m->stream>>>(m->dz, m->part, rows, o);
-        colsum_finish<<<(o + kT - 1) / kT, kT, 0, m->stream>>>(m->part, m->grad + m->b_off[l], chunks, o);
+/* Gradients of the mean loss into m->grad after forward(train); m->xt must hold the inputs
+ * transposed. */
+int backward(MindMlp *m, int64_t rows, cudaStream_t s) {
+    const int32_t R = (int32_t)rows, H = m->hidden, last = m->maps - 2;
+    const int64_t T = m->capT;
+    // output map: dW[n] = sum_r dlogit[r] SiLU(z)[r][n], db = sum_r dlogit[r], and the loss
+    rowsum_kernel<<<H, kT, 0, s>>>(m->ht_last, T, rows, m->dlogit, m->grad + m->w_off[m->maps - 1]);
+    head_scalars_kernel<<<1, kT, 0, s>>>(m->dlogit, m->row_loss, rows, m->grad + m->b_off[m->maps - 1], m->loss);
+    int cur = 0;
+    for (int32_t l = last; l >= 0; --l) {
+        const int32_t in = l == 0 ? m->dims[0] : H;
+        // dW_l [H x in] = dz_l^T h_l: A = dz_l transposed [H x R], B = h_l transposed [in x R]
+        const __nv_bfloat16 *Bt = l == 0 ? m->xt : m->ht[l - 1];
+        const int32_t tiles = ((H + 127) / 128) * ((in + 63) / 64);
+        const int32_t splits = grad_splits(tiles, rows);
+        mlp::EpiParams E{};
+        E.n_store = in;
+        E.ld_out = in;
+        E.out = m->part;
+        int32_t used = 1;
+        MLP_TRY((product<mlp::EPI_F32, 64>(m, m->dzc[cur], T, Bt, T, H, in, R, splits, E, s, &used)));
+        split_sum_kernel<<<grid((int64_t)H * in), kT, 0, s>>>(m->part, used, (int64_t)H * in, m->grad + m->w_off[l]);
+        rowsum_kernel<<<H, kT, 0, s>>>(m->dzc[cur], T, rows, nullptr, m->grad + m->b_off[l]);
         if (l == 0) break;
-        // dh[rows x i] = dz[rows x o] W[o x i]  (column-major: dhc[i x rows] = Wc[i x o] dzc[o x rows])
-        MLP_BLAS(m, cublasGemmEx(m->blas, CUBLAS_OP_N, CUBLAS_OP_N, i, (int)rows, o, &one, m->wbf + m->w_off[l],
-                                 CUDA_R_16BF, i, m->dzb, CUDA_R_16BF, o, &zero, m->dh, CUDA_R_32F, i, CUBLAS_COMPUTE_32F,
-                                 CUBLAS_GEMM_DEFAULT));
-        silu_back_kernel<<<grid(rows * i), kT, 0, m->stream>>>(m->dh, m->z[l - 1], m->dz, m->dzb, rows * i);
+        // dz_{l-1} = (dz_l W_l) * SiLU'(z_{l-1}): A = dz_l rows [R x H], B = W_l^T [H x H]
+        mlp::EpiParams B{};
+        B.ld_out = H;
+        B.ld_t = (int32_t)T;
+        B.z_prev = m->z[l - 1];
+        B.rows = m->dzr[cur ^ 1];
+        B.cols = m->dzc[cur ^ 1];
+        const __nv_bfloat16 *Wt = m->wt + (int64_t)(l - 1) * H * H;
+        MLP_TRY((product<mlp::EPI_BACK, 64>(m, m->dzr[cur], H, Wt, H, R, H, H, 1, B, s)));
+        cur ^= 1;
     }
+    MLP_CUDA(m, cudaGetLastError());
     return MIND_OK;
 }
 
+void transpose_inputs(MindMlp *m, int64_t rows, cudaStream_t s) {
+    const dim3 g((unsigned)((rows + 31) / 32), (unsigned)((m->ld0 + 31) / 32));
+    transpose_kernel<<<g, dim3(32, 8), 0, s>>>(m->x, rows, m->ld0, m->ld0, m->xt, m->capT);
+}
+
+/* Host FP32 rows into m->xin; the timed region of the call starts after the copy. */
 int upload_rows(MindMlp *m, const float *x, int64_t n) {
-    int s = reserve(m, n);
-    if (s) return s;
-    const int32_t d = m->dims[0], ld = m->ld0;
-    std::vector<__nv_bfloat16> xb((size_t)n * ld, __float2bfloat16(0.0f));
-    for (int64_t r = 0; r < n; ++r)
-        for (int32_t c = 0; c < d; ++c) xb[(size_t)r * ld + c] = __float2bfloat16(x[(size_t)r * d + c]);
-    MLP_CUDA(m, cudaMemcpyAsync(m->h[0], xb.data(), xb.size() * sizeof(__nv_bfloat16), cudaMemcpyHostToDevice, m->stream));
+    MLP_TRY(reserve(m, n));
+    MLP_CUDA(m, cudaMemcpyAsync(m->xin, x, n * m->dims[0] * sizeof(float), cudaMemcpyHostToDevice, m->stream));
+    MLP_CUDA(m, cudaEventRecord(m->t0, m->stream));
+    to_bf16_rows_kernel<<<grid(n * m->ld0), kT, 0, m->stream>>>(m->xin, m->x, n, m->dims[0], m->ld0);
+    return MIND_OK;
+}
+
+/* Ends the timed region of a call (after its network work, before its copies back). */
+int stop_clock(MindMlp *m) {
+    MLP_CUDA(m, cudaEventRecord(m->t1, m->stream));
+    return MIND_OK;
+}
+
+/* The products' status word: MIND_ETIMEOUT when a wait inside a product ran out. */
+int check(MindMlp *m) {
+    int32_t code = 0;
+    MLP_CUDA(m, cudaMemcpyAsync(&code, m->err, sizeof code, cudaMemcpyDeviceToHost, m->stream));
     MLP_CUDA(m, cudaStreamSynchronize(m->stream));
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, m->t0, m->t1) == cudaSuccess) m->last_ms = ms;
+    if (code) {
+        cudaMemsetAsync(m->err, 0, sizeof(int32_t), m->stream);
+        return fail(m, code, "a tensor-core product's wait ran out of time");
+    }
     return MIND_OK;
 }
 
 }  // namespace
 
 /* For the library's own runs (surrogate cells): probabilities of n rows of FP32 inputs that
- * are already on the device, ordered after `stream`'s work and before its later work.
- * The rows must fit the buffers reserved by mind_mlp_reserve_device. */
-int mind_mlp_forward_device(MindMlp *m, const float *x, int64_t n, float *prob, cudaStream_t stream) {
+ * are already on the device, ordered after `stream`'s work and before its later work.  The
+ * rows must fit the buffers reserved by mind_mlp_reserve_device; a product whose wait runs
+ * out raises MIND_ETIMEOUT in `err` (the run's status word). */
+int mind_mlp_forward_device(MindMlp *m, const float *x, int64_t n, float *prob, cudaStream_t stream, int32_t *err) {
     if (n > m->cap) return fail(m, MIND_ECAPACITY, "more rows than reserved");
-    cudaEvent_t ready, done;
-    MLP_CUDA(m, cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
-    MLP_CUDA(m, cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
-    cudaEventRecord(ready, stream);
-    cudaStreamWaitEvent(m->stream, ready, 0);
-    to_bf16_rows_kernel<<<grid(n * m->ld0), kT, 0, m->stream>>>(x, m->h[0], n, m->dims[0], m->ld0);
-    int s = forward(m, n);
-    if (!s) sigmoid_kernel<<<grid(n), kT, 0, m->stream>>>(m->z.back(), prob, n);
-    cudaEventRecord(done, m->stream);
-    cudaStreamWaitEvent(stream, done, 0);
-    cudaEventDestroy(ready);
-    cudaEventDestroy(done);
-    return s;
+    if (n == 0) return MIND_OK;
+    MLP_CUDA(m, cudaEventRecord(m->ready, stream));
+    MLP_CUDA(m, cudaStreamWaitEvent(m->stream, m->ready, 0));
+    to_bf16_rows_kernel<<<grid(n * m->ld0), kT, 0, m->stream>>>(x, m->x, n, m->dims[0], m->ld0);
+    int32_t *own = m->err;
+    m->err = err;
+    const int s = forward(m, n, false, m->stream, prob);
+    m->err = own;
+    if (s) return s;
+    MLP_CUDA(m, cudaEventRecord(m->done, m->stream));
+    MLP_CUDA(m, cudaStreamWaitEvent(stream, m->done, 0));
+    return MIND_OK;
 }
 
 int mind_mlp_reserve_device(MindMlp *m, int64_t rows) { return reserve(m, rows); }
@@ -330,11 +513,15 @@ extern "C" {
 int mind_mlp_create(const MindMlpConfig *config, MindMlp **out) {
     if (!config || !out) return MIND_EARG;
     *out = nullptr;
-    if (config->n_in < 1 || config->hidden < 1 || config->layers < 1) return MIND_EARG;
+    if (config->n_in < 1 || config->layers < 1 || config->hidden < 16 || config->hidden > 256 ||
+        config->hidden % 16)
+        return MIND_EARG;
     MindMlp *m = new MindMlp();
+    m->hidden = config->hidden;
     m->dims.push_back(config->n_in);
     for (int32_t l = 0; l < config->layers; ++l) m->dims.push_back(config->hidden);
     m->dims.push_back(1);
+    m->maps = (int32_t)m->dims.size() - 1;
     m->ld0 = (config->n_in + 7) / 8 * 8;
     for (size_t l = 0; l + 1 < m->dims.size(); ++l) {
         m->w_off.push_back(m->n_params);
@@ -363,8 +550,7 @@ int mind_mlp_create(const MindMlpConfig *config, MindMlp **out) {
     if (cudaMalloc(&m->grad, m->n_params * sizeof(float)) != cudaSuccess ||
         cudaMalloc(&m->m1, m->n_params * sizeof(float)) != cudaSuccess ||
         cudaMalloc(&m->m2, m->n_params * sizeof(float)) != cudaSuccess ||
-        cudaMalloc(&m->loss, sizeof(float)) != cudaSuccess ||
-        cudaMalloc(&m->gw0, (size_t)m->dims[1] * m->ld0 * sizeof(float)) != cudaSuccess)
+        cudaMalloc(&m->loss, sizeof(float)) != cudaSuccess)
         return fail(m, MIND_ECUDA, "device allocation failed");
     cudaMemset(m->m1, 0, m->n_params * sizeof(float));
     cudaMemset(m->m2, 0, m->n_params * sizeof(float));
@@ -374,19 +560,27 @@ int mind_mlp_create(const MindMlpConfig *config, MindMlp **out) {
 int mind_mlp_destroy(MindMlp *m) {
     if (!m) return MIND_OK;
     if (m->stream) cudaStreamSynchronize(m->stream);
-    for (float *p : m->z) cudaFree(p);
-    for (__nv_bfloat16 *p : m->h) cudaFree(p);
-    for (void *p : {(void *)m->master, (void *)m->grad, (void *)m->m1, (void *)m->m2, (void *)m->wbf, (void *)m->dzb,
-                    (void *)m->dh, (void *)m->dz, (void *)m->y, (void *)m->loss, (void *)m->data_x, (void *)m->data_y,
-                    (void *)m->w0, (void *)m->gw0, (void *)m->part, (void *)m->loss_hist})
+    free_activations(m);
+    for (void *p : {(void *)m->master, (void *)m->grad, (void *)m->m1, (void *)m->m2, (void *)m->wbf, (void *)m->w0,
+                    (void *)m->wt, (void *)m->loss, (void *)m->loss_hist, (void *)m->data_x, (void *)m->data_y,
+                    (void *)m->err})
         cudaFree(p);
-    if (m->blas) cublasDestroy(m->blas);
+    if (m->ready) cudaEventDestroy(m->ready);
+    if (m->done) cudaEventDestroy(m->done);
+    if (m->t0) cudaEventDestroy(m->t0);
+    if (m->t1) cudaEventDestroy(m->t1);
     if (m->stream) cudaStreamDestroy(m->stream);
     delete m;
     return MIND_OK;
 }
 
 const char *mind_mlp_last_error(const MindMlp *m) { return m ? m->error.c_str() : "no network"; }
+
+int mind_mlp_last_ms(const MindMlp *m, float *ms) {
+    if (!m || !ms) return MIND_EARG;
+    *ms = m->last_ms;
+    return MIND_OK;
+}
 
 int mind_mlp_param_count(const MindMlp *m, int64_t *n) {
     if (!m || !n) return MIND_EARG;
@@ -398,19 +592,23 @@ int mind_mlp_set_params(MindMlp *m, const float *params, int64_t n) {
     if (!m || !params || n != m->n_params) return MIND_EARG;
     if (!m->stream) {
         MLP_CUDA(m, cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
-        MLP_BLAS(m, cublasCreate(&m->blas));
-        MLP_BLAS(m, cublasSetStream(m->blas, m->stream));
-        MLP_BLAS(m, cublasSetMathMode(m->blas, CUBLAS_DEFAULT_MATH));
+        MLP_CUDA(m, cudaEventCreateWithFlags(&m->ready, cudaEventDisableTiming));
+        MLP_CUDA(m, cudaEventCreateWithFlags(&m->done, cudaEventDisableTiming));
+        MLP_CUDA(m, cudaEventCreate(&m->t0));
+        MLP_CUDA(m, cudaEventCreate(&m->t1));
+        MLP_CUDA(m, cudaMalloc(&m->err, sizeof(int32_t)));
+        MLP_CUDA(m, cudaMemsetAsync(m->err, 0, sizeof(int32_t), m->stream));
     }
     if (!m->master) {
+        const int64_t H = m->hidden;
         MLP_CUDA(m, cudaMalloc(&m->master, n * sizeof(float)));
         MLP_CUDA(m, cudaMalloc(&m->wbf, n * sizeof(__nv_bfloat16)));
-        MLP_CUDA(m, cudaMalloc(&m->w0, (size_t)m->dims[1] * m->ld0 * sizeof(__nv_bfloat16)));
+        MLP_CUDA(m, cudaMalloc(&m->w0, H * m->ld0 * sizeof(__nv_bfloat16)));
+        MLP_CUDA(m, cudaMemsetAsync(m->w0, 0, H * m->ld0 * sizeof(__nv_bfloat16), m->stream));
+        MLP_CUDA(m, cudaMalloc(&m->wt, std::max<int64_t>(1, (int64_t)(m->maps - 2) * H * H) * sizeof(__nv_bfloat16)));
     }
     MLP_CUDA(m, cudaMemcpyAsync(m->master, params, n * sizeof(float), cudaMemcpyHostToDevice, m->stream));
-    to_bf16_kernel<<<grid(n), kT, 0, m->stream>>>(m->master, m->wbf, n);
-    pad_w0_kernel<<<grid((int64_t)m->dims[1] * m->ld0), kT, 0, m->stream>>>(m->wbf + m->w_off[0], m->w0, m->dims[1],
-                                                                           m->dims[0], m->ld0);
+    copies_kernel<<<grid(n), kT, 0, m->stream>>>(m->master, n, copy_layout(m));
     MLP_CUDA(m, cudaStreamSynchronize(m->stream));
     return MIND_OK;
 }
@@ -424,29 +622,25 @@ int mind_mlp_get_params(const MindMlp *m, float *params, int64_t n) {
 int mind_mlp_predict(MindMlp *m, const float *x, int64_t n, float *prob) {
     if (!m || n < 0 || (n > 0 && (!x || !prob))) return MIND_EARG;
     if (n == 0) return MIND_OK;
-    int s = upload_rows(m, x, n);
-    if (s) return s;
-    s = forward(m, n);
-    if (s) return s;
-    sigmoid_kernel<<<grid(n), kT, 0, m->stream>>>(m->z.back(), m->dz, n);
-    MLP_CUDA(m, cudaMemcpyAsync(prob, m->dz, n * sizeof(float), cudaMemcpyDeviceToHost, m->stream));
-    MLP_CUDA(m, cudaStreamSynchronize(m->stream));
-    return MIND_OK;
+    MLP_TRY(upload_rows(m, x, n));
+    MLP_TRY(forward(m, n, false, m->stream));
+    MLP_TRY(stop_clock(m));
+    MLP_CUDA(m, cudaMemcpyAsync(prob, m->prob, n * sizeof(float), cudaMemcpyDeviceToHost, m->stream));
+    return check(m);
 }
 
 int mind_mlp_gradients(MindMlp *m, const float *x, const float *y, int64_t n, float *grad, float *loss) {
     if (!m || n < 1 || !x || !y || !grad || !loss) return MIND_EARG;
-    int s = upload_rows(m, x, n);
-    if (s) return s;
+    MLP_TRY(reserve(m, n));
     MLP_CUDA(m, cudaMemcpyAsync(m->y, y, n * sizeof(float), cudaMemcpyHostToDevice, m->stream));
-    s = forward(m, n);
-    if (s) return s;
-    s = backward(m, n);
-    if (s) return s;
+    MLP_TRY(upload_rows(m, x, n));
+    transpose_inputs(m, n, m->stream);
+    MLP_TRY(forward(m, n, true, m->stream));
+    MLP_TRY(backward(m, n, m->stream));
+    MLP_TRY(stop_clock(m));
     MLP_CUDA(m, cudaMemcpyAsync(grad, m->grad, m->n_params * sizeof(float), cudaMemcpyDeviceToHost, m->stream));
     MLP_CUDA(m, cudaMemcpyAsync(loss, m->loss, sizeof(float), cudaMemcpyDeviceToHost, m->stream));
-    MLP_CUDA(m, cudaStreamSynchronize(m->stream));
-    return MIND_OK;
+    return check(m);
 }
 
 int mind_mlp_set_data(MindMlp *m, const float *x, const float *y, int64_t n) {
@@ -468,45 +662,40 @@ int mind_mlp_set_data(MindMlp *m, const float *x, const float *y, int64_t n) {
 
 int mind_mlp_train(MindMlp *m, int32_t steps, int32_t batch, float lr, float *losses, float *ms) {
     if (!m || steps < 0 || batch < 1 || m->data_n < 1) return MIND_EARG;
-    int s = reserve(m, batch);
-    if (s) return s;
+    MLP_TRY(reserve(m, batch));
     if (steps > m->loss_cap) {
         cudaFree(m->loss_hist);
         m->loss_hist = nullptr;
         MLP_CUDA(m, cudaMalloc(&m->loss_hist, (size_t)steps * sizeof(float)));
         m->loss_cap = steps;
     }
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    cudaEventRecord(e0, m->stream);
-    for (int32_t k = 0; k < steps; ++k) {
-        gather_kernel<<<grid((int64_t)batch * m->ld0), kT, 0, m->stream>>>(m->data_x, m->data_y, m->h[0], m->y,
+    const CopyLayout C = copy_layout(m);
+    MLP_CUDA(m, cudaEventRecord(m->t0, m->stream));
+    int status = MIND_OK;
+    for (int32_t k = 0; k < steps && !status; ++k) {
+        gather_kernel<<<grid((int64_t)batch * m->ld0), kT, 0, m->stream>>>(m->data_x, m->data_y, m->x, m->y,
                                                                         m->data_n, m->dims[0], m->ld0, batch,
                                                                         (uint64_t)(m->adam_t + 1));
-        s = forward(m, batch);
-        if (s) return s;
-        s = backward(m, batch);
-        if (s) return s;
+        transpose_inputs(m, batch, m->stream);
+        status = forward(m, batch, true, m->stream);
+        if (!status) status = backward(m, batch, m->stream);
+        if (status) break;
         m->adam_t += 1;
         const float c1 = 1.0f - std::pow(0.9f, (float)m->adam_t), c2 = 1.0f - std::pow(0.999f, (float)m->adam_t);
-        adam_kernel<<<grid(m->n_params), kT, 0, m->stream>>>(m->master, m->grad, m->m1, m->m2, m->wbf, m->n_params,
-                                                             lr, c1, c2, m->w0, m->w_off[0],
-                                                             (int64_t)m->dims[0] * m->dims[1], m->dims[0], m->ld0);
+        adam_kernel<<<grid(m->n_params), kT, 0, m->stream>>>(m->master, m->grad, m->m1, m->m2, m->n_params, lr, c1,
+                                                             c2, C);
         // the step's loss stays on the device: no host round trip inside the loop
-        MLP_CUDA(m, cudaMemcpyAsync(m->loss_hist + k, m->loss, sizeof(float), cudaMemcpyDeviceToDevice, m->stream));
+        cudaMemcpyAsync(m->loss_hist + k, m->loss, sizeof(float), cudaMemcpyDeviceToDevice, m->stream);
     }
-    cudaEventRecord(e1, m->stream);
-    if (losses && steps > 0)
-        MLP_CUDA(m, cudaMemcpyAsync(losses, m->loss_hist, (size_t)steps * sizeof(float), cudaMemcpyDeviceToHost,
-                                    m->stream));
-    MLP_CUDA(m, cudaStreamSynchronize(m->stream));
-    float t = 0.0f;
-    cudaEventElapsedTime(&t, e0, e1);
-    if (ms) *ms = t;
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    return MIND_OK;
+    cudaEventRecord(m->t1, m->stream);
+    if (!status && losses && steps > 0)
+        cudaMemcpyAsync(losses, m->loss_hist, (size_t)steps * sizeof(float), cudaMemcpyDeviceToHost, m->stream);
+    const cudaError_t sync = cudaStreamSynchronize(m->stream);
+    if (status) return status;
+    MLP_CUDA(m, sync);
+    const int s = check(m);
+    if (ms) *ms = m->last_ms;
+    return s;
 }
 
 }  // extern "C"

@@ -218,6 +218,7 @@ def load_library():
     lib.mind_mlp_destroy.argtypes = [handle]
     lib.mind_mlp_last_error.argtypes = [handle]
     lib.mind_mlp_last_error.restype = c_char_p
+    lib.mind_mlp_last_ms.argtypes = [handle, f32]
     lib.mind_mlp_param_count.argtypes = [handle, POINTER(c_int64)]
     lib.mind_mlp_set_params.argtypes = [handle, f32, c_int64]
     lib.mind_mlp_get_params.argtypes = [handle, f32, c_int64]
@@ -237,7 +238,7 @@ def load_library():
                  "mind_autotune", "mind_bin_threads", "mind_set_bin_threads", "mind_set_surrogate_cells",
                  "mind_attach_macro", "mind_get_macro_trace", "mind_set_drive_recording", "mind_get_drive",
                  "mind_attach_surrogate",
-                 "mind_mlp_create", "mind_mlp_destroy",
+                 "mind_mlp_create", "mind_mlp_destroy", "mind_mlp_last_ms",
                  "mind_mlp_param_count", "mind_mlp_set_params", "mind_mlp_get_params", "mind_mlp_predict",
                  "mind_mlp_gradients", "mind_mlp_set_data", "mind_mlp_train", "mind_mechanism_count",
                  "mind_mechanism_info", "mind_mechanism_kind", "mind_discretize"):
@@ -253,7 +254,7 @@ EXPORTED_SYMBOLS = (
     "mind_run_noalloc", "mind_inject_spikes", "mind_window_steps", "mind_autotune", "mind_bin_threads",
     "mind_set_surrogate_cells",
     "mind_set_bin_threads", "mind_attach_macro", "mind_get_macro_trace",
-    "mind_set_drive_recording", "mind_get_drive", "mind_attach_surrogate", "mind_mlp_create", "mind_mlp_destroy", "mind_mlp_last_error", "mind_mlp_param_count", "mind_mlp_set_params",
+    "mind_set_drive_recording", "mind_get_drive", "mind_attach_surrogate", "mind_mlp_create", "mind_mlp_destroy", "mind_mlp_last_error", "mind_mlp_last_ms", "mind_mlp_param_count", "mind_mlp_set_params",
     "mind_mlp_get_params", "mind_mlp_predict", "mind_mlp_gradients", "mind_mlp_set_data", "mind_mlp_train",
     "mind_mechanism_count", "mind_mechanism_info", "mind_mechanism_kind", "mind_discretize",
 )

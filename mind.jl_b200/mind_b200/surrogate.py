@@ -48,6 +48,12 @@ class Mlp:
             msg = self.lib.mind_mlp_last_error(self.handle) if self.handle else b""
             raise abi.MindError(status, msg.decode() if msg else "")
 
+    def last_ms(self) -> float:
+        """Device time of the last predict / gradients / train call's network work."""
+        ms = ctypes.c_float()
+        self._check(self.lib.mind_mlp_last_ms(self.handle, ctypes.byref(ms)))
+        return ms.value
+
     @property
     def params(self) -> np.ndarray:
         out = np.zeros(self.n_params, dtype=np.float32)
@@ -273,17 +279,14 @@ def throughput(train_steps: int = 40, batch: int = 4096, rows: int = 1 << 16, in
     _, ms = net.train(x, y, train_steps, batch)
     per_step = ms / train_steps
     xi = rng.uniform(0.0, 1.0, (infer_rows, N_FEATURES)).astype(np.float32)
-    net.predict(xi[:1024])                         # warm-up
-    lib = net.lib
-    out = np.zeros(infer_rows, dtype=np.float32)
-    import time
-    t0 = time.perf_counter()
-    net._check(lib.mind_mlp_predict(net.handle, _f32(xi), infer_rows, _f32(out)))
-    infer_wall = (time.perf_counter() - t0) * 1000.0
+    net.predict(xi)                                # warm-up (buffers sized)
+    net.predict(xi)
+    infer_ms = net.last_ms()
     f = flops_per_row()
     return {"train_ms_per_step": per_step, "batch": batch,
             "train_tflops": 3 * f * batch / (per_step / 1000.0) / 1e12,
-            "infer_rows": infer_rows, "infer_wall_ms_with_copies": infer_wall,
+            "infer_rows": infer_rows, "infer_device_ms": infer_ms,
+            "infer_tflops": f * infer_rows / (infer_ms / 1000.0) / 1e12,
             "flops_per_row_forward": f}
 
 

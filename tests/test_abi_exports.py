@@ -61,7 +61,7 @@ def test_null_handles_are_refused_without_device_work():
         "mind_attach_surrogate": (None, None, None, 1.0), "mind_set_surrogate_cells": (None, None),
         "mind_last_run_ms": (None, ctypes.byref(d)), "mind_run_stats": (None, None),
         "mind_set_profiling": (None, 1), "mind_run_noalloc": (None, 1, None, 0, None),
-        "mind_mlp_param_count": (None, ctypes.byref(i64)), "mind_mlp_set_params": (None, None, 0),
+        "mind_mlp_param_count": (None, ctypes.byref(i64)), "mind_mlp_last_ms": (None, None), "mind_mlp_set_params": (None, None, 0),
         "mind_mlp_get_params": (None, None, 0), "mind_mlp_predict": (None, None, 0, None),
         "mind_mlp_gradients": (None, None, None, 1, None, None), "mind_mlp_set_data": (None, None, None, 1),
         "mind_mlp_train": (None, 1, 1, ctypes.c_float(1e-3), None, None), "mind_mlp_create": (None, None),

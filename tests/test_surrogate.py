@@ -100,3 +100,18 @@ def test_judged_run_reverts_only_the_failing_population():
     assert not final[region == 0].any()                  # population 0 reverted
     assert np.array_equal(final[region == 1], mask[region == 1])   # population 1 kept
     assert len(state.calls) == 1 and np.array_equal(state.calls[0], final)
+
+
+def test_network_shapes_the_tensor_core_kernels_cannot_tile_are_refused():
+    """mind_mlp_create checks its configuration before it touches the device: the hidden
+    width must be a multiple of 16 in [16, 256] (one tensor-core tile spans a hidden layer)."""
+    import ctypes
+
+    from mind_b200 import abi
+
+    lib = abi.load_library()
+    for n_in, hidden, layers in [(645, 20, 3), (645, 272, 3), (645, 0, 3), (0, 256, 3), (645, 256, 0)]:
+        h = ctypes.c_void_p()
+        cfg = abi.MindMlpConfig(n_in, hidden, layers, 1)
+        assert lib.mind_mlp_create(ctypes.byref(cfg), ctypes.byref(h)) == abi.MIND_EARG
+        assert not h.value

@@ -30,6 +30,31 @@ def test_gradients_and_predictions_match_the_fp64_oracle():
     net.close()
 
 
+@pytest.mark.parametrize("n_in,hidden,layers,rows", [(45, 48, 2, 37), (645, 256, 3, 300), (70, 16, 1, 129),
+                                                     (645, 128, 2, 1000)])
+def test_tensor_core_products_on_tile_edges(n_in, hidden, layers, rows):
+    """The tcgen05 products at tile edges: inputs that end inside a 64-column K block,
+    hidden widths below one N tile, one hidden layer (the head reads the inputs directly),
+    batches that end inside a 128-row tile and weight-gradient K slices that end inside a
+    64-row block; gradients and probabilities against the FP64 oracle."""
+    rng = np.random.default_rng(11 + rows)
+    net = surrogate.Mlp(n_in=n_in, hidden=hidden, layers=layers, seed=4)
+    dims = [n_in] + [hidden] * layers + [1]
+    x = rng.normal(0.0, 1.0, (rows, n_in)).astype(np.float32)
+    y = (rng.uniform(size=rows) < 0.3).astype(np.float32)
+    params = net.params.astype(np.float64)
+    want_loss, want = oracle_mlp.loss_and_gradients(params, dims, x, y)
+    got, loss = net.gradients(x, y)
+    err = np.linalg.norm(got - want) / np.linalg.norm(want)
+    cos = float(got @ want / (np.linalg.norm(got) * np.linalg.norm(want)))
+    assert err < 5e-2 and cos > 0.995, (err, cos)
+    assert abs(loss - want_loss) < 1e-2 * want_loss
+    np.testing.assert_allclose(net.predict(x), oracle_mlp.predict(params, dims, x), atol=1e-2)
+    # a second, smaller call reuses the buffers sized for the first
+    np.testing.assert_allclose(net.predict(x[:5]), oracle_mlp.predict(params, dims, x[:5]), atol=1e-2)
+    net.close()
+
+
 def test_trained_surrogate_beats_a_constant_rate():
     """200 cells of a region-coupled network, 600 ms: train on the first 70% of the 1 ms bins,
     test on the rest; the held-out cross-entropy must be 15% below the constant-probability

@@ -98,20 +98,34 @@ def test_noalloc_refuses_step_counts_whose_size_would_wrap():
     assert model.state.time()[0] == 40 and np.all(np.isfinite(trace))
 
 
-def test_noalloc_refuses_a_handle_with_surrogate_cells():
-    """Surrogate inference goes through cuBLAS, which may allocate: status 10, state unchanged."""
+def test_noalloc_runs_a_handle_with_surrogate_cells():
+    """Surrogate inference uses the buffers reserved when the network was attached (its
+    products are this library's own kernels): a noalloc run of a handle with surrogate cells
+    gives the voltages of an ordinary run, bit for bit, over several surrogate bins."""
     from mind_b200 import surrogate
 
     model, _ = netcases.coupled_regions(n_regions=2, cells_per_region=8, synapses=8, seed=3)
     net = surrogate.Mlp(seed=1)
-    state = mb.runtime.DeviceState(model.layout)
-    state.attach_macro(model.macro)
-    state.attach_surrogate(net, np.arange(model.layout.n_cells) % 2 == 0, 1.0)
-    state.initialize()
-    nodes = netcases.soma_nodes(model.layout)
-    status, _ = _noalloc(state, 8, nodes)
-    assert status == abi.MIND_ELAYOUT
-    assert b"surrogate" in state.lib.mind_last_error(state.handle)
-    assert state.time()[0] == 0
-    state.close()
+    params = net.params
+    params[-1] = -1.0                       # output bias: surrogate cells fire now and then
+    net.params = params
+    mask = np.arange(model.layout.n_cells) % 2 == 0
+    nodes = np.asarray(netcases.soma_nodes(model.layout))[~mask]
+    steps = int(round(30.0 / model.layout.dt))
+    traces = []
+    for use_noalloc in (False, True):
+        state = mb.runtime.DeviceState(model.layout)
+        state.attach_macro(model.macro)
+        state.attach_surrogate(net, mask, 1.0)
+        state.initialize()
+        if use_noalloc:
+            status, trace = _noalloc(state, steps, nodes)
+            assert status == abi.MIND_OK, state.lib.mind_last_error(state.handle)
+        else:
+            result = state.run_steps(steps, [mb.RecordSpec(int(n), f"n{n}") for n in nodes], False)
+            trace = np.stack([result.traces[f"n{n}"] for n in nodes], axis=1)
+        assert state.time()[0] == steps
+        traces.append(trace)
+        state.close()
+    np.testing.assert_array_equal(traces[1], traces[0])
     net.close()
