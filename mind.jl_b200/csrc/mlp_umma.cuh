@@ -1,17 +1,18 @@
 /*
  * mlp_umma.cuh — the surrogate network's matrix products on the sm_100a tensor cores.
  *
- * One CTA of four warps computes a 128-row tile of D = A B^T, A [M x K] and B [N x K] both
- * BF16 with K contiguous (K-major), N-tile BN (64, 128 or 256 columns):
+ * One CTA of eight warps computes a 128-row tile of D = A B^T, A [M x K] and B [N x K] both
+ * BF16 with K contiguous (K-major), N-tile BN (64 or 256 columns):
  *   * TMA (cp.async.bulk.tensor.2d) brings 64-column K blocks of A and B into shared memory
  *     in the 128-byte swizzled layout, through a ring of stages guarded by mbarriers (full:
  *     the copy landed; empty: the products reading it completed);
  *   * one thread issues tcgen05.mma (kind::f16, BF16 x BF16 -> FP32, M 128, N BN, K 16;
  *     four per K block) into a BN-column accumulator in tensor memory, and tcgen05.commit
  *     releases each stage to the copy thread;
- *   * after the last product all four warps read the accumulators back (tcgen05.ld, warp w
- *     reading tensor-memory lanes 32w..32w+31 = rows 32w.. of the tile, 16 columns at a
- *     time) and run the layer's elementwise work on them before anything leaves the SM:
+ *   * after the last product all eight warps read the accumulators back (tcgen05.ld: warp w
+ *     reads tensor-memory lanes 32 (w % 4) .. + 31, i.e. one row of the tile per thread, and
+ *     the column half w / 4, 16 columns at a time) and run the layer's elementwise work on
+ *     them before anything leaves the SM:
  *       EPI_HIDDEN  z = acc + b, h = SiLU(z): z (FP32, for the backward pass), h as BF16 rows
  *                   and, for the weight gradients, as BF16 columns (h transposed);
  *       EPI_HEAD    the last hidden map with the 1-wide output map folded in (the tile spans
@@ -44,7 +45,7 @@ namespace mlp {
 
 constexpr int kTileM = 128;           // rows per CTA (= tensor-memory lanes)
 constexpr int kBlockK = 64;           // K columns per stage: 128 bytes of BF16, one swizzle row
-constexpr int kThreads = 128;
+constexpr int kThreads = 256;            // eight warps
 constexpr uint64_t kWaitNs = 2000000000ull;   // 2 s
 
 enum Epilogue { EPI_HIDDEN = 0, EPI_HEAD = 1, EPI_BACK = 2, EPI_F32 = 3 };
@@ -184,21 +185,27 @@ __host__ __device__ constexpr uint32_t idesc_bf16(int m, int n) {
     return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
 }
 
-__device__ __forceinline__ float sigmoid_f(float x) { return 1.0f / (1.0f + __expf(-x)); }
+/* Logistic function with the fast exponential and an approximate reciprocal (relative
+ * error ~1e-7, far below the BF16 rounding of the products' operands). */
+__device__ __forceinline__ float sigmoid_f(float x) { return __fdividef(1.0f, 1.0f + __expf(-x)); }
 
 template <int BN>
 struct Shape {
-    static constexpr int kStages = BN == 256 ? 3 : 4;
+    // K blocks in flight: the products here have 4 to 11 K blocks, so a short ring suffices
+    // and leaves room for 2 (BN 256) or 3 (BN 64) CTAs per SM, whose epilogues overlap
+    static constexpr int kStages = BN == 256 ? 2 : 3;
     static constexpr int kBytesA = kTileM * kBlockK * 2;
     static constexpr int kBytesB = BN * kBlockK * 2;
     static constexpr int kStageBytes = kBytesA + kBytesB;
     // stages (1024-aligned), then 2 * kStages + 1 mbarriers and the tensor-memory slot
     static constexpr int kSmemBytes = 1024 + kStages * kStageBytes + (2 * kStages + 2) * 8;
     static constexpr uint32_t kTmemCols = BN < 32 ? 32 : BN;
+    static constexpr int kCols = BN / 2;   // columns per epilogue warp (two warps per lane quarter)
 };
 
 // ---------------------------------------------------------------------------------------
-// the epilogue: one thread per row of the tile
+// the epilogue: warp w reads tensor-memory lanes 32 (w % 4) .. + 31 (one row per thread) and
+// the column half w / 4 of the tile
 // ---------------------------------------------------------------------------------------
 
 __device__ __forceinline__ float silu_grad(float z) {
@@ -206,101 +213,147 @@ __device__ __forceinline__ float silu_grad(float z) {
     return s * (1.0f + z * (1.0f - s));
 }
 
+/* 16 consecutive floats from 16-byte-aligned memory. */
+__device__ __forceinline__ void load16(const float *p, float (&v)[16]) {
+    const float4 *q = reinterpret_cast<const float4 *>(p);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float4 t = __ldg(q + k);
+        v[4 * k] = t.x;
+        v[4 * k + 1] = t.y;
+        v[4 * k + 2] = t.z;
+        v[4 * k + 3] = t.w;
+    }
+}
+
+__device__ __forceinline__ void store16(float *p, const float (&v)[16]) {
+    float4 *q = reinterpret_cast<float4 *>(p);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) q[k] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+}
+
+/* 16 BF16 values as two 16-byte stores. */
+__device__ __forceinline__ void store16_bf16(__nv_bfloat16 *p, const float (&v)[16]) {
+    uint32_t w[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+        w[j] = (uint32_t)__bfloat16_as_ushort(h.x) | ((uint32_t)__bfloat16_as_ushort(h.y) << 16);
+    }
+    uint4 *q = reinterpret_cast<uint4 *>(p);
+    q[0] = make_uint4(w[0], w[1], w[2], w[3]);
+    q[1] = make_uint4(w[4], w[5], w[6], w[7]);
+}
+
+/* Row-major BF16 rows (vector stores for whole chunks) and, if wanted, the transposed copy. */
+__device__ __forceinline__ void store_rows_cols(const EpiParams &E, int32_t row, int32_t nc, const float (&v)[16]) {
+    if (nc + 16 <= E.N) {
+        store16_bf16(E.rows + (int64_t)row * E.ld_out + nc, v);
+    } else {
+        for (int j = 0; j < 16 && nc + j < E.N; ++j) E.rows[(int64_t)row * E.ld_out + nc + j] = __float2bfloat16(v[j]);
+    }
+    if (E.cols)
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+            if (nc + j < E.N) E.cols[(int64_t)(nc + j) * E.ld_t + row] = __float2bfloat16(v[j]);
+}
+
+/* 16 per-column parameters, zero past N (N and the tile are multiples of 16: whole chunks). */
+__device__ __forceinline__ void column_params(const float *p, int32_t nc, int32_t N, float (&v)[16]) {
+    if (nc + 16 <= N) {
+        load16(p + nc, v);
+    } else {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) v[j] = nc + j < N ? p[nc + j] : 0.0f;
+    }
+}
+
 template <int EPI, int BN>
-__device__ __forceinline__ void epilogue(const EpiParams &E, uint32_t tacc, int32_t row, int32_t n0, int32_t split) {
+__device__ __forceinline__ void epilogue(const EpiParams &E, uint32_t tacc, int32_t row, int32_t c0, int32_t half,
+                                         int32_t split, float *s_logit) {
+    constexpr int C = Shape<BN>::kCols;
     const bool live = row < E.M;
+    const int32_t r = threadIdx.x & 127;   // row within the tile (quarter * 32 + lane)
     if constexpr (EPI == EPI_HEAD) {
-        float logit = 0.0f;
+        // pass 1: this half's share of the logit, SiLU(z) transposed (training)
+        float part = 0.0f;
 #pragma unroll 1
-        for (int c = 0; c < BN; c += 16) {
-            float v[16];
+        for (int c = 0; c < C; c += 16) {
+            float v[16], b[16], w[16];
             tmem_ld16(tacc + c, v);
-            if (!live) continue;
+            const int32_t nc = c0 + c;
+            column_params(E.bias, nc, E.N, b);
+            column_params(E.w_out, nc, E.N, w);
 #pragma unroll
             for (int j = 0; j < 16; ++j) {
-                const int32_t n = n0 + c + j;
-                if (n < E.N) {
-                    const float z = v[j] + E.bias[n];
-                    const float h = z * sigmoid_f(z);
-                    logit += h * E.w_out[n];
-                    if (E.h_cols) E.h_cols[(int64_t)n * E.ld_t + row] = __float2bfloat16(h);
-                }
+                const float z = v[j] + b[j];
+                v[j] = z * sigmoid_f(z);
+                part = fmaf(v[j], w[j], part);
             }
+            if (live && E.h_cols)
+#pragma unroll
+                for (int j = 0; j < 16; ++j)
+                    if (nc + j < E.N) E.h_cols[(int64_t)(nc + j) * E.ld_t + row] = __float2bfloat16(v[j]);
         }
-        logit += E.b_out[0];
+        s_logit[half * kTileM + r] = part;
+        __syncthreads();
+        const float logit = s_logit[r] + s_logit[kTileM + r] + E.b_out[0];
         if (!E.y) {
-            if (live) E.prob[row] = sigmoid_f(logit);
+            if (live && half == 0) E.prob[row] = sigmoid_f(logit);
             return;
         }
         float g = 0.0f;
         if (live) {
             const float t = E.y[row];
-            E.row_loss[row] = fmaxf(logit, 0.0f) - logit * t + log1pf(__expf(-fabsf(logit)));
             g = (sigmoid_f(logit) - t) / E.rows_total;
-            E.dlogit[row] = g;
+            if (half == 0) {
+                E.row_loss[row] = fmaxf(logit, 0.0f) - logit * t + log1pf(__expf(-fabsf(logit)));
+                E.dlogit[row] = g;
+            }
         }
+        // pass 2: the last hidden map's dz = dlogit w_out SiLU'(z)
 #pragma unroll 1
-        for (int c = 0; c < BN; c += 16) {
-            float v[16];
+        for (int c = 0; c < C; c += 16) {
+            float v[16], b[16], w[16];
             tmem_ld16(tacc + c, v);
             if (!live) continue;
+            const int32_t nc = c0 + c;
+            column_params(E.bias, nc, E.N, b);
+            column_params(E.w_out, nc, E.N, w);
 #pragma unroll
-            for (int j = 0; j < 16; ++j) {
-                const int32_t n = n0 + c + j;
-                if (n < E.N) {
-                    const float z = v[j] + E.bias[n];
-                    const __nv_bfloat16 d = __float2bfloat16(g * E.w_out[n] * silu_grad(z));
-                    E.rows[(int64_t)row * E.ld_out + n] = d;
-                    E.cols[(int64_t)n * E.ld_t + row] = d;
-                }
-            }
+            for (int j = 0; j < 16; ++j) v[j] = g * w[j] * silu_grad(v[j] + b[j]);
+            store_rows_cols(E, row, nc, v);
         }
     } else {
 #pragma unroll 1
-        for (int c = 0; c < BN; c += 16) {
+        for (int c = 0; c < C; c += 16) {
             float v[16];
             tmem_ld16(tacc + c, v);
             if (!live) continue;
-            const int32_t nc = n0 + c;
+            const int32_t nc = c0 + c;
+            if (nc >= E.N) continue;
             if constexpr (EPI == EPI_F32) {
                 float *o = E.out + ((int64_t)split * E.M + row) * E.ld_out;
-#pragma unroll
-                for (int j = 0; j < 16; ++j)
-                    if (nc + j < E.n_store) o[nc + j] = v[j];
-            } else {
-                float out[16];
-#pragma unroll
-                for (int j = 0; j < 16; ++j) {
-                    const int32_t n = nc + j;
-                    out[j] = 0.0f;
-                    if (n < E.N) {
-                        if constexpr (EPI == EPI_HIDDEN) {
-                            const float z = v[j] + E.bias[n];
-                            if (E.z) E.z[(int64_t)row * E.ld_out + n] = z;
-                            out[j] = z * sigmoid_f(z);
-                        } else {   // EPI_BACK
-                            out[j] = v[j] * silu_grad(E.z_prev[(int64_t)row * E.ld_out + n]);
-                        }
-                    }
-                }
-                if (nc + 16 <= E.N) {
-                    // 32 bytes per row and chunk: two 16-byte stores (ld_out is a multiple of 8)
-                    uint32_t w[8];
-#pragma unroll
-                    for (int j = 0; j < 8; ++j) {
-                        const __nv_bfloat162 p = __floats2bfloat162_rn(out[2 * j], out[2 * j + 1]);
-                        w[j] = (uint32_t)__bfloat16_as_ushort(p.x) | ((uint32_t)__bfloat16_as_ushort(p.y) << 16);
-                    }
-                    uint4 *dst = reinterpret_cast<uint4 *>(E.rows + (int64_t)row * E.ld_out + nc);
-                    dst[0] = make_uint4(w[0], w[1], w[2], w[3]);
-                    dst[1] = make_uint4(w[4], w[5], w[6], w[7]);
+                if (nc + 16 <= E.n_store && E.ld_out % 4 == 0) {
+                    store16(o + nc, v);
                 } else {
-                    for (int j = 0; j < 16 && nc + j < E.N; ++j)
-                        E.rows[(int64_t)row * E.ld_out + nc + j] = __float2bfloat16(out[j]);
+                    for (int j = 0; j < 16 && nc + j < E.n_store; ++j) o[nc + j] = v[j];
                 }
-                if (E.cols)
-                    for (int j = 0; j < 16 && nc + j < E.N; ++j)
-                        E.cols[(int64_t)(nc + j) * E.ld_t + row] = __float2bfloat16(out[j]);
+            } else if constexpr (EPI == EPI_HIDDEN) {
+                float b[16];
+                column_params(E.bias, nc, E.N, b);
+#pragma unroll
+                for (int j = 0; j < 16; ++j) v[j] += b[j];
+                if (E.z) store16(E.z + (int64_t)row * E.ld_out + nc, v);
+#pragma unroll
+                for (int j = 0; j < 16; ++j) v[j] = v[j] * sigmoid_f(v[j]);
+                store_rows_cols(E, row, nc, v);
+            } else {   // EPI_BACK
+                float z[16];
+                load16(E.z_prev + (int64_t)row * E.ld_out + nc, z);
+#pragma unroll
+                for (int j = 0; j < 16; ++j) v[j] *= silu_grad(z[j]);
+                store_rows_cols(E, row, nc, v);
             }
         }
     }
@@ -310,13 +363,17 @@ __device__ __forceinline__ void epilogue(const EpiParams &E, uint32_t tacc, int3
 // the kernel
 // ---------------------------------------------------------------------------------------
 
-/* grid (ceil(M/128), ceil(N/BN), splits); K blocks [split * kb_per_split, ...) up to kb_total. */
+/* grid (ceil(M/128), ceil(N/BN), splits); K blocks [split * kb_per_split, ...) up to kb_total.
+ * Eight warps: warp 0 lane 0 issues the copies, warp 1 lane 0 the products, and all eight run
+ * the epilogue (two per tensor-memory lane quarter, one column half each). */
 template <int EPI, int BN>
 __global__ void __launch_bounds__(kThreads, 1)
     umma_gemm_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b,
                      int32_t kb_total, int32_t kb_per_split, const EpiParams E) {
     using S = Shape<BN>;
     extern __shared__ unsigned char smem_raw[];
+    __shared__ float s_logit[2 * kTileM];
+    __shared__ int failed;
     unsigned char *base = reinterpret_cast<unsigned char *>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     uint64_t *full = reinterpret_cast<uint64_t *>(base + S::kStages * S::kStageBytes);
     uint64_t *empty = full + S::kStages;
@@ -329,6 +386,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int32_t nkb = min(kb_total - kb0, kb_per_split);
 
     if (threadIdx.x == 0) {
+        failed = 0;
         tma_prefetch_map(&map_a);
         tma_prefetch_map(&map_b);
         for (int s = 0; s < S::kStages; ++s) {
@@ -346,9 +404,6 @@ __global__ void __launch_bounds__(kThreads, 1)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
-    __shared__ int failed;
-    if (threadIdx.x == 0) failed = 0;
-    __syncthreads();
 
     if (nkb > 0 && warp == 0 && lane == 0) {
         // copies: stage s is free again once the products that read it committed
@@ -365,8 +420,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
     } else if (nkb > 0 && warp == 1 && lane == 0) {
         constexpr uint32_t idesc = idesc_bf16(kTileM, BN);
-        int32_t i = 0;
-        for (; i < nkb; ++i) {
+        for (int32_t i = 0; i < nkb; ++i) {
             const int s = i % S::kStages;
             if (!mbar_wait(&full[s], (i / S::kStages) & 1)) {
                 atomicExch(&failed, 1);
@@ -384,14 +438,15 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     __syncwarp();
 
-    const bool ok = nkb > 0 && mbar_wait(done, 0);
+    if (nkb <= 0 || !mbar_wait(done, 0)) atomicExch(&failed, 1);
     __syncthreads();
-    if (!ok || failed) {
+    if (failed) {
         if (threadIdx.x == 0) atomicMax(E.err, (int32_t)MIND_ETIMEOUT);
     } else {
         tc_fence_after();
-        const uint32_t tacc = tmem + ((uint32_t)(warp * 32) << 16);
-        epilogue<EPI, BN>(E, tacc, m0 + warp * 32 + lane, n0, split);
+        const int quarter = warp & 3, half = warp >> 2;
+        const uint32_t tacc = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(half * S::kCols);
+        epilogue<EPI, BN>(E, tacc, m0 + quarter * 32 + lane, n0 + half * S::kCols, half, split, s_logit);
     }
     tc_fence_before();
     __syncthreads();

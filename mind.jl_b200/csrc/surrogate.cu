@@ -51,6 +51,7 @@ struct MindMlp {
     float *loss_hist = nullptr;      // per-step batch losses of a training call
     int32_t loss_cap = 0;
     int64_t adam_t = 0;
+    uint64_t *step_dev = nullptr;    // Adam steps taken, on the device (read by a captured step)
     cudaStream_t stream = nullptr;
     cudaEvent_t ready = nullptr, done = nullptr;
     int32_t *err = nullptr;          // device status word of the products (MIND_ETIMEOUT)
@@ -128,9 +129,12 @@ __global__ void copies_kernel(const float *w, int64_t n, CopyLayout C) {
         store_copies(C, k, w[k]);
 }
 
-/* Adam (beta1 0.9, beta2 0.999, eps 1e-8) on the FP32 masters, then the BF16 copies. */
-__global__ void adam_kernel(float *w, const float *g, float *m1, float *m2, int64_t n, float lr, float c1, float c2,
+/* Adam (beta1 0.9, beta2 0.999, eps 1e-8) on the FP32 masters, then the BF16 copies; the
+ * bias corrections use t = *step + 1. */
+__global__ void adam_kernel(float *w, const float *g, float *m1, float *m2, int64_t n, float lr, const uint64_t *step,
                             CopyLayout C) {
+    const float t = (float)(*step + 1);
+    const float c1 = 1.0f - powf(0.9f, t), c2 = 1.0f - powf(0.999f, t);
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
         const float gk = g[k];
         const float a = 0.9f * m1[k] + 0.1f * gk, b = 0.999f * m2[k] + 0.001f * gk * gk;
@@ -151,10 +155,11 @@ __global__ void to_bf16_rows_kernel(const float *x, __nv_bfloat16 *out, int64_t 
     }
 }
 
-/* Rows of the training set drawn for one step (a 64-bit mix of step and slot), as BF16 rows
- * of stride ld (zero past d), and their targets. */
+/* Rows of the training set drawn for Adam step *step + 1 (a 64-bit mix of step and slot), as
+ * BF16 rows of stride ld (zero past d), and their targets. */
 __global__ void gather_kernel(const float *x, const float *y, __nv_bfloat16 *hx, float *hy, int64_t n, int32_t d,
-                              int32_t ld, int32_t batch, uint64_t step) {
+                              int32_t ld, int32_t batch, const uint64_t *step_dev) {
+    const uint64_t step = *step_dev + 1;
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < (int64_t)batch * ld;
          k += (int64_t)gridDim.x * blockDim.x) {
         const int64_t row = k / ld, col = k % ld;
@@ -229,6 +234,12 @@ __global__ void head_scalars_kernel(const float *dlogit, const float *row_loss, 
     }
 }
 
+/* The end of an Adam step: its loss into the call's history, the step counter advanced. */
+__global__ void step_end_kernel(uint64_t *step, const float *loss, float *hist, uint64_t first) {
+    hist[*step - first] = *loss;
+    *step += 1;
+}
+
 /* grad[k] = sum over the K slices s (in order) of part[s][k], k < n. */
 __global__ void split_sum_kernel(const float *part, int32_t splits, int64_t n, float *grad) {
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
@@ -279,8 +290,6 @@ template <int EPI, int BN>
 int product(MindMlp *m, const __nv_bfloat16 *A, int64_t lda, const __nv_bfloat16 *B, int64_t ldb, int32_t M, int32_t N,
             int32_t K, int32_t splits, mlp::EpiParams E, cudaStream_t s, int32_t *splits_used = nullptr) {
     using S = mlp::Shape<BN>;
-    MLP_CUDA(m, cudaFuncSetAttribute(mlp::umma_gemm_kernel<EPI, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     S::kSmemBytes));
     if (M < 1 || N < 1 || K < 1) return fail(m, MIND_EARG, "empty product");
     CUtensorMap ma, mb;
     MLP_TRY(operand_map(m, &ma, A, K, M, lda, mlp::kTileM));
@@ -297,6 +306,19 @@ int product(MindMlp *m, const __nv_bfloat16 *A, int64_t lda, const __nv_bfloat16
     const dim3 g((M + mlp::kTileM - 1) / mlp::kTileM, (N + BN - 1) / BN, splits);
     mlp::umma_gemm_kernel<EPI, BN><<<g, mlp::kThreads, S::kSmemBytes, s>>>(ma, mb, kb_total, per, E);
     MLP_CUDA(m, cudaGetLastError());
+    return MIND_OK;
+}
+
+/* Shared-memory opt-in of the product kernels (once per network, on its device). */
+int prepare_products(MindMlp *m) {
+    MLP_CUDA(m, cudaFuncSetAttribute(mlp::umma_gemm_kernel<mlp::EPI_HIDDEN, 64>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, mlp::Shape<64>::kSmemBytes));
+    MLP_CUDA(m, cudaFuncSetAttribute(mlp::umma_gemm_kernel<mlp::EPI_BACK, 64>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, mlp::Shape<64>::kSmemBytes));
+    MLP_CUDA(m, cudaFuncSetAttribute(mlp::umma_gemm_kernel<mlp::EPI_F32, 64>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, mlp::Shape<64>::kSmemBytes));
+    MLP_CUDA(m, cudaFuncSetAttribute(mlp::umma_gemm_kernel<mlp::EPI_HEAD, 256>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, mlp::Shape<256>::kSmemBytes));
     return MIND_OK;
 }
 
@@ -563,7 +585,7 @@ int mind_mlp_destroy(MindMlp *m) {
     free_activations(m);
     for (void *p : {(void *)m->master, (void *)m->grad, (void *)m->m1, (void *)m->m2, (void *)m->wbf, (void *)m->w0,
                     (void *)m->wt, (void *)m->loss, (void *)m->loss_hist, (void *)m->data_x, (void *)m->data_y,
-                    (void *)m->err})
+                    (void *)m->err, (void *)m->step_dev})
         cudaFree(p);
     if (m->ready) cudaEventDestroy(m->ready);
     if (m->done) cudaEventDestroy(m->done);
@@ -598,6 +620,8 @@ int mind_mlp_set_params(MindMlp *m, const float *params, int64_t n) {
         MLP_CUDA(m, cudaEventCreate(&m->t1));
         MLP_CUDA(m, cudaMalloc(&m->err, sizeof(int32_t)));
         MLP_CUDA(m, cudaMemsetAsync(m->err, 0, sizeof(int32_t), m->stream));
+        MLP_CUDA(m, cudaMalloc(&m->step_dev, sizeof(uint64_t)));
+        MLP_TRY(prepare_products(m));
     }
     if (!m->master) {
         const int64_t H = m->hidden;
@@ -670,29 +694,42 @@ int mind_mlp_train(MindMlp *m, int32_t steps, int32_t batch, float lr, float *lo
         m->loss_cap = steps;
     }
     const CopyLayout C = copy_layout(m);
-    MLP_CUDA(m, cudaEventRecord(m->t0, m->stream));
-    int status = MIND_OK;
-    for (int32_t k = 0; k < steps && !status; ++k) {
-        gather_kernel<<<grid((int64_t)batch * m->ld0), kT, 0, m->stream>>>(m->data_x, m->data_y, m->x, m->y,
-                                                                        m->data_n, m->dims[0], m->ld0, batch,
-                                                                        (uint64_t)(m->adam_t + 1));
-        transpose_inputs(m, batch, m->stream);
-        status = forward(m, batch, true, m->stream);
-        if (!status) status = backward(m, batch, m->stream);
-        if (status) break;
-        m->adam_t += 1;
-        const float c1 = 1.0f - std::pow(0.9f, (float)m->adam_t), c2 = 1.0f - std::pow(0.999f, (float)m->adam_t);
-        adam_kernel<<<grid(m->n_params), kT, 0, m->stream>>>(m->master, m->grad, m->m1, m->m2, m->n_params, lr, c1,
-                                                             c2, C);
-        // the step's loss stays on the device: no host round trip inside the loop
-        cudaMemcpyAsync(m->loss_hist + k, m->loss, sizeof(float), cudaMemcpyDeviceToDevice, m->stream);
+    // One Adam step is captured as a graph and replayed `steps` times: the batch draw and the
+    // bias corrections read the device step counter, which the step's last kernel advances.
+    const uint64_t first = (uint64_t)m->adam_t;
+    MLP_CUDA(m, cudaMemcpyAsync(m->step_dev, &first, sizeof first, cudaMemcpyHostToDevice, m->stream));
+    MLP_CUDA(m, cudaStreamSynchronize(m->stream));
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    MLP_CUDA(m, cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal));
+    gather_kernel<<<grid((int64_t)batch * m->ld0), kT, 0, m->stream>>>(m->data_x, m->data_y, m->x, m->y, m->data_n,
+                                                                    m->dims[0], m->ld0, batch, m->step_dev);
+    transpose_inputs(m, batch, m->stream);
+    int status = forward(m, batch, true, m->stream);
+    if (!status) status = backward(m, batch, m->stream);
+    adam_kernel<<<grid(m->n_params), kT, 0, m->stream>>>(m->master, m->grad, m->m1, m->m2, m->n_params, lr,
+                                                         m->step_dev, C);
+    step_end_kernel<<<1, 1, 0, m->stream>>>(m->step_dev, m->loss, m->loss_hist, first);
+    const cudaError_t captured = cudaStreamEndCapture(m->stream, &graph);
+    if (status) {
+        if (graph) cudaGraphDestroy(graph);
+        return status;
     }
+    MLP_CUDA(m, captured);
+    const cudaError_t made = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    MLP_CUDA(m, made);
+    MLP_CUDA(m, cudaEventRecord(m->t0, m->stream));
+    cudaError_t launched = cudaSuccess;
+    for (int32_t k = 0; k < steps && launched == cudaSuccess; ++k) launched = cudaGraphLaunch(exec, m->stream);
     cudaEventRecord(m->t1, m->stream);
-    if (!status && losses && steps > 0)
+    if (launched == cudaSuccess && losses && steps > 0)
         cudaMemcpyAsync(losses, m->loss_hist, (size_t)steps * sizeof(float), cudaMemcpyDeviceToHost, m->stream);
     const cudaError_t sync = cudaStreamSynchronize(m->stream);
-    if (status) return status;
+    cudaGraphExecDestroy(exec);
+    MLP_CUDA(m, launched);
     MLP_CUDA(m, sync);
+    m->adam_t += steps;
     const int s = check(m);
     if (ms) *ms = m->last_ms;
     return s;
