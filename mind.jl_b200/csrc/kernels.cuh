@@ -591,10 +591,46 @@ __device__ __forceinline__ void hines_exact(double *sd, double *sr, const double
  * segment's steps (the D step is the Mobius map D -> (d D - a^2) / D, a 2x2 matrix; the R and x
  * steps are affine maps), a warp scan composes the segments, and each lane then runs the
  * ordinary recurrence over its own segment from the value the scan gives at its boundary.
- * The depth falls from L to about 2 L / 32 + 5 combining steps.  Only the rounding of the
- * boundary values changes, so this is used in the mixed mode only; the FP64 mode keeps the
- * oracle's sequential order. */
-constexpr int32_t kWarpChain = 24;   // chains at least this long are solved by a warp (mixed mode)
+ * The depth falls from L to about 2 L / 32 + 5 combining steps, at a fixed cost of three
+ * warp scans.  Only the rounding of the boundary values changes, so this is used in the mixed
+ * mode only; the FP64 mode keeps the oracle's sequential order.
+ *
+ * Which chains of a level go to warps (warp_chains): the planner orders a level's chains
+ * longest first, and a level hands its k longest chains to the last k warps of the CTA
+ * when that shortens the level, by a latency model in cycles: a thread takes
+ * kThreadNodeCycles per node, a warp kWarpFixedCycles plus kWarpSegmentCycles per node of a
+ * lane's segment.  A level with many long chains (the leaves of a pyramidal cell) keeps
+ * them on threads, which run side by side; a level whose one chain is far longer than the
+ * rest (a trunk) gives it a warp. */
+#ifndef MIND_WARP_FIXED_CYCLES
+#define MIND_WARP_FIXED_CYCLES 2600
+#endif
+#ifndef MIND_WARP_SEGMENT_CYCLES
+#define MIND_WARP_SEGMENT_CYCLES 650
+#endif
+constexpr int32_t kThreadNodeCycles = 100;
+constexpr int32_t kWarpFixedCycles = MIND_WARP_FIXED_CYCLES;
+constexpr int32_t kWarpSegmentCycles = MIND_WARP_SEGMENT_CYCLES;
+
+/* Number of the level's chains [lo, hi) (longest first) that warps solve; the same on every
+ * thread. */
+template <int NT>
+__device__ __forceinline__ int32_t warp_chains(const int32_t *clen, int32_t lo, int32_t hi) {
+    constexpr int32_t NW = NT / 32;
+    const int32_t L0 = clen[lo];
+    const int32_t wcost = kWarpFixedCycles + kWarpSegmentCycles * ((L0 + 31) / 32);
+    int32_t best = 0, best_cost = kThreadNodeCycles * L0;
+    for (int32_t k = 1; k <= NW && lo + k <= hi; ++k) {
+        const int32_t rest = lo + k < hi ? kThreadNodeCycles * clen[lo + k] : 0;
+        // with every warp busy, the thread-mode chains run on their lanes first
+        const int32_t cost = (k == NW && rest > 0) ? rest + wcost : max(rest, wcost);
+        if (cost < best_cost) {
+            best_cost = cost;
+            best = k;
+        }
+    }
+    return best;
+}
 
 struct Mobius {   // x -> (a x + b) / (c x + d)
     double a, b, c, d;
@@ -638,26 +674,6 @@ __device__ __forceinline__ Affine warp_exclusive(Affine v, int lane) {
     Affine e{__shfl_up_sync(0xffffffffu, v.m, 1), __shfl_up_sync(0xffffffffu, v.c, 1)};
     if (lane == 0) e = Affine{1.0, 0.0};
     return e;
-}
-
-/* Calls f(ch) for the chains in [lo, hi) of at least kWarpChain nodes, each on one warp of the
- * CTA in turn; every lane of every warp runs this with the same lo, hi. */
-template <int NT, class F>
-__device__ __forceinline__ void for_each_long_chain(const int32_t *clen, int32_t lo, int32_t hi, F f) {
-    constexpr int32_t NW = NT / 32;
-    const int32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int32_t k = 0;
-    __syncwarp();
-    for (int32_t base = lo; base < hi; base += 32) {
-        const int32_t ch = base + lane;
-        uint32_t mask = __ballot_sync(0xffffffffu, ch < hi && clen[ch] >= kWarpChain);
-        while (mask) {
-            const int32_t j = __ffs(mask) - 1;
-            mask &= mask - 1;
-            if (k % NW == warp) f(base + j);
-            ++k;
-        }
-    }
 }
 
 /* Elimination of one long chain by a warp, with the mixed mode's arithmetic (reciprocal
@@ -771,7 +787,7 @@ __device__ __forceinline__ void substitute_chain_warp(int32_t ch, double *sd, do
  * Hines solve, mixed mode: FP64 arithmetic with reciprocals.  Elimination keeps, per
  * node, f = a/D in place of D and R/D in place of R, so the back-substitution is one
  * FMA per node, x = f x_p + R/D; the pivot chain is D -> 1/D -> (a^2)(1/D) -> next D.
- * Chains of kWarpChain nodes or more go to a warp each (eliminate_chain_warp,
+ * A level's longest chains may go to a warp each (warp_chains, eliminate_chain_warp,
  * substitute_chain_warp); the others to one thread each.
  */
 template <int NT>
@@ -781,9 +797,12 @@ __device__ __forceinline__ void hines_mixed(double *sd, double *sr, const double
                                             const int32_t *lvc, int32_t nlev, double vscale, bool &singular) {
     constexpr int32_t T = NT;
     const int32_t tid = threadIdx.x;
+    const int32_t warp = tid >> 5;
+    constexpr int32_t NW = NT / 32;
     for (int32_t lv = 0; lv < nlev; ++lv) {
-        for (int32_t ch = lvc[lv] + tid; ch < lvc[lv + 1]; ch += T) {
-            if (clen[ch] >= kWarpChain) continue;   // a warp's, below
+        const int32_t lo = lvc[lv], hi = lvc[lv + 1];
+        const int32_t kw = warp_chains<NT>(clen, lo, hi);
+        for (int32_t ch = lo + kw + tid; ch < hi; ch += T) {
             const int32_t top = ctop[ch];
             const int32_t bottom = top + clen[ch] - 1;
             const bool rooted = cpar[ch] < 0;
@@ -833,14 +852,14 @@ __device__ __forceinline__ void hines_mixed(double *sd, double *sr, const double
             sxd[ch] = rooted ? 0.0 : pxd;
             sxr[ch] = rooted ? 0.0 : pxr;
         }
-        for_each_long_chain<NT>(clen, lvc[lv], lvc[lv + 1], [&](int32_t ch) {
-            eliminate_chain_warp(ch, sd, sr, sa, sxd, sxr, ctop, clen, cpar, ckoff, ckids, singular);
-        });
+        if (NW - 1 - warp < kw)   // the last kw warps take the level's kw longest chains
+            eliminate_chain_warp(lo + NW - 1 - warp, sd, sr, sa, sxd, sxr, ctop, clen, cpar, ckoff, ckids, singular);
         __syncthreads();
     }
     for (int32_t lv = nlev - 1; lv >= 0; --lv) {
-        for (int32_t ch = lvc[lv] + tid; ch < lvc[lv + 1]; ch += T) {
-            if (clen[ch] >= kWarpChain) continue;   // a warp's, below
+        const int32_t lo = lvc[lv], hi = lvc[lv + 1];
+        const int32_t kw = warp_chains<NT>(clen, lo, hi);
+        for (int32_t ch = lo + kw + tid; ch < hi; ch += T) {
             const int32_t top = ctop[ch];
             const int32_t bottom = top + clen[ch] - 1;
             const int32_t par = cpar[ch];
@@ -863,9 +882,7 @@ __device__ __forceinline__ void hines_mixed(double *sd, double *sr, const double
                 sv[i] = sv[i] + vscale * x;
             }
         }
-        for_each_long_chain<NT>(clen, lvc[lv], lvc[lv + 1], [&](int32_t ch) {
-            substitute_chain_warp(ch, sd, sr, sv, ctop, clen, cpar, vscale);
-        });
+        if (NW - 1 - warp < kw) substitute_chain_warp(lo + NW - 1 - warp, sd, sr, sv, ctop, clen, cpar, vscale);
         __syncthreads();
     }
 }

@@ -442,7 +442,11 @@ int create(const MindLayout *L, MindHandle *h) {
         }
         std::vector<int32_t> order(tops.size());
         for (size_t k = 0; k < order.size(); ++k) order[k] = (int32_t)k;
-        std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) { return level[x] < level[y]; });
+        // by level, and within a level longest first (the mixed mode hands a level's longest
+        // chains to warps); each chain's elimination is independent of the order of its level
+        std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) {
+            return level[x] < level[y] || (level[x] == level[y] && chains[x].size() > chains[y].size());
+        });
         std::vector<int32_t> rank(tops.size());
         for (size_t k = 0; k < order.size(); ++k) rank[order[k]] = (int32_t)k;
         // packed order: chains by rank, nodes top -> bottom

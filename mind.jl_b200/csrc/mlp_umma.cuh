@@ -23,8 +23,10 @@
  *                   and columns;
  *       EPI_BACK    dz_prev = acc * SiLU'(z_prev) (acc = dz W, the gradient reaching the
  *                   previous map's output) as BF16 rows and columns;
- *       EPI_F32     the FP32 accumulators themselves (weight gradients; a K split writes
- *                   its own slice, summed in a fixed order afterwards).
+ *       EPI_F32     the FP32 accumulators themselves, column-major so that a warp's stores
+ *                   are contiguous (weight gradients, computed transposed: the column-major
+ *                   D = dW^T is dW row-major; a K split writes its own slice, summed in a
+ *                   fixed order afterwards).
  * Rows and columns past M and N read as zeros (TMA fills them) and are not stored.
  *
  * Every wait is bounded by the global timer: past kWaitNs a thread raises MIND_ETIMEOUT in
@@ -52,7 +54,7 @@ enum Epilogue { EPI_HIDDEN = 0, EPI_HEAD = 1, EPI_BACK = 2, EPI_F32 = 3 };
 
 struct EpiParams {
     int32_t M, N;                 // valid rows and columns of D
-    int32_t n_store;              // EPI_F32: columns stored (<= N)
+    int32_t n_store;              // unused
     int32_t ld_out;               // row stride of the row-major outputs (elements)
     int32_t ld_t;                 // row stride of the transposed outputs (elements)
     const float *bias;            // [N]
@@ -68,7 +70,7 @@ struct EpiParams {
     float *row_loss;              // EPI_HEAD training: per-row cross-entropy [M]
     __nv_bfloat16 *h_cols;        // EPI_HEAD training: SiLU(z) transposed [N x ld_t]
     float rows_total;             // EPI_HEAD training: the mean's denominator
-    float *out;                   // EPI_F32: [splits][M][ld_out]
+    float *out;                   // EPI_F32: D column-major, [splits][N][ld_out] (ld_out >= M)
     int32_t *err;
 };
 
@@ -270,7 +272,7 @@ __device__ __forceinline__ void column_params(const float *p, int32_t nc, int32_
 
 template <int EPI, int BN>
 __device__ __forceinline__ void epilogue(const EpiParams &E, uint32_t tacc, int32_t row, int32_t c0, int32_t half,
-                                         int32_t split, float *s_logit) {
+                                         int32_t split, float *s_logit, const float *pre) {
     constexpr int C = Shape<BN>::kCols;
     const bool live = row < E.M;
     const int32_t r = threadIdx.x & 127;   // row within the tile (quarter * 32 + lane)
@@ -325,20 +327,19 @@ __device__ __forceinline__ void epilogue(const EpiParams &E, uint32_t tacc, int3
             store_rows_cols(E, row, nc, v);
         }
     } else {
-#pragma unroll 1
-        for (int c = 0; c < C; c += 16) {
+#pragma unroll
+        for (int c = 0; c < C; c += 16) {   // C = 32: two chunks, unrolled (pre[] stays in registers)
             float v[16];
             tmem_ld16(tacc + c, v);
             if (!live) continue;
             const int32_t nc = c0 + c;
             if (nc >= E.N) continue;
             if constexpr (EPI == EPI_F32) {
-                float *o = E.out + ((int64_t)split * E.M + row) * E.ld_out;
-                if (nc + 16 <= E.n_store && E.ld_out % 4 == 0) {
-                    store16(o + nc, v);
-                } else {
-                    for (int j = 0; j < 16 && nc + j < E.n_store; ++j) o[nc + j] = v[j];
-                }
+                // column-major: a column's 32 rows of this warp are 128 contiguous bytes
+                float *o = E.out + ((int64_t)split * E.N + nc) * E.ld_out + row;
+#pragma unroll
+                for (int j = 0; j < 16; ++j)
+                    if (nc + j < E.N) o[(int64_t)j * E.ld_out] = v[j];
             } else if constexpr (EPI == EPI_HIDDEN) {
                 float b[16];
                 column_params(E.bias, nc, E.N, b);
@@ -348,11 +349,9 @@ __device__ __forceinline__ void epilogue(const EpiParams &E, uint32_t tacc, int3
 #pragma unroll
                 for (int j = 0; j < 16; ++j) v[j] = v[j] * sigmoid_f(v[j]);
                 store_rows_cols(E, row, nc, v);
-            } else {   // EPI_BACK
-                float z[16];
-                load16(E.z_prev + (int64_t)row * E.ld_out + nc, z);
+            } else {   // EPI_BACK: z_prev was loaded while the products ran
 #pragma unroll
-                for (int j = 0; j < 16; ++j) v[j] *= silu_grad(z[j]);
+                for (int j = 0; j < 16; ++j) v[j] *= silu_grad(pre[c + j]);
                 store_rows_cols(E, row, nc, v);
             }
         }
@@ -438,15 +437,33 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     __syncwarp();
 
+    const int quarter = warp & 3, half = warp >> 2;
+    const int32_t row = m0 + quarter * 32 + lane, c0 = n0 + half * S::kCols;
+    // operands of the epilogue that do not depend on the products, loaded while they run
+    float pre[EPI == EPI_BACK ? S::kCols : 1];
+    if constexpr (EPI == EPI_BACK) {
+#pragma unroll
+        for (int c = 0; c < S::kCols; c += 16) {
+            float z[16];
+            if (row < E.M && c0 + c + 16 <= E.N) {
+                load16(E.z_prev + (int64_t)row * E.ld_out + c0 + c, z);
+            } else {
+#pragma unroll
+                for (int j = 0; j < 16; ++j)
+                    z[j] = (row < E.M && c0 + c + j < E.N) ? E.z_prev[(int64_t)row * E.ld_out + c0 + c + j] : 0.0f;
+            }
+#pragma unroll
+            for (int j = 0; j < 16; ++j) pre[c + j] = z[j];
+        }
+    }
     if (nkb <= 0 || !mbar_wait(done, 0)) atomicExch(&failed, 1);
     __syncthreads();
     if (failed) {
         if (threadIdx.x == 0) atomicMax(E.err, (int32_t)MIND_ETIMEOUT);
     } else {
         tc_fence_after();
-        const int quarter = warp & 3, half = warp >> 2;
         const uint32_t tacc = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(half * S::kCols);
-        epilogue<EPI, BN>(E, tacc, m0 + quarter * 32 + lane, n0 + half * S::kCols, half, split, s_logit);
+        epilogue<EPI, BN>(E, tacc, row, c0, half, split, s_logit, pre);
     }
     tc_fence_before();
     __syncthreads();

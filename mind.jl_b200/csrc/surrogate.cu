@@ -443,16 +443,16 @@ int backward(MindMlp *m, int64_t rows, cudaStream_t s) {
     int cur = 0;
     for (int32_t l = last; l >= 0; --l) {
         const int32_t in = l == 0 ? m->dims[0] : H;
-        // dW_l [H x in] = dz_l^T h_l: A = dz_l transposed [H x R], B = h_l transposed [in x R]
-        const __nv_bfloat16 *Bt = l == 0 ? m->xt : m->ht[l - 1];
-        const int32_t tiles = ((H + 127) / 128) * ((in + 63) / 64);
+        // dW_l^T [in x H] = h_l^T dz_l: A = h_l transposed [in x R], B = dz_l transposed [H x R];
+        // stored column-major, which is dW_l [H x in] row-major, the parameters' layout
+        const __nv_bfloat16 *At = l == 0 ? m->xt : m->ht[l - 1];
+        const int32_t tiles = ((in + 127) / 128) * ((H + 63) / 64);
         const int32_t splits = grad_splits(tiles, rows);
         mlp::EpiParams E{};
-        E.n_store = in;
         E.ld_out = in;
         E.out = m->part;
         int32_t used = 1;
-        MLP_TRY((product<mlp::EPI_F32, 64>(m, m->dzc[cur], T, Bt, T, H, in, R, splits, E, s, &used)));
+        MLP_TRY((product<mlp::EPI_F32, 64>(m, At, T, m->dzc[cur], T, in, H, R, splits, E, s, &used)));
         split_sum_kernel<<<grid((int64_t)H * in), kT, 0, s>>>(m->part, used, (int64_t)H * in, m->grad + m->w_off[l]);
         rowsum_kernel<<<H, kT, 0, s>>>(m->dzc[cur], T, rows, nullptr, m->grad + m->b_off[l]);
         if (l == 0) break;
