@@ -294,10 +294,14 @@ def measure_sharded(args, layout, rank: int, world: int, precision: str, local_r
              np.concatenate([r.spike_times for r in rasters])), clocks)
 
 
-def measure_surrogate(args, model, layout, train_ms: float = 300.0, eval_ms: float = 200.0, keep: float = 0.02):
-    """Config 4 with the surrogate: train on a detailed FP64 run of train_ms, then run eval_ms
-    from initialize twice — plain FP64, and with all but `keep` of the cells replaced — and
-    compare time per step and the regions' population rates (10 ms bins)."""
+def measure_surrogate(args, model, layout, train_ms: float = 300.0, eval_ms: float = 1000.0, keep: float = 0.02,
+                      calibration_ms: float = 100.0, calibration_rounds: int = 4):
+    """Config 4 with the surrogate: train on a detailed FP64 run of train_ms, calibrate one
+    logit offset per population on the coupled run (calibration_rounds runs of
+    calibration_ms, towards the training run's population rates), then run eval_ms from
+    initialize twice — plain FP64, and with all but `keep` of the cells replaced — and
+    compare time per step and the regions' population rates over the whole eval_ms (which
+    extends past the training period)."""
     import mind_b200 as mb
     from mind_b200 import surrogate
 
@@ -312,9 +316,14 @@ def measure_surrogate(args, model, layout, train_ms: float = 300.0, eval_ms: flo
     plain, plain_ms = device_timed(lambda: model.state.run_steps(steps, []))
     rng = np.random.default_rng(0)
     mask = rng.uniform(size=layout.n_cells) >= keep
+    target_hz = surrogate.population_rates(layout, macro, train_run, train_ms)
     state = mb.runtime.DeviceState(layout, "mixed")   # the tuned mode for the detailed sample
     state.attach_macro(macro)
     state.attach_surrogate(net, mask, scale)
+    t_c = time.perf_counter()
+    offsets, cal_rates = surrogate.calibrate(state, layout, macro, mask, target_hz, calibration_ms,
+                                             calibration_rounds)
+    calibration_s = time.perf_counter() - t_c
     state.initialize()
     sur, sur_ms = device_timed(lambda: state.run_steps(steps, []))
     state.close()
@@ -323,6 +332,7 @@ def measure_surrogate(args, model, layout, train_ms: float = 300.0, eval_ms: flo
     state = mb.runtime.DeviceState(layout, "mixed")
     state.attach_macro(macro)
     state.attach_surrogate(net, mask, scale)
+    state.set_surrogate_offsets(offsets)
     state.initialize()
     t_j = time.perf_counter()
     judged, log, final_mask = surrogate.judged_run(state, layout, macro, mask, eval_ms, window_ms=20.0, bound=0.05)
@@ -337,6 +347,11 @@ def measure_surrogate(args, model, layout, train_ms: float = 300.0, eval_ms: flo
     mean_plain = r_plain.mean(axis=0)
     rel = np.abs(r_sur.mean(axis=0) - mean_plain) / np.maximum(mean_plain, 1e-9)
     rel_j = np.abs(r_judged.mean(axis=0) - mean_plain) / np.maximum(mean_plain, 1e-9)
+    # counting noise of two independent runs' rate estimates per region: sqrt(2 / spikes)
+    spikes_plain = mean_plain * (eval_ms * 1e-3) * np.bincount(
+        surrogate.cell_regions(layout, macro)[surrogate.cell_regions(layout, macro) >= 0], minlength=macro.n_regions)
+    noise = np.sqrt(2.0 / np.maximum(spikes_plain, 1.0))
+    pooled = abs(r_sur.mean() - r_plain.mean()) / max(r_plain.mean(), 1e-9)
     units = layout.segment_count * steps
     return {
         "metric": "compartment-steps/s (config 4, equivalent: every cell's compartments counted)",
@@ -346,7 +361,8 @@ def measure_surrogate(args, model, layout, train_ms: float = 300.0, eval_ms: flo
         "surrogate": {"value": units / (sur_ms / 1000.0), "ms_per_step": sur_ms / steps},
         "speedup": plain_ms / sur_ms,
         "population_rate_error": {"per_region_mean_rel": rel.tolist(), "max_rel": float(rel.max()),
-                                  "mean_rel": float(rel.mean()),
+                                  "mean_rel": float(rel.mean()), "pooled_rel": float(pooled),
+                                  "counting_noise_per_region_mean": float(noise.mean()),
                                   "plain_rate_hz": mean_plain.tolist(),
                                   "surrogate_rate_hz": r_sur.mean(axis=0).tolist()},
         "judged": {"value": units / (judged_ms / 1000.0), "ms_per_step": judged_ms / steps,
@@ -356,6 +372,12 @@ def measure_surrogate(args, model, layout, train_ms: float = 300.0, eval_ms: flo
                    "population_rate_error": {"mean_rel": float(rel_j.mean()), "max_rel": float(rel_j.max())},
                    "rule": "every 20 ms, over the run so far: |rate(surrogate) - rate(sample)| > 0.05 rate(sample)"
                            " + 3 Poisson standard errors reverts the population"},
+        "calibration": {"rounds": calibration_rounds, "ms_per_round": calibration_ms, "wall_s": calibration_s,
+                        "target_hz": target_hz.tolist(),
+                        "surrogate_hz_per_round": [np.nan_to_num(r).tolist() for r in cal_rates],
+                        "offsets_per_region": [float(offsets[surrogate.cell_regions(layout, macro) == p][0])
+                                               if np.any(surrogate.cell_regions(layout, macro) == p) else 0.0
+                                               for p in range(macro.n_regions)]},
         "training": {"windows": int((train_run.drive.shape[0] - surrogate.WINDOW_BINS) * layout.n_cells),
                      "steps": 500, "batch": 4096, "wall_s": train_s},
         "note": "plain: every cell in FP64; surrogate: the detailed sample in the mixed mode, the rest "

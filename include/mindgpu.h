@@ -359,6 +359,12 @@ int mind_attach_surrogate(MindHandle *h, MindMlp *mlp, const uint8_t *surrogate_
  * detailed); a cell staying keeps its spike history.  This is how a host judge reverts a
  * population whose surrogate rate drifts from its detailed sample. */
 int mind_set_surrogate_cells(MindHandle *h, const uint8_t *surrogate_cells);
+/* Per-cell calibration of the surrogate (n_cells = the layout's cell count, layout order):
+ * a surrogate cell spikes with probability sigmoid(logit + logit_offset[c]) instead of
+ * sigmoid(logit).  All offsets are 0 after mind_attach_surrogate; a host sets them per
+ * population so that the coupled run keeps each population's rate
+ * (mind_b200.surrogate.calibrate).  Offsets must be finite. */
+int mind_set_surrogate_offsets(MindHandle *h, const float *logit_offset, int32_t n_cells);
 
 /* Keep a training set on the device; then `steps` Adam steps (beta 0.9/0.999, eps 1e-8) on
  * batches drawn with replacement; losses[k] = the batch loss before step k (may be NULL). */

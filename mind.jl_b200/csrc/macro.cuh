@@ -190,18 +190,26 @@ __global__ void surrogate_features_kernel(const Params P, const int32_t *cells, 
     }
 }
 
-/* Each surrogate cell spikes in bin b with the predicted probability (u0 < p, Philox on
- * (b, cell)), at b * bin_ms + bin_ms * u1; the spike is recorded, fanned out through the
- * cell's NetCons and counted in its region's bin like a detected spike. */
+/* Each surrogate cell spikes in bin b with the predicted probability, its logit shifted by
+ * the cell's calibration offset (u0 < p, Philox on (b, cell)), at b * bin_ms + bin_ms * u1;
+ * the spike is recorded, fanned out through the cell's NetCons and counted in its region's
+ * bin like a detected spike. */
 __global__ void surrogate_spike_kernel(const Params P, const int32_t *cells, const int32_t *sources, int32_t n,
-                                       const float *prob, int32_t *spikes, int64_t b, double bin_ms,
+                                       const float *prob, const float *offset, int32_t *spikes, int64_t b,
+                                       double bin_ms,
                                        const int32_t *source_region, int32_t *bins, int32_t n_regions,
                                        int32_t bin_ring, int64_t min_bin) {
     for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         uint32_t ctr[4] = {(uint32_t)b, (uint32_t)((uint64_t)b >> 32), (uint32_t)cells[i], 0x5355u};
         mind_philox4x32_10(ctr, (uint32_t)P.seed, (uint32_t)(P.seed >> 32));
         const double u0 = ((double)ctr[0] + 1.0) * MIND_INV_2P32P1, u1 = ((double)ctr[1] + 1.0) * MIND_INV_2P32P1;
-        const bool fire = u0 < (double)prob[i];
+        double p = prob[i];
+        const double shift = offset[cells[i]];
+        if (shift != 0.0) {   // sigmoid(logit + shift) from sigmoid(logit)
+            const double e = exp(shift);
+            p = p * e / (1.0 - p + p * e);
+        }
+        const bool fire = u0 < p;
         spikes[(b % 6) * (int64_t)n + i] = fire ? 1 : 0;
         const int32_t src = sources[i];
         if (!fire || src < 0) continue;

@@ -97,6 +97,7 @@ struct MindHandle {
     float sur_scale = 1.0f;
     int32_t *sur_cells = nullptr, *sur_sources = nullptr, *sur_spikes = nullptr;
     float *sur_x = nullptr, *sur_prob = nullptr;
+    float *sur_offset = nullptr;         // per cell (layout order): logit calibration offset
     // synaptic drive recording (mind_set_drive_recording)
     int32_t drive_bin_steps = 0;
     float *drive_dev = nullptr;
@@ -1145,7 +1146,7 @@ int advance(MindHandle *h, int64_t steps, bool record_spikes) {
                 if (mind_mlp_forward_device(h->sur_mlp, h->sur_x, h->n_sur, h->sur_prob, h->stream, h->P.error))
                     return fail(h, MIND_ECUDA, "surrogate inference failed");
                 surrogate_spike_kernel<<<launch_grid(h->n_sur), kThreads, 0, h->stream>>>(
-                    P, h->sur_cells, h->sur_sources, h->n_sur, h->sur_prob, h->sur_spikes, b,
+                    P, h->sur_cells, h->sur_sources, h->n_sur, h->sur_prob, h->sur_offset, h->sur_spikes, b,
                     (double)h->bin_steps * P.dt, M.source_region, M.bins, M.n, M.bin_ring, n0);
                 st.launches += 3;
             }
@@ -1542,6 +1543,7 @@ int mind_attach_surrogate(MindHandle *h, MindMlp *mlp, const uint8_t *surrogate_
         h->sur_spikes = h->alloc<int32_t>((size_t)6 * cells.size());
         h->sur_x = h->alloc<float>((size_t)645 * cells.size());
         h->sur_prob = h->alloc<float>(cells.size());
+        h->sur_offset = h->upload(std::vector<float>(h->ncells, 0.0f));
     } catch (const std::bad_alloc &) {
         return fail(h, MIND_ECUDA, "device allocation failed");
     }
@@ -1552,6 +1554,18 @@ int mind_attach_surrogate(MindHandle *h, MindMlp *mlp, const uint8_t *surrogate_
     h->sur_cap = h->n_sur;
     h->sur_attached = mode;
     h->initialized = false;
+    return MIND_OK;
+}
+
+int mind_set_surrogate_offsets(MindHandle *h, const float *logit_offset, int32_t n_cells) {
+    if (!h || !logit_offset) return MIND_EARG;
+    if (h->sur_cap == 0) return fail(h, MIND_EARG, "no surrogate is attached");
+    if (n_cells != h->ncells) return fail(h, MIND_EARG, "one offset per cell of the layout");
+    for (int32_t c = 0; c < n_cells; ++c)
+        if (!std::isfinite(logit_offset[c])) return fail(h, MIND_EARG, "offsets must be finite");
+    CUDA_TRY(h, cudaMemcpyAsync(h->sur_offset, logit_offset, (size_t)n_cells * sizeof(float), cudaMemcpyHostToDevice,
+                                h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     return MIND_OK;
 }
 

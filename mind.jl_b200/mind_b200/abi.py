@@ -195,6 +195,7 @@ def load_library():
     lib.mind_read_voltage.argtypes = [handle, c_int32, POINTER(c_double)]
     lib.mind_read_value.argtypes = [handle, POINTER(MindRecord), POINTER(c_double)]
     lib.mind_set_surrogate_cells.argtypes = [handle, POINTER(ctypes.c_uint8)]
+    lib.mind_set_surrogate_offsets.argtypes = [handle, POINTER(ctypes.c_float), c_int32]
     lib.mind_autotune.argtypes = [handle, c_int32]
     lib.mind_bin_threads.argtypes = [handle, POINTER(c_int32), c_int32, POINTER(c_int32)]
     lib.mind_set_bin_threads.argtypes = [handle, POINTER(c_int32), c_int32]
@@ -236,6 +237,7 @@ def load_library():
                  "mind_inject_event", "mind_last_run_ms", "mind_destroy", "mind_run_stats",
                  "mind_set_profiling", "mind_run_noalloc", "mind_inject_spikes", "mind_window_steps",
                  "mind_autotune", "mind_bin_threads", "mind_set_bin_threads", "mind_set_surrogate_cells",
+                 "mind_set_surrogate_offsets",
                  "mind_attach_macro", "mind_get_macro_trace", "mind_set_drive_recording", "mind_get_drive",
                  "mind_attach_surrogate",
                  "mind_mlp_create", "mind_mlp_destroy", "mind_mlp_last_ms",
@@ -252,7 +254,7 @@ EXPORTED_SYMBOLS = (
     "mind_get_trace", "mind_get_spikes", "mind_read_voltage", "mind_read_value", "mind_inject_event",
     "mind_last_error", "mind_last_run_ms", "mind_destroy", "mind_run_stats", "mind_set_profiling",
     "mind_run_noalloc", "mind_inject_spikes", "mind_window_steps", "mind_autotune", "mind_bin_threads",
-    "mind_set_surrogate_cells",
+    "mind_set_surrogate_cells", "mind_set_surrogate_offsets",
     "mind_set_bin_threads", "mind_attach_macro", "mind_get_macro_trace",
     "mind_set_drive_recording", "mind_get_drive", "mind_attach_surrogate", "mind_mlp_create", "mind_mlp_destroy", "mind_mlp_last_error", "mind_mlp_last_ms", "mind_mlp_param_count", "mind_mlp_set_params",
     "mind_mlp_get_params", "mind_mlp_predict", "mind_mlp_gradients", "mind_mlp_set_data", "mind_mlp_train",

@@ -112,6 +112,15 @@ class DeviceState:
         abi.check(self.lib, self.handle, self.lib.mind_set_surrogate_cells(
             self.handle, mask.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))))
 
+    def set_surrogate_offsets(self, offsets) -> None:
+        """mind_set_surrogate_offsets: per-cell logit offsets of the surrogate's spike
+        probability (calibration)."""
+        v = np.ascontiguousarray(np.asarray(offsets, dtype=np.float32))
+        if v.size != self.layout.n_cells:
+            raise ValueError("one offset per cell")
+        abi.check(self.lib, self.handle, self.lib.mind_set_surrogate_offsets(
+            self.handle, v.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), v.size))
+
     def set_drive_recording(self, bin_ms: float) -> None:
         """mind_set_drive_recording: each run also returns the cells' binned synaptic drive."""
         abi.check(self.lib, self.handle, self.lib.mind_set_drive_recording(self.handle, float(bin_ms)))

@@ -214,6 +214,56 @@ def judge_populations(sur_spikes, sur_cells, det_spikes, det_cells, seconds: flo
     return judged & (np.abs(r_s - r_d) > bound * r_d + z * se)
 
 
+def population_rates(layout, macro, result, t_ms: float, cells=None) -> np.ndarray:
+    """Per region: spikes per cell per second over a run of t_ms, counting only the cells
+    flagged in `cells` (every cell when None); NaN for a region without such cells."""
+    region = cell_regions(layout, macro)
+    chosen = np.ones(layout.n_cells, dtype=bool) if cells is None else np.asarray(cells, dtype=bool)
+    offsets = np.asarray(layout.cell_offsets)
+    nodes = np.asarray(layout.source_nodes)
+    sid_cell = {int(layout.source_ids[s]): int(np.searchsorted(offsets, node - 1, side="right") - 1)
+                for s, node in enumerate(nodes) if node > 0}
+    counts = np.zeros(macro.n_regions)
+    for sid in result.spike_sources:
+        c = sid_cell.get(int(sid))
+        if c is not None and chosen[c] and region[c] >= 0:
+            counts[region[c]] += 1.0
+    members = np.array([np.count_nonzero(chosen & (region == p)) for p in range(macro.n_regions)], dtype=float)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        return np.where(members > 0, counts / members / (t_ms * 1e-3), np.nan)
+
+
+def calibrate(state, layout, macro, surrogate_cells, target_hz, t_ms: float = 100.0, rounds: int = 4,
+              max_shift: float = 4.0):
+    """Per-population calibration of the surrogate in its closed loop (no counterpart in the
+    reference).  A coupled run feeds the surrogate's spikes back through the regions, so a
+    small bias of the network grows into a large rate error; the remedy here is one logit
+    offset per population, fitted on the coupled run itself: `rounds` runs of t_ms from
+    mind_initialize, after each of which every population's offset moves by
+    log(target / measured) of its surrogate cells' rate (the shift that scales a small
+    spike probability by that ratio), clipped to +-max_shift in total.  `state` has the
+    macro model and the surrogate attached; `target_hz` holds each population's rate in the
+    detailed run the network was trained on.  Returns (per-cell offsets, per-round rates)."""
+    mask = np.asarray(surrogate_cells, dtype=bool)
+    region = cell_regions(layout, macro)
+    target = np.asarray(target_hz, dtype=float)
+    shift = np.zeros(macro.n_regions)
+    history = []
+    steps = int(round(t_ms / layout.dt))
+    for _ in range(rounds):
+        per_cell = np.where(region >= 0, shift[np.maximum(region, 0)], 0.0)
+        state.set_surrogate_offsets(per_cell)
+        state.initialize()
+        measured = population_rates(layout, macro, state.run_steps(steps, []), t_ms, mask)
+        history.append(measured)
+        live = np.isfinite(measured) & (target > 0)
+        ratio = np.where(measured > 0, target / np.where(measured > 0, measured, 1.0), np.e)
+        shift = np.where(live, np.clip(shift + np.log(ratio), -max_shift, max_shift), shift)
+    per_cell = np.where(region >= 0, shift[np.maximum(region, 0)], 0.0)
+    state.set_surrogate_offsets(per_cell)
+    return per_cell, history
+
+
 def judged_run(state, layout, macro, surrogate_cells, t_ms: float, window_ms: float = 20.0,
                bound: float = 0.05, z: float = 3.0):
     """Run t_ms in windows with the cable solver as judge: the cells of each population that

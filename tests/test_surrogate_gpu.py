@@ -140,3 +140,33 @@ def test_judge_reverts_a_failing_surrogate_to_the_cable_solver():
     assert np.all(region >= 0)
     state.close()
     net.close()
+
+
+def test_surrogate_offsets_shift_the_spike_probability():
+    """mind_set_surrogate_offsets: an offset of -20 on the logit silences the surrogate cells,
+    +20 makes them fire in (almost) every bin; offsets of 0 give back the uncalibrated run,
+    spike for spike."""
+    model, macro = netcases.coupled_regions(n_regions=4, cells_per_region=50, synapses=32, seed=21)
+    layout = model.layout
+    net = surrogate.Mlp(seed=2)
+    mask = np.ones(layout.n_cells, dtype=bool)
+    mask[::10] = False
+    steps = int(round(40.0 / layout.dt))
+    state = mb.runtime.DeviceState(layout)
+    state.attach_macro(macro)
+    state.attach_surrogate(net, mask, 1.0)
+    counts, rasters = {}, {}
+    for shift in (0.0, -20.0, 20.0, 0.0):
+        state.set_surrogate_offsets(np.full(layout.n_cells, shift))
+        state.initialize()
+        res = state.run_steps(steps, [])
+        rates = surrogate.population_rates(layout, macro, res, 40.0, mask)
+        counts.setdefault(shift, []).append(float(np.nansum(rates)))
+        rasters.setdefault(shift, []).append(res.spike_times.copy())
+    assert counts[-20.0][0] == 0.0
+    assert np.nanmin(counts[20.0][0]) > 0.9 * 4 * 1000.0   # four populations near 1 spike per 1 ms bin
+    np.testing.assert_array_equal(rasters[0.0][0], rasters[0.0][1])
+    with pytest.raises(mb.abi.MindError):
+        state.set_surrogate_offsets(np.full(layout.n_cells, np.inf))
+    state.close()
+    net.close()
