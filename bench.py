@@ -53,7 +53,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=40)
     p.add_argument("--impl", default="mine", choices=["mine", "reference"])
     p.add_argument("--cells", type=int, default=None, help="cells (default: the configuration's count)")
-    p.add_argument("--config", type=int, default=2, choices=[2, 3, 4],
+    p.add_argument("--config", type=int, default=2, choices=[2, 3, 4, 5],
                    help="2: 10,000 uneven binary-tree cells (the headline); 3: 1,000 pyramidal-like cells; "
                         "4: 2,000 pyramidal-like cells coupled to 20 Jansen-Rit regions")
     p.add_argument("--no-autotune", action="store_true",
@@ -79,7 +79,9 @@ def build_network(cells, seed: int, config: int = 2, rank: int = 0, world: int =
     import mind_b200 as mb
     from mind_b200 import networks
 
-    if config == 4:
+    if config == 5:
+        model = networks.config5(n_cells=cells or 100_000)
+    elif config == 4:
         model = networks.config4(n_cells=cells or 2000)
     elif config == 3:
         model = networks.config3(n_cells=cells or 1000)
@@ -385,6 +387,72 @@ def measure_surrogate(args, model, layout, train_ms: float = 300.0, eval_ms: flo
     }
 
 
+def measure_config5(args, model, layout, train_ms: float = 500.0, eval_ms: float = 100.0, keep: float = 0.02,
+                    calibration_ms: float = 50.0, calibration_rounds: int = 3):
+    """Config 5 once: a surrogate trained on config 4 (about 1e6 windows of a detailed run of
+    train_ms), calibrated per population on the coupled 100,000-cell run against each
+    population's detailed sample, then eval_ms from initialize twice -- every cell detailed
+    (mixed mode), and all but `keep` of the cells replaced -- with time per step and the
+    regions' population rates."""
+    import mind_b200 as mb
+    from mind_b200 import networks, surrogate
+
+    macro = model.macro
+    m4 = networks.config4()
+    mb.build(m4, seed=1)
+    t0 = time.perf_counter()
+    net, scale, train_run = surrogate.train_from_run(m4, train_ms, steps=500, batch=4096)
+    train_s = time.perf_counter() - t0
+    windows = int((train_run.drive.shape[0] - surrogate.WINDOW_BINS) * m4.layout.n_cells)
+    m4.state.close()
+    del train_run, m4
+    steps = int(round(eval_ms / layout.dt))
+    plain_state = mb.runtime.DeviceState(layout, "mixed")
+    plain_state.attach_macro(macro)
+    plain_state.initialize()
+    plain, plain_ms = device_timed(lambda: plain_state.run_steps(steps, []))
+    plain_state.close()
+    rng = np.random.default_rng(0)
+    mask = rng.uniform(size=layout.n_cells) >= keep
+    state = mb.runtime.DeviceState(layout, "mixed")
+    state.attach_macro(macro)
+    state.attach_surrogate(net, mask, scale)
+    t_c = time.perf_counter()
+    offsets, _ = surrogate.calibrate(state, layout, macro, mask, None, calibration_ms, calibration_rounds)
+    calibration_s = time.perf_counter() - t_c
+    state.initialize()
+    sur, sur_ms = device_timed(lambda: state.run_steps(steps, []))
+    state.close()
+    net.close()
+    r_plain = surrogate.region_rates(layout, plain, macro, eval_ms)
+    r_sur = surrogate.region_rates(layout, sur, macro, eval_ms)
+    mean_plain = r_plain.mean(axis=0)
+    rel = np.abs(r_sur.mean(axis=0) - mean_plain) / np.maximum(mean_plain, 1e-9)
+    members = np.bincount(surrogate.cell_regions(layout, macro)[surrogate.cell_regions(layout, macro) >= 0],
+                          minlength=macro.n_regions)
+    noise = np.sqrt(2.0 / np.maximum(mean_plain * (eval_ms * 1e-3) * members, 1.0))
+    units = layout.segment_count * steps
+    return {
+        "metric": "compartment-steps/s (config 5, equivalent: every cell's compartments counted)",
+        "config": {"workload": "config5", "cells": layout.n_cells, "compartments": layout.segment_count,
+                   "populations": macro.n_regions, "surrogate_cells": int(mask.sum()), "eval_ms": eval_ms},
+        "plain_mixed": {"value": units / (plain_ms / 1000.0), "ms_per_step": plain_ms / steps},
+        "surrogate": {"value": units / (sur_ms / 1000.0), "ms_per_step": sur_ms / steps},
+        "speedup": plain_ms / sur_ms,
+        "population_rate_error": {"mean_rel": float(rel.mean()), "max_rel": float(rel.max()),
+                                  "pooled_rel": float(abs(r_sur.mean() - r_plain.mean()) / max(r_plain.mean(), 1e-9)),
+                                  "counting_noise_per_region_mean": float(noise.mean()),
+                                  "plain_rate_hz_mean": float(mean_plain.mean()),
+                                  "surrogate_rate_hz_mean": float(r_sur.mean())},
+        "calibration": {"rounds": calibration_rounds, "ms_per_round": calibration_ms, "wall_s": calibration_s,
+                        "target": "each population's detailed sample, pooled over the rounds"},
+        "training": {"source": "config 4 (2,000 cells), detailed FP64 run", "train_ms": train_ms,
+                     "windows": windows, "steps": 500, "batch": 4096, "wall_s": train_s},
+        "note": "plain: every cell in the mixed mode; surrogate: the detailed sample in the mixed mode, the rest "
+                "replaced; regions FP64 in both; rates from the rasters",
+    }
+
+
 def run_reference(args, rank: int):
     """The reference arm: the CPU FP64 restatement of MIND.jl's step loop (oracle/) on every host
     core, on the GPU arm's network and schedule -- the same untimed settle and warm-up, then
@@ -446,9 +514,12 @@ def main():
     model, layout = build_network(args.cells, seed=replicas.replica_seed(1, rank), config=args.config,
                                   rank=rank, world=world)
     sharded = world > 1 and args.config == 2
+    if args.config == 5 and not args.surrogate:
+        raise SystemExit("--config 5 runs with --surrogate")
     if args.surrogate:
         if rank == 0:
-            print(json.dumps(measure_surrogate(args, model, layout)), flush=True)
+            measure = measure_config5 if args.config == 5 else measure_surrogate
+            print(json.dumps(measure(args, model, layout)), flush=True)
         if dist is not None:
             dist.destroy_process_group()
         return

@@ -357,7 +357,18 @@ def config4(n_cells: int = 2000, populations: int = 20, synapses_per_cell: int =
     return model
 
 
-CONFIGS = {1: config1, 2: config2, 3: config3, 4: config4}
+def config5(n_cells: int = 100_000, populations: int = 200, **kwargs) -> M.MicroModel:
+    """Surrogate-coupled micro-macro: config 4 scaled to 100,000 cells in 200 populations of
+    500, each coupled to its own Jansen-Rit region (200 regions, the same random region graph
+    rule).  Each cell keeps config 4's recurrent in-degree (3% of 2,000 cells: 60 NetCons from
+    random cells), so that a cell's input statistics, and with them the surrogate trained on
+    config 4, carry over.  The surrogate that stands in for most of its cells is trained on
+    config 4."""
+    kwargs.setdefault("connectivity", 0.03 * 2000 / n_cells)
+    return config4(n_cells=n_cells, populations=populations, **kwargs)
+
+
+CONFIGS = {1: config1, 2: config2, 3: config3, 4: config4, 5: config5}
 
 
 def compartment_count(layout) -> int:

@@ -243,21 +243,30 @@ def calibrate(state, layout, macro, surrogate_cells, target_hz, t_ms: float = 10
     log(target / measured) of its surrogate cells' rate (the shift that scales a small
     spike probability by that ratio), clipped to +-max_shift in total.  `state` has the
     macro model and the surrogate attached; `target_hz` holds each population's rate in the
-    detailed run the network was trained on.  Returns (per-cell offsets, per-round rates)."""
+    detailed run the network was trained on, or is None: then each population's target is
+    the rate of its detailed sample (the cells not in `surrogate_cells`) pooled over the
+    rounds so far.  Returns (per-cell offsets, per-round rates)."""
     mask = np.asarray(surrogate_cells, dtype=bool)
     region = cell_regions(layout, macro)
-    target = np.asarray(target_hz, dtype=float)
     shift = np.zeros(macro.n_regions)
     history = []
+    sample = []
     steps = int(round(t_ms / layout.dt))
     for _ in range(rounds):
         per_cell = np.where(region >= 0, shift[np.maximum(region, 0)], 0.0)
         state.set_surrogate_offsets(per_cell)
         state.initialize()
-        measured = population_rates(layout, macro, state.run_steps(steps, []), t_ms, mask)
+        res = state.run_steps(steps, [])
+        measured = population_rates(layout, macro, res, t_ms, mask)
         history.append(measured)
-        live = np.isfinite(measured) & (target > 0)
-        ratio = np.where(measured > 0, target / np.where(measured > 0, measured, 1.0), np.e)
+        if target_hz is None:
+            sample.append(population_rates(layout, macro, res, t_ms, ~mask))
+            target = np.nanmean(np.array(sample), axis=0)
+        else:
+            target = np.asarray(target_hz, dtype=float)
+        live = np.isfinite(measured) & np.isfinite(target) & (target > 0)
+        safe_target = np.where(live, target, 1.0)
+        ratio = np.where(measured > 0, safe_target / np.where(measured > 0, measured, 1.0), np.e)
         shift = np.where(live, np.clip(shift + np.log(ratio), -max_shift, max_shift), shift)
     per_cell = np.where(region >= 0, shift[np.maximum(region, 0)], 0.0)
     state.set_surrogate_offsets(per_cell)
