@@ -601,12 +601,14 @@ __device__ __forceinline__ void hines_exact(double *sd, double *sr, const double
  * kThreadNodeCycles per node, a warp kWarpFixedCycles plus kWarpSegmentCycles per node of a
  * lane's segment.  A level with many long chains (the leaves of a pyramidal cell) keeps
  * them on threads, which run side by side; a level whose one chain is far longer than the
- * rest (a trunk) gives it a warp. */
+ * rest (a trunk) gives it a warp.  The constants are measured ones, rounded up: at full
+ * occupancy the other cells' warps fill a chain's stalls, and on the benchmark networks
+ * (config 2, config 3) the warp solve then gains within 1% either way. */
 #ifndef MIND_WARP_FIXED_CYCLES
-#define MIND_WARP_FIXED_CYCLES 2600
+#define MIND_WARP_FIXED_CYCLES 4000
 #endif
 #ifndef MIND_WARP_SEGMENT_CYCLES
-#define MIND_WARP_SEGMENT_CYCLES 650
+#define MIND_WARP_SEGMENT_CYCLES 900
 #endif
 constexpr int32_t kThreadNodeCycles = 100;
 constexpr int32_t kWarpFixedCycles = MIND_WARP_FIXED_CYCLES;
@@ -902,7 +904,8 @@ __device__ __forceinline__ void hines_mixed(double *sd, double *sr, const double
 template <bool MIXED, int NT, bool GLOBAL_IMAGE = false, bool GEN = false,
           int MINB = NT == kCellThreads ? 5 : NT == kCellThreads / 2 ? 10 : 16>
 __global__ void __launch_bounds__(NT, MINB) window_kernel(const Params P, const int32_t *cells,
-                                                                               int64_t n0, int32_t W) {
+                                                                               int64_t n0, int32_t W,
+                                                                               int32_t part_staged) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ StagedGroup sg[kMaxGroups];
     const int32_t c = cells[blockIdx.x];
@@ -959,7 +962,11 @@ __global__ void __launch_bounds__(NT, MINB) window_kernel(const Params P, const 
     int32_t *ckids = ip; ip += nkids;
     int32_t *lvc = ip; ip += nlev + 1;
     int32_t *sorder = ip; ip += P.inbox_cap;
-    int32_t *spart = ip; ip += P.ngroups * (O + 1);
+    // the threads' row ranges: staged when the launch's shared memory has room for them
+    // without costing a resident CTA, else read through the read-only cache
+    int32_t *spart = ip;
+    if (part_staged) ip += P.ngroups * (O + 1);
+    const int32_t *part = part_staged ? spart : P.part + (int64_t)c * P.ngroups * (O + 1);
     int16_t *chain_of = reinterpret_cast<int16_t *>(ip);
     {
         // The launch sized the image for this cell's bin; refuse rather than overrun.
@@ -1025,7 +1032,8 @@ __global__ void __launch_bounds__(NT, MINB) window_kernel(const Params P, const 
     if (tid == 0) ckoff[nch] = nkids;
     for (int32_t k = tid; k < nkids; k += T) ckids[k] = P.chain_kids[kb + k];
     for (int32_t k = tid; k <= nlev; k += T) lvc[k] = P.level_chain[lv0 + k];
-    for (int32_t k = tid; k < P.ngroups * (O + 1); k += T) spart[k] = P.part[(int64_t)c * P.ngroups * (O + 1) + k];
+    if (part_staged)
+        for (int32_t k = tid; k < P.ngroups * (O + 1); k += T) spart[k] = P.part[(int64_t)c * P.ngroups * (O + 1) + k];
     __syncthreads();
     for (int32_t k = tid; k < nch; k += T)
         for (int32_t i = ctop[k]; i < ctop[k] + clen[k]; ++i) chain_of[i] = (int16_t)k;
@@ -1158,7 +1166,7 @@ __global__ void __launch_bounds__(NT, MINB) window_kernel(const Params P, const 
             const DevGroup &GG = P.groups[g];
             const StagedGroup G = sg[g];
             for (int32_t slot = tid; slot < O; slot += T) {
-                const int32_t lo = spart[g * (O + 1) + slot], hi = spart[g * (O + 1) + slot + 1];
+                const int32_t lo = part[g * (O + 1) + slot], hi = part[g * (O + 1) + slot + 1];
                 if (lo >= hi) continue;
                 if (G.kind == MIND_MECH_PAS) {
                     if (MIXED) continue;  // folded into the node constants of the assembly below
