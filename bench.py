@@ -297,10 +297,10 @@ def measure_sharded(args, layout, rank: int, world: int, precision: str, local_r
 
 
 def measure_surrogate(args, model, layout, train_ms: float = 300.0, eval_ms: float = 1000.0, keep: float = 0.02,
-                      calibration_ms: float = 100.0, calibration_rounds: int = 4):
+                      calibration_rounds: int = 4):
     """Config 4 with the surrogate: train on a detailed FP64 run of train_ms, calibrate one
-    logit offset per population on the coupled run (calibration_rounds runs of
-    calibration_ms, towards the training run's population rates), then run eval_ms from
+    logit offset per population on the coupled run (calibration_rounds runs of train_ms from
+    initialize, towards the training run's population rates over the same window), then run eval_ms from
     initialize twice — plain FP64, and with all but `keep` of the cells replaced — and
     compare time per step and the regions' population rates over the whole eval_ms (which
     extends past the training period)."""
@@ -323,8 +323,7 @@ def measure_surrogate(args, model, layout, train_ms: float = 300.0, eval_ms: flo
     state.attach_macro(macro)
     state.attach_surrogate(net, mask, scale)
     t_c = time.perf_counter()
-    offsets, cal_rates = surrogate.calibrate(state, layout, macro, mask, target_hz, calibration_ms,
-                                             calibration_rounds)
+    offsets, cal_rates = surrogate.calibrate(state, layout, macro, mask, target_hz, train_ms, calibration_rounds)
     calibration_s = time.perf_counter() - t_c
     state.initialize()
     sur, sur_ms = device_timed(lambda: state.run_steps(steps, []))
@@ -374,7 +373,7 @@ def measure_surrogate(args, model, layout, train_ms: float = 300.0, eval_ms: flo
                    "population_rate_error": {"mean_rel": float(rel_j.mean()), "max_rel": float(rel_j.max())},
                    "rule": "every 20 ms, over the run so far: |rate(surrogate) - rate(sample)| > 0.05 rate(sample)"
                            " + 3 Poisson standard errors reverts the population"},
-        "calibration": {"rounds": calibration_rounds, "ms_per_round": calibration_ms, "wall_s": calibration_s,
+        "calibration": {"rounds": calibration_rounds, "ms_per_round": train_ms, "wall_s": calibration_s,
                         "target_hz": target_hz.tolist(),
                         "surrogate_hz_per_round": [np.nan_to_num(r).tolist() for r in cal_rates],
                         "offsets_per_region": [float(offsets[surrogate.cell_regions(layout, macro) == p][0])

@@ -243,7 +243,8 @@ def calibrate(state, layout, macro, surrogate_cells, target_hz, t_ms: float = 10
     log(target / measured) of its surrogate cells' rate (the shift that scales a small
     spike probability by that ratio), clipped to +-max_shift in total.  `state` has the
     macro model and the surrogate attached; `target_hz` holds each population's rate in the
-    detailed run the network was trained on, or is None: then each population's target is
+    detailed run the network was trained on over the same t_ms from initialize (a run's
+    early rates differ from its later ones), or is None: then each population's target is
     the rate of its detailed sample (the cells not in `surrogate_cells`) pooled over the
     rounds so far.  Returns (per-cell offsets, per-round rates)."""
     mask = np.asarray(surrogate_cells, dtype=bool)
