@@ -582,215 +582,11 @@ __device__ __forceinline__ void hines_exact(double *sd, double *sr, const double
     }
 }
 
-/* ---- long unbranched chains in the mixed mode: one warp per chain ----
- *
- * A chain's elimination is a recurrence from its bottom node up, D_i = d_i - a_{i+1}^2 / D_{i+1}
- * and R_i = r_i + (a_{i+1} / D_{i+1}) R_{i+1}, and its back-substitution one from the top down,
- * x_i = (a_i / D_i) x_{i-1} + R_i / D_i.  On a chain of L nodes one thread takes L dependent
- * steps.  A warp splits the chain into 32 consecutive segments: each lane composes its
- * segment's steps (the D step is the Mobius map D -> (d D - a^2) / D, a 2x2 matrix; the R and x
- * steps are affine maps), a warp scan composes the segments, and each lane then runs the
- * ordinary recurrence over its own segment from the value the scan gives at its boundary.
- * The depth falls from L to about 2 L / 32 + 5 combining steps, at a fixed cost of three
- * warp scans.  Only the rounding of the boundary values changes, so this is used in the mixed
- * mode only; the FP64 mode keeps the oracle's sequential order.
- *
- * Which chains of a level go to warps (warp_chains): the planner orders a level's chains
- * longest first, and a level hands its k longest chains to the last k warps of the CTA
- * when that shortens the level, by a latency model in cycles: a thread takes
- * kThreadNodeCycles per node, a warp kWarpFixedCycles plus kWarpSegmentCycles per node of a
- * lane's segment.  A level with many long chains (the leaves of a pyramidal cell) keeps
- * them on threads, which run side by side; a level whose one chain is far longer than the
- * rest (a trunk) gives it a warp.  The constants are measured ones, rounded up: at full
- * occupancy the other cells' warps fill a chain's stalls, and on the benchmark networks
- * (config 2, config 3) the warp solve then gains within 1% either way. */
-#ifndef MIND_WARP_FIXED_CYCLES
-#define MIND_WARP_FIXED_CYCLES 4000
-#endif
-#ifndef MIND_WARP_SEGMENT_CYCLES
-#define MIND_WARP_SEGMENT_CYCLES 900
-#endif
-constexpr int32_t kThreadNodeCycles = 100;
-constexpr int32_t kWarpFixedCycles = MIND_WARP_FIXED_CYCLES;
-constexpr int32_t kWarpSegmentCycles = MIND_WARP_SEGMENT_CYCLES;
-
-/* Number of the level's chains [lo, hi) (longest first) that warps solve; the same on every
- * thread. */
-template <int NT>
-__device__ __forceinline__ int32_t warp_chains(const int32_t *clen, int32_t lo, int32_t hi) {
-    constexpr int32_t NW = NT / 32;
-    const int32_t L0 = clen[lo];
-    const int32_t wcost = kWarpFixedCycles + kWarpSegmentCycles * ((L0 + 31) / 32);
-    int32_t best = 0, best_cost = kThreadNodeCycles * L0;
-    for (int32_t k = 1; k <= NW && lo + k <= hi; ++k) {
-        const int32_t rest = lo + k < hi ? kThreadNodeCycles * clen[lo + k] : 0;
-        // with every warp busy, the thread-mode chains run on their lanes first
-        const int32_t cost = (k == NW && rest > 0) ? rest + wcost : max(rest, wcost);
-        if (cost < best_cost) {
-            best_cost = cost;
-            best = k;
-        }
-    }
-    return best;
-}
-
-struct Mobius {   // x -> (a x + b) / (c x + d)
-    double a, b, c, d;
-};
-struct Affine {   // x -> m x + c
-    double m, c;
-};
-
-/* l after r, rescaled by a power of two (exact) so long products neither overflow nor underflow. */
-__device__ __forceinline__ Mobius mobius_after(const Mobius &l, const Mobius &r) {
-    Mobius p{l.a * r.a + l.b * r.c, l.a * r.b + l.b * r.d, l.c * r.a + l.d * r.c, l.c * r.b + l.d * r.d};
-    const double big = fmax(fmax(fabs(p.a), fabs(p.b)), fmax(fabs(p.c), fabs(p.d)));
-    if (big > 0.0 && isfinite(big)) {
-        const int e = ilogb(big);
-        p.a = ldexp(p.a, -e);
-        p.b = ldexp(p.b, -e);
-        p.c = ldexp(p.c, -e);
-        p.d = ldexp(p.d, -e);
-    }
-    return p;
-}
-__device__ __forceinline__ Affine affine_after(const Affine &l, const Affine &r) { return {l.m * r.m, l.m * r.c + l.c}; }
-
-/* Exclusive warp scans (lane k gets the composition of lanes 0 .. k-1; lane 0 the identity). */
-__device__ __forceinline__ Mobius warp_exclusive(Mobius v, int lane) {
-    for (int off = 1; off < 32; off <<= 1) {
-        const Mobius o{__shfl_up_sync(0xffffffffu, v.a, off), __shfl_up_sync(0xffffffffu, v.b, off),
-                       __shfl_up_sync(0xffffffffu, v.c, off), __shfl_up_sync(0xffffffffu, v.d, off)};
-        if (lane >= off) v = mobius_after(v, o);
-    }
-    Mobius e{__shfl_up_sync(0xffffffffu, v.a, 1), __shfl_up_sync(0xffffffffu, v.b, 1),
-             __shfl_up_sync(0xffffffffu, v.c, 1), __shfl_up_sync(0xffffffffu, v.d, 1)};
-    if (lane == 0) e = Mobius{1.0, 0.0, 0.0, 1.0};
-    return e;
-}
-__device__ __forceinline__ Affine warp_exclusive(Affine v, int lane) {
-    for (int off = 1; off < 32; off <<= 1) {
-        const Affine o{__shfl_up_sync(0xffffffffu, v.m, off), __shfl_up_sync(0xffffffffu, v.c, off)};
-        if (lane >= off) v = affine_after(v, o);
-    }
-    Affine e{__shfl_up_sync(0xffffffffu, v.m, 1), __shfl_up_sync(0xffffffffu, v.c, 1)};
-    if (lane == 0) e = Affine{1.0, 0.0};
-    return e;
-}
-
-/* Elimination of one long chain by a warp, with the mixed mode's arithmetic (reciprocal
- * pivots): leaves f = a/D in sd and R/D in sr for its nodes, and the chain's contribution to
- * its parent node in sxd, sxr. */
-__device__ __forceinline__ void eliminate_chain_warp(int32_t ch, double *sd, double *sr, const double *sa,
-                                                     double *sxd, double *sxr, const int32_t *ctop,
-                                                     const int32_t *clen, const int32_t *cpar,
-                                                     const int32_t *ckoff, const int32_t *ckids, bool &singular) {
-    const int32_t lane = threadIdx.x & 31;
-    const int32_t top = ctop[ch], L = clen[ch], bottom = top + L - 1;
-    // the bottom pivot and rhs with the child chains' contributions, in child order, on every lane
-    double Db = sd[bottom], Rb = sr[bottom];
-    for (int32_t q = ckoff[ch]; q < ckoff[ch + 1]; ++q) {
-        Db = Db - sxd[ckids[q]];
-        Rb = Rb + sxr[ckids[q]];
-    }
-    // this lane's positions p (p = 0 is the bottom node, node = bottom - p)
-    const int32_t S = (L + 31) / 32;
-    const int32_t p0 = min(L, lane * S), p1 = min(L, p0 + S), first = max(p0, 1);
-    // 1. pivots D
-    Mobius T{1.0, 0.0, 0.0, 1.0};
-    for (int32_t p = first; p < p1; ++p) {
-        const int32_t i = bottom - p;
-        const double an = sa[i + 1];
-        T = mobius_after(Mobius{sd[i], -(an * an), 1.0, 0.0}, T);
-    }
-    const Mobius E = warp_exclusive(T, lane);
-    double Dprev = (E.a * Db + E.b) / (E.c * Db + E.d);   // D at position p0 - 1 (p0 = 0: the bottom's own)
-    if (p0 == 0 && L > 0) {
-        Dprev = Db;
-        singular |= (Db == 0.0) | !isfinite(Db);
-        sd[bottom] = Db;
-    }
-    for (int32_t p = first; p < p1; ++p) {
-        const int32_t i = bottom - p;
-        const double an = sa[i + 1];
-        const double Di = sd[i] - (an * an) * approx_reciprocal(Dprev);
-        singular |= (Di == 0.0) | !isfinite(Di);
-        sd[i] = Di;
-        Dprev = Di;
-    }
-    __syncwarp();
-    // 2. right-hand sides R (the step into position p multiplies by f of position p - 1)
-    Affine A{1.0, 0.0};
-    for (int32_t p = first; p < p1; ++p) {
-        const int32_t i = bottom - p;
-        const double fn = sa[i + 1] * approx_reciprocal(sd[i + 1]);
-        A = affine_after(Affine{fn, sr[i]}, A);
-    }
-    const Affine F = warp_exclusive(A, lane);
-    double Rprev = F.m * Rb + F.c;
-    if (p0 == 0 && L > 0) {
-        Rprev = Rb;
-        sr[bottom] = Rb;
-    }
-    for (int32_t p = first; p < p1; ++p) {
-        const int32_t i = bottom - p;
-        const double fn = sa[i + 1] * approx_reciprocal(sd[i + 1]);
-        const double Ri = sr[i] + fn * Rprev;
-        sr[i] = Ri;
-        Rprev = Ri;
-    }
-    __syncwarp();
-    // 3. f = a/D and R/D in place; the top node's contribution to the parent
-    for (int32_t p = p0; p < p1; ++p) {
-        const int32_t i = bottom - p;
-        const double y = approx_reciprocal(sd[i]);
-        const double ai = sa[i];
-        const double fi = ai * y;
-        const double Ri = sr[i];
-        if (p == L - 1) {
-            const bool rooted = cpar[ch] < 0;
-            sxd[ch] = rooted ? 0.0 : (ai * ai) * y;
-            sxr[ch] = rooted ? 0.0 : fi * Ri;
-        }
-        sd[i] = fi;
-        sr[i] = Ri * y;
-    }
-    __syncwarp();
-}
-
-/* Back-substitution of one long chain by a warp (mixed mode): x = f x_prev + R/D from the
- * chain's top, the top continuing its parent node's solution. */
-__device__ __forceinline__ void substitute_chain_warp(int32_t ch, double *sd, double *sr, double *sv,
-                                                      const int32_t *ctop, const int32_t *clen, const int32_t *cpar,
-                                                      double vscale) {
-    const int32_t lane = threadIdx.x & 31;
-    const int32_t top = ctop[ch], L = clen[ch], par = cpar[ch];
-    const double xp = par >= 0 ? sr[par] : 0.0;
-    const int32_t S = (L + 31) / 32;
-    const int32_t u0 = min(L, lane * S), u1 = min(L, u0 + S);
-    Affine A{1.0, 0.0};
-    for (int32_t u = u0; u < u1; ++u) {
-        const int32_t i = top + u;
-        A = affine_after(Affine{(u == 0 && par < 0) ? 0.0 : sd[i], sr[i]}, A);
-    }
-    const Affine F = warp_exclusive(A, lane);
-    double x = F.m * xp + F.c;   // x at position u0 - 1 (u0 = 0: the parent's)
-    __syncwarp();
-    for (int32_t u = u0; u < u1; ++u) {
-        const int32_t i = top + u;
-        x = (u == 0 && par < 0) ? sr[i] : fma(sd[i], x, sr[i]);
-        sr[i] = x;
-        sv[i] = sv[i] + vscale * x;
-    }
-    __syncwarp();
-}
-
 /*
  * Hines solve, mixed mode: FP64 arithmetic with reciprocals.  Elimination keeps, per
  * node, f = a/D in place of D and R/D in place of R, so the back-substitution is one
  * FMA per node, x = f x_p + R/D; the pivot chain is D -> 1/D -> (a^2)(1/D) -> next D.
- * A level's longest chains may go to a warp each (warp_chains, eliminate_chain_warp,
- * substitute_chain_warp); the others to one thread each.
+ * One chain per thread, level by level.
  */
 template <int NT>
 __device__ __forceinline__ void hines_mixed(double *sd, double *sr, const double *sa, double *sv, double *sxd,
@@ -799,12 +595,8 @@ __device__ __forceinline__ void hines_mixed(double *sd, double *sr, const double
                                             const int32_t *lvc, int32_t nlev, double vscale, bool &singular) {
     constexpr int32_t T = NT;
     const int32_t tid = threadIdx.x;
-    const int32_t warp = tid >> 5;
-    constexpr int32_t NW = NT / 32;
     for (int32_t lv = 0; lv < nlev; ++lv) {
-        const int32_t lo = lvc[lv], hi = lvc[lv + 1];
-        const int32_t kw = warp_chains<NT>(clen, lo, hi);
-        for (int32_t ch = lo + kw + tid; ch < hi; ch += T) {
+        for (int32_t ch = lvc[lv] + tid; ch < lvc[lv + 1]; ch += T) {
             const int32_t top = ctop[ch];
             const int32_t bottom = top + clen[ch] - 1;
             const bool rooted = cpar[ch] < 0;
@@ -854,14 +646,10 @@ __device__ __forceinline__ void hines_mixed(double *sd, double *sr, const double
             sxd[ch] = rooted ? 0.0 : pxd;
             sxr[ch] = rooted ? 0.0 : pxr;
         }
-        if (NW - 1 - warp < kw)   // the last kw warps take the level's kw longest chains
-            eliminate_chain_warp(lo + NW - 1 - warp, sd, sr, sa, sxd, sxr, ctop, clen, cpar, ckoff, ckids, singular);
         __syncthreads();
     }
     for (int32_t lv = nlev - 1; lv >= 0; --lv) {
-        const int32_t lo = lvc[lv], hi = lvc[lv + 1];
-        const int32_t kw = warp_chains<NT>(clen, lo, hi);
-        for (int32_t ch = lo + kw + tid; ch < hi; ch += T) {
+        for (int32_t ch = lvc[lv] + tid; ch < lvc[lv + 1]; ch += T) {
             const int32_t top = ctop[ch];
             const int32_t bottom = top + clen[ch] - 1;
             const int32_t par = cpar[ch];
@@ -884,7 +672,6 @@ __device__ __forceinline__ void hines_mixed(double *sd, double *sr, const double
                 sv[i] = sv[i] + vscale * x;
             }
         }
-        if (NW - 1 - warp < kw) substitute_chain_warp(lo + NW - 1 - warp, sd, sr, sv, ctop, clen, cpar, vscale);
         __syncthreads();
     }
 }
@@ -904,8 +691,7 @@ __device__ __forceinline__ void hines_mixed(double *sd, double *sr, const double
 template <bool MIXED, int NT, bool GLOBAL_IMAGE = false, bool GEN = false,
           int MINB = NT == kCellThreads ? 5 : NT == kCellThreads / 2 ? 10 : 16>
 __global__ void __launch_bounds__(NT, MINB) window_kernel(const Params P, const int32_t *cells,
-                                                                               int64_t n0, int32_t W,
-                                                                               int32_t part_staged) {
+                                                                               int64_t n0, int32_t W) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ StagedGroup sg[kMaxGroups];
     const int32_t c = cells[blockIdx.x];
@@ -962,11 +748,7 @@ __global__ void __launch_bounds__(NT, MINB) window_kernel(const Params P, const 
     int32_t *ckids = ip; ip += nkids;
     int32_t *lvc = ip; ip += nlev + 1;
     int32_t *sorder = ip; ip += P.inbox_cap;
-    // the threads' row ranges: staged when the launch's shared memory has room for them
-    // without costing a resident CTA, else read through the read-only cache
-    int32_t *spart = ip;
-    if (part_staged) ip += P.ngroups * (O + 1);
-    const int32_t *part = part_staged ? spart : P.part + (int64_t)c * P.ngroups * (O + 1);
+    int32_t *spart = ip; ip += P.ngroups * (O + 1);   // the threads' row ranges per group
     int16_t *chain_of = reinterpret_cast<int16_t *>(ip);
     {
         // The launch sized the image for this cell's bin; refuse rather than overrun.
@@ -1032,8 +814,7 @@ __global__ void __launch_bounds__(NT, MINB) window_kernel(const Params P, const 
     if (tid == 0) ckoff[nch] = nkids;
     for (int32_t k = tid; k < nkids; k += T) ckids[k] = P.chain_kids[kb + k];
     for (int32_t k = tid; k <= nlev; k += T) lvc[k] = P.level_chain[lv0 + k];
-    if (part_staged)
-        for (int32_t k = tid; k < P.ngroups * (O + 1); k += T) spart[k] = P.part[(int64_t)c * P.ngroups * (O + 1) + k];
+    for (int32_t k = tid; k < P.ngroups * (O + 1); k += T) spart[k] = P.part[(int64_t)c * P.ngroups * (O + 1) + k];
     __syncthreads();
     for (int32_t k = tid; k < nch; k += T)
         for (int32_t i = ctop[k]; i < ctop[k] + clen[k]; ++i) chain_of[i] = (int16_t)k;
@@ -1166,7 +947,7 @@ __global__ void __launch_bounds__(NT, MINB) window_kernel(const Params P, const 
             const DevGroup &GG = P.groups[g];
             const StagedGroup G = sg[g];
             for (int32_t slot = tid; slot < O; slot += T) {
-                const int32_t lo = part[g * (O + 1) + slot], hi = part[g * (O + 1) + slot + 1];
+                const int32_t lo = spart[g * (O + 1) + slot], hi = spart[g * (O + 1) + slot + 1];
                 if (lo >= hi) continue;
                 if (G.kind == MIND_MECH_PAS) {
                     if (MIXED) continue;  // folded into the node constants of the assembly below

@@ -157,7 +157,6 @@ struct MindHandle {
         size_t smem_bytes;
         int32_t threads = kCellThreads;   // CTA size of the bin's launches (kCellThreads or half)
         bool tight = false;               // 128 threads, compiled for kTightBlocks CTAs per SM
-        size_t part_bytes = 0;            // the row-range table's share of smem_bytes
         int32_t max_detectors = 0;        // most threshold detectors on one of its cells
         bool global_image = false;        // cells too large for shared memory: image in HBM
     };
@@ -444,11 +443,7 @@ int create(const MindLayout *L, MindHandle *h) {
         }
         std::vector<int32_t> order(tops.size());
         for (size_t k = 0; k < order.size(); ++k) order[k] = (int32_t)k;
-        // by level, and within a level longest first (the mixed mode hands a level's longest
-        // chains to warps); each chain's elimination is independent of the order of its level
-        std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) {
-            return level[x] < level[y] || (level[x] == level[y] && chains[x].size() > chains[y].size());
-        });
+        std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) { return level[x] < level[y]; });
         std::vector<int32_t> rank(tops.size());
         for (size_t k = 0; k < order.size(); ++k) rank[order[k]] = (int32_t)k;
         // packed order: chains by rank, nodes top -> bottom
@@ -860,9 +855,8 @@ int create(const MindLayout *L, MindHandle *h) {
         bin.first = (int32_t)first;
         bin.count = (int32_t)(k - first);
         bin.smem_bytes = big ? 0 : top;
-        bin.part_bytes = big ? 0 : (size_t)L->n_mechanisms * (kCellThreads + 1) * sizeof(int32_t);
         bin.global_image = big;
-        bin.tight = !big && tight_by_default(top - bin.part_bytes);
+        bin.tight = !big && tight_by_default(top);
         if (!big) worst_smem = std::max(worst_smem, top);
         for (size_t q = first; q < k; ++q)
             bin.max_detectors = std::max(bin.max_detectors, det_off[need[q].second + 1] - det_off[need[q].second]);
@@ -1072,40 +1066,27 @@ int set_records(MindHandle *h, const MindRecord *records, int32_t nrec, int64_t 
     return MIND_OK;
 }
 
-/* Whether a bin's launches stage the row-range table in shared memory: yes unless leaving
- * it in HBM (read through the read-only cache) lets one more CTA share an SM (228 KB per
- * SM, 1 KB reserved per CTA; the register bound of the launch shape caps the count). */
-bool part_staged(const MindHandle::Bin &bin, bool generated) {
-    if (bin.global_image || generated) return true;
-    const int cap = bin.threads == kCellThreads ? (bin.tight ? kTightBlocks : 5) : bin.threads == kCellThreads / 2 ? 10 : 16;
-    const size_t sm = 228 * 1024;
-    const size_t with = std::min<size_t>(cap, sm / (bin.smem_bytes + 1024));
-    const size_t without = std::min<size_t>(cap, sm / (bin.smem_bytes - bin.part_bytes + 1024));
-    return without <= with;
-}
-
 /* One size bin's window-kernel launch in its chosen shape. */
 template <bool MIXED>
 void launch_window(const MindHandle::Bin &bin, cudaStream_t s, const Params &P, const int32_t *cells, int64_t n0,
                    int32_t W, bool generated) {
     constexpr int T = kCellThreads;
-    const int32_t staged = part_staged(bin, generated) ? 1 : 0;
-    const size_t smem = staged ? bin.smem_bytes : bin.smem_bytes - bin.part_bytes;
+    const size_t smem = bin.smem_bytes;
     if (generated) {   // models with mechanisms emitted from MOD files: the variant that runs them, 128 threads
         if (bin.global_image)
-            window_kernel<MIXED, T, true, true><<<bin.count, T, 0, s>>>(P, cells, n0, W, 1);
+            window_kernel<MIXED, T, true, true><<<bin.count, T, 0, s>>>(P, cells, n0, W);
         else
-            window_kernel<MIXED, T, false, true><<<bin.count, T, smem, s>>>(P, cells, n0, W, 1);
+            window_kernel<MIXED, T, false, true><<<bin.count, T, smem, s>>>(P, cells, n0, W);
     } else if (bin.global_image)
-        window_kernel<MIXED, T, true><<<bin.count, T, 0, s>>>(P, cells, n0, W, 1);
+        window_kernel<MIXED, T, true><<<bin.count, T, 0, s>>>(P, cells, n0, W);
     else if (bin.threads == T && bin.tight)
-        window_kernel<MIXED, T, false, false, kTightBlocks><<<bin.count, T, smem, s>>>(P, cells, n0, W, staged);
+        window_kernel<MIXED, T, false, false, kTightBlocks><<<bin.count, T, smem, s>>>(P, cells, n0, W);
     else if (bin.threads == T)
-        window_kernel<MIXED, T><<<bin.count, T, smem, s>>>(P, cells, n0, W, staged);
+        window_kernel<MIXED, T><<<bin.count, T, smem, s>>>(P, cells, n0, W);
     else if (bin.threads == T / 2)
-        window_kernel<MIXED, T / 2><<<bin.count, T / 2, smem, s>>>(P, cells, n0, W, staged);
+        window_kernel<MIXED, T / 2><<<bin.count, T / 2, smem, s>>>(P, cells, n0, W);
     else
-        window_kernel<MIXED, T / 4><<<bin.count, T / 4, smem, s>>>(P, cells, n0, W, staged);
+        window_kernel<MIXED, T / 4><<<bin.count, T / 4, smem, s>>>(P, cells, n0, W);
 }
 
 int advance(MindHandle *h, int64_t steps, bool record_spikes) {
@@ -1886,8 +1867,7 @@ int mind_set_bin_threads(MindHandle *h, const int32_t *threads, int32_t n_bins) 
     for (int32_t b = 0; b < n_bins; ++b) {
         MindHandle::Bin &bin = h->bins[b];
         bin.threads = threads[b];
-        bin.tight = threads[b] == kCellThreads && !bin.global_image &&
-                    tight_by_default(bin.smem_bytes - bin.part_bytes);
+        bin.tight = threads[b] == kCellThreads && !bin.global_image && tight_by_default(bin.smem_bytes);
     }
     return MIND_OK;
 }
