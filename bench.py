@@ -261,7 +261,11 @@ def measure_sharded(args, layout, rank: int, world: int, precision: str, local_r
     import mind_b200 as mb
     from mind_b200 import replicas, sharding
 
-    run = sharding.ShardedRun(layout, rank, world, precision=precision, device=COLLECTIVE_DEVICE, local=True)
+    # on GPUs the library exchanges the window's spikes itself (NCCL on its stream); the
+    # host exchange stands in on the CPU backend
+    exchange = "device" if COLLECTIVE_DEVICE == "cuda" else "host"
+    run = sharding.ShardedRun(layout, rank, world, precision=precision, device=COLLECTIVE_DEVICE, local=True,
+                              exchange=exchange)
     rasters = [run.run_steps(settle_steps, (), True), run.run_steps(args.warmup, (), True)]
     run.launches = 0
     sampler = ClockSampler(local_rank)
@@ -291,7 +295,8 @@ def measure_sharded(args, layout, rank: int, world: int, precision: str, local_r
              "cell_spikes_timed": int(np.sum(result.spike_sources < layout.n_cells)),
              "e2e": units / (e2e_ms / 1000.0), "d2h": d2h, "h2d": 0.0,
              "voltage_window_ms": [e2e_t0, end_ms], "raster_window_ms": [0.0, end_ms],
-             "exchange": "all-gather of (sid, time) per window over NCCL"},
+             "exchange": ("ncclAllGather of (sid, step) blocks per window inside the library, device-resident"
+                          if exchange == "device" else "all-gather of (sid, time) per window through the host")},
             (trace, np.concatenate([r.spike_sources for r in rasters]),
              np.concatenate([r.spike_times for r in rasters])), clocks)
 

@@ -248,6 +248,35 @@ int mind_autotune(MindHandle *h, int32_t windows);
 int mind_bin_threads(const MindHandle *h, int32_t *threads, int32_t cap, int32_t *n_bins);
 int mind_set_bin_threads(MindHandle *h, const int32_t *threads, int32_t n_bins);
 
+/*
+ * Spike exchange between ranks, for one network sharded by cell over GPUs (one process per
+ * GPU, each with the handle of its shard; the reference runs on one device, so there is no
+ * counterpart).  mind_exchange_id makes an NCCL unique id on one rank, which the host sends
+ * to the others (128 bytes).  mind_attach_exchange then gives the handle a communicator of
+ * `world` ranks (ncclCommInitRank, a collective call) and the maps of its shard:
+ * detector_sources[k] (0-based source index of a local detector) has global sid
+ * detector_sids[k]; spikes of global sid external_sids[k] enter through the local external
+ * input external_sources[k] (0-based).  `window` is the steps per window every rank uses
+ * (the smallest of the ranks' mind_window_steps), `width` the most spikes a rank sends per
+ * window (a window with more raises status 3).  From then on mind_run, after each window,
+ * packs the window's detector spikes, all-gathers the blocks of all ranks on the handle's
+ * stream (ncclAllGather, no host copy) and enters the received spikes through the external
+ * inputs' NetCons, the same fan-out as local spikes: the sharded run reproduces the
+ * unsharded one bit for bit.  Every rank must run the same steps.  With nccl_id NULL no
+ * communicator is made and the host drives the exchange: after a run of one window,
+ * mind_exchange_pack writes this rank's block (device memory, 1 + 2 width int64:
+ * count, then (sid, step) pairs) and mind_exchange_inject takes the gathered blocks of all
+ * ranks (device memory, world blocks).  Not with regions attached.  libnccl.so.2 is opened
+ * at run time (status 11 if absent).
+ */
+int mind_exchange_id(uint8_t id[128]);
+int mind_attach_exchange(MindHandle *h, const uint8_t *nccl_id, int32_t world, int32_t rank, int32_t window,
+                         int32_t width, const int32_t *detector_sources, const int32_t *detector_sids,
+                         int32_t n_detectors, const int32_t *external_sids, const int32_t *external_sources,
+                         int32_t n_external);
+int mind_exchange_pack(MindHandle *h, int64_t *send);
+int mind_exchange_inject(MindHandle *h, const int64_t *recv);
+
 /* Steps per device window: the largest step count a run advances without routing cell
  * spikes, set by the shortest NetCon delay out of cell detectors and external inputs.
  * A host that exchanges spikes with other handles runs at most this many steps between

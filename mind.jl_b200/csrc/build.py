@@ -47,7 +47,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if not force and up_to_date():
         return OUTPUT
     os.makedirs(OUT_DIR, exist_ok=True)
-    cmd = [nvcc(), *NVCC_FLAGS, *(["-Xptxas", "-v"] if verbose else []), "-o", OUTPUT, *SOURCES]
+    cmd = [nvcc(), *NVCC_FLAGS, *(["-Xptxas", "-v"] if verbose else []), "-o", OUTPUT, *SOURCES, "-ldl"]
     result = subprocess.run(cmd, capture_output=True, text=True)
     if result.returncode != 0:
         raise RuntimeError(f"nvcc failed ({result.returncode}):\n{result.stderr}\n{result.stdout}")

@@ -1236,6 +1236,60 @@ __global__ void record_initial_kernel(const Params P, const double *const *rec_i
 
 /* Host-injected events of one window: NetCon events into the ring, and the raster
  * entries of external spike inputs (edge < 0, point = 0-based source). */
+/* ---- spike exchange between ranks (one network sharded by cell) ----
+ *
+ * After a window, each rank packs its cells' spikes of the window into a fixed-width block
+ * (send[0] = count, then (sid, step) pairs), the blocks of all ranks are gathered
+ * (ncclAllGather, or a device copy when the host drives the exchange), and every rank
+ * enters the spikes of the sids it receives into its ring through the NetCons of the
+ * matching external sources -- the fan-out route_kernel does for local spikes, so events,
+ * bins and canonical orders are those of the unsharded run. */
+__global__ void exchange_pack_kernel(const Params P, const int32_t *sid_of_source, int64_t *send, int32_t width) {
+    __shared__ int32_t n;
+    if (threadIdx.x == 0) n = 0;
+    __syncthreads();
+    const int32_t count = min(*P.win_spike_count, P.win_spike_cap);
+    for (int32_t i = threadIdx.x; i < count; i += blockDim.x) {
+        const int32_t sid = sid_of_source[P.win_spike_source[i]];
+        if (sid < 0) continue;
+        const int32_t k = atomicAdd(&n, 1);
+        if (k < width) {
+            send[1 + 2 * (int64_t)k] = sid;
+            send[2 + 2 * (int64_t)k] = P.win_spike_step[i];
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (n > width) raise_error(P.error, MIND_ECAPACITY);
+        send[0] = min(n, width);
+    }
+}
+
+__global__ void exchange_inject_kernel(const Params P, const int64_t *recv, int32_t world, int32_t width,
+                                       const int32_t *ext_sid, const int32_t *ext_source, int32_t n_ext,
+                                       int64_t window_end) {
+    const int64_t stride = 1 + 2 * (int64_t)width;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < (int64_t)world * width;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = k / width, j = k - r * width;
+        const int64_t *block = recv + r * stride;
+        const int64_t n = block[0];
+        if (j >= n || n > width) continue;
+        const int64_t sid = block[1 + 2 * j];
+        const int64_t step = block[2 + 2 * j];
+        int32_t lo = 0, hi = n_ext;   // ext_sid ascending
+        while (lo < hi) {
+            const int32_t mid = (lo + hi) >> 1;
+            if (ext_sid[mid] < sid)
+                lo = mid + 1;
+            else
+                hi = mid;
+        }
+        if (lo == n_ext || ext_sid[lo] != sid) continue;
+        fan_out(P, ext_source[lo], (double)step * P.dt + 1.0e-10, window_end);
+    }
+}
+
 __global__ void inject_kernel(const Params P, const InjectedEvent *events, int32_t n, int64_t min_bin) {
     for (int32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         const InjectedEvent e = events[k];

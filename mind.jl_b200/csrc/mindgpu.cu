@@ -16,6 +16,8 @@
  * delivered after it, so each cell advances a whole window on its own.
  */
 #include <cuda_runtime.h>
+#include <dlfcn.h>
+#include <nccl.h>
 
 #include <algorithm>
 #include <array>
@@ -98,6 +100,12 @@ struct MindHandle {
     int32_t *sur_cells = nullptr, *sur_sources = nullptr, *sur_spikes = nullptr;
     float *sur_x = nullptr, *sur_prob = nullptr;
     float *sur_offset = nullptr;         // per cell (layout order): logit calibration offset
+    // spike exchange between ranks (mind_attach_exchange)
+    int32_t ex_world = 0, ex_rank = 0, ex_width = 0, ex_n_ext = 0;
+    int32_t *ex_sid_of_source = nullptr;   // [n_sources]: global sid of a local detector, else -1
+    int32_t *ex_ext_sid = nullptr, *ex_ext_source = nullptr;   // received sids (ascending) -> local source
+    int64_t *ex_send = nullptr, *ex_recv = nullptr;            // [1 + 2 width], [world][1 + 2 width]
+    ncclComm_t ex_comm = nullptr;
     // synaptic drive recording (mind_set_drive_recording)
     int32_t drive_bin_steps = 0;
     float *drive_dev = nullptr;
@@ -1066,6 +1074,46 @@ int set_records(MindHandle *h, const MindRecord *records, int32_t nrec, int64_t 
     return MIND_OK;
 }
 
+/* NCCL, opened at run time (libnccl.so.2, the one the process already has when torch loaded
+ * it): the library needs only these five entry points, for the exchange between ranks. */
+struct NcclApi {
+    decltype(&ncclGetUniqueId) get_unique_id = nullptr;
+    decltype(&ncclCommInitRank) comm_init_rank = nullptr;
+    decltype(&ncclAllGather) all_gather = nullptr;
+    decltype(&ncclCommDestroy) comm_destroy = nullptr;
+    decltype(&ncclGetErrorString) error_string = nullptr;
+};
+
+const NcclApi *nccl() {
+    static NcclApi api;
+    static bool ok = false;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *lib = dlopen("libnccl.so.2", RTLD_NOW | RTLD_GLOBAL);
+        if (!lib) return;
+        api.get_unique_id = reinterpret_cast<decltype(api.get_unique_id)>(dlsym(lib, "ncclGetUniqueId"));
+        api.comm_init_rank = reinterpret_cast<decltype(api.comm_init_rank)>(dlsym(lib, "ncclCommInitRank"));
+        api.all_gather = reinterpret_cast<decltype(api.all_gather)>(dlsym(lib, "ncclAllGather"));
+        api.comm_destroy = reinterpret_cast<decltype(api.comm_destroy)>(dlsym(lib, "ncclCommDestroy"));
+        api.error_string = reinterpret_cast<decltype(api.error_string)>(dlsym(lib, "ncclGetErrorString"));
+        ok = api.get_unique_id && api.comm_init_rank && api.all_gather && api.comm_destroy && api.error_string;
+    });
+    return ok ? &api : nullptr;
+}
+
+/* The window's exchange on the handle's stream: pack, all-gather (NCCL), inject. */
+int exchange_window(MindHandle *h, int64_t window_end) {
+    Params &P = h->P;
+    exchange_pack_kernel<<<1, 256, 0, h->stream>>>(P, h->ex_sid_of_source, h->ex_send, h->ex_width);
+    const size_t block = 1 + 2 * (size_t)h->ex_width;
+    const ncclResult_t r = nccl()->all_gather(h->ex_send, h->ex_recv, block, ncclInt64, h->ex_comm, h->stream);
+    if (r != ncclSuccess) return fail(h, MIND_ECUDA, std::string("ncclAllGather: ") + nccl()->error_string(r));
+    const int64_t total = (int64_t)h->ex_world * h->ex_width;
+    exchange_inject_kernel<<<launch_grid(std::max<int64_t>(total, 1)), kThreads, 0, h->stream>>>(
+        P, h->ex_recv, h->ex_world, h->ex_width, h->ex_ext_sid, h->ex_ext_source, h->ex_n_ext, window_end);
+    return MIND_OK;
+}
+
 /* One size bin's window-kernel launch in its chosen shape. */
 template <bool MIXED>
 void launch_window(const MindHandle::Bin &bin, cudaStream_t s, const Params &P, const int32_t *cells, int64_t n0,
@@ -1203,6 +1251,11 @@ int advance(MindHandle *h, int64_t steps, bool record_spikes) {
         route_kernel<<<64, kThreads, 0, h->stream>>>(P, n0 + W, M.source_region, M.bins, M.n, h->bin_steps,
                                                      M.bin_ring);
         ++st.launches;
+        if (h->ex_comm) {   // the other ranks' spikes of this window
+            const int status = exchange_window(h, n0 + W);
+            if (status) return status;
+            st.launches += 2;
+        }
         n0 += W;
     }
     CUDA_TRY(h, cudaGetLastError());
@@ -2053,9 +2106,102 @@ int mind_run_noalloc(MindHandle *h, int64_t steps, const MindRecord *records, in
     return MIND_OK;
 }
 
+int mind_exchange_id(uint8_t id[128]) {
+    if (!id) return MIND_EARG;
+    const NcclApi *api = nccl();
+    if (!api) return MIND_ECUDA;
+    ncclUniqueId u;
+    if (api->get_unique_id(&u) != ncclSuccess) return MIND_ECUDA;
+    static_assert(sizeof(u) == 128, "NCCL unique id of 128 bytes");
+    std::memcpy(id, &u, sizeof u);
+    return MIND_OK;
+}
+
+int mind_attach_exchange(MindHandle *h, const uint8_t *nccl_id, int32_t world, int32_t rank, int32_t window,
+                         int32_t width, const int32_t *detector_sources, const int32_t *detector_sids,
+                         int32_t n_detectors, const int32_t *external_sids, const int32_t *external_sources,
+                         int32_t n_external) {
+    if (!h || world < 1 || rank < 0 || rank >= world || window < 1 || width < 1 || n_detectors < 0 ||
+        n_external < 0 || (n_detectors > 0 && (!detector_sources || !detector_sids)) ||
+        (n_external > 0 && (!external_sids || !external_sources)))
+        return MIND_EARG;
+    if (h->ex_world) return fail(h, MIND_EARG, "an exchange is already attached");
+    if (h->M.n > 0) return fail(h, MIND_EARG, "a handle with regions attached runs on one GPU");
+    if ((int64_t)world * (1 + 2 * (int64_t)width) > (int64_t)1 << 31) return fail(h, MIND_EARG, "exchange too wide");
+    std::vector<int32_t> sid_of_source(std::max<int64_t>(h->n_sources, 1), -1);
+    for (int32_t k = 0; k < n_detectors; ++k) {
+        const int32_t src = detector_sources[k];
+        if (src < 0 || src >= h->n_sources || !h->source_detector[src] || detector_sids[k] < 0)
+            return fail(h, MIND_EARG, "an exchanged detector must be a detector source with a sid >= 0");
+        sid_of_source[src] = detector_sids[k];
+    }
+    std::vector<std::pair<int32_t, int32_t>> ext(n_external);
+    for (int32_t k = 0; k < n_external; ++k) {
+        const int32_t src = external_sources[k];
+        if (src < 0 || src >= h->n_sources || !h->source_external[src])
+            return fail(h, MIND_EARG, "a received sid must map to an external spike input");
+        ext[k] = {external_sids[k], src};
+    }
+    std::sort(ext.begin(), ext.end());
+    for (int32_t k = 1; k < n_external; ++k)
+        if (ext[k].first == ext[k - 1].first) return fail(h, MIND_EARG, "a sid is received by one source");
+    std::vector<int32_t> ext_sid(std::max(n_external, 1), -1), ext_source(std::max(n_external, 1), -1);
+    for (int32_t k = 0; k < n_external; ++k) {
+        ext_sid[k] = ext[k].first;
+        ext_source[k] = ext[k].second;
+    }
+    try {
+        h->ex_sid_of_source = h->upload(sid_of_source);
+        h->ex_ext_sid = h->upload(ext_sid);
+        h->ex_ext_source = h->upload(ext_source);
+        h->ex_send = h->alloc<int64_t>(1 + 2 * (size_t)width);
+        h->ex_recv = h->alloc<int64_t>((size_t)world * (1 + 2 * (size_t)width));
+    } catch (const std::bad_alloc &) {
+        return fail(h, MIND_ECUDA, "device allocation failed");
+    }
+    if (nccl_id) {
+        const NcclApi *api = nccl();
+        if (!api) return fail(h, MIND_ECUDA, "libnccl.so.2 could not be opened");
+        ncclUniqueId u;
+        std::memcpy(&u, nccl_id, sizeof u);
+        const ncclResult_t r = api->comm_init_rank(&h->ex_comm, world, u, rank);
+        if (r != ncclSuccess) {
+            h->ex_comm = nullptr;
+            return fail(h, MIND_ECUDA, std::string("ncclCommInitRank: ") + api->error_string(r));
+        }
+    }
+    h->ex_world = world;
+    h->ex_rank = rank;
+    h->ex_width = width;
+    h->ex_n_ext = n_external;
+    h->window = std::min(h->window, window);
+    return MIND_OK;
+}
+
+int mind_exchange_pack(MindHandle *h, int64_t *send) {
+    if (!h || !send) return MIND_EARG;
+    if (!h->ex_world) return fail(h, MIND_EARG, "no exchange is attached");
+    exchange_pack_kernel<<<1, 256, 0, h->stream>>>(h->P, h->ex_sid_of_source, send, h->ex_width);
+    CUDA_TRY(h, cudaGetLastError());
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    return check_device_error(h);
+}
+
+int mind_exchange_inject(MindHandle *h, const int64_t *recv) {
+    if (!h || !recv) return MIND_EARG;
+    if (!h->ex_world) return fail(h, MIND_EARG, "no exchange is attached");
+    const int64_t total = (int64_t)h->ex_world * h->ex_width;
+    exchange_inject_kernel<<<launch_grid(std::max<int64_t>(total, 1)), kThreads, 0, h->stream>>>(
+        h->P, recv, h->ex_world, h->ex_width, h->ex_ext_sid, h->ex_ext_source, h->ex_n_ext, h->step);
+    CUDA_TRY(h, cudaGetLastError());
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    return check_device_error(h);
+}
+
 int mind_destroy(MindHandle *h) {
     if (!h) return MIND_OK;
     if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->ex_comm && nccl()) nccl()->comm_destroy(h->ex_comm);
     for (cudaEvent_t e : h->prof_events) cudaEventDestroy(e);
     for (cudaEvent_t e : h->bin_done) cudaEventDestroy(e);
     for (cudaStream_t s : h->bin_streams) cudaStreamDestroy(s);

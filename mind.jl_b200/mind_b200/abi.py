@@ -196,6 +196,12 @@ def load_library():
     lib.mind_read_value.argtypes = [handle, POINTER(MindRecord), POINTER(c_double)]
     lib.mind_set_surrogate_cells.argtypes = [handle, POINTER(ctypes.c_uint8)]
     lib.mind_set_surrogate_offsets.argtypes = [handle, POINTER(ctypes.c_float), c_int32]
+    i32p = POINTER(c_int32)
+    lib.mind_exchange_id.argtypes = [POINTER(ctypes.c_uint8)]
+    lib.mind_attach_exchange.argtypes = [handle, POINTER(ctypes.c_uint8), c_int32, c_int32, c_int32, c_int32,
+                                         i32p, i32p, c_int32, i32p, i32p, c_int32]
+    lib.mind_exchange_pack.argtypes = [handle, c_void_p]
+    lib.mind_exchange_inject.argtypes = [handle, c_void_p]
     lib.mind_autotune.argtypes = [handle, c_int32]
     lib.mind_bin_threads.argtypes = [handle, POINTER(c_int32), c_int32, POINTER(c_int32)]
     lib.mind_set_bin_threads.argtypes = [handle, POINTER(c_int32), c_int32]
@@ -237,7 +243,8 @@ def load_library():
                  "mind_inject_event", "mind_last_run_ms", "mind_destroy", "mind_run_stats",
                  "mind_set_profiling", "mind_run_noalloc", "mind_inject_spikes", "mind_window_steps",
                  "mind_autotune", "mind_bin_threads", "mind_set_bin_threads", "mind_set_surrogate_cells",
-                 "mind_set_surrogate_offsets",
+                 "mind_set_surrogate_offsets", "mind_exchange_id", "mind_attach_exchange",
+                 "mind_exchange_pack", "mind_exchange_inject",
                  "mind_attach_macro", "mind_get_macro_trace", "mind_set_drive_recording", "mind_get_drive",
                  "mind_attach_surrogate",
                  "mind_mlp_create", "mind_mlp_destroy", "mind_mlp_last_ms",
@@ -254,7 +261,8 @@ EXPORTED_SYMBOLS = (
     "mind_get_trace", "mind_get_spikes", "mind_read_voltage", "mind_read_value", "mind_inject_event",
     "mind_last_error", "mind_last_run_ms", "mind_destroy", "mind_run_stats", "mind_set_profiling",
     "mind_run_noalloc", "mind_inject_spikes", "mind_window_steps", "mind_autotune", "mind_bin_threads",
-    "mind_set_surrogate_cells", "mind_set_surrogate_offsets",
+    "mind_set_surrogate_cells", "mind_set_surrogate_offsets", "mind_exchange_id", "mind_attach_exchange",
+    "mind_exchange_pack", "mind_exchange_inject",
     "mind_set_bin_threads", "mind_attach_macro", "mind_get_macro_trace",
     "mind_set_drive_recording", "mind_get_drive", "mind_attach_surrogate", "mind_mlp_create", "mind_mlp_destroy", "mind_mlp_last_error", "mind_mlp_last_ms", "mind_mlp_param_count", "mind_mlp_set_params",
     "mind_mlp_get_params", "mind_mlp_predict", "mind_mlp_gradients", "mind_mlp_set_data", "mind_mlp_train",

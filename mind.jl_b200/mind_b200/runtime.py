@@ -121,6 +121,35 @@ class DeviceState:
         abi.check(self.lib, self.handle, self.lib.mind_set_surrogate_offsets(
             self.handle, v.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), v.size))
 
+    def attach_exchange(self, nccl_id, world: int, rank: int, window: int, width: int, detector_sources,
+                        detector_sids, external_sids, external_sources) -> None:
+        """mind_attach_exchange: this handle's shard of a network over `world` ranks (0-based
+        source indices; nccl_id None: the host drives the exchange with exchange_pack /
+        exchange_inject)."""
+        def i32(a):
+            v = np.ascontiguousarray(np.asarray(a, dtype=np.int64))
+            if v.size and (v.min() < -(1 << 31) or v.max() >= (1 << 31)):
+                raise ValueError("sids and sources must fit in int32")
+            return np.ascontiguousarray(v.astype(np.int32))
+        ds, dd, es, eo = i32(detector_sources), i32(detector_sids), i32(external_sids), i32(external_sources)
+        if ds.size != dd.size or es.size != eo.size:
+            raise ValueError("one sid per detector and one source per received sid")
+        idbuf = None
+        if nccl_id is not None:
+            idbuf = (ctypes.c_uint8 * 128).from_buffer_copy(bytes(nccl_id))
+        p = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+        abi.check(self.lib, self.handle, self.lib.mind_attach_exchange(
+            self.handle, idbuf, int(world), int(rank), int(window), int(width), p(ds), p(dd), ds.size,
+            p(es), p(eo), es.size))
+
+    def exchange_pack(self, send_ptr: int) -> None:
+        """mind_exchange_pack into device memory at send_ptr (1 + 2 width int64)."""
+        abi.check(self.lib, self.handle, self.lib.mind_exchange_pack(self.handle, ctypes.c_void_p(send_ptr)))
+
+    def exchange_inject(self, recv_ptr: int) -> None:
+        """mind_exchange_inject from device memory at recv_ptr (world blocks)."""
+        abi.check(self.lib, self.handle, self.lib.mind_exchange_inject(self.handle, ctypes.c_void_p(recv_ptr)))
+
     def set_drive_recording(self, bin_ms: float) -> None:
         """mind_set_drive_recording: each run also returns the cells' binned synaptic drive."""
         abi.check(self.lib, self.handle, self.lib.mind_set_drive_recording(self.handle, float(bin_ms)))

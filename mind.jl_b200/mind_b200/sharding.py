@@ -14,8 +14,13 @@ NetCon delay in FP64, and each target cell applies a bin's events in the
 canonical (target, time, edge) order, so the sharded run reproduces the
 single-GPU run bit for bit.
 
-The exchange uses torch.distributed: NCCL over NVLink between GPUs, gloo on
-the CPU for the host-side tests.
+Two exchanges.  exchange="device" (the GPU path): the library holds an NCCL
+communicator (mind_attach_exchange) and, inside mind_run, packs each window's
+spikes on the device, all-gathers them on its own stream and enters the received
+ones through the external inputs' NetCons; nothing crosses to the host between
+windows.  exchange="host": the window's spikes come back with the run and are
+all-gathered by torch.distributed (NCCL, or gloo on the CPU for the host-side
+tests) and injected with mind_inject_spikes.
 """
 from __future__ import annotations
 
@@ -180,6 +185,16 @@ def local_shard(layout: Layout) -> Shard:
                  sids[nodes > 0].copy(), external, sids.copy())
 
 
+def exchange_maps(shard: Shard):
+    """The maps of mind_attach_exchange: (0-based sources of the shard's detectors, their
+    sids, the sids it receives, the 0-based external sources they enter through)."""
+    local_sids = np.asarray(shard.local_sids, dtype=np.int64)
+    det_src = np.nonzero(np.isin(local_sids, np.asarray(shard.detector_sids, dtype=np.int64)))[0]
+    ext_sid = np.array(sorted(shard.external_source), dtype=np.int64)
+    ext_src = np.array([shard.external_source[int(s)] - 1 for s in ext_sid], dtype=np.int64)
+    return det_src, local_sids[det_src], ext_sid, ext_src
+
+
 def exchange_spikes(sids: np.ndarray, times: np.ndarray, device="cpu"):
     """All-gather variable-length (sid, time) lists: counts first, then the padded lists."""
     import torch
@@ -219,9 +234,12 @@ class ShardedRun:
     """This rank's part of a network partitioned over the process group's ranks."""
 
     def __init__(self, layout: Layout, rank: int, world: int, *, precision: str = "fp64", device="cpu",
-                 owners: np.ndarray = None, local: bool = False):
+                 owners: np.ndarray = None, local: bool = False, exchange: str = "host"):
         """`layout` is the whole network, partitioned here (by `owners` or partition_cells), or,
-        with local=True, this rank's own part with external inputs for the other ranks' cells."""
+        with local=True, this rank's own part with external inputs for the other ranks' cells.
+        exchange: "device" (NCCL inside the library; needs the GPU and libnccl) or "host"."""
+        if exchange not in ("device", "host"):
+            raise ValueError("exchange is 'device' or 'host'")
         if local:
             self.owners = None
             self.shard = local_shard(layout)
@@ -235,6 +253,33 @@ class ShardedRun:
         self.window = global_window(self.state.window_steps(), device)
         self._external_sids = np.array(sorted(self.shard.external_source), dtype=np.int64)
         self.launches = 0
+        self.exchange = exchange
+        if exchange == "device":
+            self._attach_device_exchange(rank, world)
+
+    def _attach_device_exchange(self, rank: int, world: int):
+        import ctypes
+
+        import torch
+        import torch.distributed as dist
+
+        from . import abi
+
+        det_src, det_sid, ext_sid, ext_src = exchange_maps(self.shard)
+        most = torch.tensor([len(det_src)], dtype=torch.int64, device=self.device)
+        dist.all_reduce(most, op=dist.ReduceOp.MAX)
+        # a cell spikes at most once in a window shorter than its refractory time; the
+        # margin covers the rest, and a window with more spikes raises status 3
+        width = int(most.item()) + 16
+        ident = [None]
+        if rank == 0:
+            buf = (ctypes.c_uint8 * 128)()
+            status = self.state.lib.mind_exchange_id(buf)
+            if status != abi.MIND_OK:
+                raise abi.MindError(status, "mind_exchange_id: no NCCL")
+            ident = [bytes(buf)]
+        dist.broadcast_object_list(ident, src=0)
+        self.state.attach_exchange(ident[0], world, rank, self.window, width, det_src, det_sid, ext_sid, ext_src)
 
     def records(self, nodes: Sequence[int]):
         """RecordSpecs for global 1-based nodes of owned cells (named by the global node)."""
@@ -252,6 +297,13 @@ class ShardedRun:
         Returns this rank's result: its traces and the spikes of its own sources (remote
         inputs, which enter the local raster when injected, are left out).
         """
+        if self.exchange == "device":   # the library exchanges after every window
+            result = self.state.run_steps(steps, records, record_spikes)
+            self.launches += self.state.run_stats().launches
+            mine = ~np.isin(result.spike_sources, self._external_sids)
+            result.spike_times = result.spike_times[mine]
+            result.spike_sources = result.spike_sources[mine]
+            return result
         traces = {r.name: [] for r in records}
         times, sids = [], []
         start = None

@@ -59,7 +59,9 @@ def test_null_handles_are_refused_without_device_work():
         "mind_attach_macro": (None, None), "mind_get_macro_trace": (None, None, 0, None),
         "mind_set_drive_recording": (None, 1.0), "mind_get_drive": (None, None, 0, None),
         "mind_attach_surrogate": (None, None, None, 1.0), "mind_set_surrogate_cells": (None, None),
-            "mind_set_surrogate_offsets": (None, None, 0),
+            "mind_set_surrogate_offsets": (None, None, 0), "mind_exchange_id": (None,),
+            "mind_attach_exchange": (None, None, 2, 0, 1, 1, None, None, 0, None, None, 0),
+            "mind_exchange_pack": (None, None), "mind_exchange_inject": (None, None),
         "mind_last_run_ms": (None, ctypes.byref(d)), "mind_run_stats": (None, None),
         "mind_set_profiling": (None, 1), "mind_run_noalloc": (None, 1, None, 0, None),
         "mind_mlp_param_count": (None, ctypes.byref(i64)), "mind_mlp_last_ms": (None, None), "mind_mlp_set_params": (None, None, 0),
