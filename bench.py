@@ -392,10 +392,12 @@ def measure_surrogate(args, model, layout, train_ms: float = 300.0, eval_ms: flo
 
 
 def measure_config5(args, model, layout, train_ms: float = 500.0, eval_ms: float = 100.0, keep: float = 0.02,
-                    calibration_ms: float = 50.0, calibration_rounds: int = 3):
+                    calibration_rounds: int = 4):
     """Config 5 once: a surrogate trained on config 4 (about 1e6 windows of a detailed run of
-    train_ms), calibrated per population on the coupled 100,000-cell run against each
-    population's detailed sample, then eval_ms from initialize twice -- every cell detailed
+    train_ms), calibrated on the coupled 100,000-cell run (one offset for all populations,
+    rounds of eval_ms from initialize, against the pooled rate of the detailed sample: about
+    10 sample cells per population are too few to calibrate each), then eval_ms from
+    initialize twice -- every cell detailed
     (mixed mode), and all but `keep` of the cells replaced -- with time per step and the
     regions' population rates."""
     import mind_b200 as mb
@@ -422,7 +424,7 @@ def measure_config5(args, model, layout, train_ms: float = 500.0, eval_ms: float
     state.attach_macro(macro)
     state.attach_surrogate(net, mask, scale)
     t_c = time.perf_counter()
-    offsets, _ = surrogate.calibrate(state, layout, macro, mask, None, calibration_ms, calibration_rounds)
+    offsets, _ = surrogate.calibrate(state, layout, macro, mask, None, eval_ms, calibration_rounds, pooled=True)
     calibration_s = time.perf_counter() - t_c
     state.initialize()
     sur, sur_ms = device_timed(lambda: state.run_steps(steps, []))
@@ -448,8 +450,9 @@ def measure_config5(args, model, layout, train_ms: float = 500.0, eval_ms: float
                                   "counting_noise_per_region_mean": float(noise.mean()),
                                   "plain_rate_hz_mean": float(mean_plain.mean()),
                                   "surrogate_rate_hz_mean": float(r_sur.mean())},
-        "calibration": {"rounds": calibration_rounds, "ms_per_round": calibration_ms, "wall_s": calibration_s,
-                        "target": "each population's detailed sample, pooled over the rounds"},
+        "calibration": {"rounds": calibration_rounds, "ms_per_round": eval_ms, "wall_s": calibration_s,
+                        "offset": float(offsets[0]) if len(offsets) else 0.0,
+                        "target": "the pooled rate of the detailed sample (all populations), over the rounds"},
         "training": {"source": "config 4 (2,000 cells), detailed FP64 run", "train_ms": train_ms,
                      "windows": windows, "steps": 500, "batch": 4096, "wall_s": train_s},
         "note": "plain: every cell in the mixed mode; surrogate: the detailed sample in the mixed mode, the rest "

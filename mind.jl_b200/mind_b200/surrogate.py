@@ -234,7 +234,7 @@ def population_rates(layout, macro, result, t_ms: float, cells=None) -> np.ndarr
 
 
 def calibrate(state, layout, macro, surrogate_cells, target_hz, t_ms: float = 100.0, rounds: int = 4,
-              max_shift: float = 4.0):
+              max_shift: float = 4.0, pooled: bool = False):
     """Per-population calibration of the surrogate in its closed loop (no counterpart in the
     reference).  A coupled run feeds the surrogate's spikes back through the regions, so a
     small bias of the network grows into a large rate error; the remedy here is one logit
@@ -246,7 +246,9 @@ def calibrate(state, layout, macro, surrogate_cells, target_hz, t_ms: float = 10
     detailed run the network was trained on over the same t_ms from initialize (a run's
     early rates differ from its later ones), or is None: then each population's target is
     the rate of its detailed sample (the cells not in `surrogate_cells`) pooled over the
-    rounds so far.  Returns (per-cell offsets, per-round rates)."""
+    rounds so far.  pooled=True fits one offset for every population, from the rates of
+    all surrogate cells and all sample cells (for samples too small to judge one
+    population).  Returns (per-cell offsets, per-round rates)."""
     mask = np.asarray(surrogate_cells, dtype=bool)
     region = cell_regions(layout, macro)
     shift = np.zeros(macro.n_regions)
@@ -265,6 +267,15 @@ def calibrate(state, layout, macro, surrogate_cells, target_hz, t_ms: float = 10
             target = np.nanmean(np.array(sample), axis=0)
         else:
             target = np.asarray(target_hz, dtype=float)
+        if pooled:   # cell-weighted means over the populations
+            w_sur = np.array([np.count_nonzero(mask & (region == p)) for p in range(macro.n_regions)], float)
+            w_det = np.array([np.count_nonzero(~mask & (region == p)) for p in range(macro.n_regions)], float)
+            if target_hz is not None:
+                w_det = w_sur + w_det
+            m_all = np.nansum(np.nan_to_num(measured) * w_sur) / max(w_sur.sum(), 1.0)
+            t_all = np.nansum(np.nan_to_num(target) * w_det) / max(w_det.sum(), 1.0)
+            measured = np.full(macro.n_regions, m_all)
+            target = np.full(macro.n_regions, t_all)
         live = np.isfinite(measured) & np.isfinite(target) & (target > 0)
         safe_target = np.where(live, target, 1.0)
         ratio = np.where(measured > 0, safe_target / np.where(measured > 0, measured, 1.0), np.e)
