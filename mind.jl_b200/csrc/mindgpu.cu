@@ -873,7 +873,17 @@ int create(const MindLayout *L, MindHandle *h) {
     for (auto &x : need) bin_cells.push_back(x.second);
     h->bin_cells = h->upload(bin_cells);
     h->smem_bytes = worst_smem;
-    const int smem_attr = (int)std::max<size_t>(worst_smem, 1);
+    // The shared-memory opt-in is an attribute of the kernel function, shared by every handle
+    // of the process (and every device it runs on): it only grows, so a handle made later
+    // with smaller cells does not shrink what an earlier one launches with.
+    int smem_attr = (int)std::max<size_t>(worst_smem, 1);
+    {
+        static std::mutex mu;
+        static int largest = 0;
+        std::lock_guard<std::mutex> lock(mu);
+        largest = std::max(largest, smem_attr);
+        smem_attr = largest;
+    }
     CUDA_TRY(h, set_window_smem<kCellThreads>(smem_attr));
     CUDA_TRY(h, (set_window_smem<kCellThreads, kTightBlocks>(smem_attr)));
     CUDA_TRY(h, cudaFuncSetAttribute(window_kernel<false, kCellThreads, false, true>,
@@ -1137,7 +1147,14 @@ void launch_window(const MindHandle::Bin &bin, cudaStream_t s, const Params &P, 
         window_kernel<MIXED, T / 4><<<bin.count, T / 4, smem, s>>>(P, cells, n0, W);
 }
 
+/* The runtime's last-error slot is per thread and shared with the host's other CUDA code
+ * (a framework's lazy initialisation can leave a benign error in it): the library's launch
+ * checks must see only their own errors, so each entry that launches clears it first.  A
+ * sticky error (a lost context) is not cleared by this and fails the next call. */
+void clear_foreign_error() { (void)cudaGetLastError(); }
+
 int advance(MindHandle *h, int64_t steps, bool record_spikes) {
+    clear_foreign_error();
     Params &P = h->P;
     P.record_spikes = record_spikes ? 1 : 0;
     P.run_start = h->step;
@@ -2181,6 +2198,7 @@ int mind_attach_exchange(MindHandle *h, const uint8_t *nccl_id, int32_t world, i
 int mind_exchange_pack(MindHandle *h, int64_t *send) {
     if (!h || !send) return MIND_EARG;
     if (!h->ex_world) return fail(h, MIND_EARG, "no exchange is attached");
+    clear_foreign_error();
     exchange_pack_kernel<<<1, 256, 0, h->stream>>>(h->P, h->ex_sid_of_source, send, h->ex_width);
     CUDA_TRY(h, cudaGetLastError());
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
@@ -2190,6 +2208,7 @@ int mind_exchange_pack(MindHandle *h, int64_t *send) {
 int mind_exchange_inject(MindHandle *h, const int64_t *recv) {
     if (!h || !recv) return MIND_EARG;
     if (!h->ex_world) return fail(h, MIND_EARG, "no exchange is attached");
+    clear_foreign_error();
     const int64_t total = (int64_t)h->ex_world * h->ex_width;
     exchange_inject_kernel<<<launch_grid(std::max<int64_t>(total, 1)), kThreads, 0, h->stream>>>(
         h->P, recv, h->ex_world, h->ex_width, h->ex_ext_sid, h->ex_ext_source, h->ex_n_ext, h->step);

@@ -476,8 +476,11 @@ void transpose_inputs(MindMlp *m, int64_t rows, cudaStream_t s) {
     transpose_kernel<<<g, dim3(32, 8), 0, s>>>(m->x, rows, m->ld0, m->ld0, m->xt, m->capT);
 }
 
-/* Host FP32 rows into m->xin; the timed region of the call starts after the copy. */
+/* Host FP32 rows into m->xin; the timed region of the call starts after the copy.  The
+ * runtime's per-thread last-error slot is cleared first: the products check their launches
+ * with cudaGetLastError, which must not report the host's other CUDA code. */
 int upload_rows(MindMlp *m, const float *x, int64_t n) {
+    (void)cudaGetLastError();
     MLP_TRY(reserve(m, n));
     MLP_CUDA(m, cudaMemcpyAsync(m->xin, x, n * m->dims[0] * sizeof(float), cudaMemcpyHostToDevice, m->stream));
     MLP_CUDA(m, cudaEventRecord(m->t0, m->stream));
@@ -694,6 +697,7 @@ int mind_mlp_train(MindMlp *m, int32_t steps, int32_t batch, float lr, float *lo
         m->loss_cap = steps;
     }
     const CopyLayout C = copy_layout(m);
+    (void)cudaGetLastError();   // the products check their own launches only
     // One Adam step is captured as a graph and replayed `steps` times: the batch draw and the
     // bias corrections read the device step counter, which the step's last kernel advances.
     const uint64_t first = (uint64_t)m->adam_t;
