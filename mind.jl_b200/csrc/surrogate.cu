@@ -146,13 +146,17 @@ __global__ void adam_kernel(float *w, const float *g, float *m1, float *m2, int6
     }
 }
 
+/* Row kernels: blockIdx.y strides over rows, the threads of blockIdx.x over a row's
+ * columns (consecutive threads, consecutive columns: coalesced, no index division). */
+dim3 row_grid(int64_t rows, int32_t cols) {
+    return dim3((unsigned)((cols + kT - 1) / kT), (unsigned)std::max<int64_t>(1, std::min<int64_t>(rows, 16384)));
+}
+
 /* FP32 rows [n x d] -> BF16 rows of stride ld, zero past d. */
 __global__ void to_bf16_rows_kernel(const float *x, __nv_bfloat16 *out, int64_t n, int32_t d, int32_t ld) {
-    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n * ld; k += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t row = k / ld;
-        const int32_t col = (int32_t)(k - row * ld);
-        out[k] = __float2bfloat16(col < d ? x[row * d + col] : 0.0f);
-    }
+    for (int64_t row = blockIdx.y; row < n; row += gridDim.y)
+        for (int32_t col = blockIdx.x * blockDim.x + threadIdx.x; col < ld; col += gridDim.x * blockDim.x)
+            out[row * ld + col] = __float2bfloat16(col < d ? x[row * d + col] : 0.0f);
 }
 
 /* Rows of the training set drawn for Adam step *step + 1 (a 64-bit mix of step and slot), as
@@ -160,16 +164,16 @@ __global__ void to_bf16_rows_kernel(const float *x, __nv_bfloat16 *out, int64_t 
 __global__ void gather_kernel(const float *x, const float *y, __nv_bfloat16 *hx, float *hy, int64_t n, int32_t d,
                               int32_t ld, int32_t batch, const uint64_t *step_dev) {
     const uint64_t step = *step_dev + 1;
-    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < (int64_t)batch * ld;
-         k += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t row = k / ld, col = k % ld;
+    for (int64_t row = blockIdx.y; row < batch; row += gridDim.y) {
         uint64_t s = step * 0x9E3779B97F4A7C15ull + (uint64_t)row * 0xBF58476D1CE4E5B9ull + 0x94D049BB133111EBull;
         s ^= s >> 31;
         s *= 0xD6E8FEB86659FD93ull;
         s ^= s >> 32;
         const int64_t src = (int64_t)(s % (uint64_t)n);
-        hx[k] = __float2bfloat16(col < d ? x[src * d + col] : 0.0f);
-        if (col == 0) hy[row] = y[src];
+        for (int32_t col = blockIdx.x * blockDim.x + threadIdx.x; col < ld; col += gridDim.x * blockDim.x) {
+            hx[row * ld + col] = __float2bfloat16(col < d ? x[src * d + col] : 0.0f);
+            if (col == 0) hy[row] = y[src];
+        }
     }
 }
 
@@ -484,7 +488,7 @@ int upload_rows(MindMlp *m, const float *x, int64_t n) {
     MLP_TRY(reserve(m, n));
     MLP_CUDA(m, cudaMemcpyAsync(m->xin, x, n * m->dims[0] * sizeof(float), cudaMemcpyHostToDevice, m->stream));
     MLP_CUDA(m, cudaEventRecord(m->t0, m->stream));
-    to_bf16_rows_kernel<<<grid(n * m->ld0), kT, 0, m->stream>>>(m->xin, m->x, n, m->dims[0], m->ld0);
+    to_bf16_rows_kernel<<<row_grid(n, m->ld0), kT, 0, m->stream>>>(m->xin, m->x, n, m->dims[0], m->ld0);
     return MIND_OK;
 }
 
@@ -519,7 +523,7 @@ int mind_mlp_forward_device(MindMlp *m, const float *x, int64_t n, float *prob, 
     if (n == 0) return MIND_OK;
     MLP_CUDA(m, cudaEventRecord(m->ready, stream));
     MLP_CUDA(m, cudaStreamWaitEvent(m->stream, m->ready, 0));
-    to_bf16_rows_kernel<<<grid(n * m->ld0), kT, 0, m->stream>>>(x, m->x, n, m->dims[0], m->ld0);
+    to_bf16_rows_kernel<<<row_grid(n, m->ld0), kT, 0, m->stream>>>(x, m->x, n, m->dims[0], m->ld0);
     int32_t *own = m->err;
     m->err = err;
     const int s = forward(m, n, false, m->stream, prob);
@@ -706,7 +710,7 @@ int mind_mlp_train(MindMlp *m, int32_t steps, int32_t batch, float lr, float *lo
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     MLP_CUDA(m, cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal));
-    gather_kernel<<<grid((int64_t)batch * m->ld0), kT, 0, m->stream>>>(m->data_x, m->data_y, m->x, m->y, m->data_n,
+    gather_kernel<<<row_grid(batch, m->ld0), kT, 0, m->stream>>>(m->data_x, m->data_y, m->x, m->y, m->data_n,
                                                                     m->dims[0], m->ld0, batch, m->step_dev);
     transpose_inputs(m, batch, m->stream);
     int status = forward(m, batch, true, m->stream);
