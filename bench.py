@@ -42,6 +42,7 @@ METRIC = "compartment-steps/s (config 2: 10,000 uneven cells, recurrent Exp2Syn,
 WORKLOAD_METRICS = {
     2: METRIC,
     3: "compartment-steps/s (config 3: 1,000 uneven cells, 3e5 NetStim-driven Exp2Syn, dt 0.025 ms)",
+    4: "compartment-steps/s (config 4: 2,000 uneven cells coupled to 20 Jansen-Rit regions, dt 0.025 ms)",
 }
 UNIT = "compartment-steps/s"
 
