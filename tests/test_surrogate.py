@@ -115,3 +115,65 @@ def test_network_shapes_the_tensor_core_kernels_cannot_tile_are_refused():
         cfg = abi.MindMlpConfig(n_in, hidden, layers, 1)
         assert lib.mind_mlp_create(ctypes.byref(cfg), ctypes.byref(h)) == abi.MIND_EARG
         assert not h.value
+
+
+class _LoopState:
+    """Stands in for a coupled run on the host: each population's surrogate cells fire at
+    base_hz * exp(offset) * gain (a closed loop that scales every population's bias), the
+    detailed sample at sample_hz; spike counts are the expected counts, rounded."""
+
+    def __init__(self, layout, macro, mask, base_hz, sample_hz, gain):
+        from mind_b200 import surrogate
+
+        self.layout, self.mask = layout, np.asarray(mask, dtype=bool)
+        self.region = surrogate.cell_regions(layout, macro)
+        self.base, self.sample, self.gain = np.asarray(base_hz), np.asarray(sample_hz), gain
+        self.offsets = np.zeros(layout.n_cells)
+        offsets = np.asarray(layout.cell_offsets)
+        self.sid_of_cell = {}
+        for s, node in enumerate(np.asarray(layout.source_nodes)):
+            if node > 0:
+                self.sid_of_cell[int(np.searchsorted(offsets, node - 1, side="right") - 1)] = int(layout.source_ids[s])
+
+    def set_surrogate_offsets(self, offsets):
+        self.offsets = np.asarray(offsets, dtype=float)
+
+    def initialize(self):
+        pass
+
+    def run_steps(self, steps, records):
+        from types import SimpleNamespace
+
+        seconds = steps * self.layout.dt * 1e-3
+        sids = []
+        for c, sid in self.sid_of_cell.items():
+            p = self.region[c]
+            if p < 0:
+                continue
+            hz = self.base[p] * np.exp(self.offsets[c]) * self.gain if self.mask[c] else self.sample[p]
+            sids += [sid] * int(round(hz * seconds))
+        return SimpleNamespace(spike_sources=np.asarray(sids, dtype=np.int64),
+                               spike_times=np.zeros(len(sids)))
+
+
+def test_calibration_moves_each_population_to_its_target_rate():
+    """surrogate.calibrate on a host stand-in for the coupled run: per-population offsets
+    bring populations that start 3x too low or 2x too high to their targets; the pooled
+    mode fits one offset to the detailed sample's pooled rate."""
+    import netcases
+    from mind_b200 import surrogate
+
+    model, macro = netcases.coupled_regions(n_regions=4, cells_per_region=50, synapses=4, seed=21)
+    layout = model.layout
+    mask = np.ones(layout.n_cells, dtype=bool)
+    mask[::10] = False
+    target = np.array([5.0, 8.0, 3.0, 6.0])
+    loop = _LoopState(layout, macro, mask, base_hz=[5.0 / 3, 16.0, 3.0, 2.0], sample_hz=target, gain=1.0)
+    offsets, history = surrogate.calibrate(loop, layout, macro, mask, target, t_ms=1000.0, rounds=3)
+    final = surrogate.population_rates(layout, macro, loop.run_steps(40000, []), 1000.0, mask)
+    np.testing.assert_allclose(final, target, rtol=0.03)
+    assert len(history) == 3 and np.all(np.isfinite(offsets))
+    # detailed sample as the target, one offset for all populations
+    loop = _LoopState(layout, macro, mask, base_hz=[2.0, 2.0, 2.0, 2.0], sample_hz=[4.0] * 4, gain=1.0)
+    offsets, _ = surrogate.calibrate(loop, layout, macro, mask, None, t_ms=1000.0, rounds=3, pooled=True)
+    assert np.allclose(offsets[mask], np.log(2.0), atol=0.02)
