@@ -606,57 +606,45 @@ __device__ __forceinline__ void hines_mixed(double *sd, double *sr, const double
                 D = D - sxd[cc];
                 R = R + sxr[cc];
             }
-            if (bottom == top) {   // one node: its pivot is D
-                singular |= (D == 0.0) | !isfinite(D);
-                const double ab = sa[bottom];
-                const double y = approx_reciprocal(D);
-                const double f = ab * y;
-                sd[bottom] = f;
-                sr[bottom] = R * y;
-                sxd[ch] = rooted ? 0.0 : (ab * ab) * y;
-                sxr[ch] = rooted ? 0.0 : f * R;
-                continue;
+            singular |= (D == 0.0) | !isfinite(D);
+            const double ab = sa[bottom];
+            double dn = 0.0, rn = 0.0, an = 0.0;
+            if (bottom > top) {
+                dn = sd[bottom - 1];
+                rn = sr[bottom - 1];
+                an = sa[bottom - 1];
             }
-            // Pivots as ratios of continuants, D_i = p_i / p_{i+1} with
-            // p_i = d_i p_{i+1} - a_{i+1}^2 p_{i+2} (p_bottom = D, p_{bottom+1} = 1): one FMA per
-            // node carries the recurrence; each node's reciprocal pivot p_{i+1} / p_i and the
-            // right-hand side R_i = r_i + f_{i+1} R_{i+1} follow off that chain.  The pair
-            // (p_i, p_{i+1}) is rescaled by a power of two (exact) after every four nodes.
-            double pnn = 1.0, pn = D, Rn = R;   // p_{i+2}, p_{i+1}, R_{i+1}
-            auto node = [&](int32_t j) {
-                const double a1 = sa[j + 1];
-                const double p = fma(sd[j], pn, -((a1 * a1) * pnn));
-                singular |= (pn == 0.0) | !isfinite(pn);
-                const double y1 = pnn * approx_reciprocal(pn);   // 1 / D_{j+1}
-                const double f1 = a1 * y1;
-                sd[j + 1] = f1;
-                sr[j + 1] = Rn * y1;
-                const double Rj = fma(f1, Rn, sr[j]);
-                pnn = pn;
-                pn = p;
-                Rn = Rj;
-            };
+            const double y = approx_reciprocal(D);
+            const double f = ab * y;
+            sd[bottom] = f;
+            sr[bottom] = R * y;
+            double pxd = (ab * ab) * y, pxr = f * R;
             int32_t i = bottom - 1;
-            for (; i - 3 >= top; i -= 4) {
-                node(i);
-                node(i - 1);
-                node(i - 2);
-                node(i - 3);
-                int e = ((__double2hiint(pn) >> 20) & 0x7ff) - 1023;
-                e = max(-1000, min(1000, e));
-                const double scale = __hiloint2double((1023 - e) << 20, 0);   // 2^-e
-                pn *= scale;
-                pnn *= scale;
+            for (; i > top; --i) {
+                const double Di = dn - pxd, Ri = rn + pxr, ai = an, asq = an * an;
+                dn = sd[i - 1];
+                rn = sr[i - 1];
+                an = sa[i - 1];
+                singular |= (Di == 0.0) | !isfinite(Di);
+                const double yi = approx_reciprocal(Di);
+                const double fi = ai * yi;
+                sd[i] = fi;
+                sr[i] = Ri * yi;
+                pxd = asq * yi;
+                pxr = fi * Ri;
             }
-            for (; i >= top; --i) node(i);
-            singular |= (pn == 0.0) | !isfinite(pn);
-            const double at = sa[top];
-            const double yt = pnn * approx_reciprocal(pn);
-            const double ft = at * yt;
-            sd[top] = ft;
-            sr[top] = Rn * yt;
-            sxd[ch] = rooted ? 0.0 : (at * at) * yt;
-            sxr[ch] = rooted ? 0.0 : ft * Rn;
+            if (bottom > top) {
+                const double Dt = dn - pxd, Rt = rn + pxr;
+                singular |= (Dt == 0.0) | !isfinite(Dt);
+                const double yt = approx_reciprocal(Dt);
+                const double ft = an * yt;
+                sd[top] = ft;
+                sr[top] = Rt * yt;
+                pxd = (an * an) * yt;
+                pxr = ft * Rt;
+            }
+            sxd[ch] = rooted ? 0.0 : pxd;
+            sxr[ch] = rooted ? 0.0 : pxr;
         }
         __syncthreads();
     }
