@@ -54,7 +54,6 @@ enum Epilogue { EPI_HIDDEN = 0, EPI_HEAD = 1, EPI_BACK = 2, EPI_F32 = 3 };
 
 struct EpiParams {
     int32_t M, N;                 // valid rows and columns of D
-    int32_t n_store;              // unused
     int32_t ld_out;               // row stride of the row-major outputs (elements)
     int32_t ld_t;                 // row stride of the transposed outputs (elements)
     const float *bias;            // [N]

@@ -121,3 +121,23 @@ def test_two_gloo_ranks_exchange_variable_length_spike_lists():
         assert out[r][0] == want_s
         assert out[r][1] == want_t
         assert out[r][2] == 20
+
+
+def test_exchange_maps_pair_every_crossing_netcon_with_a_detector():
+    """The maps of the device exchange (mind_attach_exchange): each shard's packed sids are
+    its own detectors, every sid it receives is a detector of the other shard, and the
+    external source a received sid enters through is the one whose NetCons carry it."""
+    layout = mb.build(netcases.recurrent_trees())
+    owners = sharding.partition_cells(layout, 2)
+    shards = [sharding.shard_layout(layout, np.nonzero(owners == r)[0]) for r in range(2)]
+    maps = [sharding.exchange_maps(sh) for sh in shards]
+    for r, (sh, (det_src, det_sid, ext_sid, ext_src)) in enumerate(zip(shards, maps)):
+        nodes = np.asarray(sh.layout.source_nodes)
+        assert np.all(nodes[det_src] > 0)                          # detectors of this shard
+        assert set(det_sid.tolist()) == set(np.asarray(sh.detector_sids).tolist())
+        other_det = set(maps[1 - r][1].tolist())
+        assert len(ext_sid) > 0 and set(ext_sid.tolist()) <= other_det
+        ids = np.asarray(sh.layout.source_ids)
+        np.testing.assert_array_equal(ids[ext_src], ext_sid)       # the source carries that sid
+        assert np.all(np.asarray(sh.layout.source_points)[ext_src] == 0) and np.all(nodes[ext_src] == 0)
+        assert np.all(np.diff(ext_sid) > 0)
