@@ -422,8 +422,22 @@ typedef struct MindMechanismInfo {
 } MindMechanismInfo;
 int mind_mechanism_count(int32_t *n);
 int mind_mechanism_info(int32_t index, MindMechanismInfo *info);
-/* The kind code of the emitted mechanism named `name`; MIND_EARG if none is compiled in. */
+/* The kind code of the emitted mechanism named `name`; MIND_EARG if none is known. */
 int mind_mechanism_kind(const char *name, int32_t *kind);
+/*
+ * Mechanisms compiled at run time (the reference's compile_mod / CompiledMechanism seam for a
+ * user MOD file, src/compiler/frontend.jl:85-110, src/compiler/ir.jl:340-356): `module_path`
+ * is a cubin of csrc/gen_module.cu built for sm_100a with MIND_RUNTIME_MECHANISMS against a
+ * runtime_mechanisms.cuh that the MOD front end emitted for `mechanisms` (after the ones
+ * compiled into the library); `mechanisms` describes them in the module's order (name,
+ * point, net_receive, fields, defaults, digest, ion_reads; `kind` is ignored).  They get the
+ * kind codes after those already known (mind_mechanism_kind gives them) and are appended
+ * to the registry for the life of the process; a later module must list the mechanisms of
+ * the earlier ones first, unchanged, then its own.  Handles created afterwards whose
+ * layouts use them launch that module's window kernels.  mind_b200.register_mod does all
+ * of this from a MOD file.  On failure the message is mind_last_error(NULL).
+ */
+int mind_load_mechanisms(const char *module_path, const MindMechanismInfo *mechanisms, int32_t n);
 
 /*
  * discretize (src/model/micro/morphology.jl:406-484): one morphology's sections into its

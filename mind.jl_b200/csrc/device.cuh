@@ -32,7 +32,12 @@
 #include <cstdint>
 #include "mind_math.h"
 #include "../../include/mindgpu.h"
+#ifdef MIND_RUNTIME_MECHANISMS
+// a mechanism module compiled at run time: the compiled-in mechanisms and those after them
+#include "runtime_mechanisms.cuh"
+#else
 #include "generated_mechanisms.cuh"
+#endif
 
 namespace mind {
 

@@ -688,6 +688,55 @@ static const GenMechanism kGenMechanisms[] = {
     {"AlphaSynapse", 1, 0, 71, 6, 0x29B06B38B5009424ull, ""},
 };
 
+#ifdef MIND_GEN_BUILTIN_DISPATCH
+__device__ __forceinline__ void gen_builtin_initial(int32_t id, const MindGenRow &r) {
+    switch (id) {
+        case 0: gen::M0_SEClamp::initial(r); return;
+        case 1: gen::M1_VClamp::initial(r); return;
+        case 2: gen::M2_hh::initial(r); return;
+        case 3: gen::M3_pas::initial(r); return;
+        case 4: gen::M4_ExpSyn::initial(r); return;
+        case 5: gen::M5_Exp2Syn::initial(r); return;
+        case 6: gen::M6_IClamp::initial(r); return;
+        case 7: gen::M7_AlphaSynapse::initial(r); return;
+        default: break;
+    }
+}
+__device__ __forceinline__ double gen_builtin_current(int32_t id, const MindGenRow &r) {
+    switch (id) {
+        case 0: return gen::M0_SEClamp::current(r);
+        case 1: return gen::M1_VClamp::current(r);
+        case 2: return gen::M2_hh::current(r);
+        case 3: return gen::M3_pas::current(r);
+        case 4: return gen::M4_ExpSyn::current(r);
+        case 5: return gen::M5_Exp2Syn::current(r);
+        case 6: return gen::M6_IClamp::current(r);
+        case 7: return gen::M7_AlphaSynapse::current(r);
+        default: break;
+    }
+    return 0.0;
+}
+__device__ __forceinline__ void gen_builtin_advance(int32_t id, const MindGenRow &r) {
+    switch (id) {
+        case 0: gen::M0_SEClamp::advance(r); return;
+        case 1: gen::M1_VClamp::advance(r); return;
+        case 2: gen::M2_hh::advance(r); return;
+        case 3: gen::M3_pas::advance(r); return;
+        case 4: gen::M4_ExpSyn::advance(r); return;
+        case 5: gen::M5_Exp2Syn::advance(r); return;
+        case 6: gen::M6_IClamp::advance(r); return;
+        case 7: gen::M7_AlphaSynapse::advance(r); return;
+        default: break;
+    }
+}
+__device__ __forceinline__ void gen_builtin_receive(int32_t id, const MindGenRow &r, double w, double flag) {
+    switch (id) {
+        case 4: gen::M4_ExpSyn::receive(r, w, flag); return;
+        case 5: gen::M5_Exp2Syn::receive(r, w, flag); return;
+        default: break;
+    }
+}
+#else
 __device__ __forceinline__ void gen_initial(int32_t id, const MindGenRow &r) {
     switch (id) {
         case 0: gen::M0_SEClamp::initial(r); return;
@@ -735,5 +784,6 @@ __device__ __forceinline__ void gen_receive(int32_t id, const MindGenRow &r, dou
         default: break;
     }
 }
+#endif
 
 }  // namespace mind

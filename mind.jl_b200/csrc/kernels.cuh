@@ -297,6 +297,15 @@ __global__ void netstim_init_kernel(const Params P, uint64_t digest, const uint6
     }
 }
 
+/* INITIAL of a group emitted from a MOD file, at t = 0 on the initial voltage. */
+__device__ __forceinline__ void generated_init_rows(const Params &P, int32_t g) {
+    const DevGroup &G = P.groups[g];
+    for (int32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < G.rows; r += gridDim.x * blockDim.x) {
+        const MindGenRow row{G.cols, G.rows, r, P.v[G.node[r]], 0.0, P.dt, P.celsius};
+        gen_initial(G.gen, row);
+    }
+}
+
 /* INITIAL blocks of the cell mechanisms; decay factors of the synapses. */
 __global__ void mechanism_init_kernel(const Params P, int32_t g) {
     const DevGroup &G = P.groups[g];
@@ -688,10 +697,8 @@ __device__ __forceinline__ void hines_mixed(double *sd, double *sr, const double
  * one chain per thread; along a chain only subtract -> divide -> multiply stays
  * on the dependency chain, the next node's operands being loaded ahead.
  */
-template <bool MIXED, int NT, bool GLOBAL_IMAGE = false, bool GEN = false,
-          int MINB = NT == kCellThreads ? 5 : NT == kCellThreads / 2 ? 10 : 16>
-__global__ void __launch_bounds__(NT, MINB) window_kernel(const Params P, const int32_t *cells,
-                                                                               int64_t n0, int32_t W) {
+template <bool MIXED, int NT, bool GLOBAL_IMAGE = false, bool GEN = false>
+__device__ __forceinline__ void window_body(const Params &P, const int32_t *cells, int64_t n0, int32_t W) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ StagedGroup sg[kMaxGroups];
     const int32_t c = cells[blockIdx.x];
@@ -1226,6 +1233,13 @@ __global__ void __launch_bounds__(NT, MINB) window_kernel(const Params P, const 
         }
     }
     if (!finite) atomicCAS(P.error, 0, MIND_ENONFINITE);
+}
+
+template <bool MIXED, int NT, bool GLOBAL_IMAGE = false, bool GEN = false,
+          int MINB = NT == kCellThreads ? 5 : NT == kCellThreads / 2 ? 10 : 16>
+__global__ void __launch_bounds__(NT, MINB) window_kernel(const Params P, const int32_t *cells, int64_t n0,
+                                                           int32_t W) {
+    window_body<MIXED, NT, GLOBAL_IMAGE, GEN>(P, cells, n0, W);
 }
 
 /* The run's first sample: every recorded value as it stands in HBM between runs. */

@@ -21,6 +21,7 @@
 
 #include <algorithm>
 #include <array>
+#include <memory>
 #include <mutex>
 #include <cmath>
 #include <cstdio>
@@ -114,6 +115,9 @@ struct MindHandle {
     int64_t drive_bins = 0;
     std::vector<double> v0_packed;
     bool has_generated = false;              // some group runs CUDA C emitted from a MOD file
+    bool gen_runtime = false;                // ... one compiled at run time (mind_load_mechanisms)
+    cudaKernel_t rt_window[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};   // that module's kernels
+    cudaKernel_t rt_init = nullptr;
     int32_t device = -1;                     // the device current at the first allocation: state and stream live there
     int64_t n_sources = 0;
     std::vector<int64_t> source_ids;
@@ -237,6 +241,63 @@ int field_index(const MindMechanism &m, const char *name) {
     return -1;
 }
 
+/* The generated mechanisms the library knows, by generated index (kind - MIND_MECH_GENERATED):
+ * those compiled in (kGenMechanisms), then those of modules compiled at run time and
+ * loaded by mind_load_mechanisms.  Append-only, so a kind keeps its meaning for the life of
+ * the process; the latest module's kernels serve every runtime index (each module holds
+ * all runtime mechanisms registered so far). */
+struct GenEntry {
+    std::string name;
+    int32_t point = 0, net_receive = 0;
+    std::vector<std::string> fields;
+    std::vector<const char *> field_ptrs;
+    std::vector<double> defaults;
+    uint64_t digest = 0;
+    std::string ion_reads;
+};
+
+struct GenRegistry {
+    std::mutex mu;
+    std::vector<std::unique_ptr<GenEntry>> entries;
+    cudaKernel_t window[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};   // [mixed][image in HBM]
+    cudaKernel_t init = nullptr;
+};
+
+GenRegistry &gen_registry() {
+    static GenRegistry *r = [] {
+        GenRegistry *g = new GenRegistry();
+        for (int32_t k = 0; k < kGeneratedCount; ++k) {
+            const GenMechanism &m = kGenMechanisms[k];
+            auto e = std::make_unique<GenEntry>();
+            e->name = m.name;
+            e->point = m.point;
+            e->net_receive = m.net_receive;
+            for (int32_t f = 0; f < m.n_fields; ++f) {
+                e->fields.push_back(kGenFieldNames[m.first_field + f]);
+                e->defaults.push_back(kGenDefaults[m.first_field + f]);
+            }
+            e->digest = m.digest;
+            e->ion_reads = m.ion_reads;
+            g->entries.push_back(std::move(e));
+        }
+        for (auto &e : g->entries)
+            for (auto &f : e->fields) e->field_ptrs.push_back(f.c_str());
+        return g;
+    }();
+    return *r;
+}
+
+/* The generated mechanism of `kind`, or null. */
+const GenEntry *gen_entry(int32_t kind) {
+    if (kind < MIND_MECH_GENERATED) return nullptr;
+    GenRegistry &g = gen_registry();
+    std::lock_guard<std::mutex> lock(g.mu);
+    const size_t k = (size_t)(kind - MIND_MECH_GENERATED);
+    return k < g.entries.size() ? g.entries[k].get() : nullptr;
+}
+
+bool generated_kind(int32_t kind) { return gen_entry(kind) != nullptr; }
+
 struct KindSpec {
     int32_t kind;
     std::vector<const char *> fields;   // layout fields copied to device slots 0..k-1
@@ -263,10 +324,9 @@ KindSpec spec_of(int32_t kind) {
         case MIND_MECH_PATTERNSTIM:   // no fields: its spike times come with the layout
             return {kind, {}, 0, 0};
         default:
-            if (kind_generated(kind)) {   // every field of an emitted mechanism, in column order
-                const GenMechanism &g = kGenMechanisms[kind - MIND_MECH_GENERATED];
+            if (const GenEntry *g = gen_entry(kind)) {   // every field of an emitted mechanism, in column order
                 KindSpec spec{kind, {}, 0, 0};
-                for (int32_t k = 0; k < g.n_fields; ++k) spec.fields.push_back(kGenFieldNames[g.first_field + k]);
+                for (const char *f : g->field_ptrs) spec.fields.push_back(f);
                 return spec;
             }
             return {0, {}, 0, 0};
@@ -320,10 +380,9 @@ int readable_slot(int32_t kind, const char *name) {
         {MIND_MECH_NETSTIM, "ispike", NS_ISPIKE},
     };
     if (!name) return -1;
-    if (kind_generated(kind)) {   // every column of an emitted mechanism is kept
-        const GenMechanism &g = kGenMechanisms[kind - MIND_MECH_GENERATED];
-        for (int32_t k = 0; k < g.n_fields; ++k)
-            if (std::strcmp(kGenFieldNames[g.first_field + k], name) == 0) return k;
+    if (const GenEntry *g = gen_entry(kind)) {   // every column of an emitted mechanism is kept
+        for (size_t k = 0; k < g->fields.size(); ++k)
+            if (g->fields[k] == name) return (int)k;
         return -1;
     }
     for (const Entry &e : table)
@@ -569,7 +628,7 @@ int create(const MindLayout *L, MindHandle *h) {
         init.kind = m.kind;
         init.rows = rows;
         init.digest = m.digest;
-        const bool generated = kind_generated(m.kind);
+        const bool generated = generated_kind(m.kind);
         const int32_t gen_cols = (int32_t)spec.fields.size();
         // an emitted mechanism keeps every field as a column, then its current scale
         init.f.assign(generated ? gen_cols + 1 : spec.nslot, std::vector<double>(rows, generated ? 1.0 : 0.0));
@@ -594,7 +653,7 @@ int create(const MindLayout *L, MindHandle *h) {
                     seg[r] = len;
                 }
             }
-            if (generated && !kGenMechanisms[m.kind - MIND_MECH_GENERATED].point) {
+            if (generated && !gen_entry(m.kind)->point) {
                 for (int32_t r = 0; r < rows; ++r)
                     if (seg[r] > 1) return fail(h, MIND_ELAYOUT, "density mechanism twice on one node");
                 for (int32_t r = 0; r < rows; ++r)
@@ -638,6 +697,7 @@ int create(const MindLayout *L, MindHandle *h) {
         for (int k = 0; k < spec.nfloat; ++k) G.s[k] = h->alloc<float>(rows);
         G.gen = generated ? m.kind - MIND_MECH_GENERATED : -1;
         h->has_generated |= generated;
+        h->gen_runtime |= generated && m.kind - MIND_MECH_GENERATED >= kGeneratedCount;
         G.ncols = generated ? gen_cols : 0;
         G.cols = generated ? h->alloc<double>((size_t)(gen_cols + 1) * (size_t)std::max(rows, 1)) : nullptr;
         h->group_init.push_back(std::move(init));
@@ -715,7 +775,7 @@ int create(const MindLayout *L, MindHandle *h) {
             if (t < 1 || t > np) return fail(h, MIND_ELAYOUT, "edge target out of range");
             int32_t kind = L->mechanisms[point_group[t - 1]].kind;
             const bool receives = kind == MIND_MECH_EXPSYN || kind == MIND_MECH_EXP2SYN ||
-                                  (kind_generated(kind) && kGenMechanisms[kind - MIND_MECH_GENERATED].net_receive > 0);
+                                  (generated_kind(kind) && gen_entry(kind)->net_receive > 0);
             if (!receives)
                 return fail(h, MIND_ELAYOUT, "NetCon target has no NET_RECEIVE on the device (ExpSyn, Exp2Syn or an "
                                              "emitted mechanism with one)");
@@ -892,6 +952,19 @@ int create(const MindLayout *L, MindHandle *h) {
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr));
     CUDA_TRY(h, set_window_smem<kCellThreads / 2>(smem_attr));
     CUDA_TRY(h, set_window_smem<kCellThreads / 4>(smem_attr));
+    if (h->gen_runtime) {   // mechanisms compiled at run time: the kernels of the latest module
+        GenRegistry &g = gen_registry();
+        {
+            std::lock_guard<std::mutex> lock(g.mu);
+            for (int a = 0; a < 2; ++a)
+                for (int b = 0; b < 2; ++b) h->rt_window[a][b] = g.window[a][b];
+            h->rt_init = g.init;
+        }
+        if (!h->rt_init) return fail(h, MIND_ELAYOUT, "no mechanism module is loaded (mind_load_mechanisms)");
+        for (int a = 0; a < 2; ++a)
+            CUDA_TRY(h, cudaFuncSetAttribute((const void *)h->rt_window[a][0],
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr));
+    }
     CUDA_TRY(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     CUDA_TRY(h, cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming));
     for (size_t b = 0; b < h->bins.size(); ++b) {
@@ -971,7 +1044,7 @@ int resolve_record(MindHandle *h, const MindRecord &rec, RecordTarget &out) {
     if (slot < 0) return fail(h, MIND_EARG, "mechanism field is not kept on the device (ASSIGNED in BREAKPOINT)");
     const int32_t kind = h->group_init[g].kind;
     const int32_t dev = h->dev_row_of[g][rec.row - 1];
-    out.initial = kind_generated(kind) ? P.groups[g].cols + (int64_t)slot * P.groups[g].rows + dev
+    out.initial = generated_kind(kind) ? P.groups[g].cols + (int64_t)slot * P.groups[g].rows + dev
                                        : P.groups[g].f[slot] + dev;
     if (kind == MIND_MECH_NETSTIM || kind == MIND_MECH_PATTERNSTIM) {
         out.cell = -1;   // artificial cells belong to no cell's window
@@ -1126,11 +1199,15 @@ int exchange_window(MindHandle *h, int64_t window_end) {
 
 /* One size bin's window-kernel launch in its chosen shape. */
 template <bool MIXED>
-void launch_window(const MindHandle::Bin &bin, cudaStream_t s, const Params &P, const int32_t *cells, int64_t n0,
-                   int32_t W, bool generated) {
+void launch_window(const MindHandle *h, const MindHandle::Bin &bin, cudaStream_t s, const Params &P,
+                   const int32_t *cells, int64_t n0, int32_t W) {
     constexpr int T = kCellThreads;
     const size_t smem = bin.smem_bytes;
-    if (generated) {   // models with mechanisms emitted from MOD files: the variant that runs them, 128 threads
+    if (h->gen_runtime) {   // the same kernel from a module compiled at run time
+        const void *k = (const void *)h->rt_window[MIXED ? 1 : 0][bin.global_image ? 1 : 0];
+        void *args[] = {(void *)&P, (void *)&cells, (void *)&n0, (void *)&W};
+        cudaLaunchKernel(k, dim3(bin.count), dim3(T), args, bin.global_image ? 0 : smem, s);
+    } else if (h->has_generated) {   // mechanisms emitted from MOD files: the variant that runs them, 128 threads
         if (bin.global_image)
             window_kernel<MIXED, T, true, true><<<bin.count, T, 0, s>>>(P, cells, n0, W);
         else
@@ -1256,9 +1333,9 @@ int advance(MindHandle *h, int64_t steps, bool record_spikes) {
             cudaStreamWaitEvent(s, h->fork, 0);
             const int32_t *cells = h->bin_cells + bin.first;
             if (h->precision == MIND_MIXED)
-                launch_window<true>(bin, s, P, cells, n0, W, h->has_generated);
+                launch_window<true>(h, bin, s, P, cells, n0, W);
             else
-                launch_window<false>(bin, s, P, cells, n0, W, h->has_generated);
+                launch_window<false>(h, bin, s, P, cells, n0, W);
             cudaEventRecord(h->bin_done[b], s);
             cudaStreamWaitEvent(h->stream, h->bin_done[b], 0);
             ++st.launches;
@@ -1460,6 +1537,13 @@ int mind_initialize(MindHandle *h) {
     if (status) return status;
     for (int32_t g = 0; g < P.ngroups; ++g) {
         if (g == P.ns_group || P.groups[g].rows == 0) continue;
+        if (h->gen_runtime && P.groups[g].gen >= 0) {   // INITIAL from the run-time module
+            int32_t gg = g;
+            void *args[] = {(void *)&P, (void *)&gg};
+            CUDA_TRY(h, cudaLaunchKernel((const void *)h->rt_init, dim3(launch_grid(P.groups[g].rows)), dim3(kThreads),
+                                         args, 0, h->stream));
+            continue;
+        }
         mechanism_init_kernel<<<launch_grid(P.groups[g].rows), kThreads, 0, h->stream>>>(P, g);
     }
     if (P.ns_group >= 0 && P.groups[P.ns_group].rows > 0)
@@ -1950,33 +2034,100 @@ int mind_window_steps(const MindHandle *h, int32_t *steps) {
 
 int mind_mechanism_count(int32_t *n) {
     if (!n) return MIND_EARG;
-    *n = kGeneratedCount;
+    GenRegistry &g = gen_registry();
+    std::lock_guard<std::mutex> lock(g.mu);
+    *n = (int32_t)g.entries.size();
     return MIND_OK;
 }
 
 int mind_mechanism_info(int32_t index, MindMechanismInfo *info) {
-    if (!info || index < 0 || index >= kGeneratedCount) return MIND_EARG;
-    const GenMechanism &g = kGenMechanisms[index];
-    info->name = g.name;
+    if (!info || index < 0) return MIND_EARG;
+    const GenEntry *g = gen_entry(MIND_MECH_GENERATED + index);
+    if (!g) return MIND_EARG;
+    info->name = g->name.c_str();
     info->kind = MIND_MECH_GENERATED + index;
-    info->point = g.point;
-    info->net_receive = g.net_receive;
-    info->n_fields = g.n_fields;
-    info->field_names = kGenFieldNames + g.first_field;
-    info->defaults = kGenDefaults + g.first_field;
-    info->digest = g.digest;
-    info->ion_reads = g.ion_reads;
+    info->point = g->point;
+    info->net_receive = g->net_receive;
+    info->n_fields = (int32_t)g->fields.size();
+    info->field_names = g->field_ptrs.data();
+    info->defaults = g->defaults.data();
+    info->digest = g->digest;
+    info->ion_reads = g->ion_reads.c_str();
     return MIND_OK;
 }
 
 int mind_mechanism_kind(const char *name, int32_t *kind) {
     if (!name || !kind) return MIND_EARG;
-    for (int32_t k = 0; k < kGeneratedCount; ++k)
-        if (std::strcmp(kGenMechanisms[k].name, name) == 0) {
-            *kind = MIND_MECH_GENERATED + k;
+    GenRegistry &g = gen_registry();
+    std::lock_guard<std::mutex> lock(g.mu);
+    for (size_t k = 0; k < g.entries.size(); ++k)
+        if (g.entries[k]->name == name) {
+            *kind = MIND_MECH_GENERATED + (int32_t)k;
             return MIND_OK;
         }
     return MIND_EARG;
+}
+
+int mind_load_mechanisms(const char *module_path, const MindMechanismInfo *mechanisms, int32_t n) {
+    if (!module_path || n < 0 || (n > 0 && !mechanisms)) return MIND_EARG;
+    GenRegistry &g = gen_registry();
+    std::lock_guard<std::mutex> lock(g.mu);
+    const size_t have = g.entries.size() - (size_t)kGeneratedCount;
+    if ((size_t)n < have) {
+        g_create_error = "a mechanism module must hold every mechanism registered before it";
+        return MIND_EARG;
+    }
+    for (int32_t k = 0; k < n; ++k) {
+        const MindMechanismInfo &m = mechanisms[k];
+        if (!m.name || m.n_fields < 0 || (m.n_fields > 0 && (!m.field_names || !m.defaults))) {
+            g_create_error = "mechanism description incomplete";
+            return MIND_EARG;
+        }
+        if ((size_t)k < have) {
+            const GenEntry &e = *g.entries[kGeneratedCount + k];
+            if (e.name != m.name || e.digest != m.digest) {
+                g_create_error = std::string("mechanism ") + m.name + " differs from the one registered at its index";
+                return MIND_EARG;
+            }
+        } else {
+            for (auto &e : g.entries)
+                if (e->name == m.name) {
+                    g_create_error = std::string("a mechanism named ") + m.name + " is already known";
+                    return MIND_EARG;
+                }
+        }
+    }
+    cudaLibrary_t lib = nullptr;
+    cudaError_t err = cudaLibraryLoadFromFile(&lib, module_path, nullptr, nullptr, 0, nullptr, nullptr, 0);
+    cudaKernel_t k[5] = {};
+    const char *names[5] = {"mind_rt_window_fp64", "mind_rt_window_fp64_hbm", "mind_rt_window_mixed",
+                            "mind_rt_window_mixed_hbm", "mind_rt_generated_init"};
+    for (int q = 0; err == cudaSuccess && q < 5; ++q) err = cudaLibraryGetKernel(&k[q], lib, names[q]);
+    if (err != cudaSuccess) {
+        g_create_error = std::string("mechanism module ") + module_path + ": " + cudaGetErrorString(err);
+        return MIND_ECUDA;
+    }
+    for (int32_t q = (int32_t)have; q < n; ++q) {
+        const MindMechanismInfo &m = mechanisms[q];
+        auto e = std::make_unique<GenEntry>();
+        e->name = m.name;
+        e->point = m.point;
+        e->net_receive = m.net_receive;
+        for (int32_t f = 0; f < m.n_fields; ++f) {
+            e->fields.push_back(m.field_names[f] ? m.field_names[f] : "");
+            e->defaults.push_back(m.defaults[f]);
+        }
+        for (auto &f : e->fields) e->field_ptrs.push_back(f.c_str());
+        e->digest = m.digest;
+        e->ion_reads = m.ion_reads ? m.ion_reads : "";
+        g.entries.push_back(std::move(e));
+    }
+    g.window[0][0] = k[0];
+    g.window[0][1] = k[1];
+    g.window[1][0] = k[2];
+    g.window[1][1] = k[3];
+    g.init = k[4];
+    return MIND_OK;
 }
 
 const char *mind_last_error(const MindHandle *h) {

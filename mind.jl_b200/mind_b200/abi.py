@@ -236,6 +236,7 @@ def load_library():
     lib.mind_mechanism_count.argtypes = [POINTER(c_int32)]
     lib.mind_mechanism_info.argtypes = [c_int32, POINTER(MindMechanismInfo)]
     lib.mind_mechanism_kind.argtypes = [c_char_p, POINTER(c_int32)]
+    lib.mind_load_mechanisms.argtypes = [c_char_p, POINTER(MindMechanismInfo), c_int32]
     lib.mind_discretize.argtypes = [POINTER(MindSection), c_int32, c_int64, POINTER(MindMorphology), c_char_p,
                                     c_int32]
     for name in ("mind_create", "mind_initialize", "mind_set_precision", "mind_run", "mind_step",
@@ -250,7 +251,7 @@ def load_library():
                  "mind_mlp_create", "mind_mlp_destroy", "mind_mlp_last_ms",
                  "mind_mlp_param_count", "mind_mlp_set_params", "mind_mlp_get_params", "mind_mlp_predict",
                  "mind_mlp_gradients", "mind_mlp_set_data", "mind_mlp_train", "mind_mechanism_count",
-                 "mind_mechanism_info", "mind_mechanism_kind", "mind_discretize"):
+                 "mind_mechanism_info", "mind_mechanism_kind", "mind_discretize", "mind_load_mechanisms"):
         getattr(lib, name).restype = c_int32
     _LIB = lib
     return lib
@@ -262,7 +263,7 @@ EXPORTED_SYMBOLS = (
     "mind_last_error", "mind_last_run_ms", "mind_destroy", "mind_run_stats", "mind_set_profiling",
     "mind_run_noalloc", "mind_inject_spikes", "mind_window_steps", "mind_autotune", "mind_bin_threads",
     "mind_set_surrogate_cells", "mind_set_surrogate_offsets", "mind_exchange_id", "mind_attach_exchange",
-    "mind_exchange_pack", "mind_exchange_inject",
+    "mind_exchange_pack", "mind_exchange_inject", "mind_load_mechanisms",
     "mind_set_bin_threads", "mind_attach_macro", "mind_get_macro_trace",
     "mind_set_drive_recording", "mind_get_drive", "mind_attach_surrogate", "mind_mlp_create", "mind_mlp_destroy", "mind_mlp_last_error", "mind_mlp_last_ms", "mind_mlp_param_count", "mind_mlp_set_params",
     "mind_mlp_get_params", "mind_mlp_predict", "mind_mlp_gradients", "mind_mlp_set_data", "mind_mlp_train",

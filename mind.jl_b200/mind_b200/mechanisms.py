@@ -173,20 +173,107 @@ def emitted(name: str) -> Mechanism:
 
 def compile_mod(source: str, filename: str = "<string>") -> Mechanism:
     """compile_mod (src/compiler/frontend.jl:85-110): parse and lower MOD source, and select
-    the emitted mechanism compiled into the library for exactly this source (same name and
-    SHA-256 digest).  The emitted CUDA C (mind_b200.nmodl.emit) runs through the window
-    kernel's generated-mechanism path, even for names that also have hand-written code."""
+    the emitted mechanism the library knows for exactly this source (same name and SHA-256
+    digest) -- compiled in, or compiled now (register_mod) when it is new.  The emitted CUDA
+    C (mind_b200.nmodl.emit) runs through the window kernel's generated-mechanism path, even
+    for names that also have hand-written code."""
     from .nmodl.cuda import compile_source
 
     ir = compile_source(source, filename)
     compiled = compiled_mechanisms().get(ir.name)
-    if compiled is None or compiled.digest != ir.digest:
-        raise ValueError(f"{ir.name} ({filename}) is not compiled into this library; add it with "
-                         "mind.jl_b200/csrc/gen_mechanisms.py and rebuild (mind.jl_b200/csrc/build.py)")
+    if compiled is None:
+        return _register(ir)
+    if compiled.digest != ir.digest:
+        raise ValueError(f"{ir.name} ({filename}) differs from the {ir.name} this process already knows "
+                         "(a mechanism name is registered once)")
     if compiled.fields != ir.field_names:
         raise ValueError(f"{ir.name}: the library's fields differ from this source's")
     return Mechanism(ir.name, ir.kind, compiled.code, compiled.fields, compiled.defaults, ir.digest,
                      len(ir.receive_args), tuple(ir.ion_reads))
+
+
+_RUNTIME = []   # MechanismIR of the mechanisms compiled at run time, in registry order
+
+
+def register_mod(source: str, filename: str = "<string>") -> Mechanism:
+    """Compile MOD source that the library was not built with and register it
+    (mind_load_mechanisms): its CUDA C is emitted after the compiled-in mechanisms
+    (mind_b200.nmodl.library.runtime_header), the window kernel's generated-mechanism
+    variants are compiled with it into a module (nvcc for sm_100a, csrc/gen_module.cu,
+    cached by the header's digest under mind.jl_b200/lib/mechanisms/), and the library
+    loads the module.  Handles created afterwards run it.  Returns its Mechanism."""
+    from .nmodl.cuda import compile_source
+
+    ir = compile_source(source, filename)
+    known = compiled_mechanisms().get(ir.name)
+    if known is not None:
+        if known.digest != ir.digest:
+            raise ValueError(f"{ir.name} ({filename}) differs from the {ir.name} this process already knows")
+        return known
+    return _register(ir)
+
+
+def mechanism_module(irs, first_id: int) -> str:
+    """The cubin of csrc/gen_module.cu for the mechanisms `irs` as generated ids first_id..
+    (compiled with nvcc for sm_100a on first use, cached by the header's digest)."""
+    import hashlib
+    import os
+    import subprocess
+
+    from .nmodl.library import runtime_header
+
+    header = runtime_header(irs, first_id)
+    package = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    csrc = os.path.join(package, "csrc")
+    out_dir = os.path.join(package, "lib", "mechanisms", hashlib.sha256(header.encode()).hexdigest()[:16])
+    module = os.path.join(out_dir, "module.cubin")
+    if not os.path.exists(module):
+        os.makedirs(out_dir, exist_ok=True)
+        with open(os.path.join(out_dir, "runtime_mechanisms.cuh"), "w") as f:
+            f.write(header)
+        nvcc = os.environ.get("NVCC") or ("/usr/local/cuda/bin/nvcc" if os.path.exists("/usr/local/cuda/bin/nvcc")
+                                         else "nvcc")
+        cmd = [nvcc, "-cubin", "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
+               "-fmad=false", "-DMIND_RUNTIME_MECHANISMS", "-I", out_dir, "-I", csrc, "-o", module + ".tmp",
+               os.path.join(csrc, "gen_module.cu")]
+        done = subprocess.run(cmd, capture_output=True, text=True)
+        if done.returncode != 0:
+            raise RuntimeError(f"nvcc failed on the mechanism module ({done.returncode}):\n{done.stderr}")
+        os.replace(module + ".tmp", module)
+    return module
+
+
+def _register(ir) -> Mechanism:
+    import ctypes
+
+    from . import abi
+
+    global _COMPILED
+    lib = abi.load_library()
+    first_id = len(compiled_mechanisms()) - len(_RUNTIME)
+    irs = _RUNTIME + [ir]
+    module = mechanism_module(irs, first_id)
+    keep = []   # ctypes buffers that must outlive the call
+    infos = (abi.MindMechanismInfo * len(irs))()
+    for k, m in enumerate(irs):
+        names = (ctypes.c_char_p * max(1, len(m.field_names)))(*[n.encode() for n in m.field_names])
+        defaults = (ctypes.c_double * max(1, len(m.defaults)))(*[float(d) for d in m.defaults])
+        reads = " ".join(f"{f} {ion}" for f, ion in m.ion_reads).encode()
+        keep += [names, defaults, reads]
+        infos[k].name = m.name.encode()
+        infos[k].point = int(m.kind == "point")
+        infos[k].net_receive = len(m.receive_args)
+        infos[k].n_fields = len(m.field_names)
+        infos[k].field_names = names
+        infos[k].defaults = defaults
+        infos[k].digest = m.digest
+        infos[k].ion_reads = reads
+    status = lib.mind_load_mechanisms(module.encode(), infos, len(irs))
+    if status != abi.MIND_OK:
+        raise abi.MindError(status, (lib.mind_last_error(None) or b"").decode())
+    _RUNTIME.append(ir)
+    _COMPILED = None
+    return compiled_mechanisms()[ir.name]
 
 
 def load_mod(path: str) -> Mechanism:

@@ -4,8 +4,10 @@
 functions per mechanism (mind_b200.nmodl.cuda), the dispatch the window kernel calls
 for a generated kind (kind code MIND_MECH_GENERATED + its index), and the host table
 behind mind_mechanism_info (name, kind, fields, defaults, NET_RECEIVE).  The header in
-the package (csrc/generated_mechanisms.cuh) is made by csrc/gen_mechanisms.py; a user
-MOD file goes through the same path and a rebuild (build_library).
+the package (csrc/generated_mechanisms.cuh) is made by csrc/gen_mechanisms.py.  A user
+MOD file is compiled at run time instead: `runtime_header` emits it after the compiled-in
+mechanisms, as a module of the window kernel's generated-mechanism variants
+(mind_b200.mechanisms.register_mod, mind_load_mechanisms).
 """
 from __future__ import annotations
 
@@ -27,6 +29,64 @@ def library_header(sources: Sequence[Tuple[str, str]]) -> str:
     names = [ir.name for ir in irs]
     if len(set(names)) != len(names):
         raise ValueError("two MOD files declare the same mechanism name")
+    return _header(irs)
+
+
+def runtime_header(irs: Sequence[MechanismIR], first_id: int) -> str:
+    """The header of a mechanism module compiled at run time (mind_load_mechanisms): the
+    mechanisms `irs` as generated ids first_id, first_id + 1, ..., after the ones compiled
+    into the library, whose header it includes with its dispatch renamed gen_builtin_*; its
+    own dispatch serves the new ids and passes the others on."""
+    out = ["/*",
+           " * runtime_mechanisms.cuh -- CUDA C emitted from MOD files by mind_b200.nmodl at run time: the",
+           f" * generated mechanisms {first_id}.. after those compiled into libmindgpu.so.",
+           " */",
+           "#pragma once",
+           "",
+           "#define MIND_GEN_BUILTIN_DISPATCH 1",
+           '#include "generated_mechanisms.cuh"',
+           "",
+           "namespace mind {",
+           "namespace gen {",
+           ""]
+    for k, ir in enumerate(irs):
+        out.append(emit_mechanism(ir, f"M{first_id + k}_{ir.name}"))
+        out.append("")
+    out.append("}  // namespace gen")
+    out.append("")
+    _dispatch(out, irs, first_id, "gen_", "gen_builtin_")
+    out.append("")
+    out.append("}  // namespace mind")
+    return "\n".join(out) + "\n"
+
+
+def _dispatch(out: List[str], irs: Sequence[MechanismIR], first_id: int, prefix: str, fallback: str = None):
+    """The window kernel's entry points for generated ids first_id..; other ids go to
+    `fallback` (the compiled-in dispatch) or do nothing."""
+    def one(name: str, params: str, args: str, call: str, ret: str, default: str, only=None):
+        out.append(f"__device__ __forceinline__ {ret} {prefix}{name}({params}) {{")
+        out.append("    switch (id) {")
+        for k, ir in enumerate(irs):
+            if only is not None and not only(ir):
+                continue
+            target = f"gen::M{first_id + k}_{ir.name}::{call}"
+            stmt = f"return {target};" if ret != "void" else f"{target}; return;"
+            out.append(f"        case {first_id + k}: {stmt}")
+        out.append("        default: break;")
+        out.append("    }")
+        if fallback is not None:
+            out.append(f"    {'return ' if ret != 'void' else ''}{fallback}{name}({args});")
+        elif ret != "void":
+            out.append(f"    return {default};")
+        out.append("}")
+    one("initial", "int32_t id, const MindGenRow &r", "id, r", "initial(r)", "void", "")
+    one("current", "int32_t id, const MindGenRow &r", "id, r", "current(r)", "double", "0.0")
+    one("advance", "int32_t id, const MindGenRow &r", "id, r", "advance(r)", "void", "")
+    one("receive", "int32_t id, const MindGenRow &r, double w, double flag", "id, r, w, flag", "receive(r, w, flag)",
+        "void", "", only=lambda ir: bool(ir.receive_args))
+
+
+def _header(irs: Sequence[MechanismIR]) -> str:
     out = ["/*",
            " * generated_mechanisms.cuh -- CUDA C emitted from MOD files by mind_b200.nmodl.  Do not edit:",
            " * regenerate with mind.jl_b200/csrc/gen_mechanisms.py.  Each mechanism's kind code is",
@@ -69,26 +129,13 @@ def library_header(sources: Sequence[Tuple[str, str]]) -> str:
                    f"{offsets[k + 1] - offsets[k]}, 0x{ir.digest:016X}ull, {_c_string(reads)}}},")
     out.append("};")
     out.append("")
-    # device dispatch
-    def dispatch(signature: str, call: str, ret: str, default: str, only=None):
-        out.append(f"__device__ __forceinline__ {ret} gen_{signature} {{")
-        out.append("    switch (id) {")
-        for k, ir in enumerate(irs):
-            if only is not None and not only(ir):
-                continue
-            stmt = f"return gen::M{k}_{ir.name}::{call};" if ret != "void" else \
-                f"gen::M{k}_{ir.name}::{call}; return;"
-            out.append(f"        case {k}: {stmt}")
-        out.append("        default: break;")
-        out.append("    }")
-        if ret != "void":
-            out.append(f"    return {default};")
-        out.append("}")
-    dispatch("initial(int32_t id, const MindGenRow &r)", "initial(r)", "void", "")
-    dispatch("current(int32_t id, const MindGenRow &r)", "current(r)", "double", "0.0")
-    dispatch("advance(int32_t id, const MindGenRow &r)", "advance(r)", "void", "")
-    dispatch("receive(int32_t id, const MindGenRow &r, double w, double flag)", "receive(r, w, flag)", "void", "",
-             only=lambda ir: bool(ir.receive_args))
+    # device dispatch: a module compiled at run time (runtime_header) includes this header with
+    # MIND_GEN_BUILTIN_DISPATCH defined, which renames these entry points gen_builtin_*
+    out.append("#ifdef MIND_GEN_BUILTIN_DISPATCH")
+    _dispatch(out, irs, 0, "gen_builtin_")
+    out.append("#else")
+    _dispatch(out, irs, 0, "gen_")
+    out.append("#endif")
     out.append("")
     out.append("}  // namespace mind")
     return "\n".join(out) + "\n"

@@ -139,3 +139,23 @@ def test_reference_mod_directory_parses_and_regenerates_the_committed_header():
         assert f.read() == library_header(read_sources(paths))
     for name in ("hh", "SEClamp"):
         assert mb.load_mod(os.path.join(MOD_DIR, f"{name}.mod")).code == mb.compiled_mechanisms()[name].code
+
+
+def test_a_user_mod_compiles_into_a_mechanism_module_for_sm_100a():
+    """register_mod's compile step, without a GPU: a MOD file the library was not built with
+    is emitted after the compiled-in mechanisms and the window kernel's generated variants
+    compile with it into a cubin (mind_load_mechanisms loads it on a GPU)."""
+    import os
+
+    from mind_b200 import mechanisms
+    from mind_b200.nmodl.cuda import compile_source
+
+    here = os.path.dirname(os.path.abspath(__file__))
+    path = os.path.join(here, "mod", "UserExpSyn.mod")
+    ir = compile_source(open(path).read(), path)
+    assert ir.name == "UserExpSyn" and ir.kind == "point" and len(ir.receive_args) == 1
+    first = len(mechanisms.compiled_mechanisms())
+    module = mechanisms.mechanism_module([ir], first)
+    assert os.path.getsize(module) > 10000
+    header = open(os.path.join(os.path.dirname(module), "runtime_mechanisms.cuh")).read()
+    assert f"M{first}_UserExpSyn" in header and "gen_builtin_current(id, r)" in header
