@@ -53,7 +53,8 @@ def test_mods_registered_at_run_time_run_like_the_builtins_they_restate():
     np.testing.assert_array_equal(again.traces.by_record, want.traces.by_record)
     assert np.sum(want.spike_sources < hand.n_cells) > 5
     # the registry knows them by name, and a source that differs from a registered one is refused
-    assert mb.compiled_mechanisms()["UserLeak"].fields == ("g", "e", "i")
+    assert leak.name == "userleak"   # a density mechanism is named by its SUFFIX
+    assert mb.compiled_mechanisms()["userleak"].fields == ("g", "e", "i")
     with pytest.raises(ValueError):
         mb.compile_mod(open(os.path.join(HERE, "mod", "UserLeak.mod")).read().replace("-70", "-60"), "x.mod")
     s_first.close()
