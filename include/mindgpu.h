@@ -203,6 +203,9 @@ int mind_time(const MindHandle *h, int64_t *step, double *time);
 
 /* Traces of the last mind_run, sample-major [samples x n_records]; n must equal that size. */
 int mind_get_trace(const MindHandle *h, double *out, int64_t n);
+/* The same traces record-major [n_records x samples] (one record's samples contiguous, the
+ * layout of SimulationResult's per-record vectors), transposed on the device before the copy. */
+int mind_get_trace_by_record(MindHandle *h, double *out, int64_t n);
 
 /* Spikes of the last mind_run, sorted by (time, sid); *n receives the count (also when cap is short). */
 int mind_get_spikes(const MindHandle *h, double *times, int64_t *sids, int64_t cap, int64_t *n);

@@ -1242,6 +1242,25 @@ __global__ void __launch_bounds__(NT, MINB) window_kernel(const Params P, const 
     window_body<MIXED, NT, GLOBAL_IMAGE, GEN>(P, cells, n0, W);
 }
 
+/* dst [records x samples] = src [samples x records], through 32 x 32 shared-memory tiles
+ * (both sides read and written along rows). */
+__global__ void trace_transpose_kernel(const double *src, double *dst, int64_t samples, int32_t records) {
+    __shared__ double tile[32][33];
+    const int64_t s0 = (int64_t)blockIdx.x * 32;
+    const int32_t r0 = blockIdx.y * 32;
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int64_t s = s0 + k;
+        const int32_t r = r0 + threadIdx.x;
+        if (s < samples && r < records) tile[k][threadIdx.x] = src[s * records + r];
+    }
+    __syncthreads();
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int32_t r = r0 + k;
+        const int64_t s = s0 + threadIdx.x;
+        if (r < records && s < samples) dst[(int64_t)r * samples + s] = tile[threadIdx.x][k];
+    }
+}
+
 /* The run's first sample: every recorded value as it stands in HBM between runs. */
 __global__ void record_initial_kernel(const Params P, const double *const *rec_initial, int32_t nrec) {
     for (int32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nrec; k += gridDim.x * blockDim.x)

@@ -144,6 +144,8 @@ struct MindHandle {
     std::vector<std::vector<int32_t>> group_row_off;
     // results
     const double *trace_result = nullptr;   // the last run's traces (device), [samples x records]
+    double *trace_by_record = nullptr;      // their transpose for mind_get_trace_by_record (grow-only)
+    size_t trace_by_record_cap = 0;
     int64_t trace_samples = 0;
     int32_t trace_records = 0;
     std::vector<double> spike_times;
@@ -1837,6 +1839,32 @@ int mind_get_trace(const MindHandle *h, double *out, int64_t n) {
     if (n != h->trace_samples * (int64_t)h->trace_records || (n && !out)) return MIND_EARG;
     if (n && cudaMemcpy(out, h->trace_result, n * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
         return MIND_ECUDA;
+    return MIND_OK;
+}
+
+int mind_get_trace_by_record(MindHandle *h, double *out, int64_t n) {
+    if (!h) return MIND_EARG;
+    const int64_t samples = h->trace_samples, records = h->trace_records;
+    if (n != samples * records || (n && !out)) return MIND_EARG;
+    if (n == 0) return MIND_OK;
+    if ((size_t)n > h->trace_by_record_cap) {
+        h->release(h->trace_by_record);
+        h->trace_by_record = nullptr;
+        h->trace_by_record_cap = 0;
+        try {
+            h->trace_by_record = h->alloc<double>((size_t)n);
+        } catch (const std::bad_alloc &) {
+            return fail(h, MIND_ECUDA, "device allocation failed");
+        }
+        h->trace_by_record_cap = (size_t)n;
+    }
+    const dim3 g((unsigned)((samples + 31) / 32), (unsigned)((records + 31) / 32));
+    trace_transpose_kernel<<<g, dim3(32, 8), 0, h->stream>>>(h->trace_result, h->trace_by_record, samples,
+                                                             (int32_t)records);
+    CUDA_TRY(h, cudaGetLastError());
+    CUDA_TRY(h, cudaMemcpyAsync(out, h->trace_by_record, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost,
+                                h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     return MIND_OK;
 }
 

@@ -191,6 +191,7 @@ def load_library():
     lib.mind_step.argtypes = [handle]
     lib.mind_time.argtypes = [handle, POINTER(c_int64), POINTER(c_double)]
     lib.mind_get_trace.argtypes = [handle, POINTER(c_double), c_int64]
+    lib.mind_get_trace_by_record.argtypes = [handle, POINTER(c_double), c_int64]
     lib.mind_get_spikes.argtypes = [handle, POINTER(c_double), POINTER(c_int64), c_int64, POINTER(c_int64)]
     lib.mind_read_voltage.argtypes = [handle, c_int32, POINTER(c_double)]
     lib.mind_read_value.argtypes = [handle, POINTER(MindRecord), POINTER(c_double)]
@@ -251,7 +252,8 @@ def load_library():
                  "mind_mlp_create", "mind_mlp_destroy", "mind_mlp_last_ms",
                  "mind_mlp_param_count", "mind_mlp_set_params", "mind_mlp_get_params", "mind_mlp_predict",
                  "mind_mlp_gradients", "mind_mlp_set_data", "mind_mlp_train", "mind_mechanism_count",
-                 "mind_mechanism_info", "mind_mechanism_kind", "mind_discretize", "mind_load_mechanisms"):
+                 "mind_mechanism_info", "mind_mechanism_kind", "mind_discretize", "mind_load_mechanisms",
+                 "mind_get_trace_by_record"):
         getattr(lib, name).restype = c_int32
     _LIB = lib
     return lib
@@ -263,7 +265,7 @@ EXPORTED_SYMBOLS = (
     "mind_last_error", "mind_last_run_ms", "mind_destroy", "mind_run_stats", "mind_set_profiling",
     "mind_run_noalloc", "mind_inject_spikes", "mind_window_steps", "mind_autotune", "mind_bin_threads",
     "mind_set_surrogate_cells", "mind_set_surrogate_offsets", "mind_exchange_id", "mind_attach_exchange",
-    "mind_exchange_pack", "mind_exchange_inject", "mind_load_mechanisms",
+    "mind_exchange_pack", "mind_exchange_inject", "mind_load_mechanisms", "mind_get_trace_by_record",
     "mind_set_bin_threads", "mind_attach_macro", "mind_get_macro_trace",
     "mind_set_drive_recording", "mind_get_drive", "mind_attach_surrogate", "mind_mlp_create", "mind_mlp_destroy", "mind_mlp_last_error", "mind_mlp_last_ms", "mind_mlp_param_count", "mind_mlp_set_params",
     "mind_mlp_get_params", "mind_mlp_predict", "mind_mlp_gradients", "mind_mlp_set_data", "mind_mlp_train",

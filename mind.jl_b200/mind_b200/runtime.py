@@ -187,10 +187,10 @@ class DeviceState:
         abi.check(self.lib, self.handle,
                   self.lib.mind_run(self.handle, steps, recs, len(records), 1 if record_spikes else 0))
         samples = steps + 1
-        trace = np.zeros((samples, len(records)))
+        by_record = np.empty((len(records), samples))   # transposed on the device: one copy
         if records:
-            abi.check(self.lib, self.handle, self.lib.mind_get_trace(
-                self.handle, trace.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), trace.size))
+            abi.check(self.lib, self.handle, self.lib.mind_get_trace_by_record(
+                self.handle, by_record.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), by_record.size))
         n = ctypes.c_int64()
         abi.check(self.lib, self.handle, self.lib.mind_get_spikes(self.handle, None, None, 0, ctypes.byref(n)))
         times = np.zeros(n.value)
@@ -219,9 +219,8 @@ class DeviceState:
                 abi.check(self.lib, self.handle, self.lib.mind_get_macro_trace(
                     self.handle, mt.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), mt.size, ctypes.byref(samples)))
             result.macro_trace = mt
-        if records:
-            # one transposed copy; each trace is a row view of it
-            result.traces = TraceMap([r.name for r in records], np.ascontiguousarray(trace.T))
+        if records:   # each trace is a row view of the one record-major copy
+            result.traces = TraceMap([r.name for r in records], by_record)
         return result
 
     def run_stats(self) -> abi.MindRunStats:

@@ -69,7 +69,7 @@ def test_null_handles_are_refused_without_device_work():
         "mind_mlp_gradients": (None, None, None, 1, None, None), "mind_mlp_set_data": (None, None, None, 1),
         "mind_mlp_train": (None, 1, 1, ctypes.c_float(1e-3), None, None), "mind_mlp_create": (None, None),
         "mind_mechanism_count": (None,), "mind_mechanism_info": (0, None), "mind_mechanism_kind": (None, None),
-        "mind_discretize": (None, 1, 0, None, None, 0), "mind_load_mechanisms": (None, None, 0),
+        "mind_discretize": (None, 1, 0, None, None, 0), "mind_load_mechanisms": (None, None, 0), "mind_get_trace_by_record": (None, None, 0),
     }
     declared = set(declared_functions())
     for name, args in calls.items():
