@@ -197,8 +197,10 @@ function mindgpu_run!(model, stop_time::Real; records = (), record_spikes::Bool 
     recs = [c_record(spec.variable) for spec in records]
     check(h.ptr, ccall((:mind_run, libmindgpu), Cint, (Ptr{Cvoid}, Int64, Ptr{MindRecord}, Int32, Int32),
                        h.ptr, count, recs, Int32(length(recs)), Int32(record_spikes)))
-    trace = Matrix{Float64}(undef, length(recs), count + 1)   # column-major = sample-major in C
-    check(h.ptr, ccall((:mind_get_trace, libmindgpu), Cint, (Ptr{Cvoid}, Ptr{Float64}, Int64),
+    # samples x records, column-major: each record's samples contiguous, the record-major
+    # layout mind_get_trace_by_record writes (transposed on the device)
+    trace = Matrix{Float64}(undef, count + 1, length(recs))
+    check(h.ptr, ccall((:mind_get_trace_by_record, libmindgpu), Cint, (Ptr{Cvoid}, Ptr{Float64}, Int64),
                        h.ptr, trace, length(trace)))
     n = Ref{Int64}(0)
     check(h.ptr, ccall((:mind_get_spikes, libmindgpu), Cint,
@@ -208,7 +210,7 @@ function mindgpu_run!(model, stop_time::Real; records = (), record_spikes::Bool 
     check(h.ptr, ccall((:mind_get_spikes, libmindgpu), Cint,
                        (Ptr{Cvoid}, Ptr{Float64}, Ptr{Int64}, Int64, Ref{Int64}), h.ptr, times, sids, n[], n))
     time = [(step[] + k) * h.dt for k in 0:count]
-    traces = Dict(spec.name => trace[k, :] for (k, spec) in enumerate(records))
+    traces = Dict(spec.name => trace[:, k] for (k, spec) in enumerate(records))
     return (; time, traces, spike_times = times, spike_sources = sids)
 end
 
