@@ -346,14 +346,30 @@ def measure_surrogate(args, model, layout, train_ms: float = 300.0, eval_ms: flo
     judged_wall = (time.perf_counter() - t_j) * 1000.0
     state.close()
     judged_ms = sum(r.device_ms for r in judged)
+    # the same with a rotating sample: every cell attached, half of each population's sample
+    # exchanged every window (a joining cell counts from its second window)
+    state = mb.runtime.DeviceState(layout, "mixed")
+    state.attach_macro(macro)
+    state.attach_surrogate(net, np.ones(layout.n_cells, dtype=bool), scale)
+    state.set_surrogate_cells(mask)
+    state.set_surrogate_offsets(offsets)
+    state.initialize()
+    rotating, rot_log, rot_mask = surrogate.judged_run(state, layout, macro, mask, eval_ms, window_ms=20.0,
+                                                       bound=0.05, rotate=True)
+    state.close()
+    rot_ms = sum(r.device_ms for r in rotating)
     merged = type(plain)(plain.time, {}, np.concatenate([r.spike_times for r in judged]),
                          np.concatenate([r.spike_sources for r in judged]), judged_ms)
     r_judged = surrogate.region_rates(layout, merged, macro, eval_ms)
+    merged_rot = type(plain)(plain.time, {}, np.concatenate([r.spike_times for r in rotating]),
+                             np.concatenate([r.spike_sources for r in rotating]), rot_ms)
+    r_rot = surrogate.region_rates(layout, merged_rot, macro, eval_ms)
     r_plain = surrogate.region_rates(layout, plain, macro, eval_ms)
     r_sur = surrogate.region_rates(layout, sur, macro, eval_ms)
     mean_plain = r_plain.mean(axis=0)
     rel = np.abs(r_sur.mean(axis=0) - mean_plain) / np.maximum(mean_plain, 1e-9)
     rel_j = np.abs(r_judged.mean(axis=0) - mean_plain) / np.maximum(mean_plain, 1e-9)
+    rel_r = np.abs(r_rot.mean(axis=0) - mean_plain) / np.maximum(mean_plain, 1e-9)
     # counting noise of two independent runs' rate estimates per region: sqrt(2 / spikes)
     spikes_plain = mean_plain * (eval_ms * 1e-3) * np.bincount(
         surrogate.cell_regions(layout, macro)[surrogate.cell_regions(layout, macro) >= 0], minlength=macro.n_regions)
@@ -379,6 +395,11 @@ def measure_surrogate(args, model, layout, train_ms: float = 300.0, eval_ms: flo
                    "population_rate_error": {"mean_rel": float(rel_j.mean()), "max_rel": float(rel_j.max())},
                    "rule": "every 20 ms, over the run so far: |rate(surrogate) - rate(sample)| > 0.05 rate(sample)"
                            " + 3 Poisson standard errors reverts the population"},
+        "judged_rotating": {"value": units / (rot_ms / 1000.0), "speedup": plain_ms / rot_ms,
+                            "reverted": [{"t_ms": t, "regions": regs} for t, regs in rot_log],
+                            "surrogate_cells_at_end": int(rot_mask.sum()),
+                            "population_rate_error": {"mean_rel": float(rel_r.mean()), "max_rel": float(rel_r.max())},
+                            "rule": "as judged, with half of each population's sample exchanged every window"},
         "calibration": {"rounds": calibration_rounds, "ms_per_round": train_ms, "wall_s": calibration_s,
                         "target_hz": target_hz.tolist(),
                         "surrogate_hz_per_round": [np.nan_to_num(r).tolist() for r in cal_rates],

@@ -286,12 +286,20 @@ def calibrate(state, layout, macro, surrogate_cells, target_hz, t_ms: float = 10
 
 
 def judged_run(state, layout, macro, surrogate_cells, t_ms: float, window_ms: float = 20.0,
-               bound: float = 0.05, z: float = 3.0):
+               bound: float = 0.05, z: float = 3.0, rotate: bool = False, seed: int = 0):
     """Run t_ms in windows with the cable solver as judge: the cells of each population that
     stay detailed (the sample) are compared, after every window and over the run so far,
     with the population's surrogate cells (judge_populations); a population that fails is
     reverted (mind_set_surrogate_cells) and simulated from the next window on.  `state` is an
-    initialized DeviceState with the surrogate attached for `surrogate_cells`.
+    initialized DeviceState with the surrogate attached for `surrogate_cells` (for a
+    rotating sample: attached for every cell, then set to `surrogate_cells`).
+
+    rotate=True rotates the sample: after every window, half of each population's sample
+    (its longest-serving cells) returns to the surrogate and as many surrogate cells of the
+    population, drawn at random, join it, so that over a run the judge sees many more cells
+    than the sample holds at once.  A joining cell resumes from the membrane state it had
+    when it last left detailed simulation (from initialize, if never detailed), so it counts
+    toward its population's sample rate only from its second window in the sample.
     Returns (per-window results, [(time ms, reverted population indices)], final mask)."""
     mask = np.asarray(surrogate_cells, dtype=bool).copy()
     region = cell_regions(layout, macro)
@@ -306,28 +314,54 @@ def judged_run(state, layout, macro, surrogate_cells, t_ms: float, window_ms: fl
     det_count = np.zeros(n_pop)
     sur_time = np.zeros(n_pop)   # cell-seconds observed in each role
     det_time = np.zeros(n_pop)
-    results, log, done = [], [], 0
+    joined = np.full(layout.n_cells, -1)   # window a cell joined the sample (-1: from the start)
+    reverted = np.zeros(n_pop, dtype=bool)
+    rng = np.random.default_rng(seed)
+    results, log, done, w = [], [], 0, 0
     while done < total:
         k = min(steps, total - done)
         res = state.run_steps(k, [])
         results.append(res)
         seconds = k * layout.dt * 1e-3
+        counted = ~mask & (w - joined >= 1)   # sample cells past their burn-in window
         for sid in res.spike_sources:
             c = sid_cell.get(int(sid))
-            if c is not None and region[c] >= 0:
-                (sur_count if mask[c] else det_count)[region[c]] += 1.0
+            if c is None or region[c] < 0:
+                continue
+            if mask[c]:
+                sur_count[region[c]] += 1.0
+            elif counted[c]:
+                det_count[region[c]] += 1.0
         for p in range(n_pop):
             members = region == p
             sur_time[p] += seconds * np.count_nonzero(mask & members)
-            det_time[p] += seconds * np.count_nonzero(~mask & members)
+            det_time[p] += seconds * np.count_nonzero(counted & members)
         done += k
+        w += 1
         live = np.array([np.any(mask & (region == p)) for p in range(n_pop)])
         revert = live & judge_populations(sur_count, sur_time, det_count, det_time, 1.0, bound, z)
+        changed = False
         if np.any(revert):
             for p in np.nonzero(revert)[0]:
                 mask[region == p] = False
-            state.set_surrogate_cells(mask)
+            reverted |= revert
+            changed = True
             log.append((done * layout.dt, [int(p) for p in np.nonzero(revert)[0]]))
+        if rotate and done < total:
+            for p in np.nonzero(~reverted)[0]:
+                sample = np.nonzero(~mask & (region == p))[0]
+                pool = np.nonzero(mask & (region == p))[0]
+                n_out = min((len(sample) + 1) // 2, len(pool))
+                if n_out == 0:
+                    continue
+                leaving = sample[np.argsort(joined[sample], kind="stable")[:n_out]]
+                entering = rng.choice(pool, size=n_out, replace=False)
+                mask[leaving] = True
+                mask[entering] = False
+                joined[entering] = w
+                changed = True
+        if changed:
+            state.set_surrogate_cells(mask)
     return results, log, mask
 
 

@@ -170,3 +170,63 @@ def test_surrogate_offsets_shift_the_spike_probability():
         state.set_surrogate_offsets(np.full(layout.n_cells, np.inf))
     state.close()
     net.close()
+
+
+def test_rotating_judge_sample_sees_more_cells_and_still_reverts_a_failing_surrogate():
+    """judged_run(rotate=True): every cell attached to the surrogate, a 10% sample that
+    rotates by half each window.  Over the run the judge samples several times the cells
+    its sample holds at once, the run is reproducible, and a network that predicts a spike
+    in every bin is still reverted everywhere."""
+    model, macro = netcases.coupled_regions(n_regions=4, cells_per_region=50, synapses=32, seed=21)
+    layout = model.layout
+    net = surrogate.Mlp()
+    params = net.params
+    params[-1] = 20.0                       # p = 1 in every bin: a failing surrogate
+    net.params = params
+    mask = np.ones(layout.n_cells, dtype=bool)
+    mask[::10] = False
+    outs = []
+    for _ in range(2):
+        state = mb.runtime.DeviceState(layout)
+        state.attach_macro(macro)
+        state.attach_surrogate(net, np.ones(layout.n_cells, dtype=bool), 1.0)
+        state.set_surrogate_cells(mask)
+        state.initialize()
+        results, log, final = surrogate.judged_run(state, layout, macro, mask, 100.0, window_ms=10.0,
+                                                   rotate=True, seed=3)
+        outs.append((np.concatenate([r.spike_times for r in results]), log, final))
+        state.close()
+    (t0, log0, final0), (t1, log1, final1) = outs
+    np.testing.assert_array_equal(t0, t1)
+    assert log0 == log1 and log0 and sorted(sum((regs for _, regs in log0), [])) == [0, 1, 2, 3]
+    assert not final0.any()
+
+    # a sane network: the rotation moves the sample through the populations
+    net2 = surrogate.Mlp(seed=5)
+    p2 = net2.params
+    p2[-1] = -3.0
+    net2.params = p2
+    state = mb.runtime.DeviceState(layout)
+    state.attach_macro(macro)
+    state.attach_surrogate(net2, np.ones(layout.n_cells, dtype=bool), 1.0)
+    state.set_surrogate_cells(mask)
+    state.initialize()
+    masks = []
+    real = state.set_surrogate_cells
+
+    def spy(m):
+        masks.append(np.asarray(m, dtype=bool).copy())
+        real(m)
+
+    state.set_surrogate_cells = spy
+    results, log, final = surrogate.judged_run(state, layout, macro, mask, 60.0, window_ms=10.0, rotate=True,
+                                               bound=10.0, z=50.0)
+    sampled = np.zeros(layout.n_cells, dtype=bool)
+    for m in [mask] + masks:
+        sampled |= ~m
+    assert len(masks) >= 4
+    assert sampled.sum() >= 2.5 * (~mask).sum()
+    assert all(int((~m).sum()) == int((~mask).sum()) for m in masks)   # the sample keeps its size
+    state.close()
+    net.close()
+    net2.close()
