@@ -47,6 +47,11 @@ constexpr int kCellThreads = 128;  // window kernel: one cell per CTA of four wa
 // A 128-thread window launch whose cells need little shared memory can keep more CTAs per SM
 // than its registers allow at the default bound (5): the tight variant is compiled for 7.
 constexpr int kTightBlocks = 7;
+// CTAs per SM a launch shape is compiled for by default (its __launch_bounds__): 5 at 128
+// threads per cell, 10 at 64, 16 at one warp.
+constexpr int default_min_blocks(int threads) {
+    return threads == kCellThreads ? 5 : threads == kCellThreads / 2 ? 10 : 16;
+}
 constexpr int kSurrogateRing = 21;  // drive bins kept for the surrogate: the last 20 and the current
 
 

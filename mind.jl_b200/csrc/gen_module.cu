@@ -15,22 +15,22 @@
 
 extern "C" {
 
-__global__ void __launch_bounds__(mind::kCellThreads, 5)
+__global__ void __launch_bounds__(mind::kCellThreads, mind::default_min_blocks(mind::kCellThreads))
     mind_rt_window_fp64(const mind::Params P, const int32_t *cells, int64_t n0, int32_t W) {
     mind::window_body<false, mind::kCellThreads, false, true>(P, cells, n0, W);
 }
 
-__global__ void __launch_bounds__(mind::kCellThreads, 5)
+__global__ void __launch_bounds__(mind::kCellThreads, mind::default_min_blocks(mind::kCellThreads))
     mind_rt_window_mixed(const mind::Params P, const int32_t *cells, int64_t n0, int32_t W) {
     mind::window_body<true, mind::kCellThreads, false, true>(P, cells, n0, W);
 }
 
-__global__ void __launch_bounds__(mind::kCellThreads, 5)
+__global__ void __launch_bounds__(mind::kCellThreads, mind::default_min_blocks(mind::kCellThreads))
     mind_rt_window_fp64_hbm(const mind::Params P, const int32_t *cells, int64_t n0, int32_t W) {
     mind::window_body<false, mind::kCellThreads, true, true>(P, cells, n0, W);
 }
 
-__global__ void __launch_bounds__(mind::kCellThreads, 5)
+__global__ void __launch_bounds__(mind::kCellThreads, mind::default_min_blocks(mind::kCellThreads))
     mind_rt_window_mixed_hbm(const mind::Params P, const int32_t *cells, int64_t n0, int32_t W) {
     mind::window_body<true, mind::kCellThreads, true, true>(P, cells, n0, W);
 }

@@ -1236,7 +1236,7 @@ __device__ __forceinline__ void window_body(const Params &P, const int32_t *cell
 }
 
 template <bool MIXED, int NT, bool GLOBAL_IMAGE = false, bool GEN = false,
-          int MINB = NT == kCellThreads ? 5 : NT == kCellThreads / 2 ? 10 : 16>
+          int MINB = default_min_blocks(NT)>
 __global__ void __launch_bounds__(NT, MINB) window_kernel(const Params P, const int32_t *cells, int64_t n0,
                                                            int32_t W) {
     window_body<MIXED, NT, GLOBAL_IMAGE, GEN>(P, cells, n0, W);

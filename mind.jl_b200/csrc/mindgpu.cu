@@ -410,7 +410,7 @@ int launch_grid(int64_t work) {
 }
 
 /* The window kernel's launch shapes: 128 threads per cell (kCellThreads), 64, or one warp. */
-template <int NT, int MINB = NT == kCellThreads ? 5 : NT == kCellThreads / 2 ? 10 : 16>
+template <int NT, int MINB = default_min_blocks(NT)>
 cudaError_t set_window_smem(int bytes) {
     cudaError_t e = cudaFuncSetAttribute(window_kernel<false, NT, false, false, MINB>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);

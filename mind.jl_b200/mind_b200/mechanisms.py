@@ -225,7 +225,15 @@ def mechanism_module(irs, first_id: int) -> str:
     header = runtime_header(irs, first_id)
     package = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     csrc = os.path.join(package, "csrc")
-    out_dir = os.path.join(package, "lib", "mechanisms", hashlib.sha256(header.encode()).hexdigest()[:16])
+    # The key covers the kernel sources the module is compiled from, not only the emitted
+    # header: a module built from other sources than the library's could disagree with it on
+    # the launch parameters' layout.
+    key = hashlib.sha256(header.encode())
+    sources = sorted(f for f in os.listdir(csrc) if f.endswith((".cu", ".cuh", ".h")))
+    for path in [os.path.join(csrc, f) for f in sources] + [os.path.join(package, "..", "include", "mindgpu.h")]:
+        with open(path, "rb") as f:
+            key.update(os.path.basename(path).encode() + b"\0" + f.read())
+    out_dir = os.path.join(package, "lib", "mechanisms", key.hexdigest()[:16])
     module = os.path.join(out_dir, "module.cubin")
     if not os.path.exists(module):
         os.makedirs(out_dir, exist_ok=True)
