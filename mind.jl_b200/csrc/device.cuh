@@ -146,13 +146,13 @@ __host__ __device__ inline int staged_doubles(int32_t kind) {
  *            slots of the staged rows;
  *   events   the cell's inbox for the window [inbox_cap];
  *   ints     per staged row: local node; chain top, length,
- *            parent, child-chain CSR; level starts; inbox order; the
- *            threads' row ranges per group [ngroups][threads + 1];
+ *            parent, child-chain CSR; level starts; path starts; inbox
+ *            order; the threads' row ranges per group [ngroups][threads + 1];
  *   shorts   chain of every node [n].
  * Host (to size the launch) and device (to carve the buffer) use this one function.
  */
 struct CellShape {
-    int32_t n, nch, nkids, nlev;
+    int32_t n, nch, nkids, nlev, npath;
     int32_t rows[kMaxGroups];
 };
 
@@ -165,7 +165,7 @@ __host__ __device__ inline size_t cell_smem_bytes(const CellShape &s, const int3
         doubles += (size_t)staged_doubles(kinds[g]) * s.rows[g];
         ints += (size_t)s.rows[g];
     }
-    ints += 4 * (size_t)s.nch + 1 + (size_t)s.nkids + (size_t)s.nlev + 1 + (size_t)inbox_cap;
+    ints += 4 * (size_t)s.nch + 1 + (size_t)s.nkids + (size_t)s.nlev + 1 + (size_t)s.npath + 1 + (size_t)inbox_cap;
     ints += (size_t)ngroups * (kCellThreads + 1);
     return doubles * 8 + (size_t)inbox_cap * sizeof(InboxEvent) + ints * 4 + 2 * (size_t)s.n;
 }
@@ -189,8 +189,13 @@ struct Params {
     // chains
     const int32_t *chain_off;  // [ncells+1]
     const int32_t *chain_top, *chain_len, *chain_par, *chain_kid_off, *chain_kids;  // chain_kid_off global CSR
-    const int32_t *level_off;    // [ncells+1] into level_chain
-    const int32_t *level_chain;  // per cell: nlevels+1 local chain starts (chains sorted by level)
+    // paths: a chain, or a chain and the child chains it continues into, eliminated by one
+    // thread in one level (chains of a path contiguous, deepest first; paths sorted by level)
+    const int32_t *level_off;    // [ncells+1] into level_path
+    const int32_t *level_path;   // per cell: nlevels+1 local path starts
+    const int32_t *path_off;     // [ncells+1] into path_chain
+    const int32_t *path_chain;   // per cell: npaths+1 local chain starts; only the sentinel for a
+                                 // cell on the chain schedule (its paths are its chains)
     DevGroup groups[kMaxGroups];
     // per cell, group and thread: first row (relative to the cell's first row of the group)
     // of the thread's rows; thread t owns the local nodes i with i % kCellThreads == t

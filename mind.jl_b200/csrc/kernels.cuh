@@ -488,19 +488,25 @@ __device__ __forceinline__ void apply_event(const StagedGroup &G, int32_t row, d
 /*
  * Hines solve of one resident cell, FP64 mode: the reference's operations in the
  * canonical order (gather-form elimination, f = a/D, back-substitution (R + a x_p)/D).
- * Level by level, one chain per thread; along a chain only subtract -> divide ->
- * multiply stays on the dependency chain, the next node's operands being loaded
- * before the current division.
+ * Level by level, one path per thread (a path is one chain, or a chain and the child chains
+ * it continues when the cell's plan merged them): a path's chains are eliminated deepest
+ * first and back-substituted in the reverse order, each child chain ready before its parent
+ * (on the path, by the same thread; off it, in a lower level).  Along a chain only subtract
+ * -> divide -> multiply stays on the dependency chain, the next node's operands being
+ * loaded before the current division.  pch null: the cell's paths are its chains (lvp holds
+ * chain starts), the loops are the one-chain-per-thread loops.
  */
 template <int NT>
 __device__ __forceinline__ void hines_exact(double *sd, double *sr, const double *sa, double *sv, double *sxd,
                                             double *sxr, const int32_t *ctop, const int32_t *clen,
                                             const int32_t *cpar, const int32_t *ckoff, const int32_t *ckids,
-                                            const int32_t *lvc, int32_t nlev, double vscale, bool &singular) {
+                                            const int32_t *lvp, const int32_t *pch, int32_t nlev, double vscale,
+                                            bool &singular) {
     constexpr int32_t T = NT;
     const int32_t tid = threadIdx.x;
     for (int32_t lv = 0; lv < nlev; ++lv) {
-        for (int32_t ch = lvc[lv] + tid; ch < lvc[lv + 1]; ch += T) {
+        for (int32_t p = lvp[lv] + tid; p < lvp[lv + 1]; p += T)
+        for (int32_t ch = pch ? pch[p] : p, end = pch ? pch[p + 1] : p + 1; ch < end; ++ch) {
             const int32_t top = ctop[ch];
             const int32_t bottom = top + clen[ch] - 1;
             const bool rooted = cpar[ch] < 0;
@@ -557,7 +563,8 @@ __device__ __forceinline__ void hines_exact(double *sd, double *sr, const double
         __syncthreads();
     }
     for (int32_t lv = nlev - 1; lv >= 0; --lv) {
-        for (int32_t ch = lvc[lv] + tid; ch < lvc[lv + 1]; ch += T) {
+        for (int32_t p = lvp[lv] + tid; p < lvp[lv + 1]; p += T)
+        for (int32_t ch = (pch ? pch[p + 1] : p + 1) - 1, first = pch ? pch[p] : p; ch >= first; --ch) {
             const int32_t top = ctop[ch];
             const int32_t bottom = top + clen[ch] - 1;
             const int32_t par = cpar[ch];
@@ -595,17 +602,19 @@ __device__ __forceinline__ void hines_exact(double *sd, double *sr, const double
  * Hines solve, mixed mode: FP64 arithmetic with reciprocals.  Elimination keeps, per
  * node, f = a/D in place of D and R/D in place of R, so the back-substitution is one
  * FMA per node, x = f x_p + R/D; the pivot chain is D -> 1/D -> (a^2)(1/D) -> next D.
- * One chain per thread, level by level.
+ * One path per thread, level by level, as in the FP64 solve.
  */
 template <int NT>
 __device__ __forceinline__ void hines_mixed(double *sd, double *sr, const double *sa, double *sv, double *sxd,
                                             double *sxr, const int32_t *ctop, const int32_t *clen,
                                             const int32_t *cpar, const int32_t *ckoff, const int32_t *ckids,
-                                            const int32_t *lvc, int32_t nlev, double vscale, bool &singular) {
+                                            const int32_t *lvp, const int32_t *pch, int32_t nlev, double vscale,
+                                            bool &singular) {
     constexpr int32_t T = NT;
     const int32_t tid = threadIdx.x;
     for (int32_t lv = 0; lv < nlev; ++lv) {
-        for (int32_t ch = lvc[lv] + tid; ch < lvc[lv + 1]; ch += T) {
+        for (int32_t p = lvp[lv] + tid; p < lvp[lv + 1]; p += T)
+        for (int32_t ch = pch ? pch[p] : p, end = pch ? pch[p + 1] : p + 1; ch < end; ++ch) {
             const int32_t top = ctop[ch];
             const int32_t bottom = top + clen[ch] - 1;
             const bool rooted = cpar[ch] < 0;
@@ -658,7 +667,8 @@ __device__ __forceinline__ void hines_mixed(double *sd, double *sr, const double
         __syncthreads();
     }
     for (int32_t lv = nlev - 1; lv >= 0; --lv) {
-        for (int32_t ch = lvc[lv] + tid; ch < lvc[lv + 1]; ch += T) {
+        for (int32_t p = lvp[lv] + tid; p < lvp[lv + 1]; p += T)
+        for (int32_t ch = (pch ? pch[p + 1] : p + 1) - 1, first = pch ? pch[p] : p; ch >= first; --ch) {
             const int32_t top = ctop[ch];
             const int32_t bottom = top + clen[ch] - 1;
             const int32_t par = cpar[ch];
@@ -693,11 +703,13 @@ __device__ __forceinline__ void hines_mixed(double *sd, double *sr, const double
  * events.  Parameter-only data (pas rows, synapse constants, IClamp rows,
  * C/dt, axial_diagonal) is streamed from HBM each step with coalesced loads.
  *
- * The Hines solve runs level by level (a chain's level exceeds its children's),
- * one chain per thread; along a chain only subtract -> divide -> multiply stays
- * on the dependency chain, the next node's operands being loaded ahead.
+ * The Hines solve runs level by level, one path per thread (a chain, or on cells the plan
+ * gave paths a chain and the child chains it continues); along a chain only subtract ->
+ * divide -> multiply stays on the dependency chain, the next node's operands being loaded
+ * ahead.  PATHS false compiles the one-chain-per-thread loops only, for launches whose
+ * cells all have the chain schedule.
  */
-template <bool MIXED, int NT, bool GLOBAL_IMAGE = false, bool GEN = false>
+template <bool MIXED, int NT, bool GLOBAL_IMAGE = false, bool GEN = false, bool PATHS = true>
 __device__ __forceinline__ void window_body(const Params &P, const int32_t *cells, int64_t n0, int32_t W) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ StagedGroup sg[kMaxGroups];
@@ -714,6 +726,8 @@ __device__ __forceinline__ void window_body(const Params &P, const int32_t *cell
     const int32_t nkids = P.chain_kid_off[cb + nch] - kb;
     const int32_t lv0 = P.level_off[c];
     const int32_t nlev = P.level_off[c + 1] - lv0 - 1;
+    const int32_t pb = P.path_off[c];
+    const int32_t npath = P.path_off[c + 1] - pb - 1;
 
     // ---- carve the cell image (order fixed by cell_smem_bytes): shared memory, or for a
     //      cell larger than one CTA's shared memory its own slot of an HBM buffer ----
@@ -753,7 +767,8 @@ __device__ __forceinline__ void window_body(const Params &P, const int32_t *cell
     int32_t *cpar = ip; ip += nch;
     int32_t *ckoff = ip; ip += nch + 1;
     int32_t *ckids = ip; ip += nkids;
-    int32_t *lvc = ip; ip += nlev + 1;
+    int32_t *lvp = ip; ip += nlev + 1;
+    int32_t *pch = ip; ip += npath + 1;
     int32_t *sorder = ip; ip += P.inbox_cap;
     int32_t *spart = ip; ip += P.ngroups * (O + 1);   // the threads' row ranges per group
     int16_t *chain_of = reinterpret_cast<int16_t *>(ip);
@@ -820,7 +835,8 @@ __device__ __forceinline__ void window_body(const Params &P, const int32_t *cell
     }
     if (tid == 0) ckoff[nch] = nkids;
     for (int32_t k = tid; k < nkids; k += T) ckids[k] = P.chain_kids[kb + k];
-    for (int32_t k = tid; k <= nlev; k += T) lvc[k] = P.level_chain[lv0 + k];
+    for (int32_t k = tid; k <= nlev; k += T) lvp[k] = P.level_path[lv0 + k];
+    for (int32_t k = tid; k <= npath; k += T) pch[k] = P.path_chain[pb + k];
     for (int32_t k = tid; k < P.ngroups * (O + 1); k += T) spart[k] = P.part[(int64_t)c * P.ngroups * (O + 1) + k];
     __syncthreads();
     for (int32_t k = tid; k < nch; k += T)
@@ -1102,9 +1118,11 @@ __device__ __forceinline__ void window_body(const Params &P, const int32_t *cell
         // 6-7. Hines elimination level by level, each chain bottom to top into its parent,
         //      then back-substitution root chain first with the voltage update.
         if (MIXED) {
-            hines_mixed<NT>(sd, sr, sa, sv, sxd, sxr, ctop, clen, cpar, ckoff, ckids, lvc, nlev, P.vscale, singular);
+            hines_mixed<NT>(sd, sr, sa, sv, sxd, sxr, ctop, clen, cpar, ckoff, ckids, lvp,
+                          PATHS && npath ? pch : nullptr, nlev, P.vscale, singular);
         } else {
-            hines_exact<NT>(sd, sr, sa, sv, sxd, sxr, ctop, clen, cpar, ckoff, ckids, lvc, nlev, P.vscale, singular);
+            hines_exact<NT>(sd, sr, sa, sv, sxd, sxr, ctop, clen, cpar, ckoff, ckids, lvp,
+                          PATHS && npath ? pch : nullptr, nlev, P.vscale, singular);
         }
 
         // 8. cnexp state advance on the new voltage (time t + dt).
@@ -1236,10 +1254,10 @@ __device__ __forceinline__ void window_body(const Params &P, const int32_t *cell
 }
 
 template <bool MIXED, int NT, bool GLOBAL_IMAGE = false, bool GEN = false,
-          int MINB = default_min_blocks(NT)>
+          int MINB = default_min_blocks(NT), bool PATHS = true>
 __global__ void __launch_bounds__(NT, MINB) window_kernel(const Params P, const int32_t *cells, int64_t n0,
                                                            int32_t W) {
-    window_body<MIXED, NT, GLOBAL_IMAGE, GEN>(P, cells, n0, W);
+    window_body<MIXED, NT, GLOBAL_IMAGE, GEN, PATHS>(P, cells, n0, W);
 }
 
 /* dst [records x samples] = src [samples x records], through 32 x 32 shared-memory tiles

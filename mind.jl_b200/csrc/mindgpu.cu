@@ -173,6 +173,7 @@ struct MindHandle {
         bool tight = false;               // 128 threads, compiled for kTightBlocks CTAs per SM
         int32_t max_detectors = 0;        // most threshold detectors on one of its cells
         bool global_image = false;        // cells too large for shared memory: image in HBM
+        bool paths = false;               // some cell has the path schedule of the solve
     };
     std::vector<Bin> bins;           // cells grouped by shared-memory need
     std::vector<cudaStream_t> bin_streams;   // size bins run concurrently
@@ -409,13 +410,14 @@ int launch_grid(int64_t work) {
     return (int)blocks;
 }
 
-/* The window kernel's launch shapes: 128 threads per cell (kCellThreads), 64, or one warp. */
-template <int NT, int MINB = default_min_blocks(NT)>
+/* The window kernel's launch shapes: 128 threads per cell (kCellThreads), 64, or one warp;
+ * the 128-thread shapes also without the path schedule (PATHS false). */
+template <int NT, int MINB = default_min_blocks(NT), bool PATHS = true>
 cudaError_t set_window_smem(int bytes) {
-    cudaError_t e = cudaFuncSetAttribute(window_kernel<false, NT, false, false, MINB>,
+    cudaError_t e = cudaFuncSetAttribute(window_kernel<false, NT, false, false, MINB, PATHS>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(window_kernel<true, NT, false, false, MINB>,
+        e = cudaFuncSetAttribute(window_kernel<true, NT, false, false, MINB, PATHS>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     return e;
 }
@@ -465,8 +467,61 @@ int create(const MindLayout *L, MindHandle *h) {
     layout_of_packed.reserve(n);
     std::vector<int32_t> cell_of(n, -1);
     std::vector<int32_t> chain_off{0}, chain_top, chain_len, chain_par, chain_kid_off{0}, chain_kids;
-    std::vector<int32_t> level_off{0}, level_chain;
+    std::vector<int32_t> level_off{0}, level_path, path_off{0}, path_chain;
     h->packed_of_layout.assign(n, -1);
+    // Two schedules of the solve; every chain's arithmetic is the same in both.  Levels per
+    // node, carried from a chain's bottom to its top (a node with one child is inside a chain):
+    //  chains (chain_level): a chain runs one level above its highest child chain, one chain
+    //          per thread;
+    //  paths (path_level): a chain continues the path of the child chain that finishes last,
+    //          when that child is unique, so one thread eliminates both in the same level and
+    //          the chain adds no level; otherwise (a leaf, or a tie) it starts a path one level
+    //          above its children.
+    // Cells take paths when paths cut their levels at least fourfold (pyramidal trees, a long
+    // trunk with side branches: 16 levels -> 2) and such cells hold at least half of the
+    // network's nodes; on bushy random trees (11 -> 4.5 levels) the chain schedule measured
+    // faster at full occupancy, and a network of them keeps the chain-only kernels.
+    std::vector<int32_t> chain_level(n, 0), path_level(n, 0);
+    std::vector<char> path_cell(n, 0);   // by root
+    bool network_paths = false;
+    {
+        int64_t path_nodes = 0;
+        std::vector<int32_t> bfs;
+        for (int64_t root = 0; root < n; ++root) {
+            if (parent[root] >= 0) continue;
+            bfs.assign(1, (int32_t)root);
+            for (size_t k = 0; k < bfs.size(); ++k)
+                for (int64_t c = child_off[bfs[k]]; c < child_off[bfs[k] + 1]; ++c) bfs.push_back(child[c]);
+            for (size_t k = bfs.size(); k-- > 0;) {
+                const int32_t i = bfs[k];
+                const int64_t kids = child_off[i + 1] - child_off[i];
+                if (kids == 1) {
+                    chain_level[i] = chain_level[child[child_off[i]]];
+                    path_level[i] = path_level[child[child_off[i]]];
+                } else if (kids > 1) {
+                    int32_t cl = 0, last = -1, ties = 0;
+                    for (int64_t c = child_off[i]; c < child_off[i + 1]; ++c) {
+                        const int32_t j = child[c];
+                        cl = std::max(cl, chain_level[j] + 1);
+                        if (path_level[j] > last) {
+                            last = path_level[j];
+                            ties = 1;
+                        } else if (path_level[j] == last) {
+                            ++ties;
+                        }
+                    }
+                    chain_level[i] = cl;
+                    path_level[i] = ties == 1 ? last : last + 1;
+                }
+            }
+            if (chain_level[root] + 1 >= 4 * (path_level[root] + 1)) {
+                path_cell[root] = 1;
+                path_nodes += (int64_t)bfs.size();
+            }
+        }
+        network_paths = 2 * path_nodes >= n;
+    }
+    std::vector<char> cell_paths;   // by cell: the path schedule
     for (int64_t root = 0; root < n; ++root) {
         if (parent[root] >= 0) continue;
         const int32_t cell = (int32_t)(node_off.size() - 1);
@@ -501,18 +556,49 @@ int create(const MindLayout *L, MindHandle *h) {
             auto it = std::lower_bound(top_id.begin(), top_id.end(), std::make_pair(top, INT32_MIN));
             return it->second;
         };
-        // levels: children chains first (tops in reverse BFS order are processed after their subtrees)
-        std::vector<int32_t> level(tops.size(), 0);
-        for (size_t k = tops.size(); k-- > 0;) {
-            int32_t bottom = chains[k].back();
-            int32_t lv = 0;
+        // levels of the cell's schedule; on paths, the child chain a chain continues is its
+        // one child chain of the same path level
+        const bool use_paths = network_paths && path_cell[root];
+        cell_paths.push_back(use_paths ? 1 : 0);
+        std::vector<int32_t> level(tops.size(), 0), below(tops.size(), -1);
+        for (size_t k = 0; k < tops.size(); ++k) {
+            level[k] = use_paths ? path_level[tops[k]] : chain_level[tops[k]];
+            if (!use_paths) continue;
+            const int32_t bottom = chains[k].back();
             for (int64_t c = child_off[bottom]; c < child_off[bottom + 1]; ++c)
-                lv = std::max(lv, level[chain_id_of(child[c])] + 1);
-            level[k] = lv;
+                if (path_level[child[c]] == level[k]) below[k] = chain_id_of(child[c]);
         }
-        std::vector<int32_t> order(tops.size());
-        for (size_t k = 0; k < order.size(); ++k) order[k] = (int32_t)k;
-        std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) { return level[x] < level[y]; });
+        // a path is named by its head, the chain that no parent chain continues; its chains
+        // are listed deepest first (the elimination order)
+        std::vector<char> continued(tops.size(), 0);
+        for (size_t k = 0; k < tops.size(); ++k)
+            if (below[k] >= 0) continued[below[k]] = 1;
+        std::vector<std::vector<int32_t>> paths;
+        std::vector<int64_t> path_nodes;
+        for (size_t k = 0; k < tops.size(); ++k) {
+            if (continued[k]) continue;
+            std::vector<int32_t> path;
+            int64_t nodes = 0;
+            for (int32_t q = (int32_t)k; q >= 0; q = below[q]) {
+                path.push_back(q);
+                nodes += (int64_t)chains[q].size();
+            }
+            std::reverse(path.begin(), path.end());
+            paths.push_back(std::move(path));
+            path_nodes.push_back(nodes);
+        }
+        // paths by level (chains: in BFS order within a level; paths: the longest first, as the
+        // threads take them in turn)
+        std::vector<int32_t> porder(paths.size());
+        for (size_t p = 0; p < porder.size(); ++p) porder[p] = (int32_t)p;
+        std::stable_sort(porder.begin(), porder.end(), [&](int32_t x, int32_t y) {
+            const int32_t lx = level[paths[x].front()], ly = level[paths[y].front()];
+            return lx != ly ? lx < ly : use_paths && path_nodes[x] > path_nodes[y];
+        });
+        std::vector<int32_t> order;   // chains: the paths in that order, each deepest first
+        order.reserve(tops.size());
+        for (int32_t p : porder)
+            for (int32_t q : paths[p]) order.push_back(q);
         std::vector<int32_t> rank(tops.size());
         for (size_t k = 0; k < order.size(); ++k) rank[order[k]] = (int32_t)k;
         // packed order: chains by rank, nodes top -> bottom
@@ -542,11 +628,22 @@ int create(const MindLayout *L, MindHandle *h) {
         chain_off.push_back((int32_t)chain_top.size());
         int32_t nlev = 0;
         for (int32_t lv : level) nlev = std::max(nlev, lv + 1);
+        const int32_t npaths = (int32_t)porder.size();
         for (int32_t lv = 0, k = 0; lv <= nlev; ++lv) {
-            while (k < (int32_t)order.size() && level[order[k]] < lv) ++k;
-            level_chain.push_back(k);
+            while (k < npaths && level[paths[porder[k]].front()] < lv) ++k;
+            level_path.push_back(k);
         }
-        level_off.push_back((int32_t)level_chain.size());
+        level_off.push_back((int32_t)level_path.size());
+        // a cell on the chain schedule keeps only the sentinel: its paths are its chains, and
+        // level_path holds chain starts
+        int32_t first_chain = 0;
+        if (use_paths)
+            for (int32_t p : porder) {
+                path_chain.push_back(first_chain);
+                first_chain += (int32_t)paths[p].size();
+            }
+        path_chain.push_back(first_chain);
+        path_off.push_back((int32_t)path_chain.size());
     }
     if ((int64_t)layout_of_packed.size() != n) return fail(h, MIND_ELAYOUT, "parent links form a cycle");
     const int32_t ncells = (int32_t)(node_off.size() - 1);
@@ -823,7 +920,9 @@ int create(const MindLayout *L, MindHandle *h) {
     P.chain_kid_off = h->upload(chain_kid_off);
     P.chain_kids = h->upload(chain_kids);
     P.level_off = h->upload(level_off);
-    P.level_chain = h->upload(level_chain);
+    P.level_path = h->upload(level_path);
+    P.path_off = h->upload(path_off);
+    P.path_chain = h->upload(path_chain);
     P.part = h->upload(part);
     P.det_off = h->upload(det_off);
     P.det_node = h->upload(det_node);
@@ -895,6 +994,7 @@ int create(const MindLayout *L, MindHandle *h) {
             return fail(h, MIND_ELAYOUT, "a cell has more than 32767 unbranched chains");
         shape.nkids = chain_kid_off[chain_off[c + 1]] - chain_kid_off[chain_off[c]];
         shape.nlev = level_off[c + 1] - level_off[c] - 1;
+        shape.npath = path_off[c + 1] - path_off[c] - 1;
         for (int32_t g = 0; g < L->n_mechanisms; ++g) shape.rows[g] = group_row_off[g][c + 1] - group_row_off[g][c];
         const size_t bytes = cell_smem_bytes(shape, kinds.data(), L->n_mechanisms, P.inbox_cap);
         need[c] = {bytes, c};
@@ -928,8 +1028,10 @@ int create(const MindLayout *L, MindHandle *h) {
         bin.global_image = big;
         bin.tight = !big && tight_by_default(top);
         if (!big) worst_smem = std::max(worst_smem, top);
-        for (size_t q = first; q < k; ++q)
+        for (size_t q = first; q < k; ++q) {
             bin.max_detectors = std::max(bin.max_detectors, det_off[need[q].second + 1] - det_off[need[q].second]);
+            bin.paths = bin.paths || cell_paths[need[q].second];
+        }
         h->bins.push_back(bin);
     }
     for (auto &x : need) bin_cells.push_back(x.second);
@@ -948,6 +1050,8 @@ int create(const MindLayout *L, MindHandle *h) {
     }
     CUDA_TRY(h, set_window_smem<kCellThreads>(smem_attr));
     CUDA_TRY(h, (set_window_smem<kCellThreads, kTightBlocks>(smem_attr)));
+    CUDA_TRY(h, (set_window_smem<kCellThreads, default_min_blocks(kCellThreads), false>(smem_attr)));
+    CUDA_TRY(h, (set_window_smem<kCellThreads, kTightBlocks, false>(smem_attr)));
     CUDA_TRY(h, cudaFuncSetAttribute(window_kernel<false, kCellThreads, false, true>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr));
     CUDA_TRY(h, cudaFuncSetAttribute(window_kernel<true, kCellThreads, false, true>,
@@ -1216,10 +1320,15 @@ void launch_window(const MindHandle *h, const MindHandle::Bin &bin, cudaStream_t
             window_kernel<MIXED, T, false, true><<<bin.count, T, smem, s>>>(P, cells, n0, W);
     } else if (bin.global_image)
         window_kernel<MIXED, T, true><<<bin.count, T, 0, s>>>(P, cells, n0, W);
-    else if (bin.threads == T && bin.tight)
+    else if (bin.threads == T && bin.tight && bin.paths)
         window_kernel<MIXED, T, false, false, kTightBlocks><<<bin.count, T, smem, s>>>(P, cells, n0, W);
-    else if (bin.threads == T)
+    else if (bin.threads == T && bin.tight)
+        window_kernel<MIXED, T, false, false, kTightBlocks, false><<<bin.count, T, smem, s>>>(P, cells, n0, W);
+    else if (bin.threads == T && bin.paths)
         window_kernel<MIXED, T><<<bin.count, T, smem, s>>>(P, cells, n0, W);
+    else if (bin.threads == T)
+        window_kernel<MIXED, T, false, false, default_min_blocks(T), false><<<bin.count, T, smem, s>>>(P, cells, n0,
+                                                                                                       W);
     else if (bin.threads == T / 2)
         window_kernel<MIXED, T / 2><<<bin.count, T / 2, smem, s>>>(P, cells, n0, W);
     else
