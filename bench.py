@@ -56,7 +56,8 @@ def parse():
     p.add_argument("--cells", type=int, default=None, help="cells (default: the configuration's count)")
     p.add_argument("--config", type=int, default=2, choices=[2, 3, 4, 5],
                    help="2: 10,000 uneven binary-tree cells (the headline); 3: 1,000 pyramidal-like cells; "
-                        "4: 2,000 pyramidal-like cells coupled to 20 Jansen-Rit regions")
+                        "4: 2,000 pyramidal-like cells coupled to 20 Jansen-Rit regions; 5 (with --surrogate): "
+                        "100,000 config-4 cells in 200 populations")
     p.add_argument("--no-autotune", action="store_true",
                    help="keep 128 threads per cell in every size bin instead of timing the shapes")
     p.add_argument("--precision", default="both", choices=["fp64", "mixed", "both"],
