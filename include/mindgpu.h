@@ -310,8 +310,9 @@ int mind_window_steps(const MindHandle *h, int32_t *steps);
  * words of Philox4x32-10 on counter (k low, k high, input index, 0x4D4D), key = seed,
  * mapped to (w + 1)/(2^32 + 1); they then follow the source's NetCons.
  * dt_macro must be a multiple of dt and bin_ms a multiple of dt_macro; the library's
- * window becomes a divisor of the bin that is a multiple of the macro step, so bins are
- * complete before the regions read them.
+ * window becomes a multiple of the macro step no longer than the bin, and every window
+ * ends at the next bin boundary at the latest, so bins are complete before the regions
+ * read them.
  */
 typedef struct {
     int32_t n_regions;

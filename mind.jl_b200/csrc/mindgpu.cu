@@ -1373,9 +1373,9 @@ int advance(MindHandle *h, int64_t steps, bool record_spikes) {
     }
     while (n0 < end) {
         int32_t W = (int32_t)std::min<int64_t>(h->window, end - n0);
-        // With regions attached, windows stay inside multiples of the window length (a
-        // divisor of the rate bin), so a bin is complete before the regions read it.
-        if (M.n > 0) W = (int32_t)std::min<int64_t>(W, h->window - n0 % h->window);
+        // With regions attached, a window ends at the next rate-bin boundary at the latest,
+        // so every bin the regions read is complete.
+        if (M.n > 0) W = (int32_t)std::min<int64_t>(W, h->bin_steps - n0 % h->bin_steps);
         // NetStim self-events through the window's end boundary, as the reference's delivery
         // at the end of every step (time <= t + dt, src/runtime/step.jl:148): their spikes
         // enter this run's raster, their NetCon events the next window's bins
@@ -1693,10 +1693,10 @@ int mind_attach_macro(MindHandle *h, const MindMacroLayout *L) {
         if (h->source_detector[s] || (h->source_external[s] && !is_input[s]))
             for (int64_t e = h->fanout[s]; e < h->fanout[s + 1]; ++e) min_delay = std::min(min_delay, h->edge_delay[e]);
     const int32_t base_window = window_for_delay(min_delay, h->dt);
-    // the window: the longest divisor of the bin that is a multiple of the macro step
-    int32_t window = 0;
-    for (int32_t w = spm; w <= std::min(base_window, bin_steps); w += spm)
-        if (bin_steps % w == 0) window = w;
+    // the window: the longest multiple of the macro step within the delay bound and the bin;
+    // advance() also ends a window at every bin boundary, so none straddles one (config 4:
+    // windows of 16, 16 and 8 steps per 40-step bin)
+    const int32_t window = std::min(base_window, bin_steps) / spm * spm;
     if (window == 0)
         return fail(h, MIND_ELAYOUT, "the shortest NetCon delay out of a cell is shorter than a macro step");
     std::vector<int32_t> order(L->n_edges), in_off(n + 1, 0), e_src, e_delay;
