@@ -59,12 +59,13 @@ def soma_nodes(layout):
     return [layout.voltage_node(c) for c in range(1, layout.n_cells + 1)]
 
 
-def coupled_regions(n_regions=3, cells_per_region=4, synapses=8, seed=11, input_scale=300.0):
+def coupled_regions(n_regions=3, cells_per_region=4, synapses=8, seed=11, input_scale=300.0, min_cell_delay=0.6):
     """Ball-and-stick populations coupled to Jansen-Rit regions (config 4 in miniature).
 
     Every synapse (Exp2Syn) gets its own external spike input driven by its population's
     region; every cell's soma detector feeds the region's rate bin; regions are coupled by
-    random edges with delays of 1-5 macro steps; recurrent NetCons between cells (0.6-2 ms).
+    random edges with delays of 1-5 macro steps; recurrent NetCons between cells
+    (min_cell_delay-2 ms).
     Returns (model, macro) with model built.
     """
     from mind_b200.macro import MacroModel
@@ -89,7 +90,7 @@ def coupled_regions(n_regions=3, cells_per_region=4, synapses=8, seed=11, input_
                    np.zeros(n))
     k = n // 4
     M.connect_many(model, rng.choice(detectors, k), rng.integers(first, first + n, k),
-                   rng.lognormal(math.log(2.0), 0.4, k) / 1000.0, rng.uniform(0.6, 2.0, k))
+                   rng.lognormal(math.log(2.0), 0.4, k) / 1000.0, rng.uniform(min_cell_delay, 2.0, k))
     macro = MacroModel(dt_macro=0.1, bin_ms=1.0)
     for r in range(n_regions):
         macro.add_region(micro_gain=2.0, y0=[0.0, rng.uniform(0, 5), rng.uniform(0, 5), 0.0, 0.0, 0.0])

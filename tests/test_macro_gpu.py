@@ -35,6 +35,27 @@ def test_coupled_regions_match_the_oracle_exactly():
     assert np.ptp(ref.macro_trace) > 0.5
 
 
+def test_unequal_windows_within_a_bin_match_the_oracle():
+    """Cell NetCons from 0.45 ms allow windows of 16 to 19 steps: the library runs 16-step
+    windows and ends one at every 40-step rate bin (16, 16, 8 per bin), and the run must
+    still equal the oracle's step-by-step restatement bit for bit."""
+    model, macro = netcases.coupled_regions(seed=12, min_cell_delay=0.45)
+    layout = model.layout
+    nodes = netcases.soma_nodes(layout)
+    steps = 1000
+    ref = oracle.run(layout, steps, nodes, macro=macro)
+    assert ref.status == 0, ref.message
+    mb.initialize(model)
+    assert model.state.window_steps() == 16
+    got = mb.run(model, steps * layout.dt, records=[mb.RecordSpec(n, f"n{n}") for n in nodes])
+    trace = np.stack([got.traces[f"n{n}"] for n in nodes], axis=1)
+    np.testing.assert_array_equal(trace, ref.trace)
+    np.testing.assert_array_equal(got.spike_sources, ref.spike_sids)
+    np.testing.assert_array_equal(got.spike_times, ref.spike_times)
+    np.testing.assert_array_equal(got.macro_trace, ref.macro_trace)
+    assert np.sum(ref.spike_sids <= layout.n_cells) > 3
+
+
 def test_split_runs_continue_the_regions():
     model, macro = netcases.coupled_regions(n_regions=2, cells_per_region=3)
     layout = model.layout
