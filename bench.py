@@ -67,6 +67,9 @@ def parse():
     p.add_argument("--surrogate", action="store_true",
                    help="config 4: train the spike-output surrogate on a detailed run, then time the coupled run "
                         "with 98%% of the cells replaced, against the plain FP64 run, and their region rates")
+    p.add_argument("--eval-ms", type=float, default=None,
+                   help="--surrogate: simulated time of the evaluation runs (default 1000 ms for config 4, "
+                        "100 ms for config 5); longer runs shrink the counting noise of the region rates")
     p.add_argument("--settle-ms", type=float, default=50.0,
                    help="simulated time advanced untimed before --warmup in both arms, so the timed steps run "
                         "on an active network (recurrent cell spikes, routing, NET_RECEIVE); config.t_start_ms")
@@ -549,7 +552,8 @@ def main():
     if args.surrogate:
         if rank == 0:
             measure = measure_config5 if args.config == 5 else measure_surrogate
-            print(json.dumps(measure(args, model, layout)), flush=True)
+            extra = {} if args.eval_ms is None else {"eval_ms": float(args.eval_ms)}
+            print(json.dumps(measure(args, model, layout, **extra)), flush=True)
         if dist is not None:
             dist.destroy_process_group()
         return
