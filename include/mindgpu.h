@@ -336,7 +336,8 @@ typedef struct {
 } MindMacroLayout;
 
 /* Attach regions and coupling to a created handle (before mind_initialize; allocation
- * happens here).  Runs then advance regions, inputs and rate bins with the micro steps. */
+ * happens here).  Runs then advance regions, inputs and rate bins with the micro steps.
+ * A handle with a spike exchange attached (mind_attach_exchange) is refused: MIND_EARG. */
 int mind_attach_macro(MindHandle *h, const MindMacroLayout *macro);
 
 /* The regions' outputs out(k) recorded by the last run for every macro step boundary it

@@ -1675,6 +1675,8 @@ int mind_initialize(MindHandle *h) {
 int mind_attach_macro(MindHandle *h, const MindMacroLayout *L) {
     if (!h || !L) return MIND_EARG;
     if (h->M.n > 0) return fail(h, MIND_EARG, "regions are already attached");
+    // the exchange fixed a window length all ranks share; regions would change it
+    if (h->ex_world) return fail(h, MIND_EARG, "a handle with a spike exchange attached takes no regions");
     const int32_t n = L->n_regions;
     if (n < 1 || n > 1024) return fail(h, MIND_ELAYOUT, "region count must be in [1, 1024]");
     if (!L->params || !L->y0 || !L->micro_gain) return fail(h, MIND_ELAYOUT, "missing region arrays");

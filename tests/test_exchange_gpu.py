@@ -101,6 +101,14 @@ def test_nccl_exchange_inside_mind_run_on_one_rank():
     try:
         run = sharding.ShardedRun(layout, 0, 1, precision="fp64", device="cpu", exchange="device")
         res = run.run_steps(int(round(T_STOP / layout.dt)), run.records(nodes))
+        # the ranks share the exchange's window length: regions, which set their own, are refused
+        from mind_b200 import abi
+        from mind_b200.macro import MacroModel
+        lone = MacroModel(dt_macro=0.1, bin_ms=1.0)
+        lone.add_region(micro_gain=0.0)
+        with pytest.raises(abi.MindError) as err:
+            run.state.attach_macro(lone)
+        assert err.value.status == abi.MIND_EARG
         run.close()
     finally:
         dist.destroy_process_group()
