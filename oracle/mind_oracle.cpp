@@ -34,6 +34,10 @@
  * own term first, then children in ascending node index; mechanism groups in
  * layout order; rows in row order.  The library uses the same order, which
  * makes FP64 parity bit-exact.  Both sides call mind_math.h for exp/log/pow.
+ * Built with -DMIND_ORACLE_LIBM (liboracle_libm.so, the Makefile's second target) the
+ * oracle takes exp, log and pow from the C library instead: a second, independently
+ * written faithful math library, against which the tests bound how much a run depends on
+ * the choice of math library (MIND.jl's device math being a third one).
  *
  * Threads: cells are independent between two event deliveries, so each step hands
  * whole cells (currents, cable assembly and solve, state advance) to a pool of worker
@@ -60,6 +64,20 @@
 #include <thread>
 
 namespace {
+
+// The oracle's elementary functions (see the header comment).
+#ifdef MIND_ORACLE_LIBM
+inline double oexp(double x) { return std::exp(x); }
+inline double olog(double x) { return std::log(x); }
+inline double opow(double x, double y) { return std::pow(x, y); }
+#else
+inline double oexp(double x) { return mind_exp(x); }
+inline double olog(double x) { return mind_log(x); }
+inline double opow(double x, double y) { return mind_pow(x, y); }
+#endif
+// alpha(x) = x e^(1-x) on [0, 10] (mod/AlphaSynapse.mod), and random_negexp = -log(u)
+inline double oalpha(double x) { return (x < 0.0 || x > 10.0) ? 0.0 : x * oexp(1.0 - x); }
+inline double onegexp(MindRan *s, uint64_t seed) { return -olog(mind_ran_uniform(s, seed)) * 1.0; }
 
 struct Event {
     double time;
@@ -238,7 +256,7 @@ struct Oracle {
     }
 
     static double sigmoid(double v, double e0, double r, double v0) {
-        return (2.0 * e0) / (1.0 + mind_exp(r * (v0 - v)));
+        return (2.0 * e0) / (1.0 + oexp(r * (v0 - v)));
     }
     static double region_output(const double *y, const double *par) { return sigmoid(y[1] - y[2], par[4], par[5], par[6]); }
     static void region_rhs(const double *y, double p, const double *par, double *dy) {
@@ -289,7 +307,7 @@ struct Oracle {
             uint32_t ctr[4] = {(uint32_t)k, (uint32_t)((uint64_t)k >> 32), (uint32_t)q, 0x4D4Du};
             mind_philox4x32_10(ctr, (uint32_t)seed, (uint32_t)(seed >> 32));
             const double u0 = ((double)ctr[0] + 1.0) * MIND_INV_2P32P1;
-            double pr = mind_exp(-mu), F = pr;
+            double pr = oexp(-mu), F = pr;
             int count = 0;
             while (u0 > F && count < 3) {
                 ++count;
@@ -426,7 +444,7 @@ struct Oracle {
         if (mean <= 0.0) mean = 0.01;
         double noise = G.f[NS_NOISE][r];
         if (noise == 0.0) return mean;
-        double erand = mind_ran_negexp(&ran[r], seed);
+        double erand = onegexp(&ran[r], seed);
         return (1.0 - noise) * mean + noise * mean * erand;
     }
     void init_sequence(Group &G, int64_t r) {
@@ -476,31 +494,31 @@ struct Oracle {
     // ---- hh rates (mod/hh.mod) ----
     static double vtrap(double x, double y) {
         if (std::fabs(x / y) < 1e-6) return y * (1.0 - x / y / 2.0);
-        return x / (mind_exp(x / y) - 1.0);
+        return x / (oexp(x / y) - 1.0);
     }
     struct Rates { double minf, hinf, ninf, mtau, htau, ntau; };
     Rates rates(double vv) const {
         Rates R;
-        double q10 = mind_pow(3.0, (celsius - 6.3) / 10.0);
+        double q10 = opow(3.0, (celsius - 6.3) / 10.0);
         double alpha = 0.1 * vtrap(-(vv + 40.0), 10.0);
-        double beta = 4.0 * mind_exp(-(vv + 65.0) / 18.0);
+        double beta = 4.0 * oexp(-(vv + 65.0) / 18.0);
         double sum = alpha + beta;
         R.mtau = 1.0 / (q10 * sum);
         R.minf = alpha / sum;
-        alpha = 0.07 * mind_exp(-(vv + 65.0) / 20.0);
-        beta = 1.0 / (mind_exp(-(vv + 35.0) / 10.0) + 1.0);
+        alpha = 0.07 * oexp(-(vv + 65.0) / 20.0);
+        beta = 1.0 / (oexp(-(vv + 35.0) / 10.0) + 1.0);
         sum = alpha + beta;
         R.htau = 1.0 / (q10 * sum);
         R.hinf = alpha / sum;
         alpha = 0.01 * vtrap(-(vv + 55.0), 10.0);
-        beta = 0.125 * mind_exp(-(vv + 65.0) / 80.0);
+        beta = 0.125 * oexp(-(vv + 65.0) / 80.0);
         sum = alpha + beta;
         R.ntau = 1.0 / (q10 * sum);
         R.ninf = alpha / sum;
         return R;
     }
     static double cnexp(double s, double inf, double tau, double step_dt) {
-        return s + (1.0 - mind_exp(step_dt * (-1.0 / tau))) * (inf - s);
+        return s + (1.0 - oexp(step_dt * (-1.0 / tau))) * (inf - s);
     }
 
     void initialize() {
@@ -536,8 +554,8 @@ struct Oracle {
                         if (tau1 / tau2 < 1e-9) tau1 = tau2 * 1e-9;
                         G.f[E2_A][r] = 0.0;
                         G.f[E2_B][r] = 0.0;
-                        double tp = (tau1 * tau2) / (tau2 - tau1) * mind_log(tau2 / tau1);
-                        double factor = -mind_exp(-tp / tau1) + mind_exp(-tp / tau2);
+                        double tp = (tau1 * tau2) / (tau2 - tau1) * olog(tau2 / tau1);
+                        double factor = -oexp(-tp / tau1) + oexp(-tp / tau2);
                         G.f[E2_FACTOR][r] = 1.0 / factor;
                     } break;
                     default: break;
@@ -712,7 +730,7 @@ struct Oracle {
                 value = 0.0 - i;
             } break;
             case MIND_MECH_ALPHASYN: {  // mod/AlphaSynapse.mod BREAKPOINT
-                double g = G.f[AS_GMAX][r] * mind_alpha((tc - G.f[AS_ONSET][r]) / G.f[AS_TAU][r]);
+                double g = G.f[AS_GMAX][r] * oalpha((tc - G.f[AS_ONSET][r]) / G.f[AS_TAU][r]);
                 shifted = 0.0 + g * (probe - G.f[AS_E][r]);
                 value = 0.0 + g * (vv - G.f[AS_E][r]);
             } break;

@@ -2,7 +2,9 @@
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU legs import this module;
 it is the checker for the CUDA path and the timed CPU baseline, never part of it.
-`build_oracle()` compiles liboracle.so with the Makefile beside this file.
+`build_oracle()` compiles liboracle.so with the Makefile beside this file, and
+liboracle_libm.so, the same restatement on the C library's exp, log and pow
+(`run(..., libm=True)`).
 """
 from __future__ import annotations
 
@@ -15,7 +17,8 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle.so")
-_LIB = None
+LIBM_PATH = os.path.join(HERE, "liboracle_libm.so")
+_LIBS = {}
 
 
 def build_oracle() -> str:
@@ -23,12 +26,12 @@ def build_oracle() -> str:
     return LIB_PATH
 
 
-def _load():
-    global _LIB
-    if _LIB is None:
-        if not os.path.exists(LIB_PATH):
+def _load(libm: bool = False):
+    path = LIBM_PATH if libm else LIB_PATH
+    if path not in _LIBS:
+        if not os.path.exists(path):
             build_oracle()
-        lib = ctypes.CDLL(LIB_PATH)
+        lib = ctypes.CDLL(path)
         lib.oracle_run.restype = ctypes.c_int32
         lib.oracle_run.argtypes = [
             ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
@@ -59,8 +62,8 @@ def _load():
         lib.oracle_negexp_stream.restype = None
         lib.oracle_negexp_stream.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int64,
                                              ctypes.POINTER(ctypes.c_double)]
-        _LIB = lib
-    return _LIB
+        _LIBS[path] = lib
+    return _LIBS[path]
 
 
 def exp(x: float) -> float:
@@ -133,13 +136,14 @@ def _oracle_kinds(layout, c_layout) -> None:
 
 
 def run(layout, steps: int, record_nodes=(), threads: int = 0, spike_cap: int = 1 << 22, macro=None,
-        records=None, timed_from: int = 0) -> OracleResult:
+        records=None, timed_from: int = 0, libm: bool = False) -> OracleResult:
     """Initialize the layout (and the regions of `macro`, a MacroModel) on the CPU and advance
     `steps` micro steps; with regions, `macro_trace` holds out(k) for k = 0 .. steps / (dt_macro/dt).
     `threads` worker threads (0: every host core) share the cells of each step; the result
     does not depend on their number.  `run_ms` times steps timed_from .. steps-1.
     `records` (objects with kind, node, group, row, field, such as RecordSpec) replaces
-    `record_nodes` (voltages of 1-based nodes) when given."""
+    `record_nodes` (voltages of 1-based nodes) when given.  libm=True runs the restatement
+    built on the C library's exp, log and pow instead of the project's (liboracle_libm.so)."""
     import sys
 
     pkg = os.path.join(os.path.dirname(HERE), "mind.jl_b200")
@@ -147,7 +151,7 @@ def run(layout, steps: int, record_nodes=(), threads: int = 0, spike_cap: int = 
         sys.path.insert(0, pkg)
     from mind_b200 import abi
 
-    lib = _load()
+    lib = _load(libm)
     if threads <= 0:
         threads = os.cpu_count() or 1
     c_layout = layout.to_c()
