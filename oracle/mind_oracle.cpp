@@ -37,7 +37,11 @@
  * Built with -DMIND_ORACLE_LIBM (liboracle_libm.so, the Makefile's second target) the
  * oracle takes exp, log and pow from the C library instead: a second, independently
  * written faithful math library, against which the tests bound how much a run depends on
- * the choice of math library (MIND.jl's device math being a third one).
+ * the choice of math library (MIND.jl's device math being a third one).  Built with
+ * -DMIND_ORACLE_REVERSED (liboracle_rev.so) it sums every order-dependent term in the
+ * opposite order (mechanism groups and rows into a node, children into a parent in the
+ * assembly and the elimination): another order the reference's atomics may take, against
+ * which the tests bound how much a run depends on that order.
  *
  * Threads: cells are independent between two event deliveries, so each step hands
  * whole cells (currents, cable assembly and solve, state advance) to a pool of worker
@@ -768,8 +772,24 @@ struct Oracle {
             rhs[i] = 0.0;
             d[i] = 0.0;
         }
+#ifdef MIND_ORACLE_REVERSED
+        for (size_t g = groups.size(); g-- > 0;)
+            for (auto r = cell_rows[c][g].rbegin(); r != cell_rows[c][g].rend(); ++r) current_row(groups[g], *r, tc);
+#else
         for (size_t g = 0; g < groups.size(); ++g)
             for (int64_t r : cell_rows[c][g]) current_row(groups[g], r, tc);
+#endif
+    }
+
+    /* The children of node i in the order their terms are summed into it: ascending, or
+     * descending in the reversed-order variant. */
+    template <class F>
+    void each_child(int32_t i, F f) const {
+#ifdef MIND_ORACLE_REVERSED
+        for (int64_t c = child_off[i + 1]; c-- > child_off[i];) f(child[c]);
+#else
+        for (int64_t c = child_off[i]; c < child_off[i + 1]; ++c) f(child[c]);
+#endif
     }
 
     int cable(int64_t cell) {
@@ -780,20 +800,16 @@ struct Oracle {
         for (int32_t i : up) {
             double R = rhs[i];
             if (parent[i] >= 0) R = R + a[i] * (v[parent[i]] - v[i]);
-            for (int64_t c = child_off[i]; c < child_off[i + 1]; ++c) {
-                int32_t k = child[c];
-                R = R - a[k] * (v[i] - v[k]);
-            }
+            each_child(i, [&](int32_t k) { R = R - a[k] * (v[i] - v[k]); });
             rhs[i] = R;
         }
         int status = 0;
         for (int32_t i : up) {
             double D = d[i], R = rhs[i];
-            for (int64_t c = child_off[i]; c < child_off[i + 1]; ++c) {
-                int32_t k = child[c];
+            each_child(i, [&](int32_t k) {
                 D = D - xd[k];
                 R = R + xr[k];
-            }
+            });
             d[i] = D;
             rhs[i] = R;
             if (D == 0.0 || !std::isfinite(D)) status = MIND_ESINGULAR;

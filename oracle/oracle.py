@@ -4,7 +4,8 @@ Only tests/, __graft_entry__.smoke() and bench.py's CPU legs import this module;
 it is the checker for the CUDA path and the timed CPU baseline, never part of it.
 `build_oracle()` compiles liboracle.so with the Makefile beside this file, and
 liboracle_libm.so, the same restatement on the C library's exp, log and pow
-(`run(..., libm=True)`).
+(`run(..., libm=True)`), and liboracle_rev.so, which sums the order-dependent terms in
+the opposite order (`run(..., reversed_order=True)`).
 """
 from __future__ import annotations
 
@@ -18,6 +19,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle.so")
 LIBM_PATH = os.path.join(HERE, "liboracle_libm.so")
+REV_PATH = os.path.join(HERE, "liboracle_rev.so")
 _LIBS = {}
 
 
@@ -26,8 +28,10 @@ def build_oracle() -> str:
     return LIB_PATH
 
 
-def _load(libm: bool = False):
-    path = LIBM_PATH if libm else LIB_PATH
+def _load(libm: bool = False, reversed_order: bool = False):
+    if libm and reversed_order:
+        raise ValueError("one oracle variant at a time")
+    path = LIBM_PATH if libm else REV_PATH if reversed_order else LIB_PATH
     if path not in _LIBS:
         if not os.path.exists(path):
             build_oracle()
@@ -136,14 +140,16 @@ def _oracle_kinds(layout, c_layout) -> None:
 
 
 def run(layout, steps: int, record_nodes=(), threads: int = 0, spike_cap: int = 1 << 22, macro=None,
-        records=None, timed_from: int = 0, libm: bool = False) -> OracleResult:
+        records=None, timed_from: int = 0, libm: bool = False, reversed_order: bool = False) -> OracleResult:
     """Initialize the layout (and the regions of `macro`, a MacroModel) on the CPU and advance
     `steps` micro steps; with regions, `macro_trace` holds out(k) for k = 0 .. steps / (dt_macro/dt).
     `threads` worker threads (0: every host core) share the cells of each step; the result
     does not depend on their number.  `run_ms` times steps timed_from .. steps-1.
     `records` (objects with kind, node, group, row, field, such as RecordSpec) replaces
     `record_nodes` (voltages of 1-based nodes) when given.  libm=True runs the restatement
-    built on the C library's exp, log and pow instead of the project's (liboracle_libm.so)."""
+    built on the C library's exp, log and pow instead of the project's (liboracle_libm.so);
+    reversed_order=True the one that sums mechanism rows into a node and children into a
+    parent in the opposite order (liboracle_rev.so)."""
     import sys
 
     pkg = os.path.join(os.path.dirname(HERE), "mind.jl_b200")
@@ -151,7 +157,7 @@ def run(layout, steps: int, record_nodes=(), threads: int = 0, spike_cap: int = 
         sys.path.insert(0, pkg)
     from mind_b200 import abi
 
-    lib = _load(libm)
+    lib = _load(libm, reversed_order)
     if threads <= 0:
         threads = os.cpu_count() or 1
     c_layout = layout.to_c()
