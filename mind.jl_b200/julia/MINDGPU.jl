@@ -6,6 +6,12 @@
 #   allocate_simulation / initialize!  ->  mindgpu_initialize!(model)
 #   run!(model, stop; records)         ->  mindgpu_run!(model, stop; records)
 #   step!(model)                       ->  mindgpu_step!(model)
+#   read_value(state, ref)             ->  mindgpu_read_value(model, ref)
+#   inject_spike!(state, input, t)     ->  mindgpu_inject_spikes!(model, sources, times)
+#   inject_event!(state, connection, t) -> mindgpu_inject_event!(model, connection, t)
+# and, with no reference counterpart: mindgpu_autotune!(model) (launch shape per size bin),
+# mindgpu_run_noalloc!(model, steps, refs, trace) (a run that allocates no device memory),
+# mindgpu_last_run_ms(model), mindgpu_window_steps(model).
 #
 # The model builders and build! are unchanged: the library receives the
 # ModelLayout.micro that build! packs (src/model/build.jl:15-60), as a POD view
@@ -236,5 +242,62 @@ end
 
 mindgpu_step!(model) = (check(model.runtime.state.ptr,
                               ccall((:mind_step, libmindgpu), Cint, (Ptr{Cvoid},), model.runtime.state.ptr)); model)
+
+"""inject_event!: deliver NetCon `connection` (1-based edge) at absolute time `time` (ms, not
+before the current time), as if its source had fired (src/runtime/state.jl:623-641)."""
+function mindgpu_inject_event!(model, connection::Integer, time::Real)
+    h = model.runtime.state::Handle
+    check(h.ptr, ccall((:mind_inject_event, libmindgpu), Cint, (Ptr{Cvoid}, Int64, Float64),
+                       h.ptr, Int64(connection), Float64(time)))
+    return model
+end
+
+"""Time the launch shapes of each size bin on `windows` trial windows and keep the fastest;
+leaves the model initialized at t = 0 (call right after mindgpu_initialize!).  Returns
+the threads per cell chosen for each bin."""
+function mindgpu_autotune!(model; windows::Integer = 4)
+    h = model.runtime.state::Handle
+    check(h.ptr, ccall((:mind_autotune, libmindgpu), Cint, (Ptr{Cvoid}, Int32), h.ptr, Int32(windows)))
+    n = Ref{Int32}(0)
+    check(h.ptr, ccall((:mind_bin_threads, libmindgpu), Cint, (Ptr{Cvoid}, Ptr{Int32}, Int32, Ref{Int32}),
+                       h.ptr, C_NULL, Int32(0), n))
+    threads = Vector{Int32}(undef, n[])
+    check(h.ptr, ccall((:mind_bin_threads, libmindgpu), Cint, (Ptr{Cvoid}, Ptr{Int32}, Int32, Ref{Int32}),
+                       h.ptr, threads, n[], n))
+    return threads
+end
+
+"""Advance `steps` micro steps without any device allocation (mind_run_noalloc), recording
+the references `refs` into `trace`, a caller-owned Matrix{Float64} of size
+(length(refs), steps + 1): column k holds sample k - 1 of every reference, the sample-major
+layout the library writes.  No spikes are recorded.  The record maps and the trace are
+staged in the library's static device array (MIND_NOALLOC_SCRATCH_BYTES); runs that need
+more are refused with status 3, and calls that overlap on one GPU race on that array."""
+function mindgpu_run_noalloc!(model, steps::Integer, refs, trace::Matrix{Float64})
+    h = model.runtime.state::Handle
+    recs = [c_record(ref) for ref in refs]
+    size(trace) == (length(recs), steps + 1) ||
+        throw(DimensionMismatch("trace must be $(length(recs)) x $(steps + 1)"))
+    check(h.ptr, ccall((:mind_run_noalloc, libmindgpu), Cint, (Ptr{Cvoid}, Int64, Ptr{MindRecord}, Int32, Ptr{Float64}),
+                       h.ptr, Int64(steps), recs, Int32(length(recs)), trace))
+    return trace
+end
+
+"""Device time of the last run (CUDA events around its loop), in milliseconds."""
+function mindgpu_last_run_ms(model)
+    h = model.runtime.state::Handle
+    ms = Ref{Float64}(0.0)
+    check(h.ptr, ccall((:mind_last_run_ms, libmindgpu), Cint, (Ptr{Cvoid}, Ref{Float64}), h.ptr, ms))
+    return ms[]
+end
+
+"""Micro steps a run advances between two routings of cell spikes (the shortest NetCon delay
+out of a cell bounds it): the exchange interval for hosts that shard one network."""
+function mindgpu_window_steps(model)
+    h = model.runtime.state::Handle
+    w = Ref{Int32}(0)
+    check(h.ptr, ccall((:mind_window_steps, libmindgpu), Cint, (Ptr{Cvoid}, Ref{Int32}), h.ptr, w))
+    return Int(w[])
+end
 
 end # module
