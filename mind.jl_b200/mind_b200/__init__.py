@@ -7,7 +7,7 @@ the host; every simulation step runs in the CUDA library through its C-ABI.
 """
 from .mechanisms import Mechanism, builtin, compile_mod, compiled_mechanisms, emitted, load_mod, register_mod
 from .morphology import Point3D, Section, discretize, location_node
-from .model import (Cell, IonSpecies, MicroModel, PointProcess, Population, SpikeSource,
+from .model import (Cell, IonSpecies, MicroModel, PointProcess, Population, SpikeSource, ghk, nernst,
                     add_pointprocess, add_pointprocesses, add_population, connect, connect_many,
                     insert, register_external_sources, register_point_sources, register_spike_source, spike_source)
 from .layout import Layout, build
@@ -17,7 +17,7 @@ from .runtime import (RecordSpec, SimulationResult, autotune, connection_weights
 
 __all__ = [
     "Mechanism", "builtin", "compile_mod", "compiled_mechanisms", "emitted", "load_mod", "register_mod", "Point3D", "Section", "discretize", "location_node", "Cell",
-    "IonSpecies", "MicroModel", "PointProcess", "Population", "SpikeSource", "add_pointprocess",
+    "IonSpecies", "MicroModel", "PointProcess", "Population", "SpikeSource", "ghk", "nernst", "add_pointprocess",
     "add_pointprocesses", "add_population", "connect", "connect_many", "insert",
     "register_external_sources", "register_point_sources", "register_spike_source", "spike_source", "Layout", "build",
     "RecordSpec", "SimulationResult", "autotune", "connection_weights", "initialize", "inject_event",

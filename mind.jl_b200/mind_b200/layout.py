@@ -258,7 +258,7 @@ def build(model, *, dt_micro: float = 0.025, seed: int = 1, event_capacity: Opti
                 for fld, ion in mech.ion_reads:
                     override = model.cells[ci].ions.get(fld)
                     data[cursor:cursor + n, mech.field_index(fld)] = (
-                        override if override is not None else model.ions[ion].reversal)
+                        override if override is not None else model.ions[ion].reversal_at(model.celsius))
                 cursor += n
             order = np.argsort(nodes, kind="stable")
             nodes = nodes[order]

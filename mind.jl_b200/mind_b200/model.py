@@ -22,15 +22,79 @@ from .mechanisms import Mechanism, resolve_mechanism
 from .morphology import Section, discretize, MorphologyLayout
 
 
+# Gas constant and Faraday constant, mV/mM units (src/model/micro/utils/biophysics.jl:47-48)
+_GAS_CONSTANT = 1.380649e-23 * 6.02214076e23
+_FARADAY = 1.602176634e-19 * 6.02214076e23
+
+
+def _validate_ion_arguments(internal, external, valence, celsius) -> None:
+    if not (all(math.isfinite(x) for x in (internal, external, valence, celsius)) and internal >= 0
+            and external >= 0 and celsius > -273.15):
+        raise ValueError("invalid ion arguments")
+
+
+def nernst_potential(internal: float, external: float, valence: float, celsius: float) -> float:
+    """Reversal potential (mV) of concentrations in mM, with the reference's limits: 0 for
+    valence 0, +1e6 for no internal and -1e6 for no external concentration
+    (src/model/micro/utils/biophysics.jl:43-51; the same operation order)."""
+    if valence == 0.0:
+        return 0.0
+    if internal <= 0.0:
+        return 1.0e6
+    if external <= 0.0:
+        return -1.0e6
+    return (1000.0 * _GAS_CONSTANT * (celsius + 273.15) / _FARADAY) / valence * math.log(external / internal)
+
+
+def nernst(internal: float, external: float, valence: float, *, celsius: float = 6.3) -> float:
+    """nernst (src/model/micro/biophysics.jl:53-61): validated nernst_potential."""
+    _validate_ion_arguments(internal, external, valence, celsius)
+    return nernst_potential(float(internal), float(external), float(valence), float(celsius))
+
+
+def ghk(voltage: float, internal: float, external: float, valence: float, *, celsius: float = 6.3) -> float:
+    """Goldman-Hodgkin-Katz current factor in NEURON's mV and mM conventions, with its
+    small-argument branch (src/model/micro/biophysics.jl:63-74,
+    src/model/micro/utils/biophysics.jl:53-70)."""
+    _validate_ion_arguments(internal, external, valence, celsius)
+    if not math.isfinite(voltage):
+        raise ValueError("voltage must be finite")
+    thermal_voltage = 1000.0 * _GAS_CONSTANT * (float(celsius) + 273.15) / _FARADAY
+    scaled = float(valence) * float(voltage) / thermal_voltage
+
+    def quotient(x):
+        return 1.0 - x / 2.0 if abs(x) < 1.0e-4 else x / (math.exp(x) - 1.0)
+
+    return 0.001 * float(valence) * _FARADAY * (float(internal) * quotient(-scaled) - float(external) * quotient(scaled))
+
+
 @dataclass(frozen=True)
 class IonSpecies:
-    """Ion species defaults (src/model/micro/utils/biophysics.jl:31-41)."""
+    """Ion species defaults (src/model/micro/utils/biophysics.jl:31-41).  With nernst=True the
+    species' reversal potential is the Nernst potential of its concentrations at the model's
+    temperature (src/model/micro/model.jl:766-768); concentrations stay at these values,
+    since no mechanism here writes them, so that reversal holds for the whole run."""
 
     name: str
     valence: int
     internal: float
     external: float
-    reversal: float
+    reversal: float = 0.0
+    nernst: bool = False
+
+    def __post_init__(self):
+        if not math.isfinite(self.valence):
+            raise ValueError("ion valence must be finite")
+        if not all(math.isfinite(x) for x in (self.internal, self.external, self.reversal)):
+            raise ValueError("non-finite ion parameter")
+        if self.internal < 0 or self.external < 0:
+            raise ValueError("ion concentrations must be nonnegative")
+
+    def reversal_at(self, celsius: float) -> float:
+        """The reversal a mechanism's USEION READ e<ion> sees on a node without an override."""
+        if self.nernst:
+            return nernst_potential(float(self.internal), float(self.external), float(self.valence), float(celsius))
+        return self.reversal
 
 
 def default_ions() -> Dict[str, IonSpecies]:
