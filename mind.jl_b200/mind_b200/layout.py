@@ -277,6 +277,18 @@ def build(model, *, dt_micro: float = 0.025, seed: int = 1, event_capacity: Opti
                     nodes[cursor:cursor + c.count] = _point_nodes(model, morphs, offsets, c)
                 for name, value in c.params.items():
                     data[cursor:cursor + c.count, mech.field_index(name)] = value
+                if mech.kind == "point" and mech.ion_reads:
+                    # USEION READ e<ion>: the species' reversal, or the owning cell's own value
+                    # (the reference loads these from the ion table before BREAKPOINT,
+                    # src/runtime/cuda/micro.jl:436-438, so they take precedence over params)
+                    cells = np.broadcast_to(np.asarray(c.cells, dtype=np.int64), (c.count,))
+                    for fld, ion in mech.ion_reads:
+                        col = np.full(c.count, model.ions[ion].reversal_at(model.celsius))
+                        for ci in np.unique(cells[cells > 0]):
+                            override = model.cells[int(ci) - 1].ions.get(fld)
+                            if override is not None:
+                                col[cells == ci] = override
+                        data[cursor:cursor + c.count, mech.field_index(fld)] = col
                 cursor += c.count
             if mech.kind == "point":
                 order = np.argsort(nodes, kind="stable")

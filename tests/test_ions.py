@@ -91,3 +91,23 @@ def test_a_nernst_species_runs_as_its_fixed_equivalent():
     ra, rb = oracle.run(a, 400, [1, 2]), oracle.run(b, 400, [1, 2])
     assert ra.status == 0 and rb.status == 0
     np.testing.assert_array_equal(ra.trace, rb.trace)
+
+
+def test_point_processes_read_their_ion_reversal_too():
+    """A point mechanism with USEION na READ ena (a descriptor such as compile_mod returns)
+    gets the species' reversal, or its cell's own value, whatever its parameters say."""
+    from mind_b200.mechanisms import Mechanism
+
+    probe = Mechanism("NaProbe", "point", 99, ("gmax", "ena", "i"), (0.001, 0.0, 0.0), 1, 0, (("ena", "na"),))
+    model = M.MicroModel(ions=[mb.IonSpecies("na", 1, 15.0, 145.0, nernst=True)])
+    soma = mb.Section("soma", label="soma", length=20.0, diameter=20.0, nseg=1)
+    cells = M.add_population(model, [soma], 2, voltage=-65.0)
+    model.cells[cells[1].index - 1].ions["ena"] = 45.0
+    for cell in (cells[0], cells[1], cells[1]):
+        M.add_pointprocess(cell, probe, params={"ena": -1.0})
+    layout = mb.build(model)
+    group = next(g for g in layout.groups if g.mechanism.name == "NaProbe")
+    by_node = dict(zip(group.nodes.tolist(), group.data[:, 1].tolist()))
+    assert len(group.nodes) == 3
+    np.testing.assert_array_equal(sorted(group.data[:, 1]), sorted([mb.nernst(15.0, 145.0, 1), 45.0, 45.0]))
+    assert by_node[min(by_node)] == mb.nernst(15.0, 145.0, 1)      # cell 1's node comes first
