@@ -18,6 +18,7 @@
 #include <cuda_runtime.h>
 #include <dlfcn.h>
 #include <nccl.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <array>
@@ -1341,7 +1342,17 @@ void launch_window(const MindHandle *h, const MindHandle::Bin &bin, cudaStream_t
  * sticky error (a lost context) is not cleared by this and fails the next call. */
 void clear_foreign_error() { (void)cudaGetLastError(); }
 
+/* A named NVTX range for the lifetime of a scope: runs and their windows show up by name on
+ * an Nsight timeline.  Without a profiler attached the calls do nothing. */
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
+
 int advance(MindHandle *h, int64_t steps, bool record_spikes) {
+    const NvtxRange run_range("mind run");
     clear_foreign_error();
     Params &P = h->P;
     P.record_spikes = record_spikes ? 1 : 0;
@@ -1372,6 +1383,7 @@ int advance(MindHandle *h, int64_t steps, bool record_spikes) {
         ++st.launches;
     }
     while (n0 < end) {
+        const NvtxRange window_range("mind window");
         int32_t W = (int32_t)std::min<int64_t>(h->window, end - n0);
         // With regions attached, a window ends at the next rate-bin boundary at the latest,
         // so every bin the regions read is complete.
