@@ -5,7 +5,8 @@ The Julia names map one to one (`add_population!` -> `add_population`,
 `run!` -> `run`, `step!` -> `step`).  Model construction and packing run on
 the host; every simulation step runs in the CUDA library through its C-ABI.
 """
-from .mechanisms import Mechanism, builtin, compile_mod, compiled_mechanisms, emitted, load_mod, register_mod
+from .mechanisms import (Mechanism, builtin, clear_mod_cache, compile_mod, compiled_mechanisms, emitted, load_mod,
+                         mechanism_ir, register_mod)
 from .morphology import Point3D, Section, discretize, location_node
 from .model import (Cell, IonSpecies, MicroModel, PointProcess, Population, SpikeSource, ghk, nernst,
                     add_pointprocess, add_pointprocesses, add_population, connect, connect_many,
@@ -16,7 +17,8 @@ from .runtime import (RecordSpec, SimulationResult, autotune, connection_weights
                       simulation_time, step, voltage_record, voltage_ref)
 
 __all__ = [
-    "Mechanism", "builtin", "compile_mod", "compiled_mechanisms", "emitted", "load_mod", "register_mod", "Point3D", "Section", "discretize", "location_node", "Cell",
+    "Mechanism", "builtin", "clear_mod_cache", "compile_mod", "compiled_mechanisms", "emitted", "load_mod",
+    "mechanism_ir", "register_mod", "Point3D", "Section", "discretize", "location_node", "Cell",
     "IonSpecies", "MicroModel", "PointProcess", "Population", "SpikeSource", "ghk", "nernst", "add_pointprocess",
     "add_pointprocesses", "add_population", "connect", "connect_many", "insert",
     "register_external_sources", "register_point_sources", "register_spike_source", "spike_source", "Layout", "build",

@@ -15,8 +15,9 @@ reference's mod/*.mod files; only NetStim draws random numbers.
 """
 from __future__ import annotations
 
+import dataclasses
 from dataclasses import dataclass, field
-from typing import Dict, Tuple
+from typing import Any, Dict, Tuple
 
 # C-ABI kind codes (include/mindgpu.h).
 MIND_MECH_HH = 1
@@ -42,6 +43,9 @@ class Mechanism:
     receive_arity: int = 0
     # Fields filled from ion species at build time (USEION ... READ e<ion>).
     ion_reads: Tuple[Tuple[str, str], ...] = field(default_factory=tuple)
+    # The lowered MOD (mind_b200.nmodl.cuda.MechanismIR) when this process compiled the
+    # source (compile_mod, load_mod, register_mod); None for hand-written device code.
+    ir: Any = field(default=None, compare=False, repr=False)
 
     def field_index(self, name: str) -> int:
         try:
@@ -189,7 +193,7 @@ def compile_mod(source: str, filename: str = "<string>") -> Mechanism:
     if compiled.fields != ir.field_names:
         raise ValueError(f"{ir.name}: the library's fields differ from this source's")
     return Mechanism(ir.name, ir.kind, compiled.code, compiled.fields, compiled.defaults, ir.digest,
-                     len(ir.receive_args), tuple(ir.ion_reads))
+                     len(ir.receive_args), tuple(ir.ion_reads), ir)
 
 
 _RUNTIME = []   # MechanismIR of the mechanisms compiled at run time, in registry order
@@ -209,7 +213,7 @@ def register_mod(source: str, filename: str = "<string>") -> Mechanism:
     if known is not None:
         if known.digest != ir.digest:
             raise ValueError(f"{ir.name} ({filename}) differs from the {ir.name} this process already knows")
-        return known
+        return dataclasses.replace(known, ir=ir)
     return _register(ir)
 
 
@@ -281,7 +285,26 @@ def _register(ir) -> Mechanism:
         raise abi.MindError(status, (lib.mind_last_error(None) or b"").decode())
     _RUNTIME.append(ir)
     _COMPILED = None
-    return compiled_mechanisms()[ir.name]
+    return dataclasses.replace(compiled_mechanisms()[ir.name], ir=ir)
+
+
+def mechanism_ir(mechanism: Mechanism):
+    """mechanism_ir (src/compiler/ir.jl:359): the lowered MOD of a mechanism this process
+    compiled (compile_mod, load_mod, register_mod): its fields, currents, ion reads, NET_RECEIVE
+    arguments and blocks."""
+    if mechanism.ir is None:
+        raise ValueError(f"{mechanism.name} has no IR in this process: it runs hand-written device code or "
+                         "came from the library's registry; load its MOD file with load_mod")
+    return mechanism.ir
+
+
+def clear_mod_cache() -> None:
+    """clear_mod_cache! (src/compiler/frontend.jl:113-120): forget this process's view of the
+    library's mechanism registry, which the next lookup reads again.  Mechanisms compiled at
+    run time stay registered: the registry is append-only, so handles and kind codes made
+    from them stay valid."""
+    global _COMPILED
+    _COMPILED = None
 
 
 def load_mod(path: str) -> Mechanism:

@@ -141,6 +141,24 @@ def test_reference_mod_directory_parses_and_regenerates_the_committed_header():
         assert mb.load_mod(os.path.join(MOD_DIR, f"{name}.mod")).code == mb.compiled_mechanisms()[name].code
 
 
+@pytest.mark.skipif(not os.path.isdir(MOD_DIR), reason="MIND.jl checkout not present")
+def test_mechanism_ir_of_a_compiled_mod_and_clear_mod_cache():
+    """mechanism_ir gives the lowered MOD of what compile_mod returned; clear_mod_cache drops
+    the cached view of the library's registry, which reads back the same."""
+    seclamp = mb.load_mod(os.path.join(MOD_DIR, "SEClamp.mod"))
+    ir = mb.mechanism_ir(seclamp)
+    assert ir.name == "SEClamp" and ir.kind == "point"
+    assert tuple(ir.field_names) == seclamp.fields and ir.digest == seclamp.digest
+    before = mb.compiled_mechanisms()
+    mb.clear_mod_cache()
+    assert mb.compiled_mechanisms() == before
+
+
+def test_hand_written_builtins_have_no_ir():
+    with pytest.raises(ValueError, match="hand-written"):
+        mb.mechanism_ir(mb.builtin("hh"))
+
+
 def test_a_user_mod_compiles_into_a_mechanism_module_for_sm_100a():
     """register_mod's compile step, without a GPU: a MOD file the library was not built with
     is emitted after the compiled-in mechanisms and the window kernel's generated variants
